@@ -1,0 +1,166 @@
+"""Seeded procedural workloads for the intersection and path-tracing paths.
+
+Nothing here is a reference dataset: the reference ships no scenes, so every
+workload is generated from a seed with the shapes and sizes it is quoted on.
+
+* ``heightfield`` - a W x H grid of cells over [0,1]^2, two triangles per cell,
+  height = amplitude * value-noise fBm. The noise is defined here: a PCG
+  lattice hash of (ix, iy, octave, seed) mapped to [0,1), smoothstep
+  interpolation, base frequency 8, lacunarity 2, gain 0.5, normalised to [0,1).
+* ``coherent_rays`` - one pinhole ray per pixel centre.
+* ``incoherent_rays`` - origins uniform on random triangles (uniform triangle
+  index, point by the reference's UniformSampleTriangle warp,
+  Core/Maths/Montecarlo.h:59-64), lifted 1e-4 along the +z-facing geometric
+  normal, directions cosine-distributed about that normal
+  (Montecarlo.h:31-37 in the frame of Core/Geometry/Basis.cpp:85-99).
+
+Rays are two float32 (N, 4) arrays: (ox, oy, oz, tmin) and (dx, dy, dz, tmax).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+FLT_MAX = np.float32(np.finfo(np.float32).max)
+
+_M32 = np.uint64(0xFFFFFFFF)
+
+
+def _pcg_hash(x: np.ndarray) -> np.ndarray:
+    """32-bit PCG output permutation of a linear step (Jarzynski & Olano 2020)."""
+    x = x.astype(np.uint64) & _M32
+    state = (x * np.uint64(747796405) + np.uint64(2891336453)) & _M32
+    shift = (state >> np.uint64(28)) + np.uint64(4)
+    word = (((state >> shift) ^ state) * np.uint64(277803737)) & _M32
+    return ((word >> np.uint64(22)) ^ word) & _M32
+
+
+def _lattice(ix, iy, octave: int, seed: int) -> np.ndarray:
+    h = _pcg_hash(np.full(np.shape(ix), seed, dtype=np.uint64))
+    h = _pcg_hash(h + np.uint64(octave))
+    h = _pcg_hash(h + (np.asarray(iy).astype(np.int64).astype(np.uint64) & _M32))
+    h = _pcg_hash(h + (np.asarray(ix).astype(np.int64).astype(np.uint64) & _M32))
+    return h.astype(np.float64) * (1.0 / 4294967296.0)
+
+
+def value_noise_fbm(x, y, seed: int = 1, octaves: int = 6, base_freq: float = 8.0,
+                    lacunarity: float = 2.0, gain: float = 0.5) -> np.ndarray:
+    x = np.asarray(x, dtype=np.float64)
+    y = np.asarray(y, dtype=np.float64)
+    total = np.zeros(np.broadcast(x, y).shape)
+    norm = 0.0
+    freq, amp = base_freq, 1.0
+    for o in range(octaves):
+        X, Y = x * freq, y * freq
+        ix, iy = np.floor(X), np.floor(Y)
+        fx, fy = X - ix, Y - iy
+        sx, sy = fx * fx * (3 - 2 * fx), fy * fy * (3 - 2 * fy)
+        v00 = _lattice(ix, iy, o, seed)
+        v10 = _lattice(ix + 1, iy, o, seed)
+        v01 = _lattice(ix, iy + 1, o, seed)
+        v11 = _lattice(ix + 1, iy + 1, o, seed)
+        a = v00 + (v10 - v00) * sx
+        b = v01 + (v11 - v01) * sx
+        total += amp * (a + (b - a) * sy)
+        norm += amp
+        freq *= lacunarity
+        amp *= gain
+    return total / norm
+
+
+def heightfield(nx: int = 1024, ny: int = 512, amplitude: float = 0.2, seed: int = 1):
+    """Return (positions float32 (V,3), indices uint32 (T,3)) with T = 2*nx*ny."""
+    gx = np.arange(nx + 1, dtype=np.float64) / nx
+    gy = np.arange(ny + 1, dtype=np.float64) / ny
+    X, Y = np.meshgrid(gx, gy)                      # (ny+1, nx+1)
+    Z = amplitude * value_noise_fbm(X, Y, seed=seed)
+    pos = np.stack([X, Y, Z], axis=-1).reshape(-1, 3).astype(np.float32)
+    i = np.arange(nx)[None, :]
+    j = np.arange(ny)[:, None]
+    a = j * (nx + 1) + i
+    b = a + 1
+    c = a + (nx + 1) + 1
+    d = a + (nx + 1)
+    t0 = np.stack([a, b, c], axis=-1)
+    t1 = np.stack([a, c, d], axis=-1)
+    idx = np.stack([t0, t1], axis=2).reshape(-1, 3).astype(np.uint32)
+    return pos, idx
+
+
+def _normalize(v):
+    return v / np.linalg.norm(v, axis=-1, keepdims=True)
+
+
+def pinhole_rays(width: int, height: int, eye, look_at, up, vfov_deg: float):
+    """One ray per pixel centre, row-major, rows top to bottom."""
+    eye = np.asarray(eye, np.float64)
+    fwd = _normalize(np.asarray(look_at, np.float64) - eye)
+    right = _normalize(np.cross(fwd, np.asarray(up, np.float64)))
+    upv = np.cross(right, fwd)
+    th = np.tan(np.radians(vfov_deg) * 0.5)
+    aspect = width / height
+    px = (np.arange(width) + 0.5) / width * 2 - 1
+    py = 1 - (np.arange(height) + 0.5) / height * 2
+    PX, PY = np.meshgrid(px * th * aspect, py * th)
+    d = fwd[None, None, :] + PX[..., None] * right + PY[..., None] * upv
+    d = _normalize(d).reshape(-1, 3)
+    n = d.shape[0]
+    o4 = np.empty((n, 4), np.float32)
+    d4 = np.empty((n, 4), np.float32)
+    o4[:, :3] = eye
+    o4[:, 3] = 0.0
+    d4[:, :3] = d
+    d4[:, 3] = FLT_MAX
+    return o4, d4
+
+
+def coherent_rays(side: int = 2048):
+    return pinhole_rays(side, side, (0.5, -0.6, 0.8), (0.5, 0.5, 0.0), (0, 0, 1), 60.0)
+
+
+def onb_from_w(w):
+    """Frame of Core/Geometry/Basis.cpp:85-99 (InitFromW), vectorised."""
+    w = _normalize(w)
+    use_x = np.abs(w[:, 0]) > np.abs(w[:, 1])
+    v = np.empty_like(w)
+    inv_a = 1.0 / np.sqrt(w[:, 0] ** 2 + w[:, 2] ** 2)
+    inv_b = 1.0 / np.sqrt(w[:, 1] ** 2 + w[:, 2] ** 2)
+    v[:, 0] = np.where(use_x, -w[:, 2] * inv_a, 0.0)
+    v[:, 1] = np.where(use_x, 0.0, w[:, 2] * inv_b)
+    v[:, 2] = np.where(use_x, w[:, 0] * inv_a, -w[:, 1] * inv_b)
+    u = np.cross(w, v)
+    return u, v, w
+
+
+def incoherent_rays(pos, idx, n: int = 4194304, seed: int = 2, offset: float = 1e-4):
+    rng = np.random.Generator(np.random.PCG64(seed))
+    tri = rng.integers(0, idx.shape[0], size=n)
+    u1, u2, u3, u4 = (rng.random(n) for _ in range(4))
+    p0 = pos[idx[tri, 0]].astype(np.float64)
+    p1 = pos[idx[tri, 1]].astype(np.float64)
+    p2 = pos[idx[tri, 2]].astype(np.float64)
+    su = np.sqrt(u1)
+    b0 = 1.0 - su
+    b1 = u2 * su
+    p = b0[:, None] * p0 + b1[:, None] * p1 + (1.0 - b0 - b1)[:, None] * p2
+    nrm = _normalize(np.cross(p1 - p0, p2 - p0))
+    nrm = np.where(nrm[:, 2:3] < 0, -nrm, nrm)
+    U, V, W = onb_from_w(nrm)
+    a = 2 * np.pi * u4
+    r = np.sqrt(u3)
+    lx, ly, lz = r * np.cos(a), r * np.sin(a), np.sqrt(np.maximum(0.0, 1 - u3))
+    d = _normalize(lx[:, None] * U + ly[:, None] * V + lz[:, None] * W)
+    o4 = np.empty((n, 4), np.float32)
+    d4 = np.empty((n, 4), np.float32)
+    o4[:, :3] = p + offset * nrm
+    o4[:, 3] = 0.0
+    d4[:, :3] = d
+    d4[:, 3] = FLT_MAX
+    return o4, d4
+
+
+def ray_batch_workload(nx=1024, ny=512, side=2048, n_incoherent=4194304, seed=1):
+    """The 1,048,576-triangle heightfield with coherent + incoherent ray sets."""
+    pos, idx = heightfield(nx, ny, 0.2, seed)
+    co, cd = coherent_rays(side)
+    io, idr = incoherent_rays(pos, idx, n_incoherent, seed + 1)
+    return pos, idx, (co, cd), (io, idr)

@@ -1,0 +1,153 @@
+"""ctypes bindings for the two CPU checkers - TEST INFRASTRUCTURE ONLY.
+
+* ``Oracle``: our C restatement of the reference's query (oracle/ilg_oracle.c).
+* ``RefLib``: the reference's own sources compiled by oracle/Makefile into
+  oracle/_ref/libilref.so (present only where the reference tree was
+  available at build time, or where the built library was carried along).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libilref.so")
+REF_TREE = "/root/reference/Core"
+
+_f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+_u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
+_i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+_u8p = np.ctypeslib.ndpointer(np.uint8, flags="C_CONTIGUOUS")
+_u64p = np.ctypeslib.ndpointer(np.uint64, flags="C_CONTIGUOUS")
+
+
+def build(ref: bool = True) -> None:
+    """Compile the oracle (always) and the reference library (when its tree exists)."""
+    subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
+    if ref and os.path.isdir(REF_TREE):
+        subprocess.run(["make", "-s", "-j8", "-C", HERE, "ref", f"REF={REF_TREE}"], check=True)
+
+
+def _ensure_oracle():
+    srcs = [os.path.join(HERE, f) for f in ("ilg_oracle.c", "ilg_oracle.h")]
+    if not os.path.exists(ORACLE_SO) or any(os.path.getmtime(s) > os.path.getmtime(ORACLE_SO) for s in srcs):
+        subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
+
+
+class Oracle:
+    def __init__(self):
+        _ensure_oracle()
+        L = ctypes.CDLL(ORACLE_SO)
+        L.orc_shirley.argtypes = [_f32p, _u32p, ctypes.c_uint32, _f32p, _f32p, ctypes.c_float,
+                                  ctypes.POINTER(ctypes.c_float), ctypes.POINTER(ctypes.c_float),
+                                  ctypes.POINTER(ctypes.c_float)]
+        L.orc_shirley.restype = ctypes.c_int
+        L.orc_intersect_brute.argtypes = [_f32p, _u32p, ctypes.c_uint32, _f32p, _f32p, ctypes.c_int64,
+                                          _i32p, _f32p, _f32p, _f32p]
+        L.orc_bvh_create.argtypes = [_f32p, ctypes.c_uint32, _u32p, ctypes.c_uint32]
+        L.orc_bvh_create.restype = ctypes.c_void_p
+        L.orc_bvh_destroy.argtypes = [ctypes.c_void_p]
+        L.orc_bvh_intersect.argtypes = [ctypes.c_void_p, _f32p, _f32p, ctypes.c_int64, _i32p, _f32p, _f32p,
+                                        _f32p, ctypes.c_int, ctypes.c_void_p]
+        L.orc_bvh_occluded.argtypes = [ctypes.c_void_p, _f32p, _f32p, ctypes.c_int64, _u8p, ctypes.c_int]
+        self.L = L
+
+    def shirley(self, pos, idx, tri, o, d, tmax=np.finfo(np.float32).max):
+        t, b, g = ctypes.c_float(), ctypes.c_float(), ctypes.c_float()
+        ok = self.L.orc_shirley(pos, idx, int(tri), np.ascontiguousarray(o[:3], np.float32),
+                                np.ascontiguousarray(d[:3], np.float32), float(tmax),
+                                ctypes.byref(t), ctypes.byref(b), ctypes.byref(g))
+        return bool(ok), t.value, b.value, g.value
+
+    def intersect_brute(self, pos, idx, o4, d4):
+        n = o4.shape[0]
+        out = (np.empty(n, np.int32), np.empty(n, np.float32), np.empty(n, np.float32), np.empty(n, np.float32))
+        self.L.orc_intersect_brute(pos, idx.reshape(-1), idx.shape[0], o4, d4, n, *out)
+        return out
+
+    def bvh(self, pos, idx):
+        return OracleBVH(self, pos, idx)
+
+
+class OracleBVH:
+    def __init__(self, orc: Oracle, pos, idx):
+        self.o = orc
+        self.pos = np.ascontiguousarray(pos, np.float32)
+        self.idx = np.ascontiguousarray(idx, np.uint32)
+        self.h = orc.L.orc_bvh_create(self.pos.reshape(-1), self.pos.shape[0], self.idx.reshape(-1), self.idx.shape[0])
+
+    def intersect(self, o4, d4, nthreads=None, stats=False):
+        n = o4.shape[0]
+        nthreads = nthreads or os.cpu_count() or 1
+        out = (np.empty(n, np.int32), np.empty(n, np.float32), np.empty(n, np.float32), np.empty(n, np.float32))
+        st = np.zeros(2, np.uint64)
+        self.o.L.orc_bvh_intersect(self.h, o4, d4, n, *out, nthreads, st.ctypes.data)
+        return (out, st) if stats else out
+
+    def occluded(self, o4, d4, nthreads=None):
+        n = o4.shape[0]
+        occ = np.empty(n, np.uint8)
+        self.o.L.orc_bvh_occluded(self.h, o4, d4, n, occ, nthreads or os.cpu_count() or 1)
+        return occ
+
+    def __del__(self):
+        try:
+            self.o.L.orc_bvh_destroy(self.h)
+        except Exception:
+            pass
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+class RefLib:
+    """The reference's BasicSpace -> KDTreeMesh / BVHMesh path (compiled)."""
+
+    def __init__(self):
+        if not ref_available():
+            raise FileNotFoundError(REF_SO)
+        L = ctypes.CDLL(REF_SO)
+        L.ilref_mesh_create.argtypes = [ctypes.c_int, _f32p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int]
+        L.ilref_mesh_create.restype = ctypes.c_void_p
+        L.ilref_mesh_destroy.argtypes = [ctypes.c_void_p]
+        L.ilref_mesh_build_seconds.argtypes = [ctypes.c_void_p]
+        L.ilref_mesh_build_seconds.restype = ctypes.c_double
+        L.ilref_intersect.argtypes = [ctypes.c_void_p, _f32p, _f32p, ctypes.c_long, _i32p, _f32p, _f32p, _f32p,
+                                      ctypes.c_int]
+        L.ilref_occluded.argtypes = [ctypes.c_void_p, _f32p, _f32p, ctypes.c_long, _u8p, ctypes.c_int]
+        self.L = L
+
+    def mesh(self, pos, idx, kind: str = "bvh"):
+        return RefMesh(self, pos, idx, 0 if kind == "kd" else 1)
+
+
+class RefMesh:
+    def __init__(self, lib: RefLib, pos, idx, kind: int):
+        self.lib = lib
+        pos = np.ascontiguousarray(pos, np.float32)
+        idx32 = np.ascontiguousarray(idx, np.int32)
+        self.h = lib.L.ilref_mesh_create(kind, pos.reshape(-1), pos.shape[0], idx32.ctypes.data, idx32.shape[0])
+        self.build_seconds = lib.L.ilref_mesh_build_seconds(self.h)
+
+    def intersect(self, o4, d4, nthreads=None):
+        n = o4.shape[0]
+        out = (np.empty(n, np.int32), np.empty(n, np.float32), np.empty(n, np.float32), np.empty(n, np.float32))
+        self.lib.L.ilref_intersect(self.h, o4, d4, n, *out, nthreads or os.cpu_count() or 1)
+        return out
+
+    def occluded(self, o4, d4, nthreads=None):
+        n = o4.shape[0]
+        occ = np.empty(n, np.uint8)
+        self.lib.L.ilref_occluded(self.h, o4, d4, n, occ, nthreads or os.cpu_count() or 1)
+        return occ
+
+    def __del__(self):
+        try:
+            self.lib.L.ilref_mesh_destroy(self.h)
+        except Exception:
+            pass

@@ -1,0 +1,3 @@
+#pragma once
+#include <chrono>
+namespace boost { namespace chrono = std::chrono; }

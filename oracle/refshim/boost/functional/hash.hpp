@@ -1,0 +1,3 @@
+#pragma once
+#include <functional>
+namespace boost { using std::hash; }

@@ -1,0 +1,3 @@
+#pragma once
+#include <mutex>
+namespace boost { using std::recursive_mutex; }

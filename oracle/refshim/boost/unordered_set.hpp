@@ -1,0 +1,3 @@
+#pragma once
+#include <unordered_set>
+namespace boost { using std::unordered_set; }
