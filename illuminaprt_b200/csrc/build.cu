@@ -1,0 +1,512 @@
+// Device build of the 8-wide BVH (replaces the reference's per-mesh CPU tree
+// builders, KDTreeMesh::Compile / BVHMesh::Compile, KDTreeMesh.cpp:114-275 and
+// BVHMesh.cpp:78-107, which take ~6-20 s per million triangles on one core).
+//
+// Pipeline, all on the context's stream:
+//   1. k_tri_bounds   per-triangle AABB + centroid, scene centroid bounds
+//   2. k_morton       30-bit Morton code of each centroid
+//   3. radix sort     (code, triangle) pairs (CUB)
+//   4. k_karras       binary radix tree over the sorted codes (Karras 2012),
+//                     duplicate codes split by index
+//   5. k_refit        bottom-up AABBs, one atomic arrival counter per node
+//   6. k_collapse     level by level: each work item turns one binary node
+//                     into one 8-wide node (greedy: open the widest child
+//                     with more than 3 triangles until 8 slots are used),
+//                     orders the slots by octant, quantises the child boxes
+//                     to 8 bits against the node origin, and writes the
+//                     triangle records of its leaf children.
+#include "bvh8.cuh"
+#include "build.cuh"
+
+#include <cub/device/device_radix_sort.cuh>
+
+#include <cfloat>
+#include <cmath>
+#include <utility>
+
+namespace ilg {
+
+namespace {
+
+__device__ __forceinline__ uint32_t float_flip(float f)
+{
+    uint32_t u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float float_unflip(uint32_t u)
+{
+    return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
+}
+
+__device__ __forceinline__ uint32_t expand_bits10(uint32_t v)
+{
+    v &= 0x3ffu;
+    v = (v * 0x00010001u) & 0xFF0000FFu;
+    v = (v * 0x00000101u) & 0x0F00F00Fu;
+    v = (v * 0x00000011u) & 0xC30C30C3u;
+    v = (v * 0x00000005u) & 0x49249249u;
+    return v;
+}
+
+struct Box {
+    float3 lo, hi;
+};
+
+__device__ __forceinline__ float area(const float3 &lo, const float3 &hi)
+{
+    float dx = fmaxf(hi.x - lo.x, 0.f), dy = fmaxf(hi.y - lo.y, 0.f), dz = fmaxf(hi.z - lo.z, 0.f);
+    return dx * dy + dy * dz + dz * dx;
+}
+
+// ---------------------------------------------------------------- step 1 ----
+__global__ void k_tri_bounds(const float *__restrict__ pos, uint32_t n_verts, const uint32_t *__restrict__ idx,
+                             uint32_t n, float4 *__restrict__ tlo, float4 *__restrict__ thi,
+                             uint32_t *__restrict__ cbounds /* 6 flipped floats: min xyz, max xyz */,
+                             uint32_t *__restrict__ err)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    float3 clo = make_float3(FLT_MAX, FLT_MAX, FLT_MAX), chi = make_float3(-FLT_MAX, -FLT_MAX, -FLT_MAX);
+    if (i < n) {
+        uint32_t a = idx[3 * i], b = idx[3 * i + 1], c = idx[3 * i + 2];
+        if (a >= n_verts || b >= n_verts || c >= n_verts) {
+            atomicOr(err, 1u);
+            a = b = c = 0;
+        }
+        float3 p0 = make_float3(pos[3 * a], pos[3 * a + 1], pos[3 * a + 2]);
+        float3 p1 = make_float3(pos[3 * b], pos[3 * b + 1], pos[3 * b + 2]);
+        float3 p2 = make_float3(pos[3 * c], pos[3 * c + 1], pos[3 * c + 2]);
+        float3 lo = make_float3(fminf(p0.x, fminf(p1.x, p2.x)), fminf(p0.y, fminf(p1.y, p2.y)),
+                                fminf(p0.z, fminf(p1.z, p2.z)));
+        float3 hi = make_float3(fmaxf(p0.x, fmaxf(p1.x, p2.x)), fmaxf(p0.y, fmaxf(p1.y, p2.y)),
+                                fmaxf(p0.z, fmaxf(p1.z, p2.z)));
+        tlo[i] = make_float4(lo.x, lo.y, lo.z, 0.f);
+        thi[i] = make_float4(hi.x, hi.y, hi.z, 0.f);
+        clo = make_float3(0.5f * (lo.x + hi.x), 0.5f * (lo.y + hi.y), 0.5f * (lo.z + hi.z));
+        chi = clo;
+    }
+    // warp reduce, then one atomic per warp
+    for (int o = 16; o > 0; o >>= 1) {
+        clo.x = fminf(clo.x, __shfl_xor_sync(0xffffffffu, clo.x, o));
+        clo.y = fminf(clo.y, __shfl_xor_sync(0xffffffffu, clo.y, o));
+        clo.z = fminf(clo.z, __shfl_xor_sync(0xffffffffu, clo.z, o));
+        chi.x = fmaxf(chi.x, __shfl_xor_sync(0xffffffffu, chi.x, o));
+        chi.y = fmaxf(chi.y, __shfl_xor_sync(0xffffffffu, chi.y, o));
+        chi.z = fmaxf(chi.z, __shfl_xor_sync(0xffffffffu, chi.z, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMin(&cbounds[0], float_flip(clo.x));
+        atomicMin(&cbounds[1], float_flip(clo.y));
+        atomicMin(&cbounds[2], float_flip(clo.z));
+        atomicMax(&cbounds[3], float_flip(chi.x));
+        atomicMax(&cbounds[4], float_flip(chi.y));
+        atomicMax(&cbounds[5], float_flip(chi.z));
+    }
+}
+
+// ---------------------------------------------------------------- step 2 ----
+__global__ void k_morton(const float4 *__restrict__ tlo, const float4 *__restrict__ thi, uint32_t n,
+                         const uint32_t *__restrict__ cbounds, uint32_t *__restrict__ keys,
+                         uint32_t *__restrict__ vals)
+{
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float3 lo = make_float3(float_unflip(cbounds[0]), float_unflip(cbounds[1]), float_unflip(cbounds[2]));
+    float3 hi = make_float3(float_unflip(cbounds[3]), float_unflip(cbounds[4]), float_unflip(cbounds[5]));
+    float4 a = tlo[i], b = thi[i];
+    float cx = 0.5f * (a.x + b.x), cy = 0.5f * (a.y + b.y), cz = 0.5f * (a.z + b.z);
+    float ex = hi.x - lo.x, ey = hi.y - lo.y, ez = hi.z - lo.z;
+    float nx = ex > 0.f ? (cx - lo.x) / ex : 0.f;
+    float ny = ey > 0.f ? (cy - lo.y) / ey : 0.f;
+    float nz = ez > 0.f ? (cz - lo.z) / ez : 0.f;
+    uint32_t ix = (uint32_t)fminf(fmaxf(nx * 1024.f, 0.f), 1023.f);
+    uint32_t iy = (uint32_t)fminf(fmaxf(ny * 1024.f, 0.f), 1023.f);
+    uint32_t iz = (uint32_t)fminf(fmaxf(nz * 1024.f, 0.f), 1023.f);
+    keys[i] = (expand_bits10(ix) << 2) | (expand_bits10(iy) << 1) | expand_bits10(iz);
+    vals[i] = i;
+}
+
+// ---------------------------------------------------------------- step 4 ----
+// Internal node i of n-1; children encoded >= 0 internal, < 0 leaf ~sorted_pos.
+__device__ __forceinline__ int delta(const uint32_t *keys, int n, int i, int j)
+{
+    if (j < 0 || j >= n) return -1;
+    uint32_t a = keys[i], b = keys[j];
+    if (a == b) return 32 + __clz((uint32_t)i ^ (uint32_t)j);
+    return __clz(a ^ b);
+}
+
+__global__ void k_karras(const uint32_t *__restrict__ keys, int n, int2 *__restrict__ child,
+                         int *__restrict__ parent_int, int *__restrict__ parent_leaf, int2 *__restrict__ range)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n - 1) return;
+    int dl = delta(keys, n, i, i - 1), dr = delta(keys, n, i, i + 1);
+    int d = dr > dl ? 1 : -1;
+    int dmin = d > 0 ? dl : dr;
+    int lmax = 2;
+    while (lmax < (1 << 30) && delta(keys, n, i, i + lmax * d) > dmin) lmax <<= 1;
+    int l = 0;
+    for (int t = lmax >> 1; t >= 1; t >>= 1)
+        if (delta(keys, n, i, i + (l + t) * d) > dmin) l += t;
+    int j = i + l * d;
+    int dnode = delta(keys, n, i, j);
+    int s = 0;
+    int len = l;
+    int t = (len + 1) >> 1;
+    for (int it = 0; it < 64 && t >= 1; it++) {  // t halves (rounding up) to 1; the cap is only a guard
+        if (delta(keys, n, i, i + (s + t) * d) > dnode) s += t;
+        if (t == 1) break;
+        t = (t + 1) >> 1;
+    }
+    int gamma = i + s * d + min(d, 0);
+    int first = min(i, j), last = max(i, j);
+    int left = (first == gamma) ? ~gamma : gamma;
+    int right = (last == gamma + 1) ? ~(gamma + 1) : gamma + 1;
+    child[i] = make_int2(left, right);
+    range[i] = make_int2(first, last);
+    if (left >= 0) parent_int[left] = i; else parent_leaf[~left] = i;
+    if (right >= 0) parent_int[right] = i; else parent_leaf[~right] = i;
+}
+
+// ---------------------------------------------------------------- step 5 ----
+__global__ void k_refit(int n, const uint32_t *__restrict__ sorted_tri, const float4 *__restrict__ tlo,
+                        const float4 *__restrict__ thi, const int2 *__restrict__ child,
+                        const int *__restrict__ parent_int, const int *__restrict__ parent_leaf,
+                        uint32_t *__restrict__ arrivals, float4 *__restrict__ nlo, float4 *__restrict__ nhi)
+{
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int p = parent_leaf[i];
+    // bounded by the tree height (< n); each node's second arrival proceeds
+    for (int guard = 0; p >= 0 && guard < n; guard++) {
+        __threadfence();
+        if (atomicAdd(&arrivals[p], 1u) == 0) return;
+        __threadfence();
+        int2 c = child[p];
+        float4 alo, ahi, blo, bhi;
+        if (c.x >= 0) { alo = __ldcg(&nlo[c.x]); ahi = __ldcg(&nhi[c.x]); }
+        else { uint32_t t = sorted_tri[~c.x]; alo = tlo[t]; ahi = thi[t]; }
+        if (c.y >= 0) { blo = __ldcg(&nlo[c.y]); bhi = __ldcg(&nhi[c.y]); }
+        else { uint32_t t = sorted_tri[~c.y]; blo = tlo[t]; bhi = thi[t]; }
+        __stcg(&nlo[p], make_float4(fminf(alo.x, blo.x), fminf(alo.y, blo.y), fminf(alo.z, blo.z), 0.f));
+        __stcg(&nhi[p], make_float4(fmaxf(ahi.x, bhi.x), fmaxf(ahi.y, bhi.y), fmaxf(ahi.z, bhi.z), 0.f));
+        p = parent_int[p];
+    }
+}
+
+// ---------------------------------------------------------------- step 6 ----
+struct Work {
+    int bin;       // binary node: >= 0 internal, < 0 leaf ~sorted_pos (only for n == 1)
+    uint32_t node; // 8-wide node index to fill
+};
+
+static_assert(sizeof(Work) == 8, "work item is 8 bytes");
+
+__device__ __forceinline__ void child_box(int c, const uint32_t *sorted_tri, const float4 *tlo, const float4 *thi,
+                                          const float4 *nlo, const float4 *nhi, float3 &lo, float3 &hi)
+{
+    float4 a, b;
+    if (c >= 0) { a = nlo[c]; b = nhi[c]; }
+    else { uint32_t t = sorted_tri[~c]; a = tlo[t]; b = thi[t]; }
+    lo = make_float3(a.x, a.y, a.z);
+    hi = make_float3(b.x, b.y, b.z);
+}
+
+__device__ __forceinline__ int2 child_range(int c, const int2 *range)
+{
+    return c >= 0 ? range[c] : make_int2(~c, ~c);
+}
+
+// Quantisation step for one axis: the smallest power of two 2^e with
+// extent / 2^e <= 255 - 2 (one step of slack each side), and never below
+// `min_step` so that a step stays many float ulps wide.
+__device__ __forceinline__ int quant_exp(float extent, float min_step)
+{
+    float target = fmaxf(extent / 253.0f, min_step);
+    int e;
+    frexpf(target, &e);  // target = m * 2^e, m in [0.5, 1)  ->  2^e >= target
+    e = max(e, -120);
+    e = min(e, 127);
+    return e;
+}
+
+__device__ __forceinline__ float exp2i(int e) { return ldexpf(1.0f, e); }
+
+__global__ void k_collapse(const Work *__restrict__ in, const uint32_t *__restrict__ in_count, Work *__restrict__ out,
+                           uint32_t *__restrict__ out_count, uint32_t out_cap, const int2 *__restrict__ child,
+                           const int2 *__restrict__ range, const float4 *__restrict__ nlo,
+                           const float4 *__restrict__ nhi, const uint32_t *__restrict__ sorted_tri,
+                           const float4 *__restrict__ tlo, const float4 *__restrict__ thi,
+                           const float *__restrict__ pos, const uint32_t *__restrict__ idx, Node8 *__restrict__ nodes,
+                           uint32_t *__restrict__ node_count, uint32_t node_cap, Tri *__restrict__ tris,
+                           uint32_t *__restrict__ prim_of, uint32_t *__restrict__ tri_count, uint32_t tri_cap,
+                           float min_step, uint32_t *__restrict__ err)
+{
+    uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
+    if (w >= *in_count) return;
+    const Work job = in[w];
+
+    int ch[8];
+    int m = 0;
+    if (job.bin >= 0) {
+        int2 c = child[job.bin];
+        ch[m++] = c.x;
+        ch[m++] = c.y;
+        // open the widest child that must stay internal until 8 slots are used
+        while (m < 8) {
+            int best = -1;
+            float best_a = -1.f;
+            for (int k = 0; k < m; k++) {
+                if (ch[k] < 0) continue;
+                int2 r = range[ch[k]];
+                if (r.y - r.x + 1 <= kLeafMax) continue;
+                float3 lo, hi;
+                child_box(ch[k], sorted_tri, tlo, thi, nlo, nhi, lo, hi);
+                float a = area(lo, hi);
+                if (a > best_a) { best_a = a; best = k; }
+            }
+            if (best < 0) break;
+            int2 c2 = child[ch[best]];
+            ch[best] = c2.x;
+            ch[m++] = c2.y;
+        }
+    } else {
+        ch[m++] = job.bin;  // single-triangle scene
+    }
+
+    // child boxes, centroids, classification
+    float3 clo[8], chi[8];
+    float3 plo = make_float3(FLT_MAX, FLT_MAX, FLT_MAX), phi = make_float3(-FLT_MAX, -FLT_MAX, -FLT_MAX);
+    int n_int = 0, n_leaf_tris = 0;
+    for (int k = 0; k < m; k++) {
+        child_box(ch[k], sorted_tri, tlo, thi, nlo, nhi, clo[k], chi[k]);
+        plo = make_float3(fminf(plo.x, clo[k].x), fminf(plo.y, clo[k].y), fminf(plo.z, clo[k].z));
+        phi = make_float3(fmaxf(phi.x, chi[k].x), fmaxf(phi.y, chi[k].y), fmaxf(phi.z, chi[k].z));
+        int2 r = child_range(ch[k], range);
+        int cnt = r.y - r.x + 1;
+        if (ch[k] >= 0 && cnt > kLeafMax) n_int++;
+        else n_leaf_tris += cnt;
+    }
+
+    // slot assignment: slot s is the corner with bit k set = positive along axis k
+    int slot_of[8];
+    {
+        float3 pc = make_float3(0.5f * (plo.x + phi.x), 0.5f * (plo.y + phi.y), 0.5f * (plo.z + phi.z));
+        float score[8][8];
+        for (int k = 0; k < m; k++) {
+            float3 c = make_float3(0.5f * (clo[k].x + chi[k].x) - pc.x, 0.5f * (clo[k].y + chi[k].y) - pc.y,
+                                   0.5f * (clo[k].z + chi[k].z) - pc.z);
+            for (int s = 0; s < 8; s++)
+                score[k][s] = ((s & 1) ? c.x : -c.x) + ((s & 2) ? c.y : -c.y) + ((s & 4) ? c.z : -c.z);
+        }
+        uint32_t used_slots = 0, used_kids = 0;
+        for (int it = 0; it < m; it++) {
+            float best = -FLT_MAX;
+            int bk = -1, bs = -1;
+            for (int k = 0; k < m; k++) {
+                if (used_kids & (1u << k)) continue;
+                for (int s = 0; s < 8; s++) {
+                    if (used_slots & (1u << s)) continue;
+                    if (score[k][s] > best || bk < 0) { best = score[k][s]; bk = k; bs = s; }
+                }
+            }
+            used_kids |= 1u << bk;
+            used_slots |= 1u << bs;
+            slot_of[bk] = bs;
+        }
+    }
+
+    // allocate children and triangle records
+    uint32_t child_base = 0, tri_base = 0;
+    if (n_int) {
+        child_base = atomicAdd(node_count, (uint32_t)n_int);
+        if (child_base + n_int > node_cap) { atomicOr(err, 2u); return; }
+    }
+    if (n_leaf_tris) {
+        tri_base = atomicAdd(tri_count, (uint32_t)n_leaf_tris);
+        if (tri_base + n_leaf_tris > tri_cap) { atomicOr(err, 4u); return; }
+    }
+
+    // quantisation frame
+    int ex = quant_exp(phi.x - plo.x, min_step), ey = quant_exp(phi.y - plo.y, min_step),
+        ez = quant_exp(phi.z - plo.z, min_step);
+    float sx = exp2i(ex), sy = exp2i(ey), sz = exp2i(ez);
+    // origin one step below the union so that floor() never goes negative
+    float3 org = make_float3(plo.x - sx, plo.y - sy, plo.z - sz);
+
+    uint8_t meta[8], qlx[8], qly[8], qlz[8], qhx[8], qhy[8], qhz[8];
+    for (int s = 0; s < 8; s++) meta[s] = qlx[s] = qly[s] = qlz[s] = qhx[s] = qhy[s] = qhz[s] = 0;
+
+    // internal children in slot order -> contiguous child nodes
+    uint32_t imask = 0;
+    for (int k = 0; k < m; k++) {
+        int2 r = child_range(ch[k], range);
+        if (ch[k] >= 0 && r.y - r.x + 1 > kLeafMax) imask |= 1u << slot_of[k];
+    }
+    int tri_off = 0;
+    for (int s = 0; s < 8; s++) {
+        int k = -1;
+        for (int q = 0; q < m; q++)
+            if (slot_of[q] == s) k = q;
+        if (k < 0) continue;
+        // conservative 8-bit box: floor/ceil in double (exact for float inputs),
+        // one extra step of slack each side
+        double lx = floor(((double)clo[k].x - org.x) / sx) - 1, ly = floor(((double)clo[k].y - org.y) / sy) - 1,
+               lz = floor(((double)clo[k].z - org.z) / sz) - 1;
+        double hx = ceil(((double)chi[k].x - org.x) / sx) + 1, hy = ceil(((double)chi[k].y - org.y) / sy) + 1,
+               hz = ceil(((double)chi[k].z - org.z) / sz) + 1;
+        qlx[s] = (uint8_t)fmin(fmax(lx, 0.0), 255.0);
+        qly[s] = (uint8_t)fmin(fmax(ly, 0.0), 255.0);
+        qlz[s] = (uint8_t)fmin(fmax(lz, 0.0), 255.0);
+        qhx[s] = (uint8_t)fmin(fmax(hx, 0.0), 255.0);
+        qhy[s] = (uint8_t)fmin(fmax(hy, 0.0), 255.0);
+        qhz[s] = (uint8_t)fmin(fmax(hz, 0.0), 255.0);
+        int2 r = child_range(ch[k], range);
+        int cnt = r.y - r.x + 1;
+        if (imask & (1u << s)) {
+            meta[s] = (uint8_t)kMetaInternal;
+            uint32_t ci = child_base + __popc(imask & ((1u << s) - 1u));
+            uint32_t slot = atomicAdd(out_count, 1u);
+            if (slot >= out_cap) { atomicOr(err, 8u); continue; }
+            out[slot] = Work{ch[k], ci};
+        } else {
+            meta[s] = (uint8_t)((cnt << 5) | tri_off);
+            for (int q = 0; q < cnt; q++) {
+                uint32_t t = sorted_tri[r.x + q];
+                uint32_t a = idx[3 * t], b = idx[3 * t + 1], c = idx[3 * t + 2];
+                float v0x = pos[3 * a], v0y = pos[3 * a + 1], v0z = pos[3 * a + 2];
+                float e1x = __fsub_rn(pos[3 * b], v0x), e1y = __fsub_rn(pos[3 * b + 1], v0y),
+                      e1z = __fsub_rn(pos[3 * b + 2], v0z);
+                float e2x = __fsub_rn(pos[3 * c], v0x), e2y = __fsub_rn(pos[3 * c + 1], v0y),
+                      e2z = __fsub_rn(pos[3 * c + 2], v0z);
+                float nx = __fsub_rn(__fmul_rn(e1y, e2z), __fmul_rn(e1z, e2y));
+                float ny = __fsub_rn(__fmul_rn(e1z, e2x), __fmul_rn(e1x, e2z));
+                float nz = __fsub_rn(__fmul_rn(e1x, e2y), __fmul_rn(e1y, e2x));
+                Tri tr;
+                tr.a = make_float4(v0x, v0y, v0z, nx);
+                tr.b = make_float4(e1x, e1y, e1z, ny);
+                tr.c = make_float4(e2x, e2y, e2z, nz);
+                tris[tri_base + tri_off + q] = tr;
+                prim_of[tri_base + tri_off + q] = t;
+            }
+            tri_off += cnt;
+        }
+    }
+
+    auto pack4 = [](const uint8_t *b) {
+        return (uint32_t)b[0] | ((uint32_t)b[1] << 8) | ((uint32_t)b[2] << 16) | ((uint32_t)b[3] << 24);
+    };
+    Node8 nd;
+    nd.q[0] = make_uint4(__float_as_uint(org.x), __float_as_uint(org.y), __float_as_uint(org.z),
+                         (uint32_t)(ex + 127) | ((uint32_t)(ey + 127) << 8) | ((uint32_t)(ez + 127) << 16) |
+                             (imask << 24));
+    nd.q[1] = make_uint4(child_base, tri_base, pack4(meta), pack4(meta + 4));
+    nd.q[2] = make_uint4(pack4(qlx), pack4(qlx + 4), pack4(qhx), pack4(qhx + 4));
+    nd.q[3] = make_uint4(pack4(qly), pack4(qly + 4), pack4(qhy), pack4(qhy + 4));
+    nd.q[4] = make_uint4(pack4(qlz), pack4(qlz + 4), pack4(qhz), pack4(qhz + 4));
+    nodes[job.node] = nd;
+}
+
+__global__ void k_root(Work *q, uint32_t *count, int n, uint32_t *node_count)
+{
+    q[0] = Work{n > 1 ? 0 : ~0, 0u};
+    *count = 1;
+    *node_count = 1;
+}
+
+inline uint32_t div_up(uint64_t a, uint32_t b) { return (uint32_t)((a + b - 1) / b); }
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+#define ILG_CK(call)                                                                       \
+    do {                                                                                   \
+        cudaError_t e_ = (call);                                                           \
+        if (e_ != cudaSuccess) {                                                           \
+            snprintf(err, err_len, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+            return 3;                                                                      \
+        }                                                                                  \
+    } while (0)
+
+int bvh_build(BuildBuffers &B, const float *d_pos, uint32_t n_verts, const uint32_t *d_idx, uint32_t n,
+              cudaStream_t st, BuildResult &res, char *err, size_t err_len)
+{
+    if (n == 0) {
+        snprintf(err, err_len, "ilg_build: empty mesh");
+        return 1;
+    }
+    // scratch sizing
+    size_t sort_tmp = 0;
+    ILG_CK(cub::DeviceRadixSort::SortPairs(nullptr, sort_tmp, (uint32_t *)nullptr, (uint32_t *)nullptr,
+                                           (uint32_t *)nullptr, (uint32_t *)nullptr, (int)n, 0, 30, st));
+    const uint32_t node_cap = n;           // 8-wide nodes never exceed the triangle count
+    const uint32_t tri_cap = n;
+    const uint32_t queue_cap = n + 1;
+    ILG_CK(B.reserve(n, sort_tmp, node_cap, queue_cap, st));
+
+    ILG_CK(cudaMemsetAsync(B.err, 0, sizeof(uint32_t), st));
+    uint32_t init[6] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0u, 0u, 0u};
+    ILG_CK(cudaMemcpyAsync(B.cbounds, init, sizeof(init), cudaMemcpyHostToDevice, st));
+    const uint32_t T = 256;
+    k_tri_bounds<<<div_up(n, T), T, 0, st>>>(d_pos, n_verts, d_idx, n, B.tlo, B.thi, B.cbounds, B.err);
+    k_morton<<<div_up(n, T), T, 0, st>>>(B.tlo, B.thi, n, B.cbounds, B.keys, B.vals);
+    ILG_CK(cudaGetLastError());
+    ILG_CK(cub::DeviceRadixSort::SortPairs(B.sort_tmp, sort_tmp, B.keys, B.keys_alt, B.vals, B.vals_alt, (int)n, 0,
+                                           30, st));
+    if (n > 1) {
+        k_karras<<<div_up(n - 1, T), T, 0, st>>>(B.keys_alt, (int)n, B.child, B.parent_int, B.parent_leaf, B.range);
+        ILG_CK(cudaMemsetAsync(B.arrivals, 0, sizeof(uint32_t) * (n - 1), st));
+        k_refit<<<div_up(n, T), T, 0, st>>>((int)n, B.vals_alt, B.tlo, B.thi, B.child, B.parent_int, B.parent_leaf,
+                                             B.arrivals, B.nlo, B.nhi);
+        ILG_CK(cudaGetLastError());
+    }
+    ILG_CK(cudaMemsetAsync(B.counters, 0, 4 * sizeof(uint32_t), st));
+    // counters: [0] node_count, [1] tri_count, [2] queue A count, [3] queue B count
+    k_root<<<1, 1, 0, st>>>((Work *)B.qa_raw, B.counters + 2, (int)n, B.counters + 0);
+    ILG_CK(cudaGetLastError());
+
+    const float min_step = res.min_step;
+    Work *qin = (Work *)B.qa_raw, *qout = (Work *)B.qb_raw;
+    uint32_t *cin = B.counters + 2, *cout = B.counters + 3;
+    uint32_t host_in = 1;
+    uint32_t depth = 0;
+    while (host_in > 0) {
+        ILG_CK(cudaMemsetAsync(cout, 0, sizeof(uint32_t), st));
+        k_collapse<<<div_up(host_in, 64), 64, 0, st>>>(qin, cin, qout, cout, queue_cap, B.child, B.range, B.nlo,
+                                                        B.nhi, B.vals_alt, B.tlo, B.thi, d_pos, d_idx, B.nodes,
+                                                        B.counters + 0, node_cap, B.tris, B.prim_of, B.counters + 1,
+                                                        tri_cap, min_step, B.err);
+        ILG_CK(cudaGetLastError());
+        ILG_CK(cudaMemcpyAsync(&host_in, cout, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        ILG_CK(cudaStreamSynchronize(st));
+        depth++;
+        if (depth > 200) {
+            snprintf(err, err_len, "ilg_build: collapse did not converge");
+            return 5;
+        }
+        std::swap(qin, qout);
+        std::swap(cin, cout);
+    }
+    uint32_t h[4], herr = 0;
+    ILG_CK(cudaMemcpyAsync(h, B.counters, sizeof(h), cudaMemcpyDeviceToHost, st));
+    ILG_CK(cudaMemcpyAsync(&herr, B.err, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    ILG_CK(cudaStreamSynchronize(st));
+    if (herr & 1u) {
+        snprintf(err, err_len, "ilg_build: triangle index out of range of the vertex array");
+        return 1;
+    }
+    if (herr) {
+        snprintf(err, err_len, "ilg_build: capacity exceeded (flags 0x%x)", herr);
+        return 5;
+    }
+    if (h[1] != n) {
+        snprintf(err, err_len, "ilg_build: %u triangle records written for %u triangles", h[1], n);
+        return 5;
+    }
+    res.n_nodes = h[0];
+    res.n_tris = h[1];
+    res.depth = depth;
+    return 0;
+}
+
+}  // namespace ilg

@@ -1,0 +1,91 @@
+// Device data layout of the 8-wide BVH and the reference-compatible triangle
+// test shared by the build and the traversal kernels.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace ilg {
+
+// ---------------------------------------------------------------------------
+// Node record: 80 bytes = 5 x uint4, 16-byte aligned, read with 128-bit loads.
+//   q0: origin.xyz (float bits), w = ex | ey << 8 | ez << 16 | imask << 24
+//       (e* are biased power-of-two exponents of the quantisation step,
+//        imask bit s = slot s holds an internal child)
+//   q1: x = first child node, y = first triangle record,
+//       z = meta[0..3], w = meta[4..7]
+//   q2: x/y = qlo.x[0..7], z/w = qhi.x[0..7]   (one byte per slot)
+//   q3: same for y, q4: same for z
+// meta byte: 0 = empty slot; 0x80 = internal child; otherwise a leaf with
+// count (1..3) in bits 5-6 and the offset of its first triangle from the
+// node's first triangle record (0..23) in bits 0-4.
+// Internal children of a node are stored contiguously in slot order, so the
+// child in slot s is node first_child + popc(imask & ((1 << s) - 1)).
+// Slots are assigned so that a ray in octant o visits children in
+// descending order of (slot ^ (7 - o)), which approximates front to back.
+// ---------------------------------------------------------------------------
+struct __align__(16) Node8 {
+    uint4 q[5];
+};
+static_assert(sizeof(Node8) == 80, "node record must be 80 bytes");
+
+// Triangle record: 48 bytes = 3 x float4.
+//   a = (v0.x, v0.y, v0.z, n.x), b = (e1.xyz, n.y), c = (e2.xyz, n.z)
+// with e1 = v1 - v0, e2 = v2 - v0, n = e1 x e2 evaluated exactly as the
+// reference does (IndexedTriangle.cpp:44-45, :103), one rounding per op.
+struct __align__(16) Tri {
+    float4 a, b, c;
+};
+static_assert(sizeof(Tri) == 48, "triangle record must be 48 bytes");
+
+constexpr int kMaxStack = 64;      // traversal stack entries (node groups)
+constexpr int kLeafMax = 3;        // triangles per leaf child
+constexpr uint32_t kMetaInternal = 0x80u;
+
+// Lower bound of the reference's triangle window, `t < 1e-5` evaluated in
+// double (IndexedTriangle.cpp:115): for a float t this is t < the smallest
+// float >= 1e-5, i.e. 0x3727C5AD.
+__device__ __forceinline__ float window_lo() { return __int_as_float(0x3727C5AD); }
+
+// Upper bound: `t > Max - 1e-5` in double holds for a float t exactly when
+// t > (Max - 1e-5) rounded down to float.
+__device__ __forceinline__ float window_hi(float tmax)
+{
+    return __double2float_rd(__dsub_rn((double)tmax, 1e-5));
+}
+
+// Shirley-form test of IndexedTriangle::Intersects (IndexedTriangle.cpp:92-128)
+// with every product and sum rounded separately (no contraction), so that t,
+// beta and gamma are bit-identical to the reference compiled without FMA.
+// `hi` is window_hi(current Max).
+__device__ __forceinline__ bool shirley(const Tri &tr, float ox, float oy, float oz, float dx, float dy,
+                                        float dz, float hi, float &t_out, float &b_out, float &g_out)
+{
+    const float nx = tr.a.w, ny = tr.b.w, nz = tr.c.w;
+    const float den = __fadd_rn(__fadd_rn(__fmul_rn(nx, dx), __fmul_rn(ny, dy)), __fmul_rn(nz, dz));
+    const float rcp = __fdiv_rn(1.0f, den);
+    const float ex = __fsub_rn(tr.a.x, ox), ey = __fsub_rn(tr.a.y, oy), ez = __fsub_rn(tr.a.z, oz);
+    const float num = __fadd_rn(__fadd_rn(__fmul_rn(nx, ex), __fmul_rn(ny, ey)), __fmul_rn(nz, ez));
+    const float t = __fmul_rn(num, rcp);
+    if (t > hi || t < window_lo()) return false;
+    // interm = d x edge2
+    const float ix = __fsub_rn(__fmul_rn(dy, ez), __fmul_rn(dz, ey));
+    const float iy = __fsub_rn(__fmul_rn(dz, ex), __fmul_rn(dx, ez));
+    const float iz = __fsub_rn(__fmul_rn(dx, ey), __fmul_rn(dy, ex));
+    const float beta =
+        __fmul_rn(__fadd_rn(__fadd_rn(__fmul_rn(ix, tr.c.x), __fmul_rn(iy, tr.c.y)), __fmul_rn(iz, tr.c.z)), -rcp);
+    if (beta < 0.0f) return false;
+    const float gamma =
+        __fmul_rn(__fadd_rn(__fadd_rn(__fmul_rn(ix, tr.b.x), __fmul_rn(iy, tr.b.y)), __fmul_rn(iz, tr.b.z)), rcp);
+    if (__fadd_rn(beta, gamma) > 1.0f || gamma < 0.0f) return false;
+    // A NaN t (origin in the triangle's plane, direction parallel to it)
+    // passes the reference's comparisons and poisons its ray.Max; it is
+    // rejected here instead.
+    if (!(t <= hi)) return false;
+    t_out = t;
+    b_out = beta;
+    g_out = gamma;
+    return true;
+}
+
+}  // namespace ilg

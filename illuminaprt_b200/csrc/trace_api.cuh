@@ -1,0 +1,23 @@
+// Host-side launch interface of the traversal kernels.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "bvh8.cuh"
+
+namespace ilg {
+
+struct SceneView {
+    const Node8 *nodes;
+    const Tri *tris;
+    const uint32_t *prim_of;
+    uint32_t n_nodes, n_tris;
+};
+
+cudaError_t launch_closest(const SceneView &s, const float4 *ro, const float4 *rd, uint32_t n, int32_t *prim,
+                           float *t, float *u, float *v, uint32_t *err, unsigned long long *stats, cudaStream_t st);
+cudaError_t launch_any(const SceneView &s, const float4 *ro, const float4 *rd, uint32_t n, uint8_t *occ,
+                       uint32_t *err, cudaStream_t st);
+
+}  // namespace ilg

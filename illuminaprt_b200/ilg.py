@@ -1,0 +1,183 @@
+"""Python binding of the C ABI in include/ilg.h (ctypes over libilg.so).
+
+The names mirror the reference's space interface (Core/Space/Space.h:23-46):
+``GpuSpace.initialise`` / ``build`` / ``intersects`` / ``occluded`` stand for
+ISpace::Initialise / Build / Intersects(ray, isect) / Intersects(ray), batched
+over arrays of rays. Errors raise ``IlgError`` carrying the library's status
+code and message (the reference throws ``Exception*``; here it is a Python
+exception). There is no CPU fallback: without the CUDA library or a GPU,
+construction fails loudly.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from . import build as _build
+
+ILG_OK, ILG_EINVAL, ILG_ENOMEM, ILG_ECUDA, ILG_ETIMEOUT, ILG_EOVERFLOW, ILG_ESTATE = range(7)
+ILG_DEVICE_PTRS = 0x1
+
+STATUS_NAMES = {0: "ILG_OK", 1: "ILG_EINVAL", 2: "ILG_ENOMEM", 3: "ILG_ECUDA", 4: "ILG_ETIMEOUT",
+                5: "ILG_EOVERFLOW", 6: "ILG_ESTATE"}
+
+# Every symbol the public headers declare; tests check the library exports them.
+EXPORTED = ["ilg_create", "ilg_destroy", "ilg_last_error", "ilg_set_mesh", "ilg_build", "ilg_get_stats",
+            "ilg_intersect", "ilg_intersect_counted", "ilg_occluded", "ilg_sync", "ilg_stream"]
+
+
+class IlgError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{STATUS_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+class ilg_opts(ctypes.Structure):
+    _fields_ = [("device", ctypes.c_int32), ("reserved", ctypes.c_uint32 * 7)]
+
+
+class ilg_stats(ctypes.Structure):
+    _fields_ = [("n_tris", ctypes.c_uint32), ("n_nodes", ctypes.c_uint32), ("n_leaf_tris", ctypes.c_uint32),
+                ("max_depth", ctypes.c_uint32), ("build_ms", ctypes.c_float), ("node_bytes", ctypes.c_uint64),
+                ("tri_bytes", ctypes.c_uint64)]
+
+
+_lib = None
+
+
+def lib_path() -> str:
+    return _build.LIB
+
+
+def load(build_if_missing: bool = True) -> ctypes.CDLL:
+    """Load libilg.so (building it first when it is absent or stale)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if build_if_missing:
+        _build.build()
+    if not os.path.exists(_build.LIB):
+        raise IlgError(ILG_ESTATE, f"CUDA library not built: {_build.LIB}")
+    L = ctypes.CDLL(_build.LIB)
+    vp, u32, i32 = ctypes.c_void_p, ctypes.c_uint32, ctypes.c_int32
+    L.ilg_create.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(ilg_opts)]
+    L.ilg_destroy.argtypes = [vp]
+    L.ilg_last_error.argtypes = [vp]
+    L.ilg_last_error.restype = ctypes.c_char_p
+    L.ilg_set_mesh.argtypes = [vp, vp, u32, vp, u32, vp]
+    L.ilg_build.argtypes = [vp]
+    L.ilg_get_stats.argtypes = [vp, ctypes.POINTER(ilg_stats)]
+    L.ilg_intersect.argtypes = [vp, vp, vp, u32, vp, vp, vp, vp, u32]
+    L.ilg_intersect_counted.argtypes = [vp, vp, vp, u32, vp, vp, vp, vp, vp, u32]
+    L.ilg_occluded.argtypes = [vp, vp, vp, u32, vp, u32]
+    L.ilg_sync.argtypes = [vp]
+    L.ilg_stream.argtypes = [vp]
+    L.ilg_stream.restype = vp
+    for f in ("ilg_create", "ilg_destroy", "ilg_set_mesh", "ilg_build", "ilg_get_stats", "ilg_intersect",
+              "ilg_intersect_counted", "ilg_occluded", "ilg_sync"):
+        getattr(L, f).restype = i32
+    _lib = L
+    return L
+
+
+def _ptr(a) -> int:
+    """Address of a numpy array or a torch tensor."""
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data
+    return a.data_ptr()
+
+
+class GpuSpace:
+    """A triangle scene on one GPU with batched closest-hit / any-hit queries."""
+
+    def __init__(self, device: int = 0):
+        self.L = load()
+        self.h = ctypes.c_void_p()
+        opts = ilg_opts(device=device)
+        rc = self.L.ilg_create(ctypes.byref(self.h), ctypes.byref(opts))
+        if rc != ILG_OK:
+            raise IlgError(rc, f"ilg_create(device={device}) failed")
+        self.n_tris = 0
+
+    def _check(self, rc: int):
+        if rc != ILG_OK:
+            raise IlgError(rc, self.L.ilg_last_error(self.h).decode(errors="replace"))
+
+    # ISpace::Initialise + PrimitiveList fill
+    def initialise(self, positions, indices, material_ids=None):
+        pos = np.ascontiguousarray(positions, np.float32).reshape(-1, 3)
+        idx = np.ascontiguousarray(indices, np.uint32).reshape(-1, 3)
+        mat = None if material_ids is None else np.ascontiguousarray(material_ids, np.uint32)
+        self._check(self.L.ilg_set_mesh(self.h, pos.ctypes.data, pos.shape[0], idx.ctypes.data, idx.shape[0],
+                                        None if mat is None else mat.ctypes.data))
+        self.n_tris = idx.shape[0]
+
+    # ISpace::Build
+    def build(self):
+        self._check(self.L.ilg_build(self.h))
+
+    def stats(self) -> dict:
+        s = ilg_stats()
+        self._check(self.L.ilg_get_stats(self.h, ctypes.byref(s)))
+        return {k: getattr(s, k) for k, _ in s._fields_}
+
+    @property
+    def stream(self) -> int:
+        return self.L.ilg_stream(self.h) or 0
+
+    # ISpace::Intersects(ray, isect), batched; host arrays
+    def intersects(self, o4: np.ndarray, d4: np.ndarray):
+        o4 = np.ascontiguousarray(o4, np.float32)
+        d4 = np.ascontiguousarray(d4, np.float32)
+        n = o4.shape[0]
+        prim = np.empty(n, np.int32)
+        t, u, v = (np.empty(n, np.float32) for _ in range(3))
+        self._check(self.L.ilg_intersect(self.h, o4.ctypes.data, d4.ctypes.data, n, prim.ctypes.data,
+                                         t.ctypes.data, u.ctypes.data, v.ctypes.data, 0))
+        return prim, t, u, v
+
+    def intersects_into(self, o4, d4, prim, t, u, v, device_ptrs: bool):
+        """Same query on caller-owned buffers (numpy, pinned or device torch tensors)."""
+        n = o4.shape[0]
+        self._check(self.L.ilg_intersect(self.h, _ptr(o4), _ptr(d4), n, _ptr(prim), _ptr(t), _ptr(u), _ptr(v),
+                                         ILG_DEVICE_PTRS if device_ptrs else 0))
+
+    def traversal_counts(self, o4, d4):
+        """(node records read, triangle records tested) for one closest-hit pass
+        over device-resident rays (torch tensors)."""
+        import torch
+        n = o4.shape[0]
+        prim = torch.empty(n, dtype=torch.int32, device=o4.device)
+        t, u, v = (torch.empty(n, dtype=torch.float32, device=o4.device) for _ in range(3))
+        counts = np.zeros(2, np.uint64)
+        self._check(self.L.ilg_intersect_counted(self.h, _ptr(o4), _ptr(d4), n, _ptr(prim), _ptr(t), _ptr(u),
+                                                 _ptr(v), counts.ctypes.data, ILG_DEVICE_PTRS))
+        return int(counts[0]), int(counts[1])
+
+    # ISpace::Intersects(ray), batched
+    def occluded(self, o4: np.ndarray, d4: np.ndarray) -> np.ndarray:
+        o4 = np.ascontiguousarray(o4, np.float32)
+        d4 = np.ascontiguousarray(d4, np.float32)
+        occ = np.empty(o4.shape[0], np.uint8)
+        self._check(self.L.ilg_occluded(self.h, o4.ctypes.data, d4.ctypes.data, o4.shape[0], occ.ctypes.data, 0))
+        return occ
+
+    def occluded_into(self, o4, d4, occ, device_ptrs: bool):
+        self._check(self.L.ilg_occluded(self.h, _ptr(o4), _ptr(d4), o4.shape[0], _ptr(occ),
+                                        ILG_DEVICE_PTRS if device_ptrs else 0))
+
+    def sync(self):
+        self._check(self.L.ilg_sync(self.h))
+
+    def close(self):
+        if self.h:
+            self.L.ilg_destroy(self.h)
+            self.h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

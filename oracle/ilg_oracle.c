@@ -47,6 +47,11 @@ static int shirley_tri(const otri *tr, const float o[3], const float d[3], float
     if (beta < 0.0f) return 0;
     const float gamma = DOT(interm, tr->e1) * rcp;
     if (beta + gamma > 1.0f || gamma < 0.0f) return 0;
+    /* A zero-area triangle gives n = 0 and t = 0 * inf = NaN, which passes
+     * every comparison above in the reference and is then reported as a hit
+     * whose distance poisons ray.Max; which rays meet it depends on the tree.
+     * The oracle (like the device) rejects it. */
+    if (t != t) return 0;
     *t_out = t;
     *b_out = beta;
     *g_out = gamma;

@@ -1,0 +1,43 @@
+"""The C ABI library: builds for sm_100a, loads, exports every declared symbol."""
+import ctypes
+import os
+import re
+
+import pytest
+
+from tests.conftest import ROOT, cuda_available
+
+
+def declared_symbols():
+    names = set()
+    for h in os.listdir(os.path.join(ROOT, "include")):
+        if h.endswith(".h"):
+            src = open(os.path.join(ROOT, "include", h)).read()
+            names |= set(re.findall(r"^\s*(?:const\s+)?(?:int|void|const char|char)\s*\*?\s*(ilg_\w+)\s*\(", src, re.M))
+    return sorted(names)
+
+
+def test_header_declares_entry_points():
+    names = declared_symbols()
+    for must in ("ilg_create", "ilg_destroy", "ilg_set_mesh", "ilg_build", "ilg_intersect", "ilg_occluded"):
+        assert must in names
+
+
+def test_library_exports_every_declared_symbol():
+    from illuminaprt_b200 import build
+    lib = ctypes.CDLL(build.build())
+    missing = [s for s in declared_symbols() if not hasattr(lib, s)]
+    assert missing == []
+
+
+def test_binding_lists_every_symbol():
+    from illuminaprt_b200.ilg import EXPORTED
+    assert sorted(EXPORTED) == sorted(s for s in declared_symbols() if s in EXPORTED)
+    assert set(declared_symbols()) <= set(EXPORTED) | {s for s in declared_symbols() if not s.startswith("ilg_")}
+
+
+@pytest.mark.skipif(cuda_available(), reason="checks the no-GPU error path")
+def test_create_without_gpu_fails_loudly():
+    from illuminaprt_b200.ilg import GpuSpace, IlgError
+    with pytest.raises(IlgError):
+        GpuSpace()

@@ -1,0 +1,63 @@
+"""The CPU oracle against the reference's own outputs (golden fixtures)."""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from tests.parity import classify
+
+GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "heightfield_*.npz")))
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p) for p in GOLDEN])
+@pytest.mark.parametrize("tree", ["kd", "bvh"])
+def test_oracle_matches_reference_golden(path, tree, oracle):
+    g = np.load(path)
+    pos, idx, o4, d4 = g["pos"], g["idx"], g["o4"], g["d4"]
+    ref = (g[f"{tree}_prim"], g[f"{tree}_t"], g[f"{tree}_u"], g[f"{tree}_v"])
+    bvh = oracle.bvh(pos, idx)
+    got = bvh.intersect(o4, d4, nthreads=2)
+    n_same, ties, bad, bits_ok = classify(pos, idx, o4, d4, got, ref, oracle)
+    assert bad == [], f"non-tie mismatches at {bad[:10]}"
+    assert bits_ok, "t/u/v differ in bits where the hit matches"
+    assert ties <= max(2, len(o4) // 1000)
+    # brute force over all triangles (the reference's linear loop) agrees too
+    bf = oracle.intersect_brute(pos, idx, o4, d4)
+    n_same, ties, bad, bits_ok = classify(pos, idx, o4, d4, bf, ref, oracle)
+    assert bad == [] and bits_ok
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p) for p in GOLDEN])
+def test_oracle_any_hit_matches_reference_golden(path, oracle):
+    g = np.load(path)
+    bvh = oracle.bvh(g["pos"], g["idx"])
+    occ = bvh.occluded(g["so"], g["sd"], nthreads=2)
+    assert np.array_equal(occ, g["kd_occ"])
+    assert np.array_equal(occ, g["bvh_occ"])
+
+
+def test_shirley_window_edges(oracle):
+    """The reference's window: 1e-5 <= t <= Max - 1e-5, both sides in double."""
+    pos = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0]], np.float32)
+    idx = np.array([[0, 1, 2]], np.uint32)
+    d = np.array([0, 0, -1, 0], np.float32)
+    for oz, tmax, expect in [(1.0, 3.4e38, True), (1.0, 1.0, False), (1.0, 1.00002, True),
+                             (5e-6, 3.4e38, False), (2e-5, 3.4e38, True)]:
+        o = np.array([0.25, 0.25, oz, 0], np.float32)
+        acc, t, b, g = oracle.shirley(pos, idx.reshape(-1), 0, o, d, tmax)
+        assert acc == expect, (oz, tmax)
+        if acc:
+            assert (b, g) == (np.float32(0.25), np.float32(0.25))
+
+
+def test_edge_cases_miss_parallel_empty(oracle):
+    pos = np.array([[0, 0, 0], [1, 0, 0], [0, 1, 0]], np.float32)
+    idx = np.array([[0, 1, 2]], np.uint32)
+    o4 = np.array([[0.25, 0.25, 1, 0], [5, 5, 1, 0], [0.25, 0.25, 1, 0], [0.25, 0.25, 1, 0]], np.float32)
+    d4 = np.array([[0, 0, -1, 3.4e38], [0, 0, -1, 3.4e38], [1, 0, 0, 3.4e38], [0, 0, 1, 3.4e38]], np.float32)
+    p, t, u, v = oracle.intersect_brute(pos, idx, o4, d4)
+    assert list(p) == [0, -1, -1, -1]
+    assert np.isinf(t[1:]).all()
+    p2 = oracle.bvh(pos, idx).intersect(o4, d4, nthreads=1)[0]
+    assert list(p2) == [0, -1, -1, -1]

@@ -1,0 +1,141 @@
+"""Parity of the sm_100a closest-hit / any-hit kernels (through the C ABI)."""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from illuminaprt_b200 import scenes
+from tests.parity import classify
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "heightfield_*.npz")))
+
+
+def space_for(pos, idx):
+    from illuminaprt_b200.ilg import GpuSpace
+    s = GpuSpace()
+    s.initialise(pos, idx)
+    s.build()
+    return s
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p) for p in GOLDEN])
+def test_closest_hit_matches_reference_golden(path, oracle):
+    g = np.load(path)
+    pos, idx, o4, d4 = g["pos"], g["idx"], g["o4"], g["d4"]
+    got = space_for(pos, idx).intersects(o4, d4)
+    for tree in ("kd", "bvh"):
+        ref = (g[f"{tree}_prim"], g[f"{tree}_t"], g[f"{tree}_u"], g[f"{tree}_v"])
+        n_same, ties, bad, bits_ok = classify(pos, idx, o4, d4, got, ref, oracle)
+        assert bad == [], f"{tree}: non-tie mismatches at {bad[:10]}"
+        assert bits_ok, f"{tree}: t/u/v bits differ on matching hits"
+        assert ties <= max(2, len(o4) // 1000)
+
+
+@pytest.mark.parametrize("path", GOLDEN, ids=[os.path.basename(p) for p in GOLDEN])
+def test_any_hit_matches_reference_golden(path):
+    g = np.load(path)
+    occ = space_for(g["pos"], g["idx"]).occluded(g["so"], g["sd"])
+    assert np.array_equal(occ, g["kd_occ"])
+
+
+@pytest.mark.parametrize("nx,ny", [(256, 128), (97, 61)])
+def test_closest_hit_matches_oracle_seeded(nx, ny, oracle):
+    pos, idx = scenes.heightfield(nx, ny, 0.2, 7)
+    co, cd = scenes.pinhole_rays(256, 256, (0.5, -0.6, 0.8), (0.5, 0.5, 0.0), (0, 0, 1), 60.0)
+    io, idr = scenes.incoherent_rays(pos, idx, 65536, 8)
+    o4 = np.concatenate([co, io])
+    d4 = np.concatenate([cd, idr])
+    got = space_for(pos, idx).intersects(o4, d4)
+    ref = oracle.bvh(pos, idx).intersect(o4, d4)
+    n_same, ties, bad, bits_ok = classify(pos, idx, o4, d4, got, ref, oracle)
+    assert bad == [] and bits_ok
+    assert ties <= len(o4) // 10000 + 2
+    occ = space_for(pos, idx).occluded(o4, d4)
+    assert np.array_equal(occ.astype(bool), ref[0] >= 0)
+
+
+def test_full_size_heightfield_sample(oracle):
+    """The 1,048,576-triangle heightfield; a seeded sample of both ray sets."""
+    pos, idx = scenes.heightfield(1024, 512, 0.2, 1)
+    co, cd = scenes.coherent_rays(2048)
+    io, idr = scenes.incoherent_rays(pos, idx, 1 << 20, 2)
+    rng = np.random.default_rng(5)
+    pick = rng.choice(co.shape[0], 1 << 17, replace=False)
+    o4 = np.concatenate([co[pick], io[: 1 << 17]])
+    d4 = np.concatenate([cd[pick], idr[: 1 << 17]])
+    sp = space_for(pos, idx)
+    st = sp.stats()
+    assert st["n_leaf_tris"] == idx.shape[0]
+    got = sp.intersects(o4, d4)
+    ref = oracle.bvh(pos, idx).intersect(o4, d4)
+    n_same, ties, bad, bits_ok = classify(pos, idx, o4, d4, got, ref, oracle)
+    assert bad == [] and bits_ok
+    assert ties / len(o4) < 1e-3
+    # size-independent property on the whole incoherent set: a ray that hits
+    # reports a t inside its window and barycentrics inside the triangle
+    p, t, u, v = sp.intersects(io, idr)
+    h = p >= 0
+    assert (t[h] >= 1e-5).all() and (u[h] >= 0).all() and (v[h] >= 0).all() and ((u + v)[h] <= 1.0).all()
+    # determinism
+    p2, t2, _, _ = sp.intersects(io, idr)
+    assert np.array_equal(p, p2) and np.array_equal(t.view(np.uint32), t2.view(np.uint32))
+
+
+@pytest.mark.parametrize("ntris", [1, 2, 3, 4, 9])
+def test_tiny_scenes(ntris, oracle):
+    rng = np.random.default_rng(ntris)
+    pos = rng.random((3 * ntris, 3)).astype(np.float32)
+    idx = np.arange(3 * ntris, dtype=np.uint32).reshape(-1, 3)
+    o4 = np.zeros((4096, 4), np.float32)
+    d4 = np.zeros((4096, 4), np.float32)
+    o4[:, :3] = rng.random((4096, 3)) * 2 - 0.5
+    dd = rng.normal(size=(4096, 3))
+    d4[:, :3] = dd / np.linalg.norm(dd, axis=1, keepdims=True)
+    d4[:, 3] = 3.4e38
+    got = space_for(pos, idx).intersects(o4, d4)
+    ref = oracle.intersect_brute(pos, idx, o4, d4)
+    n_same, ties, bad, bits_ok = classify(pos, idx, o4, d4, got, ref, oracle)
+    assert bad == [] and bits_ok
+
+
+def test_degenerate_and_duplicate_triangles(oracle):
+    pos, idx = scenes.heightfield(32, 16, 0.1, 3)
+    # duplicate every triangle and add zero-area ones: identical centroids stress the build
+    idx = np.concatenate([idx, idx, np.array([[0, 0, 0], [1, 1, 2]], np.uint32)])
+    co, cd = scenes.pinhole_rays(64, 64, (0.5, -0.6, 0.8), (0.5, 0.5, 0.0), (0, 0, 1), 60.0)
+    got = space_for(pos, idx).intersects(co, cd)
+    ref = oracle.intersect_brute(pos, idx, co, cd)
+    n_same, ties, bad, bits_ok = classify(pos, idx, co, cd, got, ref, oracle)
+    assert bad == [] and bits_ok
+
+
+def test_device_pointer_path_and_errors():
+    import torch
+    from illuminaprt_b200.ilg import GpuSpace, IlgError, ILG_ESTATE, ILG_EINVAL
+    pos, idx = scenes.heightfield(64, 32, 0.2, 1)
+    co, cd = scenes.pinhole_rays(64, 64, (0.5, -0.6, 0.8), (0.5, 0.5, 0.0), (0, 0, 1), 60.0)
+    s = GpuSpace()
+    with pytest.raises(IlgError) as e:
+        s.intersects(co, cd)
+    assert e.value.code == ILG_ESTATE
+    with pytest.raises(IlgError) as e:
+        s.initialise(pos, np.array([[0, 1, 10 ** 7]], np.uint32))
+    assert e.value.code == ILG_EINVAL
+    s.initialise(pos, idx)
+    s.build()
+    host = s.intersects(co, cd)
+    o = torch.from_numpy(co).cuda()
+    d = torch.from_numpy(cd).cuda()
+    n = co.shape[0]
+    prim = torch.empty(n, dtype=torch.int32, device="cuda")
+    t, u, v = (torch.empty(n, dtype=torch.float32, device="cuda") for _ in range(3))
+    torch.cuda.synchronize()
+    s.intersects_into(o, d, prim, t, u, v, device_ptrs=True)
+    s.sync()
+    assert np.array_equal(prim.cpu().numpy(), host[0])
+    assert np.array_equal(t.cpu().numpy().view(np.uint32), host[1].view(np.uint32))
+    # zero rays is a no-op
+    s.intersects(co[:0], cd[:0])
