@@ -164,6 +164,7 @@ __global__ void k_karras(const uint32_t *__restrict__ keys, int n, int2 *__restr
     int right = (last == gamma + 1) ? ~(gamma + 1) : gamma + 1;
     child[i] = make_int2(left, right);
     range[i] = make_int2(first, last);
+    if (i == 0) parent_int[0] = -1;  // the root ends every bottom-up walk
     if (left >= 0) parent_int[left] = i; else parent_leaf[~left] = i;
     if (right >= 0) parent_int[right] = i; else parent_leaf[~right] = i;
 }
@@ -178,7 +179,7 @@ __global__ void k_refit(int n, const uint32_t *__restrict__ sorted_tri, const fl
     if (i >= n) return;
     int p = parent_leaf[i];
     // bounded by the tree height (< n); each node's second arrival proceeds
-    for (int guard = 0; p >= 0 && guard < n; guard++) {
+    for (int guard = 0; p >= 0 && p < n - 1 && guard < n; guard++) {
         __threadfence();
         if (atomicAdd(&arrivals[p], 1u) == 0) return;
         __threadfence();
