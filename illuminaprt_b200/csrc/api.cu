@@ -11,6 +11,7 @@
 #include "build.cuh"
 #include "trace_api.cuh"
 #include "ctx.cuh"
+#include "render.cuh"
 
 using namespace ilg;
 
@@ -117,6 +118,7 @@ int ilg_set_mesh(ilg_ctx *ctx, const float *pos_xyz, uint32_t n_verts, const uin
     ctx->has_mat = mat_ids != nullptr;
     ctx->max_abs = maxabs;
     ctx->built = false;
+    ctx->attr_dirty = true;
     return ILG_OK;
 }
 
@@ -144,6 +146,7 @@ int ilg_build(ilg_ctx *ctx)
     ctx->stats.node_bytes = (uint64_t)res.n_nodes * sizeof(Node8);
     ctx->stats.tri_bytes = (uint64_t)res.n_tris * sizeof(Tri);
     ctx->built = true;
+    ctx->attr_dirty = true;
     return ILG_OK;
 }
 
@@ -236,6 +239,178 @@ int ilg_occluded(ilg_ctx *ctx, const float *ray_o_tmin, const float *ray_d_tmax,
     CK(cudaMemcpyAsync(occ, ctx->hocc.ptr, n, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     return ctx->check_device_error();
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// path tracing
+// ---------------------------------------------------------------------------
+namespace {
+
+struct V3 {
+    float x, y, z;
+};
+inline V3 v3(const float *a) { return V3{a[0], a[1], a[2]}; }
+inline V3 operator-(V3 a, V3 b) { return V3{a.x - b.x, a.y - b.y, a.z - b.z}; }
+inline V3 operator+(V3 a, V3 b) { return V3{a.x + b.x, a.y + b.y, a.z + b.z}; }
+inline V3 operator*(float s, V3 a) { return V3{s * a.x, s * a.y, s * a.z}; }
+inline float dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+inline V3 cross(V3 a, V3 b) { return V3{a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; }
+inline V3 normalize(V3 a)
+{
+    float l = std::sqrt(dot(a, a));
+    return l > 0.f ? (1.f / l) * a : a;
+}
+inline float3 f3(V3 a) { return make_float3(a.x, a.y, a.z); }
+
+}  // namespace
+
+extern "C" {
+
+int ilg_set_materials(ilg_ctx *ctx, const ilg_material *mats, uint32_t n)
+{
+    if (!ctx) return ILG_EINVAL;
+    if (!mats || n == 0 || n > 0xffffu) return fail(ctx, ILG_EINVAL, "ilg_set_materials: need 1..65535 materials");
+    static_assert(sizeof(ilg_material) == sizeof(Mat), "ilg_material layout");
+    for (uint32_t i = 0; i < n; i++) {
+        if (mats[i].kind > ILG_MAT_GGX) return fail(ctx, ILG_EINVAL, "ilg_set_materials: material %u has unknown kind %u", i, mats[i].kind);
+        if (mats[i].kind == ILG_MAT_GGX && !(mats[i].alpha > 0.f && mats[i].alpha <= 1.f))
+            return fail(ctx, ILG_EINVAL, "ilg_set_materials: material %u needs 0 < alpha <= 1", i);
+    }
+    CK(cudaSetDevice(ctx->device));
+    CK(ctx->mats.reserve(n));
+    CK(cudaMemcpyAsync(ctx->mats.ptr, mats, n * sizeof(Mat), cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->n_mats = n;
+    return ILG_OK;
+}
+
+int ilg_set_quad_lights(ilg_ctx *ctx, const ilg_quad_light *lights, uint32_t n)
+{
+    if (!ctx) return ILG_EINVAL;
+    if (n > kMaxLights) return fail(ctx, ILG_EINVAL, "ilg_set_quad_lights: at most %u lights", kMaxLights);
+    if (n && !lights) return fail(ctx, ILG_EINVAL, "ilg_set_quad_lights: null lights");
+    QuadLight hl[kMaxLights];
+    uint32_t first[kMaxLights];
+    for (uint32_t i = 0; i < n; i++) {
+        const ilg_quad_light &L = lights[i];
+        if (ctx->n_tris && (uint64_t)L.first_tri + 1 >= ctx->n_tris)
+            return fail(ctx, ILG_EINVAL, "ilg_set_quad_lights: light %u triangles out of range", i);
+        V3 p0 = v3(L.v[0]), p1 = v3(L.v[1]), p2 = v3(L.v[2]), p3 = v3(L.v[3]);
+        V3 n0 = cross(p2 - p0, p1 - p0);   // triangle (v1, v3, v2)
+        V3 n1 = cross(p3 - p0, p2 - p0);   // triangle (v1, v4, v3)
+        float area = 0.5f * std::sqrt(dot(n0, n0)) + 0.5f * std::sqrt(dot(n1, n1));
+        if (!(area > 0.f)) return fail(ctx, ILG_EINVAL, "ilg_set_quad_lights: light %u has zero area", i);
+        hl[i].p[0] = f3(p0); hl[i].p[1] = f3(p1); hl[i].p[2] = f3(p2); hl[i].p[3] = f3(p3);
+        hl[i].emit = make_float3(L.emit[0], L.emit[1], L.emit[2]);
+        hl[i].n = f3(normalize(n0));
+        hl[i].area = area;
+        first[i] = L.first_tri;
+    }
+    CK(cudaSetDevice(ctx->device));
+    CK(ctx->lights.reserve(kMaxLights));
+    CK(ctx->light_first_tri.reserve(kMaxLights));
+    if (n) {
+        CK(cudaMemcpyAsync(ctx->lights.ptr, hl, n * sizeof(QuadLight), cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaMemcpyAsync(ctx->light_first_tri.ptr, first, n * sizeof(uint32_t), cudaMemcpyHostToDevice, ctx->stream));
+    }
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->n_lights = n;
+    memcpy(ctx->light_first_host, first, n * sizeof(uint32_t));
+    ctx->attr_dirty = true;
+    return ILG_OK;
+}
+
+int ilg_render(ilg_ctx *ctx, const ilg_camera *cam, const ilg_render_opts *opts, float *out_rgb, uint32_t flags)
+{
+    if (!ctx) return ILG_EINVAL;
+    if (!cam || !opts || !out_rgb) return fail(ctx, ILG_EINVAL, "ilg_render: null argument");
+    if (flags & ~ILG_DEVICE_PTRS) return fail(ctx, ILG_EINVAL, "ilg_render: unknown flags 0x%x", flags);
+    if (!ctx->built) return fail(ctx, ILG_ESTATE, "ilg_render: scene not built");
+    if (!ctx->has_mat || ctx->n_mats == 0) return fail(ctx, ILG_ESTATE, "ilg_render: materials not set");
+    const uint32_t W = opts->width, H = opts->height;
+    if (W == 0 || H == 0 || opts->spp == 0 || (uint64_t)W * H > (1u << 26))
+        return fail(ctx, ILG_EINVAL, "ilg_render: bad image size %ux%u or spp %u", W, H, opts->spp);
+    if (opts->max_depth == 0 || opts->max_depth > 64) return fail(ctx, ILG_EINVAL, "ilg_render: max_depth must be 1..64");
+    for (uint32_t l = 0; l < ctx->n_lights; l++)
+        if ((uint64_t)ctx->light_first_host[l] + 1 >= ctx->n_tris)
+            return fail(ctx, ILG_EINVAL, "ilg_render: light %u triangles out of range of the mesh", l);
+    CK(cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    const uint32_t n = ctx->n_tris;
+    if (ctx->attr_dirty) {
+        CK(ctx->tri_attr.reserve(n));
+        CK(ctx->light_of_prim.reserve(n));
+        CK(build_tri_attr(ctx->bb.prim_of, n, ctx->mat.ptr, ctx->light_first_tri.ptr, ctx->n_lights,
+                          ctx->light_of_prim.ptr, ctx->tri_attr.ptr, st));
+        ctx->attr_dirty = false;
+    }
+    const uint32_t wh = W * H;
+    uint32_t cap = opts->paths_per_wave ? opts->paths_per_wave : (1u << 22);
+    uint32_t spp_per_wave = std::max<uint32_t>(1u, cap / wh);
+    spp_per_wave = std::min(spp_per_wave, opts->spp);
+    cap = wh * spp_per_wave;
+    const uint32_t nl = std::max<uint32_t>(1u, ctx->n_lights);
+    CK(ctx->q_o0.reserve(cap)); CK(ctx->q_d0.reserve(cap)); CK(ctx->q_o1.reserve(cap)); CK(ctx->q_d1.reserve(cap));
+    CK(ctx->q_p0.reserve(cap)); CK(ctx->q_p1.reserve(cap)); CK(ctx->beta.reserve(cap));
+    CK(ctx->hit_tri.reserve(cap)); CK(ctx->hit_t.reserve(cap));
+    CK(ctx->s_o.reserve((size_t)cap * nl)); CK(ctx->s_d.reserve((size_t)cap * nl)); CK(ctx->s_c.reserve((size_t)cap * nl));
+    CK(ctx->counts.reserve(4)); CK(ctx->accum.reserve(wh));
+    CK(cudaMemsetAsync(ctx->accum.ptr, 0, sizeof(float4) * wh, st));
+
+    // camera frame: PerspectiveCamera(eye, normalize(target - eye), up, -1,1,-1,1, 1)
+    // + SetFieldOfView (Core/Camera/Camera.cpp:30-44, Basis.cpp:28-44)
+    V3 eye = v3(cam->eye);
+    V3 w = normalize(normalize(v3(cam->target) - eye));
+    V3 v = normalize(v3(cam->up));
+    v = v - dot(v, w) * w;
+    if (dot(v, v) <= 1.1920929e-7f) {
+        v = V3{w.z, w.x, w.y};
+        v = normalize(cross(v, w));
+        v = normalize(v - dot(v, w) * w);
+    }
+    V3 u = cross(v, w);
+    const float half = cam->fov_deg * (std::atan(1.0f) / 45.0f) * 0.5f;
+    const float v1 = std::tan(half), v0 = -v1, u0 = v0 * cam->aspect, u1 = v1 * cam->aspect;
+
+    RenderDev R = {};
+    R.nodes = ctx->bb.nodes; R.tris = ctx->bb.tris; R.n_nodes = ctx->stats.n_nodes; R.n_tris = ctx->stats.n_tris;
+    R.tri_attr = ctx->tri_attr.ptr; R.mats = ctx->mats.ptr; R.n_mats = ctx->n_mats;
+    R.lights = ctx->lights.ptr; R.n_lights = ctx->n_lights;
+    R.sky = make_float3(opts->sky[0], opts->sky[1], opts->sky[2]);
+    R.centre = f3(eye);
+    R.corner = f3(eye + u0 * u + v0 * v + 1.0f * w);
+    R.across = f3((u1 - u0) * u);
+    R.up = f3((v1 - v0) * v);
+    R.width = W; R.height = H; R.wh = wh; R.rcp_w = 1.f / W; R.rcp_h = 1.f / H;
+    R.max_depth = opts->max_depth; R.eps = opts->epsilon; R.seed = opts->seed;
+    R.q_o[0] = ctx->q_o0.ptr; R.q_o[1] = ctx->q_o1.ptr; R.q_d[0] = ctx->q_d0.ptr; R.q_d[1] = ctx->q_d1.ptr;
+    R.q_path[0] = ctx->q_p0.ptr; R.q_path[1] = ctx->q_p1.ptr;
+    R.count = ctx->counts.ptr; R.capacity = cap;
+    R.hit_tri = ctx->hit_tri.ptr; R.hit_t = ctx->hit_t.ptr; R.beta = ctx->beta.ptr;
+    R.s_o = ctx->s_o.ptr; R.s_d = ctx->s_d.ptr; R.s_c = ctx->s_c.ptr;
+    R.sh_count = ctx->counts.ptr + 2; R.sh_capacity = cap * nl;
+    R.accum = ctx->accum.ptr; R.err = ctx->derr.ptr;
+
+    uint32_t launches = 0;
+    for (uint32_t s0 = 0; s0 < opts->spp; s0 += spp_per_wave) {
+        const uint32_t k = std::min(spp_per_wave, opts->spp - s0);
+        CK(render_wave(R, wh * k, s0, st, &launches));
+    }
+    float *out_dev = out_rgb;
+    if (!(flags & ILG_DEVICE_PTRS)) {
+        CK(ctx->out_dev.reserve(3ull * wh));
+        out_dev = ctx->out_dev.ptr;
+    }
+    CK(render_resolve(ctx->accum.ptr, wh, 1.f / opts->spp, out_dev, st));
+    ctx->last_render_launches = launches + 1;
+    if (!(flags & ILG_DEVICE_PTRS)) {
+        CK(cudaMemcpyAsync(out_rgb, out_dev, 12ull * wh, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        return ctx->check_device_error();
+    }
+    return ILG_OK;
 }
 
 }  // extern "C"

@@ -6,6 +6,7 @@
 #include "build.cuh"
 #include "ilg.h"
 #include "trace_api.cuh"
+#include "render.cuh"
 
 struct ilg_ctx {
     int device = 0;
@@ -35,6 +36,22 @@ struct ilg_ctx {
     ilg::DevBuf<uint32_t> derr;
     ilg::DevBuf<unsigned long long> dstats;
 
+    // path tracing: scene attributes
+    ilg::DevBuf<ilg::Mat> mats;
+    uint32_t n_mats = 0;
+    ilg::DevBuf<ilg::QuadLight> lights;
+    ilg::DevBuf<uint32_t> light_first_tri;
+    uint32_t n_lights = 0;
+    uint32_t light_first_host[ilg::kMaxLights] = {};
+    ilg::DevBuf<uint32_t> tri_attr, light_of_prim;
+    bool attr_dirty = true;
+    // path tracing: wavefront buffers
+    ilg::DevBuf<float4> q_o0, q_d0, q_o1, q_d1, beta, s_o, s_d, s_c, accum;
+    ilg::DevBuf<uint32_t> q_p0, q_p1, counts;
+    ilg::DevBuf<int> hit_tri;
+    ilg::DevBuf<float> hit_t, out_dev;
+    uint32_t last_render_launches = 0;
+
     ilg::SceneView view() const
     {
         return ilg::SceneView{bb.nodes, bb.tris, bb.prim_of, stats.n_nodes, stats.n_tris};
@@ -61,5 +78,9 @@ struct ilg_ctx {
         bb.release_all();
         ro.release(); rd.release(); hprim.release(); ht.release(); hu.release(); hv.release(); hocc.release();
         derr.release(); dstats.release();
+        mats.release(); lights.release(); light_first_tri.release(); tri_attr.release(); light_of_prim.release();
+        q_o0.release(); q_d0.release(); q_o1.release(); q_d1.release(); beta.release(); s_o.release();
+        s_d.release(); s_c.release(); accum.release(); q_p0.release(); q_p1.release(); counts.release();
+        hit_tri.release(); hit_t.release(); out_dev.release();
     }
 };

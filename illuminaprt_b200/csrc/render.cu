@@ -1,0 +1,430 @@
+// Wavefront path tracer: the reference's PathIntegrator::Radiance bounce loop
+// (Core/Integrator/PathIntegrator.cpp:44-367) restated as queue-driven
+// kernels over SoA path state:
+//
+//   k_camera   one camera ray per (pixel, sample) of the wave
+//              (BaseRenderer::RenderRegion, Core/Renderer/BaseRenderer.cpp:62-169;
+//               PerspectiveCamera::GetRay, Core/Camera/PerspectiveCamera.cpp:44-60)
+//   k_extend   closest hit of every queued ray (the traversal of trace.cuh)
+//   k_shade    emission at depth 0, NEE toward every quad light but the hit one
+//              (IIntegrator::SampleAllLights / EstimateDirectLighting,
+//               Core/Integrator/Integrator.cpp:114-185; DiffuseAreaLight,
+//               Core/Light/DiffuseAreaLight.cpp:52-69), BSDF sample, throughput,
+//              Russian roulette after depth 3, spawn offset along the
+//              geometric normal; pushes shadow rays and continuations with
+//              warp-aggregated atomics (the queue compaction)
+//   k_shadow   any hit of every shadow segment; unoccluded contributions are
+//              added to the pixel
+//   k_resolve  pixel sums / spp
+//
+// Random numbers come from a counter-based hash of (seed, pixel, sample,
+// depth, dimension) instead of the reference's shared Mersenne twister, so
+// images agree with the reference statistically, not bit for bit.
+#include "bvh8.cuh"
+#include "render.cuh"
+#include "trace.cuh"
+
+#include <cfloat>
+
+namespace ilg {
+
+namespace {
+
+constexpr float kInvPi = 0.318309886183790671538f;
+constexpr float kTwoPi = 6.28318530717958647692f;
+
+__device__ __forceinline__ uint64_t mix64(uint64_t x)
+{
+    x += 0x9E3779B97F4A7C15ull;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    return x ^ (x >> 31);
+}
+
+// uniform float in [0, 1) for one (path, dimension)
+__device__ __forceinline__ float rnd(uint64_t key, uint32_t dim)
+{
+    return (float)(uint32_t)(mix64(key + (uint64_t)dim * 0xD1B54A32D192ED03ull) >> 40) * 0x1p-24f;
+}
+
+__device__ __forceinline__ uint64_t path_key(uint32_t seed, uint64_t path_global)
+{
+    return mix64(path_global ^ ((uint64_t)seed * 0xA24BAED4963EE407ull));
+}
+
+// dimensions: per depth d, base 32*d: lights 2l, 2l+1 (l < 8); bsdf 20, 21, 22; roulette 23
+constexpr uint32_t kDimCam = 0xFFFFFF00u;
+__device__ __forceinline__ uint32_t dim_of(uint32_t depth, uint32_t k) { return depth * 32u + k; }
+
+__device__ __forceinline__ float3 operator+(float3 a, float3 b) { return make_float3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ float3 operator-(float3 a, float3 b) { return make_float3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ float3 operator*(float3 a, float s) { return make_float3(a.x * s, a.y * s, a.z * s); }
+__device__ __forceinline__ float3 operator*(float3 a, float3 b) { return make_float3(a.x * b.x, a.y * b.y, a.z * b.z); }
+__device__ __forceinline__ float dot3(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ float3 cross3(float3 a, float3 b)
+{
+    return make_float3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
+__device__ __forceinline__ float3 normalize3(float3 a) { return a * rsqrtf(dot3(a, a)); }
+__device__ __forceinline__ bool is_black(float3 a) { return a.x == 0.f && a.y == 0.f && a.z == 0.f; }
+
+// OrthonormalBasis::InitFromW, Core/Geometry/Basis.cpp:85-99
+__device__ __forceinline__ void onb_from_w(float3 w, float3 &u, float3 &v)
+{
+    if (fabsf(w.x) > fabsf(w.y)) {
+        float inv = 1.f / sqrtf(w.x * w.x + w.z * w.z);
+        v = make_float3(-w.z * inv, 0.f, w.x * inv);
+    } else {
+        float inv = 1.f / sqrtf(w.y * w.y + w.z * w.z);
+        v = make_float3(0.f, w.z * inv, -w.y * inv);
+    }
+    u = cross3(w, v);
+}
+
+// warp-aggregated queue push: returns this lane's slot (or 0xffffffff if !want)
+__device__ __forceinline__ uint32_t push_slot(bool want, uint32_t *count)
+{
+    const uint32_t mask = __ballot_sync(__activemask(), want);
+    if (!want) return 0xffffffffu;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t leader = __ffs(mask) - 1u;
+    uint32_t base = 0;
+    if (lane == leader) base = atomicAdd(count, (uint32_t)__popc(mask));
+    base = __shfl_sync(mask, base, leader);
+    return base + __popc(mask & ((1u << lane) - 1u));
+}
+
+__device__ __forceinline__ void add_pixel(float4 *accum, uint32_t pixel, float3 c)
+{
+    float *a = reinterpret_cast<float *>(accum + pixel);
+    atomicAdd(a, c.x);
+    atomicAdd(a + 1, c.y);
+    atomicAdd(a + 2, c.z);
+}
+
+__global__ void k_camera(RenderDev R, uint32_t n_paths, uint64_t sample0)
+{
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n_paths) return;
+    const uint32_t pixel = p % R.wh;
+    const uint64_t sample = sample0 + p / R.wh;
+    const uint32_t x = pixel % R.width, y = pixel / R.width;
+    const uint64_t key = path_key(R.seed, sample * R.wh + pixel);
+    // BoxFilter shifts the [0,1) sample by -0.5 (Core/Filter/BoxFilter.cpp:20-28)
+    const float xi1 = rnd(key, kDimCam) - 0.5f, xi2 = rnd(key, kDimCam + 1) - 0.5f;
+    const float fx = x * R.rcp_w + xi1 * R.rcp_w, fy = y * R.rcp_h + xi2 * R.rcp_h;
+    const float3 target = R.corner + R.across * fx + R.up * fy;
+    const float3 d = normalize3(target - R.centre);
+    R.q_o[0][p] = make_float4(R.centre.x, R.centre.y, R.centre.z, 0.f);
+    R.q_d[0][p] = make_float4(d.x, d.y, d.z, FLT_MAX);
+    R.q_path[0][p] = p;
+    R.beta[p] = make_float4(1.f, 1.f, 1.f, 0.f);
+}
+
+__global__ void __launch_bounds__(128) k_extend(RenderDev R, int cur)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= R.count[cur]) return;
+    const float4 o = R.q_o[cur][i], d = R.q_d[cur][i];
+    int best;
+    float bt, bu, bv;
+    unsigned long long nn = 0, nt = 0;
+    trace_one<false, false>(R.nodes, R.tris, R.n_nodes, R.n_tris, o, d, best, bt, bu, bv, R.err, nn, nt);
+    R.hit_tri[i] = best;
+    R.hit_t[i] = bt;
+}
+
+// GGX conductor (Trowbridge-Reitz D, Smith G1 separable, Schlick F), sampled
+// with the visible-normal distribution (Heitz 2018). Local frame: z = normal.
+__device__ __forceinline__ float ggx_d(float3 h, float a)
+{
+    const float a2 = a * a;
+    const float t = h.x * h.x / a2 + h.y * h.y / a2 + h.z * h.z;
+    return 1.f / (3.14159265358979f * a2 * t * t);
+}
+__device__ __forceinline__ float ggx_g1(float3 w, float a)
+{
+    const float z2 = w.z * w.z;
+    if (z2 <= 0.f) return 0.f;
+    const float t2 = (w.x * w.x + w.y * w.y) * a * a / z2;
+    return 2.f / (1.f + sqrtf(1.f + t2));
+}
+__device__ __forceinline__ float3 schlick(float3 f0, float c)
+{
+    const float m = 1.f - fminf(fmaxf(c, 0.f), 1.f);
+    const float m5 = m * m * m * m * m;
+    return f0 + (make_float3(1.f, 1.f, 1.f) - f0) * m5;
+}
+__device__ __forceinline__ float3 ggx_f(float3 wo, float3 wi, float3 f0, float a)
+{
+    if (wo.z <= 0.f || wi.z <= 0.f) return make_float3(0.f, 0.f, 0.f);
+    const float3 h = normalize3(wo + wi);
+    const float g = ggx_g1(wo, a) * ggx_g1(wi, a);
+    return schlick(f0, dot3(wi, h)) * (ggx_d(h, a) * g / (4.f * wo.z * wi.z));
+}
+__device__ __forceinline__ float ggx_pdf(float3 wo, float3 wi, float a)
+{
+    if (wo.z <= 0.f || wi.z <= 0.f) return 0.f;
+    const float3 h = normalize3(wo + wi);
+    // pdf of the visible normal h, times the reflection Jacobian 1 / (4 wo.h)
+    return ggx_g1(wo, a) * fmaxf(dot3(wo, h), 0.f) * ggx_d(h, a) / wo.z / (4.f * dot3(wo, h));
+}
+__device__ __forceinline__ float3 ggx_sample_vndf(float3 wo, float a, float u1, float u2)
+{
+    const float3 vh = normalize3(make_float3(a * wo.x, a * wo.y, wo.z));
+    const float lensq = vh.x * vh.x + vh.y * vh.y;
+    const float3 t1 = lensq > 0.f ? make_float3(-vh.y, vh.x, 0.f) * rsqrtf(lensq) : make_float3(1.f, 0.f, 0.f);
+    const float3 t2 = cross3(vh, t1);
+    const float r = sqrtf(u1);
+    float s, c;
+    sincosf(kTwoPi * u2, &s, &c);
+    const float p1 = r * c;
+    float p2 = r * s;
+    const float sh = 0.5f * (1.f + vh.z);
+    p2 = (1.f - sh) * sqrtf(fmaxf(0.f, 1.f - p1 * p1)) + sh * p2;
+    const float3 nh = t1 * p1 + t2 * p2 + vh * sqrtf(fmaxf(0.f, 1.f - p1 * p1 - p2 * p2));
+    const float3 h = normalize3(make_float3(a * nh.x, a * nh.y, fmaxf(0.f, nh.z)));
+    const float3 wi = h * (2.f * dot3(wo, h)) - wo;
+    return wi;
+}
+
+// BSDF::F for one material in the local frame (Core/Material/BSDF.cpp:214-234:
+// reflection lobes only count when wi.z > 0)
+__device__ __forceinline__ float3 bsdf_f(const Mat &m, float3 wo, float3 wi)
+{
+    if (m.kind == 1u) return ggx_f(wo, wi, m.f0, m.alpha);
+    if (wi.z > 0.f) return m.albedo * kInvPi;
+    return make_float3(0.f, 0.f, 0.f);
+}
+
+__global__ void __launch_bounds__(128) k_shade(RenderDev R, int cur, uint32_t depth, uint64_t sample0)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nxt = cur ^ 1;
+    bool cont = false;
+    float4 no = make_float4(0.f, 0.f, 0.f, 0.f), nd = no;
+    uint32_t path = 0;
+    // shadow segments of this vertex (at most kMaxLights)
+    float4 so[kMaxLights], sd[kMaxLights];
+    float3 sc[kMaxLights];
+    uint32_t n_sh = 0;
+    uint32_t pixel = 0;
+
+    if (i < R.count[cur]) {
+        path = R.q_path[cur][i];
+        const float4 o = R.q_o[cur][i], d = R.q_d[cur][i];
+        const int ti = R.hit_tri[i];
+        pixel = path % R.wh;
+        const uint64_t sample = sample0 + path / R.wh;
+        const uint64_t key = path_key(R.seed, sample * R.wh + pixel);
+        float3 beta = make_float3(R.beta[path].x, R.beta[path].y, R.beta[path].z);
+        float3 add = make_float3(0.f, 0.f, 0.f);
+
+        if (ti < 0) {
+            // escape: constant environment (zero for the reference's area-light scenes)
+            add = beta * R.sky;
+        } else if (depth <= R.max_depth) {
+            const uint32_t attr = R.tri_attr[ti];
+            const uint32_t mat_id = attr & 0xffffu, light_id = attr >> 16;
+            const Mat m = R.mats[mat_id < R.n_mats ? mat_id : 0];
+            const Tri tr = R.tris[ti];
+            const float3 ng = normalize3(make_float3(tr.a.w, tr.b.w, tr.c.w));
+            const float t = R.hit_t[i];
+            const float3 dd = make_float3(d.x, d.y, d.z);
+            const float3 p = make_float3(o.x + t * d.x, o.y + t * d.y, o.z + t * d.z);
+            const float3 wo = normalize3(dd) * -1.f;
+            // flat shading: the shading normal is the face normal
+            const float3 W = ng;
+            float3 U, V;
+            onb_from_w(W, U, V);
+            const float3 wo_l = make_float3(dot3(U, wo), dot3(V, wo), dot3(W, wo));
+
+            // emission only at depth 0 (no specular lobes here), one-sided
+            // (DiffuseAreaLight::Radiance, DiffuseAreaLight.cpp:47-50)
+            if (depth == 0 && light_id != 0xffffu && light_id < R.n_lights && dot3(W, wo) > 0.f)
+                add = add + beta * R.lights[light_id].emit;
+
+            if (depth < R.max_depth) {
+                // next-event estimation toward every light but the one hit
+                for (uint32_t l = 0; l < R.n_lights && l < kMaxLights; l++) {
+                    if (l == light_id) continue;
+                    const QuadLight &L = R.lights[l];
+                    const float u = rnd(key, dim_of(depth, 2 * l)), v = rnd(key, dim_of(depth, 2 * l + 1));
+                    // Quad::SamplePoint (Core/Shape/Quad.cpp:144-153): a bilinear
+                    // patch over the reference's tessellation vertices
+                    const float3 P = L.p[0] + (L.p[2] - L.p[0]) * u + (L.p[3] - L.p[2]) * v +
+                                     (L.p[0] - L.p[2] + L.p[1] - L.p[3]) * (u * v);
+                    float3 win = p - P;
+                    const float dist2 = dot3(win, win);
+                    win = normalize3(win);
+                    const float cl = fmaxf(0.f, dot3(win, L.n));
+                    const float3 Ls = L.emit * (cl * L.area / dist2);
+                    if (is_black(Ls)) continue;
+                    const float3 wi = win * -1.f;
+                    const float3 wi_l = make_float3(dot3(U, wi), dot3(V, wi), dot3(W, wi));
+                    const float3 c = beta * Ls * (fmaxf(0.f, dot3(wi, W))) * bsdf_f(m, wo_l, wi_l);
+                    if (is_black(c)) continue;
+                    const float3 seg = P - p;
+                    so[n_sh] = make_float4(p.x, p.y, p.z, R.eps);
+                    sd[n_sh] = make_float4(seg.x, seg.y, seg.z, 1.f - R.eps);
+                    sc[n_sh] = c;
+                    n_sh++;
+                }
+
+                // sample the BSDF (BSDF::SampleF, Core/Material/BSDF.cpp:141-211)
+                const float u1 = rnd(key, dim_of(depth, 20)), u2 = rnd(key, dim_of(depth, 21));
+                float3 wi_l, f;
+                float pdf;
+                if (m.kind == 1u) {
+                    wi_l = ggx_sample_vndf(wo_l, m.alpha, u1, u2);
+                    pdf = ggx_pdf(wo_l, wi_l, m.alpha);
+                    f = ggx_f(wo_l, wi_l, m.f0, m.alpha);
+                } else {
+                    // Lambertian::SampleF (Core/Material/LambertianBxDF.cpp:27-37)
+                    const float r = sqrtf(u1);
+                    float s, c;
+                    sincosf(kTwoPi * u2, &s, &c);
+                    wi_l = make_float3(r * c, r * s, sqrtf(1.f - u1));
+                    if (wo_l.z < 0.f) wi_l.z = -wi_l.z;
+                    pdf = fabsf(wi_l.z) * kInvPi;
+                    f = bsdf_f(m, wo_l, wi_l);
+                }
+                if (!is_black(f) && pdf > 0.f) {
+                    const float3 wi = U * wi_l.x + V * wi_l.y + W * wi_l.z;
+                    beta = beta * f * (fabsf(dot3(wi, W)) / pdf);
+                    bool alive = true;
+                    if (depth > 3) {
+                        const float q = fminf(0.5f, 0.212671f * beta.x + 0.715160f * beta.y + 0.072169f * beta.z);
+                        if (rnd(key, dim_of(depth, 23)) > q) alive = false;
+                        else beta = beta * (1.f / q);
+                    }
+                    if (alive) {
+                        const float3 org = p + ng * R.eps;
+                        no = make_float4(org.x, org.y, org.z, R.eps);
+                        nd = make_float4(wi.x, wi.y, wi.z, FLT_MAX);
+                        cont = true;
+                        R.beta[path] = make_float4(beta.x, beta.y, beta.z, 0.f);
+                    }
+                }
+            }
+        }
+        if (!is_black(add)) add_pixel(R.accum, pixel, add);
+    }
+
+    const uint32_t slot = push_slot(cont, &R.count[nxt]);
+    if (cont) {
+        if (slot < R.capacity) {
+            R.q_o[nxt][slot] = no;
+            R.q_d[nxt][slot] = nd;
+            R.q_path[nxt][slot] = path;
+        } else {
+            atomicOr(R.err, 8u);
+        }
+    }
+    for (uint32_t k = 0; k < kMaxLights; k++) {
+        const bool want = k < n_sh;
+        const uint32_t s = push_slot(want, R.sh_count);
+        if (want) {
+            if (s < R.sh_capacity) {
+                R.s_o[s] = so[k];
+                R.s_d[s] = sd[k];
+                R.s_c[s] = make_float4(sc[k].x, sc[k].y, sc[k].z, __uint_as_float(pixel));
+            } else {
+                atomicOr(R.err, 16u);
+            }
+        }
+        if (!__any_sync(__activemask(), k + 1 < n_sh)) break;
+    }
+}
+
+__global__ void __launch_bounds__(128) k_shadow(RenderDev R)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= *R.sh_count) return;
+    const float4 o = R.s_o[i], d = R.s_d[i];
+    int best;
+    float bt, bu, bv;
+    unsigned long long nn = 0, nt = 0;
+    trace_one<true, false>(R.nodes, R.tris, R.n_nodes, R.n_tris, o, d, best, bt, bu, bv, R.err, nn, nt);
+    if (best == -1) {
+        const float4 c = R.s_c[i];
+        add_pixel(R.accum, __float_as_uint(c.w), make_float3(c.x, c.y, c.z));
+    }
+}
+
+__global__ void k_resolve(const float4 *__restrict__ accum, uint32_t wh, float scale, float *__restrict__ out)
+{
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= wh) return;
+    const float4 a = accum[p];
+    out[3 * p] = a.x * scale;
+    out[3 * p + 1] = a.y * scale;
+    out[3 * p + 2] = a.z * scale;
+}
+
+__global__ void k_tri_attr(const uint32_t *__restrict__ prim_of, uint32_t n, const uint32_t *__restrict__ mat_ids,
+                           const uint32_t *__restrict__ light_of_prim, uint32_t *__restrict__ attr)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t p = prim_of[i];
+    attr[i] = (mat_ids ? (mat_ids[p] & 0xffffu) : 0u) | (light_of_prim[p] << 16);
+}
+
+__global__ void k_light_of_prim(uint32_t *lop, uint32_t n_prims, const uint32_t *first_tri, uint32_t n_lights)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n_prims) return;
+    uint32_t id = 0xffffu;
+    for (uint32_t l = 0; l < n_lights; l++)
+        if (i == first_tri[l] || i == first_tri[l] + 1u) id = l;
+    lop[i] = id;
+}
+
+inline uint32_t blocks_for(uint64_t n, uint32_t t) { return (uint32_t)((n + t - 1) / t); }
+
+}  // namespace
+
+cudaError_t build_tri_attr(const uint32_t *prim_of, uint32_t n_tris, const uint32_t *mat_ids,
+                           const uint32_t *light_first_tri, uint32_t n_lights, uint32_t *light_of_prim,
+                           uint32_t *attr, cudaStream_t st)
+{
+    k_light_of_prim<<<blocks_for(n_tris, 256), 256, 0, st>>>(light_of_prim, n_tris, light_first_tri, n_lights);
+    k_tri_attr<<<blocks_for(n_tris, 256), 256, 0, st>>>(prim_of, n_tris, mat_ids, light_of_prim, attr);
+    return cudaGetLastError();
+}
+
+cudaError_t render_wave(const RenderDev &R, uint32_t n_paths, uint64_t sample0, cudaStream_t st,
+                        uint32_t *launches)
+{
+    const uint32_t T = 128;
+    cudaError_t e;
+    if ((e = cudaMemsetAsync(R.count, 0, 2 * sizeof(uint32_t), st)) != cudaSuccess) return e;
+    k_camera<<<blocks_for(n_paths, T), T, 0, st>>>(R, n_paths, sample0);
+    if ((e = cudaMemcpyAsync(R.count, &n_paths, sizeof(uint32_t), cudaMemcpyHostToDevice, st)) != cudaSuccess) return e;
+    uint32_t n_launch = 1;
+    int cur = 0;
+    for (uint32_t depth = 0; depth <= R.max_depth; depth++) {
+        if ((e = cudaMemsetAsync(R.count + (cur ^ 1), 0, sizeof(uint32_t), st)) != cudaSuccess) return e;
+        if ((e = cudaMemsetAsync(R.sh_count, 0, sizeof(uint32_t), st)) != cudaSuccess) return e;
+        k_extend<<<blocks_for(n_paths, T), T, 0, st>>>(R, cur);
+        k_shade<<<blocks_for(n_paths, T), T, 0, st>>>(R, cur, depth, sample0);
+        n_launch += 2;
+        if (depth < R.max_depth) {
+            k_shadow<<<blocks_for((uint64_t)n_paths * (R.n_lights ? R.n_lights : 1), T), T, 0, st>>>(R);
+            n_launch++;
+        }
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+        cur ^= 1;
+    }
+    if (launches) *launches += n_launch;
+    return cudaSuccess;
+}
+
+cudaError_t render_resolve(const float4 *accum, uint32_t wh, float scale, float *out, cudaStream_t st)
+{
+    k_resolve<<<blocks_for(wh, 256), 256, 0, st>>>(accum, wh, scale, out);
+    return cudaGetLastError();
+}
+
+}  // namespace ilg

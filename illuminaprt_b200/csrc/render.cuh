@@ -1,0 +1,70 @@
+// Device state of the wavefront path tracer (render.cu).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "bvh8.cuh"
+
+namespace ilg {
+
+constexpr uint32_t kMaxLights = 8;
+
+struct Mat {  // mirrors ilg_material (32 bytes)
+    float3 albedo;
+    uint32_t kind;
+    float3 f0;
+    float alpha;
+};
+static_assert(sizeof(Mat) == 32, "material record is 32 bytes");
+
+struct QuadLight {
+    float3 p[4];   // the reference's Quad vertices v1..v4
+    float3 emit;
+    float3 n;      // unit normal (v3 - v1) x (v2 - v1), as Quad::SamplePoint returns it, normalised
+    float area;    // area of the two tessellation triangles
+};
+
+// Everything the kernels of one render need, passed by value.
+struct RenderDev {
+    // scene
+    const Node8 *nodes;
+    const Tri *tris;
+    uint32_t n_nodes, n_tris;
+    const uint32_t *tri_attr;  // per triangle record: material (low 16) | light (high 16, 0xffff none)
+    const Mat *mats;
+    uint32_t n_mats;
+    const QuadLight *lights;
+    uint32_t n_lights;
+    float3 sky;
+    // camera (PerspectiveCamera after SetFieldOfView)
+    float3 centre, corner, across, up;
+    uint32_t width, height, wh;
+    float rcp_w, rcp_h;
+    // integrator
+    uint32_t max_depth;
+    float eps;
+    uint32_t seed;
+    // wavefront queues (ping-pong) and path state
+    float4 *q_o[2], *q_d[2];
+    uint32_t *q_path[2];
+    uint32_t *count;       // [2]
+    uint32_t capacity;
+    int *hit_tri;
+    float *hit_t;
+    float4 *beta;
+    float4 *s_o, *s_d, *s_c;  // shadow segments and their contribution (w = pixel bits)
+    uint32_t *sh_count;
+    uint32_t sh_capacity;
+    float4 *accum;         // per pixel rgb sums
+    uint32_t *err;
+};
+
+cudaError_t build_tri_attr(const uint32_t *prim_of, uint32_t n_tris, const uint32_t *mat_ids,
+                           const uint32_t *light_first_tri, uint32_t n_lights, uint32_t *light_of_prim,
+                           uint32_t *attr, cudaStream_t st);
+cudaError_t render_wave(const RenderDev &R, uint32_t n_paths, uint64_t sample0, cudaStream_t st,
+                        uint32_t *launches);
+cudaError_t render_resolve(const float4 *accum, uint32_t wh, float scale, float *out, cudaStream_t st);
+
+}  // namespace ilg

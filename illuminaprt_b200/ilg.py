@@ -25,7 +25,10 @@ STATUS_NAMES = {0: "ILG_OK", 1: "ILG_EINVAL", 2: "ILG_ENOMEM", 3: "ILG_ECUDA", 4
 
 # Every symbol the public headers declare; tests check the library exports them.
 EXPORTED = ["ilg_create", "ilg_destroy", "ilg_last_error", "ilg_set_mesh", "ilg_build", "ilg_get_stats",
-            "ilg_intersect", "ilg_intersect_counted", "ilg_occluded", "ilg_sync", "ilg_stream"]
+            "ilg_intersect", "ilg_intersect_counted", "ilg_occluded", "ilg_sync", "ilg_stream",
+            "ilg_set_materials", "ilg_set_quad_lights", "ilg_render"]
+
+ILG_MAT_LAMBERT, ILG_MAT_GGX = 0, 1
 
 
 class IlgError(RuntimeError):
@@ -42,6 +45,26 @@ class ilg_stats(ctypes.Structure):
     _fields_ = [("n_tris", ctypes.c_uint32), ("n_nodes", ctypes.c_uint32), ("n_leaf_tris", ctypes.c_uint32),
                 ("max_depth", ctypes.c_uint32), ("build_ms", ctypes.c_float), ("node_bytes", ctypes.c_uint64),
                 ("tri_bytes", ctypes.c_uint64)]
+
+
+class ilg_material(ctypes.Structure):
+    _fields_ = [("albedo", ctypes.c_float * 3), ("kind", ctypes.c_uint32), ("f0", ctypes.c_float * 3),
+                ("alpha", ctypes.c_float)]
+
+
+class ilg_quad_light(ctypes.Structure):
+    _fields_ = [("v", (ctypes.c_float * 3) * 4), ("emit", ctypes.c_float * 3), ("first_tri", ctypes.c_uint32)]
+
+
+class ilg_camera(ctypes.Structure):
+    _fields_ = [("eye", ctypes.c_float * 3), ("target", ctypes.c_float * 3), ("up", ctypes.c_float * 3),
+                ("fov_deg", ctypes.c_float), ("aspect", ctypes.c_float)]
+
+
+class ilg_render_opts(ctypes.Structure):
+    _fields_ = [("width", ctypes.c_uint32), ("height", ctypes.c_uint32), ("spp", ctypes.c_uint32),
+                ("max_depth", ctypes.c_uint32), ("epsilon", ctypes.c_float), ("seed", ctypes.c_uint32),
+                ("paths_per_wave", ctypes.c_uint32), ("sky", ctypes.c_float * 3), ("reserved", ctypes.c_uint32 * 6)]
 
 
 _lib = None
@@ -72,11 +95,15 @@ def load(build_if_missing: bool = True) -> ctypes.CDLL:
     L.ilg_intersect.argtypes = [vp, vp, vp, u32, vp, vp, vp, vp, u32]
     L.ilg_intersect_counted.argtypes = [vp, vp, vp, u32, vp, vp, vp, vp, vp, u32]
     L.ilg_occluded.argtypes = [vp, vp, vp, u32, vp, u32]
+    L.ilg_set_materials.argtypes = [vp, vp, u32]
+    L.ilg_set_quad_lights.argtypes = [vp, vp, u32]
+    L.ilg_render.argtypes = [vp, ctypes.POINTER(ilg_camera), ctypes.POINTER(ilg_render_opts), vp, u32]
     L.ilg_sync.argtypes = [vp]
     L.ilg_stream.argtypes = [vp]
     L.ilg_stream.restype = vp
     for f in ("ilg_create", "ilg_destroy", "ilg_set_mesh", "ilg_build", "ilg_get_stats", "ilg_intersect",
-              "ilg_intersect_counted", "ilg_occluded", "ilg_sync"):
+              "ilg_intersect_counted", "ilg_occluded", "ilg_sync", "ilg_set_materials", "ilg_set_quad_lights",
+              "ilg_render"):
         getattr(L, f).restype = i32
     _lib = L
     return L
@@ -167,6 +194,46 @@ class GpuSpace:
     def occluded_into(self, o4, d4, occ, device_ptrs: bool):
         self._check(self.L.ilg_occluded(self.h, _ptr(o4), _ptr(d4), o4.shape[0], _ptr(occ),
                                         ILG_DEVICE_PTRS if device_ptrs else 0))
+
+    # --- path tracing: PathIntegrator + RenderRegion over the whole image ----
+    def set_materials(self, mats):
+        """mats: sequence of dicts {albedo, kind=0, f0=(0,0,0), alpha=0}."""
+        arr = (ilg_material * len(mats))()
+        for i, m in enumerate(mats):
+            arr[i].albedo[:] = list(m.get("albedo", (0.0, 0.0, 0.0)))
+            arr[i].kind = int(m.get("kind", ILG_MAT_LAMBERT))
+            arr[i].f0[:] = list(m.get("f0", (0.0, 0.0, 0.0)))
+            arr[i].alpha = float(m.get("alpha", 0.0))
+        self._check(self.L.ilg_set_materials(self.h, ctypes.addressof(arr), len(mats)))
+
+    def set_quad_lights(self, lights):
+        """lights: sequence of dicts {v: 4x3 (reference Quad order), emit: 3, first_tri}."""
+        arr = (ilg_quad_light * max(1, len(lights)))()
+        for i, l in enumerate(lights):
+            for k in range(4):
+                arr[i].v[k][:] = [float(x) for x in l["v"][k]]
+            arr[i].emit[:] = [float(x) for x in l["emit"]]
+            arr[i].first_tri = int(l["first_tri"])
+        self._check(self.L.ilg_set_quad_lights(self.h, ctypes.addressof(arr), len(lights)))
+
+    def render(self, camera: dict, width: int, height: int, spp: int, max_depth: int = 6, epsilon: float = 1e-4,
+               seed: int = 1, sky=(0.0, 0.0, 0.0), paths_per_wave: int = 0, out=None):
+        """Returns (height, width, 3) float32 (or fills `out`, a CUDA tensor, in place)."""
+        cam = ilg_camera()
+        cam.eye[:] = list(camera["eye"])
+        cam.target[:] = list(camera["target"])
+        cam.up[:] = list(camera["up"])
+        cam.fov_deg = float(camera["fov"])
+        cam.aspect = float(camera.get("aspect", width / height))
+        o = ilg_render_opts(width=width, height=height, spp=spp, max_depth=max_depth, epsilon=epsilon, seed=seed,
+                            paths_per_wave=paths_per_wave)
+        o.sky[:] = list(sky)
+        if out is not None:
+            self._check(self.L.ilg_render(self.h, ctypes.byref(cam), ctypes.byref(o), _ptr(out), ILG_DEVICE_PTRS))
+            return out
+        img = np.empty((height, width, 3), np.float32)
+        self._check(self.L.ilg_render(self.h, ctypes.byref(cam), ctypes.byref(o), img.ctypes.data, 0))
+        return img
 
     def sync(self):
         self._check(self.L.ilg_sync(self.h))

@@ -164,3 +164,100 @@ def ray_batch_workload(nx=1024, ny=512, side=2048, n_incoherent=4194304, seed=1)
     co, cd = coherent_rays(side)
     io, idr = incoherent_rays(pos, idx, n_incoherent, seed + 1)
     return pos, idx, (co, cd), (io, idr)
+
+
+# ---------------------------------------------------------------------------
+# Procedural box scene (the reference's CPU-runnable path-tracing case)
+# ---------------------------------------------------------------------------
+GREY = (0.73, 0.73, 0.73)
+RED = (0.63, 0.065, 0.05)
+GREEN = (0.14, 0.45, 0.09)
+
+
+def _rot_y(deg):
+    a = np.radians(deg)
+    c, s = np.cos(a), np.sin(a)
+    return np.array([[c, 0, s], [0, 1, 0], [-s, 0, c]])
+
+
+def _box_tris(center, half, rot_deg):
+    """12 triangles of an axis-aligned box rotated about y, normals outward
+    (n = (v1 - v0) x (v2 - v0), the reference's edge convention)."""
+    hx, hy, hz = half
+    c = np.array([[-hx, -hy, -hz], [hx, -hy, -hz], [hx, hy, -hz], [-hx, hy, -hz],
+                  [-hx, -hy, hz], [hx, -hy, hz], [hx, hy, hz], [-hx, hy, hz]], np.float64)
+    faces = [(1, 0, 3, 2), (4, 5, 6, 7), (0, 4, 7, 3), (5, 1, 2, 6), (3, 7, 6, 2), (0, 1, 5, 4)]
+    R = _rot_y(rot_deg)
+    p = c @ R.T + np.asarray(center)
+    tris = []
+    for a, b, cc, d in faces:
+        tris.append((p[a], p[b], p[cc]))
+        tris.append((p[a], p[cc], p[d]))
+    return tris
+
+
+def _quad_tris(v0, v1, v2, v3):
+    return [(v0, v1, v2), (v0, v2, v3)]
+
+
+def box_scene():
+    """Closed box [-1,1]^3 with the front (z = +1) open, walls two triangles
+    each (normals inward), left wall red, right green, others grey; two inner
+    boxes rotated +-17 deg about y; a 0.5 x 0.4 ceiling quad light with
+    radiance (17, 12, 4) facing -y; pinhole camera at z = 3.5, 40 deg.
+
+    Returns a dict with flattened world-space triangles (unshared vertices),
+    a per-triangle primitive index, per-primitive albedo, the light quad in
+    the reference's Quad vertex order, and the camera.
+    """
+    prims = []  # (triangles, albedo)
+    L, H = -1.0, 1.0
+    walls = [
+        ("floor", _quad_tris((L, L, L), (L, L, H), (H, L, H), (H, L, L)), GREY),      # +y
+        ("ceiling", _quad_tris((L, H, L), (H, H, L), (H, H, H), (L, H, H)), GREY),    # -y
+        ("back", _quad_tris((L, L, L), (H, L, L), (H, H, L), (L, H, L)), GREY),       # +z
+        ("left", _quad_tris((L, L, L), (L, H, L), (L, H, H), (L, L, H)), RED),        # +x
+        ("right", _quad_tris((H, L, L), (H, L, H), (H, H, H), (H, H, L)), GREEN),     # -x
+    ]
+    for _, tris, alb in walls:
+        prims.append((tris, alb))
+    prims.append((_box_tris((0.35, -0.7, 0.35), (0.3, 0.3, 0.3), -17.0), GREY))
+    prims.append((_box_tris((-0.35, -0.4, -0.3), (0.3, 0.6, 0.3), 17.0), GREY))
+    # light quad, reference Quad vertex order: its triangles are (v1, v3, v2)
+    # and (v1, v4, v3) (Core/Shape/Quad.cpp), normal (v3-v1) x (v2-v1) = -y
+    yl = 0.999
+    q = np.array([(-0.25, yl, -0.2), (-0.25, yl, 0.2), (0.25, yl, 0.2), (0.25, yl, -0.2)], np.float64)
+    light_tris = [(q[0], q[2], q[1]), (q[0], q[3], q[2])]
+    prims.append((light_tris, GREY))
+    pos, prim_of_tri = [], []
+    for pi, (tris, _) in enumerate(prims):
+        for t in tris:
+            pos.extend(t)
+            prim_of_tri.append(pi)
+    pos = np.asarray(pos, np.float32).reshape(-1, 3)
+    n_tris = pos.shape[0] // 3
+    return {
+        "pos": pos,
+        "idx": np.arange(3 * n_tris, dtype=np.uint32).reshape(-1, 3),
+        "prim_of_tri": np.asarray(prim_of_tri, np.uint32),
+        "albedo": np.asarray([p[1] for p in prims], np.float32),
+        "light_prim": len(prims) - 1,
+        "light_quad": q.astype(np.float32),
+        "light_emit": np.array([17.0, 12.0, 4.0], np.float32),
+        "camera": {"eye": (0.0, 0.0, 3.5), "target": (0.0, 0.0, 0.0), "up": (0.0, 1.0, 0.0),
+                   "fov": 40.0, "aspect": 1.0},
+        "max_depth": 6, "epsilon": 1e-4,
+    }
+
+
+def load_box_scene(space, scene=None):
+    """Upload the box scene to a GpuSpace: mesh with per-triangle material
+    ids (one material per primitive, as MatteMaterial per primitive), the
+    light quad, then build."""
+    scene = scene or box_scene()
+    space.initialise(scene["pos"], scene["idx"], scene["prim_of_tri"])
+    space.build()
+    space.set_materials([{"albedo": tuple(a)} for a in scene["albedo"]])
+    first = int(np.nonzero(scene["prim_of_tri"] == scene["light_prim"])[0][0])
+    space.set_quad_lights([{"v": scene["light_quad"], "emit": scene["light_emit"], "first_tri": first}])
+    return scene

@@ -92,6 +92,67 @@ int ilg_intersect_counted(ilg_ctx *ctx, const float *ray_o_tmin, const float *ra
 int ilg_occluded(ilg_ctx *ctx, const float *ray_o_tmin, const float *ray_d_tmax, uint32_t n,
                  uint8_t *occ, uint32_t flags);
 
+/* ------------------------------------------------------------------------
+ * Path tracing (the reference's PathIntegrator::Radiance bounce loop,
+ * Core/Integrator/PathIntegrator.cpp:44-367, driven per pixel as
+ * BaseRenderer::RenderRegion does, Core/Renderer/BaseRenderer.cpp:62-169).
+ * ---------------------------------------------------------------------- */
+
+#define ILG_MAT_LAMBERT 0u /* MatteMaterial: Lambertian BxDF (Core/Material/Matte.h) */
+#define ILG_MAT_GGX 1u     /* GGX conductor (no reference counterpart) */
+
+typedef struct ilg_material {
+    float albedo[3];  /* Lambertian reflectance */
+    uint32_t kind;    /* ILG_MAT_* */
+    float f0[3];      /* GGX: Schlick reflectance at normal incidence */
+    float alpha;      /* GGX: roughness (alpha) */
+} ilg_material;
+
+/* A one-sided area light on a Quad (DiffuseAreaLight over Core/Shape/Quad.cpp).
+ * v holds the reference's Quad vertices in its order; the quad's two
+ * triangles must be in the mesh at first_tri and first_tri + 1 as
+ * (v[0], v[2], v[1]) and (v[0], v[3], v[2]), which is how the reference
+ * tessellates a Quad. */
+typedef struct ilg_quad_light {
+    float v[4][3];
+    float emit[3];
+    uint32_t first_tri;
+} ilg_quad_light;
+
+/* Pinhole camera as the reference's camera factory builds it
+ * (Core/Camera/CameraFactories.h:40-80): frame from (target - eye, up),
+ * image plane at distance 1, SetFieldOfView(fov_deg, aspect). */
+typedef struct ilg_camera {
+    float eye[3];
+    float target[3];
+    float up[3];
+    float fov_deg;
+    float aspect;
+} ilg_camera;
+
+typedef struct ilg_render_opts {
+    uint32_t width, height;
+    uint32_t spp;            /* samples per pixel */
+    uint32_t max_depth;      /* RayDepth (factory default 6) */
+    float epsilon;           /* reflect epsilon (factory default 1e-4) */
+    uint32_t seed;           /* sample-sequence seed */
+    uint32_t paths_per_wave; /* wavefront size; 0 = automatic */
+    float sky[3];            /* constant environment radiance; 0 = none */
+    uint32_t reserved[6];
+} ilg_render_opts;
+
+/* Materials indexed by the mat_ids given to ilg_set_mesh. */
+int ilg_set_materials(ilg_ctx *ctx, const ilg_material *mats, uint32_t n);
+int ilg_set_quad_lights(ilg_ctx *ctx, const ilg_quad_light *lights, uint32_t n);
+
+/* Renders width x height pixels at spp samples each into out_rgb
+ * (height x width x 3 floats, row y = image-plane 'up' coordinate y, as the
+ * reference's RenderRegion indexes its buffer). Host pointer unless
+ * ILG_DEVICE_PTRS. Needs ilg_build, ilg_set_mesh with mat_ids, and
+ * ilg_set_materials. */
+int ilg_render(ilg_ctx *ctx, const ilg_camera *cam, const ilg_render_opts *opts, float *out_rgb,
+               uint32_t flags);
+
 /* Blocks until the context's stream is idle (for ILG_DEVICE_PTRS callers). */
 int ilg_sync(ilg_ctx *ctx);
 

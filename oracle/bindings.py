@@ -33,7 +33,7 @@ def build(ref: bool = True) -> None:
 
 
 def _ensure_oracle():
-    srcs = [os.path.join(HERE, f) for f in ("ilg_oracle.c", "ilg_oracle.h")]
+    srcs = [os.path.join(HERE, f) for f in ("ilg_oracle.c", "ilg_oracle.h", "pt_oracle.c")]
     if not os.path.exists(ORACLE_SO) or any(os.path.getmtime(s) > os.path.getmtime(ORACLE_SO) for s in srcs):
         subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
 
@@ -54,7 +54,37 @@ class Oracle:
         L.orc_bvh_intersect.argtypes = [ctypes.c_void_p, _f32p, _f32p, ctypes.c_int64, _i32p, _f32p, _f32p,
                                         _f32p, ctypes.c_int, ctypes.c_void_p]
         L.orc_bvh_occluded.argtypes = [ctypes.c_void_p, _f32p, _f32p, ctypes.c_int64, _u8p, ctypes.c_int]
+        L.orc_render.argtypes = [_f32p, ctypes.c_uint32, _u32p, ctypes.c_uint32, _u32p, ctypes.c_void_p,
+                                 ctypes.c_uint32, ctypes.c_void_p, ctypes.c_uint32, _f32p, ctypes.c_uint32,
+                                 ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_float, ctypes.c_uint32,
+                                 _f32p, ctypes.c_int, _f32p]
         self.L = L
+
+    def render(self, pos, idx, mat_ids, mats, lights, camera, width, height, spp, max_depth=6, epsilon=1e-4,
+               seed=1, sky=(0.0, 0.0, 0.0), nthreads=None):
+        """CPU restatement of the path tracer with the device's random numbers.
+        mats: list of dicts {albedo, kind, f0, alpha}; lights: list of dicts {v, emit, first_tri}."""
+        M = np.zeros((len(mats), 8), np.float32)
+        for i, m in enumerate(mats):
+            M[i, 0:3] = m.get("albedo", (0, 0, 0))
+            M[i, 3] = np.array([m.get("kind", 0)], np.uint32).view(np.float32)[0]
+            M[i, 4:7] = m.get("f0", (0, 0, 0))
+            M[i, 7] = m.get("alpha", 0.0)
+        Lt = np.zeros((max(1, len(lights)), 16), np.float32)
+        for i, l in enumerate(lights):
+            Lt[i, 0:12] = np.asarray(l["v"], np.float32).reshape(-1)
+            Lt[i, 12:15] = l["emit"]
+            Lt[i, 15] = np.array([l["first_tri"]], np.uint32).view(np.float32)[0]
+        cam = np.array([*camera["eye"], *camera["target"], *camera["up"], camera["fov"],
+                        camera.get("aspect", width / height)], np.float32)
+        out = np.zeros((height, width, 3), np.float32)
+        pos = np.ascontiguousarray(pos, np.float32)
+        idx = np.ascontiguousarray(idx, np.uint32)
+        self.L.orc_render(pos.reshape(-1), pos.shape[0], idx.reshape(-1), idx.shape[0],
+                          np.ascontiguousarray(mat_ids, np.uint32), M.ctypes.data, len(mats), Lt.ctypes.data,
+                          len(lights), cam, width, height, spp, max_depth, epsilon, seed,
+                          np.asarray(sky, np.float32), nthreads or os.cpu_count() or 1, out.reshape(-1))
+        return out
 
     def shirley(self, pos, idx, tri, o, d, tmax=np.finfo(np.float32).max):
         t, b, g = ctypes.c_float(), ctypes.c_float(), ctypes.c_float()
@@ -120,7 +150,24 @@ class RefLib:
         L.ilref_intersect.argtypes = [ctypes.c_void_p, _f32p, _f32p, ctypes.c_long, _i32p, _f32p, _f32p, _f32p,
                                       ctypes.c_int]
         L.ilref_occluded.argtypes = [ctypes.c_void_p, _f32p, _f32p, ctypes.c_long, _u8p, ctypes.c_int]
+        L.ilref_render_box.argtypes = [_f32p, _i32p, ctypes.c_int, ctypes.c_int, _f32p, ctypes.c_int, _f32p, _f32p,
+                                       _f32p, _f32p, _f32p, ctypes.c_float, ctypes.c_float, ctypes.c_int,
+                                       ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_uint32,
+                                       ctypes.c_int, _f32p]
         self.L = L
+
+    def render_box(self, scene: dict, width: int, height: int, spp: int, seed: int = 1, nthreads=None):
+        """The reference's PathIntegrator on the box scene; returns (H, W, 3) float32."""
+        f = lambda a: np.ascontiguousarray(a, np.float32)
+        cam = scene["camera"]
+        out = np.zeros((height, width, 3), np.float32)
+        self.L.ilref_render_box(f(scene["pos"]).reshape(-1), np.ascontiguousarray(scene["prim_of_tri"], np.int32),
+                                scene["pos"].shape[0] // 3, scene["albedo"].shape[0], f(scene["albedo"]).reshape(-1),
+                                int(scene["light_prim"]), f(scene["light_quad"]).reshape(-1), f(scene["light_emit"]),
+                                f(cam["eye"]), f(cam["target"]), f(cam["up"]), float(cam["fov"]),
+                                float(cam["aspect"]), width, height, spp, int(scene["max_depth"]),
+                                float(scene["epsilon"]), seed, nthreads or os.cpu_count() or 1, out.reshape(-1))
+        return out
 
     def mesh(self, pos, idx, kind: str = "bvh"):
         return RefMesh(self, pos, idx, 0 if kind == "kd" else 1)

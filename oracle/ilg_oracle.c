@@ -226,48 +226,77 @@ typedef struct {
     uint64_t visits, tests;
 } job;
 
+/* Closest hit (returns triangle index or -1) of one ray on the oracle BVH. */
+static int32_t bvh_closest1(obvh *b, const float o[3], const float d[3], float rmin, float rmax0, float *t_out,
+                            float *u_out, float *v_out, uint64_t *visits, uint64_t *tests)
+{
+    int32_t stack[128];
+    double inv[3] = {1.0 / d[0], 1.0 / d[1], 1.0 / d[2]};
+    float rmax = rmax0;
+    int32_t best = -1;
+    float bt = INFINITY, bu = 0, bv = 0;
+    int sp = 0;
+    if (b->ntris) stack[sp++] = 0;
+    while (sp) {
+        const onode *nd = &b->nodes[stack[--sp]];
+        double tn;
+        if (visits) (*visits)++;
+        if (!slab(nd, o, inv, rmin, rmax, &tn)) continue;
+        if (nd->left < 0) {
+            for (int32_t i = nd->first; i < nd->first + nd->count; i++) {
+                uint32_t tri = b->order[i];
+                float th, bh, gh;
+                if (tests) (*tests)++;
+                if (shirley_tri(&b->tris[tri], o, d, rmax, &th, &bh, &gh)) {
+                    best = (int32_t)tri; bt = th; bu = bh; bv = gh;
+                    rmax = th < rmax ? th : rmax;
+                }
+            }
+        } else {
+            if (sp + 2 > 128) abort();
+            stack[sp++] = nd->left + 1;
+            stack[sp++] = nd->left;
+        }
+    }
+    *t_out = bt; *u_out = bu; *v_out = bv;
+    return best;
+}
+
+static int bvh_any1(obvh *b, const float o[3], const float d[3], float rmin, float rmax)
+{
+    int32_t stack[128];
+    double inv[3] = {1.0 / d[0], 1.0 / d[1], 1.0 / d[2]};
+    int sp = 0;
+    if (b->ntris) stack[sp++] = 0;
+    while (sp) {
+        const onode *nd = &b->nodes[stack[--sp]];
+        double tn;
+        if (!slab(nd, o, inv, rmin, rmax, &tn)) continue;
+        if (nd->left < 0) {
+            for (int32_t i = nd->first; i < nd->first + nd->count; i++) {
+                float th, bh, gh;
+                if (shirley_tri(&b->tris[b->order[i]], o, d, rmax, &th, &bh, &gh)) return 1;
+            }
+        } else {
+            if (sp + 2 > 128) abort();
+            stack[sp++] = nd->left + 1;
+            stack[sp++] = nd->left;
+        }
+    }
+    return 0;
+}
+
 static void trace_range(job *j)
 {
-    obvh *b = j->b;
-    int32_t stack[128];
     for (int64_t r = j->begin; r < j->end; r++) {
         const float *o = j->o4 + 4 * r, *d = j->d4 + 4 * r;
-        double inv[3] = {1.0 / d[0], 1.0 / d[1], 1.0 / d[2]};
-        float rmax = d[3];
-        float rmin = o[3];
-        int32_t best = -1;
-        float bt = INFINITY, bu = 0, bv = 0;
-        int sp = 0, any = 0;
-        if (b->ntris) stack[sp++] = 0;
-        while (sp && !any) {
-            const onode *nd = &b->nodes[stack[--sp]];
-            double tn;
-            j->visits++;
-            if (!slab(nd, o, inv, rmin, rmax, &tn)) continue;
-            if (nd->left < 0) {
-                for (int32_t i = nd->first; i < nd->first + nd->count; i++) {
-                    uint32_t tri = b->order[i];
-                    float th, bh, gh;
-                    j->tests++;
-                    if (shirley_tri(&b->tris[tri], o, d, rmax, &th, &bh, &gh)) {
-                        if (j->occ) { any = 1; break; }
-                        /* Among hits the window admits, keep the lowest t and
-                         * then the lowest index: a fixed rule, independent of
-                         * visit order, for the tests to classify ties against. */
-                        if (best < 0 || th < bt || (th == bt && (int32_t)tri < best)) {
-                            best = (int32_t)tri; bt = th; bu = bh; bv = gh;
-                        }
-                        rmax = th < rmax ? th : rmax;
-                    }
-                }
-            } else {
-                if (sp + 2 > 128) abort();
-                stack[sp++] = nd->left + 1;
-                stack[sp++] = nd->left;
-            }
+        if (j->occ) {
+            j->occ[r] = (uint8_t)bvh_any1(j->b, o, d, o[3], d[3]);
+        } else {
+            float t, u, v;
+            int32_t p = bvh_closest1(j->b, o, d, o[3], d[3], &t, &u, &v, &j->visits, &j->tests);
+            j->prim[r] = p; j->t[r] = t; j->u[r] = u; j->v[r] = v;
         }
-        if (j->occ) j->occ[r] = (uint8_t)any;
-        else { j->prim[r] = best; j->t[r] = bt; j->u[r] = bu; j->v[r] = bv; }
     }
 }
 
@@ -309,4 +338,15 @@ void orc_bvh_intersect(void *h, const float *o4, const float *d4, int64_t n, int
 void orc_bvh_occluded(void *h, const float *o4, const float *d4, int64_t n, uint8_t *occ, int nthreads)
 {
     run_jobs((obvh *)h, o4, d4, n, NULL, NULL, NULL, NULL, occ, nthreads, NULL);
+}
+
+int32_t orc_bvh_closest1(void *h, const float o[3], const float d[3], float rmin, float rmax, float *t)
+{
+    float u, v;
+    return bvh_closest1((obvh *)h, o, d, rmin, rmax, t, &u, &v, NULL, NULL);
+}
+
+int orc_bvh_any1(void *h, const float o[3], const float d[3], float rmin, float rmax)
+{
+    return bvh_any1((obvh *)h, o, d, rmin, rmax);
 }

@@ -42,6 +42,20 @@ void orc_bvh_intersect(void *h, const float *o4, const float *d4, int64_t n,
 void orc_bvh_occluded(void *h, const float *o4, const float *d4, int64_t n,
                       uint8_t *occ, int nthreads);
 
+/* Single-ray queries on an oracle BVH (triangle index or -1; t on a hit). */
+int32_t orc_bvh_closest1(void *h, const float o[3], const float d[3], float rmin, float rmax, float *t);
+int orc_bvh_any1(void *h, const float o[3], const float d[3], float rmin, float rmax);
+
+/* Path tracing restatement (pt_oracle.c). Layouts match the device's
+ * ilg_material / ilg_quad_light. cam = eye[3], target[3], up[3], fov, aspect.
+ * out: H x W x 3 floats. */
+typedef struct { float albedo[3]; uint32_t kind; float f0[3]; float alpha; } orc_material;
+typedef struct { float v[4][3]; float emit[3]; uint32_t first_tri; } orc_quad_light;
+int orc_render(const float *pos, uint32_t nverts, const uint32_t *idx, uint32_t ntris, const uint32_t *mat_ids,
+               const orc_material *mats, uint32_t nmats, const orc_quad_light *lights, uint32_t nlights,
+               const float cam[11], uint32_t W, uint32_t H, uint32_t spp, uint32_t max_depth, float eps,
+               uint32_t seed, const float sky[3], int nthreads, float *out);
+
 #ifdef __cplusplus
 }
 #endif

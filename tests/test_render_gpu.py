@@ -1,0 +1,105 @@
+"""The sm_100a wavefront path tracer against the reference's own
+PathIntegrator (box scene, golden image rendered by the compiled reference)."""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from illuminaprt_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN_DIR = os.path.join(os.path.dirname(__file__), "golden")
+REL_MSE_TOL = 1e-3  # north-star parity bar for the converged image
+
+
+def rel_mse(x, ref, eps=1e-2):
+    return float(np.mean((x.astype(np.float64) - ref) ** 2 / (ref.astype(np.float64) ** 2 + eps)))
+
+
+def golden(spp):
+    p = sorted(glob.glob(os.path.join(GOLDEN_DIR, f"box_256_{spp}spp_seed*.npz")))
+    if not p:
+        pytest.skip(f"no {spp}-spp reference image")
+    return np.load(p[0])["image"]
+
+
+@pytest.fixture(scope="module")
+def box_space():
+    from illuminaprt_b200.ilg import GpuSpace
+    sp = GpuSpace()
+    scene = scenes.load_box_scene(sp)
+    return sp, scene
+
+
+def test_box_4096spp_matches_reference(box_space):
+    sp, scene = box_space
+    ref = golden(4096)
+    img = sp.render(scene["camera"], 256, 256, 4096, max_depth=6, epsilon=1e-4, seed=12345)
+    err = rel_mse(img, ref)
+    print(f"relMSE(GPU 4096 spp, reference 4096 spp) = {err:.3e}; mean GPU {img.mean((0, 1))} ref {ref.mean((0, 1))}")
+    assert np.isfinite(img).all()
+    assert err < REL_MSE_TOL
+    # channel means agree to well under a percent (bias check)
+    assert np.allclose(img.mean((0, 1)), ref.mean((0, 1)), rtol=5e-3)
+
+
+def test_box_error_falls_with_samples(box_space):
+    sp, scene = box_space
+    ref = golden(4096)
+    e16 = rel_mse(sp.render(scene["camera"], 256, 256, 16, seed=7), ref)
+    e256 = rel_mse(sp.render(scene["camera"], 256, 256, 256, seed=8), ref)
+    assert e256 < e16 / 8  # ~1/spp convergence (16x more samples)
+
+
+def test_render_is_deterministic_and_seeded(box_space):
+    sp, scene = box_space
+    a = sp.render(scene["camera"], 64, 64, 8, seed=3)
+    b = sp.render(scene["camera"], 64, 64, 8, seed=3)
+    c = sp.render(scene["camera"], 64, 64, 8, seed=4)
+    assert np.allclose(a, b, rtol=1e-5, atol=1e-6)  # float atomics may reorder sums
+    assert not np.allclose(a, c)
+
+
+def test_wave_size_does_not_change_the_image(box_space):
+    sp, scene = box_space
+    a = sp.render(scene["camera"], 64, 48, 16, seed=9, paths_per_wave=64 * 48)
+    b = sp.render(scene["camera"], 64, 48, 16, seed=9, paths_per_wave=64 * 48 * 16)
+    assert np.allclose(a, b, rtol=1e-5, atol=1e-6)
+
+
+def test_render_edge_cases(box_space):
+    from illuminaprt_b200.ilg import GpuSpace, IlgError, ILG_ESTATE, ILG_EINVAL
+    sp, scene = box_space
+    one = sp.render(scene["camera"], 1, 1, 4)
+    assert one.shape == (1, 1, 3) and np.isfinite(one).all()
+    d1 = sp.render(scene["camera"], 32, 32, 64, max_depth=1, seed=2)
+    d6 = sp.render(scene["camera"], 32, 32, 64, max_depth=6, seed=2)
+    assert d1.mean() < d6.mean()  # more bounces, more light
+    with pytest.raises(IlgError) as e:
+        sp.render(scene["camera"], 0, 16, 1)
+    assert e.value.code == ILG_EINVAL
+    fresh = GpuSpace()
+    fresh.initialise(scene["pos"], scene["idx"])
+    fresh.build()
+    with pytest.raises(IlgError) as e:
+        fresh.render(scene["camera"], 8, 8, 1)
+    assert e.value.code == ILG_ESTATE
+
+
+def test_gpu_follows_the_cpu_port_path_for_path(box_space, oracle):
+    """Same counter-based random numbers on both sides: the images differ only
+    where float rounding flips a decision on some path."""
+    sp, scene = box_space
+    s = scene
+    first = int(np.nonzero(s["prim_of_tri"] == s["light_prim"])[0][0])
+    cpu = oracle.render(s["pos"], s["idx"], s["prim_of_tri"], [{"albedo": tuple(a)} for a in s["albedo"]],
+                        [{"v": s["light_quad"], "emit": s["light_emit"], "first_tri": first}], s["camera"],
+                        96, 96, 16, seed=21)
+    gpu = sp.render(s["camera"], 96, 96, 16, seed=21)
+    err = rel_mse(gpu, cpu)
+    close = np.mean(np.abs(gpu - cpu) <= 1e-3 * (np.abs(cpu) + 1e-3))
+    print(f"GPU vs CPU port, same paths: relMSE {err:.3e}, {100 * close:.2f}% of pixels within 0.1%")
+    assert err < 2e-4
+    assert close > 0.97
