@@ -26,7 +26,10 @@ STATUS_NAMES = {0: "ILG_OK", 1: "ILG_EINVAL", 2: "ILG_ENOMEM", 3: "ILG_ECUDA", 4
 # Every symbol the public headers declare; tests check the library exports them.
 EXPORTED = ["ilg_create", "ilg_destroy", "ilg_last_error", "ilg_set_mesh", "ilg_build", "ilg_get_stats",
             "ilg_intersect", "ilg_intersect_counted", "ilg_occluded", "ilg_sync", "ilg_stream",
-            "ilg_set_materials", "ilg_set_quad_lights", "ilg_render"]
+            "ilg_set_materials", "ilg_set_quad_lights", "ilg_render", "ilg_intersect_noalloc"]
+
+# Largest batch ilg_intersect_noalloc accepts (include/ilg.h).
+ILG_NOALLOC_MAX_RAYS = 262144
 
 ILG_MAT_LAMBERT, ILG_MAT_GGX = 0, 1
 
@@ -98,6 +101,8 @@ def load(build_if_missing: bool = True) -> ctypes.CDLL:
     L.ilg_set_materials.argtypes = [vp, vp, u32]
     L.ilg_set_quad_lights.argtypes = [vp, vp, u32]
     L.ilg_render.argtypes = [vp, ctypes.POINTER(ilg_camera), ctypes.POINTER(ilg_render_opts), vp, u32]
+    L.ilg_intersect_noalloc.argtypes = [vp, vp, vp, u32, vp, vp, vp, vp]
+    L.ilg_intersect_noalloc.restype = i32
     L.ilg_sync.argtypes = [vp]
     L.ilg_stream.argtypes = [vp]
     L.ilg_stream.restype = vp

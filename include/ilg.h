@@ -88,6 +88,20 @@ int ilg_intersect(ilg_ctx *ctx, const float *ray_o_tmin, const float *ray_d_tmax
 int ilg_intersect_counted(ilg_ctx *ctx, const float *ray_o_tmin, const float *ray_d_tmax, uint32_t n,
                           int32_t *prim, float *t, float *u, float *v, uint64_t counts[2], uint32_t flags);
 
+/* Closest hit from host buffers that allocates no device memory. This entry
+ * point has no counterpart in the reference. It is for callers that must not
+ * trigger a cudaMalloc at query time (a fixed per-frame device budget, or
+ * device memory owned by another allocator): it stages rays and hits through
+ * one fixed device array per GPU (12 MiB, resident until exit) instead of the
+ * context's growable buffers. At most ILG_NOALLOC_MAX_RAYS rays per call
+ * (more is ILG_EINVAL). All calls on a device share that array, so calls whose
+ * device work overlaps race; serialise them. The first call on each device
+ * looks the array up (cudaGetSymbolAddress); make it before any stream
+ * capture. Results equal ilg_intersect's. */
+#define ILG_NOALLOC_MAX_RAYS 262144u
+int ilg_intersect_noalloc(ilg_ctx *ctx, const float *ray_o_tmin, const float *ray_d_tmax, uint32_t n,
+                          int32_t *prim, float *t, float *u, float *v);
+
 /* Any hit: occ[i] = 1 when some triangle is hit inside the ray's window. */
 int ilg_occluded(ilg_ctx *ctx, const float *ray_o_tmin, const float *ray_d_tmax, uint32_t n,
                  uint8_t *occ, uint32_t flags);
