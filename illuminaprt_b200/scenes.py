@@ -261,3 +261,103 @@ def load_box_scene(space, scene=None):
     first = int(np.nonzero(scene["prim_of_tri"] == scene["light_prim"])[0][0])
     space.set_quad_lights([{"v": scene["light_quad"], "emit": scene["light_emit"], "first_tri": first}])
     return scene
+
+
+# ---------------------------------------------------------------------------
+# Icosphere field (the at-scale path-tracing scene)
+# ---------------------------------------------------------------------------
+def icosphere(subdiv: int):
+    """Unit icosphere: (verts float64 (V,3), faces int64 (F,3)), F = 20 * 4^subdiv,
+    outward winding ((v1 - v0) x (v2 - v0) points out)."""
+    t = (1.0 + 5 ** 0.5) / 2
+    v = np.array([[-1, t, 0], [1, t, 0], [-1, -t, 0], [1, -t, 0], [0, -1, t], [0, 1, t], [0, -1, -t],
+                  [0, 1, -t], [t, 0, -1], [t, 0, 1], [-t, 0, -1], [-t, 0, 1]], np.float64)
+    v /= np.linalg.norm(v, axis=1, keepdims=True)
+    f = np.array([[0, 11, 5], [0, 5, 1], [0, 1, 7], [0, 7, 10], [0, 10, 11], [1, 5, 9], [5, 11, 4], [11, 10, 2],
+                  [10, 7, 6], [7, 1, 8], [3, 9, 4], [3, 4, 2], [3, 2, 6], [3, 6, 8], [3, 8, 9], [4, 9, 5],
+                  [2, 4, 11], [6, 2, 10], [8, 6, 7], [9, 8, 1]], np.int64)
+    for _ in range(subdiv):
+        e = np.concatenate([f[:, [0, 1]], f[:, [1, 2]], f[:, [2, 0]]])
+        e.sort(axis=1)
+        key = e[:, 0] * (v.shape[0] + 1) + e[:, 1]
+        uk, inv = np.unique(key, return_inverse=True)
+        a, b = uk // (v.shape[0] + 1), uk % (v.shape[0] + 1)
+        mid = v[a] + v[b]
+        mid /= np.linalg.norm(mid, axis=1, keepdims=True)
+        m = inv.reshape(3, -1).T + v.shape[0]  # midpoints of edges (01, 12, 20)
+        v = np.concatenate([v, mid])
+        f0, f1, f2 = f[:, 0], f[:, 1], f[:, 2]
+        m01, m12, m20 = m[:, 0], m[:, 1], m[:, 2]
+        f = np.concatenate([np.stack([f0, m01, m20], 1), np.stack([f1, m12, m01], 1),
+                            np.stack([f2, m20, m12], 1), np.stack([m01, m12, m20], 1)])
+    # make the winding outward
+    p = v[f]
+    n = np.cross(p[:, 1] - p[:, 0], p[:, 2] - p[:, 0])
+    flip = (n * p.mean(1)).sum(1) < 0
+    f[flip] = f[flip][:, [0, 2, 1]]
+    return v, f
+
+
+def sphere_field(n_side: int = 8, subdiv: int = 7, seed: int = 3, width: int = 1920, height: int = 1080):
+    """n_side^2 icospheres on a jittered grid (radius U[0.3, 0.6], resting on a
+    ground plane), 50% Lambertian (albedo U[0.1, 0.9]^3) and 50% GGX conductors
+    (alpha U[0.05, 0.5], F0 U[0.5, 1]^3), four 2 x 2 quad lights at height 6
+    with radiance U[10, 30], a constant sky of 0.1. Material 0 is the ground
+    (Lambertian 0.5); materials 1.. belong to the spheres in order; the lights
+    use material 0."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    uv, uf = icosphere(subdiv)
+    ns = n_side * n_side
+    coords = (np.arange(n_side) - (n_side - 1) / 2.0)
+    gx, gz = np.meshgrid(coords, coords)
+    cx = gx.reshape(-1) + rng.uniform(-0.15, 0.15, ns)
+    cz = gz.reshape(-1) + rng.uniform(-0.15, 0.15, ns)
+    r = rng.uniform(0.3, 0.6, ns)
+    nv, nf = uv.shape[0], uf.shape[0]
+    pos = np.empty((ns * nv + 4 + 16, 3), np.float32)
+    idx = np.empty((ns * nf + 2 + 8, 3), np.uint32)
+    mat = np.empty(ns * nf + 2 + 8, np.uint32)
+    mats = [{"albedo": (0.5, 0.5, 0.5), "kind": 0}]
+    is_ggx = rng.permutation(np.arange(ns) < ns // 2)  # exactly half the spheres are conductors
+    for i in range(ns):
+        pos[i * nv:(i + 1) * nv] = uv * r[i] + np.array([cx[i], r[i], cz[i]])
+        idx[i * nf:(i + 1) * nf] = uf + i * nv
+        mat[i * nf:(i + 1) * nf] = i + 1
+        if not is_ggx[i]:
+            mats.append({"albedo": tuple(rng.uniform(0.1, 0.9, 3)), "kind": 0})
+        else:
+            mats.append({"albedo": (0.0, 0.0, 0.0), "kind": 1, "f0": tuple(rng.uniform(0.5, 1.0, 3)),
+                         "alpha": float(rng.uniform(0.05, 0.5))})
+    base_v, base_f = ns * nv, ns * nf
+    G = 50.0
+    pos[base_v:base_v + 4] = [(-G, 0, -G), (-G, 0, G), (G, 0, G), (G, 0, -G)]
+    idx[base_f:base_f + 2] = [(base_v, base_v + 1, base_v + 2), (base_v, base_v + 2, base_v + 3)]  # +y
+    mat[base_f:base_f + 2] = 0
+    lights = []
+    vi, fi = base_v + 4, base_f + 2
+    for k, (lx, lz) in enumerate([(-3, -3), (3, -3), (-3, 3), (3, 3)]):
+        y = 6.0
+        q = np.array([(lx - 1, y, lz - 1), (lx - 1, y, lz + 1), (lx + 1, y, lz + 1), (lx + 1, y, lz - 1)], np.float32)
+        pos[vi:vi + 4] = q
+        # reference Quad tessellation (v1, v3, v2), (v1, v4, v3): normal -y
+        idx[fi:fi + 2] = [(vi, vi + 2, vi + 1), (vi, vi + 3, vi + 2)]
+        mat[fi:fi + 2] = 0
+        e = float(rng.uniform(10.0, 30.0))
+        lights.append({"v": q, "emit": (e, e, e), "first_tri": fi})
+        vi += 4
+        fi += 2
+    return {
+        "pos": pos, "idx": idx, "mat_ids": mat, "materials": mats, "lights": lights,
+        "camera": {"eye": (0.0, 3.5, 9.5), "target": (0.0, 0.3, 0.0), "up": (0.0, 1.0, 0.0), "fov": 40.0,
+                   "aspect": width / height},
+        "width": width, "height": height, "sky": (0.1, 0.1, 0.1), "max_depth": 12, "spp": 64,
+        "epsilon": 1e-4,
+    }
+
+
+def load_sphere_field(space, scene):
+    space.initialise(scene["pos"], scene["idx"], scene["mat_ids"])
+    space.build()
+    space.set_materials(scene["materials"])
+    space.set_quad_lights(scene["lights"])
+    return scene
