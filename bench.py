@@ -153,11 +153,20 @@ def run_reference(args, world, rank):
         tracer(oi, di)
         t_total += time.perf_counter() - t0
     value = per_step * args.steps / t_total / 1e6
+    extra = {}
+    if kind == "reference":
+        box = scenes.box_scene()
+        spp = 4
+        t0 = time.perf_counter()
+        ref.render_box(box, 256, 256, spp, seed=1, nthreads=nthreads)
+        dt = time.perf_counter() - t0
+        extra = {"pt_box_msamples_s": round(256 * 256 * spp / dt / 1e6, 4),
+                 "pt_box_sample": f"256x256 at {spp} spp of the box scene through the reference's PathIntegrator"}
     line = {
         "impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * t_total / args.steps, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "sample_rays_per_step": per_step},
+        "config": {"workload": WORKLOAD, "sample_rays_per_step": per_step, **extra},
         "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": nthreads, "kind": kind,
                          "sample": f"{per_step} random rays per step (half coherent, half incoherent) of the "
                                    f"8,388,608-ray workload; {what}; tree build {build_s} s not timed"},
@@ -166,26 +175,83 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
-def cpu_baseline_sample(pos, idx, co, cd, io, idr):
-    """The reference's CPU path on a bounded sample, for the cpu_baseline key."""
+def cpu_baseline_sample(pos, idx, co, cd, io, idr, seconds=10.0):
+    """The reference's CPU path on a bounded random sample (about `seconds` of
+    work on all host cores), for the cpu_baseline key."""
     from oracle import bindings
     nthreads = os.cpu_count() or 1
     try:
         mesh = bindings.RefLib().mesh(pos, idx, "bvh")
         kind, tracer = "reference", (lambda o, d: mesh.intersect(o, d, nthreads))
-        what = "reference BasicSpace->BVHMesh"
+        what = "reference BasicSpace->BVHMesh (Core/Space/BasicSpace.cpp:58-73, Core/Shape/BVHMesh.cpp:169-198)"
     except FileNotFoundError:
         bvh = bindings.Oracle().bvh(pos, idx)
         kind, tracer = "port", (lambda o, d: bvh.intersect(o, d, nthreads))
         what = "oracle C restatement"
-    n = min(co.shape[0], 16384 * max(1, nthreads))
+    rng = np.random.default_rng(11)
+    probe = rng.choice(co.shape[0], 4096 * nthreads, replace=False)
     t0 = time.perf_counter()
-    tracer(co[:n // 2], cd[:n // 2])
-    tracer(io[:n // 2], idr[:n // 2])
+    tracer(co[probe], cd[probe])
+    tracer(io[probe], idr[probe])
+    rate = 2 * len(probe) / max(time.perf_counter() - t0, 1e-6)
+    half = int(min(co.shape[0], max(16384, rate * seconds / 2)))
+    pick = rng.choice(co.shape[0], half, replace=False)
+    oc, dc, oi, di = co[pick], cd[pick], io[pick], idr[pick]
+    t0 = time.perf_counter()
+    tracer(oc, dc)
+    tracer(oi, di)
     dt = time.perf_counter() - t0
-    return {"value": round(n / dt / 1e6, 4), "unit": UNIT, "cores": nthreads, "kind": kind,
-            "sample": f"first {n // 2} coherent + first {n // 2} incoherent rays of the workload, {what}, "
-                      f"{dt:.1f} s"}
+    return {"value": round(2 * half / dt / 1e6, 4), "unit": UNIT, "cores": nthreads, "kind": kind,
+            "sample": f"{half} random coherent + {half} random incoherent rays of the workload through the {what}, "
+                      f"{dt:.1f} s on {nthreads} threads"}
+
+
+def bench_path_tracer(dev, local, quick=False):
+    """Samples/s of the wavefront path tracer on the box scene (256^2, 16 spp,
+    depth 6) and on the icosphere field (1920x1080, 64 spp, depth 12;
+    64 spheres x 327,680 triangles + ground + 4 lights = 20,971,530 triangles)."""
+    import torch
+    from illuminaprt_b200 import scenes
+    from illuminaprt_b200.ilg import GpuSpace
+    res = {}
+    sp = GpuSpace(device=local)
+    box = scenes.load_box_scene(sp)
+    out = torch.empty((256, 256, 3), dtype=torch.float32, device=dev)
+    st = torch.cuda.ExternalStream(sp.stream, device=dev)
+    sp.render(box["camera"], 256, 256, 16, seed=1, out=out)
+    sp.sync()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 3
+    e0.record(st)
+    for r in range(reps):
+        sp.render(box["camera"], 256, 256, 16, seed=2 + r, out=out)
+    e1.record(st)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    res["pt_box_256x256x16spp_ms"] = round(ms, 3)
+    res["pt_box_msamples_s"] = round(256 * 256 * 16 / (ms / 1e3) / 1e6, 3)
+    sp.close()
+    if quick:
+        return res
+    field = scenes.sphere_field(8, 7, seed=3)
+    sp = GpuSpace(device=local)
+    scenes.load_sphere_field(sp, field)
+    W, H, spp = field["width"], field["height"], field["spp"]
+    out = torch.empty((H, W, 3), dtype=torch.float32, device=dev)
+    st = torch.cuda.ExternalStream(sp.stream, device=dev)
+    sp.render(field["camera"], W, H, 1, max_depth=12, seed=1, sky=field["sky"], out=out)
+    sp.sync()
+    e0.record(st)
+    sp.render(field["camera"], W, H, spp, max_depth=12, seed=2, sky=field["sky"], out=out)
+    e1.record(st)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    res["pt_field_triangles"] = int(field["idx"].shape[0])
+    res["pt_field_bvh_build_ms"] = round(sp.stats()["build_ms"], 2)
+    res["pt_field_1080p_64spp_ms"] = round(ms, 2)
+    res["pt_field_msamples_s"] = round(W * H * spp / (ms / 1e3) / 1e6, 3)
+    sp.close()
+    return res
 
 
 def main():
@@ -195,6 +261,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-path-tracer", action="store_true")
     args = ap.parse_args()
     world, rank, local = dist_setup()
 
@@ -295,6 +362,7 @@ def main():
     # the e2e hits must equal the device-resident ones
     assert torch.equal(hout["incoherent"][0], out["incoherent"][0].cpu())
 
+    pt = {} if args.no_path_tracer else bench_path_tracer(dev, local)
     hbm, peak_kind = load_peaks()
     # algorithmic bytes of one incoherent launch (the dominant kernel): rays in,
     # hits out, and every node / triangle record the traversal reads
@@ -316,7 +384,7 @@ def main():
                        "coherent_mrays_s": round(n_co * args.steps / (t_co / 1e3) / 1e6, 3),
                        "incoherent_mrays_s": round(n_in * args.steps / (t_in / 1e3) / 1e6, 3),
                        "bvh_nodes": stats["n_nodes"], "bvh_build_ms": round(stats["build_ms"], 3),
-                       "scene_bytes": stats["node_bytes"] + stats["tri_bytes"]},
+                       "scene_bytes": stats["node_bytes"] + stats["tri_bytes"], **pt},
             "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": rays_per_step * RAY_IN,
                     "d2h_bytes_per_step": rays_per_step * HIT_OUT},
             "gpu_launches": 2 * args.steps,
