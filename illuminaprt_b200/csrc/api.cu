@@ -414,3 +414,131 @@ int ilg_render(ilg_ctx *ctx, const ilg_camera *cam, const ilg_render_opts *opts,
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// radiance-cache network
+// ---------------------------------------------------------------------------
+namespace {
+
+int mlp_reserve_train(ilg_ctx *ctx, uint32_t n)
+{
+    const size_t cap = ((size_t)n + 15) / 16 * 16;
+    if (ctx->mlp_xcm.cap >= cap * kMlpIn) return ILG_OK;
+    CK(ctx->mlp_xcm.reserve(cap * kMlpIn));
+    CK(ctx->mlp_hcm.reserve(cap * 5 * kMlpHid));
+    CK(ctx->mlp_dzcm.reserve(cap * (5 * kMlpHid + kMlpOutP)));
+    return ILG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ilg_mlp_init(ilg_ctx *ctx, uint32_t seed, float learning_rate)
+{
+    if (!ctx) return ILG_EINVAL;
+    if (!(learning_rate > 0.f)) return fail(ctx, ILG_EINVAL, "ilg_mlp_init: learning rate must be > 0");
+    CK(cudaSetDevice(ctx->device));
+    CK(ctx->mlp_w.reserve(kMlpParams)); CK(ctx->mlp_m.reserve(kMlpParams)); CK(ctx->mlp_v.reserve(kMlpParams));
+    CK(ctx->mlp_grad.reserve(kMlpParams)); CK(ctx->mlp_loss.reserve(1));
+    CK(ctx->mlp_wf.reserve(kFwdElems)); CK(ctx->mlp_wb.reserve(kBwdElems));
+    CK(mlp_init(ctx->mlp_view(), seed, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->mlp_ready = true;
+    ctx->mlp_step = 0;
+    ctx->mlp_lr = learning_rate;
+    return ILG_OK;
+}
+
+int ilg_mlp_get_params(ilg_ctx *ctx, float *params)
+{
+    if (!ctx || !params) return ILG_EINVAL;
+    if (!ctx->mlp_ready) return fail(ctx, ILG_ESTATE, "ilg_mlp_get_params: network not initialised");
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaMemcpyAsync(params, ctx->mlp_w.ptr, sizeof(float) * kMlpParams, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return ILG_OK;
+}
+
+int ilg_mlp_set_params(ilg_ctx *ctx, const float *params)
+{
+    if (!ctx || !params) return ILG_EINVAL;
+    if (!ctx->mlp_ready) return fail(ctx, ILG_ESTATE, "ilg_mlp_set_params: network not initialised");
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaMemcpyAsync(ctx->mlp_w.ptr, params, sizeof(float) * kMlpParams, cudaMemcpyHostToDevice, ctx->stream));
+    CK(mlp_refresh_copies(ctx->mlp_view(), ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return ILG_OK;
+}
+
+int ilg_mlp_infer(ilg_ctx *ctx, const float *raw, uint32_t n, float *out, uint32_t flags)
+{
+    if (!ctx) return ILG_EINVAL;
+    if (!ctx->mlp_ready) return fail(ctx, ILG_ESTATE, "ilg_mlp_infer: network not initialised");
+    if (n == 0) return ILG_OK;
+    if (!raw || !out) return fail(ctx, ILG_EINVAL, "ilg_mlp_infer: null array");
+    CK(cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    if (flags & ILG_DEVICE_PTRS) {
+        CK(mlp_infer(ctx->mlp_view(), raw, n, out, st));
+        return ILG_OK;
+    }
+    CK(ctx->mlp_raw.reserve((size_t)n * kMlpRaw));
+    CK(ctx->mlp_out.reserve((size_t)n * 3));
+    CK(cudaMemcpyAsync(ctx->mlp_raw.ptr, raw, sizeof(float) * kMlpRaw * n, cudaMemcpyHostToDevice, st));
+    CK(mlp_infer(ctx->mlp_view(), ctx->mlp_raw.ptr, n, ctx->mlp_out.ptr, st));
+    CK(cudaMemcpyAsync(out, ctx->mlp_out.ptr, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return ILG_OK;
+}
+
+static int mlp_grads_common(ilg_ctx *ctx, const float *raw, const float *target, uint32_t n, uint32_t flags,
+                            float *loss)
+{
+    if (!ctx->mlp_ready) return fail(ctx, ILG_ESTATE, "network not initialised");
+    if (n == 0 || !raw || !target) return fail(ctx, ILG_EINVAL, "empty batch or null array");
+    CK(cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    int rc = mlp_reserve_train(ctx, n);
+    if (rc) return rc;
+    const float *draw = raw, *dtgt = target;
+    if (!(flags & ILG_DEVICE_PTRS)) {
+        CK(ctx->mlp_raw.reserve((size_t)n * kMlpRaw));
+        CK(ctx->mlp_tgt.reserve((size_t)n * 3));
+        CK(cudaMemcpyAsync(ctx->mlp_raw.ptr, raw, sizeof(float) * kMlpRaw * n, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(ctx->mlp_tgt.ptr, target, sizeof(float) * 3 * n, cudaMemcpyHostToDevice, st));
+        draw = ctx->mlp_raw.ptr;
+        dtgt = ctx->mlp_tgt.ptr;
+    }
+    CK(mlp_grads(ctx->mlp_view(), draw, dtgt, n, st));
+    if (loss) {
+        CK(cudaMemcpyAsync(loss, ctx->mlp_loss.ptr, sizeof(float), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+    }
+    return ILG_OK;
+}
+
+int ilg_mlp_grads(ilg_ctx *ctx, const float *raw, const float *target, uint32_t n, float *grad, float *loss,
+                  uint32_t flags)
+{
+    if (!ctx) return ILG_EINVAL;
+    if (!grad) return fail(ctx, ILG_EINVAL, "ilg_mlp_grads: null grad");
+    int rc = mlp_grads_common(ctx, raw, target, n, flags, loss);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(grad, ctx->mlp_grad.ptr, sizeof(float) * kMlpParams, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return ILG_OK;
+}
+
+int ilg_mlp_train_step(ilg_ctx *ctx, const float *raw, const float *target, uint32_t n, float *loss, uint32_t flags)
+{
+    if (!ctx) return ILG_EINVAL;
+    int rc = mlp_grads_common(ctx, raw, target, n, flags, loss);
+    if (rc) return rc;
+    ctx->mlp_step++;
+    CK(mlp_adam(ctx->mlp_view(), ctx->mlp_step, ctx->mlp_lr, ctx->stream));
+    if (!(flags & ILG_DEVICE_PTRS)) CK(cudaStreamSynchronize(ctx->stream));
+    return ILG_OK;
+}
+
+}  // extern "C"

@@ -7,6 +7,7 @@
 #include "ilg.h"
 #include "trace_api.cuh"
 #include "render.cuh"
+#include "mlp.cuh"
 
 struct ilg_ctx {
     int device = 0;
@@ -52,6 +53,22 @@ struct ilg_ctx {
     ilg::DevBuf<float> hit_t, out_dev;
     uint32_t last_render_launches = 0;
 
+    // radiance-cache network
+    ilg::DevBuf<float> mlp_w, mlp_m, mlp_v, mlp_grad, mlp_loss, mlp_raw, mlp_tgt, mlp_out;
+    ilg::DevBuf<__nv_bfloat16> mlp_wf, mlp_wb, mlp_xcm, mlp_hcm, mlp_dzcm;
+    bool mlp_ready = false;
+    uint32_t mlp_step = 0;
+    float mlp_lr = 1e-2f;
+
+    ilg::MlpDev mlp_view() const
+    {
+        ilg::MlpDev M;
+        M.w = mlp_w.ptr; M.m = mlp_m.ptr; M.v = mlp_v.ptr; M.grad = mlp_grad.ptr; M.loss = mlp_loss.ptr;
+        M.wf = mlp_wf.ptr; M.wb = mlp_wb.ptr; M.xcm = mlp_xcm.ptr; M.hcm = mlp_hcm.ptr; M.dzcm = mlp_dzcm.ptr;
+        M.cap = (uint32_t)(mlp_xcm.cap / ilg::kMlpIn);
+        return M;
+    }
+
     ilg::SceneView view() const
     {
         return ilg::SceneView{bb.nodes, bb.tris, bb.prim_of, stats.n_nodes, stats.n_tris};
@@ -82,5 +99,8 @@ struct ilg_ctx {
         q_o0.release(); q_d0.release(); q_o1.release(); q_d1.release(); beta.release(); s_o.release();
         s_d.release(); s_c.release(); accum.release(); q_p0.release(); q_p1.release(); counts.release();
         hit_tri.release(); hit_t.release(); out_dev.release();
+        mlp_w.release(); mlp_m.release(); mlp_v.release(); mlp_grad.release(); mlp_loss.release();
+        mlp_raw.release(); mlp_tgt.release(); mlp_out.release(); mlp_wf.release(); mlp_wb.release();
+        mlp_xcm.release(); mlp_hcm.release(); mlp_dzcm.release();
     }
 };

@@ -26,7 +26,12 @@ STATUS_NAMES = {0: "ILG_OK", 1: "ILG_EINVAL", 2: "ILG_ENOMEM", 3: "ILG_ECUDA", 4
 # Every symbol the public headers declare; tests check the library exports them.
 EXPORTED = ["ilg_create", "ilg_destroy", "ilg_last_error", "ilg_set_mesh", "ilg_build", "ilg_get_stats",
             "ilg_intersect", "ilg_intersect_counted", "ilg_occluded", "ilg_sync", "ilg_stream",
-            "ilg_set_materials", "ilg_set_quad_lights", "ilg_render", "ilg_intersect_noalloc"]
+            "ilg_set_materials", "ilg_set_quad_lights", "ilg_render", "ilg_intersect_noalloc",
+            "ilg_mlp_init", "ilg_mlp_get_params", "ilg_mlp_set_params", "ilg_mlp_infer", "ilg_mlp_grads",
+            "ilg_mlp_train_step"]
+
+ILG_MLP_RAW = 16
+ILG_MLP_PARAMS = 23040
 
 # Largest batch ilg_intersect_noalloc accepts (include/ilg.h).
 ILG_NOALLOC_MAX_RAYS = 262144
@@ -103,6 +108,15 @@ def load(build_if_missing: bool = True) -> ctypes.CDLL:
     L.ilg_render.argtypes = [vp, ctypes.POINTER(ilg_camera), ctypes.POINTER(ilg_render_opts), vp, u32]
     L.ilg_intersect_noalloc.argtypes = [vp, vp, vp, u32, vp, vp, vp, vp]
     L.ilg_intersect_noalloc.restype = i32
+    L.ilg_mlp_init.argtypes = [vp, u32, ctypes.c_float]
+    L.ilg_mlp_get_params.argtypes = [vp, vp]
+    L.ilg_mlp_set_params.argtypes = [vp, vp]
+    L.ilg_mlp_infer.argtypes = [vp, vp, u32, vp, u32]
+    L.ilg_mlp_grads.argtypes = [vp, vp, vp, u32, vp, vp, u32]
+    L.ilg_mlp_train_step.argtypes = [vp, vp, vp, u32, vp, u32]
+    for f in ("ilg_mlp_init", "ilg_mlp_get_params", "ilg_mlp_set_params", "ilg_mlp_infer", "ilg_mlp_grads",
+              "ilg_mlp_train_step"):
+        getattr(L, f).restype = i32
     L.ilg_sync.argtypes = [vp]
     L.ilg_stream.argtypes = [vp]
     L.ilg_stream.restype = vp
@@ -239,6 +253,43 @@ class GpuSpace:
         img = np.empty((height, width, 3), np.float32)
         self._check(self.L.ilg_render(self.h, ctypes.byref(cam), ctypes.byref(o), img.ctypes.data, 0))
         return img
+
+    # --- radiance-cache network -------------------------------------------
+    def mlp_init(self, seed: int = 1, lr: float = 1e-2):
+        self._check(self.L.ilg_mlp_init(self.h, seed, lr))
+
+    def mlp_params(self) -> np.ndarray:
+        p = np.empty(ILG_MLP_PARAMS, np.float32)
+        self._check(self.L.ilg_mlp_get_params(self.h, p.ctypes.data))
+        return p
+
+    def mlp_set_params(self, p):
+        p = np.ascontiguousarray(p, np.float32)
+        assert p.size == ILG_MLP_PARAMS
+        self._check(self.L.ilg_mlp_set_params(self.h, p.ctypes.data))
+
+    def mlp_infer(self, raw) -> np.ndarray:
+        raw = np.ascontiguousarray(raw, np.float32).reshape(-1, ILG_MLP_RAW)
+        out = np.empty((raw.shape[0], 3), np.float32)
+        self._check(self.L.ilg_mlp_infer(self.h, raw.ctypes.data, raw.shape[0], out.ctypes.data, 0))
+        return out
+
+    def mlp_grads(self, raw, target):
+        raw = np.ascontiguousarray(raw, np.float32).reshape(-1, ILG_MLP_RAW)
+        target = np.ascontiguousarray(target, np.float32).reshape(-1, 3)
+        g = np.empty(ILG_MLP_PARAMS, np.float32)
+        loss = ctypes.c_float()
+        self._check(self.L.ilg_mlp_grads(self.h, raw.ctypes.data, target.ctypes.data, raw.shape[0], g.ctypes.data,
+                                         ctypes.byref(loss), 0))
+        return loss.value, g
+
+    def mlp_train_step(self, raw, target) -> float:
+        raw = np.ascontiguousarray(raw, np.float32).reshape(-1, ILG_MLP_RAW)
+        target = np.ascontiguousarray(target, np.float32).reshape(-1, 3)
+        loss = ctypes.c_float()
+        self._check(self.L.ilg_mlp_train_step(self.h, raw.ctypes.data, target.ctypes.data, raw.shape[0],
+                                              ctypes.byref(loss), 0))
+        return loss.value
 
     def sync(self):
         self._check(self.L.ilg_sync(self.h))

@@ -167,6 +167,29 @@ int ilg_set_quad_lights(ilg_ctx *ctx, const ilg_quad_light *lights, uint32_t n);
 int ilg_render(ilg_ctx *ctx, const ilg_camera *cam, const ilg_render_opts *opts, float *out_rgb,
                uint32_t flags);
 
+/* ------------------------------------------------------------------------
+ * Radiance-cache network (no counterpart in the reference, whose closest
+ * analogue is the irradiance cache of Core/Integrator/ICIntegrator.*): a
+ * 96 -> 64 x 5 (ReLU) -> 3 MLP, BF16 weights and activations, FP32
+ * accumulation on the tensor cores, trained with Adam on a relative L2 loss.
+ * Queries are ILG_MLP_RAW floats per row: position normalised to [0,1]^3,
+ * outgoing direction, normal, roughness, albedo, 3 unused. The position is
+ * encoded with 12 sine/cosine frequency bands per axis on the device.
+ * ---------------------------------------------------------------------- */
+#define ILG_MLP_RAW 16u
+#define ILG_MLP_PARAMS 23040u /* FP32 weights, per layer row-major [in][out] */
+
+int ilg_mlp_init(ilg_ctx *ctx, uint32_t seed, float learning_rate);
+int ilg_mlp_get_params(ilg_ctx *ctx, float *params /* ILG_MLP_PARAMS */);
+int ilg_mlp_set_params(ilg_ctx *ctx, const float *params);
+/* out: n x 3 radiance. Host pointers unless ILG_DEVICE_PTRS. */
+int ilg_mlp_infer(ilg_ctx *ctx, const float *raw, uint32_t n, float *out, uint32_t flags);
+/* Gradient of the mean relative L2 loss over the batch (no update). */
+int ilg_mlp_grads(ilg_ctx *ctx, const float *raw, const float *target, uint32_t n, float *grad /* ILG_MLP_PARAMS */,
+                  float *loss, uint32_t flags);
+/* One Adam step on the batch; *loss (optional) receives the loss before the step. */
+int ilg_mlp_train_step(ilg_ctx *ctx, const float *raw, const float *target, uint32_t n, float *loss, uint32_t flags);
+
 /* Blocks until the context's stream is idle (for ILG_DEVICE_PTRS callers). */
 int ilg_sync(ilg_ctx *ctx);
 

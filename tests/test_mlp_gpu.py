@@ -1,0 +1,70 @@
+"""The BF16 tensor-core MLP kernels against the float64 CPU oracle."""
+import numpy as np
+import pytest
+
+from oracle import mlp_oracle as mo
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def net():
+    from illuminaprt_b200.ilg import GpuSpace
+    sp = GpuSpace()
+    sp.mlp_init(seed=7, lr=1e-2)
+    return sp
+
+
+def test_forward_matches_oracle(net):
+    raw, _ = mo.random_batch(5000, seed=1)  # not a multiple of 16: ragged last tile
+    p = net.mlp_params()
+    y_gpu = net.mlp_infer(raw)
+    y_ref, _, _ = mo.forward(p, raw, bf=True)
+    scale = np.abs(y_ref).max()
+    err = np.abs(y_gpu - y_ref).max() / scale
+    print(f"forward: max |gpu - oracle| / max|y| = {err:.2e}")
+    assert err < 1e-2
+    assert np.mean(np.abs(y_gpu - y_ref)) / np.mean(np.abs(y_ref)) < 2e-3
+
+
+@pytest.mark.parametrize("n", [16, 1000, 20000])
+def test_gradients_match_oracle(net, n):
+    raw, tgt = mo.random_batch(n, seed=n)
+    p = net.mlp_params()
+    loss_g, g_gpu = net.mlp_grads(raw, tgt)
+    loss_r, g_ref = mo.loss_and_grads(p, raw, tgt, bf=True)
+    loss_x, g_exact = mo.loss_and_grads(p, raw, tgt, bf=False)
+    rel = np.linalg.norm(g_gpu - g_ref) / np.linalg.norm(g_ref)
+    cos_exact = g_gpu @ g_exact / (np.linalg.norm(g_gpu) * np.linalg.norm(g_exact))
+    print(f"n={n}: loss gpu {loss_g:.6f} oracle {loss_r:.6f}; grad rel err vs bf16 oracle {rel:.2e}; "
+          f"cosine vs exact float64 {cos_exact:.5f}")
+    assert abs(loss_g - loss_r) <= 1e-3 * abs(loss_r) + 1e-6
+    assert rel < 3e-2
+    assert cos_exact > 0.995
+    # per layer, too
+    for l in range(mo.LAYERS):
+        a, b = g_gpu[mo.OFFS[l]:mo.OFFS[l + 1]], g_ref[mo.OFFS[l]:mo.OFFS[l + 1]]
+        assert np.linalg.norm(a - b) <= 5e-2 * np.linalg.norm(b) + 1e-9, l
+
+
+def test_set_get_params_round_trip(net):
+    p = mo.init_params(seed=3)
+    net.mlp_set_params(p)
+    assert np.array_equal(net.mlp_params(), p)
+    raw, _ = mo.random_batch(333, seed=9)
+    y_ref, _, _ = mo.forward(p, raw, bf=True)
+    assert np.abs(net.mlp_infer(raw) - y_ref).max() < 1e-2 * np.abs(y_ref).max()
+
+
+def test_training_fits_a_smooth_field():
+    from illuminaprt_b200.ilg import GpuSpace
+    sp = GpuSpace()
+    sp.mlp_init(seed=11, lr=1e-2)
+    raw, tgt = mo.random_batch(1 << 15, seed=12)
+    losses = [sp.mlp_train_step(raw[i % 4::4], tgt[i % 4::4]) for i in range(400)]
+    test_raw, test_tgt = mo.random_batch(4096, seed=13)
+    y = sp.mlp_infer(test_raw)
+    rel = np.mean((y - test_tgt) ** 2 / (test_tgt ** 2 + 0.01))
+    print(f"training: loss {losses[0]:.4f} -> {losses[-1]:.5f}; held-out relative L2 {rel:.5f}")
+    assert losses[-1] < losses[0] / 20
+    assert rel < 0.01

@@ -1,0 +1,59 @@
+"""The MLP oracle's hand-written backward pass against torch float64 autograd
+and finite differences (no GPU)."""
+import numpy as np
+
+from oracle import mlp_oracle as mo
+
+
+def test_backward_matches_autograd():
+    import torch
+    raw, tgt = mo.random_batch(64, seed=3)
+    p = mo.init_params(seed=1).astype(np.float64)
+    loss, g = mo.loss_and_grads(p, raw, tgt, bf=False)
+    pt = torch.tensor(p, dtype=torch.float64, requires_grad=True)
+    x = torch.tensor(mo.encode(raw), dtype=torch.float64)
+    h = x
+    for l in range(mo.LAYERS):
+        w = pt[mo.OFFS[l]:mo.OFFS[l + 1]].reshape(mo.DIMS[l])
+        h = h @ w
+        if l < mo.LAYERS - 1:
+            h = torch.relu(h)
+    y = h[:, :3]
+    t = torch.tensor(tgt, dtype=torch.float64)
+    tl = (((y - t) ** 2) / (y.detach() ** 2 + 0.01)).mean()
+    tl.backward()
+    ga = pt.grad.numpy().copy()
+    ga[mo.OFFS[5]:].reshape(mo.HID, mo.OUTP)[:, 3:] = 0.0
+    assert abs(tl.item() - loss) < 1e-12
+    assert np.allclose(g, ga, rtol=1e-9, atol=1e-12)
+
+
+def test_backward_matches_finite_differences():
+    raw, tgt = mo.random_batch(32, seed=4)
+    p = mo.init_params(seed=2).astype(np.float64)
+    _, g = mo.loss_and_grads(p, raw, tgt, bf=False)
+
+    def f(q):
+        y, _, _ = mo.forward(q, raw, bf=False)
+        # the loss treats its denominator as a constant, evaluated at p
+        y0, _, _ = mo.forward(p, raw, bf=False)
+        return np.sum((y - tgt) ** 2 / (y0 * y0 + 0.01)) / (3 * y.shape[0])
+
+    rng = np.random.default_rng(0)
+    for i in rng.choice(mo.OFFS[5] + 3, 12, replace=False):
+        e = np.zeros_like(p)
+        e[i] = 1e-6
+        fd = (f(p + e) - f(p - e)) / 2e-6
+        assert abs(fd - g[i]) <= 1e-6 + 1e-4 * abs(fd), (i, fd, g[i])
+
+
+def test_bf16_rounding():
+    # bf16 keeps 7 fraction bits: the spacing above 1 is 2^-7
+    x = np.array([1.0, 1.00390625, 1.001953125, 1.005859375, -3.14159, 0.0, 1.01171875])
+    r = mo.bf16(x)
+    assert r[0] == 1.0
+    assert r[1] == 1.0          # 1 + 2^-8: a tie, rounds to the even neighbour
+    assert r[2] == 1.0          # below the midpoint
+    assert r[3] == 1.0078125    # above the midpoint
+    assert r[6] == 1.015625     # 1 + 3 * 2^-8: a tie, rounds to even (1 + 2^-6)
+    assert abs(r[4] + 3.140625) < 1e-12
