@@ -98,10 +98,17 @@ int ilg_set_mesh(ilg_ctx *ctx, const float *pos_xyz, uint32_t n_verts, const uin
     for (uint64_t i = 0; i < 3ull * n_tris; i++)
         if (idx[i] >= n_verts) return fail(ctx, ILG_EINVAL, "ilg_set_mesh: index %u out of range at %llu", idx[i], (unsigned long long)i);
     float maxabs = 0.f;
+    float lo[3] = {3.0e38f, 3.0e38f, 3.0e38f}, hi[3] = {-3.0e38f, -3.0e38f, -3.0e38f};
     for (uint64_t i = 0; i < 3ull * n_verts; i++) {
         float a = fabsf(pos_xyz[i]);
         if (!(a <= 3.0e38f)) return fail(ctx, ILG_EINVAL, "ilg_set_mesh: non-finite position at %llu", (unsigned long long)i);
         maxabs = std::max(maxabs, a);
+        lo[i % 3] = std::min(lo[i % 3], pos_xyz[i]);
+        hi[i % 3] = std::max(hi[i % 3], pos_xyz[i]);
+    }
+    for (int k = 0; k < 3; k++) {
+        ctx->scene_lo[k] = lo[k];
+        ctx->scene_hi[k] = hi[k];
     }
     CK(cudaSetDevice(ctx->device));
     CK(ctx->pos.reserve(3ull * n_verts));
@@ -247,6 +254,7 @@ int ilg_occluded(ilg_ctx *ctx, const float *ray_o_tmin, const float *ray_d_tmax,
 // path tracing
 // ---------------------------------------------------------------------------
 namespace {
+int mlp_reserve_train(ilg_ctx *ctx, uint32_t n);
 
 struct V3 {
     float x, y, z;
@@ -333,6 +341,12 @@ int ilg_render(ilg_ctx *ctx, const ilg_camera *cam, const ilg_render_opts *opts,
     if (W == 0 || H == 0 || opts->spp == 0 || (uint64_t)W * H > (1u << 26))
         return fail(ctx, ILG_EINVAL, "ilg_render: bad image size %ux%u or spp %u", W, H, opts->spp);
     if (opts->max_depth == 0 || opts->max_depth > 64) return fail(ctx, ILG_EINVAL, "ilg_render: max_depth must be 1..64");
+    const uint32_t cache_depth = opts->cache_depth;
+    if (cache_depth) {
+        if (!ctx->mlp_ready) return fail(ctx, ILG_ESTATE, "ilg_render: cache_depth set but ilg_mlp_init not called");
+        if (cache_depth >= opts->max_depth)
+            return fail(ctx, ILG_EINVAL, "ilg_render: cache_depth %u must be below max_depth %u", cache_depth, opts->max_depth);
+    }
     for (uint32_t l = 0; l < ctx->n_lights; l++)
         if ((uint64_t)ctx->light_first_host[l] + 1 >= ctx->n_tris)
             return fail(ctx, ILG_EINVAL, "ilg_render: light %u triangles out of range of the mesh", l);
@@ -393,10 +407,71 @@ int ilg_render(ilg_ctx *ctx, const ilg_camera *cam, const ilg_render_opts *opts,
     R.sh_count = ctx->counts.ptr + 2; R.sh_capacity = cap * nl;
     R.accum = ctx->accum.ptr; R.err = ctx->derr.ptr;
 
+    const uint32_t train_every = opts->train_every ? opts->train_every : 16u;
+    const uint32_t train_steps = opts->train_steps ? opts->train_steps : 4u;
+    const uint32_t train_batch = opts->train_batch ? opts->train_batch : 16384u;
+    MlpDev mlp = {};
+    if (cache_depth) {
+        const uint32_t train_cap = cap / train_every * 2u + 1024u;
+        const uint32_t rec_cap = train_steps * train_batch;
+        CK(ctx->counts.reserve(8));
+        CK(ctx->train_slot.reserve(cap));
+        CK(ctx->rec_of.reserve((size_t)train_cap * (opts->max_depth + 1)));
+        CK(ctx->s_meta.reserve((size_t)cap * nl));
+        CK(ctx->rec_feat.reserve((size_t)rec_cap * kMlpRaw));
+        CK(ctx->rec_tgt.reserve((size_t)rec_cap * 3));
+        CK(ctx->rec_beta.reserve(rec_cap));
+        CK(ctx->qry_feat.reserve((size_t)cap * kMlpRaw));
+        CK(ctx->qry_out.reserve((size_t)cap * 3));
+        CK(ctx->qry_beta.reserve(cap));
+        {
+            int rc = mlp_reserve_train(ctx, train_batch);
+            if (rc) return rc;
+        }
+        R.cache_depth = cache_depth;
+        R.train_every = train_every;
+        R.scene_lo = make_float3(ctx->scene_lo[0], ctx->scene_lo[1], ctx->scene_lo[2]);
+        R.scene_inv_ext = make_float3(1.f / std::max(ctx->scene_hi[0] - ctx->scene_lo[0], 1e-20f),
+                                      1.f / std::max(ctx->scene_hi[1] - ctx->scene_lo[1], 1e-20f),
+                                      1.f / std::max(ctx->scene_hi[2] - ctx->scene_lo[2], 1e-20f));
+        R.train_slot = ctx->train_slot.ptr;
+        R.train_count = ctx->counts.ptr + 3;
+        R.train_cap = train_cap;
+        R.rec_of = ctx->rec_of.ptr;
+        R.rec_feat = ctx->rec_feat.ptr;
+        R.rec_beta = ctx->rec_beta.ptr;
+        R.rec_tgt = ctx->rec_tgt.ptr;
+        R.rec_count = ctx->counts.ptr + 4;
+        R.rec_cap = rec_cap;
+        R.qry_feat = ctx->qry_feat.ptr;
+        R.qry_beta = ctx->qry_beta.ptr;
+        R.qry_out = ctx->qry_out.ptr;
+        R.qry_count = ctx->counts.ptr + 5;
+        R.s_meta = ctx->s_meta.ptr;
+        CK(cudaMemsetAsync(R.rec_count, 0, sizeof(uint32_t), st));
+        mlp = ctx->mlp_view();
+    }
+
     uint32_t launches = 0;
     for (uint32_t s0 = 0; s0 < opts->spp; s0 += spp_per_wave) {
         const uint32_t k = std::min(spp_per_wave, opts->spp - s0);
-        CK(render_wave(R, wh * k, s0, st, &launches));
+        CK(render_wave(R, wh * k, s0, st, &launches, cache_depth ? &mlp : nullptr));
+    }
+    if (cache_depth) {
+        // online training on this call's records (the next call renders with the update)
+        uint32_t n_rec = 0;
+        CK(cudaMemcpyAsync(&n_rec, R.rec_count, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        n_rec = std::min(n_rec, R.rec_cap);
+        ctx->last_train_records = n_rec;
+        for (uint32_t s = 0; s < train_steps && (uint64_t)s * train_batch < n_rec; s++) {
+            const uint32_t nb = std::min(train_batch, n_rec - s * train_batch);
+            CK(mlp_grads(mlp, R.rec_feat + (size_t)s * train_batch * kMlpRaw, R.rec_tgt + (size_t)s * train_batch * 3,
+                         nb, st));
+            ctx->mlp_step++;
+            CK(mlp_adam(mlp, ctx->mlp_step, ctx->mlp_lr, st));
+            launches += 9;
+        }
     }
     float *out_dev = out_rgb;
     if (!(flags & ILG_DEVICE_PTRS)) {

@@ -21,6 +21,7 @@ struct ilg_ctx {
     uint32_t n_verts = 0, n_tris = 0;
     bool has_mat = false;
     float max_abs = 0.f;
+    float scene_lo[3] = {0.f, 0.f, 0.f}, scene_hi[3] = {1.f, 1.f, 1.f};
 
     // built scene
     ilg::BuildBuffers bb;
@@ -51,6 +52,12 @@ struct ilg_ctx {
     ilg::DevBuf<uint32_t> q_p0, q_p1, counts;
     ilg::DevBuf<int> hit_tri;
     ilg::DevBuf<float> hit_t, out_dev;
+    // path tracing with the radiance cache
+    ilg::DevBuf<uint32_t> train_slot, rec_of, s_meta;
+    ilg::DevBuf<float> rec_feat, rec_tgt, qry_feat, qry_out;
+    ilg::DevBuf<float4> rec_beta, qry_beta;
+    uint32_t last_train_records = 0;
+    float last_train_loss = 0.f;
     uint32_t last_render_launches = 0;
 
     // radiance-cache network
@@ -99,6 +106,8 @@ struct ilg_ctx {
         q_o0.release(); q_d0.release(); q_o1.release(); q_d1.release(); beta.release(); s_o.release();
         s_d.release(); s_c.release(); accum.release(); q_p0.release(); q_p1.release(); counts.release();
         hit_tri.release(); hit_t.release(); out_dev.release();
+        train_slot.release(); rec_of.release(); s_meta.release(); rec_feat.release(); rec_tgt.release();
+        qry_feat.release(); qry_out.release(); rec_beta.release(); qry_beta.release();
         mlp_w.release(); mlp_m.release(); mlp_v.release(); mlp_grad.release(); mlp_loss.release();
         mlp_raw.release(); mlp_tgt.release(); mlp_out.release(); mlp_wf.release(); mlp_wb.release();
         mlp_xcm.release(); mlp_hcm.release(); mlp_dzcm.release();

@@ -150,9 +150,10 @@ __device__ __forceinline__ void encode_rows(const float *raw, uint32_t n, uint32
 
 template <bool kTrain>
 __global__ void __launch_bounds__(128) k_mlp_fwd(MlpDev M, const float *__restrict__ raw, uint32_t n,
-                                                 float *__restrict__ out)
+                                                 float *__restrict__ out, const uint32_t *__restrict__ n_dev)
 {
     extern __shared__ __align__(16) __nv_bfloat16 sw[];
+    if (n_dev) n = min(n, *n_dev);  // row count produced on the device (capped by the launch size)
     load_smem(sw, M.wf, kFwdElems);
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, tig = lane & 3;
@@ -454,7 +455,8 @@ cudaError_t mlp_refresh_copies(const MlpDev &M, cudaStream_t st)
     return cudaGetLastError();
 }
 
-cudaError_t mlp_infer(const MlpDev &M, const float *raw, uint32_t n, float *out, cudaStream_t st)
+cudaError_t mlp_infer(const MlpDev &M, const float *raw, uint32_t n, float *out, cudaStream_t st,
+                      const uint32_t *n_dev)
 {
     if (n == 0) return cudaSuccess;
     const size_t smem = kFwdElems * sizeof(__nv_bfloat16);
@@ -464,7 +466,7 @@ cudaError_t mlp_infer(const MlpDev &M, const float *raw, uint32_t n, float *out,
         cudaFuncSetAttribute(k_mlp_fwd<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         attr = true;
     }
-    k_mlp_fwd<false><<<grid_for(n, num_sms()), 128, smem, st>>>(M, raw, n, out);
+    k_mlp_fwd<false><<<grid_for(n, num_sms()), 128, smem, st>>>(M, raw, n, out, n_dev);
     return cudaGetLastError();
 }
 
@@ -487,7 +489,7 @@ cudaError_t mlp_grads(const MlpDev &M, const float *raw, const float *target, ui
         attr = true;
     }
     const uint32_t grid = grid_for(n, num_sms());
-    k_mlp_fwd<true><<<grid, 128, smem_f, st>>>(M, raw, n, nullptr);
+    k_mlp_fwd<true><<<grid, 128, smem_f, st>>>(M, raw, n, nullptr, nullptr);
     k_mlp_bwd<<<grid, 128, smem_b, st>>>(M, raw, target, n);
     const uint32_t chunks = (n_pad + kDwChunk - 1) / kDwChunk;
     for (int l = 0; l < kMlpLayers; l++) {

@@ -60,7 +60,9 @@ struct MlpDev {
 // Host entry points (mlp.cu). All enqueue on `st`.
 cudaError_t mlp_init(const MlpDev &M, uint32_t seed, cudaStream_t st);
 cudaError_t mlp_refresh_copies(const MlpDev &M, cudaStream_t st);
-cudaError_t mlp_infer(const MlpDev &M, const float *raw, uint32_t n, float *out, cudaStream_t st);
+// n_dev (optional): a device word holding the actual row count (<= n).
+cudaError_t mlp_infer(const MlpDev &M, const float *raw, uint32_t n, float *out, cudaStream_t st,
+                      const uint32_t *n_dev = nullptr);
 // Forward + loss + backward + weight gradients into M.grad (zeroed first).
 cudaError_t mlp_grads(const MlpDev &M, const float *raw, const float *target, uint32_t n, cudaStream_t st);
 cudaError_t mlp_adam(const MlpDev &M, uint32_t step, float lr, cudaStream_t st);

@@ -23,6 +23,7 @@
 #include "bvh8.cuh"
 #include "render.cuh"
 #include "trace.cuh"
+#include "mlp.cuh"
 
 #include <cfloat>
 
@@ -119,6 +120,45 @@ __global__ void k_camera(RenderDev R, uint32_t n_paths, uint64_t sample0)
     R.q_d[0][p] = make_float4(d.x, d.y, d.z, FLT_MAX);
     R.q_path[0][p] = p;
     R.beta[p] = make_float4(1.f, 1.f, 1.f, 0.f);
+    if (R.cache_depth) {
+        uint32_t slot = 0xffffffffu;
+        if (mix64(key ^ 0x5851F42D4C957F2Dull) % R.train_every == 0) {
+            const uint32_t s = atomicAdd(R.train_count, 1u);
+            if (s < R.train_cap) slot = s;
+        }
+        R.train_slot[p] = slot;
+    }
+}
+
+// Adds contribution c, found at vertex `vert` of a training path, to the
+// targets of that path's recorded vertices 1..vert (each in units of the
+// radiance leaving its own vertex: divided by the throughput there).
+__device__ __forceinline__ void credit(const RenderDev &R, uint32_t slot, uint32_t vert, float3 c)
+{
+    const uint32_t stride = R.max_depth + 1;
+    for (uint32_t k = 1; k <= vert && k <= R.max_depth; k++) {
+        const uint32_t ri = R.rec_of[slot * stride + k];
+        if (ri == 0xffffffffu || ri >= R.rec_cap) continue;
+        const float4 b = R.rec_beta[ri];
+        atomicAdd(&R.rec_tgt[3 * ri], c.x / fmaxf(b.x, 1e-8f));
+        atomicAdd(&R.rec_tgt[3 * ri + 1], c.y / fmaxf(b.y, 1e-8f));
+        atomicAdd(&R.rec_tgt[3 * ri + 2], c.z / fmaxf(b.z, 1e-8f));
+    }
+}
+
+__device__ __forceinline__ void write_features(float *f, const RenderDev &R, float3 p, float3 wo, float3 n,
+                                               const Mat &m)
+{
+    f[0] = (p.x - R.scene_lo.x) * R.scene_inv_ext.x;
+    f[1] = (p.y - R.scene_lo.y) * R.scene_inv_ext.y;
+    f[2] = (p.z - R.scene_lo.z) * R.scene_inv_ext.z;
+    f[3] = wo.x; f[4] = wo.y; f[5] = wo.z;
+    f[6] = n.x; f[7] = n.y; f[8] = n.z;
+    const bool ggx = m.kind == 1u;
+    f[9] = ggx ? m.alpha : 1.f;
+    const float3 a = ggx ? m.f0 : m.albedo;
+    f[10] = a.x; f[11] = a.y; f[12] = a.z;
+    f[13] = f[14] = f[15] = 0.f;
 }
 
 __global__ void __launch_bounds__(128) k_extend(RenderDev R, int cur)
@@ -209,9 +249,14 @@ __global__ void __launch_bounds__(128) k_shade(RenderDev R, int cur, uint32_t de
     float3 sc[kMaxLights];
     uint32_t n_sh = 0;
     uint32_t pixel = 0;
+    bool query = false;           // rendering path stopping into the cache here
+    float4 qb = make_float4(0.f, 0.f, 0.f, 0.f);
+    float qf[kMlpRaw];
+    uint32_t tslot = 0xffffffffu;  // training slot of this path
 
     if (i < R.count[cur]) {
         path = R.q_path[cur][i];
+        if (R.cache_depth) tslot = R.train_slot[path];
         const float4 o = R.q_o[cur][i], d = R.q_d[cur][i];
         const int ti = R.hit_tri[i];
         pixel = path % R.wh;
@@ -223,6 +268,7 @@ __global__ void __launch_bounds__(128) k_shade(RenderDev R, int cur, uint32_t de
         if (ti < 0) {
             // escape: constant environment (zero for the reference's area-light scenes)
             add = beta * R.sky;
+            if (tslot != 0xffffffffu && depth >= 2 && !is_black(add)) credit(R, tslot, depth - 1, add);
         } else if (depth <= R.max_depth) {
             const uint32_t attr = R.tri_attr[ti];
             const uint32_t mat_id = attr & 0xffffu, light_id = attr >> 16;
@@ -244,7 +290,27 @@ __global__ void __launch_bounds__(128) k_shade(RenderDev R, int cur, uint32_t de
             if (depth == 0 && light_id != 0xffffu && light_id < R.n_lights && dot3(W, wo) > 0.f)
                 add = add + beta * R.lights[light_id].emit;
 
-            if (depth < R.max_depth) {
+            if (depth < R.max_depth && R.cache_depth && tslot == 0xffffffffu && depth == R.cache_depth) {
+                // a rendering path stops here: the cache supplies the radiance leaving this vertex
+                query = true;
+                write_features(qf, R, p, wo, W, m);
+                qb = make_float4(beta.x, beta.y, beta.z, __uint_as_float(pixel));
+            } else if (depth < R.max_depth) {
+                if (tslot != 0xffffffffu && depth >= 1) {
+                    // training record of this vertex; its target fills in as the tail is traced
+                    const uint32_t ri = atomicAdd(R.rec_count, 1u);
+                    uint32_t stored = 0xffffffffu;
+                    if (ri < R.rec_cap) {
+                        float f[kMlpRaw];
+                        write_features(f, R, p, wo, W, m);
+#pragma unroll
+                        for (int k = 0; k < kMlpRaw; k++) R.rec_feat[(size_t)ri * kMlpRaw + k] = f[k];
+                        R.rec_beta[ri] = make_float4(beta.x, beta.y, beta.z, 0.f);
+                        R.rec_tgt[3 * ri] = R.rec_tgt[3 * ri + 1] = R.rec_tgt[3 * ri + 2] = 0.f;
+                        stored = ri;
+                    }
+                    R.rec_of[tslot * (R.max_depth + 1) + depth] = stored;
+                }
                 // next-event estimation toward every light but the one hit
                 for (uint32_t l = 0; l < R.n_lights && l < kMaxLights; l++) {
                     if (l == light_id) continue;
@@ -329,12 +395,36 @@ __global__ void __launch_bounds__(128) k_shade(RenderDev R, int cur, uint32_t de
                 R.s_o[s] = so[k];
                 R.s_d[s] = sd[k];
                 R.s_c[s] = make_float4(sc[k].x, sc[k].y, sc[k].z, __uint_as_float(pixel));
+                if (R.cache_depth) R.s_meta[s] = tslot == 0xffffffffu ? 0xffffffffu : ((tslot << 8) | depth);
             } else {
                 atomicOr(R.err, 16u);
             }
         }
         if (!__any_sync(__activemask(), k + 1 < n_sh)) break;
     }
+    if (R.cache_depth) {
+        const uint32_t q = push_slot(query, R.qry_count);
+        if (query) {
+            if (q < R.capacity) {
+#pragma unroll
+                for (int k = 0; k < kMlpRaw; k++) R.qry_feat[(size_t)q * kMlpRaw + k] = qf[k];
+                R.qry_beta[q] = qb;
+            } else {
+                atomicOr(R.err, 32u);
+            }
+        }
+    }
+}
+
+// pixel += throughput * max(cache output, 0) for every cache query of the wave
+__global__ void k_cache_apply(RenderDev R)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= *R.qry_count || i >= R.capacity) return;
+    const float4 b = R.qry_beta[i];
+    const float3 y = make_float3(fmaxf(R.qry_out[3 * i], 0.f), fmaxf(R.qry_out[3 * i + 1], 0.f),
+                                 fmaxf(R.qry_out[3 * i + 2], 0.f));
+    add_pixel(R.accum, __float_as_uint(b.w), make_float3(b.x * y.x, b.y * y.y, b.z * y.z));
 }
 
 __global__ void __launch_bounds__(128) k_shadow(RenderDev R)
@@ -349,6 +439,10 @@ __global__ void __launch_bounds__(128) k_shadow(RenderDev R)
     if (best == -1) {
         const float4 c = R.s_c[i];
         add_pixel(R.accum, __float_as_uint(c.w), make_float3(c.x, c.y, c.z));
+        if (R.cache_depth) {
+            const uint32_t meta = R.s_meta[i];
+            if (meta != 0xffffffffu) credit(R, meta >> 8, meta & 0xffu, make_float3(c.x, c.y, c.z));
+        }
     }
 }
 
@@ -395,11 +489,18 @@ cudaError_t build_tri_attr(const uint32_t *prim_of, uint32_t n_tris, const uint3
 }
 
 cudaError_t render_wave(const RenderDev &R, uint32_t n_paths, uint64_t sample0, cudaStream_t st,
-                        uint32_t *launches)
+                        uint32_t *launches, const MlpDev *cache)
 {
     const uint32_t T = 128;
     cudaError_t e;
     if ((e = cudaMemsetAsync(R.count, 0, 2 * sizeof(uint32_t), st)) != cudaSuccess) return e;
+    if (R.cache_depth) {
+        if ((e = cudaMemsetAsync(R.train_count, 0, sizeof(uint32_t), st)) != cudaSuccess) return e;
+        if ((e = cudaMemsetAsync(R.qry_count, 0, sizeof(uint32_t), st)) != cudaSuccess) return e;
+        if ((e = cudaMemsetAsync(R.rec_of, 0xff, sizeof(uint32_t) * R.train_cap * (R.max_depth + 1), st)) !=
+            cudaSuccess)
+            return e;
+    }
     k_camera<<<blocks_for(n_paths, T), T, 0, st>>>(R, n_paths, sample0);
     if ((e = cudaMemcpyAsync(R.count, &n_paths, sizeof(uint32_t), cudaMemcpyHostToDevice, st)) != cudaSuccess) return e;
     uint32_t n_launch = 1;
@@ -410,6 +511,11 @@ cudaError_t render_wave(const RenderDev &R, uint32_t n_paths, uint64_t sample0, 
         k_extend<<<blocks_for(n_paths, T), T, 0, st>>>(R, cur);
         k_shade<<<blocks_for(n_paths, T), T, 0, st>>>(R, cur, depth, sample0);
         n_launch += 2;
+        if (R.cache_depth && depth == R.cache_depth && cache) {
+            if ((e = mlp_infer(*cache, R.qry_feat, n_paths, R.qry_out, st, R.qry_count)) != cudaSuccess) return e;
+            k_cache_apply<<<blocks_for(n_paths, T), T, 0, st>>>(R);
+            n_launch += 2;
+        }
         if (depth < R.max_depth) {
             k_shadow<<<blocks_for((uint64_t)n_paths * (R.n_lights ? R.n_lights : 1), T), T, 0, st>>>(R);
             n_launch++;

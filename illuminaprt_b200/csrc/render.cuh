@@ -58,13 +58,33 @@ struct RenderDev {
     uint32_t sh_capacity;
     float4 *accum;         // per pixel rgb sums
     uint32_t *err;
+
+    // radiance cache (cache_depth == 0: plain path tracing, none of this is used)
+    uint32_t cache_depth;      // rendering paths stop into the cache at this vertex
+    uint32_t train_every;      // one path in train_every is a training path
+    float3 scene_lo, scene_inv_ext;
+    uint32_t *train_slot;      // per path of the wave: training slot or ~0
+    uint32_t *train_count;     // training slots handed out in this wave
+    uint32_t train_cap;
+    uint32_t *rec_of;          // train_cap x (max_depth + 1): record of (slot, vertex) or ~0
+    float *rec_feat;           // rec_cap x 16 raw features
+    float4 *rec_beta;          // throughput at the recorded vertex
+    float *rec_tgt;            // rec_cap x 3: radiance leaving the vertex, summed over the path's tail
+    uint32_t *rec_count;
+    uint32_t rec_cap;
+    float *qry_feat;           // cache queries of rendering paths: cap x 16
+    float4 *qry_beta;          // throughput (w = pixel bits)
+    float *qry_out;            // cap x 3 network outputs
+    uint32_t *qry_count;
+    uint32_t *s_meta;          // per shadow segment: (slot << 8 | vertex) of a training path, or ~0
 };
 
 cudaError_t build_tri_attr(const uint32_t *prim_of, uint32_t n_tris, const uint32_t *mat_ids,
                            const uint32_t *light_first_tri, uint32_t n_lights, uint32_t *light_of_prim,
                            uint32_t *attr, cudaStream_t st);
+struct MlpDev;
 cudaError_t render_wave(const RenderDev &R, uint32_t n_paths, uint64_t sample0, cudaStream_t st,
-                        uint32_t *launches);
+                        uint32_t *launches, const MlpDev *cache);
 cudaError_t render_resolve(const float4 *accum, uint32_t wh, float scale, float *out, cudaStream_t st);
 
 }  // namespace ilg

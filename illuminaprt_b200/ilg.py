@@ -72,7 +72,9 @@ class ilg_camera(ctypes.Structure):
 class ilg_render_opts(ctypes.Structure):
     _fields_ = [("width", ctypes.c_uint32), ("height", ctypes.c_uint32), ("spp", ctypes.c_uint32),
                 ("max_depth", ctypes.c_uint32), ("epsilon", ctypes.c_float), ("seed", ctypes.c_uint32),
-                ("paths_per_wave", ctypes.c_uint32), ("sky", ctypes.c_float * 3), ("reserved", ctypes.c_uint32 * 6)]
+                ("paths_per_wave", ctypes.c_uint32), ("sky", ctypes.c_float * 3), ("cache_depth", ctypes.c_uint32),
+                ("train_every", ctypes.c_uint32), ("train_steps", ctypes.c_uint32), ("train_batch", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32 * 2)]
 
 
 _lib = None
@@ -236,8 +238,10 @@ class GpuSpace:
         self._check(self.L.ilg_set_quad_lights(self.h, ctypes.addressof(arr), len(lights)))
 
     def render(self, camera: dict, width: int, height: int, spp: int, max_depth: int = 6, epsilon: float = 1e-4,
-               seed: int = 1, sky=(0.0, 0.0, 0.0), paths_per_wave: int = 0, out=None):
-        """Returns (height, width, 3) float32 (or fills `out`, a CUDA tensor, in place)."""
+               seed: int = 1, sky=(0.0, 0.0, 0.0), paths_per_wave: int = 0, out=None, cache_depth: int = 0,
+               train_every: int = 16, train_steps: int = 4, train_batch: int = 16384):
+        """Returns (height, width, 3) float32 (or fills `out`, a CUDA tensor, in place).
+        cache_depth > 0 renders with the radiance cache (mlp_init first) and trains it afterwards."""
         cam = ilg_camera()
         cam.eye[:] = list(camera["eye"])
         cam.target[:] = list(camera["target"])
@@ -245,7 +249,8 @@ class GpuSpace:
         cam.fov_deg = float(camera["fov"])
         cam.aspect = float(camera.get("aspect", width / height))
         o = ilg_render_opts(width=width, height=height, spp=spp, max_depth=max_depth, epsilon=epsilon, seed=seed,
-                            paths_per_wave=paths_per_wave)
+                            paths_per_wave=paths_per_wave, cache_depth=cache_depth, train_every=train_every,
+                            train_steps=train_steps, train_batch=train_batch)
         o.sky[:] = list(sky)
         if out is not None:
             self._check(self.L.ilg_render(self.h, ctypes.byref(cam), ctypes.byref(o), _ptr(out), ILG_DEVICE_PTRS))

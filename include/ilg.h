@@ -152,7 +152,15 @@ typedef struct ilg_render_opts {
     uint32_t seed;           /* sample-sequence seed */
     uint32_t paths_per_wave; /* wavefront size; 0 = automatic */
     float sky[3];            /* constant environment radiance; 0 = none */
-    uint32_t reserved[6];
+    /* radiance cache (needs ilg_mlp_init): 0 = plain path tracing; k >= 1 =
+     * rendering paths stop into the cache at their k-th bounce vertex, one
+     * path in train_every is traced to full depth and its vertices train the
+     * cache after the call (train_steps Adam steps of train_batch records) */
+    uint32_t cache_depth;
+    uint32_t train_every;    /* 0 = 16 */
+    uint32_t train_steps;    /* 0 = 4 */
+    uint32_t train_batch;    /* 0 = 16384 */
+    uint32_t reserved[2];
 } ilg_render_opts;
 
 /* Materials indexed by the mat_ids given to ilg_set_mesh. */

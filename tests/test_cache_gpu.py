@@ -1,0 +1,61 @@
+"""The radiance-cached path tracer: online training on the path tracer's own
+tails, and its error at equal wall time against plain path tracing."""
+import numpy as np
+import pytest
+
+from illuminaprt_b200 import scenes
+from illuminaprt_b200.cache_experiment import equal_time, rel_mse
+
+pytestmark = pytest.mark.gpu
+
+W, H = 192, 108
+
+
+@pytest.fixture(scope="module")
+def field():
+    from illuminaprt_b200.ilg import GpuSpace
+    s = scenes.sphere_field(4, 4, seed=5, width=W, height=H)
+    sp = GpuSpace()
+    scenes.load_sphere_field(sp, s)
+    gt = sp.render(dict(s["camera"], aspect=W / H), W, H, 16384, max_depth=12, seed=424242, sky=s["sky"])
+    return sp, s, gt
+
+
+def test_plain_render_unchanged_by_cache_support(field):
+    sp, s, _ = field
+    a = sp.render(s["camera"], 64, 36, 4, max_depth=12, seed=3, sky=s["sky"])
+    b = sp.render(s["camera"], 64, 36, 4, max_depth=12, seed=3, sky=s["sky"], cache_depth=0)
+    assert np.allclose(a, b, rtol=1e-5, atol=1e-6)
+
+
+def test_cache_trains_online(field):
+    sp, s, gt = field
+    sp.mlp_init(seed=1, lr=1e-2)
+    cam = dict(s["camera"], aspect=W / H)
+    errs = []
+    for f in range(40):
+        img = sp.render(cam, W, H, 1, max_depth=12, seed=1000 + f, sky=s["sky"], cache_depth=1)
+        assert np.isfinite(img).all()
+        # how well does the cache alone (no noise averaging) match the truth?
+        if f in (0, 39):
+            errs.append(rel_mse(sp.render(cam, W, H, 64, max_depth=12, seed=77 + f, sky=s["sky"], cache_depth=1,
+                                          train_steps=0), gt))
+    print(f"cached 64-spp relMSE before / after 40 training frames: {errs[0]:.4f} / {errs[1]:.4f}")
+    assert errs[1] < errs[0]
+
+
+def test_equal_time_gain_over_plain(field):
+    sp, s, gt = field
+    r = equal_time(sp, s, W, H, gt, frames=96, warmup=16, cache_depth=1)
+    print({k: v for k, v in r.items() if not k.endswith("image")})
+    assert r["relmse_cached"] < r["relmse_plain"]
+    assert max(abs(b) for b in r["bias_cached"]) < 0.1
+
+
+def test_training_is_what_helps(field):
+    """Ablation: the same cached renderer with a network that never trains."""
+    sp, s, gt = field
+    trained = equal_time(sp, s, W, H, gt, frames=48, warmup=16, cache_depth=1)
+    frozen = equal_time(sp, s, W, H, gt, frames=48, warmup=16, cache_depth=1, ablate_training=True)
+    print(f"relMSE trained {trained['relmse_cached']:.5f} vs untrained {frozen['relmse_cached']:.5f}")
+    assert trained["relmse_cached"] < frozen["relmse_cached"] / 2
