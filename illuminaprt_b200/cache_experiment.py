@@ -40,8 +40,8 @@ def equal_time(space, scene, width, height, gt, frames=64, warmup=8, spp_per_fra
     t0 = time.perf_counter()
     for f in range(frames):
         img = space.render(cam, width, height, spp_per_frame, seed=seed + f, cache_depth=cache_depth,
-                           train_every=train_every, train_steps=1 if ablate_training else train_steps,
-                           train_batch=1 if ablate_training else train_batch, **kw)
+                           train_every=train_every, train_steps=0 if ablate_training else train_steps,
+                           train_batch=train_batch, **kw)
         if f >= warmup:
             acc += img
             n_acc += 1

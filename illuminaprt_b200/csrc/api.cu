@@ -408,12 +408,12 @@ int ilg_render(ilg_ctx *ctx, const ilg_camera *cam, const ilg_render_opts *opts,
     R.accum = ctx->accum.ptr; R.err = ctx->derr.ptr;
 
     const uint32_t train_every = opts->train_every ? opts->train_every : 16u;
-    const uint32_t train_steps = opts->train_steps ? opts->train_steps : 4u;
+    const uint32_t train_steps = opts->train_steps;
     const uint32_t train_batch = opts->train_batch ? opts->train_batch : 16384u;
     MlpDev mlp = {};
     if (cache_depth) {
         const uint32_t train_cap = cap / train_every * 2u + 1024u;
-        const uint32_t rec_cap = train_steps * train_batch;
+        const uint32_t rec_cap = std::max<uint32_t>(1u, train_steps) * train_batch;
         CK(ctx->counts.reserve(8));
         CK(ctx->train_slot.reserve(cap));
         CK(ctx->rec_of.reserve((size_t)train_cap * (opts->max_depth + 1)));

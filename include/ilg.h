@@ -158,7 +158,7 @@ typedef struct ilg_render_opts {
      * cache after the call (train_steps Adam steps of train_batch records) */
     uint32_t cache_depth;
     uint32_t train_every;    /* 0 = 16 */
-    uint32_t train_steps;    /* 0 = 4 */
+    uint32_t train_steps;    /* Adam steps after the call; 0 = none (the cache stays frozen) */
     uint32_t train_batch;    /* 0 = 16384 */
     uint32_t reserved[2];
 } ilg_render_opts;
