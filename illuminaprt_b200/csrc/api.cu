@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <cstring>
 #include <new>
+#include <vector>
 
 #include "build.cuh"
 #include "trace_api.cuh"
@@ -35,6 +36,14 @@ int fail(ilg_ctx *c, int code, const char *fmt, ...)
         cudaError_t e_ = (call);                                                                     \
         if (e_ != cudaSuccess)                                                                       \
             return fail(ctx, e_ == cudaErrorMemoryAllocation ? ILG_ENOMEM : ILG_ECUDA, "%s: %s", #call, \
+                        cudaGetErrorString(e_));                                                     \
+    } while (0)
+
+#define CK2(c, call)                                                                                 \
+    do {                                                                                             \
+        cudaError_t e_ = (call);                                                                     \
+        if (e_ != cudaSuccess)                                                                       \
+            return fail(c, e_ == cudaErrorMemoryAllocation ? ILG_ENOMEM : ILG_ECUDA, "%s: %s", #call,   \
                         cudaGetErrorString(e_));                                                     \
     } while (0)
 
@@ -330,51 +339,32 @@ int ilg_set_quad_lights(ilg_ctx *ctx, const ilg_quad_light *lights, uint32_t n)
     return ILG_OK;
 }
 
-int ilg_render(ilg_ctx *ctx, const ilg_camera *cam, const ilg_render_opts *opts, float *out_rgb, uint32_t flags)
+// Validates a scene context for rendering and fills its scene record
+// (camera frame as PerspectiveCamera(eye, normalize(target - eye), up,
+// -1,1,-1,1, 1) + SetFieldOfView builds it: Core/Camera/Camera.cpp:30-44,
+// Core/Geometry/Basis.cpp:28-44). Builds the per-triangle attributes on `st`.
+static int prepare_scene(ilg_ctx *runner, ilg_ctx *ctx, const ilg_camera *cam, uint32_t W, uint32_t H, uint32_t spp,
+                         uint32_t max_depth, float eps, uint32_t seed, const float sky[3], cudaStream_t st,
+                         SceneRec &S)
 {
-    if (!ctx) return ILG_EINVAL;
-    if (!cam || !opts || !out_rgb) return fail(ctx, ILG_EINVAL, "ilg_render: null argument");
-    if (flags & ~ILG_DEVICE_PTRS) return fail(ctx, ILG_EINVAL, "ilg_render: unknown flags 0x%x", flags);
-    if (!ctx->built) return fail(ctx, ILG_ESTATE, "ilg_render: scene not built");
-    if (!ctx->has_mat || ctx->n_mats == 0) return fail(ctx, ILG_ESTATE, "ilg_render: materials not set");
-    const uint32_t W = opts->width, H = opts->height;
-    if (W == 0 || H == 0 || opts->spp == 0 || (uint64_t)W * H > (1u << 26))
-        return fail(ctx, ILG_EINVAL, "ilg_render: bad image size %ux%u or spp %u", W, H, opts->spp);
-    if (opts->max_depth == 0 || opts->max_depth > 64) return fail(ctx, ILG_EINVAL, "ilg_render: max_depth must be 1..64");
-    const uint32_t cache_depth = opts->cache_depth;
-    if (cache_depth) {
-        if (!ctx->mlp_ready) return fail(ctx, ILG_ESTATE, "ilg_render: cache_depth set but ilg_mlp_init not called");
-        if (cache_depth >= opts->max_depth)
-            return fail(ctx, ILG_EINVAL, "ilg_render: cache_depth %u must be below max_depth %u", cache_depth, opts->max_depth);
-    }
+    if (!ctx || !cam) return fail(runner, ILG_EINVAL, "render: null scene or camera");
+    if (ctx->device != runner->device) return fail(runner, ILG_EINVAL, "render: scene on another device");
+    if (!ctx->built) return fail(runner, ILG_ESTATE, "ilg_render: scene not built");
+    if (!ctx->has_mat || ctx->n_mats == 0) return fail(runner, ILG_ESTATE, "ilg_render: materials not set");
+    if (W == 0 || H == 0 || spp == 0 || (uint64_t)W * H > (1u << 26))
+        return fail(runner, ILG_EINVAL, "ilg_render: bad image size %ux%u or spp %u", W, H, spp);
+    if (max_depth == 0 || max_depth > 64) return fail(runner, ILG_EINVAL, "ilg_render: max_depth must be 1..64");
     for (uint32_t l = 0; l < ctx->n_lights; l++)
         if ((uint64_t)ctx->light_first_host[l] + 1 >= ctx->n_tris)
-            return fail(ctx, ILG_EINVAL, "ilg_render: light %u triangles out of range of the mesh", l);
-    CK(cudaSetDevice(ctx->device));
-    cudaStream_t st = ctx->stream;
+            return fail(runner, ILG_EINVAL, "ilg_render: light %u triangles out of range of the mesh", l);
     const uint32_t n = ctx->n_tris;
     if (ctx->attr_dirty) {
-        CK(ctx->tri_attr.reserve(n));
-        CK(ctx->light_of_prim.reserve(n));
-        CK(build_tri_attr(ctx->bb.prim_of, n, ctx->mat.ptr, ctx->light_first_tri.ptr, ctx->n_lights,
-                          ctx->light_of_prim.ptr, ctx->tri_attr.ptr, st));
+        CK2(runner, ctx->tri_attr.reserve(n));
+        CK2(runner, ctx->light_of_prim.reserve(n));
+        CK2(runner, build_tri_attr(ctx->bb.prim_of, n, ctx->mat.ptr, ctx->light_first_tri.ptr, ctx->n_lights,
+                                   ctx->light_of_prim.ptr, ctx->tri_attr.ptr, st));
         ctx->attr_dirty = false;
     }
-    const uint32_t wh = W * H;
-    uint32_t cap = opts->paths_per_wave ? opts->paths_per_wave : (1u << 22);
-    uint32_t spp_per_wave = std::max<uint32_t>(1u, cap / wh);
-    spp_per_wave = std::min(spp_per_wave, opts->spp);
-    cap = wh * spp_per_wave;
-    const uint32_t nl = std::max<uint32_t>(1u, ctx->n_lights);
-    CK(ctx->q_o0.reserve(cap)); CK(ctx->q_d0.reserve(cap)); CK(ctx->q_o1.reserve(cap)); CK(ctx->q_d1.reserve(cap));
-    CK(ctx->q_p0.reserve(cap)); CK(ctx->q_p1.reserve(cap)); CK(ctx->beta.reserve(cap));
-    CK(ctx->hit_tri.reserve(cap)); CK(ctx->hit_t.reserve(cap));
-    CK(ctx->s_o.reserve((size_t)cap * nl)); CK(ctx->s_d.reserve((size_t)cap * nl)); CK(ctx->s_c.reserve((size_t)cap * nl));
-    CK(ctx->counts.reserve(4)); CK(ctx->accum.reserve(wh));
-    CK(cudaMemsetAsync(ctx->accum.ptr, 0, sizeof(float4) * wh, st));
-
-    // camera frame: PerspectiveCamera(eye, normalize(target - eye), up, -1,1,-1,1, 1)
-    // + SetFieldOfView (Core/Camera/Camera.cpp:30-44, Basis.cpp:28-44)
     V3 eye = v3(cam->eye);
     V3 w = normalize(normalize(v3(cam->target) - eye));
     V3 v = normalize(v3(cam->up));
@@ -387,18 +377,61 @@ int ilg_render(ilg_ctx *ctx, const ilg_camera *cam, const ilg_render_opts *opts,
     V3 u = cross(v, w);
     const float half = cam->fov_deg * (std::atan(1.0f) / 45.0f) * 0.5f;
     const float v1 = std::tan(half), v0 = -v1, u0 = v0 * cam->aspect, u1 = v1 * cam->aspect;
+    S = SceneRec{};
+    S.nodes = ctx->bb.nodes; S.tris = ctx->bb.tris; S.n_nodes = ctx->stats.n_nodes; S.n_tris = ctx->stats.n_tris;
+    S.tri_attr = ctx->tri_attr.ptr; S.mats = ctx->mats.ptr; S.n_mats = ctx->n_mats;
+    S.lights = ctx->lights.ptr; S.n_lights = ctx->n_lights;
+    S.sky = make_float3(sky[0], sky[1], sky[2]);
+    S.centre = f3(eye);
+    S.corner = f3(eye + u0 * u + v0 * v + 1.0f * w);
+    S.across = f3((u1 - u0) * u);
+    S.up = f3((v1 - v0) * v);
+    S.width = W; S.height = H; S.wh = W * H; S.rcp_w = 1.f / W; S.rcp_h = 1.f / H;
+    S.max_depth = max_depth; S.eps = eps; S.spp = spp; S.seed = seed;
+    return ILG_OK;
+}
+
+// Renders the scenes of `recs` (path ranges and pixel bases filled here) in
+// waves of at most `cap_req` paths on the runner's buffers and stream.
+static int run_render(ilg_ctx *ctx, std::vector<SceneRec> &recs, uint32_t cap_req, uint32_t block,
+                      uint32_t cache_depth, uint32_t train_every, uint32_t train_steps, uint32_t train_batch,
+                      uint64_t *total_paths_out)
+{
+    cudaStream_t st = ctx->stream;
+    uint64_t total = 0;
+    uint32_t pixels = 0, depth_max = 0, nl = 1;
+    for (auto &S : recs) {
+        S.path_begin = total;
+        S.pixel_base = pixels;
+        total += (uint64_t)S.wh * S.spp;
+        pixels += S.wh;
+        depth_max = std::max(depth_max, S.max_depth);
+        nl = std::max(nl, S.n_lights);
+    }
+    if (total_paths_out) *total_paths_out = total;
+    // wave size: whole samples for a single scene (so a wave never splits a pixel's sample)
+    uint32_t cap = cap_req ? cap_req : (1u << 22);
+    if (recs.size() == 1) {
+        const uint32_t wh = recs[0].wh;
+        uint32_t spw = std::max<uint32_t>(1u, cap / wh);
+        spw = std::min(spw, recs[0].spp);
+        cap = wh * spw;
+    } else {
+        cap = (uint32_t)std::min<uint64_t>(cap, total);
+    }
+    CK(ctx->q_o0.reserve(cap)); CK(ctx->q_d0.reserve(cap)); CK(ctx->q_o1.reserve(cap)); CK(ctx->q_d1.reserve(cap));
+    CK(ctx->q_p0.reserve(cap)); CK(ctx->q_p1.reserve(cap)); CK(ctx->beta.reserve(cap));
+    CK(ctx->hit_tri.reserve(cap)); CK(ctx->hit_t.reserve(cap)); CK(ctx->path_scene.reserve(cap));
+    CK(ctx->s_o.reserve((size_t)cap * nl)); CK(ctx->s_d.reserve((size_t)cap * nl)); CK(ctx->s_c.reserve((size_t)cap * nl));
+    CK(ctx->s_sid.reserve((size_t)cap * nl));
+    CK(ctx->counts.reserve(8)); CK(ctx->accum.reserve(pixels));
+    CK(ctx->scene_table.reserve(recs.size()));
+    CK(cudaMemcpyAsync(ctx->scene_table.ptr, recs.data(), recs.size() * sizeof(SceneRec), cudaMemcpyHostToDevice, st));
+    CK(cudaMemsetAsync(ctx->accum.ptr, 0, sizeof(float4) * pixels, st));
 
     RenderDev R = {};
-    R.nodes = ctx->bb.nodes; R.tris = ctx->bb.tris; R.n_nodes = ctx->stats.n_nodes; R.n_tris = ctx->stats.n_tris;
-    R.tri_attr = ctx->tri_attr.ptr; R.mats = ctx->mats.ptr; R.n_mats = ctx->n_mats;
-    R.lights = ctx->lights.ptr; R.n_lights = ctx->n_lights;
-    R.sky = make_float3(opts->sky[0], opts->sky[1], opts->sky[2]);
-    R.centre = f3(eye);
-    R.corner = f3(eye + u0 * u + v0 * v + 1.0f * w);
-    R.across = f3((u1 - u0) * u);
-    R.up = f3((v1 - v0) * v);
-    R.width = W; R.height = H; R.wh = wh; R.rcp_w = 1.f / W; R.rcp_h = 1.f / H;
-    R.max_depth = opts->max_depth; R.eps = opts->epsilon; R.seed = opts->seed;
+    R.scenes = ctx->scene_table.ptr; R.n_scenes = (uint32_t)recs.size(); R.depth_max = depth_max;
+    R.path_scene = ctx->path_scene.ptr; R.s_sid = ctx->s_sid.ptr;
     R.q_o[0] = ctx->q_o0.ptr; R.q_o[1] = ctx->q_o1.ptr; R.q_d[0] = ctx->q_d0.ptr; R.q_d[1] = ctx->q_d1.ptr;
     R.q_path[0] = ctx->q_p0.ptr; R.q_path[1] = ctx->q_p1.ptr;
     R.count = ctx->counts.ptr; R.capacity = cap;
@@ -407,16 +440,12 @@ int ilg_render(ilg_ctx *ctx, const ilg_camera *cam, const ilg_render_opts *opts,
     R.sh_count = ctx->counts.ptr + 2; R.sh_capacity = cap * nl;
     R.accum = ctx->accum.ptr; R.err = ctx->derr.ptr;
 
-    const uint32_t train_every = opts->train_every ? opts->train_every : 16u;
-    const uint32_t train_steps = opts->train_steps;
-    const uint32_t train_batch = opts->train_batch ? opts->train_batch : 16384u;
     MlpDev mlp = {};
     if (cache_depth) {
         const uint32_t train_cap = cap / train_every * 2u + 1024u;
         const uint32_t rec_cap = std::max<uint32_t>(1u, train_steps) * train_batch;
-        CK(ctx->counts.reserve(8));
         CK(ctx->train_slot.reserve(cap));
-        CK(ctx->rec_of.reserve((size_t)train_cap * (opts->max_depth + 1)));
+        CK(ctx->rec_of.reserve((size_t)train_cap * (depth_max + 1)));
         CK(ctx->s_meta.reserve((size_t)cap * nl));
         CK(ctx->rec_feat.reserve((size_t)rec_cap * kMlpRaw));
         CK(ctx->rec_tgt.reserve((size_t)rec_cap * 3));
@@ -453,9 +482,9 @@ int ilg_render(ilg_ctx *ctx, const ilg_camera *cam, const ilg_render_opts *opts,
     }
 
     uint32_t launches = 0;
-    for (uint32_t s0 = 0; s0 < opts->spp; s0 += spp_per_wave) {
-        const uint32_t k = std::min(spp_per_wave, opts->spp - s0);
-        CK(render_wave(R, wh * k, s0, st, &launches, cache_depth ? &mlp : nullptr));
+    for (uint64_t g0 = 0; g0 < total; g0 += cap) {
+        const uint32_t k = (uint32_t)std::min<uint64_t>(cap, total - g0);
+        CK(render_wave(R, k, g0, st, &launches, cache_depth ? &mlp : nullptr, block));
     }
     if (cache_depth) {
         // online training on this call's records (the next call renders with the update)
@@ -473,18 +502,79 @@ int ilg_render(ilg_ctx *ctx, const ilg_camera *cam, const ilg_render_opts *opts,
             launches += 9;
         }
     }
+    ctx->last_render_launches = launches;
+    return ILG_OK;
+}
+
+int ilg_render(ilg_ctx *ctx, const ilg_camera *cam, const ilg_render_opts *opts, float *out_rgb, uint32_t flags)
+{
+    if (!ctx) return ILG_EINVAL;
+    if (!cam || !opts || !out_rgb) return fail(ctx, ILG_EINVAL, "ilg_render: null argument");
+    if (flags & ~ILG_DEVICE_PTRS) return fail(ctx, ILG_EINVAL, "ilg_render: unknown flags 0x%x", flags);
+    const uint32_t cache_depth = opts->cache_depth;
+    if (cache_depth) {
+        if (!ctx->mlp_ready) return fail(ctx, ILG_ESTATE, "ilg_render: cache_depth set but ilg_mlp_init not called");
+        if (cache_depth >= opts->max_depth)
+            return fail(ctx, ILG_EINVAL, "ilg_render: cache_depth %u must be below max_depth %u", cache_depth, opts->max_depth);
+    }
+    CK(cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    std::vector<SceneRec> recs(1);
+    int rc = prepare_scene(ctx, ctx, cam, opts->width, opts->height, opts->spp, opts->max_depth, opts->epsilon,
+                           opts->seed, opts->sky, st, recs[0]);
+    if (rc) return rc;
+    const uint32_t wh = opts->width * opts->height;
+    rc = run_render(ctx, recs, opts->paths_per_wave, 128, cache_depth, opts->train_every ? opts->train_every : 16u,
+                    opts->train_steps, opts->train_batch ? opts->train_batch : 16384u, nullptr);
+    if (rc) return rc;
     float *out_dev = out_rgb;
     if (!(flags & ILG_DEVICE_PTRS)) {
         CK(ctx->out_dev.reserve(3ull * wh));
         out_dev = ctx->out_dev.ptr;
     }
     CK(render_resolve(ctx->accum.ptr, wh, 1.f / opts->spp, out_dev, st));
-    ctx->last_render_launches = launches + 1;
+    ctx->last_render_launches += 1;
     if (!(flags & ILG_DEVICE_PTRS)) {
         CK(cudaMemcpyAsync(out_rgb, out_dev, 12ull * wh, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         return ctx->check_device_error();
     }
+    return ILG_OK;
+}
+
+int ilg_render_batch(ilg_ctx *runner, const ilg_batch_item *items, uint32_t n, uint32_t paths_per_wave,
+                     uint32_t block, uint32_t flags)
+{
+    if (!runner) return ILG_EINVAL;
+    if (!items || n == 0 || n > 4096) return fail(runner, ILG_EINVAL, "ilg_render_batch: need 1..4096 items");
+    if (flags & ~ILG_DEVICE_PTRS) return fail(runner, ILG_EINVAL, "ilg_render_batch: unknown flags 0x%x", flags);
+    if (block != 0 && block != 64 && block != 128 && block != 256)
+        return fail(runner, ILG_EINVAL, "ilg_render_batch: block must be 64, 128 or 256");
+    CK2(runner, cudaSetDevice(runner->device));
+    cudaStream_t st = runner->stream;
+    std::vector<SceneRec> recs(n);
+    for (uint32_t i = 0; i < n; i++) {
+        const ilg_batch_item &it = items[i];
+        if (!it.out_rgb) return fail(runner, ILG_EINVAL, "ilg_render_batch: item %u has no output", i);
+        int rc = prepare_scene(runner, it.scene, &it.camera, it.width, it.height, it.spp, it.max_depth, it.epsilon,
+                               it.seed, it.sky, st, recs[i]);
+        if (rc) return rc;
+    }
+    int rc = run_render(runner, recs, paths_per_wave, block ? block : 128, 0, 16, 0, 16384, nullptr);
+    if (rc) return rc;
+    uint32_t max_wh = 0;
+    for (auto &S : recs) max_wh = std::max(max_wh, S.wh);
+    if (!(flags & ILG_DEVICE_PTRS)) CK2(runner, runner->out_dev.reserve(3ull * max_wh));
+    for (uint32_t i = 0; i < n; i++) {
+        const SceneRec &S = recs[i];
+        float *dst = (flags & ILG_DEVICE_PTRS) ? items[i].out_rgb : runner->out_dev.ptr;
+        CK2(runner, render_resolve(runner->accum.ptr + S.pixel_base, S.wh, 1.f / S.spp, dst, st));
+        if (!(flags & ILG_DEVICE_PTRS))
+            CK2(runner, cudaMemcpyAsync(items[i].out_rgb, dst, 12ull * S.wh, cudaMemcpyDeviceToHost, st));
+        if (!(flags & ILG_DEVICE_PTRS)) CK2(runner, cudaStreamSynchronize(st));  // runner->out_dev is reused per item
+    }
+    runner->last_render_launches += n;
+    if (!(flags & ILG_DEVICE_PTRS)) return runner->check_device_error();
     return ILG_OK;
 }
 

@@ -103,22 +103,46 @@ __device__ __forceinline__ void add_pixel(float4 *accum, uint32_t pixel, float3 
     atomicAdd(a + 2, c.z);
 }
 
-__global__ void k_camera(RenderDev R, uint32_t n_paths, uint64_t sample0)
+// scene of a global path index (the scenes' path ranges are consecutive)
+__device__ __forceinline__ uint32_t scene_of(const RenderDev &R, uint64_t g)
+{
+    uint32_t lo = 0, hi = R.n_scenes;
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (R.scenes[mid].path_begin <= g) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+// path identity inside its scene: (pixel, sample-sequence key)
+__device__ __forceinline__ void path_ident(const SceneRec &S, uint64_t g, uint32_t &pixel, uint64_t &key)
+{
+    const uint64_t local = g - S.path_begin;
+    pixel = (uint32_t)(local % S.wh);
+    key = path_key(S.seed, local);
+}
+
+__global__ void k_camera(RenderDev R, uint32_t n_paths, uint64_t wave_begin)
 {
     const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= n_paths) return;
-    const uint32_t pixel = p % R.wh;
-    const uint64_t sample = sample0 + p / R.wh;
-    const uint32_t x = pixel % R.width, y = pixel / R.width;
-    const uint64_t key = path_key(R.seed, sample * R.wh + pixel);
+    const uint64_t g = wave_begin + p;
+    const uint32_t sid = scene_of(R, g);
+    const SceneRec &S = R.scenes[sid];
+    uint32_t pixel;
+    uint64_t key;
+    path_ident(S, g, pixel, key);
+    const uint32_t x = pixel % S.width, y = pixel / S.width;
     // BoxFilter shifts the [0,1) sample by -0.5 (Core/Filter/BoxFilter.cpp:20-28)
     const float xi1 = rnd(key, kDimCam) - 0.5f, xi2 = rnd(key, kDimCam + 1) - 0.5f;
-    const float fx = x * R.rcp_w + xi1 * R.rcp_w, fy = y * R.rcp_h + xi2 * R.rcp_h;
-    const float3 target = R.corner + R.across * fx + R.up * fy;
-    const float3 d = normalize3(target - R.centre);
-    R.q_o[0][p] = make_float4(R.centre.x, R.centre.y, R.centre.z, 0.f);
+    const float fx = x * S.rcp_w + xi1 * S.rcp_w, fy = y * S.rcp_h + xi2 * S.rcp_h;
+    const float3 target = S.corner + S.across * fx + S.up * fy;
+    const float3 d = normalize3(target - S.centre);
+    R.q_o[0][p] = make_float4(S.centre.x, S.centre.y, S.centre.z, 0.f);
     R.q_d[0][p] = make_float4(d.x, d.y, d.z, FLT_MAX);
     R.q_path[0][p] = p;
+    R.path_scene[p] = sid;
     R.beta[p] = make_float4(1.f, 1.f, 1.f, 0.f);
     if (R.cache_depth) {
         uint32_t slot = 0xffffffffu;
@@ -135,8 +159,8 @@ __global__ void k_camera(RenderDev R, uint32_t n_paths, uint64_t sample0)
 // radiance leaving its own vertex: divided by the throughput there).
 __device__ __forceinline__ void credit(const RenderDev &R, uint32_t slot, uint32_t vert, float3 c)
 {
-    const uint32_t stride = R.max_depth + 1;
-    for (uint32_t k = 1; k <= vert && k <= R.max_depth; k++) {
+    const uint32_t stride = R.depth_max + 1;
+    for (uint32_t k = 1; k <= vert && k <= R.depth_max; k++) {
         const uint32_t ri = R.rec_of[slot * stride + k];
         if (ri == 0xffffffffu || ri >= R.rec_cap) continue;
         const float4 b = R.rec_beta[ri];
@@ -161,15 +185,16 @@ __device__ __forceinline__ void write_features(float *f, const RenderDev &R, flo
     f[13] = f[14] = f[15] = 0.f;
 }
 
-__global__ void __launch_bounds__(128) k_extend(RenderDev R, int cur)
+__global__ void __launch_bounds__(256) k_extend(RenderDev R, int cur)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= R.count[cur]) return;
     const float4 o = R.q_o[cur][i], d = R.q_d[cur][i];
+    const SceneRec &S = R.scenes[R.path_scene[R.q_path[cur][i]]];
     int best;
     float bt, bu, bv;
     unsigned long long nn = 0, nt = 0;
-    trace_one<false, false>(R.nodes, R.tris, R.n_nodes, R.n_tris, o, d, best, bt, bu, bv, R.err, nn, nt);
+    trace_one<false, false>(S.nodes, S.tris, S.n_nodes, S.n_tris, o, d, best, bt, bu, bv, R.err, nn, nt);
     R.hit_tri[i] = best;
     R.hit_t[i] = bt;
 }
@@ -237,7 +262,7 @@ __device__ __forceinline__ float3 bsdf_f(const Mat &m, float3 wo, float3 wi)
     return make_float3(0.f, 0.f, 0.f);
 }
 
-__global__ void __launch_bounds__(128) k_shade(RenderDev R, int cur, uint32_t depth, uint64_t sample0)
+__global__ void __launch_bounds__(256) k_shade(RenderDev R, int cur, uint32_t depth, uint64_t wave_begin)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     const int nxt = cur ^ 1;
@@ -253,27 +278,32 @@ __global__ void __launch_bounds__(128) k_shade(RenderDev R, int cur, uint32_t de
     float4 qb = make_float4(0.f, 0.f, 0.f, 0.f);
     float qf[kMlpRaw];
     uint32_t tslot = 0xffffffffu;  // training slot of this path
+    uint32_t sid = 0;
+    float eps = 0.f;
 
     if (i < R.count[cur]) {
         path = R.q_path[cur][i];
         if (R.cache_depth) tslot = R.train_slot[path];
+        sid = R.path_scene[path];
+        const SceneRec &S = R.scenes[sid];
+        eps = S.eps;
         const float4 o = R.q_o[cur][i], d = R.q_d[cur][i];
         const int ti = R.hit_tri[i];
-        pixel = path % R.wh;
-        const uint64_t sample = sample0 + path / R.wh;
-        const uint64_t key = path_key(R.seed, sample * R.wh + pixel);
+        uint64_t key;
+        path_ident(S, wave_begin + path, pixel, key);
+        pixel += S.pixel_base;
         float3 beta = make_float3(R.beta[path].x, R.beta[path].y, R.beta[path].z);
         float3 add = make_float3(0.f, 0.f, 0.f);
 
         if (ti < 0) {
             // escape: constant environment (zero for the reference's area-light scenes)
-            add = beta * R.sky;
+            add = beta * S.sky;
             if (tslot != 0xffffffffu && depth >= 2 && !is_black(add)) credit(R, tslot, depth - 1, add);
-        } else if (depth <= R.max_depth) {
-            const uint32_t attr = R.tri_attr[ti];
+        } else if (depth <= S.max_depth) {
+            const uint32_t attr = S.tri_attr[ti];
             const uint32_t mat_id = attr & 0xffffu, light_id = attr >> 16;
-            const Mat m = R.mats[mat_id < R.n_mats ? mat_id : 0];
-            const Tri tr = R.tris[ti];
+            const Mat m = S.mats[mat_id < S.n_mats ? mat_id : 0];
+            const Tri tr = S.tris[ti];
             const float3 ng = normalize3(make_float3(tr.a.w, tr.b.w, tr.c.w));
             const float t = R.hit_t[i];
             const float3 dd = make_float3(d.x, d.y, d.z);
@@ -287,15 +317,15 @@ __global__ void __launch_bounds__(128) k_shade(RenderDev R, int cur, uint32_t de
 
             // emission only at depth 0 (no specular lobes here), one-sided
             // (DiffuseAreaLight::Radiance, DiffuseAreaLight.cpp:47-50)
-            if (depth == 0 && light_id != 0xffffu && light_id < R.n_lights && dot3(W, wo) > 0.f)
-                add = add + beta * R.lights[light_id].emit;
+            if (depth == 0 && light_id != 0xffffu && light_id < S.n_lights && dot3(W, wo) > 0.f)
+                add = add + beta * S.lights[light_id].emit;
 
-            if (depth < R.max_depth && R.cache_depth && tslot == 0xffffffffu && depth == R.cache_depth) {
+            if (depth < S.max_depth && R.cache_depth && tslot == 0xffffffffu && depth == R.cache_depth) {
                 // a rendering path stops here: the cache supplies the radiance leaving this vertex
                 query = true;
                 write_features(qf, R, p, wo, W, m);
                 qb = make_float4(beta.x, beta.y, beta.z, __uint_as_float(pixel));
-            } else if (depth < R.max_depth) {
+            } else if (depth < S.max_depth) {
                 if (tslot != 0xffffffffu && depth >= 1) {
                     // training record of this vertex; its target fills in as the tail is traced
                     const uint32_t ri = atomicAdd(R.rec_count, 1u);
@@ -309,12 +339,12 @@ __global__ void __launch_bounds__(128) k_shade(RenderDev R, int cur, uint32_t de
                         R.rec_tgt[3 * ri] = R.rec_tgt[3 * ri + 1] = R.rec_tgt[3 * ri + 2] = 0.f;
                         stored = ri;
                     }
-                    R.rec_of[tslot * (R.max_depth + 1) + depth] = stored;
+                    R.rec_of[tslot * (R.depth_max + 1) + depth] = stored;
                 }
                 // next-event estimation toward every light but the one hit
-                for (uint32_t l = 0; l < R.n_lights && l < kMaxLights; l++) {
+                for (uint32_t l = 0; l < S.n_lights && l < kMaxLights; l++) {
                     if (l == light_id) continue;
-                    const QuadLight &L = R.lights[l];
+                    const QuadLight &L = S.lights[l];
                     const float u = rnd(key, dim_of(depth, 2 * l)), v = rnd(key, dim_of(depth, 2 * l + 1));
                     // Quad::SamplePoint (Core/Shape/Quad.cpp:144-153): a bilinear
                     // patch over the reference's tessellation vertices
@@ -331,8 +361,8 @@ __global__ void __launch_bounds__(128) k_shade(RenderDev R, int cur, uint32_t de
                     const float3 c = beta * Ls * (fmaxf(0.f, dot3(wi, W))) * bsdf_f(m, wo_l, wi_l);
                     if (is_black(c)) continue;
                     const float3 seg = P - p;
-                    so[n_sh] = make_float4(p.x, p.y, p.z, R.eps);
-                    sd[n_sh] = make_float4(seg.x, seg.y, seg.z, 1.f - R.eps);
+                    so[n_sh] = make_float4(p.x, p.y, p.z, S.eps);
+                    sd[n_sh] = make_float4(seg.x, seg.y, seg.z, 1.f - S.eps);
                     sc[n_sh] = c;
                     n_sh++;
                 }
@@ -365,8 +395,8 @@ __global__ void __launch_bounds__(128) k_shade(RenderDev R, int cur, uint32_t de
                         else beta = beta * (1.f / q);
                     }
                     if (alive) {
-                        const float3 org = p + ng * R.eps;
-                        no = make_float4(org.x, org.y, org.z, R.eps);
+                        const float3 org = p + ng * S.eps;
+                        no = make_float4(org.x, org.y, org.z, S.eps);
                         nd = make_float4(wi.x, wi.y, wi.z, FLT_MAX);
                         cont = true;
                         R.beta[path] = make_float4(beta.x, beta.y, beta.z, 0.f);
@@ -395,6 +425,7 @@ __global__ void __launch_bounds__(128) k_shade(RenderDev R, int cur, uint32_t de
                 R.s_o[s] = so[k];
                 R.s_d[s] = sd[k];
                 R.s_c[s] = make_float4(sc[k].x, sc[k].y, sc[k].z, __uint_as_float(pixel));
+                R.s_sid[s] = sid;
                 if (R.cache_depth) R.s_meta[s] = tslot == 0xffffffffu ? 0xffffffffu : ((tslot << 8) | depth);
             } else {
                 atomicOr(R.err, 16u);
@@ -427,15 +458,16 @@ __global__ void k_cache_apply(RenderDev R)
     add_pixel(R.accum, __float_as_uint(b.w), make_float3(b.x * y.x, b.y * y.y, b.z * y.z));
 }
 
-__global__ void __launch_bounds__(128) k_shadow(RenderDev R)
+__global__ void __launch_bounds__(256) k_shadow(RenderDev R)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= *R.sh_count) return;
     const float4 o = R.s_o[i], d = R.s_d[i];
+    const SceneRec &S = R.scenes[R.s_sid[i]];
     int best;
     float bt, bu, bv;
     unsigned long long nn = 0, nt = 0;
-    trace_one<true, false>(R.nodes, R.tris, R.n_nodes, R.n_tris, o, d, best, bt, bu, bv, R.err, nn, nt);
+    trace_one<true, false>(S.nodes, S.tris, S.n_nodes, S.n_tris, o, d, best, bt, bu, bv, R.err, nn, nt);
     if (best == -1) {
         const float4 c = R.s_c[i];
         add_pixel(R.accum, __float_as_uint(c.w), make_float3(c.x, c.y, c.z));
@@ -488,41 +520,43 @@ cudaError_t build_tri_attr(const uint32_t *prim_of, uint32_t n_tris, const uint3
     return cudaGetLastError();
 }
 
-cudaError_t render_wave(const RenderDev &R, uint32_t n_paths, uint64_t sample0, cudaStream_t st,
-                        uint32_t *launches, const MlpDev *cache)
+cudaError_t render_wave(const RenderDev &R, uint32_t n_paths, uint64_t wave_begin, cudaStream_t st,
+                        uint32_t *launches, const MlpDev *cache, uint32_t block)
 {
-    const uint32_t T = 128;
+    const uint32_t T = block;
     cudaError_t e;
     if ((e = cudaMemsetAsync(R.count, 0, 2 * sizeof(uint32_t), st)) != cudaSuccess) return e;
     if (R.cache_depth) {
         if ((e = cudaMemsetAsync(R.train_count, 0, sizeof(uint32_t), st)) != cudaSuccess) return e;
         if ((e = cudaMemsetAsync(R.qry_count, 0, sizeof(uint32_t), st)) != cudaSuccess) return e;
-        if ((e = cudaMemsetAsync(R.rec_of, 0xff, sizeof(uint32_t) * R.train_cap * (R.max_depth + 1), st)) !=
+        if ((e = cudaMemsetAsync(R.rec_of, 0xff, sizeof(uint32_t) * R.train_cap * (R.depth_max + 1), st)) !=
             cudaSuccess)
             return e;
     }
-    k_camera<<<blocks_for(n_paths, T), T, 0, st>>>(R, n_paths, sample0);
+    k_camera<<<blocks_for(n_paths, 128), 128, 0, st>>>(R, n_paths, wave_begin);
     if ((e = cudaMemcpyAsync(R.count, &n_paths, sizeof(uint32_t), cudaMemcpyHostToDevice, st)) != cudaSuccess) return e;
     uint32_t n_launch = 1;
     int cur = 0;
-    for (uint32_t depth = 0; depth <= R.max_depth; depth++) {
+    uint32_t nl_max = 1;
+    for (uint32_t depth = 0; depth <= R.depth_max; depth++) {
         if ((e = cudaMemsetAsync(R.count + (cur ^ 1), 0, sizeof(uint32_t), st)) != cudaSuccess) return e;
         if ((e = cudaMemsetAsync(R.sh_count, 0, sizeof(uint32_t), st)) != cudaSuccess) return e;
         k_extend<<<blocks_for(n_paths, T), T, 0, st>>>(R, cur);
-        k_shade<<<blocks_for(n_paths, T), T, 0, st>>>(R, cur, depth, sample0);
+        k_shade<<<blocks_for(n_paths, T), T, 0, st>>>(R, cur, depth, wave_begin);
         n_launch += 2;
         if (R.cache_depth && depth == R.cache_depth && cache) {
             if ((e = mlp_infer(*cache, R.qry_feat, n_paths, R.qry_out, st, R.qry_count)) != cudaSuccess) return e;
-            k_cache_apply<<<blocks_for(n_paths, T), T, 0, st>>>(R);
+            k_cache_apply<<<blocks_for(n_paths, 128), 128, 0, st>>>(R);
             n_launch += 2;
         }
-        if (depth < R.max_depth) {
-            k_shadow<<<blocks_for((uint64_t)n_paths * (R.n_lights ? R.n_lights : 1), T), T, 0, st>>>(R);
+        if (depth < R.depth_max) {
+            k_shadow<<<blocks_for((uint64_t)R.sh_capacity, T), T, 0, st>>>(R);
             n_launch++;
         }
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
         cur ^= 1;
     }
+    (void)nl_max;
     if (launches) *launches += n_launch;
     return cudaSuccess;
 }

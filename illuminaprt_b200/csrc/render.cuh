@@ -25,9 +25,9 @@ struct QuadLight {
     float area;    // area of the two tessellation triangles
 };
 
-// Everything the kernels of one render need, passed by value.
-struct RenderDev {
-    // scene
+// One scene of a (batched) render: its BVH, shading data, camera and where
+// its paths and pixels sit in the wave's global index spaces.
+struct SceneRec {
     const Node8 *nodes;
     const Tri *tris;
     uint32_t n_nodes, n_tris;
@@ -41,10 +41,21 @@ struct RenderDev {
     float3 centre, corner, across, up;
     uint32_t width, height, wh;
     float rcp_w, rcp_h;
-    // integrator
     uint32_t max_depth;
     float eps;
+    uint32_t spp;
     uint32_t seed;
+    uint64_t path_begin;   // first global path index (paths are sample-major: sample * wh + pixel)
+    uint32_t pixel_base;   // first pixel of this scene in the accumulation buffer
+};
+
+// Everything the kernels of one render need, passed by value.
+struct RenderDev {
+    const SceneRec *scenes;
+    uint32_t n_scenes;
+    uint32_t depth_max;    // largest max_depth over the scenes
+    uint32_t *path_scene;  // per path of the wave: its scene
+    uint32_t *s_sid;       // per shadow segment: its scene
     // wavefront queues (ping-pong) and path state
     float4 *q_o[2], *q_d[2];
     uint32_t *q_path[2];
@@ -83,8 +94,9 @@ cudaError_t build_tri_attr(const uint32_t *prim_of, uint32_t n_tris, const uint3
                            const uint32_t *light_first_tri, uint32_t n_lights, uint32_t *light_of_prim,
                            uint32_t *attr, cudaStream_t st);
 struct MlpDev;
-cudaError_t render_wave(const RenderDev &R, uint32_t n_paths, uint64_t sample0, cudaStream_t st,
-                        uint32_t *launches, const MlpDev *cache);
+// One wave: global paths [wave_begin, wave_begin + n_paths).
+cudaError_t render_wave(const RenderDev &R, uint32_t n_paths, uint64_t wave_begin, cudaStream_t st,
+                        uint32_t *launches, const MlpDev *cache, uint32_t block = 128);
 cudaError_t render_resolve(const float4 *accum, uint32_t wh, float scale, float *out, cudaStream_t st);
 
 }  // namespace ilg

@@ -28,7 +28,7 @@ EXPORTED = ["ilg_create", "ilg_destroy", "ilg_last_error", "ilg_set_mesh", "ilg_
             "ilg_intersect", "ilg_intersect_counted", "ilg_occluded", "ilg_sync", "ilg_stream",
             "ilg_set_materials", "ilg_set_quad_lights", "ilg_render", "ilg_intersect_noalloc",
             "ilg_mlp_init", "ilg_mlp_get_params", "ilg_mlp_set_params", "ilg_mlp_infer", "ilg_mlp_grads",
-            "ilg_mlp_train_step"]
+            "ilg_mlp_train_step", "ilg_render_batch"]
 
 ILG_MLP_RAW = 16
 ILG_MLP_PARAMS = 23040
@@ -69,6 +69,10 @@ class ilg_camera(ctypes.Structure):
                 ("fov_deg", ctypes.c_float), ("aspect", ctypes.c_float)]
 
 
+class ilg_batch_item(ctypes.Structure):
+    pass
+
+
 class ilg_render_opts(ctypes.Structure):
     _fields_ = [("width", ctypes.c_uint32), ("height", ctypes.c_uint32), ("spp", ctypes.c_uint32),
                 ("max_depth", ctypes.c_uint32), ("epsilon", ctypes.c_float), ("seed", ctypes.c_uint32),
@@ -76,6 +80,11 @@ class ilg_render_opts(ctypes.Structure):
                 ("train_every", ctypes.c_uint32), ("train_steps", ctypes.c_uint32), ("train_batch", ctypes.c_uint32),
                 ("reserved", ctypes.c_uint32 * 2)]
 
+
+ilg_batch_item._fields_ = [("scene", ctypes.c_void_p), ("camera", ilg_camera), ("width", ctypes.c_uint32),
+                           ("height", ctypes.c_uint32), ("spp", ctypes.c_uint32), ("max_depth", ctypes.c_uint32),
+                           ("epsilon", ctypes.c_float), ("seed", ctypes.c_uint32), ("sky", ctypes.c_float * 3),
+                           ("out_rgb", ctypes.c_void_p)]
 
 _lib = None
 
@@ -119,6 +128,8 @@ def load(build_if_missing: bool = True) -> ctypes.CDLL:
     for f in ("ilg_mlp_init", "ilg_mlp_get_params", "ilg_mlp_set_params", "ilg_mlp_infer", "ilg_mlp_grads",
               "ilg_mlp_train_step"):
         getattr(L, f).restype = i32
+    L.ilg_render_batch.argtypes = [vp, vp, u32, u32, u32, u32]
+    L.ilg_render_batch.restype = i32
     L.ilg_sync.argtypes = [vp]
     L.ilg_stream.argtypes = [vp]
     L.ilg_stream.restype = vp
@@ -295,6 +306,37 @@ class GpuSpace:
         self._check(self.L.ilg_mlp_train_step(self.h, raw.ctypes.data, target.ctypes.data, raw.shape[0],
                                               ctypes.byref(loss), 0))
         return loss.value
+
+    def render_batch(self, items, paths_per_wave: int = 0, block: int = 0, device_ptrs: bool = False):
+        """items: list of dicts {space: GpuSpace, camera, width, height, spp, max_depth=6, epsilon=1e-4,
+        seed=1, sky=(0,0,0), out=None}. Renders all in one wavefront on this context; returns the images
+        (numpy arrays, or the given CUDA tensors when device_ptrs)."""
+        arr = (ilg_batch_item * len(items))()
+        outs = []
+        for i, it in enumerate(items):
+            cam = it["camera"]
+            a = arr[i]
+            a.scene = it["space"].h.value
+            a.camera.eye[:] = list(cam["eye"])
+            a.camera.target[:] = list(cam["target"])
+            a.camera.up[:] = list(cam["up"])
+            a.camera.fov_deg = float(cam["fov"])
+            a.camera.aspect = float(cam.get("aspect", it["width"] / it["height"]))
+            a.width, a.height, a.spp = it["width"], it["height"], it["spp"]
+            a.max_depth = it.get("max_depth", 6)
+            a.epsilon = it.get("epsilon", 1e-4)
+            a.seed = it.get("seed", 1)
+            a.sky[:] = list(it.get("sky", (0.0, 0.0, 0.0)))
+            if device_ptrs:
+                out = it["out"]
+                a.out_rgb = out.data_ptr()
+            else:
+                out = np.empty((it["height"], it["width"], 3), np.float32)
+                a.out_rgb = out.ctypes.data
+            outs.append(out)
+        self._check(self.L.ilg_render_batch(self.h, ctypes.addressof(arr), len(items), paths_per_wave, block,
+                                            ILG_DEVICE_PTRS if device_ptrs else 0))
+        return outs
 
     def sync(self):
         self._check(self.L.ilg_sync(self.h))

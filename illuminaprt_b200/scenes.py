@@ -361,3 +361,29 @@ def load_sphere_field(space, scene):
     space.set_materials(scene["materials"])
     space.set_quad_lights(scene["lights"])
     return scene
+
+
+def batch_workload(n_scenes: int = 32, seed: int = 9, tri_range=(10_000, 2_000_000), side_range=(256, 1024)):
+    """Independent icosphere-field scenes with uneven sizes: triangle counts
+    log-uniform in tri_range (grid side and subdivision picked to match),
+    square images with side log-uniform in side_range, spp from
+    {4, 8, 16, 32, 64}, max depth uniform in [4, 16]."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    items = []
+    for i in range(n_scenes):
+        target = float(np.exp(rng.uniform(np.log(tri_range[0]), np.log(tri_range[1]))))
+        best = None
+        for s in range(2, 8):
+            for n_side in range(1, 9):
+                t = n_side * n_side * 20 * 4 ** s
+                err = abs(np.log(t / target))
+                if best is None or err < best[0]:
+                    best = (err, n_side, s)
+        _, n_side, subdiv = best
+        side = int(round(np.exp(rng.uniform(np.log(side_range[0]), np.log(side_range[1])))))
+        scene = sphere_field(n_side, subdiv, seed=1000 + i, width=side, height=side)
+        scene["spp"] = int(rng.choice([4, 8, 16, 32, 64]))
+        scene["max_depth"] = int(rng.integers(4, 17))
+        scene["target_tris"] = int(target)
+        items.append(scene)
+    return items

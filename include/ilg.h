@@ -198,6 +198,26 @@ int ilg_mlp_grads(ilg_ctx *ctx, const float *raw, const float *target, uint32_t 
 /* One Adam step on the batch; *loss (optional) receives the loss before the step. */
 int ilg_mlp_train_step(ilg_ctx *ctx, const float *raw, const float *target, uint32_t n, float *loss, uint32_t flags);
 
+/* Many independent scenes rendered together: one wavefront over the paths of
+ * every item (a scene context with its built mesh, materials and lights, a
+ * camera, image size, spp and depth), so scenes of very different sizes and
+ * path lengths share the queues. The runner context supplies the wavefront
+ * buffers and the stream; all contexts must be on its device.
+ * paths_per_wave: 0 = automatic; block: threads per block of the extend,
+ * shade and shadow kernels (64, 128 or 256; 0 = 128). */
+typedef struct ilg_batch_item {
+    ilg_ctx *scene;
+    ilg_camera camera;
+    uint32_t width, height, spp, max_depth;
+    float epsilon;
+    uint32_t seed;
+    float sky[3];
+    float *out_rgb; /* height x width x 3 */
+} ilg_batch_item;
+
+int ilg_render_batch(ilg_ctx *runner, const ilg_batch_item *items, uint32_t n, uint32_t paths_per_wave,
+                     uint32_t block, uint32_t flags);
+
 /* Blocks until the context's stream is idle (for ILG_DEVICE_PTRS callers). */
 int ilg_sync(ilg_ctx *ctx);
 
