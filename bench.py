@@ -251,6 +251,30 @@ def bench_path_tracer(dev, local, quick=False):
     res["pt_field_1080p_64spp_ms"] = round(ms, 2)
     res["pt_field_msamples_s"] = round(W * H * spp / (ms / 1e3) / 1e6, 3)
     sp.close()
+    # 32 independent scenes of uneven size in one wavefront, autotuned
+    from illuminaprt_b200.autotune import tune_batch
+    items = scenes.batch_workload(32, seed=9)
+    spaces, batch = [], []
+    for i, s in enumerate(items):
+        sp_i = GpuSpace(device=local)
+        scenes.load_sphere_field(sp_i, s)
+        spaces.append(sp_i)
+        batch.append({"space": sp_i, "camera": s["camera"], "width": s["width"], "height": s["height"],
+                      "spp": s["spp"], "max_depth": s["max_depth"], "seed": 7 + i, "sky": s["sky"]})
+    runner = GpuSpace(device=local)
+    choice, _ = tune_batch(runner, batch, waves=(1 << 21, 1 << 22, 1 << 23), blocks=(128, 256))
+    t0 = time.perf_counter()
+    runner.render_batch(batch, paths_per_wave=choice["paths_per_wave"], block=choice["block"])
+    dt = time.perf_counter() - t0
+    samples = sum(b["width"] * b["height"] * b["spp"] for b in batch)
+    res["pt_batch32_triangles"] = int(sum(s["idx"].shape[0] for s in items))
+    res["pt_batch32_samples"] = int(samples)
+    res["pt_batch32_ms"] = round(dt * 1e3, 2)
+    res["pt_batch32_msamples_s"] = round(samples / dt / 1e6, 3)
+    res["pt_batch32_autotuned"] = {"paths_per_wave": choice["paths_per_wave"], "block": choice["block"]}
+    for sp_i in spaces:
+        sp_i.close()
+    runner.close()
     return res
 
 
