@@ -414,7 +414,7 @@ def main():
             "gpu_launches": 2 * args.steps,
             "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": hbm, "unit": "GB/s",
                          "frac": round(achieved / hbm, 4), "traffic": None,
-                         "kernel": "k_closest (incoherent launch)",
+                         "kernel": "k_trace_dyn<closest> (incoherent launch)",
                          "peak_source": f"{peak_kind} hbm_gbs",
                          "alg_bytes_per_launch": int(alg_bytes),
                          "node_visits_per_ray": None if vin is None else round(vin[0] / n_in, 3),

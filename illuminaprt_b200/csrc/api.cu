@@ -185,9 +185,10 @@ int ilg_intersect(ilg_ctx *ctx, const float *ray_o_tmin, const float *ray_d_tmax
         return fail(ctx, ILG_EINVAL, "ilg_intersect: ray arrays must be 16-byte aligned");
     CK(cudaSetDevice(ctx->device));
     const SceneView sv = ctx->view();
+    uint32_t *next = ctx->derr.ptr + 1;  // ray counter of the persistent kernels
     if (flags & ILG_DEVICE_PTRS) {
-        CK(launch_closest(sv, (const float4 *)ray_o_tmin, (const float4 *)ray_d_tmax, n, prim, t, u, v, ctx->derr.ptr,
-                          nullptr, ctx->stream));
+        CK(launch_closest_dyn(sv, (const float4 *)ray_o_tmin, (const float4 *)ray_d_tmax, n, prim, t, u, v, next,
+                              ctx->derr.ptr, ctx->stream));
         return ILG_OK;
     }
     CK(ctx->ro.reserve(n));
@@ -199,8 +200,8 @@ int ilg_intersect(ilg_ctx *ctx, const float *ray_o_tmin, const float *ray_d_tmax
     cudaStream_t st = ctx->stream;
     CK(cudaMemcpyAsync(ctx->ro.ptr, ray_o_tmin, 16ull * n, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(ctx->rd.ptr, ray_d_tmax, 16ull * n, cudaMemcpyHostToDevice, st));
-    CK(launch_closest(sv, ctx->ro.ptr, ctx->rd.ptr, n, ctx->hprim.ptr, ctx->ht.ptr, ctx->hu.ptr, ctx->hv.ptr,
-                      ctx->derr.ptr, nullptr, st));
+    CK(launch_closest_dyn(sv, ctx->ro.ptr, ctx->rd.ptr, n, ctx->hprim.ptr, ctx->ht.ptr, ctx->hu.ptr, ctx->hv.ptr,
+                          next, ctx->derr.ptr, st));
     CK(cudaMemcpyAsync(prim, ctx->hprim.ptr, 4ull * n, cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(t, ctx->ht.ptr, 4ull * n, cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(u, ctx->hu.ptr, 4ull * n, cudaMemcpyDeviceToHost, st));
@@ -241,8 +242,10 @@ int ilg_occluded(ilg_ctx *ctx, const float *ray_o_tmin, const float *ray_d_tmax,
         return fail(ctx, ILG_EINVAL, "ilg_occluded: ray arrays must be 16-byte aligned");
     CK(cudaSetDevice(ctx->device));
     const SceneView sv = ctx->view();
+    uint32_t *next = ctx->derr.ptr + 1;
     if (flags & ILG_DEVICE_PTRS) {
-        CK(launch_any(sv, (const float4 *)ray_o_tmin, (const float4 *)ray_d_tmax, n, occ, ctx->derr.ptr, ctx->stream));
+        CK(launch_any_dyn(sv, (const float4 *)ray_o_tmin, (const float4 *)ray_d_tmax, n, occ, next, ctx->derr.ptr,
+                          ctx->stream));
         return ILG_OK;
     }
     CK(ctx->ro.reserve(n));
@@ -251,7 +254,7 @@ int ilg_occluded(ilg_ctx *ctx, const float *ray_o_tmin, const float *ray_d_tmax,
     cudaStream_t st = ctx->stream;
     CK(cudaMemcpyAsync(ctx->ro.ptr, ray_o_tmin, 16ull * n, cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(ctx->rd.ptr, ray_d_tmax, 16ull * n, cudaMemcpyHostToDevice, st));
-    CK(launch_any(sv, ctx->ro.ptr, ctx->rd.ptr, n, ctx->hocc.ptr, ctx->derr.ptr, st));
+    CK(launch_any_dyn(sv, ctx->ro.ptr, ctx->rd.ptr, n, ctx->hocc.ptr, next, ctx->derr.ptr, st));
     CK(cudaMemcpyAsync(occ, ctx->hocc.ptr, n, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     return ctx->check_device_error();

@@ -2,6 +2,8 @@
 #include "trace.cuh"
 #include "trace_api.cuh"
 
+#include <algorithm>
+
 namespace ilg {
 
 namespace {
@@ -47,7 +49,91 @@ __global__ void __launch_bounds__(128) k_any(const Node8 *__restrict__ nodes, co
     occ[i] = best >= 0 ? 1 : 0;
 }
 
+// Persistent closest / any hit with dynamic ray fetch (see trace.cuh).
+template <bool kAnyHit>
+__global__ void __launch_bounds__(128) k_trace_dyn(const Node8 *__restrict__ nodes, const Tri *__restrict__ tris,
+                                                   const uint32_t *__restrict__ prim_of, uint32_t n_nodes_total,
+                                                   uint32_t n_tris_total, const float4 *__restrict__ ro,
+                                                   const float4 *__restrict__ rd, uint32_t n,
+                                                   int32_t *__restrict__ prim, float *__restrict__ tout,
+                                                   float *__restrict__ uout, float *__restrict__ vout,
+                                                   uint8_t *__restrict__ occ, uint32_t *__restrict__ next,
+                                                   uint32_t *__restrict__ err)
+{
+    const uint32_t lane = threadIdx.x & 31u;
+    uint2 stack[kMaxStack];
+    RayState r;
+    bool active = false, exhausted = false;  // exhausted is warp-uniform
+    uint32_t id = 0;
+    while (true) {
+        const uint32_t idle = __ballot_sync(0xffffffffu, !active);
+        if (!exhausted && (__popc(idle) >= kRefillLanes || idle == 0xffffffffu)) {
+            const uint32_t leader = __ffs(idle) - 1u;
+            uint32_t base = 0;
+            if (lane == leader) base = atomicAdd(next, (uint32_t)__popc(idle));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (base >= n) exhausted = true;
+            if (!active) {
+                const uint32_t k = base + __popc(idle & ((1u << lane) - 1u));
+                if (k < n) {
+                    id = k;
+                    ray_init(r, __ldcs(ro + id), __ldcs(rd + id), n_nodes_total);
+                    active = true;
+                }
+            }
+        }
+        if (__ballot_sync(0xffffffffu, active) == 0u) break;
+        if (active && ray_step<kAnyHit>(r, stack, nodes, tris, n_nodes_total, n_tris_total, err)) {
+            if (kAnyHit) {
+                occ[id] = r.best >= 0 ? 1 : 0;
+            } else {
+                __stcs(prim + id, r.best >= 0 ? (int32_t)__ldg(prim_of + r.best) : (r.best == -2 ? -2 : -1));
+                __stcs(tout + id, r.best >= 0 ? r.tcur : __int_as_float(0x7f800000));
+                __stcs(uout + id, r.best >= 0 ? r.bu : 0.f);
+                __stcs(vout + id, r.best >= 0 ? r.bv : 0.f);
+            }
+            active = false;
+        }
+    }
+}
+
+int sm_count()
+{
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 148;
+    }
+    return sms;
+}
+
 }  // namespace
+
+cudaError_t launch_closest_dyn(const SceneView &s, const float4 *ro, const float4 *rd, uint32_t n, int32_t *prim,
+                               float *t, float *u, float *v, uint32_t *next, uint32_t *err, cudaStream_t st)
+{
+    if (n == 0) return cudaSuccess;
+    cudaError_t e = cudaMemsetAsync(next, 0, sizeof(uint32_t), st);
+    if (e != cudaSuccess) return e;
+    const uint32_t blocks = std::min<uint32_t>((n + 127) / 128, (uint32_t)sm_count() * 16u);
+    k_trace_dyn<false><<<blocks, 128, 0, st>>>(s.nodes, s.tris, s.prim_of, s.n_nodes, s.n_tris, ro, rd, n, prim, t,
+                                               u, v, nullptr, next, err);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_any_dyn(const SceneView &s, const float4 *ro, const float4 *rd, uint32_t n, uint8_t *occ,
+                           uint32_t *next, uint32_t *err, cudaStream_t st)
+{
+    if (n == 0) return cudaSuccess;
+    cudaError_t e = cudaMemsetAsync(next, 0, sizeof(uint32_t), st);
+    if (e != cudaSuccess) return e;
+    const uint32_t blocks = std::min<uint32_t>((n + 127) / 128, (uint32_t)sm_count() * 16u);
+    k_trace_dyn<true><<<blocks, 128, 0, st>>>(s.nodes, s.tris, nullptr, s.n_nodes, s.n_tris, ro, rd, n, nullptr,
+                                              nullptr, nullptr, nullptr, occ, next, err);
+    return cudaGetLastError();
+}
 
 cudaError_t launch_closest(const SceneView &s, const float4 *ro, const float4 *rd, uint32_t n, int32_t *prim,
                            float *t, float *u, float *v, uint32_t *err, unsigned long long *stats, cudaStream_t st)

@@ -155,4 +155,148 @@ __device__ __forceinline__ void trace_one(const Node8 *__restrict__ nodes, const
     }
 }
 
+
+// ---------------------------------------------------------------------------
+// Persistent traversal with dynamic ray fetch: each warp keeps its lanes busy
+// by handing a finished lane a new ray from a global counter whenever at least
+// kRefillLanes lanes are idle (Aila & Laine 2009, "Understanding the
+// efficiency of ray traversal on GPUs"). One loop iteration = one node visit
+// and the triangle tests it enables, so lanes stay in step on the same code.
+// ---------------------------------------------------------------------------
+constexpr uint32_t kRefillLanes = 8;
+
+struct RayState {
+    float ox, oy, oz, dx, dy, dz;
+    float ix, iy, iz;
+    float tmin, tcur, whi;
+    uint32_t octinv;
+    uint32_t ng_base, ng_hits, tg_base, tg_hits;
+    uint32_t budget;
+    int sp;
+    int best;
+    float bu, bv;
+};
+
+__device__ __forceinline__ void ray_init(RayState &r, float4 o, float4 d, uint32_t n_nodes_total)
+{
+    const float kTiny = 1e-20f;
+    r.ox = o.x; r.oy = o.y; r.oz = o.z; r.dx = d.x; r.dy = d.y; r.dz = d.z;
+    r.ix = __frcp_rn(fabsf(d.x) > kTiny ? d.x : copysignf(kTiny, d.x));
+    r.iy = __frcp_rn(fabsf(d.y) > kTiny ? d.y : copysignf(kTiny, d.y));
+    r.iz = __frcp_rn(fabsf(d.z) > kTiny ? d.z : copysignf(kTiny, d.z));
+    const uint32_t oct = (d.x < 0.f ? 1u : 0u) | (d.y < 0.f ? 2u : 0u) | (d.z < 0.f ? 4u : 0u);
+    r.octinv = 7u - oct;
+    r.tmin = o.w;
+    r.tcur = d.w;
+    r.whi = window_hi(r.tcur);
+    r.ng_base = 0;
+    r.ng_hits = (1u << (24 + r.octinv)) | 1u;
+    r.tg_base = 0;
+    r.tg_hits = 0;
+    r.budget = n_nodes_total + 1u;
+    r.sp = 0;
+    r.best = -1;
+    r.bu = r.bv = 0.f;
+}
+
+// One traversal step. Returns true when the ray is finished (r.best is the
+// hit record, -1 for a miss, -2 for a reported error).
+template <bool kAnyHit>
+__device__ __forceinline__ bool ray_step(RayState &r, uint2 *stack, const Node8 *__restrict__ nodes,
+                                         const Tri *__restrict__ tris, uint32_t n_nodes_total, uint32_t n_tris_total,
+                                         uint32_t *__restrict__ err)
+{
+    if (r.ng_hits & 0xff000000u) {
+        if (r.budget-- == 0u) {
+            atomicOr(err, 4u);
+            r.best = -2;
+            return true;
+        }
+        const uint32_t bit = 31u - __clz(r.ng_hits & 0xff000000u);
+        r.ng_hits &= ~(1u << bit);
+        const uint32_t slot = (bit - 24u) ^ r.octinv;
+        const uint32_t node_idx = r.ng_base + __popc(r.ng_hits & 0xffu & ((1u << slot) - 1u));
+        if (r.ng_hits & 0xff000000u) {
+            if (r.sp >= kMaxStack) {
+                atomicOr(err, 1u);
+                r.best = -2;
+                return true;
+            }
+            stack[r.sp++] = make_uint2(r.ng_base, r.ng_hits);
+        }
+        if (node_idx >= n_nodes_total) {
+            atomicOr(err, 2u);
+            r.best = -2;
+            return true;
+        }
+        const uint4 *q = reinterpret_cast<const uint4 *>(nodes + node_idx);
+        const uint4 q0 = __ldg(q), q1 = __ldg(q + 1), q2 = __ldg(q + 2), q3 = __ldg(q + 3), q4 = __ldg(q + 4);
+        const float sx = __uint_as_float((q0.w & 0xffu) << 23);
+        const float sy = __uint_as_float(((q0.w >> 8) & 0xffu) << 23);
+        const float sz = __uint_as_float(((q0.w >> 16) & 0xffu) << 23);
+        const float ax = (__uint_as_float(q0.x) - r.ox) * r.ix, ay = (__uint_as_float(q0.y) - r.oy) * r.iy,
+                    az = (__uint_as_float(q0.z) - r.oz) * r.iz;
+        const float bx = sx * r.ix, by = sy * r.iy, bz = sz * r.iz;
+        const uint32_t nxl = r.ix >= 0.f ? q2.x : q2.z, nxh = r.ix >= 0.f ? q2.y : q2.w;
+        const uint32_t fxl = r.ix >= 0.f ? q2.z : q2.x, fxh = r.ix >= 0.f ? q2.w : q2.y;
+        const uint32_t nyl = r.iy >= 0.f ? q3.x : q3.z, nyh = r.iy >= 0.f ? q3.y : q3.w;
+        const uint32_t fyl = r.iy >= 0.f ? q3.z : q3.x, fyh = r.iy >= 0.f ? q3.w : q3.y;
+        const uint32_t nzl = r.iz >= 0.f ? q4.x : q4.z, nzh = r.iz >= 0.f ? q4.y : q4.w;
+        const uint32_t fzl = r.iz >= 0.f ? q4.z : q4.x, fzh = r.iz >= 0.f ? q4.w : q4.y;
+        uint32_t hits_int = 0, hits_tri = 0;
+#pragma unroll
+        for (int s = 0; s < 8; s++) {
+            const uint32_t sh = (s & 3) * 8;
+            const uint32_t meta = ((s < 4 ? q1.z : q1.w) >> sh) & 0xffu;
+            const float tnx = fmaf((float)(((s < 4 ? nxl : nxh) >> sh) & 0xffu), bx, ax);
+            const float tfx = fmaf((float)(((s < 4 ? fxl : fxh) >> sh) & 0xffu), bx, ax);
+            const float tny = fmaf((float)(((s < 4 ? nyl : nyh) >> sh) & 0xffu), by, ay);
+            const float tfy = fmaf((float)(((s < 4 ? fyl : fyh) >> sh) & 0xffu), by, ay);
+            const float tnz = fmaf((float)(((s < 4 ? nzl : nzh) >> sh) & 0xffu), bz, az);
+            const float tfz = fmaf((float)(((s < 4 ? fzl : fzh) >> sh) & 0xffu), bz, az);
+            const float tn = fmaxf(fmaxf(fmaxf(tnx, tny), tnz) * 0.9999990f, r.tmin);
+            const float tf = fminf(fminf(fminf(tfx, tfy), tfz) * 1.0000010f, r.tcur);
+            if (meta != 0u && tn <= tf) {
+                if (meta == kMetaInternal) hits_int |= 1u << (24u + ((uint32_t)s ^ r.octinv));
+                else hits_tri |= ((1u << (meta >> 5)) - 1u) << (meta & 31u);
+            }
+        }
+        r.ng_base = q1.x;
+        r.ng_hits = hits_int | (q0.w >> 24);
+        r.tg_base = q1.y;
+        r.tg_hits = hits_tri;
+    }
+    while (r.tg_hits) {
+        const uint32_t b = __ffs(r.tg_hits) - 1u;
+        r.tg_hits &= r.tg_hits - 1u;
+        const uint32_t ti = r.tg_base + b;
+        if (ti >= n_tris_total) {
+            atomicOr(err, 2u);
+            r.best = -2;
+            return true;
+        }
+        const float4 *tp = reinterpret_cast<const float4 *>(tris + ti);
+        Tri tr;
+        tr.a = __ldg(tp);
+        tr.b = __ldg(tp + 1);
+        tr.c = __ldg(tp + 2);
+        float th, bh, gh;
+        if (shirley(tr, r.ox, r.oy, r.oz, r.dx, r.dy, r.dz, r.whi, th, bh, gh)) {
+            r.best = (int)ti;
+            if (kAnyHit) return true;
+            r.bu = bh;
+            r.bv = gh;
+            r.tcur = th;
+            r.whi = window_hi(r.tcur);
+        }
+    }
+    if (!(r.ng_hits & 0xff000000u)) {
+        if (r.sp == 0) return true;
+        const uint2 e = stack[--r.sp];
+        r.ng_base = e.x;
+        r.ng_hits = e.y;
+    }
+    return false;
+}
+
 }  // namespace ilg
