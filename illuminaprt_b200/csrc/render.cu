@@ -537,7 +537,6 @@ cudaError_t render_wave(const RenderDev &R, uint32_t n_paths, uint64_t wave_begi
     if ((e = cudaMemcpyAsync(R.count, &n_paths, sizeof(uint32_t), cudaMemcpyHostToDevice, st)) != cudaSuccess) return e;
     uint32_t n_launch = 1;
     int cur = 0;
-    uint32_t nl_max = 1;
     for (uint32_t depth = 0; depth <= R.depth_max; depth++) {
         if ((e = cudaMemsetAsync(R.count + (cur ^ 1), 0, sizeof(uint32_t), st)) != cudaSuccess) return e;
         if ((e = cudaMemsetAsync(R.sh_count, 0, sizeof(uint32_t), st)) != cudaSuccess) return e;
@@ -556,7 +555,6 @@ cudaError_t render_wave(const RenderDev &R, uint32_t n_paths, uint64_t wave_begi
         if ((e = cudaGetLastError()) != cudaSuccess) return e;
         cur ^= 1;
     }
-    (void)nl_max;
     if (launches) *launches += n_launch;
     return cudaSuccess;
 }

@@ -26,144 +26,10 @@ struct TraceStats {
     unsigned long long nodes, tris;
 };
 
-template <bool kAnyHit, bool kStats>
-__device__ __forceinline__ void trace_one(const Node8 *__restrict__ nodes, const Tri *__restrict__ tris,
-                                          uint32_t n_nodes_total, uint32_t n_tris_total,
-                                          float4 o, float4 d, int &best, float &bt, float &bu, float &bv,
-                                          uint32_t *__restrict__ err, unsigned long long &n_nodes,
-                                          unsigned long long &n_tris)
-{
-    const float kTiny = 1e-20f;
-    const float ix = __frcp_rn(fabsf(d.x) > kTiny ? d.x : copysignf(kTiny, d.x));
-    const float iy = __frcp_rn(fabsf(d.y) > kTiny ? d.y : copysignf(kTiny, d.y));
-    const float iz = __frcp_rn(fabsf(d.z) > kTiny ? d.z : copysignf(kTiny, d.z));
-    const uint32_t oct = (d.x < 0.f ? 1u : 0u) | (d.y < 0.f ? 2u : 0u) | (d.z < 0.f ? 4u : 0u);
-    const uint32_t octinv = 7u - oct;
-    const float tmin = o.w;
-    float tcur = d.w;
-    float whi = window_hi(tcur);
-
-    uint2 stack[kMaxStack];
-    int sp = 0;
-    uint32_t ng_base = 0, ng_hits = (1u << (24 + octinv)) | 1u;  // virtual parent: root in slot 0
-    uint32_t tg_base = 0, tg_hits = 0;
-    best = -1;
-    bt = __int_as_float(0x7f800000);
-    bu = bv = 0.f;
-
-    // A ray reads each node at most once in a well-formed tree; the budget
-    // turns a corrupt (cyclic) tree into an error instead of a hang.
-    uint32_t budget = n_nodes_total + 1u;
-    while (true) {
-        if (ng_hits & 0xff000000u) {
-            if (budget-- == 0u) {
-                atomicOr(err, 4u);
-                best = -2;
-                return;
-            }
-            const uint32_t bit = 31u - __clz(ng_hits & 0xff000000u);
-            ng_hits &= ~(1u << bit);
-            const uint32_t slot = (bit - 24u) ^ octinv;
-            const uint32_t node_idx = ng_base + __popc(ng_hits & 0xffu & ((1u << slot) - 1u));
-            if (ng_hits & 0xff000000u) {
-                if (sp >= kMaxStack) {
-                    atomicOr(err, 1u);
-                    best = -2;
-                    return;
-                }
-                stack[sp++] = make_uint2(ng_base, ng_hits);
-            }
-            if (node_idx >= n_nodes_total) {  // corrupt tree: report, never read out of bounds
-                atomicOr(err, 2u);
-                best = -2;
-                return;
-            }
-            const uint4 *q = reinterpret_cast<const uint4 *>(nodes + node_idx);
-            const uint4 q0 = __ldg(q), q1 = __ldg(q + 1), q2 = __ldg(q + 2), q3 = __ldg(q + 3), q4 = __ldg(q + 4);
-            if (kStats) n_nodes++;
-            const float sx = __uint_as_float((q0.w & 0xffu) << 23);
-            const float sy = __uint_as_float(((q0.w >> 8) & 0xffu) << 23);
-            const float sz = __uint_as_float(((q0.w >> 16) & 0xffu) << 23);
-            const float ax = (__uint_as_float(q0.x) - o.x) * ix, ay = (__uint_as_float(q0.y) - o.y) * iy,
-                        az = (__uint_as_float(q0.z) - o.z) * iz;
-            const float bx = sx * ix, by = sy * iy, bz = sz * iz;
-            // near/far quantised planes per axis, chosen by direction sign
-            const uint32_t nxl = ix >= 0.f ? q2.x : q2.z, nxh = ix >= 0.f ? q2.y : q2.w;
-            const uint32_t fxl = ix >= 0.f ? q2.z : q2.x, fxh = ix >= 0.f ? q2.w : q2.y;
-            const uint32_t nyl = iy >= 0.f ? q3.x : q3.z, nyh = iy >= 0.f ? q3.y : q3.w;
-            const uint32_t fyl = iy >= 0.f ? q3.z : q3.x, fyh = iy >= 0.f ? q3.w : q3.y;
-            const uint32_t nzl = iz >= 0.f ? q4.x : q4.z, nzh = iz >= 0.f ? q4.y : q4.w;
-            const uint32_t fzl = iz >= 0.f ? q4.z : q4.x, fzh = iz >= 0.f ? q4.w : q4.y;
-            uint32_t hits_int = 0, hits_tri = 0;
-#pragma unroll
-            for (int s = 0; s < 8; s++) {
-                const uint32_t sh = (s & 3) * 8;
-                const uint32_t meta = ((s < 4 ? q1.z : q1.w) >> sh) & 0xffu;
-                const float tnx = fmaf((float)(((s < 4 ? nxl : nxh) >> sh) & 0xffu), bx, ax);
-                const float tfx = fmaf((float)(((s < 4 ? fxl : fxh) >> sh) & 0xffu), bx, ax);
-                const float tny = fmaf((float)(((s < 4 ? nyl : nyh) >> sh) & 0xffu), by, ay);
-                const float tfy = fmaf((float)(((s < 4 ? fyl : fyh) >> sh) & 0xffu), by, ay);
-                const float tnz = fmaf((float)(((s < 4 ? nzl : nzh) >> sh) & 0xffu), bz, az);
-                const float tfz = fmaf((float)(((s < 4 ? fzl : fzh) >> sh) & 0xffu), bz, az);
-                // relative padding absorbs the rounding of the three fmas
-                const float tn = fmaxf(fmaxf(fmaxf(tnx, tny), tnz) * 0.9999990f, tmin);
-                const float tf = fminf(fminf(fminf(tfx, tfy), tfz) * 1.0000010f, tcur);
-                if (meta != 0u && tn <= tf) {
-                    if (meta == kMetaInternal) hits_int |= 1u << (24u + ((uint32_t)s ^ octinv));
-                    else hits_tri |= ((1u << (meta >> 5)) - 1u) << (meta & 31u);
-                }
-            }
-            ng_base = q1.x;
-            ng_hits = hits_int | (q0.w >> 24);
-            tg_base = q1.y;
-            tg_hits = hits_tri;
-        }
-
-        while (tg_hits) {
-            const uint32_t b = __ffs(tg_hits) - 1u;
-            tg_hits &= tg_hits - 1u;
-            const uint32_t ti = tg_base + b;
-            if (ti >= n_tris_total) {
-                atomicOr(err, 2u);
-                best = -2;
-                return;
-            }
-            const float4 *tp = reinterpret_cast<const float4 *>(tris + ti);
-            Tri tr;
-            tr.a = __ldg(tp);
-            tr.b = __ldg(tp + 1);
-            tr.c = __ldg(tp + 2);
-            if (kStats) n_tris++;
-            float th, bh, gh;
-            if (shirley(tr, o.x, o.y, o.z, d.x, d.y, d.z, whi, th, bh, gh)) {
-                best = (int)ti;
-                if (kAnyHit) return;
-                bt = th;
-                bu = bh;
-                bv = gh;
-                tcur = th;  // ray.Max = Min(ray.Max, distance), BVHMesh.cpp:189
-                whi = window_hi(tcur);
-            }
-        }
-
-        if (!(ng_hits & 0xff000000u)) {
-            if (sp == 0) break;
-            const uint2 e = stack[--sp];
-            ng_base = e.x;
-            ng_hits = e.y;
-        }
-    }
-}
-
-
 // ---------------------------------------------------------------------------
-// Persistent traversal with dynamic ray fetch: each warp keeps its lanes busy
-// by handing a finished lane a new ray from a global counter whenever at least
-// kRefillLanes lanes are idle (Aila & Laine 2009, "Understanding the
-// efficiency of ray traversal on GPUs"). One loop iteration = one node visit
-// and the triangle tests it enables, so lanes stay in step on the same code.
+// Traversal state machine shared by every kernel
 // ---------------------------------------------------------------------------
-constexpr uint32_t kRefillLanes = 8;
+
 
 struct RayState {
     float ox, oy, oz, dx, dy, dz;
@@ -201,10 +67,11 @@ __device__ __forceinline__ void ray_init(RayState &r, float4 o, float4 d, uint32
 
 // One traversal step. Returns true when the ray is finished (r.best is the
 // hit record, -1 for a miss, -2 for a reported error).
-template <bool kAnyHit>
+template <bool kAnyHit, bool kStats = false>
 __device__ __forceinline__ bool ray_step(RayState &r, uint2 *stack, const Node8 *__restrict__ nodes,
                                          const Tri *__restrict__ tris, uint32_t n_nodes_total, uint32_t n_tris_total,
-                                         uint32_t *__restrict__ err)
+                                         uint32_t *__restrict__ err, unsigned long long *n_nodes = nullptr,
+                                         unsigned long long *n_tris = nullptr)
 {
     if (r.ng_hits & 0xff000000u) {
         if (r.budget-- == 0u) {
@@ -231,6 +98,7 @@ __device__ __forceinline__ bool ray_step(RayState &r, uint2 *stack, const Node8 
         }
         const uint4 *q = reinterpret_cast<const uint4 *>(nodes + node_idx);
         const uint4 q0 = __ldg(q), q1 = __ldg(q + 1), q2 = __ldg(q + 2), q3 = __ldg(q + 3), q4 = __ldg(q + 4);
+        if (kStats) (*n_nodes)++;
         const float sx = __uint_as_float((q0.w & 0xffu) << 23);
         const float sy = __uint_as_float(((q0.w >> 8) & 0xffu) << 23);
         const float sz = __uint_as_float(((q0.w >> 16) & 0xffu) << 23);
@@ -280,6 +148,7 @@ __device__ __forceinline__ bool ray_step(RayState &r, uint2 *stack, const Node8 
         tr.a = __ldg(tp);
         tr.b = __ldg(tp + 1);
         tr.c = __ldg(tp + 2);
+        if (kStats) (*n_tris)++;
         float th, bh, gh;
         if (shirley(tr, r.ox, r.oy, r.oz, r.dx, r.dy, r.dz, r.whi, th, bh, gh)) {
             r.best = (int)ti;
@@ -298,5 +167,33 @@ __device__ __forceinline__ bool ray_step(RayState &r, uint2 *stack, const Node8 
     }
     return false;
 }
+
+// Whole traversal of one ray (one ray per thread).
+template <bool kAnyHit, bool kStats>
+__device__ __forceinline__ void trace_one(const Node8 *__restrict__ nodes, const Tri *__restrict__ tris,
+                                          uint32_t n_nodes_total, uint32_t n_tris_total,
+                                          float4 o, float4 d, int &best, float &bt, float &bu, float &bv,
+                                          uint32_t *__restrict__ err, unsigned long long &n_nodes,
+                                          unsigned long long &n_tris)
+{
+    uint2 stack[kMaxStack];
+    RayState r;
+    ray_init(r, o, d, n_nodes_total);
+    while (!ray_step<kAnyHit, kStats>(r, stack, nodes, tris, n_nodes_total, n_tris_total, err, &n_nodes, &n_tris)) {
+    }
+    best = r.best;
+    bt = r.best >= 0 ? r.tcur : __int_as_float(0x7f800000);
+    bu = r.best >= 0 ? r.bu : 0.f;
+    bv = r.best >= 0 ? r.bv : 0.f;
+}
+
+// ---------------------------------------------------------------------------
+// Persistent traversal with dynamic ray fetch: each warp keeps its lanes busy
+// by handing a finished lane a new ray from a global counter whenever at least
+// kRefillLanes lanes are idle (Aila & Laine 2009, "Understanding the
+// efficiency of ray traversal on GPUs"). One loop iteration = one node visit
+// and the triangle tests it enables, so lanes stay in step on the same code.
+// ---------------------------------------------------------------------------
+constexpr uint32_t kRefillLanes = 8;
 
 }  // namespace ilg
