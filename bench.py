@@ -397,6 +397,11 @@ def main():
         alg_bytes = n_in * (RAY_IN + HIT_OUT)
     launch_s = (t_in / args.steps) / 1e3
     achieved = alg_bytes / launch_s / 1e9
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tp):  # DRAM bytes of one incoherent launch from the committed ncu capture
+        with open(tp) as f:
+            traffic = json.load(f).get("k_trace_dyn_incoherent_dram_bytes")
     if rank == 0:
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -413,7 +418,7 @@ def main():
                     "d2h_bytes_per_step": rays_per_step * HIT_OUT},
             "gpu_launches": 2 * args.steps,
             "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": hbm, "unit": "GB/s",
-                         "frac": round(achieved / hbm, 4), "traffic": None,
+                         "frac": round(achieved / hbm, 4), "traffic": traffic,
                          "kernel": "k_trace_dyn<closest> (incoherent launch)",
                          "peak_source": f"{peak_kind} hbm_gbs",
                          "alg_bytes_per_launch": int(alg_bytes),

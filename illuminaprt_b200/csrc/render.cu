@@ -279,14 +279,12 @@ __global__ void __launch_bounds__(256) k_shade(RenderDev R, int cur, uint32_t de
     float qf[kMlpRaw];
     uint32_t tslot = 0xffffffffu;  // training slot of this path
     uint32_t sid = 0;
-    float eps = 0.f;
 
     if (i < R.count[cur]) {
         path = R.q_path[cur][i];
         if (R.cache_depth) tslot = R.train_slot[path];
         sid = R.path_scene[path];
         const SceneRec &S = R.scenes[sid];
-        eps = S.eps;
         const float4 o = R.q_o[cur][i], d = R.q_d[cur][i];
         const int ti = R.hit_tri[i];
         uint64_t key;
