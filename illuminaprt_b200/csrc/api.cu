@@ -609,7 +609,7 @@ int ilg_mlp_init(ilg_ctx *ctx, uint32_t seed, float learning_rate)
     CK(cudaSetDevice(ctx->device));
     CK(ctx->mlp_w.reserve(kMlpParams)); CK(ctx->mlp_m.reserve(kMlpParams)); CK(ctx->mlp_v.reserve(kMlpParams));
     CK(ctx->mlp_grad.reserve(kMlpParams)); CK(ctx->mlp_loss.reserve(1));
-    CK(ctx->mlp_wf.reserve(kFwdElems)); CK(ctx->mlp_wb.reserve(kBwdElems));
+    CK(ctx->mlp_wf.reserve(kFwdElems)); CK(ctx->mlp_wb.reserve(kBwdElems)); CK(ctx->mlp_wu.reserve(kUmmaElems));
     CK(mlp_init(ctx->mlp_view(), seed, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     ctx->mlp_ready = true;
@@ -645,19 +645,24 @@ int ilg_mlp_infer(ilg_ctx *ctx, const float *raw, uint32_t n, float *out, uint32
     if (!ctx->mlp_ready) return fail(ctx, ILG_ESTATE, "ilg_mlp_infer: network not initialised");
     if (n == 0) return ILG_OK;
     if (!raw || !out) return fail(ctx, ILG_EINVAL, "ilg_mlp_infer: null array");
+    if (flags & ~(ILG_DEVICE_PTRS | ILG_MLP_WARP_MMA)) return fail(ctx, ILG_EINVAL, "ilg_mlp_infer: unknown flags");
     CK(cudaSetDevice(ctx->device));
     cudaStream_t st = ctx->stream;
+    const bool warp_mma = (flags & ILG_MLP_WARP_MMA) != 0;
+    auto run = [&](const float *r, float *o) {
+        return warp_mma ? mlp_infer_warp(ctx->mlp_view(), r, n, o, st) : mlp_infer(ctx->mlp_view(), r, n, o, st);
+    };
     if (flags & ILG_DEVICE_PTRS) {
-        CK(mlp_infer(ctx->mlp_view(), raw, n, out, st));
+        CK(run(raw, out));
         return ILG_OK;
     }
     CK(ctx->mlp_raw.reserve((size_t)n * kMlpRaw));
     CK(ctx->mlp_out.reserve((size_t)n * 3));
     CK(cudaMemcpyAsync(ctx->mlp_raw.ptr, raw, sizeof(float) * kMlpRaw * n, cudaMemcpyHostToDevice, st));
-    CK(mlp_infer(ctx->mlp_view(), ctx->mlp_raw.ptr, n, ctx->mlp_out.ptr, st));
+    CK(run(ctx->mlp_raw.ptr, ctx->mlp_out.ptr));
     CK(cudaMemcpyAsync(out, ctx->mlp_out.ptr, sizeof(float) * 3 * n, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
-    return ILG_OK;
+    return ctx->check_device_error();
 }
 
 static int mlp_grads_common(ilg_ctx *ctx, const float *raw, const float *target, uint32_t n, uint32_t flags,

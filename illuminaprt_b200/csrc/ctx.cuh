@@ -63,7 +63,7 @@ struct ilg_ctx {
 
     // radiance-cache network
     ilg::DevBuf<float> mlp_w, mlp_m, mlp_v, mlp_grad, mlp_loss, mlp_raw, mlp_tgt, mlp_out;
-    ilg::DevBuf<__nv_bfloat16> mlp_wf, mlp_wb, mlp_xcm, mlp_hcm, mlp_dzcm;
+    ilg::DevBuf<__nv_bfloat16> mlp_wf, mlp_wb, mlp_wu, mlp_xcm, mlp_hcm, mlp_dzcm;
     bool mlp_ready = false;
     uint32_t mlp_step = 0;
     float mlp_lr = 1e-2f;
@@ -72,7 +72,7 @@ struct ilg_ctx {
     {
         ilg::MlpDev M;
         M.w = mlp_w.ptr; M.m = mlp_m.ptr; M.v = mlp_v.ptr; M.grad = mlp_grad.ptr; M.loss = mlp_loss.ptr;
-        M.wf = mlp_wf.ptr; M.wb = mlp_wb.ptr; M.xcm = mlp_xcm.ptr; M.hcm = mlp_hcm.ptr; M.dzcm = mlp_dzcm.ptr;
+        M.wf = mlp_wf.ptr; M.wb = mlp_wb.ptr; M.wu = mlp_wu.ptr; M.err = derr.ptr; M.xcm = mlp_xcm.ptr; M.hcm = mlp_hcm.ptr; M.dzcm = mlp_dzcm.ptr;
         M.cap = (uint32_t)(mlp_xcm.cap / ilg::kMlpIn);
         return M;
     }
@@ -111,7 +111,7 @@ struct ilg_ctx {
         train_slot.release(); rec_of.release(); s_meta.release(); rec_feat.release(); rec_tgt.release();
         qry_feat.release(); qry_out.release(); rec_beta.release(); qry_beta.release();
         mlp_w.release(); mlp_m.release(); mlp_v.release(); mlp_grad.release(); mlp_loss.release();
-        mlp_raw.release(); mlp_tgt.release(); mlp_out.release(); mlp_wf.release(); mlp_wb.release();
+        mlp_raw.release(); mlp_tgt.release(); mlp_out.release(); mlp_wf.release(); mlp_wb.release(); mlp_wu.release();
         mlp_xcm.release(); mlp_hcm.release(); mlp_dzcm.release();
     }
 };

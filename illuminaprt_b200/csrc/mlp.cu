@@ -45,29 +45,6 @@ __device__ __forceinline__ void mma16816(float (&c)[4], const uint32_t (&a)[4], 
 
 __device__ __forceinline__ uint32_t ld_u32(const __nv_bfloat16 *p) { return *reinterpret_cast<const uint32_t *>(p); }
 
-// Encoded input columns (c, c+1), c even. Columns 0..71: for axis a and band
-// b, column 24a + 2b is sin(2^b pi x_a) and the next cos(2^b pi x_a);
-// 72..74 direction, 75..77 normal, 78 roughness, 79..81 albedo, 82 constant 1.
-__device__ __forceinline__ float2 encode_pair(const float *f, int c)
-{
-    if (c < 72) {
-        const int axis = c / 24, band = (c % 24) >> 1;
-        const float x = axis == 0 ? f[0] : (axis == 1 ? f[1] : f[2]);
-        float s, co;
-        sincospif(ldexpf(x, band), &s, &co);
-        return make_float2(s, co);
-    }
-    switch (c) {
-    case 72: return make_float2(f[3], f[4]);
-    case 74: return make_float2(f[5], f[6]);
-    case 76: return make_float2(f[7], f[8]);
-    case 78: return make_float2(f[9], f[10]);
-    case 80: return make_float2(f[11], f[12]);
-    case 82: return make_float2(1.f, 0.f);
-    default: return make_float2(0.f, 0.f);
-    }
-}
-
 // C[8 tiles of n8] += A[KB k16 blocks] x W^T, W given as [n][k] rows with `stride`
 template <int KB>
 __device__ __forceinline__ void layer64(const uint32_t (&a)[KB][4], const __nv_bfloat16 *w, int stride, int g, int tig,
@@ -369,6 +346,11 @@ __device__ __forceinline__ void write_copies(const MlpDev &M, int i, float w)
     const __nv_bfloat16 b = __float2bfloat16_rn(w);
     M.wf[fwd_off(l) + o * fwd_stride(l) + in] = b;
     if (l >= 1) M.wb[bwd_off(l) + in * bwd_stride(l) + o] = b;
+    if (M.wu) {
+        // element (n = o, k = in) of the K-major core-matrix layout
+        const int kc = mlp_in(l) / 8;
+        M.wu[umma_off(l) + (o / 8) * kc * 64 + (in / 8) * 64 + (o % 8) * 8 + (in % 8)] = b;
+    }
 }
 
 __device__ __forceinline__ float hash_uniform(uint32_t seed, uint32_t i)
@@ -445,6 +427,7 @@ cudaError_t mlp_init(const MlpDev &M, uint32_t seed, cudaStream_t st)
     cudaError_t e;
     if ((e = cudaMemsetAsync(M.wf, 0, kFwdElems * sizeof(__nv_bfloat16), st)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(M.wb, 0, kBwdElems * sizeof(__nv_bfloat16), st)) != cudaSuccess) return e;
+    if (M.wu && (e = cudaMemsetAsync(M.wu, 0, kUmmaElems * sizeof(__nv_bfloat16), st)) != cudaSuccess) return e;
     k_mlp_init<<<(kMlpParams + 255) / 256, 256, 0, st>>>(M, seed);
     return cudaGetLastError();
 }
@@ -457,6 +440,12 @@ cudaError_t mlp_refresh_copies(const MlpDev &M, cudaStream_t st)
 
 cudaError_t mlp_infer(const MlpDev &M, const float *raw, uint32_t n, float *out, cudaStream_t st,
                       const uint32_t *n_dev)
+{
+    return mlp_infer_tc(M, raw, n, out, st, n_dev, M.err);
+}
+
+cudaError_t mlp_infer_warp(const MlpDev &M, const float *raw, uint32_t n, float *out, cudaStream_t st,
+                           const uint32_t *n_dev)
 {
     if (n == 0) return cudaSuccess;
     const size_t smem = kFwdElems * sizeof(__nv_bfloat16);

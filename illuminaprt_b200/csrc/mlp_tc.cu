@@ -1,0 +1,259 @@
+// Radiance-cache inference on the 5th-generation tensor cores.
+//
+// One CTA of 128 threads owns 128 query rows at a time (one row per thread,
+// which is the TMEM lane the row's accumulator lives in). All six layers run
+// without leaving the CTA:
+//   * the weights (all layers, 46 KiB of BF16) sit in shared memory as W^T in
+//     the UMMA K-major no-swizzle layout: 8-row x 16-byte core matrices, the
+//     two K halves of one instruction 128 bytes apart (LBO), consecutive
+//     8-row groups K/8 x 128 bytes apart (SBO);
+//   * each thread writes its row's activations (the encoded input, then each
+//     hidden layer after ReLU and rounding to BF16) into a shared-memory A
+//     tile in the same layout;
+//   * one elected thread issues the layer's K/16 tcgen05.mma instructions
+//     (M = 128, N = 64 or 16, K = 16, BF16 x BF16 -> FP32 in TMEM) and
+//     commits them to an mbarrier;
+//   * every thread waits on the mbarrier (bounded), reads its row back from
+//     TMEM with tcgen05.ld, applies ReLU and writes the next A tile.
+// The TMEM accumulator (64 columns) is allocated once per CTA and freed on
+// exit; every wait has an iteration limit that raises an error bit instead of
+// hanging.
+#include "mlp.cuh"
+
+namespace ilg {
+
+namespace {
+
+constexpr int kTcRows = 128;
+constexpr uint32_t kTmemCols = 64;
+constexpr uint32_t kWaitLimit = 1u << 22;  // try_wait calls before giving up (seconds at most)
+constexpr uint32_t kErrWait = 64u;
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p)
+{
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// UMMA shared-memory matrix descriptor, K-major, no swizzle.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo_bytes, uint32_t sbo_bytes)
+{
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+    d |= (uint64_t)((lbo_bytes >> 4) & 0x3FFFu) << 16;
+    d |= (uint64_t)((sbo_bytes >> 4) & 0x3FFFu) << 32;
+    d |= (uint64_t)1 << 46;  // descriptor version for sm_100
+    // base offset 0, legacy LBO mode, layout type 0 = no swizzle
+    return d;
+}
+
+// Instruction descriptor: D = F32, A = B = BF16, both K-major, M x N.
+__host__ __device__ constexpr uint32_t umma_idesc(int m, int n)
+{
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc,
+                                         uint32_t accumulate)
+{
+    asm volatile(
+        "{\n\t"
+        ".reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t"
+        "}\n"
+        :
+        : "r"(tmem_d), "l"(da), "l"(db), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+__device__ __forceinline__ void mma_commit(uint32_t bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
+{
+    for (uint32_t it = 0; it < kWaitLimit; it++) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t"
+            ".reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t"
+            "}\n"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16])
+{
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+#pragma unroll
+    for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+__device__ __forceinline__ void fence_before_sync() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after_sync() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+__device__ __forceinline__ uint32_t pack2(float a, float b)
+{
+    __nv_bfloat162 v = __floats2bfloat162_rn(a, b);
+    return *reinterpret_cast<uint32_t *>(&v);
+}
+
+// 8 consecutive K values (one 16-byte core-matrix row) of row r at K chunk c
+__device__ __forceinline__ void put_chunk(unsigned char *a_tile, int r, int c, int k_total, const float *v)
+{
+    const int kc = k_total / 8;
+    uint4 q = make_uint4(pack2(v[0], v[1]), pack2(v[2], v[3]), pack2(v[4], v[5]), pack2(v[6], v[7]));
+    *reinterpret_cast<uint4 *>(a_tile + (size_t)(r / 8) * kc * 128 + (size_t)c * 128 + (r % 8) * 16) = q;
+}
+
+__global__ void __launch_bounds__(kTcRows) k_mlp_infer_tc(const __nv_bfloat16 *__restrict__ wu,
+                                                          const float *__restrict__ raw, uint32_t n,
+                                                          const uint32_t *__restrict__ n_dev,
+                                                          float *__restrict__ out, uint32_t *__restrict__ err)
+{
+    extern __shared__ __align__(1024) unsigned char smem[];
+    unsigned char *w_s = smem;                                         // kUmmaElems bf16
+    unsigned char *a_s = smem + ((kUmmaElems * 2 + 1023) / 1024) * 1024;  // 128 x 96 bf16
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ uint32_t tmem_base_s;
+
+    if (n_dev) n = min(n, *n_dev);
+    const int tid = threadIdx.x, warp = tid >> 5;
+    // weights -> shared memory (16-byte vectors)
+    {
+        const uint4 *src = reinterpret_cast<const uint4 *>(wu);
+        uint4 *dst = reinterpret_cast<uint4 *>(w_s);
+        for (int i = tid; i < kUmmaElems / 8; i += kTcRows) dst[i] = src[i];
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_s)),
+                     "r"(kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bar)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    fence_async_smem();
+    fence_before_sync();
+    __syncthreads();
+    fence_after_sync();
+    const uint32_t tmem = tmem_base_s;
+    const uint32_t bar_a = smem_u32(&bar);
+    const uint32_t w_a = smem_u32(w_s), a_a = smem_u32(a_s);
+    uint32_t phase = 0;
+    bool ok = true;
+
+    const uint32_t n_tiles = (n + kTcRows - 1) / kTcRows;
+    for (uint32_t tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x) {
+        const uint32_t row = tile * kTcRows + tid;
+        // encoded input row -> A tile (K = 96)
+        {
+            float f[kMlpRaw];
+#pragma unroll
+            for (int k = 0; k < kMlpRaw; k++) f[k] = row < n ? raw[(size_t)row * kMlpRaw + k] : 0.f;
+#pragma unroll
+            for (int c = 0; c < kMlpIn / 8; c++) {
+                float v[8];
+#pragma unroll
+                for (int e = 0; e < 8; e += 2) {
+                    const float2 p = encode_pair(f, 8 * c + e);
+                    v[e] = row < n ? p.x : 0.f;
+                    v[e + 1] = row < n ? p.y : 0.f;
+                }
+                put_chunk(a_s, tid, c, kMlpIn, v);
+            }
+        }
+#pragma unroll 1
+        for (int l = 0; l < kMlpLayers; l++) {
+            const int K = mlp_in(l), N = umma_n(l);
+            fence_async_smem();
+            fence_before_sync();
+            __syncthreads();
+            fence_after_sync();
+            if (tid == 0) {
+                const uint32_t idesc = umma_idesc(kTcRows, N);
+                for (int s = 0; s < K / 16; s++) {
+                    // K step s covers core-matrix chunks 2s, 2s+1
+                    const uint64_t da = umma_desc(a_a + s * 256, 128, (K / 8) * 128);
+                    const uint64_t db = umma_desc(w_a + umma_off(l) * 2 + s * 256, 128, (K / 8) * 128);
+                    mma_bf16(tmem, da, db, idesc, s > 0 ? 1u : 0u);
+                }
+                mma_commit(bar_a);
+            }
+            const bool waited = mbar_wait(bar_a, phase);
+            if (!waited) atomicOr(err, kErrWait);
+            ok = __syncthreads_and(waited) != 0;  // every thread leaves together
+            if (!ok) break;
+            phase ^= 1u;
+            fence_after_sync();
+            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16);
+            if (l < kMlpLayers - 1) {
+#pragma unroll
+                for (int q = 0; q < 4; q++) {
+                    float v[16];
+                    tmem_ld16(taddr + q * 16, v);
+                    tmem_wait_ld();
+#pragma unroll
+                    for (int e = 0; e < 16; e++) v[e] = fmaxf(v[e], 0.f);
+                    put_chunk(a_s, tid, 2 * q, kMlpHid, v);
+                    put_chunk(a_s, tid, 2 * q + 1, kMlpHid, v + 8);
+                }
+            } else {
+                float v[16];
+                tmem_ld16(taddr, v);
+                tmem_wait_ld();
+                if (row < n) {
+                    out[(size_t)row * 3] = v[0];
+                    out[(size_t)row * 3 + 1] = v[1];
+                    out[(size_t)row * 3 + 2] = v[2];
+                }
+            }
+        }
+    }
+    fence_before_sync();
+    __syncthreads();
+    fence_after_sync();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+}
+
+}  // namespace
+
+cudaError_t mlp_infer_tc(const MlpDev &M, const float *raw, uint32_t n, float *out, cudaStream_t st,
+                         const uint32_t *n_dev, uint32_t *err)
+{
+    if (n == 0) return cudaSuccess;
+    const size_t smem = ((kUmmaElems * 2 + 1023) / 1024) * 1024 + (size_t)kTcRows * kMlpIn * 2;
+    static bool attr = false;
+    if (!attr) {
+        cudaError_t e =
+            cudaFuncSetAttribute(k_mlp_infer_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const uint32_t tiles = (n + kTcRows - 1) / kTcRows;
+    const uint32_t grid = tiles < (uint32_t)sms * 3u ? tiles : (uint32_t)sms * 3u;
+    k_mlp_infer_tc<<<grid, kTcRows, smem, st>>>(M.wu, raw, n, n_dev, out, err);
+    return cudaGetLastError();
+}
+
+}  // namespace ilg

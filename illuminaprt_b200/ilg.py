@@ -31,6 +31,7 @@ EXPORTED = ["ilg_create", "ilg_destroy", "ilg_last_error", "ilg_set_mesh", "ilg_
             "ilg_mlp_train_step", "ilg_render_batch"]
 
 ILG_MLP_RAW = 16
+ILG_MLP_WARP_MMA = 0x10
 ILG_MLP_PARAMS = 23040
 
 # Largest batch ilg_intersect_noalloc accepts (include/ilg.h).
@@ -284,10 +285,12 @@ class GpuSpace:
         assert p.size == ILG_MLP_PARAMS
         self._check(self.L.ilg_mlp_set_params(self.h, p.ctypes.data))
 
-    def mlp_infer(self, raw) -> np.ndarray:
+    def mlp_infer(self, raw, warp_mma: bool = False) -> np.ndarray:
+        """Cache network outputs (tcgen05 tensor cores; warp_mma selects the mma.sync kernel)."""
         raw = np.ascontiguousarray(raw, np.float32).reshape(-1, ILG_MLP_RAW)
         out = np.empty((raw.shape[0], 3), np.float32)
-        self._check(self.L.ilg_mlp_infer(self.h, raw.ctypes.data, raw.shape[0], out.ctypes.data, 0))
+        self._check(self.L.ilg_mlp_infer(self.h, raw.ctypes.data, raw.shape[0], out.ctypes.data,
+                                         ILG_MLP_WARP_MMA if warp_mma else 0))
         return out
 
     def mlp_grads(self, raw, target):

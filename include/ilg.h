@@ -190,7 +190,10 @@ int ilg_render(ilg_ctx *ctx, const ilg_camera *cam, const ilg_render_opts *opts,
 int ilg_mlp_init(ilg_ctx *ctx, uint32_t seed, float learning_rate);
 int ilg_mlp_get_params(ilg_ctx *ctx, float *params /* ILG_MLP_PARAMS */);
 int ilg_mlp_set_params(ilg_ctx *ctx, const float *params);
-/* out: n x 3 radiance. Host pointers unless ILG_DEVICE_PTRS. */
+/* out: n x 3 radiance. Host pointers unless ILG_DEVICE_PTRS. Runs on the
+ * tcgen05 tensor cores (accumulators in TMEM); ILG_MLP_WARP_MMA selects the
+ * warp-level mma.sync kernel that training's forward pass uses instead. */
+#define ILG_MLP_WARP_MMA 0x10u
 int ilg_mlp_infer(ilg_ctx *ctx, const float *raw, uint32_t n, float *out, uint32_t flags);
 /* Gradient of the mean relative L2 loss over the batch (no update). */
 int ilg_mlp_grads(ilg_ctx *ctx, const float *raw, const float *target, uint32_t n, float *grad /* ILG_MLP_PARAMS */,

@@ -68,3 +68,21 @@ def test_training_fits_a_smooth_field():
     print(f"training: loss {losses[0]:.4f} -> {losses[-1]:.5f}; held-out relative L2 {rel:.5f}")
     assert losses[-1] < losses[0] / 20
     assert rel < 0.01
+
+
+@pytest.mark.parametrize("n", [1, 127, 128, 129, 70000])
+def test_tcgen05_inference_matches_warp_mma(net, n):
+    """The tcgen05 (TMEM-accumulating) inference kernel against the warp-level
+    mma.sync kernel and the oracle, on ragged row counts."""
+    raw, tgt = mo.random_batch(max(n, 1), seed=n + 5)
+    for _ in range(3):  # move the weights away from their initial values
+        net.mlp_train_step(raw[:4096], tgt[:4096])
+    y_tc = net.mlp_infer(raw)
+    y_warp = net.mlp_infer(raw, warp_mma=True)
+    y_ref, _, _ = mo.forward(net.mlp_params(), raw, bf=True)
+    scale = np.abs(y_ref).max() + 1e-6
+    d_warp = np.abs(y_tc - y_warp).max() / scale
+    d_ref = np.abs(y_tc - y_ref).max() / scale
+    print(f"n={n}: tcgen05 vs mma.sync {d_warp:.2e}, vs oracle {d_ref:.2e}")
+    assert d_warp < 1e-2 and d_ref < 1e-2
+    assert np.mean(np.abs(y_tc - y_warp)) / (np.mean(np.abs(y_warp)) + 1e-9) < 2e-3
