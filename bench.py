@@ -206,7 +206,7 @@ def cpu_baseline_sample(pos, idx, co, cd, io, idr, seconds=10.0):
                       f"{dt:.1f} s on {nthreads} threads"}
 
 
-def bench_path_tracer(dev, local, quick=False):
+def bench_path_tracer(dev, local, legs=("box", "field", "mlp", "batch")):
     """Samples/s of the wavefront path tracer on the box scene (256^2, 16 spp,
     depth 6) and on the icosphere field (1920x1080, 64 spp, depth 12;
     64 spheres x 327,680 triangles + ground + 4 lights = 20,971,530 triangles)."""
@@ -231,8 +231,19 @@ def bench_path_tracer(dev, local, quick=False):
     res["pt_box_256x256x16spp_ms"] = round(ms, 3)
     res["pt_box_msamples_s"] = round(256 * 256 * 16 / (ms / 1e3) / 1e6, 3)
     sp.close()
-    if quick:
-        return res
+    if "field" in legs:
+        bench_field(res, dev, local, e0, e1)
+    if "mlp" in legs:
+        bench_mlp(res, dev, local, e0, e1)
+    if "batch" in legs:
+        bench_batch(res, local)
+    return res
+
+
+def bench_field(res, dev, local, e0, e1):
+    import torch
+    from illuminaprt_b200 import scenes
+    from illuminaprt_b200.ilg import GpuSpace
     field = scenes.sphere_field(8, 7, seed=3)
     sp = GpuSpace(device=local)
     scenes.load_sphere_field(sp, field)
@@ -251,7 +262,36 @@ def bench_path_tracer(dev, local, quick=False):
     res["pt_field_1080p_64spp_ms"] = round(ms, 2)
     res["pt_field_msamples_s"] = round(W * H * spp / (ms / 1e3) / 1e6, 3)
     sp.close()
-    # 32 independent scenes of uneven size in one wavefront, autotuned
+
+
+def bench_mlp(res, dev, local, e0, e1):
+    """Cache-network inference: 2,097,152 queries, tcgen05 kernel vs mma.sync."""
+    import torch
+    from illuminaprt_b200.ilg import GpuSpace
+    nq = 1 << 21
+    q = torch.rand((nq, 16), device=dev)
+    yq = torch.empty((nq, 3), device=dev)
+    sp = GpuSpace(device=local)
+    sp.mlp_init(seed=1)
+    st = torch.cuda.ExternalStream(sp.stream, device=dev)
+    for flag, key in ((0, "tcgen05"), (0x10, "mma_sync")):
+        sp.L.ilg_mlp_infer(sp.h, q.data_ptr(), nq, yq.data_ptr(), 0x1 | flag)
+        sp.sync()
+        e0.record(st)
+        for _ in range(10):
+            sp.L.ilg_mlp_infer(sp.h, q.data_ptr(), nq, yq.data_ptr(), 0x1 | flag)
+        e1.record(st)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / 10
+        res[f"mlp_infer_{key}_mqueries_s"] = round(nq / (ms / 1e3) / 1e6, 1)
+        res[f"mlp_infer_{key}_tflops"] = round(nq * 45440 / (ms / 1e3) / 1e12, 2)
+    sp.close()
+
+
+def bench_batch(res, local):
+    """32 independent scenes of uneven size in one wavefront, autotuned."""
+    from illuminaprt_b200 import scenes
+    from illuminaprt_b200.ilg import GpuSpace
     from illuminaprt_b200.autotune import tune_batch
     items = scenes.batch_workload(32, seed=9)
     spaces, batch = [], []
@@ -286,6 +326,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-path-tracer", action="store_true")
+    ap.add_argument("--legs", default="box,field,mlp,batch",
+                    help="extra measurements after the ray query: box,field,mlp,batch")
     args = ap.parse_args()
     world, rank, local = dist_setup()
 
@@ -386,7 +428,7 @@ def main():
     # the e2e hits must equal the device-resident ones
     assert torch.equal(hout["incoherent"][0], out["incoherent"][0].cpu())
 
-    pt = {} if args.no_path_tracer else bench_path_tracer(dev, local)
+    pt = {} if args.no_path_tracer else bench_path_tracer(dev, local, tuple(args.legs.split(",")))
     hbm, peak_kind = load_peaks()
     # algorithmic bytes of one incoherent launch (the dominant kernel): rays in,
     # hits out, and every node / triangle record the traversal reads
