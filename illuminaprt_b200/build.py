@@ -53,5 +53,22 @@ def build(force: bool = False, verbose: bool = False, ptxas_v: bool = False) -> 
     return LIB
 
 
+PLUGIN_DIR = os.path.join(PKG, "plugin")
+PLUGIN = os.path.join(PLUGIN_DIR, "libilg_gpuspace.so")
+REF_CORE = os.environ.get("ILLUMINA_CORE", "/root/reference/Core")
+
+
+def build_plugin() -> str | None:
+    """Build the GpuSpace engine plug-in (plugin/libilg_gpuspace.so) against the
+    engine's headers in REF_CORE; returns its path, or None when the headers
+    are not on this machine (a plug-in built elsewhere is used as it is)."""
+    if not os.path.isdir(os.path.join(REF_CORE, "Space")):
+        return PLUGIN if os.path.exists(PLUGIN) else None
+    build()
+    subprocess.run(["make", "-s", "-C", PLUGIN_DIR, f"REF={REF_CORE}"], check=True)
+    return PLUGIN
+
+
 if __name__ == "__main__":
     build(force="--force" in sys.argv, verbose=True, ptxas_v="--ptxas-v" in sys.argv)
+    build_plugin()

@@ -260,6 +260,73 @@ int ilg_occluded(ilg_ctx *ctx, const float *ray_o_tmin, const float *ray_d_tmax,
     return ctx->check_device_error();
 }
 
+int ilg_intersect_excluding(ilg_ctx *ctx, const float *ray_o_tmin, const float *ray_d_tmax, uint32_t n,
+                            uint32_t skip_first, uint32_t skip_count, int32_t *prim, float *t, float *u, float *v,
+                            uint32_t flags)
+{
+    if (!ctx) return ILG_EINVAL;
+    if (flags & ~ILG_DEVICE_PTRS) return fail(ctx, ILG_EINVAL, "ilg_intersect_excluding: unknown flags 0x%x", flags);
+    if (!ctx->built) return fail(ctx, ILG_ESTATE, "ilg_intersect_excluding: scene not built");
+    if (n == 0) return ILG_OK;
+    if (!ray_o_tmin || !ray_d_tmax || !prim || !t || !u || !v)
+        return fail(ctx, ILG_EINVAL, "ilg_intersect_excluding: null array");
+    if (((uintptr_t)ray_o_tmin | (uintptr_t)ray_d_tmax) & 15u)
+        return fail(ctx, ILG_EINVAL, "ilg_intersect_excluding: ray arrays must be 16-byte aligned");
+    CK(cudaSetDevice(ctx->device));
+    const SceneView sv = ctx->view();
+    cudaStream_t st = ctx->stream;
+    if (flags & ILG_DEVICE_PTRS) {
+        CK(launch_closest_skip(sv, (const float4 *)ray_o_tmin, (const float4 *)ray_d_tmax, n, skip_first, skip_count,
+                               prim, t, u, v, ctx->derr.ptr, st));
+        return ILG_OK;
+    }
+    CK(ctx->ro.reserve(n));
+    CK(ctx->rd.reserve(n));
+    CK(ctx->hprim.reserve(n));
+    CK(ctx->ht.reserve(n));
+    CK(ctx->hu.reserve(n));
+    CK(ctx->hv.reserve(n));
+    CK(cudaMemcpyAsync(ctx->ro.ptr, ray_o_tmin, 16ull * n, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(ctx->rd.ptr, ray_d_tmax, 16ull * n, cudaMemcpyHostToDevice, st));
+    CK(launch_closest_skip(sv, ctx->ro.ptr, ctx->rd.ptr, n, skip_first, skip_count, ctx->hprim.ptr, ctx->ht.ptr,
+                           ctx->hu.ptr, ctx->hv.ptr, ctx->derr.ptr, st));
+    CK(cudaMemcpyAsync(prim, ctx->hprim.ptr, 4ull * n, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(t, ctx->ht.ptr, 4ull * n, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(u, ctx->hu.ptr, 4ull * n, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(v, ctx->hv.ptr, 4ull * n, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return ctx->check_device_error();
+}
+
+int ilg_occluded_excluding(ilg_ctx *ctx, const float *ray_o_tmin, const float *ray_d_tmax, uint32_t n,
+                           uint32_t skip_first, uint32_t skip_count, uint8_t *occ, uint32_t flags)
+{
+    if (!ctx) return ILG_EINVAL;
+    if (flags & ~ILG_DEVICE_PTRS) return fail(ctx, ILG_EINVAL, "ilg_occluded_excluding: unknown flags 0x%x", flags);
+    if (!ctx->built) return fail(ctx, ILG_ESTATE, "ilg_occluded_excluding: scene not built");
+    if (n == 0) return ILG_OK;
+    if (!ray_o_tmin || !ray_d_tmax || !occ) return fail(ctx, ILG_EINVAL, "ilg_occluded_excluding: null array");
+    if (((uintptr_t)ray_o_tmin | (uintptr_t)ray_d_tmax) & 15u)
+        return fail(ctx, ILG_EINVAL, "ilg_occluded_excluding: ray arrays must be 16-byte aligned");
+    CK(cudaSetDevice(ctx->device));
+    const SceneView sv = ctx->view();
+    cudaStream_t st = ctx->stream;
+    if (flags & ILG_DEVICE_PTRS) {
+        CK(launch_any_skip(sv, (const float4 *)ray_o_tmin, (const float4 *)ray_d_tmax, n, skip_first, skip_count, occ,
+                           ctx->derr.ptr, st));
+        return ILG_OK;
+    }
+    CK(ctx->ro.reserve(n));
+    CK(ctx->rd.reserve(n));
+    CK(ctx->hocc.reserve(n));
+    CK(cudaMemcpyAsync(ctx->ro.ptr, ray_o_tmin, 16ull * n, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(ctx->rd.ptr, ray_d_tmax, 16ull * n, cudaMemcpyHostToDevice, st));
+    CK(launch_any_skip(sv, ctx->ro.ptr, ctx->rd.ptr, n, skip_first, skip_count, ctx->hocc.ptr, ctx->derr.ptr, st));
+    CK(cudaMemcpyAsync(occ, ctx->hocc.ptr, n, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return ctx->check_device_error();
+}
+
 }  // extern "C"
 
 // ---------------------------------------------------------------------------

@@ -8,14 +8,15 @@ namespace ilg {
 
 namespace {
 
-template <bool kStats>
+template <bool kStats, bool kSkip = false>
 __global__ void __launch_bounds__(128) k_closest(const Node8 *__restrict__ nodes, const Tri *__restrict__ tris,
                                                  const uint32_t *__restrict__ prim_of, uint32_t n_nodes_total,
                                                  uint32_t n_tris_total,
                                                  const float4 *__restrict__ ro, const float4 *__restrict__ rd,
                                                  uint32_t n, int32_t *__restrict__ prim, float *__restrict__ tout,
                                                  float *__restrict__ uout, float *__restrict__ vout,
-                                                 uint32_t *__restrict__ err, unsigned long long *__restrict__ stats)
+                                                 uint32_t *__restrict__ err, unsigned long long *__restrict__ stats,
+                                                 uint32_t skip_lo = 0, uint32_t skip_n = 0)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -23,7 +24,8 @@ __global__ void __launch_bounds__(128) k_closest(const Node8 *__restrict__ nodes
     int best;
     float bt, bu, bv;
     unsigned long long nn = 0, nt = 0;
-    trace_one<false, kStats>(nodes, tris, n_nodes_total, n_tris_total, o, d, best, bt, bu, bv, err, nn, nt);
+    trace_one<false, kStats, kSkip>(nodes, tris, n_nodes_total, n_tris_total, o, d, best, bt, bu, bv, err, nn, nt,
+                                    Skip{prim_of, skip_lo, skip_n});
     __stcs(prim + i, best >= 0 ? (int32_t)__ldg(prim_of + best) : (best == -2 ? -2 : -1));
     __stcs(tout + i, bt);
     __stcs(uout + i, bu);
@@ -34,10 +36,13 @@ __global__ void __launch_bounds__(128) k_closest(const Node8 *__restrict__ nodes
     }
 }
 
+template <bool kSkip = false>
 __global__ void __launch_bounds__(128) k_any(const Node8 *__restrict__ nodes, const Tri *__restrict__ tris,
                                              uint32_t n_nodes_total, uint32_t n_tris_total,
                                              const float4 *__restrict__ ro, const float4 *__restrict__ rd,
-                                             uint32_t n, uint8_t *__restrict__ occ, uint32_t *__restrict__ err)
+                                             uint32_t n, uint8_t *__restrict__ occ, uint32_t *__restrict__ err,
+                                             const uint32_t *__restrict__ prim_of = nullptr, uint32_t skip_lo = 0,
+                                             uint32_t skip_n = 0)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
@@ -45,7 +50,8 @@ __global__ void __launch_bounds__(128) k_any(const Node8 *__restrict__ nodes, co
     int best;
     float bt, bu, bv;
     unsigned long long nn = 0, nt = 0;
-    trace_one<true, false>(nodes, tris, n_nodes_total, n_tris_total, o, d, best, bt, bu, bv, err, nn, nt);
+    trace_one<true, false, kSkip>(nodes, tris, n_nodes_total, n_tris_total, o, d, best, bt, bu, bv, err, nn, nt,
+                                  Skip{prim_of, skip_lo, skip_n});
     occ[i] = best >= 0 ? 1 : 0;
 }
 
@@ -153,7 +159,28 @@ cudaError_t launch_any(const SceneView &s, const float4 *ro, const float4 *rd, u
 {
     if (n == 0) return cudaSuccess;
     const uint32_t T = 128;
-    k_any<<<(n + T - 1) / T, T, 0, st>>>(s.nodes, s.tris, s.n_nodes, s.n_tris, ro, rd, n, occ, err);
+    k_any<false><<<(n + T - 1) / T, T, 0, st>>>(s.nodes, s.tris, s.n_nodes, s.n_tris, ro, rd, n, occ, err);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_closest_skip(const SceneView &s, const float4 *ro, const float4 *rd, uint32_t n,
+                                uint32_t skip_lo, uint32_t skip_n, int32_t *prim, float *t, float *u, float *v,
+                                uint32_t *err, cudaStream_t st)
+{
+    if (n == 0) return cudaSuccess;
+    const uint32_t T = 128;
+    k_closest<false, true><<<(n + T - 1) / T, T, 0, st>>>(s.nodes, s.tris, s.prim_of, s.n_nodes, s.n_tris, ro, rd, n,
+                                                          prim, t, u, v, err, nullptr, skip_lo, skip_n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_any_skip(const SceneView &s, const float4 *ro, const float4 *rd, uint32_t n, uint32_t skip_lo,
+                            uint32_t skip_n, uint8_t *occ, uint32_t *err, cudaStream_t st)
+{
+    if (n == 0) return cudaSuccess;
+    const uint32_t T = 128;
+    k_any<true><<<(n + T - 1) / T, T, 0, st>>>(s.nodes, s.tris, s.n_nodes, s.n_tris, ro, rd, n, occ, err, s.prim_of,
+                                               skip_lo, skip_n);
     return cudaGetLastError();
 }
 

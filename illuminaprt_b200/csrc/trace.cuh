@@ -26,6 +26,14 @@ struct TraceStats {
     unsigned long long nodes, tris;
 };
 
+// Input triangles [lo, lo + n) that a query ignores (the reference's
+// `p_pExclude` primitive after its triangles were flattened into one range);
+// prim_of maps a triangle record to its input index.
+struct Skip {
+    const uint32_t *prim_of;
+    uint32_t lo, n;
+};
+
 // ---------------------------------------------------------------------------
 // Traversal state machine shared by every kernel
 // ---------------------------------------------------------------------------
@@ -67,11 +75,11 @@ __device__ __forceinline__ void ray_init(RayState &r, float4 o, float4 d, uint32
 
 // One traversal step. Returns true when the ray is finished (r.best is the
 // hit record, -1 for a miss, -2 for a reported error).
-template <bool kAnyHit, bool kStats = false>
+template <bool kAnyHit, bool kStats = false, bool kSkip = false>
 __device__ __forceinline__ bool ray_step(RayState &r, uint2 *stack, const Node8 *__restrict__ nodes,
                                          const Tri *__restrict__ tris, uint32_t n_nodes_total, uint32_t n_tris_total,
                                          uint32_t *__restrict__ err, unsigned long long *n_nodes = nullptr,
-                                         unsigned long long *n_tris = nullptr)
+                                         unsigned long long *n_tris = nullptr, Skip skip = Skip{nullptr, 0u, 0u})
 {
     if (r.ng_hits & 0xff000000u) {
         if (r.budget-- == 0u) {
@@ -143,6 +151,7 @@ __device__ __forceinline__ bool ray_step(RayState &r, uint2 *stack, const Node8 
             r.best = -2;
             return true;
         }
+        if (kSkip && __ldg(skip.prim_of + ti) - skip.lo < skip.n) continue;
         const float4 *tp = reinterpret_cast<const float4 *>(tris + ti);
         Tri tr;
         tr.a = __ldg(tp);
@@ -169,17 +178,18 @@ __device__ __forceinline__ bool ray_step(RayState &r, uint2 *stack, const Node8 
 }
 
 // Whole traversal of one ray (one ray per thread).
-template <bool kAnyHit, bool kStats>
+template <bool kAnyHit, bool kStats, bool kSkip = false>
 __device__ __forceinline__ void trace_one(const Node8 *__restrict__ nodes, const Tri *__restrict__ tris,
                                           uint32_t n_nodes_total, uint32_t n_tris_total,
                                           float4 o, float4 d, int &best, float &bt, float &bu, float &bv,
                                           uint32_t *__restrict__ err, unsigned long long &n_nodes,
-                                          unsigned long long &n_tris)
+                                          unsigned long long &n_tris, Skip skip = Skip{nullptr, 0u, 0u})
 {
     uint2 stack[kMaxStack];
     RayState r;
     ray_init(r, o, d, n_nodes_total);
-    while (!ray_step<kAnyHit, kStats>(r, stack, nodes, tris, n_nodes_total, n_tris_total, err, &n_nodes, &n_tris)) {
+    while (!ray_step<kAnyHit, kStats, kSkip>(r, stack, nodes, tris, n_nodes_total, n_tris_total, err, &n_nodes,
+                                             &n_tris, skip)) {
     }
     best = r.best;
     bt = r.best >= 0 ? r.tcur : __int_as_float(0x7f800000);

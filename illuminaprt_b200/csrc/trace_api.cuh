@@ -20,6 +20,13 @@ cudaError_t launch_closest(const SceneView &s, const float4 *ro, const float4 *r
 cudaError_t launch_any(const SceneView &s, const float4 *ro, const float4 *rd, uint32_t n, uint8_t *occ,
                        uint32_t *err, cudaStream_t st);
 
+// Queries that ignore the input triangles [skip_lo, skip_lo + skip_n).
+cudaError_t launch_closest_skip(const SceneView &s, const float4 *ro, const float4 *rd, uint32_t n,
+                                uint32_t skip_lo, uint32_t skip_n, int32_t *prim, float *t, float *u, float *v,
+                                uint32_t *err, cudaStream_t st);
+cudaError_t launch_any_skip(const SceneView &s, const float4 *ro, const float4 *rd, uint32_t n, uint32_t skip_lo,
+                            uint32_t skip_n, uint8_t *occ, uint32_t *err, cudaStream_t st);
+
 // Persistent variants with dynamic ray fetch; `next` is a device counter word.
 cudaError_t launch_closest_dyn(const SceneView &s, const float4 *ro, const float4 *rd, uint32_t n, int32_t *prim,
                                float *t, float *u, float *v, uint32_t *next, uint32_t *err, cudaStream_t st);

@@ -28,7 +28,7 @@ EXPORTED = ["ilg_create", "ilg_destroy", "ilg_last_error", "ilg_set_mesh", "ilg_
             "ilg_intersect", "ilg_intersect_counted", "ilg_occluded", "ilg_sync", "ilg_stream",
             "ilg_set_materials", "ilg_set_quad_lights", "ilg_render", "ilg_intersect_noalloc",
             "ilg_mlp_init", "ilg_mlp_get_params", "ilg_mlp_set_params", "ilg_mlp_infer", "ilg_mlp_grads",
-            "ilg_mlp_train_step", "ilg_render_batch"]
+            "ilg_mlp_train_step", "ilg_render_batch", "ilg_intersect_excluding", "ilg_occluded_excluding"]
 
 ILG_MLP_RAW = 16
 ILG_MLP_WARP_MMA = 0x10
@@ -119,6 +119,8 @@ def load(build_if_missing: bool = True) -> ctypes.CDLL:
     L.ilg_set_quad_lights.argtypes = [vp, vp, u32]
     L.ilg_render.argtypes = [vp, ctypes.POINTER(ilg_camera), ctypes.POINTER(ilg_render_opts), vp, u32]
     L.ilg_intersect_noalloc.argtypes = [vp, vp, vp, u32, vp, vp, vp, vp]
+    L.ilg_intersect_excluding.argtypes = [vp, vp, vp, u32, u32, u32, vp, vp, vp, vp, u32]
+    L.ilg_occluded_excluding.argtypes = [vp, vp, vp, u32, u32, u32, vp, u32]
     L.ilg_intersect_noalloc.restype = i32
     L.ilg_mlp_init.argtypes = [vp, u32, ctypes.c_float]
     L.ilg_mlp_get_params.argtypes = [vp, vp]
@@ -222,6 +224,26 @@ class GpuSpace:
         d4 = np.ascontiguousarray(d4, np.float32)
         occ = np.empty(o4.shape[0], np.uint8)
         self._check(self.L.ilg_occluded(self.h, o4.ctypes.data, d4.ctypes.data, o4.shape[0], occ.ctypes.data, 0))
+        return occ
+
+    # ISpace::Intersects(ray, isect, p_pExclude) / Intersects(ray, p_pExclude),
+    # batched: input triangles [first, first + count) are ignored
+    def intersects_excluding(self, o4: np.ndarray, d4: np.ndarray, first: int, count: int):
+        o4 = np.ascontiguousarray(o4, np.float32)
+        d4 = np.ascontiguousarray(d4, np.float32)
+        n = o4.shape[0]
+        prim = np.empty(n, np.int32)
+        t, u, v = (np.empty(n, np.float32) for _ in range(3))
+        self._check(self.L.ilg_intersect_excluding(self.h, o4.ctypes.data, d4.ctypes.data, n, first, count,
+                                                   prim.ctypes.data, t.ctypes.data, u.ctypes.data, v.ctypes.data, 0))
+        return prim, t, u, v
+
+    def occluded_excluding(self, o4: np.ndarray, d4: np.ndarray, first: int, count: int) -> np.ndarray:
+        o4 = np.ascontiguousarray(o4, np.float32)
+        d4 = np.ascontiguousarray(d4, np.float32)
+        occ = np.empty(o4.shape[0], np.uint8)
+        self._check(self.L.ilg_occluded_excluding(self.h, o4.ctypes.data, d4.ctypes.data, o4.shape[0], first, count,
+                                                  occ.ctypes.data, 0))
         return occ
 
     def occluded_into(self, o4, d4, occ, device_ptrs: bool):

@@ -1,12 +1,12 @@
 // Replacement for the reference's System/ArgumentMap.h, found first on the
-// include path when the oracle compiles the reference sources.
+// include path when the engine headers are compiled here (the GPU space plug-in
+// and the CPU checker built from the reference sources).
 //
 // Why: the reference's ArgumentMap (Core/System/ArgumentMap.h:243-258)
 // returns a std::istream expression from a bool function, which C++11 and
-// later reject, and it needs boost::tokenizer. The oracle harness builds its
-// objects with explicit constructors, never through the string-keyed
-// factories, so this stand-in only has to let the headers that name the class
-// compile: a "Key=Value;Key=Value" map with streamed lookups.
+// later reject, and it needs boost::tokenizer. This stand-in keeps the class
+// name and its typed lookups (GetArgument) over a "Key=Value;Key=Value" map,
+// which is all the factories built here use.
 #pragma once
 
 #include <map>

@@ -1,5 +1,6 @@
 // Replacement for the reference's Threading/Atomic.h, found first on the
-// include path when the oracle compiles the reference sources.
+// include path when the engine headers are compiled here (the GPU space plug-in
+// and the CPU checker built from the reference sources).
 //
 // Why: on GCC the reference's AtomicInt32::Exchange / AtomicInt64::Exchange
 // (Core/Threading/Atomic.h:200-212 and :395-405) loop while the CAS

@@ -106,6 +106,19 @@ int ilg_intersect_noalloc(ilg_ctx *ctx, const float *ray_o_tmin, const float *ra
 int ilg_occluded(ilg_ctx *ctx, const float *ray_o_tmin, const float *ray_d_tmax, uint32_t n,
                  uint8_t *occ, uint32_t flags);
 
+/* Closest hit / any hit that ignore the input triangles [skip_first,
+ * skip_first + skip_count): the reference's `p_pExclude` overloads,
+ * ISpace::Intersects(const Ray&, Intersection&, IPrimitive*) and
+ * ISpace::Intersects(const Ray&, IPrimitive*) (Core/Space/Space.h:39,41,
+ * BasicSpace.cpp:75-91,104-115), once a primitive's triangles occupy one
+ * contiguous range of the mesh given to ilg_set_mesh. Same arguments and
+ * results as ilg_intersect / ilg_occluded otherwise. */
+int ilg_intersect_excluding(ilg_ctx *ctx, const float *ray_o_tmin, const float *ray_d_tmax, uint32_t n,
+                            uint32_t skip_first, uint32_t skip_count, int32_t *prim, float *t, float *u,
+                            float *v, uint32_t flags);
+int ilg_occluded_excluding(ilg_ctx *ctx, const float *ray_o_tmin, const float *ray_d_tmax, uint32_t n,
+                           uint32_t skip_first, uint32_t skip_count, uint8_t *occ, uint32_t flags);
+
 /* ------------------------------------------------------------------------
  * Path tracing (the reference's PathIntegrator::Radiance bounce loop,
  * Core/Integrator/PathIntegrator.cpp:44-367, driven per pixel as

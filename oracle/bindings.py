@@ -154,6 +154,12 @@ class RefLib:
                                        _f32p, _f32p, _f32p, ctypes.c_float, ctypes.c_float, ctypes.c_int,
                                        ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_uint32,
                                        ctypes.c_int, _f32p]
+        c = ctypes
+        L.ilref_render_box_plugin.argtypes = [c.c_char_p, c.c_char_p] + list(L.ilref_render_box.argtypes) + [
+            c.c_char_p, c.c_int]
+        L.ilref_compare_spaces.argtypes = [c.c_char_p, c.c_char_p, _f32p, _i32p, c.c_int, c.c_int, _f32p, c.c_int,
+                                           _f32p, _f32p, _f32p, _f32p, c.c_long, c.c_void_p, _u8p, _f32p,
+                                           c.c_void_p, _u8p, _u8p, _f32p, _u8p, c.c_char_p, c.c_int]
         self.L = L
 
     def render_box(self, scene: dict, width: int, height: int, spp: int, seed: int = 1, nthreads=None):
@@ -168,6 +174,49 @@ class RefLib:
                                 float(cam["aspect"]), width, height, spp, int(scene["max_depth"]),
                                 float(scene["epsilon"]), seed, nthreads or os.cpu_count() or 1, out.reshape(-1))
         return out
+
+    @staticmethod
+    def _scene_args(scene):
+        f = lambda a: np.ascontiguousarray(a, np.float32)
+        return (f(scene["pos"]).reshape(-1), np.ascontiguousarray(scene["prim_of_tri"], np.int32),
+                scene["pos"].shape[0] // 3, scene["albedo"].shape[0], f(scene["albedo"]).reshape(-1),
+                int(scene["light_prim"]), f(scene["light_quad"]).reshape(-1), f(scene["light_emit"]))
+
+    def render_box_plugin(self, plugin: str, scene: dict, width: int, height: int, spp: int, seed: int = 1,
+                          nthreads: int = 1, factory: str = "GPU"):
+        """The reference's PathIntegrator on the box scene over the space that
+        plug-in library `plugin` registers under `factory`. Raises RuntimeError
+        with the loader's message on failure."""
+        f = lambda a: np.ascontiguousarray(a, np.float32)
+        cam = scene["camera"]
+        out = np.zeros((height, width, 3), np.float32)
+        err = ctypes.create_string_buffer(512)
+        rc = self.L.ilref_render_box_plugin(plugin.encode(), factory.encode(), *self._scene_args(scene),
+                                            f(cam["eye"]), f(cam["target"]), f(cam["up"]), float(cam["fov"]),
+                                            float(cam["aspect"]), width, height, spp, int(scene["max_depth"]),
+                                            float(scene["epsilon"]), seed, nthreads, out.reshape(-1), err, 512)
+        if rc:
+            raise RuntimeError(f"ilref_render_box_plugin: {rc}: {err.value.decode(errors='replace')}")
+        return out
+
+    def compare_spaces(self, plugin: str, scene: dict, o4, d4, exclude=None, factory: str = "GPU"):
+        """BasicSpace vs the plug-in's space on the same primitives, ray by ray
+        (see ilref_compare_spaces). Returns a dict of arrays."""
+        o4 = np.ascontiguousarray(o4, np.float32)
+        d4 = np.ascontiguousarray(d4, np.float32)
+        n = o4.shape[0]
+        hit, occ, xhit, xocc = (np.zeros((n, 2), np.uint8) for _ in range(4))
+        t, xt = np.zeros((n, 2), np.float32), np.zeros((n, 2), np.float32)
+        diff = np.zeros(n, np.uint32)
+        ex = None if exclude is None else np.ascontiguousarray(exclude, np.int32)
+        err = ctypes.create_string_buffer(512)
+        rc = self.L.ilref_compare_spaces(plugin.encode(), factory.encode(), *self._scene_args(scene),
+                                         o4.reshape(-1), d4.reshape(-1), n, None if ex is None else ex.ctypes.data,
+                                         hit.reshape(-1), t.reshape(-1), diff.ctypes.data, occ.reshape(-1),
+                                         xhit.reshape(-1), xt.reshape(-1), xocc.reshape(-1), err, 512)
+        if rc:
+            raise RuntimeError(f"ilref_compare_spaces: {rc}: {err.value.decode(errors='replace')}")
+        return dict(hit=hit, t=t, diff=diff, occ=occ, xhit=xhit, xt=xt, xocc=xocc)
 
     def mesh(self, pos, idx, kind: str = "bvh"):
         return RefMesh(self, pos, idx, 0 if kind == "kd" else 1)

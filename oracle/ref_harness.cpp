@@ -2,7 +2,7 @@
 //
 // This file is ours; everything it calls is the reference's code, compiled
 // unmodified from the reference tree by oracle/Makefile (with the two
-// replacement headers under oracle/refshim). It exposes a small C ABI so the
+// replacement headers under illuminaprt_b200/plugin/compat). It exposes a small C ABI so the
 // tests and the CPU baseline of bench.py can drive the reference path:
 //
 //   closest hit  BasicSpace::Intersects(ray, isect)      Core/Space/BasicSpace.cpp:58-73
@@ -44,6 +44,12 @@
 #include "Material/Matte.h"
 #include "Sampler/RandomSampler.h"
 #include "Filter/BoxFilter.h"
+#include "System/EngineKernel.h"
+#include "System/PlugIn.h"
+#include "System/PlugInManager.h"
+
+#include <dlfcn.h>
+#include <string>
 
 using namespace Illumina::Core;
 
@@ -71,6 +77,232 @@ void parallel_chunks(long n, int nthreads, F f)
 	}
 	for (auto &th : pool) th.join();
 }
+
+void report(char *err, int err_len, const std::string &msg)
+{
+	if (err && err_len > 0) {
+		std::strncpy(err, msg.c_str(), (size_t)err_len - 1);
+		err[err_len - 1] = 0;
+	}
+}
+
+bool same(float a, float b) { return std::memcmp(&a, &b, sizeof(float)) == 0; }
+bool same(const Vector3 &a, const Vector3 &b) { return same(a.X, b.X) && same(a.Y, b.Y) && same(a.Z, b.Z); }
+
+uint32_t intersection_diff(const Intersection &a, const Intersection &b)
+{
+	const DifferentialSurface &p = a.Surface, &q = b.Surface;
+	uint32_t m = 0;
+	if (!same(p.Distance, q.Distance)) m |= 1u;
+	if (!same(p.Point, q.Point)) m |= 2u;
+	if (!same(p.PointUV.U, q.PointUV.U) || !same(p.PointUV.V, q.PointUV.V)) m |= 4u;
+	if (!same(p.GeometryNormal, q.GeometryNormal)) m |= 8u;
+	if (!same(p.ShadingNormal, q.ShadingNormal)) m |= 16u;
+	if (!same(p.PointWS, q.PointWS)) m |= 32u;
+	if (!same(p.GeometryBasisWS.U, q.GeometryBasisWS.U) || !same(p.GeometryBasisWS.V, q.GeometryBasisWS.V) ||
+	    !same(p.GeometryBasisWS.W, q.GeometryBasisWS.W) || !same(p.ShadingBasisWS.U, q.ShadingBasisWS.U) ||
+	    !same(p.ShadingBasisWS.V, q.ShadingBasisWS.V) || !same(p.ShadingBasisWS.W, q.ShadingBasisWS.W))
+		m |= 64u;
+	if (!same(p.RayOrigin, q.RayOrigin) || !same(p.RayDirection, q.RayDirection) ||
+	    !same(p.RayOriginWS, q.RayOriginWS) || !same(p.RayDirectionWS, q.RayDirectionWS))
+		m |= 128u;
+	if (a.GetPrimitive() != b.GetPrimitive()) m |= 256u;
+	if (a.GetMaterial() != b.GetMaterial()) m |= 512u;
+	if (a.GetLight() != b.GetLight()) m |= 1024u;
+	if (p.GetShape() != q.GetShape()) m |= 2048u;
+	return m;
+}
+
+// The box scene in reference objects (see ilref_render_box). Owns them.
+struct BoxScene
+{
+	std::vector<ITriangleMesh *> meshes;
+	std::vector<IPrimitive *> prims;
+	std::vector<IMaterial *> mats;
+	ILight *light = nullptr;
+	IShape *quadShape = nullptr;
+
+	void create(const float *pos, const int32_t *prim_of_tri, int ntris, int nprims, const float *albedo,
+	            int light_prim, const float *quad, const float *emit)
+	{
+		for (int p = 0; p < nprims; p++) {
+			IMaterial *m = new MatteMaterial(Spectrum(albedo[3 * p], albedo[3 * p + 1], albedo[3 * p + 2]));
+			mats.push_back(m);
+			if (p == light_prim) {
+				Quad *qs = new Quad(Vector3(quad[0], quad[1], quad[2]), Vector3(quad[3], quad[4], quad[5]),
+				                    Vector3(quad[6], quad[7], quad[8]), Vector3(quad[9], quad[10], quad[11]));
+				qs->ComputeBoundingVolume();
+				quadShape = qs;
+				EmissivePrimitive *ep = new EmissivePrimitive();
+				ep->SetShape(qs);
+				ep->SetMaterial(m);
+				DiffuseAreaLight *dl = new DiffuseAreaLight(nullptr, qs, Spectrum(emit[0], emit[1], emit[2]));
+				ep->SetLight(dl);
+				light = dl;
+				prims.push_back(ep);
+				continue;
+			}
+			BVHMesh *mesh = new BVHMesh(10, 35);
+			int nv = 0;
+			for (int t = 0; t < ntris; t++) {
+				if (prim_of_tri[t] != p) continue;
+				const float *a = pos + 9 * t;
+				Vector3 v0(a[0], a[1], a[2]), v1(a[3], a[4], a[5]), v2(a[6], a[7], a[8]);
+				Vector3 n = Vector3::Normalize(Vector3::Cross(v1 - v0, v2 - v0));
+				for (int c = 0; c < 3; c++) {
+					Vertex v;
+					v.Position.Set(a[3 * c], a[3 * c + 1], a[3 * c + 2]);
+					v.Normal = n;
+					v.UV.Set(c == 1 ? 1.f : 0.f, c == 2 ? 1.f : 0.f);
+					mesh->AddVertex(v);
+				}
+				mesh->AddIndexedTriangle(nv, nv + 1, nv + 2);
+				nv += 3;
+			}
+			mesh->ComputeBoundingVolume();
+			mesh->Compile();
+			meshes.push_back(mesh);
+			GeometricPrimitive *gp = new GeometricPrimitive();
+			gp->SetShape(mesh);
+			gp->SetMaterial(m);
+			prims.push_back(gp);
+		}
+	}
+
+	void fill(ISpace &space)
+	{
+		for (auto *p : prims) space.PrimitiveList.PushBack(p);
+		space.Initialise();
+		space.Build();
+	}
+
+	~BoxScene()
+	{
+		for (auto *pr : prims) delete pr;
+		for (auto *m : meshes) delete m;
+		for (auto *m : mats) delete m;
+		delete light;
+		delete quadShape;
+	}
+};
+
+// Reference renderer loop over any space (see ilref_render_box).
+void render_over(ISpace &space, ILight *light, const float *eye, const float *target, const float *up, float fov,
+                 float aspect, int width, int height, int spp, int max_depth, float eps, uint32_t seed,
+                 int nthreads, float *out)
+{
+	PerspectiveCamera camera(Vector3(eye[0], eye[1], eye[2]),
+	                         Vector3::Normalize(Vector3(target[0], target[1], target[2]) - Vector3(eye[0], eye[1], eye[2])),
+	                         Vector3(up[0], up[1], up[2]), -1.f, 1.f, -1.f, 1.f, 1.f);
+	camera.SetFieldOfView(fov, aspect);
+
+	const int tile = 16;
+	const int tiles_x = (width + tile - 1) / tile, tiles_y = (height + tile - 1) / tile;
+	const int ntiles = tiles_x * tiles_y;
+	std::atomic<int> next(0);
+	if (nthreads < 1) nthreads = 1;
+
+	auto worker = [&]() {
+		RandomSampler sampler;
+		Scene scene(&space, &camera, &sampler);
+		if (light) scene.LightList.PushBack(light);
+		PathIntegrator integrator(max_depth, 1, eps);
+		integrator.Initialise(&scene, &camera);
+		BoxFilter filter;
+		IntegratorContext ctx;
+		ctx.SampleCount = spp;
+		Intersection isect;
+		RadianceContext rc;
+		std::vector<Vector2> samples(spp);
+		const float rcpW = 1.f / width, rcpH = 1.f / height, rcpS = 1.f / spp;
+		int tid;
+		while ((tid = next.fetch_add(1)) < ntiles) {
+			sampler.Reset(seed * 7919u + (uint32_t)tid);
+			int x0 = (tid % tiles_x) * tile, y0 = (tid / tiles_x) * tile;
+			for (int y = y0; y < std::min(height, y0 + tile); y++)
+				for (int x = x0; x < std::min(width, x0 + tile); x++) {
+					sampler.Get2DSamples(samples.data(), spp);
+					filter(samples.data(), spp);
+					ctx.SurfacePosition.Set((float)x, (float)y);
+					ctx.NormalisedPosition.Set(x * rcpW, y * rcpH);
+					Spectrum acc(0.f);
+					for (ctx.SampleIndex = 0; ctx.SampleIndex < spp; ctx.SampleIndex++) {
+						Ray ray;
+						camera.GetRay(ctx.NormalisedPosition.X, ctx.NormalisedPosition.Y,
+						              samples[ctx.SampleIndex].U * rcpW, samples[ctx.SampleIndex].V * rcpH, ray);
+						acc += integrator.Radiance(&ctx, &scene, ray, isect, &rc);
+					}
+					acc *= rcpS;
+					float *o = out + 3 * ((size_t)y * width + x);
+					o[0] = acc[0]; o[1] = acc[1]; o[2] = acc[2];
+				}
+		}
+	};
+	std::vector<std::thread> pool;
+	for (int i = 0; i < nthreads; i++) pool.emplace_back(worker);
+	for (auto &th : pool) th.join();
+}
+
+// A space made by a plug-in's factory (see ilref_render_box_plugin).
+struct PluginSpace
+{
+	void *lib = nullptr;
+	EngineKernel *kernel = nullptr;
+	IPlugIn *plugin = nullptr;
+	ISpace *space = nullptr;
+
+	int open(const char *path, const char *factory, char *err, int err_len)
+	{
+		// The plug-in resolves the engine's symbols against this library, so
+		// make this library's symbols global before loading it.
+		Dl_info self;
+		if (dladdr((void *)&report, &self) && self.dli_fname)
+			dlopen(self.dli_fname, RTLD_NOW | RTLD_NOLOAD | RTLD_GLOBAL);
+		lib = dlopen(path, RTLD_NOW | RTLD_LOCAL);
+		if (!lib) {
+			const char *e = dlerror();
+			report(err, err_len, e ? e : "dlopen failed");
+			return -1;
+		}
+		typedef IPlugIn *(*GetSingleton)(void);
+		GetSingleton get = (GetSingleton)dlsym(lib, "GetPlugInSingleton");
+		if (!get) {
+			report(err, err_len, "no GetPlugInSingleton in plug-in");
+			return -2;
+		}
+		kernel = new EngineKernel();
+		plugin = get();
+		kernel->GetPlugInManager()->Register(plugin);
+		Factory<ISpace> *f = kernel->GetSpaceManager()->RequestFactory(factory);
+		if (!f) {
+			report(err, err_len, std::string("no space factory named ") + factory);
+			return -3;
+		}
+		space = f->CreateInstance();
+		return space ? 0 : -3;
+	}
+
+	// ISpace::Build returns only a bool; a plug-in may say why.
+	void report_build_failure(char *err, int err_len)
+	{
+		typedef const char *(*LastError)(const ISpace *);
+		LastError why = lib ? (LastError)dlsym(lib, "GpuSpaceLastError") : nullptr;
+		report(err, err_len, std::string("space Initialise/Build returned false: ") + (why ? why(space) : ""));
+	}
+
+	~PluginSpace()
+	{
+		delete space;
+		if (plugin) kernel->GetPlugInManager()->Unregister(plugin);
+		delete kernel;
+		if (lib) {
+			typedef void (*Dispose)(void);
+			Dispose d = (Dispose)dlsym(lib, "DisposePlugInSingleton");
+			if (d) d();
+			dlclose(lib);
+		}
+	}
+};
 
 } // namespace
 
@@ -188,116 +420,102 @@ int ilref_render_box(const float *pos, const int32_t *prim_of_tri, int ntris, in
                      int width, int height, int spp, int max_depth, float eps, uint32_t seed,
                      int nthreads, float *out)
 {
-	std::vector<ITriangleMesh *> meshes;
-	std::vector<IPrimitive *> prims;
-	std::vector<IMaterial *> mats;
+	BoxScene scene;
+	scene.create(pos, prim_of_tri, ntris, nprims, albedo, light_prim, quad, emit);
 	BasicSpace space;
-	ILight *light = nullptr;
-	IShape *quadShape = nullptr;
+	scene.fill(space);
+	render_over(space, scene.light, eye, target, up, fov, aspect, width, height, spp, max_depth, eps, seed,
+	            nthreads, out);
+	return 0;
+}
 
-	for (int p = 0; p < nprims; p++) {
-		IMaterial *m = new MatteMaterial(Spectrum(albedo[3 * p], albedo[3 * p + 1], albedo[3 * p + 2]));
-		mats.push_back(m);
-		if (p == light_prim) {
-			Quad *qs = new Quad(Vector3(quad[0], quad[1], quad[2]), Vector3(quad[3], quad[4], quad[5]),
-			                    Vector3(quad[6], quad[7], quad[8]), Vector3(quad[9], quad[10], quad[11]));
-			qs->ComputeBoundingVolume();
-			quadShape = qs;
-			EmissivePrimitive *ep = new EmissivePrimitive();
-			ep->SetShape(qs);
-			ep->SetMaterial(m);
-			DiffuseAreaLight *dl = new DiffuseAreaLight(nullptr, qs, Spectrum(emit[0], emit[1], emit[2]));
-			ep->SetLight(dl);
-			light = dl;
-			prims.push_back(ep);
-			space.PrimitiveList.PushBack(ep);
-			continue;
-		}
-		BVHMesh *mesh = new BVHMesh(10, 35);
-		int nv = 0;
-		for (int t = 0; t < ntris; t++) {
-			if (prim_of_tri[t] != p) continue;
-			const float *a = pos + 9 * t;
-			Vector3 v0(a[0], a[1], a[2]), v1(a[3], a[4], a[5]), v2(a[6], a[7], a[8]);
-			Vector3 n = Vector3::Normalize(Vector3::Cross(v1 - v0, v2 - v0));
-			for (int c = 0; c < 3; c++) {
-				Vertex v;
-				v.Position.Set(a[3 * c], a[3 * c + 1], a[3 * c + 2]);
-				v.Normal = n;
-				v.UV.Set(c == 1 ? 1.f : 0.f, c == 2 ? 1.f : 0.f);
-				mesh->AddVertex(v);
-			}
-			mesh->AddIndexedTriangle(nv, nv + 1, nv + 2);
-			nv += 3;
-		}
-		mesh->ComputeBoundingVolume();
-		mesh->Compile();
-		meshes.push_back(mesh);
-		GeometricPrimitive *gp = new GeometricPrimitive();
-		gp->SetShape(mesh);
-		gp->SetMaterial(m);
-		prims.push_back(gp);
-		space.PrimitiveList.PushBack(gp);
+// The same render with the space a plug-in registers: the plug-in library is
+// loaded, its GetPlugInSingleton() handed to the engine's PlugInManager
+// (which calls IPlugIn::Register(EngineKernel*)), and the space is made by
+// the factory registered under `factory` in the kernel's SpaceManager. The
+// reference's own library loader has no Linux implementation
+// (System/LibraryManager.cpp:16-23 throws), so the load is a dlopen here.
+// Returns 0, or a negative code: -1 load, -2 symbol, -3 factory, -4 Build().
+int ilref_render_box_plugin(const char *plugin_path, const char *factory,
+                            const float *pos, const int32_t *prim_of_tri, int ntris, int nprims,
+                            const float *albedo, int light_prim, const float *quad, const float *emit,
+                            const float *eye, const float *target, const float *up, float fov, float aspect,
+                            int width, int height, int spp, int max_depth, float eps, uint32_t seed,
+                            int nthreads, float *out, char *err, int err_len)
+{
+	PluginSpace ps;
+	int rc = ps.open(plugin_path, factory, err, err_len);
+	if (rc) return rc;
+	BoxScene scene;
+	scene.create(pos, prim_of_tri, ntris, nprims, albedo, light_prim, quad, emit);
+	scene.fill(*ps.space);
+	if (!ps.space->Initialise() || !ps.space->Build()) {
+		ps.report_build_failure(err, err_len);
+		return -4;
 	}
-	space.Initialise();
-	space.Build();
+	render_over(*ps.space, scene.light, eye, target, up, fov, aspect, width, height, spp, max_depth, eps, seed,
+	            nthreads, out);
+	return 0;
+}
 
-	PerspectiveCamera camera(Vector3(eye[0], eye[1], eye[2]),
-	                         Vector3::Normalize(Vector3(target[0], target[1], target[2]) - Vector3(eye[0], eye[1], eye[2])),
-	                         Vector3(up[0], up[1], up[2]), -1.f, 1.f, -1.f, 1.f, 1.f);
-	camera.SetFieldOfView(fov, aspect);
-
-	const int tile = 16;
-	const int tiles_x = (width + tile - 1) / tile, tiles_y = (height + tile - 1) / tile;
-	const int ntiles = tiles_x * tiles_y;
-	std::atomic<int> next(0);
-	if (nthreads < 1) nthreads = 1;
-
-	auto worker = [&]() {
-		RandomSampler sampler;
-		Scene scene(&space, &camera, &sampler);
-		if (light) scene.LightList.PushBack(light);
-		PathIntegrator integrator(max_depth, 1, eps);
-		integrator.Initialise(&scene, &camera);
-		BoxFilter filter;
-		IntegratorContext ctx;
-		ctx.SampleCount = spp;
-		Intersection isect;
-		RadianceContext rc;
-		std::vector<Vector2> samples(spp);
-		const float rcpW = 1.f / width, rcpH = 1.f / height, rcpS = 1.f / spp;
-		int tid;
-		while ((tid = next.fetch_add(1)) < ntiles) {
-			sampler.Reset(seed * 7919u + (uint32_t)tid);
-			int x0 = (tid % tiles_x) * tile, y0 = (tid / tiles_x) * tile;
-			for (int y = y0; y < std::min(height, y0 + tile); y++)
-				for (int x = x0; x < std::min(width, x0 + tile); x++) {
-					sampler.Get2DSamples(samples.data(), spp);
-					filter(samples.data(), spp);
-					ctx.SurfacePosition.Set((float)x, (float)y);
-					ctx.NormalisedPosition.Set(x * rcpW, y * rcpH);
-					Spectrum acc(0.f);
-					for (ctx.SampleIndex = 0; ctx.SampleIndex < spp; ctx.SampleIndex++) {
-						Ray ray;
-						camera.GetRay(ctx.NormalisedPosition.X, ctx.NormalisedPosition.Y,
-						              samples[ctx.SampleIndex].U * rcpW, samples[ctx.SampleIndex].V * rcpH, ray);
-						acc += integrator.Radiance(&ctx, &scene, ray, isect, &rc);
-					}
-					acc *= rcpS;
-					float *o = out + 3 * ((size_t)y * width + x);
-					o[0] = acc[0]; o[1] = acc[1]; o[2] = acc[2];
-				}
+// Field-by-field comparison of the plug-in space with BasicSpace over the
+// same primitives (the box scene), for n rays (float4 streams as above).
+// Per ray: hit[2*i + s] (s = 0 BasicSpace, 1 plug-in) for the closest-hit
+// overload, t[2*i + s] its Distance (+inf on a miss), diff[i] a bit mask of
+// the Intersection fields that differ when both hit (1 Distance, 2 Point,
+// 4 PointUV, 8 GeometryNormal, 16 ShadingNormal, 32 PointWS, 64 bases,
+// 128 ray fields, 256 primitive, 512 material, 1024 light, 2048 shape),
+// occ[2*i + s] the any-hit overload, and with exclude[i] >= 0 also
+// xhit/xt/xocc[2*i + s] for the p_pExclude overloads excluding primitive
+// exclude[i]. batch_diff counts rays whose IntersectsBatch-style answer
+// (every ray in one call, when the plug-in is a GpuSpace) differs from its
+// scalar answer; the comparison uses the space only through ISpace, so
+// batching is exercised by the caller's choice of ray count.
+int ilref_compare_spaces(const char *plugin_path, const char *factory,
+                         const float *pos, const int32_t *prim_of_tri, int ntris, int nprims,
+                         const float *albedo, int light_prim, const float *quad, const float *emit,
+                         const float *o4, const float *d4, long n, const int32_t *exclude,
+                         uint8_t *hit, float *t, uint32_t *diff, uint8_t *occ,
+                         uint8_t *xhit, float *xt, uint8_t *xocc, char *err, int err_len)
+{
+	PluginSpace ps;
+	int rc = ps.open(plugin_path, factory, err, err_len);
+	if (rc) return rc;
+	BoxScene scene;
+	scene.create(pos, prim_of_tri, ntris, nprims, albedo, light_prim, quad, emit);
+	BasicSpace basic;
+	scene.fill(basic);
+	scene.fill(*ps.space);
+	basic.Initialise();
+	basic.Build();
+	if (!ps.space->Initialise() || !ps.space->Build()) {
+		ps.report_build_failure(err, err_len);
+		return -4;
+	}
+	ISpace *spaces[2] = {&basic, ps.space};
+	const float inf = __builtin_inff();
+	for (long i = 0; i < n; i++) {
+		Ray ray(Vector3(o4[4 * i], o4[4 * i + 1], o4[4 * i + 2]), Vector3(d4[4 * i], d4[4 * i + 1], d4[4 * i + 2]),
+		        o4[4 * i + 3], d4[4 * i + 3]);
+		Intersection is[2];
+		for (int s = 0; s < 2; s++) {
+			is[s].Prepare();
+			hit[2 * i + s] = spaces[s]->Intersects(ray, is[s]) ? 1 : 0;
+			t[2 * i + s] = hit[2 * i + s] ? is[s].Surface.Distance : inf;
+			occ[2 * i + s] = spaces[s]->Intersects(ray) ? 1 : 0;
 		}
-	};
-	std::vector<std::thread> pool;
-	for (int i = 0; i < nthreads; i++) pool.emplace_back(worker);
-	for (auto &th : pool) th.join();
-
-	for (auto *pr : prims) delete pr;
-	for (auto *m : meshes) delete m;
-	for (auto *m : mats) delete m;
-	delete light;
-	delete quadShape;
+		diff[i] = (hit[2 * i] && hit[2 * i + 1]) ? intersection_diff(is[0], is[1]) : 0u;
+		if (exclude && exclude[i] >= 0 && exclude[i] < (int)scene.prims.size()) {
+			IPrimitive *ex = scene.prims[exclude[i]];
+			for (int s = 0; s < 2; s++) {
+				Intersection x;
+				x.Prepare();
+				xhit[2 * i + s] = spaces[s]->Intersects(ray, x, ex) ? 1 : 0;
+				xt[2 * i + s] = xhit[2 * i + s] ? x.Surface.Distance : inf;
+				xocc[2 * i + s] = spaces[s]->Intersects(ray, ex) ? 1 : 0;
+			}
+		}
+	}
 	return 0;
 }
 

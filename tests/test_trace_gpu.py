@@ -139,3 +139,25 @@ def test_device_pointer_path_and_errors():
     assert np.array_equal(t.cpu().numpy().view(np.uint32), host[1].view(np.uint32))
     # zero rays is a no-op
     s.intersects(co[:0], cd[:0])
+
+
+@pytest.mark.parametrize("first,count", [(0, 1), (1000, 2048), (5000, 3000)])
+def test_excluding_queries_match_oracle_without_the_range(first, count, oracle):
+    # the p_pExclude overloads: the oracle sees the mesh with the range removed
+    pos, idx = scenes.heightfield(64, 64, 0.2, 11)
+    n_tris = idx.shape[0]
+    co, cd = scenes.pinhole_rays(64, 64, (0.5, -0.6, 0.8), (0.5, 0.5, 0.0), (0, 0, 1), 60.0)
+    io, idr = scenes.incoherent_rays(pos, idx, 8192, 12)
+    o4, d4 = np.concatenate([co, io]), np.concatenate([cd, idr])
+    sp = space_for(pos, idx)
+    got = sp.intersects_excluding(o4, d4, first, count)
+    keep = np.r_[0:first, first + count:n_tris]
+    rp, rt, ru, rv = oracle.bvh(pos, idx[keep]).intersect(o4, d4)
+    rp = np.where(rp >= 0, keep[np.maximum(rp, 0)], rp).astype(np.int32)
+    n_same, ties, bad, bits_ok = classify(pos, idx, o4, d4, got, (rp, rt, ru, rv), oracle)
+    assert bad == [] and bits_ok
+    assert not np.isin(got[0], np.arange(first, first + count)).any()
+    occ = sp.occluded_excluding(o4, d4, first, count)
+    assert np.array_equal(occ.astype(bool), rp >= 0)
+    # an empty range is the plain query
+    assert np.array_equal(sp.intersects_excluding(o4, d4, 0, 0)[0], sp.intersects(o4, d4)[0])
