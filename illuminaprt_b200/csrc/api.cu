@@ -409,20 +409,48 @@ int ilg_set_quad_lights(ilg_ctx *ctx, const ilg_quad_light *lights, uint32_t n)
     return ILG_OK;
 }
 
-// Validates a scene context for rendering and fills its scene record
-// (camera frame as PerspectiveCamera(eye, normalize(target - eye), up,
-// -1,1,-1,1, 1) + SetFieldOfView builds it: Core/Camera/Camera.cpp:30-44,
-// Core/Geometry/Basis.cpp:28-44). Builds the per-triangle attributes on `st`.
-static int prepare_scene(ilg_ctx *runner, ilg_ctx *ctx, const ilg_camera *cam, uint32_t W, uint32_t H, uint32_t spp,
-                         uint32_t max_depth, float eps, uint32_t seed, const float sky[3], cudaStream_t st,
-                         SceneRec &S)
+// The camera frame PerspectiveCamera(eye, normalize(target - eye), up,
+// -1,1,-1,1, 1) + SetFieldOfView builds (Core/Camera/Camera.cpp:30-44,
+// Core/Geometry/Basis.cpp:28-44).
+static void camera_frame_of(const ilg_camera &cam, ilg_camera_frame &f)
 {
-    if (!ctx || !cam) return fail(runner, ILG_EINVAL, "render: null scene or camera");
+    V3 eye = v3(cam.eye);
+    V3 w = normalize(normalize(v3(cam.target) - eye));
+    V3 v = normalize(v3(cam.up));
+    v = v - dot(v, w) * w;
+    if (dot(v, v) <= 1.1920929e-7f) {
+        v = V3{w.z, w.x, w.y};
+        v = normalize(cross(v, w));
+        v = normalize(v - dot(v, w) * w);
+    }
+    V3 u = cross(v, w);
+    const float half = cam.fov_deg * (std::atan(1.0f) / 45.0f) * 0.5f;
+    const float v1 = std::tan(half), v0 = -v1, u0 = v0 * cam.aspect, u1 = v1 * cam.aspect;
+    const V3 corner = eye + u0 * u + v0 * v + 1.0f * w, across = (u1 - u0) * u, up = (v1 - v0) * v;
+    const V3 *src[4] = {&eye, &corner, &across, &up};
+    float *dst[4] = {f.centre, f.corner, f.across, f.up};
+    for (int k = 0; k < 4; k++) {
+        dst[k][0] = src[k]->x;
+        dst[k][1] = src[k]->y;
+        dst[k][2] = src[k]->z;
+    }
+}
+
+// Validates a scene context for rendering and fills its scene record for the
+// region (rx, ry, rw, rh) of a W x H image. Builds the per-triangle
+// attributes on `st`.
+static int prepare_scene(ilg_ctx *runner, ilg_ctx *ctx, const ilg_camera_frame &cam, uint32_t W, uint32_t H,
+                         uint32_t rx, uint32_t ry, uint32_t rw, uint32_t rh, uint32_t spp, uint32_t max_depth,
+                         float eps, uint32_t seed, const float sky[3], cudaStream_t st, SceneRec &S)
+{
+    if (!ctx) return fail(runner, ILG_EINVAL, "render: null scene");
     if (ctx->device != runner->device) return fail(runner, ILG_EINVAL, "render: scene on another device");
     if (!ctx->built) return fail(runner, ILG_ESTATE, "ilg_render: scene not built");
     if (!ctx->has_mat || ctx->n_mats == 0) return fail(runner, ILG_ESTATE, "ilg_render: materials not set");
     if (W == 0 || H == 0 || spp == 0 || (uint64_t)W * H > (1u << 26))
         return fail(runner, ILG_EINVAL, "ilg_render: bad image size %ux%u or spp %u", W, H, spp);
+    if (rw == 0 || rh == 0 || (uint64_t)rx + rw > W || (uint64_t)ry + rh > H)
+        return fail(runner, ILG_EINVAL, "ilg_render: region %u,%u %ux%u outside the %ux%u image", rx, ry, rw, rh, W, H);
     if (max_depth == 0 || max_depth > 64) return fail(runner, ILG_EINVAL, "ilg_render: max_depth must be 1..64");
     for (uint32_t l = 0; l < ctx->n_lights; l++)
         if ((uint64_t)ctx->light_first_host[l] + 1 >= ctx->n_tris)
@@ -435,28 +463,17 @@ static int prepare_scene(ilg_ctx *runner, ilg_ctx *ctx, const ilg_camera *cam, u
                                    ctx->light_of_prim.ptr, ctx->tri_attr.ptr, st));
         ctx->attr_dirty = false;
     }
-    V3 eye = v3(cam->eye);
-    V3 w = normalize(normalize(v3(cam->target) - eye));
-    V3 v = normalize(v3(cam->up));
-    v = v - dot(v, w) * w;
-    if (dot(v, v) <= 1.1920929e-7f) {
-        v = V3{w.z, w.x, w.y};
-        v = normalize(cross(v, w));
-        v = normalize(v - dot(v, w) * w);
-    }
-    V3 u = cross(v, w);
-    const float half = cam->fov_deg * (std::atan(1.0f) / 45.0f) * 0.5f;
-    const float v1 = std::tan(half), v0 = -v1, u0 = v0 * cam->aspect, u1 = v1 * cam->aspect;
     S = SceneRec{};
     S.nodes = ctx->bb.nodes; S.tris = ctx->bb.tris; S.n_nodes = ctx->stats.n_nodes; S.n_tris = ctx->stats.n_tris;
     S.tri_attr = ctx->tri_attr.ptr; S.mats = ctx->mats.ptr; S.n_mats = ctx->n_mats;
     S.lights = ctx->lights.ptr; S.n_lights = ctx->n_lights;
     S.sky = make_float3(sky[0], sky[1], sky[2]);
-    S.centre = f3(eye);
-    S.corner = f3(eye + u0 * u + v0 * v + 1.0f * w);
-    S.across = f3((u1 - u0) * u);
-    S.up = f3((v1 - v0) * v);
-    S.width = W; S.height = H; S.wh = W * H; S.rcp_w = 1.f / W; S.rcp_h = 1.f / H;
+    S.centre = make_float3(cam.centre[0], cam.centre[1], cam.centre[2]);
+    S.corner = make_float3(cam.corner[0], cam.corner[1], cam.corner[2]);
+    S.across = make_float3(cam.across[0], cam.across[1], cam.across[2]);
+    S.up = make_float3(cam.up[0], cam.up[1], cam.up[2]);
+    S.width = W; S.height = H; S.full_wh = W * H; S.rcp_w = 1.f / W; S.rcp_h = 1.f / H;
+    S.region_x = rx; S.region_y = ry; S.region_w = rw; S.wh = rw * rh;
     S.max_depth = max_depth; S.eps = eps; S.spp = spp; S.seed = seed;
     return ILG_OK;
 }
@@ -465,19 +482,22 @@ static int prepare_scene(ilg_ctx *runner, ilg_ctx *ctx, const ilg_camera *cam, u
 // waves of at most `cap_req` paths on the runner's buffers and stream.
 static int run_render(ilg_ctx *ctx, std::vector<SceneRec> &recs, uint32_t cap_req, uint32_t block,
                       uint32_t cache_depth, uint32_t train_every, uint32_t train_steps, uint32_t train_batch,
-                      uint64_t *total_paths_out)
+                      uint64_t *total_paths_out, bool aux = false)
 {
     cudaStream_t st = ctx->stream;
-    uint64_t total = 0;
+    uint64_t total = 0, pixels64 = 0;
     uint32_t pixels = 0, depth_max = 0, nl = 1;
     for (auto &S : recs) {
         S.path_begin = total;
         S.pixel_base = pixels;
         total += (uint64_t)S.wh * S.spp;
-        pixels += S.wh;
+        pixels64 += S.wh;
+        pixels = (uint32_t)std::min<uint64_t>(pixels64, 0xffffffffu);
         depth_max = std::max(depth_max, S.max_depth);
         nl = std::max(nl, S.n_lights);
     }
+    // shadow segments carry the pixel in 31 bits (bit 31 tags Direct)
+    if (pixels64 >= 0x80000000u) return fail(ctx, ILG_EINVAL, "render: more than 2^31 pixels in one call");
     if (total_paths_out) *total_paths_out = total;
     // wave size: whole samples for a single scene (so a wave never splits a pixel's sample)
     uint32_t cap = cap_req ? cap_req : (1u << 22);
@@ -509,6 +529,14 @@ static int run_render(ilg_ctx *ctx, std::vector<SceneRec> &recs, uint32_t cap_re
     R.s_o = ctx->s_o.ptr; R.s_d = ctx->s_d.ptr; R.s_c = ctx->s_c.ptr;
     R.sh_count = ctx->counts.ptr + 2; R.sh_capacity = cap * nl;
     R.accum = ctx->accum.ptr; R.err = ctx->derr.ptr;
+    if (aux) {
+        CK(ctx->accum_direct.reserve(pixels));
+        CK(ctx->accum_albedo.reserve(pixels));
+        CK(cudaMemsetAsync(ctx->accum_direct.ptr, 0, sizeof(float4) * pixels, st));
+        CK(cudaMemsetAsync(ctx->accum_albedo.ptr, 0, sizeof(float4) * pixels, st));
+        R.accum_direct = ctx->accum_direct.ptr;
+        R.accum_albedo = ctx->accum_albedo.ptr;
+    }
 
     MlpDev mlp = {};
     if (cache_depth) {
@@ -576,12 +604,15 @@ static int run_render(ilg_ctx *ctx, std::vector<SceneRec> &recs, uint32_t cap_re
     return ILG_OK;
 }
 
-int ilg_render(ilg_ctx *ctx, const ilg_camera *cam, const ilg_render_opts *opts, float *out_rgb, uint32_t flags)
+}  // extern "C"
+
+namespace {
+
+// One scene, one region: the body of ilg_render and ilg_render_region.
+int render_one(ilg_ctx *ctx, const ilg_camera_frame &frame, const ilg_render_opts *opts, const ilg_region &reg,
+               float *final_rgb, float *direct_rgb, float *albedo_rgb, uint32_t flags, bool use_cache)
 {
-    if (!ctx) return ILG_EINVAL;
-    if (!cam || !opts || !out_rgb) return fail(ctx, ILG_EINVAL, "ilg_render: null argument");
-    if (flags & ~ILG_DEVICE_PTRS) return fail(ctx, ILG_EINVAL, "ilg_render: unknown flags 0x%x", flags);
-    const uint32_t cache_depth = opts->cache_depth;
+    const uint32_t cache_depth = use_cache ? opts->cache_depth : 0u;
     if (cache_depth) {
         if (!ctx->mlp_ready) return fail(ctx, ILG_ESTATE, "ilg_render: cache_depth set but ilg_mlp_init not called");
         if (cache_depth >= opts->max_depth)
@@ -590,26 +621,62 @@ int ilg_render(ilg_ctx *ctx, const ilg_camera *cam, const ilg_render_opts *opts,
     CK(cudaSetDevice(ctx->device));
     cudaStream_t st = ctx->stream;
     std::vector<SceneRec> recs(1);
-    int rc = prepare_scene(ctx, ctx, cam, opts->width, opts->height, opts->spp, opts->max_depth, opts->epsilon,
-                           opts->seed, opts->sky, st, recs[0]);
+    int rc = prepare_scene(ctx, ctx, frame, opts->width, opts->height, reg.x, reg.y, reg.width, reg.height,
+                           opts->spp, opts->max_depth, opts->epsilon, opts->seed, opts->sky, st, recs[0]);
     if (rc) return rc;
-    const uint32_t wh = opts->width * opts->height;
+    const uint32_t wh = recs[0].wh;
+    const bool aux = direct_rgb || albedo_rgb;
     rc = run_render(ctx, recs, opts->paths_per_wave, 128, cache_depth, opts->train_every ? opts->train_every : 16u,
-                    opts->train_steps, opts->train_batch ? opts->train_batch : 16384u, nullptr);
+                    opts->train_steps, opts->train_batch ? opts->train_batch : 16384u, nullptr, aux);
     if (rc) return rc;
-    float *out_dev = out_rgb;
-    if (!(flags & ILG_DEVICE_PTRS)) {
-        CK(ctx->out_dev.reserve(3ull * wh));
-        out_dev = ctx->out_dev.ptr;
+    const bool dev = (flags & ILG_DEVICE_PTRS) != 0;
+    const float4 *sums[3] = {ctx->accum.ptr, ctx->accum_direct.ptr, ctx->accum_albedo.ptr};
+    float *outs[3] = {final_rgb, direct_rgb, albedo_rgb};
+    if (!dev) CK(ctx->out_dev.reserve(3ull * wh));
+    for (int k = 0; k < 3; k++) {
+        if (!outs[k]) continue;
+        float *dst = dev ? outs[k] : ctx->out_dev.ptr;
+        CK(render_resolve(sums[k], wh, 1.f / opts->spp, dst, st));
+        ctx->last_render_launches += 1;
+        if (!dev) {
+            CK(cudaMemcpyAsync(outs[k], dst, 12ull * wh, cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));  // out_dev is reused for the next output
+        }
     }
-    CK(render_resolve(ctx->accum.ptr, wh, 1.f / opts->spp, out_dev, st));
-    ctx->last_render_launches += 1;
-    if (!(flags & ILG_DEVICE_PTRS)) {
-        CK(cudaMemcpyAsync(out_rgb, out_dev, 12ull * wh, cudaMemcpyDeviceToHost, st));
-        CK(cudaStreamSynchronize(st));
-        return ctx->check_device_error();
-    }
+    if (!dev) return ctx->check_device_error();
     return ILG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int ilg_camera_frame_of(const ilg_camera *cam, ilg_camera_frame *out)
+{
+    if (!cam || !out) return ILG_EINVAL;
+    camera_frame_of(*cam, *out);
+    return ILG_OK;
+}
+
+int ilg_render(ilg_ctx *ctx, const ilg_camera *cam, const ilg_render_opts *opts, float *out_rgb, uint32_t flags)
+{
+    if (!ctx) return ILG_EINVAL;
+    if (!cam || !opts || !out_rgb) return fail(ctx, ILG_EINVAL, "ilg_render: null argument");
+    if (flags & ~ILG_DEVICE_PTRS) return fail(ctx, ILG_EINVAL, "ilg_render: unknown flags 0x%x", flags);
+    ilg_camera_frame frame;
+    camera_frame_of(*cam, frame);
+    const ilg_region whole = {0u, 0u, opts->width, opts->height};
+    return render_one(ctx, frame, opts, whole, out_rgb, nullptr, nullptr, flags, true);
+}
+
+int ilg_render_region(ilg_ctx *ctx, const ilg_camera_frame *frame, const ilg_render_opts *opts,
+                      const ilg_region *region, float *final_rgb, float *direct_rgb, float *albedo_rgb,
+                      uint32_t flags)
+{
+    if (!ctx) return ILG_EINVAL;
+    if (!frame || !opts || !region || !final_rgb) return fail(ctx, ILG_EINVAL, "ilg_render_region: null argument");
+    if (flags & ~ILG_DEVICE_PTRS) return fail(ctx, ILG_EINVAL, "ilg_render_region: unknown flags 0x%x", flags);
+    return render_one(ctx, *frame, opts, *region, final_rgb, direct_rgb, albedo_rgb, flags, false);
 }
 
 int ilg_render_batch(ilg_ctx *runner, const ilg_batch_item *items, uint32_t n, uint32_t paths_per_wave,
@@ -626,8 +693,10 @@ int ilg_render_batch(ilg_ctx *runner, const ilg_batch_item *items, uint32_t n, u
     for (uint32_t i = 0; i < n; i++) {
         const ilg_batch_item &it = items[i];
         if (!it.out_rgb) return fail(runner, ILG_EINVAL, "ilg_render_batch: item %u has no output", i);
-        int rc = prepare_scene(runner, it.scene, &it.camera, it.width, it.height, it.spp, it.max_depth, it.epsilon,
-                               it.seed, it.sky, st, recs[i]);
+        ilg_camera_frame frame;
+        camera_frame_of(it.camera, frame);
+        int rc = prepare_scene(runner, it.scene, frame, it.width, it.height, 0, 0, it.width, it.height, it.spp,
+                               it.max_depth, it.epsilon, it.seed, it.sky, st, recs[i]);
         if (rc) return rc;
     }
     int rc = run_render(runner, recs, paths_per_wave, block ? block : 128, 0, 16, 0, 16384, nullptr);

@@ -48,7 +48,7 @@ struct ilg_ctx {
     ilg::DevBuf<uint32_t> tri_attr, light_of_prim;
     bool attr_dirty = true;
     // path tracing: wavefront buffers
-    ilg::DevBuf<float4> q_o0, q_d0, q_o1, q_d1, beta, s_o, s_d, s_c, accum;
+    ilg::DevBuf<float4> q_o0, q_d0, q_o1, q_d1, beta, s_o, s_d, s_c, accum, accum_direct, accum_albedo;
     ilg::DevBuf<uint32_t> q_p0, q_p1, counts, path_scene, s_sid;
     ilg::DevBuf<ilg::SceneRec> scene_table;
     ilg::DevBuf<int> hit_tri;
@@ -105,7 +105,7 @@ struct ilg_ctx {
         derr.release(); dstats.release();
         mats.release(); lights.release(); light_first_tri.release(); tri_attr.release(); light_of_prim.release();
         q_o0.release(); q_d0.release(); q_o1.release(); q_d1.release(); beta.release(); s_o.release();
-        s_d.release(); s_c.release(); accum.release(); q_p0.release(); q_p1.release(); counts.release();
+        s_d.release(); s_c.release(); accum.release(); accum_direct.release(); accum_albedo.release(); q_p0.release(); q_p1.release(); counts.release();
         hit_tri.release(); hit_t.release(); out_dev.release(); path_scene.release(); s_sid.release();
         scene_table.release();
         train_slot.release(); rec_of.release(); s_meta.release(); rec_feat.release(); rec_tgt.release();

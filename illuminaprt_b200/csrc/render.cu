@@ -116,11 +116,18 @@ __device__ __forceinline__ uint32_t scene_of(const RenderDev &R, uint64_t g)
 }
 
 // path identity inside its scene: (pixel, sample-sequence key)
-__device__ __forceinline__ void path_ident(const SceneRec &S, uint64_t g, uint32_t &pixel, uint64_t &key)
+// (pixel = index in the rendered region, image coordinates x, y). The key
+// depends on the image pixel and the sample only, so a region renders exactly
+// the paths the whole image renders there.
+__device__ __forceinline__ void path_ident(const SceneRec &S, uint64_t g, uint32_t &pixel, uint64_t &key,
+                                           uint32_t &x, uint32_t &y)
 {
     const uint64_t local = g - S.path_begin;
-    pixel = (uint32_t)(local % S.wh);
-    key = path_key(S.seed, local);
+    const uint64_t sample = local / S.wh;
+    pixel = (uint32_t)(local - sample * S.wh);
+    x = S.region_x + pixel % S.region_w;
+    y = S.region_y + pixel / S.region_w;
+    key = path_key(S.seed, sample * S.full_wh + (uint64_t)y * S.width + x);
 }
 
 __global__ void k_camera(RenderDev R, uint32_t n_paths, uint64_t wave_begin)
@@ -130,10 +137,9 @@ __global__ void k_camera(RenderDev R, uint32_t n_paths, uint64_t wave_begin)
     const uint64_t g = wave_begin + p;
     const uint32_t sid = scene_of(R, g);
     const SceneRec &S = R.scenes[sid];
-    uint32_t pixel;
+    uint32_t pixel, x, y;
     uint64_t key;
-    path_ident(S, g, pixel, key);
-    const uint32_t x = pixel % S.width, y = pixel / S.width;
+    path_ident(S, g, pixel, key, x, y);
     // BoxFilter shifts the [0,1) sample by -0.5 (Core/Filter/BoxFilter.cpp:20-28)
     const float xi1 = rnd(key, kDimCam) - 0.5f, xi2 = rnd(key, kDimCam + 1) - 0.5f;
     const float fx = x * S.rcp_w + xi1 * S.rcp_w, fy = y * S.rcp_h + xi2 * S.rcp_h;
@@ -288,7 +294,8 @@ __global__ void __launch_bounds__(256) k_shade(RenderDev R, int cur, uint32_t de
         const float4 o = R.q_o[cur][i], d = R.q_d[cur][i];
         const int ti = R.hit_tri[i];
         uint64_t key;
-        path_ident(S, wave_begin + path, pixel, key);
+        uint32_t px, py;
+        path_ident(S, wave_begin + path, pixel, key, px, py);
         pixel += S.pixel_base;
         float3 beta = make_float3(R.beta[path].x, R.beta[path].y, R.beta[path].z);
         float3 add = make_float3(0.f, 0.f, 0.f);
@@ -317,6 +324,9 @@ __global__ void __launch_bounds__(256) k_shade(RenderDev R, int cur, uint32_t de
             // (DiffuseAreaLight::Radiance, DiffuseAreaLight.cpp:47-50)
             if (depth == 0 && light_id != 0xffffu && light_id < S.n_lights && dot3(W, wo) > 0.f)
                 add = add + beta * S.lights[light_id].emit;
+            // RadianceContext::Albedo = the first hit's Material::Rho
+            // (PathIntegrator.cpp:121); for the GGX conductor, its F0
+            if (depth == 0 && R.accum_albedo) add_pixel(R.accum_albedo, pixel, m.kind == 1u ? m.f0 : m.albedo);
 
             if (depth < S.max_depth && R.cache_depth && tslot == 0xffffffffu && depth == R.cache_depth) {
                 // a rendering path stops here: the cache supplies the radiance leaving this vertex
@@ -402,7 +412,11 @@ __global__ void __launch_bounds__(256) k_shade(RenderDev R, int cur, uint32_t de
                 }
             }
         }
-        if (!is_black(add)) add_pixel(R.accum, pixel, add);
+        if (!is_black(add)) {
+            add_pixel(R.accum, pixel, add);
+            // what the first vertex adds is RadianceContext::Direct (PathIntegrator.cpp:102)
+            if (depth == 0 && R.accum_direct) add_pixel(R.accum_direct, pixel, add);
+        }
     }
 
     const uint32_t slot = push_slot(cont, &R.count[nxt]);
@@ -422,7 +436,9 @@ __global__ void __launch_bounds__(256) k_shade(RenderDev R, int cur, uint32_t de
             if (s < R.sh_capacity) {
                 R.s_o[s] = so[k];
                 R.s_d[s] = sd[k];
-                R.s_c[s] = make_float4(sc[k].x, sc[k].y, sc[k].z, __uint_as_float(pixel));
+                // bit 31 marks a light sample of the first vertex (Direct)
+                const uint32_t tag = (depth == 0 && R.accum_direct) ? 0x80000000u : 0u;
+                R.s_c[s] = make_float4(sc[k].x, sc[k].y, sc[k].z, __uint_as_float(pixel | tag));
                 R.s_sid[s] = sid;
                 if (R.cache_depth) R.s_meta[s] = tslot == 0xffffffffu ? 0xffffffffu : ((tslot << 8) | depth);
             } else {
@@ -468,7 +484,9 @@ __global__ void __launch_bounds__(256) k_shadow(RenderDev R)
     trace_one<true, false>(S.nodes, S.tris, S.n_nodes, S.n_tris, o, d, best, bt, bu, bv, R.err, nn, nt);
     if (best == -1) {
         const float4 c = R.s_c[i];
-        add_pixel(R.accum, __float_as_uint(c.w), make_float3(c.x, c.y, c.z));
+        const uint32_t bits = __float_as_uint(c.w);
+        add_pixel(R.accum, bits & 0x7fffffffu, make_float3(c.x, c.y, c.z));
+        if (bits >> 31) add_pixel(R.accum_direct, bits & 0x7fffffffu, make_float3(c.x, c.y, c.z));
         if (R.cache_depth) {
             const uint32_t meta = R.s_meta[i];
             if (meta != 0xffffffffu) credit(R, meta >> 8, meta & 0xffu, make_float3(c.x, c.y, c.z));

@@ -39,7 +39,10 @@ struct SceneRec {
     float3 sky;
     // camera (PerspectiveCamera after SetFieldOfView)
     float3 centre, corner, across, up;
-    uint32_t width, height, wh;
+    uint32_t width, height;  // the whole image (the camera's normalisation)
+    uint32_t wh;             // pixels rendered: the region's
+    uint32_t region_x, region_y, region_w;  // the rendered region of the image
+    uint32_t full_wh;        // width * height: the sample-sequence stride
     float rcp_w, rcp_h;
     uint32_t max_depth;
     float eps;
@@ -68,6 +71,8 @@ struct RenderDev {
     uint32_t *sh_count;
     uint32_t sh_capacity;
     float4 *accum;         // per pixel rgb sums
+    float4 *accum_direct;  // per pixel sums of the first vertex's emission and light samples (or null)
+    float4 *accum_albedo;  // per pixel sums of the first hit's albedo (or null)
     uint32_t *err;
 
     // radiance cache (cache_depth == 0: plain path tracing, none of this is used)

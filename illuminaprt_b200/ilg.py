@@ -28,7 +28,8 @@ EXPORTED = ["ilg_create", "ilg_destroy", "ilg_last_error", "ilg_set_mesh", "ilg_
             "ilg_intersect", "ilg_intersect_counted", "ilg_occluded", "ilg_sync", "ilg_stream",
             "ilg_set_materials", "ilg_set_quad_lights", "ilg_render", "ilg_intersect_noalloc",
             "ilg_mlp_init", "ilg_mlp_get_params", "ilg_mlp_set_params", "ilg_mlp_infer", "ilg_mlp_grads",
-            "ilg_mlp_train_step", "ilg_render_batch", "ilg_intersect_excluding", "ilg_occluded_excluding"]
+            "ilg_mlp_train_step", "ilg_render_batch", "ilg_intersect_excluding", "ilg_occluded_excluding",
+            "ilg_camera_frame_of", "ilg_render_region"]
 
 ILG_MLP_RAW = 16
 ILG_MLP_WARP_MMA = 0x10
@@ -68,6 +69,16 @@ class ilg_quad_light(ctypes.Structure):
 class ilg_camera(ctypes.Structure):
     _fields_ = [("eye", ctypes.c_float * 3), ("target", ctypes.c_float * 3), ("up", ctypes.c_float * 3),
                 ("fov_deg", ctypes.c_float), ("aspect", ctypes.c_float)]
+
+
+class ilg_camera_frame(ctypes.Structure):
+    _fields_ = [("centre", ctypes.c_float * 3), ("corner", ctypes.c_float * 3), ("across", ctypes.c_float * 3),
+                ("up", ctypes.c_float * 3)]
+
+
+class ilg_region(ctypes.Structure):
+    _fields_ = [("x", ctypes.c_uint32), ("y", ctypes.c_uint32), ("width", ctypes.c_uint32),
+                ("height", ctypes.c_uint32)]
 
 
 class ilg_batch_item(ctypes.Structure):
@@ -119,6 +130,9 @@ def load(build_if_missing: bool = True) -> ctypes.CDLL:
     L.ilg_set_quad_lights.argtypes = [vp, vp, u32]
     L.ilg_render.argtypes = [vp, ctypes.POINTER(ilg_camera), ctypes.POINTER(ilg_render_opts), vp, u32]
     L.ilg_intersect_noalloc.argtypes = [vp, vp, vp, u32, vp, vp, vp, vp]
+    L.ilg_camera_frame_of.argtypes = [ctypes.POINTER(ilg_camera), ctypes.POINTER(ilg_camera_frame)]
+    L.ilg_render_region.argtypes = [vp, ctypes.POINTER(ilg_camera_frame), ctypes.POINTER(ilg_render_opts),
+                                    ctypes.POINTER(ilg_region), vp, vp, vp, u32]
     L.ilg_intersect_excluding.argtypes = [vp, vp, vp, u32, u32, u32, vp, vp, vp, vp, u32]
     L.ilg_occluded_excluding.argtypes = [vp, vp, vp, u32, u32, u32, vp, u32]
     L.ilg_intersect_noalloc.restype = i32
@@ -271,17 +285,44 @@ class GpuSpace:
             arr[i].first_tri = int(l["first_tri"])
         self._check(self.L.ilg_set_quad_lights(self.h, ctypes.addressof(arr), len(lights)))
 
-    def render(self, camera: dict, width: int, height: int, spp: int, max_depth: int = 6, epsilon: float = 1e-4,
-               seed: int = 1, sky=(0.0, 0.0, 0.0), paths_per_wave: int = 0, out=None, cache_depth: int = 0,
-               train_every: int = 16, train_steps: int = 4, train_batch: int = 16384):
-        """Returns (height, width, 3) float32 (or fills `out`, a CUDA tensor, in place).
-        cache_depth > 0 renders with the radiance cache (mlp_init first) and trains it afterwards."""
+    @staticmethod
+    def _camera(camera: dict, width: int, height: int) -> ilg_camera:
         cam = ilg_camera()
         cam.eye[:] = list(camera["eye"])
         cam.target[:] = list(camera["target"])
         cam.up[:] = list(camera["up"])
         cam.fov_deg = float(camera["fov"])
         cam.aspect = float(camera.get("aspect", width / height))
+        return cam
+
+    def camera_frame(self, camera: dict, width: int, height: int) -> ilg_camera_frame:
+        """The (centre, corner, across, up) frame the reference's PerspectiveCamera builds."""
+        f = ilg_camera_frame()
+        self._check(self.L.ilg_camera_frame_of(ctypes.byref(self._camera(camera, width, height)), ctypes.byref(f)))
+        return f
+
+    def render_region(self, frame: ilg_camera_frame, width: int, height: int, spp: int, region, max_depth: int = 6,
+                      epsilon: float = 1e-4, seed: int = 1, sky=(0.0, 0.0, 0.0), aux: bool = True):
+        """IRenderer::RenderRegion: region = (x, y, w, h) of the width x height image.
+        Returns (final, direct, albedo), each (h, w, 3) float32 (direct/albedo None without aux)."""
+        x, y, w, h = (int(v) for v in region)
+        o = ilg_render_opts(width=width, height=height, spp=spp, max_depth=max_depth, epsilon=epsilon, seed=seed)
+        o.sky[:] = list(sky)
+        r = ilg_region(x=x, y=y, width=w, height=h)
+        final = np.empty((h, w, 3), np.float32)
+        direct = np.empty((h, w, 3), np.float32) if aux else None
+        albedo = np.empty((h, w, 3), np.float32) if aux else None
+        self._check(self.L.ilg_render_region(self.h, ctypes.byref(frame), ctypes.byref(o), ctypes.byref(r),
+                                             final.ctypes.data, direct.ctypes.data if aux else None,
+                                             albedo.ctypes.data if aux else None, 0))
+        return final, direct, albedo
+
+    def render(self, camera: dict, width: int, height: int, spp: int, max_depth: int = 6, epsilon: float = 1e-4,
+               seed: int = 1, sky=(0.0, 0.0, 0.0), paths_per_wave: int = 0, out=None, cache_depth: int = 0,
+               train_every: int = 16, train_steps: int = 4, train_batch: int = 16384):
+        """Returns (height, width, 3) float32 (or fills `out`, a CUDA tensor, in place).
+        cache_depth > 0 renders with the radiance cache (mlp_init first) and trains it afterwards."""
+        cam = self._camera(camera, width, height)
         o = ilg_render_opts(width=width, height=height, spp=spp, max_depth=max_depth, epsilon=epsilon, seed=seed,
                             paths_per_wave=paths_per_wave, cache_depth=cache_depth, train_every=train_every,
                             train_steps=train_steps, train_batch=train_batch)

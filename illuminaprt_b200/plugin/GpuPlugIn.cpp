@@ -1,16 +1,20 @@
-// The plug-in that registers GpuSpace with the engine: a "GPU" factory in the
-// EngineKernel's SpaceManager (System/EngineKernel.h:54, typedef
-// FactoryManager<ISpace> SpaceManager in Space/Space.h:42), so a scene
-// description naming space type "GPU" gets the device space. It exports the
+// The plug-in that registers the device space and renderer with the engine:
+// factory "GPU" in the EngineKernel's SpaceManager (System/EngineKernel.h:54,
+// FactoryManager<ISpace>, Space/Space.h:42) makes a GpuSpace, and factory
+// "GPU" in its RendererManager (FactoryManager<IRenderer>,
+// Renderer/Renderer.h:80) makes a GpuRenderer, so a scene description naming
+// space or renderer type "GPU" gets the device path. It exports the
 // symbol set that the reference's LibraryManager looks up in a plug-in
 // library (System/LibrarySymbols.h, System/LibraryManager.cpp:62-170):
 // GetPlugInSingleton, DisposePlugInSingleton, CreatePlugInInstance,
 // GetPlugInInstance, DisposePlugInInstance, DisposePlugInInstances.
 //
-// Factory arguments (ArgumentMap): Id (instance name), Device (CUDA ordinal,
-// default 0).
+// Factory arguments (ArgumentMap). Space: Id (instance name), Device (CUDA
+// ordinal, default 0). Renderer: Id, Samples (per pixel, default 1, as
+// BasicRendererFactory, Renderer/RendererFactories.h:34-44), Seed (default 1).
 #include <string>
 
+#include "GpuRenderer.h"
 #include "GpuSpace.h"
 #include "System/ArgumentMap.h"
 #include "System/EngineKernel.h"
@@ -38,10 +42,29 @@ public:
     }
 };
 
+class GpuRendererFactory : public Factory<IRenderer> {
+public:
+    IRenderer *CreateInstance(void) { return new GpuRenderer(); }
+
+    IRenderer *CreateInstance(ArgumentMap &p_argumentMap)
+    {
+        int samples = 1, seed = 1;
+        std::string id = "GpuRenderer";
+        p_argumentMap.GetArgument("Samples", samples);
+        p_argumentMap.GetArgument("Seed", seed);
+        p_argumentMap.GetArgument("Id", id);
+        return new GpuRenderer(id, NULL, NULL, NULL, NULL, NULL, samples, (uint32_t)seed);
+    }
+};
+
 class GpuPlugIn : public IPlugIn {
 public:
-    GpuPlugIn(void) : m_strName("GPU Space"), m_version(1, 0, 0), m_pFactory(NULL) {}
-    ~GpuPlugIn(void) { delete m_pFactory; }
+    GpuPlugIn(void) : m_strName("GPU Space"), m_version(1, 0, 0), m_pFactory(NULL), m_pRendererFactory(NULL) {}
+    ~GpuPlugIn(void)
+    {
+        delete m_pFactory;
+        delete m_pRendererFactory;
+    }
 
     const std::string &GetName(void) const { return m_strName; }
     const Version &GetVersion(void) const { return m_version; }
@@ -49,12 +72,15 @@ public:
     void Register(EngineKernel *p_pEngineKernel)
     {
         if (!m_pFactory) m_pFactory = new GpuSpaceFactory();
+        if (!m_pRendererFactory) m_pRendererFactory = new GpuRendererFactory();
         p_pEngineKernel->GetSpaceManager()->RegisterFactory("GPU", m_pFactory);
+        p_pEngineKernel->GetRendererManager()->RegisterFactory("GPU", m_pRendererFactory);
     }
 
     void Unregister(EngineKernel *p_pEngineKernel)
     {
         p_pEngineKernel->GetSpaceManager()->UnregisterFactory("GPU");
+        p_pEngineKernel->GetRendererManager()->UnregisterFactory("GPU");
     }
 
     void Initialise(void) {}
@@ -64,6 +90,7 @@ private:
     std::string m_strName;
     Version m_version;
     GpuSpaceFactory *m_pFactory;
+    GpuRendererFactory *m_pRendererFactory;
 };
 
 }  // namespace PlugIn

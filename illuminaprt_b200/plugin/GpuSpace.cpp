@@ -1,5 +1,6 @@
 // GpuSpace: ISpace over the device BVH. See GpuSpace.h for the contract.
 #include "GpuSpace.h"
+#include "EngineAccess.h"
 
 #include <cmath>
 #include <cstdio>
@@ -25,16 +26,6 @@ namespace PlugIn {
 
 namespace {
 
-// Quad keeps its two triangles protected (Shape/Quad.h:23); a member pointer
-// formed in a derived class's scope reads them without changing the shape.
-struct QuadTriangles : public Quad {
-    static const Triangle *Of(const Quad *p_pQuad)
-    {
-        Triangle(Quad::*member)[2] = &QuadTriangles::m_tesselatedQuad;
-        return (p_pQuad->*member);
-    }
-};
-
 // te1 x te2 in the component order of the reference's CROSS macro
 // (Shape/IndexedTriangle.cpp:16-19); the plug-in is compiled without FMA
 // contraction, so each component rounds as there.
@@ -46,13 +37,14 @@ inline Vector3 EdgeCross(const Vector3 &a, const Vector3 &b)
 }  // namespace
 
 GpuSpace::GpuSpace(const std::string &p_strName, int p_nDevice)
-    : ISpace(p_strName), m_nDevice(p_nDevice), m_pContext(NULL), m_bBuilt(false), m_pOrigin4(NULL),
-      m_pDirection4(NULL)
+    : ISpace(p_strName), m_nDevice(p_nDevice), m_pContext(NULL), m_bBuilt(false), m_nBuildCount(0),
+      m_pOrigin4(NULL), m_pDirection4(NULL)
 {
 }
 
 GpuSpace::GpuSpace(void)
-    : ISpace(), m_nDevice(0), m_pContext(NULL), m_bBuilt(false), m_pOrigin4(NULL), m_pDirection4(NULL)
+    : ISpace(), m_nDevice(0), m_pContext(NULL), m_bBuilt(false), m_nBuildCount(0), m_pOrigin4(NULL),
+      m_pDirection4(NULL)
 {
 }
 
@@ -111,9 +103,22 @@ bool GpuSpace::Build(void)
     std::lock_guard<std::mutex> lock(m_mutex);
     m_triangles.clear();
     m_ranges.clear();
+    m_materials.clear();
     m_aabb.Invalidate();
     std::vector<float> positions;
-    std::vector<uint32_t> indices;
+    std::vector<uint32_t> indices, slots;
+
+    // material slot of one triangle, resolved as FillIntersection resolves it
+    auto slot_of = [&](IMaterial *material, const IShape *triangle) -> uint32_t {
+        if (material != NULL && material->IsComposite()) {
+            MaterialGroup *group = (MaterialGroup *)material;
+            material = triangle->HasGroup() ? group->GetByGroupId(triangle->GetGroupId()) : group->GetByIndex(0);
+        }
+        for (size_t k = 0; k < m_materials.size(); k++)
+            if (m_materials[k] == material) return (uint32_t)k;
+        m_materials.push_back(material);
+        return (uint32_t)(m_materials.size() - 1);
+    };
 
     // One world-space triangle: three fresh vertices (no sharing), so each
     // device triangle's edges are p1 - p0 and p2 - p0 of exactly these floats.
@@ -152,18 +157,21 @@ bool GpuSpace::Build(void)
                      mesh->VertexList[tri.GetVertexIndex(2)].Position, xf);
                 TriangleSource src = {(uint32_t)index, kMesh, &tri, mesh};
                 m_triangles.push_back(src);
+                slots.push_back(slot_of(geometric->GetMaterial(), &tri));
             }
         } else if (Quad *quad = dynamic_cast<Quad *>(shape)) {
-            const Triangle *half = QuadTriangles::Of(quad);
+            const Triangle *half = Access::QuadTriangles::Of(quad);
             for (int k = 0; k < 2; k++) {
                 push(half[k].Vertex[0], half[k].Vertex[1], half[k].Vertex[2], xf);
                 TriangleSource src = {(uint32_t)index, kTriangle, &half[k], NULL};
                 m_triangles.push_back(src);
+                slots.push_back(slot_of(geometric->GetMaterial(), &half[k]));
             }
         } else if (Triangle *tri = dynamic_cast<Triangle *>(shape)) {
             push(tri->Vertex[0], tri->Vertex[1], tri->Vertex[2], xf);
             TriangleSource src = {(uint32_t)index, kTriangle, tri, NULL};
             m_triangles.push_back(src);
+            slots.push_back(slot_of(geometric->GetMaterial(), tri));
         } else {
             std::ostringstream s;
             s << "GpuSpace: primitive " << index << " has a shape the device space does not trace ("
@@ -178,7 +186,7 @@ bool GpuSpace::Build(void)
     if (m_triangles.size() > 0x7fffffffu) return Fail("GpuSpace: too many triangles");
 
     int status = ilg_set_mesh(m_pContext, positions.data(), (uint32_t)(positions.size() / 3), indices.data(),
-                              (uint32_t)m_triangles.size(), NULL);
+                              (uint32_t)m_triangles.size(), slots.data());
     if (status == ILG_OK) status = ilg_build(m_pContext);
     if (status != ILG_OK) {
         std::ostringstream s;
@@ -186,7 +194,17 @@ bool GpuSpace::Build(void)
         return Fail(s.str());
     }
     m_bBuilt = true;
+    m_nBuildCount++;
     m_strLastError.clear();
+    return true;
+}
+
+bool GpuSpace::GetTriangleRange(const IPrimitive *p_pPrimitive, uint32_t &p_nFirst, uint32_t &p_nCount) const
+{
+    const PrimitiveRange *range = FindRange(p_pPrimitive);
+    if (!range) return false;
+    p_nFirst = range->first;
+    p_nCount = range->count;
     return true;
 }
 

@@ -44,6 +44,7 @@ class ITriangleMesh;
 class IndexedTriangle;
 class Triangle;
 class IAreaLight;
+class IMaterial;
 }  // namespace Core
 
 namespace PlugIn {
@@ -75,6 +76,18 @@ public:
 
     // Triangles handed to the device (valid after Build).
     size_t GetTriangleCount(void) const { return m_triangles.size(); }
+
+    // For a device renderer over this space (GpuRenderer): the device
+    // context, the material of every device triangle as a slot into
+    // GetMaterialSlots() (one slot per distinct IMaterial*, MaterialGroups
+    // resolved per triangle as the hit record resolves them; a primitive
+    // without material gets a NULL slot), a primitive's triangle range, and
+    // a counter that changes with every successful Build.
+    ilg_ctx *GetContext(void) const { return m_pContext; }
+    const std::vector<Illumina::Core::IMaterial *> &GetMaterialSlots(void) const { return m_materials; }
+    bool GetTriangleRange(const Illumina::Core::IPrimitive *p_pPrimitive, uint32_t &p_nFirst,
+                          uint32_t &p_nCount) const;
+    uint64_t GetBuildCount(void) const { return m_nBuildCount; }
     const std::string &GetLastError(void) const { return m_strLastError; }
     std::string ToString(void) const { return "GpuSpace"; }
 
@@ -107,6 +120,8 @@ private:
     Illumina::Core::AxisAlignedBoundingBox m_aabb;
     std::vector<TriangleSource> m_triangles;
     std::vector<PrimitiveRange> m_ranges;
+    std::vector<Illumina::Core::IMaterial *> m_materials;
+    uint64_t m_nBuildCount;
     std::string m_strLastError;
 
     // staging for the device calls (guarded by m_mutex)

@@ -188,6 +188,40 @@ int ilg_set_quad_lights(ilg_ctx *ctx, const ilg_quad_light *lights, uint32_t n);
 int ilg_render(ilg_ctx *ctx, const ilg_camera *cam, const ilg_render_opts *opts, float *out_rgb,
                uint32_t flags);
 
+/* A camera as the reference's ICamera holds it after construction
+ * (Core/Camera/Camera.h:23-28: m_centre, m_corner, m_across, m_up): the ray
+ * through normalised image point (px, py) is normalize(corner + across * px
+ * + up * py - centre) (PerspectiveCamera::GetRay, PerspectiveCamera.cpp:44-60). */
+typedef struct ilg_camera_frame {
+    float centre[3];
+    float corner[3];
+    float across[3];
+    float up[3];
+} ilg_camera_frame;
+
+/* The frame PerspectiveCamera(eye, normalize(target - eye), up, -1, 1, -1, 1, 1)
+ * + SetFieldOfView(fov_deg, aspect) builds (Core/Camera/Camera.cpp:30-44). */
+int ilg_camera_frame_of(const ilg_camera *cam, ilg_camera_frame *out);
+
+/* Pixels [x, x + width) x [y, y + height) of the opts->width x opts->height image. */
+typedef struct ilg_region {
+    uint32_t x, y, width, height;
+} ilg_region;
+
+/* IRenderer::RenderRegion(buffer, x, y, w, h) with a PathIntegrator
+ * (BaseRenderer.cpp:62-169): renders one region of the image, each pixel
+ * with exactly the paths a whole-image render gives it (same seed), so
+ * regions tile the image seamlessly. Outputs are region-sized (region height
+ * x width x 3): final_rgb = RadianceContext::Final; direct_rgb (optional) =
+ * RadianceContext::Direct, what the first vertex adds (emission seen
+ * directly and its light samples; Indirect = Final - Direct); albedo_rgb
+ * (optional) = RadianceContext::Albedo, the first hit's reflectance. All are
+ * per-sample averages. Host pointers unless ILG_DEVICE_PTRS. The radiance
+ * cache options of opts are not used here. */
+int ilg_render_region(ilg_ctx *ctx, const ilg_camera_frame *frame, const ilg_render_opts *opts,
+                      const ilg_region *region, float *final_rgb, float *direct_rgb, float *albedo_rgb,
+                      uint32_t flags);
+
 /* ------------------------------------------------------------------------
  * Radiance-cache network (no counterpart in the reference, whose closest
  * analogue is the irradiance cache of Core/Integrator/ICIntegrator.*): a

@@ -157,6 +157,9 @@ class RefLib:
         c = ctypes
         L.ilref_render_box_plugin.argtypes = [c.c_char_p, c.c_char_p] + list(L.ilref_render_box.argtypes) + [
             c.c_char_p, c.c_int]
+        L.ilref_render_box_aov.argtypes = list(L.ilref_render_box.argtypes) + [_f32p, _f32p]
+        L.ilref_render_box_renderer.argtypes = ([c.c_char_p, c.c_char_p] + list(L.ilref_render_box.argtypes[:17])
+                                                + [c.c_float, c.c_int, _f32p, _f32p, _f32p, c.c_char_p, c.c_int])
         L.ilref_compare_spaces.argtypes = [c.c_char_p, c.c_char_p, _f32p, _i32p, c.c_int, c.c_int, _f32p, c.c_int,
                                            _f32p, _f32p, _f32p, _f32p, c.c_long, c.c_void_p, _u8p, _f32p,
                                            c.c_void_p, _u8p, _u8p, _f32p, _u8p, c.c_char_p, c.c_int]
@@ -198,6 +201,35 @@ class RefLib:
         if rc:
             raise RuntimeError(f"ilref_render_box_plugin: {rc}: {err.value.decode(errors='replace')}")
         return out
+
+    def render_box_aov(self, scene: dict, width: int, height: int, spp: int, seed: int = 1, nthreads=None):
+        """render_box plus the RadianceContext Direct and Albedo: (final, direct, albedo)."""
+        f = lambda a: np.ascontiguousarray(a, np.float32)
+        cam = scene["camera"]
+        outs = [np.zeros((height, width, 3), np.float32) for _ in range(3)]
+        self.L.ilref_render_box_aov(*self._scene_args(scene), f(cam["eye"]), f(cam["target"]), f(cam["up"]),
+                                    float(cam["fov"]), float(cam["aspect"]), width, height, spp,
+                                    int(scene["max_depth"]), float(scene["epsilon"]), seed,
+                                    nthreads or os.cpu_count() or 1, *(o.reshape(-1) for o in outs))
+        return tuple(outs)
+
+    def render_box_renderer(self, plugin: str, scene: dict, width: int, height: int, spp: int, tile: int = 0,
+                            factory: str = "GPU"):
+        """The box scene through the plug-in's renderer over its space, driven by
+        the engine's objects; tile > 0 renders tile x tile RenderRegion calls.
+        Returns (final, direct, albedo) from the RadianceBuffer."""
+        f = lambda a: np.ascontiguousarray(a, np.float32)
+        cam = scene["camera"]
+        outs = [np.zeros((height, width, 3), np.float32) for _ in range(3)]
+        err = ctypes.create_string_buffer(512)
+        rc = self.L.ilref_render_box_renderer(plugin.encode(), factory.encode(), *self._scene_args(scene),
+                                              f(cam["eye"]), f(cam["target"]), f(cam["up"]), float(cam["fov"]),
+                                              float(cam["aspect"]), width, height, spp, int(scene["max_depth"]),
+                                              float(scene["epsilon"]), tile, *(o.reshape(-1) for o in outs),
+                                              err, 512)
+        if rc:
+            raise RuntimeError(f"ilref_render_box_renderer: {rc}: {err.value.decode(errors='replace')}")
+        return tuple(outs)
 
     def compare_spaces(self, plugin: str, scene: dict, o4, d4, exclude=None, factory: str = "GPU"):
         """BasicSpace vs the plug-in's space on the same primitives, ray by ray

@@ -45,10 +45,15 @@
 #include "Sampler/RandomSampler.h"
 #include "Filter/BoxFilter.h"
 #include "System/EngineKernel.h"
+#include "System/ArgumentMap.h"
+#include "Device/Device.h"
+#include "Renderer/Renderer.h"
+#include "Exception/Exception.h"
 #include "System/PlugIn.h"
 #include "System/PlugInManager.h"
 
 #include <dlfcn.h>
+#include <map>
 #include <string>
 
 using namespace Illumina::Core;
@@ -189,7 +194,7 @@ struct BoxScene
 // Reference renderer loop over any space (see ilref_render_box).
 void render_over(ISpace &space, ILight *light, const float *eye, const float *target, const float *up, float fov,
                  float aspect, int width, int height, int spp, int max_depth, float eps, uint32_t seed,
-                 int nthreads, float *out)
+                 int nthreads, float *out, float *out_direct = nullptr, float *out_albedo = nullptr)
 {
 	PerspectiveCamera camera(Vector3(eye[0], eye[1], eye[2]),
 	                         Vector3::Normalize(Vector3(target[0], target[1], target[2]) - Vector3(eye[0], eye[1], eye[2])),
@@ -225,16 +230,27 @@ void render_over(ISpace &space, ILight *light, const float *eye, const float *ta
 					filter(samples.data(), spp);
 					ctx.SurfacePosition.Set((float)x, (float)y);
 					ctx.NormalisedPosition.Set(x * rcpW, y * rcpH);
-					Spectrum acc(0.f);
+					Spectrum acc(0.f), direct(0.f), albedo(0.f);
 					for (ctx.SampleIndex = 0; ctx.SampleIndex < spp; ctx.SampleIndex++) {
 						Ray ray;
 						camera.GetRay(ctx.NormalisedPosition.X, ctx.NormalisedPosition.Y,
 						              samples[ctx.SampleIndex].U * rcpW, samples[ctx.SampleIndex].V * rcpH, ray);
 						acc += integrator.Radiance(&ctx, &scene, ray, isect, &rc);
+						direct += rc.Direct;
+						albedo += rc.Albedo;
 					}
 					acc *= rcpS;
-					float *o = out + 3 * ((size_t)y * width + x);
+					const size_t px = 3 * ((size_t)y * width + x);
+					float *o = out + px;
 					o[0] = acc[0]; o[1] = acc[1]; o[2] = acc[2];
+					if (out_direct) {
+						direct *= rcpS;
+						for (int c = 0; c < 3; c++) out_direct[px + c] = direct[c];
+					}
+					if (out_albedo) {
+						albedo *= rcpS;
+						for (int c = 0; c < 3; c++) out_albedo[px + c] = albedo[c];
+					}
 				}
 		}
 	};
@@ -242,6 +258,30 @@ void render_over(ISpace &space, ILight *light, const float *eye, const float *ta
 	for (int i = 0; i < nthreads; i++) pool.emplace_back(worker);
 	for (auto &th : pool) th.join();
 }
+
+// An IDevice that only has a size: what BaseRenderer asks of its device
+// (GetWidth / GetHeight for normalisation) plus no-op frame calls.
+class MemoryDevice : public IDevice
+{
+	int m_w, m_h;
+
+public:
+	MemoryDevice(int w, int h) : m_w(w), m_h(h) {}
+	int GetWidth(void) const { return m_w; }
+	int GetHeight(void) const { return m_h; }
+	AccessType GetAccessType(void) const { return Write; }
+	bool Open(void) { return true; }
+	void Close(void) {}
+	void BeginFrame(void) {}
+	void EndFrame(void) {}
+	void Set(int, int, const Spectrum &) {}
+	void Set(float, float, const Spectrum &) {}
+	void Get(int, int, Spectrum &s) const { s = Spectrum(0.f); }
+	void Get(float, float, Spectrum &s) const { s = Spectrum(0.f); }
+	Spectrum Get(int, int) const { return Spectrum(0.f); }
+	Spectrum Get(float, float) const { return Spectrum(0.f); }
+	void WriteRadianceBufferToDevice(int, int, int, int, RadianceBuffer *, int, int) {}
+};
 
 // A space made by a plug-in's factory (see ilref_render_box_plugin).
 struct PluginSpace
@@ -426,6 +466,105 @@ int ilref_render_box(const float *pos, const int32_t *prim_of_tri, int ntris, in
 	scene.fill(space);
 	render_over(space, scene.light, eye, target, up, fov, aspect, width, height, spp, max_depth, eps, seed,
 	            nthreads, out);
+	return 0;
+}
+
+// ilref_render_box plus the RadianceContext's Direct and Albedo per pixel,
+// averaged over the samples as BaseRenderer::RenderRegion averages them
+// (Core/Renderer/BaseRenderer.cpp:95-130).
+int ilref_render_box_aov(const float *pos, const int32_t *prim_of_tri, int ntris, int nprims,
+                         const float *albedo, int light_prim, const float *quad, const float *emit,
+                         const float *eye, const float *target, const float *up, float fov, float aspect,
+                         int width, int height, int spp, int max_depth, float eps, uint32_t seed,
+                         int nthreads, float *out, float *out_direct, float *out_albedo)
+{
+	BoxScene scene;
+	scene.create(pos, prim_of_tri, ntris, nprims, albedo, light_prim, quad, emit);
+	BasicSpace space;
+	scene.fill(space);
+	render_over(space, scene.light, eye, target, up, fov, aspect, width, height, spp, max_depth, eps, seed,
+	            nthreads, out, out_direct, out_albedo);
+	return 0;
+}
+
+// The box scene through a plug-in's renderer and space (both made by the
+// factories registered under `factory`): the engine's own objects (Scene,
+// PerspectiveCamera, PathIntegrator(max_depth, 1, eps), BoxFilter,
+// RadianceBuffer) wired to the renderer as the Sandbox wires a BasicRenderer,
+// and rendered with IRenderer::Render(buffer) (tile <= 0) or with
+// RenderRegion(buffer, x, y, w, h, x, y) over tile x tile regions. Outputs
+// the buffer's Final, Direct and Albedo (height x width x 3 each).
+int ilref_render_box_renderer(const char *plugin_path, const char *factory,
+                              const float *pos, const int32_t *prim_of_tri, int ntris, int nprims,
+                              const float *albedo, int light_prim, const float *quad, const float *emit,
+                              const float *eye, const float *target, const float *up, float fov, float aspect,
+                              int width, int height, int spp, int max_depth, float eps, int tile,
+                              float *out, float *out_direct, float *out_albedo, char *err, int err_len)
+{
+	PluginSpace ps;
+	int rc = ps.open(plugin_path, factory, err, err_len);
+	if (rc) return rc;
+	Factory<IRenderer> *rf = ps.kernel->GetRendererManager()->RequestFactory(factory);
+	if (!rf) {
+		report(err, err_len, std::string("no renderer factory named ") + factory);
+		return -3;
+	}
+	BoxScene boxes;
+	boxes.create(pos, prim_of_tri, ntris, nprims, albedo, light_prim, quad, emit);
+	boxes.fill(*ps.space);
+	if (!ps.space->Initialise() || !ps.space->Build()) {
+		ps.report_build_failure(err, err_len);
+		return -4;
+	}
+	PerspectiveCamera camera(Vector3(eye[0], eye[1], eye[2]),
+	                         Vector3::Normalize(Vector3(target[0], target[1], target[2]) - Vector3(eye[0], eye[1], eye[2])),
+	                         Vector3(up[0], up[1], up[2]), -1.f, 1.f, -1.f, 1.f, 1.f);
+	camera.SetFieldOfView(fov, aspect);
+	RandomSampler sampler;
+	Scene scene(ps.space, &camera, &sampler);
+	if (boxes.light) scene.LightList.PushBack(boxes.light);
+	PathIntegrator integrator(max_depth, 1, eps);
+	integrator.Initialise(&scene, &camera);
+	BoxFilter filter;
+	MemoryDevice device(width, height);
+	RadianceBuffer buffer(width, height);
+	IRenderer *renderer = nullptr;
+	try {
+		std::map<std::string, std::string> args;
+		args["Samples"] = std::to_string(spp);
+		ArgumentMap am(args);
+		renderer = rf->CreateInstance(am);
+		renderer->SetScene(&scene);
+		renderer->SetIntegrator(&integrator);
+		renderer->SetDevice(&device);
+		renderer->SetFilter(&filter);
+		// (IRenderer::SetRadianceBuffer is declared but never defined in the
+		// engine, so the buffer goes to the calls that take one)
+		renderer->Initialise();
+		if (tile <= 0) {
+			renderer->Render(&buffer);
+		} else {
+			for (int y = 0; y < height; y += tile)
+				for (int x = 0; x < width; x += tile)
+					renderer->RenderRegion(&buffer, x, y, std::min(tile, width - x), std::min(tile, height - y), x, y);
+		}
+		renderer->Commit(&buffer);
+	} catch (const Exception &e) {
+		report(err, err_len, e.GetMessage());
+		delete renderer;
+		return -5;
+	}
+	for (int y = 0; y < height; y++)
+		for (int x = 0; x < width; x++) {
+			const RadianceContext *c = buffer.GetP(x, y);
+			const size_t px = 3 * ((size_t)y * width + x);
+			for (int k = 0; k < 3; k++) {
+				out[px + k] = c->Final[k];
+				out_direct[px + k] = c->Direct[k];
+				out_albedo[px + k] = c->Albedo[k];
+			}
+		}
+	delete renderer;
 	return 0;
 }
 

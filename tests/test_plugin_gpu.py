@@ -86,3 +86,35 @@ def test_reference_path_integrator_over_gpu_space():
     # a path diverges only where a near tie picked the other of two coincident
     # surfaces (shared edges of the box walls)
     assert same.mean() >= 0.99, f"{int((~same).sum())} of {same.size} pixels differ"
+
+
+def _rel_mse(x, ref, eps=1e-2):
+    return float(np.mean((x.astype(np.float64) - ref) ** 2 / (ref.astype(np.float64) ** 2 + eps)))
+
+
+def test_gpu_renderer_through_the_engine_matches_the_reference_image():
+    # the engine's Scene / camera / PathIntegrator / filter / RadianceBuffer
+    # driving the plug-in's GpuRenderer over its GpuSpace, against the
+    # reference's own 4096-spp render of the same scene
+    import glob
+    paths = sorted(glob.glob(os.path.join(os.path.dirname(__file__), "golden", "box_256_4096spp_seed*.npz")))
+    if not paths:
+        pytest.skip("no reference image")
+    ref_img = np.load(paths[0])["image"]
+    scene = scenes.box_scene()
+    final, direct, albedo = bindings.RefLib().render_box_renderer(pkg_build.PLUGIN, scene, 256, 256, 1024)
+    err = _rel_mse(final, ref_img)
+    print(f"relMSE(GpuRenderer 1024 spp, reference 4096 spp) = {err:.2e}")
+    assert np.isfinite(final).all()
+    assert err < 1e-3
+    assert np.allclose(final.mean((0, 1)), ref_img.mean((0, 1)), rtol=1e-2)
+    assert (direct <= final + 1e-4).all() and albedo.mean() > 0.2
+
+
+def test_gpu_renderer_regions_tile_the_frame():
+    scene = scenes.box_scene()
+    ref = bindings.RefLib()
+    whole = ref.render_box_renderer(pkg_build.PLUGIN, scene, 100, 72, 4)
+    tiled = ref.render_box_renderer(pkg_build.PLUGIN, scene, 100, 72, 4, tile=32)
+    for a, b in zip(whole, tiled):  # same paths; float atomics may sum them in another order
+        assert np.allclose(a, b, rtol=1e-5, atol=1e-6)
