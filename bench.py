@@ -427,6 +427,19 @@ def main():
     e2e_value = world * rays_per_step * e2e_steps / (e2e_ms / 1e3) / 1e6
     # the e2e hits must equal the device-resident ones
     assert torch.equal(hout["incoherent"][0], out["incoherent"][0].cpu())
+    # the copy bound of e2e: the same host->device bytes as one plain pinned copy
+    h2d_src = torch.cat([pin["coherent"][0], pin["coherent"][1], pin["incoherent"][0],
+                         pin["incoherent"][1]]).pin_memory()
+    h2d_dst = torch.empty_like(h2d_src, device=dev)
+    h2d_dst.copy_(h2d_src, non_blocking=True)
+    c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    c0.record()
+    for _ in range(3):
+        h2d_dst.copy_(h2d_src, non_blocking=True)
+    c1.record()
+    c1.synchronize()
+    h2d_gbs = 3 * h2d_src.numel() * h2d_src.element_size() / (c0.elapsed_time(c1) / 1e3) / 1e9
+    del h2d_src, h2d_dst
 
     pt = {} if args.no_path_tracer else bench_path_tracer(dev, local, tuple(args.legs.split(",")))
     hbm, peak_kind = load_peaks()
@@ -457,7 +470,11 @@ def main():
                        "bvh_nodes": stats["n_nodes"], "bvh_build_ms": round(stats["build_ms"], 3),
                        "scene_bytes": stats["node_bytes"] + stats["tri_bytes"], **pt},
             "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": rays_per_step * RAY_IN,
-                    "d2h_bytes_per_step": rays_per_step * HIT_OUT},
+                    "d2h_bytes_per_step": rays_per_step * HIT_OUT,
+                    "pinned_h2d_gbs": round(h2d_gbs, 2),
+                    "copy_bound_mrays_s": round(h2d_gbs * 1e3 / RAY_IN, 3),
+                    "pipeline": "host-buffer calls run in chunks over three streams: upload, traversal and "
+                                "download of neighbouring chunks overlap"},
             "gpu_launches": 2 * args.steps,
             "roofline": {"bound": "hbm", "achieved": round(achieved, 2), "peak": hbm, "unit": "GB/s",
                          "frac": round(achieved / hbm, 4), "traffic": traffic,

@@ -47,6 +47,77 @@ int fail(ilg_ctx *c, int code, const char *fmt, ...)
                         cudaGetErrorString(e_));                                                     \
     } while (0)
 
+namespace {
+
+// Closest hit (occ == nullptr) or any hit of rays in host memory. Large
+// batches go in chunks round-robin over three streams, so the upload of one
+// chunk, the traversal of the previous one and the download of the one
+// before that run at once; for host-resident rays the PCIe copies, not the
+// traversal, bound the call.
+int query_host(ilg_ctx *ctx, const float *o4, const float *d4, uint32_t n, int32_t *prim, float *t, float *u,
+               float *v, uint8_t *occ)
+{
+    const bool any = occ != nullptr;
+    CK(ctx->ro.reserve(n));
+    CK(ctx->rd.reserve(n));
+    if (any) {
+        CK(ctx->hocc.reserve(n));
+    } else {
+        CK(ctx->hprim.reserve(n));
+        CK(ctx->ht.reserve(n));
+        CK(ctx->hu.reserve(n));
+        CK(ctx->hv.reserve(n));
+    }
+    const uint32_t kMinChunk = 1u << 18, kMaxChunks = 8u;
+    const uint32_t chunks = n >= 2u * kMinChunk ? std::min<uint32_t>(kMaxChunks, n / kMinChunk) : 1u;
+    const uint32_t chunk = ((n + chunks - 1) / chunks + 127u) & ~127u;
+    cudaStream_t ss[3] = {ctx->stream, ctx->stream, ctx->stream};
+    if (chunks > 1) {
+        for (int k = 0; k < 2; k++)
+            if (!ctx->side[k]) CK(cudaStreamCreateWithFlags(&ctx->side[k], cudaStreamNonBlocking));
+        for (int k = 0; k < 3; k++)
+            if (!ctx->side_ev[k]) CK(cudaEventCreateWithFlags(&ctx->side_ev[k], cudaEventDisableTiming));
+        // the side streams start after everything already queued on the main one
+        CK(cudaEventRecord(ctx->side_ev[2], ctx->stream));
+        for (int k = 0; k < 2; k++) {
+            CK(cudaStreamWaitEvent(ctx->side[k], ctx->side_ev[2], 0));
+            ss[1 + k] = ctx->side[k];
+        }
+    }
+    const SceneView sv = ctx->view();
+    uint32_t c = 0;
+    for (uint32_t off = 0; off < n; off += chunk, c++) {
+        const uint32_t len = std::min(chunk, n - off);
+        cudaStream_t st = ss[c % 3];
+        uint32_t *next = ctx->derr.ptr + 1 + (c % 3);  // ray counter of this stream's persistent kernels
+        CK(cudaMemcpyAsync(ctx->ro.ptr + off, o4 + 4ull * off, 16ull * len, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(ctx->rd.ptr + off, d4 + 4ull * off, 16ull * len, cudaMemcpyHostToDevice, st));
+        if (any) {
+            CK(launch_any_dyn(sv, ctx->ro.ptr + off, ctx->rd.ptr + off, len, ctx->hocc.ptr + off, next, ctx->derr.ptr,
+                              st));
+            CK(cudaMemcpyAsync(occ + off, ctx->hocc.ptr + off, len, cudaMemcpyDeviceToHost, st));
+        } else {
+            CK(launch_closest_dyn(sv, ctx->ro.ptr + off, ctx->rd.ptr + off, len, ctx->hprim.ptr + off,
+                                  ctx->ht.ptr + off, ctx->hu.ptr + off, ctx->hv.ptr + off, next, ctx->derr.ptr, st));
+            CK(cudaMemcpyAsync(prim + off, ctx->hprim.ptr + off, 4ull * len, cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(t + off, ctx->ht.ptr + off, 4ull * len, cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(u + off, ctx->hu.ptr + off, 4ull * len, cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(v + off, ctx->hv.ptr + off, 4ull * len, cudaMemcpyDeviceToHost, st));
+        }
+    }
+    if (chunks > 1) {
+        // the main stream ends after the side streams' work
+        for (int k = 0; k < 2; k++) {
+            CK(cudaEventRecord(ctx->side_ev[k], ctx->side[k]));
+            CK(cudaStreamWaitEvent(ctx->stream, ctx->side_ev[k], 0));
+        }
+    }
+    CK(cudaStreamSynchronize(ctx->stream));
+    return ctx->check_device_error();
+}
+
+}  // namespace
+
 extern "C" {
 
 int ilg_create(ilg_ctx **out, const ilg_opts *opts)
@@ -77,9 +148,15 @@ int ilg_destroy(ilg_ctx *ctx)
     if (!ctx) return ILG_EINVAL;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
+    for (auto s : ctx->side)
+        if (s) cudaStreamSynchronize(s);
     ctx->release_all();
     cudaEventDestroy(ctx->ev0);
     cudaEventDestroy(ctx->ev1);
+    for (auto e : ctx->side_ev)
+        if (e) cudaEventDestroy(e);
+    for (auto s : ctx->side)
+        if (s) cudaStreamDestroy(s);
     cudaStreamDestroy(ctx->stream);
     delete ctx;
     return ILG_OK;
@@ -191,23 +268,7 @@ int ilg_intersect(ilg_ctx *ctx, const float *ray_o_tmin, const float *ray_d_tmax
                               ctx->derr.ptr, ctx->stream));
         return ILG_OK;
     }
-    CK(ctx->ro.reserve(n));
-    CK(ctx->rd.reserve(n));
-    CK(ctx->hprim.reserve(n));
-    CK(ctx->ht.reserve(n));
-    CK(ctx->hu.reserve(n));
-    CK(ctx->hv.reserve(n));
-    cudaStream_t st = ctx->stream;
-    CK(cudaMemcpyAsync(ctx->ro.ptr, ray_o_tmin, 16ull * n, cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(ctx->rd.ptr, ray_d_tmax, 16ull * n, cudaMemcpyHostToDevice, st));
-    CK(launch_closest_dyn(sv, ctx->ro.ptr, ctx->rd.ptr, n, ctx->hprim.ptr, ctx->ht.ptr, ctx->hu.ptr, ctx->hv.ptr,
-                          next, ctx->derr.ptr, st));
-    CK(cudaMemcpyAsync(prim, ctx->hprim.ptr, 4ull * n, cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(t, ctx->ht.ptr, 4ull * n, cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(u, ctx->hu.ptr, 4ull * n, cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(v, ctx->hv.ptr, 4ull * n, cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    return ctx->check_device_error();
+    return query_host(ctx, ray_o_tmin, ray_d_tmax, n, prim, t, u, v, nullptr);
 }
 
 int ilg_intersect_counted(ilg_ctx *ctx, const float *ray_o_tmin, const float *ray_d_tmax, uint32_t n, int32_t *prim,
@@ -248,16 +309,7 @@ int ilg_occluded(ilg_ctx *ctx, const float *ray_o_tmin, const float *ray_d_tmax,
                           ctx->stream));
         return ILG_OK;
     }
-    CK(ctx->ro.reserve(n));
-    CK(ctx->rd.reserve(n));
-    CK(ctx->hocc.reserve(n));
-    cudaStream_t st = ctx->stream;
-    CK(cudaMemcpyAsync(ctx->ro.ptr, ray_o_tmin, 16ull * n, cudaMemcpyHostToDevice, st));
-    CK(cudaMemcpyAsync(ctx->rd.ptr, ray_d_tmax, 16ull * n, cudaMemcpyHostToDevice, st));
-    CK(launch_any_dyn(sv, ctx->ro.ptr, ctx->rd.ptr, n, ctx->hocc.ptr, next, ctx->derr.ptr, st));
-    CK(cudaMemcpyAsync(occ, ctx->hocc.ptr, n, cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    return ctx->check_device_error();
+    return query_host(ctx, ray_o_tmin, ray_d_tmax, n, nullptr, nullptr, nullptr, nullptr, occ);
 }
 
 int ilg_intersect_excluding(ilg_ctx *ctx, const float *ray_o_tmin, const float *ray_d_tmax, uint32_t n,

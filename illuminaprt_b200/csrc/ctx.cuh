@@ -13,6 +13,9 @@ struct ilg_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    // two more streams for chunked host-buffer queries (made on first use)
+    cudaStream_t side[2] = {nullptr, nullptr};
+    cudaEvent_t side_ev[3] = {nullptr, nullptr, nullptr};
     char err[512] = {0};
 
     // mesh as uploaded
