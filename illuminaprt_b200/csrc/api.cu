@@ -68,7 +68,7 @@ int query_host(ilg_ctx *ctx, const float *o4, const float *d4, uint32_t n, int32
         CK(ctx->hu.reserve(n));
         CK(ctx->hv.reserve(n));
     }
-    const uint32_t kMinChunk = 1u << 18, kMaxChunks = 8u;
+    const uint32_t kMinChunk = 1u << 17, kMaxChunks = 16u;
     const uint32_t chunks = n >= 2u * kMinChunk ? std::min<uint32_t>(kMaxChunks, n / kMinChunk) : 1u;
     const uint32_t chunk = ((n + chunks - 1) / chunks + 127u) & ~127u;
     cudaStream_t ss[3] = {ctx->stream, ctx->stream, ctx->stream};
@@ -631,11 +631,41 @@ static int run_render(ilg_ctx *ctx, std::vector<SceneRec> &recs, uint32_t cap_re
         mlp = ctx->mlp_view();
     }
 
+    // The frame (every wave, every bounce) is one CUDA graph. Nothing in it
+    // depends on the host between launches (queue counts stay on the device),
+    // so a call whose launch configuration equals the previous one replays
+    // the instantiated graph; a different one is captured afresh.
     uint32_t launches = 0;
-    for (uint64_t g0 = 0; g0 < total; g0 += cap) {
-        const uint32_t k = (uint32_t)std::min<uint64_t>(cap, total - g0);
-        CK(render_wave(R, k, g0, st, &launches, cache_depth ? &mlp : nullptr, block));
+    unsigned char key[sizeof(RenderDev) + sizeof(MlpDev) + 4 * sizeof(uint64_t)];
+    {
+        const uint64_t extra[4] = {cap, total, block, cache_depth};
+        memcpy(key, &R, sizeof(RenderDev));
+        memcpy(key + sizeof(RenderDev), &mlp, sizeof(MlpDev));
+        memcpy(key + sizeof(RenderDev) + sizeof(MlpDev), extra, sizeof(extra));
     }
+    if (!ctx->graph_exec || ctx->graph_key.size() != sizeof(key) || memcmp(ctx->graph_key.data(), key, sizeof(key))) {
+        ctx->drop_graph();
+        CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
+        cudaError_t ce = cudaSuccess;
+        for (uint64_t g0 = 0; g0 < total && ce == cudaSuccess; g0 += cap) {
+            const uint32_t k = (uint32_t)std::min<uint64_t>(cap, total - g0);
+            ce = render_wave(R, k, g0, st, &launches, cache_depth ? &mlp : nullptr, block);
+        }
+        cudaGraph_t graph = nullptr;
+        const cudaError_t ee = cudaStreamEndCapture(st, &graph);
+        if (ce == cudaSuccess) ce = ee;
+        if (ce == cudaSuccess) ce = cudaGraphInstantiate(&ctx->graph_exec, graph, 0);
+        if (graph) cudaGraphDestroy(graph);
+        if (ce != cudaSuccess) {
+            ctx->graph_exec = nullptr;
+            CK(ce);
+        }
+        ctx->graph_key.assign(key, key + sizeof(key));
+        ctx->graph_kernels = launches;
+    } else {
+        launches = ctx->graph_kernels;
+    }
+    CK(cudaGraphLaunch(ctx->graph_exec, st));
     if (cache_depth) {
         // online training on this call's records (the next call renders with the update)
         uint32_t n_rec = 0;

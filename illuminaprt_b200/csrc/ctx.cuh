@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cstdio>
+#include <vector>
 
 #include "build.cuh"
 #include "ilg.h"
@@ -63,6 +64,16 @@ struct ilg_ctx {
     uint32_t last_train_records = 0;
     float last_train_loss = 0.f;
     uint32_t last_render_launches = 0;
+    // the last frame's instantiated CUDA graph and the launch configuration it was captured for
+    cudaGraphExec_t graph_exec = nullptr;
+    std::vector<unsigned char> graph_key;
+    uint32_t graph_kernels = 0;
+    void drop_graph()
+    {
+        if (graph_exec) cudaGraphExecDestroy(graph_exec);
+        graph_exec = nullptr;
+        graph_key.clear();
+    }
 
     // radiance-cache network
     ilg::DevBuf<float> mlp_w, mlp_m, mlp_v, mlp_grad, mlp_loss, mlp_raw, mlp_tgt, mlp_out;
@@ -102,6 +113,7 @@ struct ilg_ctx {
 
     void release_all()
     {
+        drop_graph();
         pos.release(); idx.release(); mat.release();
         bb.release_all();
         ro.release(); rd.release(); hprim.release(); ht.release(); hu.release(); hv.release(); hocc.release();

@@ -133,6 +133,7 @@ __device__ __forceinline__ void path_ident(const SceneRec &S, uint64_t g, uint32
 __global__ void k_camera(RenderDev R, uint32_t n_paths, uint64_t wave_begin)
 {
     const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p == 0) R.count[0] = n_paths;  // the wave's first extend queue is every path
     if (p >= n_paths) return;
     const uint64_t g = wave_begin + p;
     const uint32_t sid = scene_of(R, g);
@@ -549,8 +550,7 @@ cudaError_t render_wave(const RenderDev &R, uint32_t n_paths, uint64_t wave_begi
             cudaSuccess)
             return e;
     }
-    k_camera<<<blocks_for(n_paths, 128), 128, 0, st>>>(R, n_paths, wave_begin);
-    if ((e = cudaMemcpyAsync(R.count, &n_paths, sizeof(uint32_t), cudaMemcpyHostToDevice, st)) != cudaSuccess) return e;
+    k_camera<<<blocks_for(n_paths, 128), 128, 0, st>>>(R, n_paths, wave_begin);  // also sets count[0]
     uint32_t n_launch = 1;
     int cur = 0;
     for (uint32_t depth = 0; depth <= R.depth_max; depth++) {
