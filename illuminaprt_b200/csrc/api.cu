@@ -68,7 +68,7 @@ int query_host(ilg_ctx *ctx, const float *o4, const float *d4, uint32_t n, int32
         CK(ctx->hu.reserve(n));
         CK(ctx->hv.reserve(n));
     }
-    const uint32_t kMinChunk = 1u << 17, kMaxChunks = 16u;
+    const uint32_t kMinChunk = 1u << 18, kMaxChunks = 8u;
     const uint32_t chunks = n >= 2u * kMinChunk ? std::min<uint32_t>(kMaxChunks, n / kMinChunk) : 1u;
     const uint32_t chunk = ((n + chunks - 1) / chunks + 127u) & ~127u;
     cudaStream_t ss[3] = {ctx->stream, ctx->stream, ctx->stream};
