@@ -401,6 +401,21 @@ def main():
     rays_per_step = n_co + n_in
     value = world * rays_per_step * args.steps / (total_ms / 1e3) / 1e6
 
+    # the same incoherent batch with the watertight triangle test (ILG_WATERTIGHT)
+    o, d = rays["incoherent"]
+    wt_out = [torch.empty_like(x) for x in out["incoherent"]]
+    sp.intersects_into(o, d, *wt_out, device_ptrs=True, watertight=True)
+    w0, w1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    w0.record(stream)
+    for _ in range(args.steps):
+        sp.intersects_into(o, d, *wt_out, device_ptrs=True, watertight=True)
+    w1.record(stream)
+    sp.sync()
+    w1.synchronize()
+    wt_mrays = n_in * args.steps / (w0.elapsed_time(w1) / 1e3) / 1e6
+    wt_same = float((wt_out[0] == out["incoherent"][0]).float().mean().item())
+    del wt_out
+
     # end to end through the public API: pinned host rays in, hits out
     pin = {k: (torch.from_numpy(v[0].cpu().numpy()).pin_memory(), torch.from_numpy(v[1].cpu().numpy()).pin_memory())
            for k, v in rays.items()}
@@ -467,6 +482,8 @@ def main():
                        "parallelism": f"replicas x{world}",
                        "coherent_mrays_s": round(n_co * args.steps / (t_co / 1e3) / 1e6, 3),
                        "incoherent_mrays_s": round(n_in * args.steps / (t_in / 1e3) / 1e6, 3),
+                       "incoherent_watertight_mrays_s": round(wt_mrays, 3),
+                       "watertight_same_hit_fraction": round(wt_same, 6),
                        "bvh_nodes": stats["n_nodes"], "bvh_build_ms": round(stats["build_ms"], 3),
                        "scene_bytes": stats["node_bytes"] + stats["tri_bytes"], **pt},
             "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": rays_per_step * RAY_IN,

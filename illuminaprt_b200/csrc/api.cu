@@ -49,13 +49,25 @@ int fail(ilg_ctx *c, int code, const char *fmt, ...)
 
 namespace {
 
+// The watertight test reads each triangle record's own vertices; they are
+// copied out of the uploaded mesh once per build, on first use.
+int ensure_raw_tris(ilg_ctx *ctx)
+{
+    if (ctx->raw_ready) return ILG_OK;
+    const uint32_t n = ctx->stats.n_tris;
+    CK(ctx->raw_tris.reserve(3ull * n));
+    CK(build_raw_tris(ctx->bb.prim_of, ctx->idx.ptr, ctx->pos.ptr, n, ctx->raw_tris.ptr, ctx->stream));
+    ctx->raw_ready = true;
+    return ILG_OK;
+}
+
 // Closest hit (occ == nullptr) or any hit of rays in host memory. Large
 // batches go in chunks round-robin over three streams, so the upload of one
 // chunk, the traversal of the previous one and the download of the one
 // before that run at once; for host-resident rays the PCIe copies, not the
 // traversal, bound the call.
 int query_host(ilg_ctx *ctx, const float *o4, const float *d4, uint32_t n, int32_t *prim, float *t, float *u,
-               float *v, uint8_t *occ)
+               float *v, uint8_t *occ, bool wt)
 {
     const bool any = occ != nullptr;
     CK(ctx->ro.reserve(n));
@@ -92,13 +104,23 @@ int query_host(ilg_ctx *ctx, const float *o4, const float *d4, uint32_t n, int32
         uint32_t *next = ctx->derr.ptr + 1 + (c % 3);  // ray counter of this stream's persistent kernels
         CK(cudaMemcpyAsync(ctx->ro.ptr + off, o4 + 4ull * off, 16ull * len, cudaMemcpyHostToDevice, st));
         CK(cudaMemcpyAsync(ctx->rd.ptr + off, d4 + 4ull * off, 16ull * len, cudaMemcpyHostToDevice, st));
-        if (any) {
+        if (any && wt) {
+            CK(launch_any_wt(sv, ctx->raw_tris.ptr, ctx->ro.ptr + off, ctx->rd.ptr + off, len, ctx->hocc.ptr + off,
+                             next, ctx->derr.ptr, st));
+            CK(cudaMemcpyAsync(occ + off, ctx->hocc.ptr + off, len, cudaMemcpyDeviceToHost, st));
+        } else if (any) {
             CK(launch_any_dyn(sv, ctx->ro.ptr + off, ctx->rd.ptr + off, len, ctx->hocc.ptr + off, next, ctx->derr.ptr,
                               st));
             CK(cudaMemcpyAsync(occ + off, ctx->hocc.ptr + off, len, cudaMemcpyDeviceToHost, st));
         } else {
-            CK(launch_closest_dyn(sv, ctx->ro.ptr + off, ctx->rd.ptr + off, len, ctx->hprim.ptr + off,
-                                  ctx->ht.ptr + off, ctx->hu.ptr + off, ctx->hv.ptr + off, next, ctx->derr.ptr, st));
+            if (wt)
+                CK(launch_closest_wt(sv, ctx->raw_tris.ptr, ctx->ro.ptr + off, ctx->rd.ptr + off, len,
+                                     ctx->hprim.ptr + off, ctx->ht.ptr + off, ctx->hu.ptr + off, ctx->hv.ptr + off,
+                                     next, ctx->derr.ptr, st));
+            else
+                CK(launch_closest_dyn(sv, ctx->ro.ptr + off, ctx->rd.ptr + off, len, ctx->hprim.ptr + off,
+                                      ctx->ht.ptr + off, ctx->hu.ptr + off, ctx->hv.ptr + off, next, ctx->derr.ptr,
+                                      st));
             CK(cudaMemcpyAsync(prim + off, ctx->hprim.ptr + off, 4ull * len, cudaMemcpyDeviceToHost, st));
             CK(cudaMemcpyAsync(t + off, ctx->ht.ptr + off, 4ull * len, cudaMemcpyDeviceToHost, st));
             CK(cudaMemcpyAsync(u + off, ctx->hu.ptr + off, 4ull * len, cudaMemcpyDeviceToHost, st));
@@ -240,6 +262,7 @@ int ilg_build(ilg_ctx *ctx)
     ctx->stats.tri_bytes = (uint64_t)res.n_tris * sizeof(Tri);
     ctx->built = true;
     ctx->attr_dirty = true;
+    ctx->raw_ready = false;
     return ILG_OK;
 }
 
@@ -254,7 +277,8 @@ int ilg_intersect(ilg_ctx *ctx, const float *ray_o_tmin, const float *ray_d_tmax
                   float *t, float *u, float *v, uint32_t flags)
 {
     if (!ctx) return ILG_EINVAL;
-    if (flags & ~ILG_DEVICE_PTRS) return fail(ctx, ILG_EINVAL, "ilg_intersect: unknown flags 0x%x", flags);
+    if (flags & ~(ILG_DEVICE_PTRS | ILG_WATERTIGHT))
+        return fail(ctx, ILG_EINVAL, "ilg_intersect: unknown flags 0x%x", flags);
     if (!ctx->built) return fail(ctx, ILG_ESTATE, "ilg_intersect: scene not built");
     if (n == 0) return ILG_OK;
     if (!ray_o_tmin || !ray_d_tmax || !prim || !t || !u || !v) return fail(ctx, ILG_EINVAL, "ilg_intersect: null array");
@@ -263,12 +287,21 @@ int ilg_intersect(ilg_ctx *ctx, const float *ray_o_tmin, const float *ray_d_tmax
     CK(cudaSetDevice(ctx->device));
     const SceneView sv = ctx->view();
     uint32_t *next = ctx->derr.ptr + 1;  // ray counter of the persistent kernels
+    const bool wt = (flags & ILG_WATERTIGHT) != 0;
+    if (wt) {
+        int rc = ensure_raw_tris(ctx);
+        if (rc) return rc;
+    }
     if (flags & ILG_DEVICE_PTRS) {
-        CK(launch_closest_dyn(sv, (const float4 *)ray_o_tmin, (const float4 *)ray_d_tmax, n, prim, t, u, v, next,
-                              ctx->derr.ptr, ctx->stream));
+        if (wt)
+            CK(launch_closest_wt(sv, ctx->raw_tris.ptr, (const float4 *)ray_o_tmin, (const float4 *)ray_d_tmax, n,
+                                 prim, t, u, v, next, ctx->derr.ptr, ctx->stream));
+        else
+            CK(launch_closest_dyn(sv, (const float4 *)ray_o_tmin, (const float4 *)ray_d_tmax, n, prim, t, u, v, next,
+                                  ctx->derr.ptr, ctx->stream));
         return ILG_OK;
     }
-    return query_host(ctx, ray_o_tmin, ray_d_tmax, n, prim, t, u, v, nullptr);
+    return query_host(ctx, ray_o_tmin, ray_d_tmax, n, prim, t, u, v, nullptr, wt);
 }
 
 int ilg_intersect_counted(ilg_ctx *ctx, const float *ray_o_tmin, const float *ray_d_tmax, uint32_t n, int32_t *prim,
@@ -295,7 +328,8 @@ int ilg_occluded(ilg_ctx *ctx, const float *ray_o_tmin, const float *ray_d_tmax,
                  uint32_t flags)
 {
     if (!ctx) return ILG_EINVAL;
-    if (flags & ~ILG_DEVICE_PTRS) return fail(ctx, ILG_EINVAL, "ilg_occluded: unknown flags 0x%x", flags);
+    if (flags & ~(ILG_DEVICE_PTRS | ILG_WATERTIGHT))
+        return fail(ctx, ILG_EINVAL, "ilg_occluded: unknown flags 0x%x", flags);
     if (!ctx->built) return fail(ctx, ILG_ESTATE, "ilg_occluded: scene not built");
     if (n == 0) return ILG_OK;
     if (!ray_o_tmin || !ray_d_tmax || !occ) return fail(ctx, ILG_EINVAL, "ilg_occluded: null array");
@@ -304,12 +338,21 @@ int ilg_occluded(ilg_ctx *ctx, const float *ray_o_tmin, const float *ray_d_tmax,
     CK(cudaSetDevice(ctx->device));
     const SceneView sv = ctx->view();
     uint32_t *next = ctx->derr.ptr + 1;
+    const bool wt = (flags & ILG_WATERTIGHT) != 0;
+    if (wt) {
+        int rc = ensure_raw_tris(ctx);
+        if (rc) return rc;
+    }
     if (flags & ILG_DEVICE_PTRS) {
-        CK(launch_any_dyn(sv, (const float4 *)ray_o_tmin, (const float4 *)ray_d_tmax, n, occ, next, ctx->derr.ptr,
-                          ctx->stream));
+        if (wt)
+            CK(launch_any_wt(sv, ctx->raw_tris.ptr, (const float4 *)ray_o_tmin, (const float4 *)ray_d_tmax, n, occ,
+                             next, ctx->derr.ptr, ctx->stream));
+        else
+            CK(launch_any_dyn(sv, (const float4 *)ray_o_tmin, (const float4 *)ray_d_tmax, n, occ, next, ctx->derr.ptr,
+                              ctx->stream));
         return ILG_OK;
     }
-    return query_host(ctx, ray_o_tmin, ray_d_tmax, n, nullptr, nullptr, nullptr, nullptr, occ);
+    return query_host(ctx, ray_o_tmin, ray_d_tmax, n, nullptr, nullptr, nullptr, nullptr, occ, wt);
 }
 
 int ilg_intersect_excluding(ilg_ctx *ctx, const float *ray_o_tmin, const float *ray_d_tmax, uint32_t n,

@@ -88,4 +88,77 @@ __device__ __forceinline__ bool shirley(const Tri &tr, float ox, float oy, float
     return true;
 }
 
+// ---------------------------------------------------------------------------
+// Watertight test (Woop, Benthin and Wald 2013, "Watertight Ray/Triangle
+// Intersection", JCGT 2(1)): the triangle is sheared into the ray's frame
+// (the ray's largest direction component becomes z) and the three 2D edge
+// functions U, V, W are evaluated from the vertices themselves, so two
+// triangles that share an edge evaluate it with the same numbers and a ray
+// through it cannot slip between them. Edge functions that come out exactly
+// zero are recomputed in double. Every operation is rounded separately. The
+// rejection window is the reference's (t < 1e-5 or t > Max - 1e-5); beta
+// and gamma are the weights of v1 and v2, as in the reference.
+// ---------------------------------------------------------------------------
+struct Shear {
+    uint32_t kx, ky, kz;
+    float sx, sy, sz;
+};
+
+__device__ __forceinline__ float pick(float x, float y, float z, uint32_t k) { return k == 0u ? x : (k == 1u ? y : z); }
+
+__device__ __forceinline__ Shear shear_of(float dx, float dy, float dz)
+{
+    const float ax = fabsf(dx), ay = fabsf(dy), az = fabsf(dz);
+    Shear s;
+    s.kz = ax >= ay ? (ax >= az ? 0u : 2u) : (ay >= az ? 1u : 2u);
+    s.kx = s.kz == 2u ? 0u : s.kz + 1u;
+    s.ky = s.kx == 2u ? 0u : s.kx + 1u;
+    const float dkz = pick(dx, dy, dz, s.kz);
+    if (dkz < 0.f) {
+        const uint32_t k = s.kx;
+        s.kx = s.ky;
+        s.ky = k;
+    }
+    s.sx = __fdiv_rn(pick(dx, dy, dz, s.kx), dkz);
+    s.sy = __fdiv_rn(pick(dx, dy, dz, s.ky), dkz);
+    s.sz = __fdiv_rn(1.0f, dkz);
+    return s;
+}
+
+// v0, v1, v2: the triangle's own vertices (w unused).
+__device__ __forceinline__ bool watertight(float4 v0, float4 v1, float4 v2, float ox, float oy, float oz,
+                                           const Shear &sh, float hi, float &t_out, float &b_out, float &g_out)
+{
+    const float a0 = __fsub_rn(v0.x, ox), a1 = __fsub_rn(v0.y, oy), a2 = __fsub_rn(v0.z, oz);
+    const float b0 = __fsub_rn(v1.x, ox), b1 = __fsub_rn(v1.y, oy), b2 = __fsub_rn(v1.z, oz);
+    const float c0 = __fsub_rn(v2.x, ox), c1 = __fsub_rn(v2.y, oy), c2 = __fsub_rn(v2.z, oz);
+    const float akz = pick(a0, a1, a2, sh.kz), bkz = pick(b0, b1, b2, sh.kz), ckz = pick(c0, c1, c2, sh.kz);
+    const float Ax = __fsub_rn(pick(a0, a1, a2, sh.kx), __fmul_rn(sh.sx, akz));
+    const float Ay = __fsub_rn(pick(a0, a1, a2, sh.ky), __fmul_rn(sh.sy, akz));
+    const float Bx = __fsub_rn(pick(b0, b1, b2, sh.kx), __fmul_rn(sh.sx, bkz));
+    const float By = __fsub_rn(pick(b0, b1, b2, sh.ky), __fmul_rn(sh.sy, bkz));
+    const float Cx = __fsub_rn(pick(c0, c1, c2, sh.kx), __fmul_rn(sh.sx, ckz));
+    const float Cy = __fsub_rn(pick(c0, c1, c2, sh.ky), __fmul_rn(sh.sy, ckz));
+    float U = __fsub_rn(__fmul_rn(Cx, By), __fmul_rn(Cy, Bx));
+    float V = __fsub_rn(__fmul_rn(Ax, Cy), __fmul_rn(Ay, Cx));
+    float W = __fsub_rn(__fmul_rn(Bx, Ay), __fmul_rn(By, Ax));
+    if (U == 0.f || V == 0.f || W == 0.f) {
+        U = __double2float_rn(__dsub_rn(__dmul_rn(Cx, By), __dmul_rn(Cy, Bx)));
+        V = __double2float_rn(__dsub_rn(__dmul_rn(Ax, Cy), __dmul_rn(Ay, Cx)));
+        W = __double2float_rn(__dsub_rn(__dmul_rn(Bx, Ay), __dmul_rn(By, Ax)));
+    }
+    if ((U < 0.f || V < 0.f || W < 0.f) && (U > 0.f || V > 0.f || W > 0.f)) return false;
+    const float det = __fadd_rn(__fadd_rn(U, V), W);
+    if (det == 0.f) return false;
+    const float Az = __fmul_rn(sh.sz, akz), Bz = __fmul_rn(sh.sz, bkz), Cz = __fmul_rn(sh.sz, ckz);
+    const float T = __fadd_rn(__fadd_rn(__fmul_rn(U, Az), __fmul_rn(V, Bz)), __fmul_rn(W, Cz));
+    const float rcp = __fdiv_rn(1.0f, det);
+    const float t = __fmul_rn(T, rcp);
+    if (!(t <= hi) || t < window_lo()) return false;
+    t_out = t;
+    b_out = __fmul_rn(V, rcp);
+    g_out = __fmul_rn(W, rcp);
+    return true;
+}
+
 }  // namespace ilg

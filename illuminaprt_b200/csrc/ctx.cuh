@@ -32,6 +32,10 @@ struct ilg_ctx {
     bool built = false;
     ilg_stats stats = {};
 
+    // the watertight test's vertex records (three float4 per triangle record)
+    ilg::DevBuf<float4> raw_tris;
+    bool raw_ready = false;
+
     // staging for host-pointer queries
     ilg::DevBuf<float4> ro, rd;
     ilg::DevBuf<int32_t> hprim;
@@ -116,6 +120,7 @@ struct ilg_ctx {
         drop_graph();
         pos.release(); idx.release(); mat.release();
         bb.release_all();
+        raw_tris.release(); raw_ready = false;
         ro.release(); rd.release(); hprim.release(); ht.release(); hu.release(); hv.release(); hocc.release();
         derr.release(); dstats.release();
         mats.release(); lights.release(); light_first_tri.release(); tri_attr.release(); light_of_prim.release();

@@ -55,8 +55,9 @@ __global__ void __launch_bounds__(128) k_any(const Node8 *__restrict__ nodes, co
     occ[i] = best >= 0 ? 1 : 0;
 }
 
-// Persistent closest / any hit with dynamic ray fetch (see trace.cuh).
-template <bool kAnyHit>
+// Persistent closest / any hit with dynamic ray fetch (see trace.cuh);
+// kWT: the watertight triangle test over `raw`.
+template <bool kAnyHit, bool kWT = false>
 __global__ void __launch_bounds__(128) k_trace_dyn(const Node8 *__restrict__ nodes, const Tri *__restrict__ tris,
                                                    const uint32_t *__restrict__ prim_of, uint32_t n_nodes_total,
                                                    uint32_t n_tris_total, const float4 *__restrict__ ro,
@@ -64,7 +65,7 @@ __global__ void __launch_bounds__(128) k_trace_dyn(const Node8 *__restrict__ nod
                                                    int32_t *__restrict__ prim, float *__restrict__ tout,
                                                    float *__restrict__ uout, float *__restrict__ vout,
                                                    uint8_t *__restrict__ occ, uint32_t *__restrict__ next,
-                                                   uint32_t *__restrict__ err)
+                                                   uint32_t *__restrict__ err, const float4 *__restrict__ raw = nullptr)
 {
     const uint32_t lane = threadIdx.x & 31u;
     uint2 stack[kMaxStack];
@@ -83,13 +84,14 @@ __global__ void __launch_bounds__(128) k_trace_dyn(const Node8 *__restrict__ nod
                 const uint32_t k = base + __popc(idle & ((1u << lane) - 1u));
                 if (k < n) {
                     id = k;
-                    ray_init(r, __ldcs(ro + id), __ldcs(rd + id), n_nodes_total);
+                    ray_init<kWT>(r, __ldcs(ro + id), __ldcs(rd + id), n_nodes_total);
                     active = true;
                 }
             }
         }
         if (__ballot_sync(0xffffffffu, active) == 0u) break;
-        if (active && ray_step<kAnyHit>(r, stack, nodes, tris, n_nodes_total, n_tris_total, err)) {
+        if (active && ray_step<kAnyHit, false, false, kWT>(r, stack, nodes, tris, n_nodes_total, n_tris_total, err,
+                                                            nullptr, nullptr, Skip{nullptr, 0u, 0u}, raw)) {
             if (kAnyHit) {
                 occ[id] = r.best >= 0 ? 1 : 0;
             } else {
@@ -138,6 +140,54 @@ cudaError_t launch_any_dyn(const SceneView &s, const float4 *ro, const float4 *r
     const uint32_t blocks = std::min<uint32_t>((n + 127) / 128, (uint32_t)sm_count() * 16u);
     k_trace_dyn<true><<<blocks, 128, 0, st>>>(s.nodes, s.tris, nullptr, s.n_nodes, s.n_tris, ro, rd, n, nullptr,
                                               nullptr, nullptr, nullptr, occ, next, err);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_closest_wt(const SceneView &s, const float4 *raw, const float4 *ro, const float4 *rd, uint32_t n,
+                              int32_t *prim, float *t, float *u, float *v, uint32_t *next, uint32_t *err,
+                              cudaStream_t st)
+{
+    if (n == 0) return cudaSuccess;
+    cudaError_t e = cudaMemsetAsync(next, 0, sizeof(uint32_t), st);
+    if (e != cudaSuccess) return e;
+    const uint32_t blocks = std::min<uint32_t>((n + 127) / 128, (uint32_t)sm_count() * 16u);
+    k_trace_dyn<false, true><<<blocks, 128, 0, st>>>(s.nodes, s.tris, s.prim_of, s.n_nodes, s.n_tris, ro, rd, n,
+                                                     prim, t, u, v, nullptr, next, err, raw);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_any_wt(const SceneView &s, const float4 *raw, const float4 *ro, const float4 *rd, uint32_t n,
+                          uint8_t *occ, uint32_t *next, uint32_t *err, cudaStream_t st)
+{
+    if (n == 0) return cudaSuccess;
+    cudaError_t e = cudaMemsetAsync(next, 0, sizeof(uint32_t), st);
+    if (e != cudaSuccess) return e;
+    const uint32_t blocks = std::min<uint32_t>((n + 127) / 128, (uint32_t)sm_count() * 16u);
+    k_trace_dyn<true, true><<<blocks, 128, 0, st>>>(s.nodes, s.tris, nullptr, s.n_nodes, s.n_tris, ro, rd, n,
+                                                    nullptr, nullptr, nullptr, nullptr, occ, next, err, raw);
+    return cudaGetLastError();
+}
+
+// Three float4 vertices per triangle record, in record order: the input
+// vertices of the record's triangle, copied bit for bit.
+__global__ void k_raw_tris(const uint32_t *__restrict__ prim_of, const uint32_t *__restrict__ idx,
+                           const float *__restrict__ pos, uint32_t n, float4 *__restrict__ raw)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t p = prim_of[i];
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        const uint32_t v = idx[3ull * p + c];
+        raw[3ull * i + c] = make_float4(pos[3ull * v], pos[3ull * v + 1], pos[3ull * v + 2], 0.f);
+    }
+}
+
+cudaError_t build_raw_tris(const uint32_t *prim_of, const uint32_t *idx, const float *pos, uint32_t n, float4 *raw,
+                           cudaStream_t st)
+{
+    if (n == 0) return cudaSuccess;
+    k_raw_tris<<<(n + 255) / 256, 256, 0, st>>>(prim_of, idx, pos, n, raw);
     return cudaGetLastError();
 }
 

@@ -49,10 +49,13 @@ struct RayState {
     int sp;
     int best;
     float bu, bv;
+    Shear sh;  // watertight test only
 };
 
+template <bool kWT = false>
 __device__ __forceinline__ void ray_init(RayState &r, float4 o, float4 d, uint32_t n_nodes_total)
 {
+    if (kWT) r.sh = shear_of(d.x, d.y, d.z);
     const float kTiny = 1e-20f;
     r.ox = o.x; r.oy = o.y; r.oz = o.z; r.dx = d.x; r.dy = d.y; r.dz = d.z;
     r.ix = __frcp_rn(fabsf(d.x) > kTiny ? d.x : copysignf(kTiny, d.x));
@@ -75,11 +78,14 @@ __device__ __forceinline__ void ray_init(RayState &r, float4 o, float4 d, uint32
 
 // One traversal step. Returns true when the ray is finished (r.best is the
 // hit record, -1 for a miss, -2 for a reported error).
-template <bool kAnyHit, bool kStats = false, bool kSkip = false>
+// kWT selects the watertight triangle test over `raw` (three float4
+// vertices per triangle record) instead of the reference's Shirley test.
+template <bool kAnyHit, bool kStats = false, bool kSkip = false, bool kWT = false>
 __device__ __forceinline__ bool ray_step(RayState &r, uint2 *stack, const Node8 *__restrict__ nodes,
                                          const Tri *__restrict__ tris, uint32_t n_nodes_total, uint32_t n_tris_total,
                                          uint32_t *__restrict__ err, unsigned long long *n_nodes = nullptr,
-                                         unsigned long long *n_tris = nullptr, Skip skip = Skip{nullptr, 0u, 0u})
+                                         unsigned long long *n_tris = nullptr, Skip skip = Skip{nullptr, 0u, 0u},
+                                         const float4 *__restrict__ raw = nullptr)
 {
     if (r.ng_hits & 0xff000000u) {
         if (r.budget-- == 0u) {
@@ -152,14 +158,21 @@ __device__ __forceinline__ bool ray_step(RayState &r, uint2 *stack, const Node8 
             return true;
         }
         if (kSkip && __ldg(skip.prim_of + ti) - skip.lo < skip.n) continue;
-        const float4 *tp = reinterpret_cast<const float4 *>(tris + ti);
-        Tri tr;
-        tr.a = __ldg(tp);
-        tr.b = __ldg(tp + 1);
-        tr.c = __ldg(tp + 2);
         if (kStats) (*n_tris)++;
         float th, bh, gh;
-        if (shirley(tr, r.ox, r.oy, r.oz, r.dx, r.dy, r.dz, r.whi, th, bh, gh)) {
+        bool hit;
+        if (kWT) {
+            const float4 *vp = raw + 3ull * ti;
+            hit = watertight(__ldg(vp), __ldg(vp + 1), __ldg(vp + 2), r.ox, r.oy, r.oz, r.sh, r.whi, th, bh, gh);
+        } else {
+            const float4 *tp = reinterpret_cast<const float4 *>(tris + ti);
+            Tri tr;
+            tr.a = __ldg(tp);
+            tr.b = __ldg(tp + 1);
+            tr.c = __ldg(tp + 2);
+            hit = shirley(tr, r.ox, r.oy, r.oz, r.dx, r.dy, r.dz, r.whi, th, bh, gh);
+        }
+        if (hit) {
             r.best = (int)ti;
             if (kAnyHit) return true;
             r.bu = bh;

@@ -27,6 +27,16 @@ cudaError_t launch_closest_skip(const SceneView &s, const float4 *ro, const floa
 cudaError_t launch_any_skip(const SceneView &s, const float4 *ro, const float4 *rd, uint32_t n, uint32_t skip_lo,
                             uint32_t skip_n, uint8_t *occ, uint32_t *err, cudaStream_t st);
 
+// Watertight test (persistent kernels); raw = three float4 vertices per
+// triangle record, made by build_raw_tris from the input mesh.
+cudaError_t launch_closest_wt(const SceneView &s, const float4 *raw, const float4 *ro, const float4 *rd, uint32_t n,
+                              int32_t *prim, float *t, float *u, float *v, uint32_t *next, uint32_t *err,
+                              cudaStream_t st);
+cudaError_t launch_any_wt(const SceneView &s, const float4 *raw, const float4 *ro, const float4 *rd, uint32_t n,
+                          uint8_t *occ, uint32_t *next, uint32_t *err, cudaStream_t st);
+cudaError_t build_raw_tris(const uint32_t *prim_of, const uint32_t *idx, const float *pos, uint32_t n, float4 *raw,
+                           cudaStream_t st);
+
 // Persistent variants with dynamic ray fetch; `next` is a device counter word.
 cudaError_t launch_closest_dyn(const SceneView &s, const float4 *ro, const float4 *rd, uint32_t n, int32_t *prim,
                                float *t, float *u, float *v, uint32_t *next, uint32_t *err, cudaStream_t st);

@@ -19,6 +19,7 @@ from . import build as _build
 
 ILG_OK, ILG_EINVAL, ILG_ENOMEM, ILG_ECUDA, ILG_ETIMEOUT, ILG_EOVERFLOW, ILG_ESTATE = range(7)
 ILG_DEVICE_PTRS = 0x1
+ILG_WATERTIGHT = 0x2
 
 STATUS_NAMES = {0: "ILG_OK", 1: "ILG_EINVAL", 2: "ILG_ENOMEM", 3: "ILG_ECUDA", 4: "ILG_ETIMEOUT",
                 5: "ILG_EOVERFLOW", 6: "ILG_ESTATE"}
@@ -204,21 +205,23 @@ class GpuSpace:
         return self.L.ilg_stream(self.h) or 0
 
     # ISpace::Intersects(ray, isect), batched; host arrays
-    def intersects(self, o4: np.ndarray, d4: np.ndarray):
+    def intersects(self, o4: np.ndarray, d4: np.ndarray, watertight: bool = False):
         o4 = np.ascontiguousarray(o4, np.float32)
         d4 = np.ascontiguousarray(d4, np.float32)
         n = o4.shape[0]
         prim = np.empty(n, np.int32)
         t, u, v = (np.empty(n, np.float32) for _ in range(3))
         self._check(self.L.ilg_intersect(self.h, o4.ctypes.data, d4.ctypes.data, n, prim.ctypes.data,
-                                         t.ctypes.data, u.ctypes.data, v.ctypes.data, 0))
+                                         t.ctypes.data, u.ctypes.data, v.ctypes.data,
+                                         ILG_WATERTIGHT if watertight else 0))
         return prim, t, u, v
 
-    def intersects_into(self, o4, d4, prim, t, u, v, device_ptrs: bool):
+    def intersects_into(self, o4, d4, prim, t, u, v, device_ptrs: bool, watertight: bool = False):
         """Same query on caller-owned buffers (numpy, pinned or device torch tensors)."""
         n = o4.shape[0]
+        flags = (ILG_DEVICE_PTRS if device_ptrs else 0) | (ILG_WATERTIGHT if watertight else 0)
         self._check(self.L.ilg_intersect(self.h, _ptr(o4), _ptr(d4), n, _ptr(prim), _ptr(t), _ptr(u), _ptr(v),
-                                         ILG_DEVICE_PTRS if device_ptrs else 0))
+                                         flags))
 
     def traversal_counts(self, o4, d4):
         """(node records read, triangle records tested) for one closest-hit pass
@@ -233,11 +236,12 @@ class GpuSpace:
         return int(counts[0]), int(counts[1])
 
     # ISpace::Intersects(ray), batched
-    def occluded(self, o4: np.ndarray, d4: np.ndarray) -> np.ndarray:
+    def occluded(self, o4: np.ndarray, d4: np.ndarray, watertight: bool = False) -> np.ndarray:
         o4 = np.ascontiguousarray(o4, np.float32)
         d4 = np.ascontiguousarray(d4, np.float32)
         occ = np.empty(o4.shape[0], np.uint8)
-        self._check(self.L.ilg_occluded(self.h, o4.ctypes.data, d4.ctypes.data, o4.shape[0], occ.ctypes.data, 0))
+        self._check(self.L.ilg_occluded(self.h, o4.ctypes.data, d4.ctypes.data, o4.shape[0], occ.ctypes.data,
+                                        ILG_WATERTIGHT if watertight else 0))
         return occ
 
     # ISpace::Intersects(ray, isect, p_pExclude) / Intersects(ray, p_pExclude),

@@ -44,6 +44,13 @@ typedef enum ilg_status {
 
 /* ilg_intersect / ilg_occluded flags */
 #define ILG_DEVICE_PTRS 0x1u /* ray and hit arrays are device pointers */
+/* ilg_intersect / ilg_occluded: the watertight triangle test (Woop, Benthin
+ * and Wald 2013) instead of the reference's Shirley test. A ray through an
+ * edge or vertex shared by two triangles hits one of them, where the
+ * reference's test can let it through ("edge cracks"); elsewhere the hit is
+ * the reference's up to float rounding of t, beta and gamma. Same rejection
+ * window (t < 1e-5 or t > Max - 1e-5). */
+#define ILG_WATERTIGHT 0x2u
 
 typedef struct ilg_ctx ilg_ctx;
 

@@ -48,6 +48,8 @@ class Oracle:
         L.orc_shirley.restype = ctypes.c_int
         L.orc_intersect_brute.argtypes = [_f32p, _u32p, ctypes.c_uint32, _f32p, _f32p, ctypes.c_int64,
                                           _i32p, _f32p, _f32p, _f32p]
+        L.orc_watertight_brute.argtypes = [_f32p, _u32p, ctypes.c_uint32, _f32p, _f32p, ctypes.c_int64,
+                                           _i32p, _f32p, _f32p, _f32p, _u8p]
         L.orc_bvh_create.argtypes = [_f32p, ctypes.c_uint32, _u32p, ctypes.c_uint32]
         L.orc_bvh_create.restype = ctypes.c_void_p
         L.orc_bvh_destroy.argtypes = [ctypes.c_void_p]
@@ -97,6 +99,16 @@ class Oracle:
         n = o4.shape[0]
         out = (np.empty(n, np.int32), np.empty(n, np.float32), np.empty(n, np.float32), np.empty(n, np.float32))
         self.L.orc_intersect_brute(pos, idx.reshape(-1), idx.shape[0], o4, d4, n, *out)
+        return out
+
+    def watertight_brute(self, pos, idx, o4, d4):
+        """Closest hit and any hit with the watertight test: (prim, t, u, v, occ)."""
+        n = o4.shape[0]
+        out = (np.empty(n, np.int32), np.empty(n, np.float32), np.empty(n, np.float32), np.empty(n, np.float32),
+               np.empty(n, np.uint8))
+        self.L.orc_watertight_brute(np.ascontiguousarray(pos, np.float32), np.ascontiguousarray(idx, np.uint32).reshape(-1),
+                                    idx.shape[0], np.ascontiguousarray(o4, np.float32),
+                                    np.ascontiguousarray(d4, np.float32), n, *out)
         return out
 
     def bvh(self, pos, idx):

@@ -87,6 +87,88 @@ void orc_intersect_brute(const float *pos, const uint32_t *idx, uint32_t ntris, 
     free(tris);
 }
 
+/* ---------------- watertight test (Woop, Benthin, Wald 2013) ----------------
+ * Not in the reference: the restatement the device's ILG_WATERTIGHT mode
+ * follows, operation for operation (shear into the ray's frame with the
+ * largest direction component as z, 2D edge functions from the vertices,
+ * double-precision recomputation of edge functions that are exactly zero),
+ * with the reference's window t in [1e-5, Max - 1e-5]. */
+typedef struct {
+    int kx, ky, kz;
+    float sx, sy, sz;
+} oshear;
+
+static oshear shear_of(const float d[3])
+{
+    oshear s;
+    const float ax = fabsf(d[0]), ay = fabsf(d[1]), az = fabsf(d[2]);
+    s.kz = ax >= ay ? (ax >= az ? 0 : 2) : (ay >= az ? 1 : 2);
+    s.kx = s.kz == 2 ? 0 : s.kz + 1;
+    s.ky = s.kx == 2 ? 0 : s.kx + 1;
+    if (d[s.kz] < 0.f) {
+        const int k = s.kx;
+        s.kx = s.ky;
+        s.ky = k;
+    }
+    s.sx = d[s.kx] / d[s.kz];
+    s.sy = d[s.ky] / d[s.kz];
+    s.sz = 1.0f / d[s.kz];
+    return s;
+}
+
+static int watertight_tri(const float *p0, const float *p1, const float *p2, const float o[3], const oshear *sh,
+                          float rmax, float *t_out, float *b_out, float *g_out)
+{
+    float A[3], B[3], C[3];
+    SUB(A, p0, o);
+    SUB(B, p1, o);
+    SUB(C, p2, o);
+    const float Ax = A[sh->kx] - sh->sx * A[sh->kz], Ay = A[sh->ky] - sh->sy * A[sh->kz];
+    const float Bx = B[sh->kx] - sh->sx * B[sh->kz], By = B[sh->ky] - sh->sy * B[sh->kz];
+    const float Cx = C[sh->kx] - sh->sx * C[sh->kz], Cy = C[sh->ky] - sh->sy * C[sh->kz];
+    float U = Cx * By - Cy * Bx, V = Ax * Cy - Ay * Cx, W = Bx * Ay - By * Ax;
+    if (U == 0.f || V == 0.f || W == 0.f) {
+        U = (float)((double)Cx * (double)By - (double)Cy * (double)Bx);
+        V = (float)((double)Ax * (double)Cy - (double)Ay * (double)Cx);
+        W = (float)((double)Bx * (double)Ay - (double)By * (double)Ax);
+    }
+    if ((U < 0.f || V < 0.f || W < 0.f) && (U > 0.f || V > 0.f || W > 0.f)) return 0;
+    const float det = U + V + W;
+    if (det == 0.f) return 0;
+    const float Az = sh->sz * A[sh->kz], Bz = sh->sz * B[sh->kz], Cz = sh->sz * C[sh->kz];
+    const float T = U * Az + V * Bz + W * Cz;
+    const float rcp = 1.0f / det;
+    const float t = T * rcp;
+    if (!(t <= rmax - 1e-5) || t < 1e-5) return 0; /* double comparisons; NaN rejected */
+    *t_out = t;
+    *b_out = V * rcp;
+    *g_out = W * rcp;
+    return 1;
+}
+
+void orc_watertight_brute(const float *pos, const uint32_t *idx, uint32_t ntris, const float *o4, const float *d4,
+                          int64_t n, int32_t *prim, float *t, float *u, float *v, uint8_t *occ)
+{
+    for (int64_t r = 0; r < n; r++) {
+        const float *o = o4 + 4 * r, *d = d4 + 4 * r;
+        const oshear sh = shear_of(d);
+        float rmax = d[3], th, bh, gh;
+        int32_t best = -1;
+        float bt = INFINITY, bu = 0, bv = 0;
+        int any = 0;
+        for (uint32_t i = 0; i < ntris; i++) {
+            const float *p0 = pos + 3 * idx[3 * i], *p1 = pos + 3 * idx[3 * i + 1], *p2 = pos + 3 * idx[3 * i + 2];
+            if (!any && watertight_tri(p0, p1, p2, o, &sh, d[3], &th, &bh, &gh)) any = 1;
+            if (watertight_tri(p0, p1, p2, o, &sh, rmax, &th, &bh, &gh)) {
+                best = (int32_t)i; bt = th; bu = bh; bv = gh;
+                rmax = th < rmax ? th : rmax;
+            }
+        }
+        prim[r] = best; t[r] = bt; u[r] = bu; v[r] = bv;
+        if (occ) occ[r] = (uint8_t)any;
+    }
+}
+
 /* ---------------- binary BVH (ours: median split, <= 4 triangles a leaf) --- */
 typedef struct {
     float lo[3], hi[3];

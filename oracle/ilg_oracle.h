@@ -33,6 +33,12 @@ void orc_intersect_brute(const float *pos, const uint32_t *idx, uint32_t ntris,
                          const float *o4, const float *d4, int64_t n,
                          int32_t *prim, float *t, float *u, float *v);
 
+/* Closest hit (and any hit into occ, when not NULL) with the watertight test
+ * of Woop, Benthin and Wald 2013 - the restatement behind the device's
+ * ILG_WATERTIGHT mode, not a reference function. */
+void orc_watertight_brute(const float *pos, const uint32_t *idx, uint32_t ntris, const float *o4, const float *d4,
+                          int64_t n, int32_t *prim, float *t, float *u, float *v, uint8_t *occ);
+
 void *orc_bvh_create(const float *pos, uint32_t nverts, const uint32_t *idx, uint32_t ntris);
 void orc_bvh_destroy(void *h);
 /* stats (optional, 2 x uint64): total node visits, total triangle tests. */
