@@ -206,7 +206,7 @@ def cpu_baseline_sample(pos, idx, co, cd, io, idr, seconds=10.0):
                       f"{dt:.1f} s on {nthreads} threads"}
 
 
-def bench_path_tracer(dev, local, legs=("box", "field", "mlp", "batch")):
+def bench_path_tracer(dev, local, legs=("box", "field", "mlp", "batch", "cache")):
     """Samples/s of the wavefront path tracer on the box scene (256^2, 16 spp,
     depth 6) and on the icosphere field (1920x1080, 64 spp, depth 12;
     64 spheres x 327,680 triangles + ground + 4 lights = 20,971,530 triangles)."""
@@ -237,7 +237,32 @@ def bench_path_tracer(dev, local, legs=("box", "field", "mlp", "batch")):
         bench_mlp(res, dev, local, e0, e1)
     if "batch" in legs:
         bench_batch(res, local)
+    if "cache" in legs:
+        bench_cache(res, local)
     return res
+
+
+def bench_cache(res, local):
+    """Equal-time relMSE of the radiance-cached path tracer against plain path
+    tracing on the 20,971,530-triangle icosphere field at 480x270 (reduced
+    from 1080p so the ground truth fits the bench's time: 4096 spp instead of
+    16384), 64 frames of 1 spp, cache at the first bounce vertex, 8 Adam
+    steps of 32768 records per frame."""
+    from illuminaprt_b200 import scenes
+    from illuminaprt_b200.cache_experiment import equal_time
+    from illuminaprt_b200.ilg import GpuSpace
+    w, h = 480, 270
+    field = scenes.sphere_field(8, 7, seed=3, width=w, height=h)
+    sp = GpuSpace(device=local)
+    scenes.load_sphere_field(sp, field)
+    gt = sp.render(dict(field["camera"], aspect=w / h), w, h, 4096, max_depth=12, seed=424242, sky=field["sky"])
+    r = equal_time(sp, field, w, h, gt, frames=64, warmup=8, cache_depth=1, train_steps=8, train_batch=32768)
+    res["cache_equal_time"] = {
+        "scene": "icosphere field 480x270, ground truth 4096 spp", "relmse_plain": round(r["relmse_plain"], 6),
+        "relmse_cached": round(r["relmse_cached"], 6), "gain": round(r["gain"], 3),
+        "bias_cached": [round(b, 5) for b in r["bias_cached"]], "seconds": round(r["seconds_cached"], 4),
+        "frames_cached": r["frames_cached"], "frames_plain": r["frames_plain"]}
+    sp.close()
 
 
 def bench_field(res, dev, local, e0, e1):
@@ -326,7 +351,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-path-tracer", action="store_true")
-    ap.add_argument("--legs", default="box,field,mlp,batch",
+    ap.add_argument("--legs", default="box,field,mlp,batch,cache",
                     help="extra measurements after the ray query: box,field,mlp,batch")
     args = ap.parse_args()
     world, rank, local = dist_setup()

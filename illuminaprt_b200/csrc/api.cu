@@ -871,6 +871,8 @@ int ilg_mlp_init(ilg_ctx *ctx, uint32_t seed, float learning_rate)
     CK(ctx->mlp_w.reserve(kMlpParams)); CK(ctx->mlp_m.reserve(kMlpParams)); CK(ctx->mlp_v.reserve(kMlpParams));
     CK(ctx->mlp_grad.reserve(kMlpParams)); CK(ctx->mlp_loss.reserve(1));
     CK(ctx->mlp_wf.reserve(kFwdElems)); CK(ctx->mlp_wb.reserve(kBwdElems)); CK(ctx->mlp_wu.reserve(kUmmaElems));
+    CK(ctx->mlp_grid.reserve(kGridParams)); CK(ctx->mlp_grid_grad.reserve(kGridParams));
+    CK(ctx->mlp_grid_m.reserve(kGridParams)); CK(ctx->mlp_grid_v.reserve(kGridParams));
     CK(mlp_init(ctx->mlp_view(), seed, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     ctx->mlp_ready = true;
@@ -878,6 +880,23 @@ int ilg_mlp_init(ilg_ctx *ctx, uint32_t seed, float learning_rate)
     ctx->mlp_lr = learning_rate;
     return ILG_OK;
 }
+
+// which = 0: the grid features, 1: their gradient from the last ilg_mlp_grads.
+static int grid_copy(ilg_ctx *ctx, float *dst, const float *src, int which)
+{
+    if (!ctx || (!dst && !src)) return ILG_EINVAL;
+    if (!ctx->mlp_ready) return fail(ctx, ILG_ESTATE, "ilg_mlp grid: network not initialised");
+    CK(cudaSetDevice(ctx->device));
+    float *dev = which == 0 ? ctx->mlp_grid.ptr : ctx->mlp_grid_grad.ptr;
+    if (dst) CK(cudaMemcpyAsync(dst, dev, sizeof(float) * kGridParams, cudaMemcpyDeviceToHost, ctx->stream));
+    else CK(cudaMemcpyAsync(dev, src, sizeof(float) * kGridParams, cudaMemcpyHostToDevice, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return ILG_OK;
+}
+
+int ilg_mlp_get_grid(ilg_ctx *ctx, float *grid) { return grid_copy(ctx, grid, nullptr, 0); }
+int ilg_mlp_set_grid(ilg_ctx *ctx, const float *grid) { return grid_copy(ctx, nullptr, grid, 0); }
+int ilg_mlp_get_grid_grads(ilg_ctx *ctx, float *grad) { return grid_copy(ctx, grad, nullptr, 1); }
 
 int ilg_mlp_get_params(ilg_ctx *ctx, float *params)
 {

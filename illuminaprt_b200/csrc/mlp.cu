@@ -13,9 +13,13 @@
 //                    through the layers on the tensor cores, stores dZ
 //   k_mlp_dw         dW_l = H_{l-1}^T dZ_l as a split-K tensor-core GEMM over
 //                    the batch, FP32 partial sums added atomically
-// followed by k_mlp_adam (FP32 master weights, refreshes the BF16 copies).
+//   k_grid_bwd       dX of the grid columns = dZ0 W0^T, scattered to the
+//                    hash-grid corners of every level (FP32 atomics)
+// followed by k_mlp_adam (FP32 master weights, refreshes the BF16 copies)
+// and k_grid_adam (the grid features).
 #include "mlp.cuh"
 
+#include <cmath>
 #include <cstdio>
 
 namespace ilg {
@@ -100,7 +104,7 @@ __device__ __forceinline__ void load_smem(__nv_bfloat16 *dst, const __nv_bfloat1
 }
 
 // input A fragments (6 k16 blocks) of rows r0+g, r0+g+8 from raw features
-__device__ __forceinline__ void encode_rows(const float *raw, uint32_t n, uint32_t r0, int g, int tig,
+__device__ __forceinline__ void encode_rows(const MlpDev &M, const float *raw, uint32_t n, uint32_t r0, int g, int tig,
                                            uint32_t (&a)[6][4])
 {
     float f0[kMlpRaw], f1[kMlpRaw];
@@ -114,13 +118,13 @@ __device__ __forceinline__ void encode_rows(const float *raw, uint32_t n, uint32
     for (int kk = 0; kk < 6; kk++) {
         const int c = 16 * kk + 2 * tig;
         float2 p;
-        p = encode_pair(f0, c);
+        p = encode_pair(f0, c, M);
         a[kk][0] = ra < n ? pack_bf16(p.x, p.y) : 0u;
-        p = encode_pair(f1, c);
+        p = encode_pair(f1, c, M);
         a[kk][1] = rb < n ? pack_bf16(p.x, p.y) : 0u;
-        p = encode_pair(f0, c + 8);
+        p = encode_pair(f0, c + 8, M);
         a[kk][2] = ra < n ? pack_bf16(p.x, p.y) : 0u;
-        p = encode_pair(f1, c + 8);
+        p = encode_pair(f1, c + 8, M);
         a[kk][3] = rb < n ? pack_bf16(p.x, p.y) : 0u;
     }
 }
@@ -138,7 +142,7 @@ __global__ void __launch_bounds__(128) k_mlp_fwd(MlpDev M, const float *__restri
     for (uint32_t tile = blockIdx.x * 4 + warp; tile < n_tiles; tile += gridDim.x * 4) {
         const uint32_t r0 = tile * 16;
         uint32_t a0[6][4];
-        encode_rows(raw, n, r0, g, tig, a0);
+        encode_rows(M, raw, n, r0, g, tig, a0);
         if (kTrain) {
 #pragma unroll
             for (int kk = 0; kk < 6; kk++) store_cm(M.xcm, M.cap, 16 * kk, r0, g, tig, a0[kk]);
@@ -211,7 +215,7 @@ __global__ void __launch_bounds__(128) k_mlp_bwd(MlpDev M, const float *__restri
         uint32_t h[5][4][4];
         {
             uint32_t a0[6][4];
-            encode_rows(raw, n, r0, g, tig, a0);
+            encode_rows(M, raw, n, r0, g, tig, a0);
             float c[8][4];
             layer64<6>(a0, swf + fwd_off(0), fwd_stride(0), g, tig, c);
             relu_pack(c, h[0]);
@@ -400,6 +404,74 @@ __global__ void k_mlp_adam(MlpDev M, float lr, float bc1, float bc2)
     write_copies(M, i, w);
 }
 
+__global__ void k_grid_init(MlpDev M, uint32_t seed)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= kGridParams) return;
+    M.grid[i] = (2.f * hash_uniform(seed ^ 0xA5A5A5A5u, i) - 1.f) * 1e-4f;
+    M.grid_m[i] = 0.f;
+    M.grid_v[i] = 0.f;
+}
+
+// Gradient of the loss with respect to the grid features: per row, dX of the
+// 32 grid columns = dZ0 W0^T (W0 as the forward used it, in BF16), then
+// scattered to the eight corners of every level with the trilinear weights.
+constexpr int kGridBwdThreads = 128;
+
+__global__ void __launch_bounds__(kGridBwdThreads) k_grid_bwd(MlpDev M, const float *__restrict__ raw, uint32_t n)
+{
+    __shared__ float w0[2 * kGridLevels][kMlpHid];
+    for (int i = threadIdx.x; i < 2 * kGridLevels * kMlpHid; i += blockDim.x)
+        w0[i / kMlpHid][i % kMlpHid] = __bfloat162float(__float2bfloat16_rn(M.w[mlp_off(0) + i]));
+    __syncthreads();
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n) return;
+    float dz[kMlpHid];
+#pragma unroll
+    for (int j = 0; j < kMlpHid; j++) dz[j] = __bfloat162float(M.dzcm[(size_t)j * M.cap + r]);
+    const float x = raw[(size_t)r * kMlpRaw], y = raw[(size_t)r * kMlpRaw + 1], z = raw[(size_t)r * kMlpRaw + 2];
+    float2 *gg = reinterpret_cast<float2 *>(M.grid_grad);
+#pragma unroll 1
+    for (int l = 0; l < kGridLevels; l++) {
+        float d0 = 0.f, d1 = 0.f;
+#pragma unroll
+        for (int j = 0; j < kMlpHid; j++) {
+            d0 = fmaf(dz[j], w0[2 * l][j], d0);
+            d1 = fmaf(dz[j], w0[2 * l + 1][j], d1);
+        }
+        if (d0 == 0.f && d1 == 0.f) continue;
+        const uint32_t res = M.grid_res[l];
+        uint32_t ix, iy, iz;
+        float fx, fy, fz;
+        grid_cell(x, res, ix, fx);
+        grid_cell(y, res, iy, fy);
+        grid_cell(z, res, iz, fz);
+#pragma unroll
+        for (int c = 0; c < 8; c++) {
+            const float wx = (c & 1) ? fx : __fsub_rn(1.f, fx);
+            const float wy = (c & 2) ? fy : __fsub_rn(1.f, fy);
+            const float wz = (c & 4) ? fz : __fsub_rn(1.f, fz);
+            const float w = __fmul_rn(__fmul_rn(wx, wy), wz);
+            float2 *e = gg + (size_t)l * kGridSize + grid_index(res, ix + (c & 1), iy + ((c >> 1) & 1), iz + (c >> 2));
+            atomicAdd(&e->x, w * d0);
+            atomicAdd(&e->y, w * d1);
+        }
+    }
+}
+
+__global__ void k_grid_adam(MlpDev M, float lr, float bc1, float bc2)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= kGridParams) return;
+    const float b1 = 0.9f, b2 = 0.99f, eps = 1e-15f;
+    const float gr = M.grid_grad[i];
+    const float m = b1 * M.grid_m[i] + (1.f - b1) * gr;
+    const float v = b2 * M.grid_v[i] + (1.f - b2) * gr * gr;
+    M.grid_m[i] = m;
+    M.grid_v[i] = v;
+    M.grid[i] -= lr * (m / bc1) / (sqrtf(v / bc2) + eps);
+}
+
 inline uint32_t grid_for(uint32_t n_rows, int sms)
 {
     const uint32_t tiles = (n_rows + 15) / 16;
@@ -422,8 +494,14 @@ int num_sms()
 
 }  // namespace
 
+void grid_resolution(uint32_t (&res)[kGridLevels])
+{
+    for (int l = 0; l < kGridLevels; l++) res[l] = (uint32_t)std::floor(16.0 * std::pow(2.0, 7.0 * l / 15.0));
+}
+
 cudaError_t mlp_init(const MlpDev &M, uint32_t seed, cudaStream_t st)
 {
+    k_grid_init<<<(kGridParams + 255) / 256, 256, 0, st>>>(M, seed);
     cudaError_t e;
     if ((e = cudaMemsetAsync(M.wf, 0, kFwdElems * sizeof(__nv_bfloat16), st)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(M.wb, 0, kBwdElems * sizeof(__nv_bfloat16), st)) != cudaSuccess) return e;
@@ -468,6 +546,7 @@ cudaError_t mlp_grads(const MlpDev &M, const float *raw, const float *target, ui
     // write exact zeros for them, but clear once so stale rows never leak
     if ((e = cudaMemsetAsync(M.grad, 0, kMlpParams * sizeof(float), st)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(M.loss, 0, sizeof(float), st)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(M.grid_grad, 0, kGridParams * sizeof(float), st)) != cudaSuccess) return e;
     const size_t smem_f = kFwdElems * sizeof(__nv_bfloat16);
     const size_t smem_b = (kFwdElems + kBwdElems) * sizeof(__nv_bfloat16);
     static bool attr = false;
@@ -480,6 +559,7 @@ cudaError_t mlp_grads(const MlpDev &M, const float *raw, const float *target, ui
     const uint32_t grid = grid_for(n, num_sms());
     k_mlp_fwd<true><<<grid, 128, smem_f, st>>>(M, raw, n, nullptr, nullptr);
     k_mlp_bwd<<<grid, 128, smem_b, st>>>(M, raw, target, n);
+    k_grid_bwd<<<(n + kGridBwdThreads - 1) / kGridBwdThreads, kGridBwdThreads, 0, st>>>(M, raw, n);
     const uint32_t chunks = (n_pad + kDwChunk - 1) / kDwChunk;
     for (int l = 0; l < kMlpLayers; l++) {
         const __nv_bfloat16 *A = l == 0 ? M.xcm : M.hcm + (size_t)(l - 1) * kMlpHid * M.cap;
@@ -498,6 +578,7 @@ cudaError_t mlp_adam(const MlpDev &M, uint32_t step, float lr, cudaStream_t st)
 {
     const float bc1 = 1.f - powf(0.9f, (float)step), bc2 = 1.f - powf(0.99f, (float)step);
     k_mlp_adam<<<(kMlpParams + 255) / 256, 256, 0, st>>>(M, lr, bc1, bc2);
+    k_grid_adam<<<(kGridParams + 255) / 256, 256, 0, st>>>(M, lr, bc1, bc2);
     return cudaGetLastError();
 }
 

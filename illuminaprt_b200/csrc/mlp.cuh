@@ -1,7 +1,9 @@
-// Online-trained radiance cache: a 96 -> 64 x 5 (ReLU) -> 3 MLP in BF16 with
-// FP32 accumulation on the tensor cores (mlp.cu). The reference has no
-// learned component; the closest analogue is its irradiance cache
-// (Core/Integrator/ICIntegrator.*), which this does not reproduce.
+// Online-trained radiance cache: a multiresolution hash-grid encoding of
+// position (Mueller et al. 2022, "Instant neural graphics primitives")
+// feeding a 96 -> 64 x 5 (ReLU) -> 3 MLP in BF16 with FP32 accumulation on
+// the tensor cores (mlp.cu). The reference has no learned component; the
+// closest analogue is its irradiance cache (Core/Integrator/ICIntegrator.*),
+// which this does not reproduce.
 #pragma once
 
 #include <cstdint>
@@ -17,7 +19,19 @@ constexpr int kMlpIn = 96;     // encoded input width (82 used + constant 1 + ze
 constexpr int kMlpHid = 64;
 constexpr int kMlpOutP = 8;    // output columns computed (3 used)
 constexpr int kMlpLayers = 6;
-constexpr int kMlpBands = 12;
+constexpr int kMlpBands = 4;       // frequency bands of position next to the grid
+
+// Hash grid: kGridLevels levels of kGridFeat trainable features, each level a
+// table of kGridSize entries. Level l has resolution N_l = floor(16 *
+// 2^(7 l / 15)) cells per unit (16 .. 2048; grid_resolution() on the host
+// fills MlpDev::grid_res). Levels whose (N_l + 1)^3 corners fit the table are
+// indexed densely, the others through the spatial hash
+// (x * 1) ^ (y * 2654435761) ^ (z * 805459861) mod kGridSize.
+constexpr int kGridLevels = 16;
+constexpr int kGridFeat = 2;
+constexpr int kGridLog2Size = 15;
+constexpr uint32_t kGridSize = 1u << kGridLog2Size;
+constexpr uint32_t kGridParams = (uint32_t)kGridLevels * kGridSize * kGridFeat;  // 1,048,576
 
 __host__ __device__ constexpr int mlp_in(int l) { return l == 0 ? kMlpIn : kMlpHid; }
 __host__ __device__ constexpr int mlp_out(int l) { return l == kMlpLayers - 1 ? kMlpOutP : kMlpHid; }
@@ -65,27 +79,80 @@ struct MlpDev {
     __nv_bfloat16 *dzcm;      // (5 x kMlpHid + kMlpOutP) x cap
     uint32_t cap;             // rows the scratch holds (multiple of 16)
     uint32_t *err;            // device error word (bounded waits)
+    // hash grid: FP32 features [level][entry][feature], their gradient and Adam moments
+    float *grid, *grid_grad, *grid_m, *grid_v;
+    uint32_t grid_res[kGridLevels];
 };
 
-// Encoded input columns (c, c+1), c even. Columns 0..71: for axis a and band
-// b, column 24a + 2b is sin(2^b pi x_a) and the next cos(2^b pi x_a);
-// 72..74 direction, 75..77 normal, 78 roughness, 79..81 albedo, 82 constant 1.
-__device__ __forceinline__ float2 encode_pair(const float *f, int c)
+// N_l of every level (host).
+void grid_resolution(uint32_t (&res)[kGridLevels]);
+
+// Table entry of corner (x, y, z) of level l.
+__host__ __device__ __forceinline__ uint32_t grid_index(uint32_t res, uint32_t x, uint32_t y, uint32_t z)
 {
-    if (c < 72) {
-        const int axis = c / 24, band = (c % 24) >> 1;
+    const uint32_t side = res + 1u;
+    if ((uint64_t)side * side * side <= kGridSize) return x + side * (y + side * z);
+    return (x ^ (y * 2654435761u) ^ (z * 805459861u)) & (kGridSize - 1u);
+}
+
+// Cell and trilinear fractions of position coordinate x in [0, 1] at resolution res.
+__device__ __forceinline__ void grid_cell(float x, uint32_t res, uint32_t &i, float &f)
+{
+    x = fminf(fmaxf(x, 0.f), 1.f);
+    const float p = __fmul_rn(x, (float)res);
+    const uint32_t c = (uint32_t)floorf(p);
+    i = c < res ? c : res - 1u;
+    f = __fsub_rn(p, (float)i);
+}
+
+// The two features of level l at normalised position (x, y, z): the eight
+// corners weighted trilinearly, summed in corner order (bit 0 = x, 1 = y,
+// 2 = z), every product and sum rounded separately.
+__device__ __forceinline__ float2 grid_features(const MlpDev &M, int l, float x, float y, float z)
+{
+    const uint32_t res = M.grid_res[l];
+    uint32_t ix, iy, iz;
+    float fx, fy, fz;
+    grid_cell(x, res, ix, fx);
+    grid_cell(y, res, iy, fy);
+    grid_cell(z, res, iz, fz);
+    const float2 *table = reinterpret_cast<const float2 *>(M.grid) + (size_t)l * kGridSize;
+    float a0 = 0.f, a1 = 0.f;
+#pragma unroll
+    for (int c = 0; c < 8; c++) {
+        const float wx = (c & 1) ? fx : __fsub_rn(1.f, fx);
+        const float wy = (c & 2) ? fy : __fsub_rn(1.f, fy);
+        const float wz = (c & 4) ? fz : __fsub_rn(1.f, fz);
+        const float w = __fmul_rn(__fmul_rn(wx, wy), wz);
+        const float2 t = __ldg(table + grid_index(res, ix + (c & 1), iy + ((c >> 1) & 1), iz + (c >> 2)));
+        a0 = __fadd_rn(a0, __fmul_rn(w, t.x));
+        a1 = __fadd_rn(a1, __fmul_rn(w, t.y));
+    }
+    return make_float2(a0, a1);
+}
+
+// Encoded input columns (c, c+1), c even. Columns 0..31: the two hash-grid
+// features of level c / 2. Columns 32..55: for axis a and band b < 4, column
+// 32 + 8a + 2b is sin(2^b pi x_a) and the next cos(2^b pi x_a). Then 56..58
+// direction, 59..61 normal, 62 roughness, 63..65 albedo, 66 constant 1,
+// 67..95 zero.
+__device__ __forceinline__ float2 encode_pair(const float *f, int c, const MlpDev &M)
+{
+    if (c < 2 * kGridLevels) return grid_features(M, c >> 1, f[0], f[1], f[2]);
+    if (c < 56) {
+        const int k = c - 32, axis = k >> 3, band = (k & 7) >> 1;
         const float x = axis == 0 ? f[0] : (axis == 1 ? f[1] : f[2]);
         float s, co;
         sincospif(ldexpf(x, band), &s, &co);
         return make_float2(s, co);
     }
     switch (c) {
-    case 72: return make_float2(f[3], f[4]);
-    case 74: return make_float2(f[5], f[6]);
-    case 76: return make_float2(f[7], f[8]);
-    case 78: return make_float2(f[9], f[10]);
-    case 80: return make_float2(f[11], f[12]);
-    case 82: return make_float2(1.f, 0.f);
+    case 56: return make_float2(f[3], f[4]);
+    case 58: return make_float2(f[5], f[6]);
+    case 60: return make_float2(f[7], f[8]);
+    case 62: return make_float2(f[9], f[10]);
+    case 64: return make_float2(f[11], f[12]);
+    case 66: return make_float2(1.f, 0.f);
     default: return make_float2(0.f, 0.f);
     }
 }

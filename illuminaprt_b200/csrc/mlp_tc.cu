@@ -120,8 +120,7 @@ __device__ __forceinline__ void put_chunk(unsigned char *a_tile, int r, int c, i
     *reinterpret_cast<uint4 *>(a_tile + (size_t)(r / 8) * kc * 128 + (size_t)c * 128 + (r % 8) * 16) = q;
 }
 
-__global__ void __launch_bounds__(kTcRows) k_mlp_infer_tc(const __nv_bfloat16 *__restrict__ wu,
-                                                          const float *__restrict__ raw, uint32_t n,
+__global__ void __launch_bounds__(kTcRows) k_mlp_infer_tc(const MlpDev M, const float *__restrict__ raw, uint32_t n,
                                                           const uint32_t *__restrict__ n_dev,
                                                           float *__restrict__ out, uint32_t *__restrict__ err)
 {
@@ -135,7 +134,7 @@ __global__ void __launch_bounds__(kTcRows) k_mlp_infer_tc(const __nv_bfloat16 *_
     const int tid = threadIdx.x, warp = tid >> 5;
     // weights -> shared memory (16-byte vectors)
     {
-        const uint4 *src = reinterpret_cast<const uint4 *>(wu);
+        const uint4 *src = reinterpret_cast<const uint4 *>(M.wu);
         uint4 *dst = reinterpret_cast<uint4 *>(w_s);
         for (int i = tid; i < kUmmaElems / 8; i += kTcRows) dst[i] = src[i];
     }
@@ -172,7 +171,7 @@ __global__ void __launch_bounds__(kTcRows) k_mlp_infer_tc(const __nv_bfloat16 *_
                 float v[8];
 #pragma unroll
                 for (int e = 0; e < 8; e += 2) {
-                    const float2 p = encode_pair(f, 8 * c + e);
+                    const float2 p = encode_pair(f, 8 * c + e, M);
                     v[e] = row < n ? p.x : 0.f;
                     v[e + 1] = row < n ? p.y : 0.f;
                 }
@@ -252,7 +251,7 @@ cudaError_t mlp_infer_tc(const MlpDev &M, const float *raw, uint32_t n, float *o
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const uint32_t tiles = (n + kTcRows - 1) / kTcRows;
     const uint32_t grid = tiles < (uint32_t)sms * 3u ? tiles : (uint32_t)sms * 3u;
-    k_mlp_infer_tc<<<grid, kTcRows, smem, st>>>(M.wu, raw, n, n_dev, out, err);
+    k_mlp_infer_tc<<<grid, kTcRows, smem, st>>>(M, raw, n, n_dev, out, err);
     return cudaGetLastError();
 }
 

@@ -30,11 +30,13 @@ EXPORTED = ["ilg_create", "ilg_destroy", "ilg_last_error", "ilg_set_mesh", "ilg_
             "ilg_set_materials", "ilg_set_quad_lights", "ilg_render", "ilg_intersect_noalloc",
             "ilg_mlp_init", "ilg_mlp_get_params", "ilg_mlp_set_params", "ilg_mlp_infer", "ilg_mlp_grads",
             "ilg_mlp_train_step", "ilg_render_batch", "ilg_intersect_excluding", "ilg_occluded_excluding",
-            "ilg_camera_frame_of", "ilg_render_region"]
+            "ilg_camera_frame_of", "ilg_render_region", "ilg_mlp_get_grid", "ilg_mlp_set_grid",
+            "ilg_mlp_get_grid_grads"]
 
 ILG_MLP_RAW = 16
 ILG_MLP_WARP_MMA = 0x10
 ILG_MLP_PARAMS = 23040
+ILG_MLP_GRID_PARAMS = 1048576
 
 # Largest batch ilg_intersect_noalloc accepts (include/ilg.h).
 ILG_NOALLOC_MAX_RAYS = 262144
@@ -140,6 +142,9 @@ def load(build_if_missing: bool = True) -> ctypes.CDLL:
     L.ilg_mlp_init.argtypes = [vp, u32, ctypes.c_float]
     L.ilg_mlp_get_params.argtypes = [vp, vp]
     L.ilg_mlp_set_params.argtypes = [vp, vp]
+    L.ilg_mlp_get_grid.argtypes = [vp, vp]
+    L.ilg_mlp_set_grid.argtypes = [vp, vp]
+    L.ilg_mlp_get_grid_grads.argtypes = [vp, vp]
     L.ilg_mlp_infer.argtypes = [vp, vp, u32, vp, u32]
     L.ilg_mlp_grads.argtypes = [vp, vp, vp, u32, vp, vp, u32]
     L.ilg_mlp_train_step.argtypes = [vp, vp, vp, u32, vp, u32]
@@ -351,6 +356,22 @@ class GpuSpace:
         p = np.ascontiguousarray(p, np.float32)
         assert p.size == ILG_MLP_PARAMS
         self._check(self.L.ilg_mlp_set_params(self.h, p.ctypes.data))
+
+    def mlp_grid(self) -> np.ndarray:
+        g = np.empty(ILG_MLP_GRID_PARAMS, np.float32)
+        self._check(self.L.ilg_mlp_get_grid(self.h, g.ctypes.data))
+        return g
+
+    def mlp_set_grid(self, g):
+        g = np.ascontiguousarray(g, np.float32)
+        assert g.size == ILG_MLP_GRID_PARAMS
+        self._check(self.L.ilg_mlp_set_grid(self.h, g.ctypes.data))
+
+    def mlp_grid_grads(self) -> np.ndarray:
+        """The grid part of the gradient of the last mlp_grads call."""
+        g = np.empty(ILG_MLP_GRID_PARAMS, np.float32)
+        self._check(self.L.ilg_mlp_get_grid_grads(self.h, g.ctypes.data))
+        return g
 
     def mlp_infer(self, raw, warp_mma: bool = False) -> np.ndarray:
         """Cache network outputs (tcgen05 tensor cores; warp_mma selects the mma.sync kernel)."""

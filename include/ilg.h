@@ -236,14 +236,22 @@ int ilg_render_region(ilg_ctx *ctx, const ilg_camera_frame *frame, const ilg_ren
  * accumulation on the tensor cores, trained with Adam on a relative L2 loss.
  * Queries are ILG_MLP_RAW floats per row: position normalised to [0,1]^3,
  * outgoing direction, normal, roughness, albedo, 3 unused. The position is
- * encoded with 12 sine/cosine frequency bands per axis on the device.
+ * encoded on the device by a trainable multiresolution hash grid (16 levels
+ * of 2 features, 2^15 entries a level, resolutions floor(16 * 2^(7 l / 15))
+ * per unit; Mueller et al. 2022) and by 4 sine/cosine frequency bands per
+ * axis.
  * ---------------------------------------------------------------------- */
 #define ILG_MLP_RAW 16u
 #define ILG_MLP_PARAMS 23040u /* FP32 weights, per layer row-major [in][out] */
+#define ILG_MLP_GRID_PARAMS 1048576u /* FP32 grid features [level][entry][feature] */
 
 int ilg_mlp_init(ilg_ctx *ctx, uint32_t seed, float learning_rate);
 int ilg_mlp_get_params(ilg_ctx *ctx, float *params /* ILG_MLP_PARAMS */);
 int ilg_mlp_set_params(ilg_ctx *ctx, const float *params);
+int ilg_mlp_get_grid(ilg_ctx *ctx, float *grid /* ILG_MLP_GRID_PARAMS */);
+int ilg_mlp_set_grid(ilg_ctx *ctx, const float *grid);
+/* The grid part of the gradient the last ilg_mlp_grads computed. */
+int ilg_mlp_get_grid_grads(ilg_ctx *ctx, float *grad /* ILG_MLP_GRID_PARAMS */);
 /* out: n x 3 radiance. Host pointers unless ILG_DEVICE_PTRS. Runs on the
  * tcgen05 tensor cores (accumulators in TMEM); ILG_MLP_WARP_MMA selects the
  * warp-level mma.sync kernel that training's forward pass uses instead. */

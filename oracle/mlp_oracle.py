@@ -3,10 +3,17 @@
 Restates, in float64 numpy, what the device network computes (the reference
 has no learned component, so this is this project's own oracle):
 
-* encoding: 16 raw floats per query -> 96 columns. For axis a in 0..2 and
-  band b in 0..11, column 24a + 2b = sin(2^b pi x_a), 24a + 2b + 1 =
-  cos(2^b pi x_a); 72..74 direction, 75..77 normal, 78 roughness, 79..81
-  albedo, 82 constant 1, 83..95 zero.
+* encoding: 16 raw floats per query -> 96 columns. Columns 0..31: a
+  multiresolution hash grid over the normalised position (Mueller et al.
+  2022): level l < 16 has resolution N_l = floor(16 * 2^(7 l / 15)) and a
+  table of 2^15 entries of 2 features, indexed densely when (N_l + 1)^3
+  corners fit and otherwise by (x ^ 2654435761 y ^ 805459861 z) mod 2^15;
+  column 2l + f is feature f of level l, trilinearly interpolated from the
+  cell's eight corners in float32 exactly as the device does it (corner
+  order x, y, z bits; every product and sum rounded). Columns 32..55: for
+  axis a and band b in 0..3, column 32 + 8a + 2b = sin(2^b pi x_a), the next
+  cos; 56..58 direction, 59..61 normal, 62 roughness, 63..65 albedo, 66
+  constant 1, 67..95 zero.
 * network: 96 -> 64 -> 64 -> 64 -> 64 -> 64 -> 8 (3 used), ReLU after every
   hidden layer, no biases, weights per layer row-major [in][out] in one flat
   vector of 23,040 floats.
@@ -23,6 +30,9 @@ from __future__ import annotations
 import numpy as np
 
 IN, HID, OUTP, LAYERS, RAW = 96, 64, 8, 6, 16
+GRID_LEVELS, GRID_FEAT, GRID_SIZE = 16, 2, 1 << 15
+GRID_PARAMS = GRID_LEVELS * GRID_SIZE * GRID_FEAT
+GRID_RES = [int(np.floor(16.0 * 2.0 ** (7.0 * l / 15.0))) for l in range(GRID_LEVELS)]
 DIMS = [(IN, HID)] + [(HID, HID)] * 4 + [(HID, OUTP)]
 OFFS = np.cumsum([0] + [i * o for i, o in DIMS]).tolist()
 N_PARAMS = OFFS[-1]
@@ -37,20 +47,64 @@ def bf16(x):
     return np.where(np.isfinite(f), out, f.astype(np.float64))
 
 
-def encode(raw):
-    raw = np.asarray(raw, np.float64)
+def grid_corners(pos, l):
+    """Entry indices (n, 8) and float32 trilinear weights (n, 8) of level l."""
+    res = GRID_RES[l]
+    p = np.clip(np.asarray(pos, np.float32), np.float32(0), np.float32(1)) * np.float32(res)
+    i = np.minimum(np.floor(p).astype(np.int64), res - 1)
+    f = (p - i.astype(np.float32)).astype(np.float32)
+    one = np.float32(1)
+    side = res + 1
+    idx = np.zeros((p.shape[0], 8), np.int64)
+    w = np.zeros((p.shape[0], 8), np.float32)
+    for c in range(8):
+        b = [(c >> k) & 1 for k in range(3)]
+        cx, cy, cz = (i[:, k] + b[k] for k in range(3))
+        if side ** 3 <= GRID_SIZE:
+            idx[:, c] = cx + side * (cy + side * cz)
+        else:
+            h = (cx.astype(np.uint32) ^ (cy.astype(np.uint32) * np.uint32(2654435761))
+                 ^ (cz.astype(np.uint32) * np.uint32(805459861))) & np.uint32(GRID_SIZE - 1)
+            idx[:, c] = h.astype(np.int64)
+        wx, wy, wz = (f[:, k] if b[k] else (one - f[:, k]) for k in range(3))
+        w[:, c] = (wx * wy) * wz
+    return idx, w
+
+
+def grid_features(grid, pos):
+    """(n, 32) float32 grid columns."""
+    g = np.asarray(grid, np.float32).reshape(GRID_LEVELS, GRID_SIZE, GRID_FEAT)
+    out = np.zeros((pos.shape[0], 2 * GRID_LEVELS), np.float32)
+    for l in range(GRID_LEVELS):
+        idx, w = grid_corners(pos, l)
+        a = np.zeros((pos.shape[0], GRID_FEAT), np.float32)
+        for c in range(8):
+            a = a + w[:, c:c + 1] * g[l, idx[:, c]]
+        out[:, 2 * l:2 * l + 2] = a
+    return out
+
+
+def init_grid(seed=0):
+    rng = np.random.default_rng(seed + 7)
+    return rng.uniform(-1e-4, 1e-4, GRID_PARAMS).astype(np.float32)
+
+
+def encode(raw, grid):
+    raw = np.asarray(raw, np.float32)
     n = raw.shape[0]
     x = np.zeros((n, IN))
+    x[:, 0:32] = grid_features(grid, raw[:, 0:3])
+    r = raw.astype(np.float64)
     for a in range(3):
-        for b in range(12):
-            arg = np.pi * raw[:, a] * (2.0 ** b)
-            x[:, 24 * a + 2 * b] = np.sin(arg)
-            x[:, 24 * a + 2 * b + 1] = np.cos(arg)
-    x[:, 72:75] = raw[:, 3:6]
-    x[:, 75:78] = raw[:, 6:9]
-    x[:, 78] = raw[:, 9]
-    x[:, 79:82] = raw[:, 10:13]
-    x[:, 82] = 1.0
+        for b in range(4):
+            arg = np.pi * r[:, a] * (2.0 ** b)
+            x[:, 32 + 8 * a + 2 * b] = np.sin(arg)
+            x[:, 32 + 8 * a + 2 * b + 1] = np.cos(arg)
+    x[:, 56:59] = r[:, 3:6]
+    x[:, 59:62] = r[:, 6:9]
+    x[:, 62] = r[:, 9]
+    x[:, 63:66] = r[:, 10:13]
+    x[:, 66] = 1.0
     return x
 
 
@@ -59,10 +113,10 @@ def unflatten(params):
     return [p[OFFS[l]:OFFS[l + 1]].reshape(DIMS[l]) for l in range(LAYERS)]
 
 
-def forward(params, raw, bf=True):
+def forward(params, raw, grid, bf=True):
     r = bf16 if bf else (lambda v: v)
     W = [r(w) for w in unflatten(params)]
-    h = r(encode(raw))
+    h = r(encode(raw, grid))
     acts = [h]
     for l in range(LAYERS - 1):
         h = r(np.maximum(h @ W[l], 0.0))
@@ -71,9 +125,10 @@ def forward(params, raw, bf=True):
     return y[:, :3], acts, W
 
 
-def loss_and_grads(params, raw, target, bf=True):
+def loss_and_grads(params, raw, target, grid, bf=True):
+    """(loss, weight gradient, grid gradient)."""
     r = bf16 if bf else (lambda v: v)
-    y, acts, W = forward(params, raw, bf)
+    y, acts, W = forward(params, raw, grid, bf)
     t = np.asarray(target, np.float64)
     n = y.shape[0]
     den = y * y + 0.01
@@ -89,7 +144,16 @@ def loss_and_grads(params, raw, target, bf=True):
             dz = r(np.where(acts[l] > 0, dh, 0.0))
     g = np.concatenate([gl.reshape(-1) for gl in grads])
     g[OFFS[5]:].reshape(HID, OUTP)[:, 3:] = 0.0
-    return loss, g
+    # through the encoding: dX of the grid columns, scattered to the corners
+    dx = dz @ W[0].T
+    gg = np.zeros((GRID_LEVELS, GRID_SIZE, GRID_FEAT))
+    pos = np.asarray(raw, np.float32)[:, 0:3]
+    for l in range(GRID_LEVELS):
+        idx, w = grid_corners(pos, l)
+        for c in range(8):
+            for f in range(GRID_FEAT):
+                np.add.at(gg[l, :, f], idx[:, c], w[:, c].astype(np.float64) * dx[:, 2 * l + f])
+    return loss, g, gg.reshape(-1)
 
 
 def init_params(seed=0):

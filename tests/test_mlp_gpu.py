@@ -7,11 +7,15 @@ from oracle import mlp_oracle as mo
 pytestmark = pytest.mark.gpu
 
 
+GRID = np.random.default_rng(17).uniform(-0.3, 0.3, mo.GRID_PARAMS).astype(np.float32)
+
+
 @pytest.fixture(scope="module")
 def net():
     from illuminaprt_b200.ilg import GpuSpace
     sp = GpuSpace()
     sp.mlp_init(seed=7, lr=1e-2)
+    sp.mlp_set_grid(GRID)  # features large enough that the encoding matters
     return sp
 
 
@@ -19,7 +23,7 @@ def test_forward_matches_oracle(net):
     raw, _ = mo.random_batch(5000, seed=1)  # not a multiple of 16: ragged last tile
     p = net.mlp_params()
     y_gpu = net.mlp_infer(raw)
-    y_ref, _, _ = mo.forward(p, raw, bf=True)
+    y_ref, _, _ = mo.forward(p, raw, net.mlp_grid(), bf=True)
     scale = np.abs(y_ref).max()
     err = np.abs(y_gpu - y_ref).max() / scale
     print(f"forward: max |gpu - oracle| / max|y| = {err:.2e}")
@@ -31,9 +35,11 @@ def test_forward_matches_oracle(net):
 def test_gradients_match_oracle(net, n):
     raw, tgt = mo.random_batch(n, seed=n)
     p = net.mlp_params()
+    grid = net.mlp_grid()
     loss_g, g_gpu = net.mlp_grads(raw, tgt)
-    loss_r, g_ref = mo.loss_and_grads(p, raw, tgt, bf=True)
-    loss_x, g_exact = mo.loss_and_grads(p, raw, tgt, bf=False)
+    gg_gpu = net.mlp_grid_grads()
+    loss_r, g_ref, gg_ref = mo.loss_and_grads(p, raw, tgt, grid, bf=True)
+    loss_x, g_exact, _ = mo.loss_and_grads(p, raw, tgt, grid, bf=False)
     rel = np.linalg.norm(g_gpu - g_ref) / np.linalg.norm(g_ref)
     cos_exact = g_gpu @ g_exact / (np.linalg.norm(g_gpu) * np.linalg.norm(g_exact))
     print(f"n={n}: loss gpu {loss_g:.6f} oracle {loss_r:.6f}; grad rel err vs bf16 oracle {rel:.2e}; "
@@ -41,6 +47,11 @@ def test_gradients_match_oracle(net, n):
     assert abs(loss_g - loss_r) <= 1e-3 * abs(loss_r) + 1e-6
     assert rel < 3e-2
     assert cos_exact > 0.995
+    # the hash-grid part: every touched entry, against the bf16 oracle
+    rel_g = np.linalg.norm(gg_gpu - gg_ref) / np.linalg.norm(gg_ref)
+    print(f"n={n}: grid grad rel err {rel_g:.2e}, {np.count_nonzero(gg_ref)} entries touched")
+    assert rel_g < 3e-2
+    assert np.array_equal(gg_gpu != 0, gg_ref != 0) or n >= 1000
     # per layer, too
     for l in range(mo.LAYERS):
         a, b = g_gpu[mo.OFFS[l]:mo.OFFS[l + 1]], g_ref[mo.OFFS[l]:mo.OFFS[l + 1]]
@@ -51,8 +62,10 @@ def test_set_get_params_round_trip(net):
     p = mo.init_params(seed=3)
     net.mlp_set_params(p)
     assert np.array_equal(net.mlp_params(), p)
+    net.mlp_set_grid(GRID)
+    assert np.array_equal(net.mlp_grid(), GRID)
     raw, _ = mo.random_batch(333, seed=9)
-    y_ref, _, _ = mo.forward(p, raw, bf=True)
+    y_ref, _, _ = mo.forward(p, raw, GRID, bf=True)
     assert np.abs(net.mlp_infer(raw) - y_ref).max() < 1e-2 * np.abs(y_ref).max()
 
 
@@ -79,7 +92,7 @@ def test_tcgen05_inference_matches_warp_mma(net, n):
         net.mlp_train_step(raw[:4096], tgt[:4096])
     y_tc = net.mlp_infer(raw)
     y_warp = net.mlp_infer(raw, warp_mma=True)
-    y_ref, _, _ = mo.forward(net.mlp_params(), raw, bf=True)
+    y_ref, _, _ = mo.forward(net.mlp_params(), raw, net.mlp_grid(), bf=True)
     scale = np.abs(y_ref).max() + 1e-6
     d_warp = np.abs(y_tc - y_warp).max() / scale
     d_ref = np.abs(y_tc - y_ref).max() / scale
