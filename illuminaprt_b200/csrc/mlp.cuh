@@ -131,11 +131,30 @@ __device__ __forceinline__ float2 grid_features(const MlpDev &M, int l, float x,
     return make_float2(a0, a1);
 }
 
+// Real spherical harmonics of degree < 4 of the unit vector (x, y, z), two at
+// a time (pair k = coefficients 2k, 2k + 1; order l = 0..3, m = -l..l), with
+// the usual orthonormal constants sqrt((2l + 1) / 4pi * (l - |m|)! / (l + |m|)!)
+// folded in.
+__device__ __forceinline__ float2 sh_pair(float x, float y, float z, int k)
+{
+    const float xx = x * x, yy = y * y, zz = z * z;
+    switch (k) {
+    case 0: return make_float2(0.28209479177387814f, -0.48860251190291987f * y);
+    case 1: return make_float2(0.48860251190291987f * z, -0.48860251190291987f * x);
+    case 2: return make_float2(1.0925484305920792f * x * y, -1.0925484305920792f * y * z);
+    case 3: return make_float2(0.94617469575755997f * zz - 0.31539156525251999f, -1.0925484305920792f * x * z);
+    case 4: return make_float2(0.54627421529603959f * (xx - yy), 0.59004358992664352f * y * (3.f * xx - yy));
+    case 5: return make_float2(2.8906114426405538f * x * y * z, 0.45704579946446572f * y * (5.f * zz - 1.f));
+    case 6: return make_float2(0.3731763325901154f * z * (5.f * zz - 3.f), 0.45704579946446572f * x * (5.f * zz - 1.f));
+    default: return make_float2(1.4453057213202769f * z * (xx - yy), 0.59004358992664352f * x * (xx - 3.f * yy));
+    }
+}
+
 // Encoded input columns (c, c+1), c even. Columns 0..31: the two hash-grid
 // features of level c / 2. Columns 32..55: for axis a and band b < 4, column
-// 32 + 8a + 2b is sin(2^b pi x_a) and the next cos(2^b pi x_a). Then 56..58
-// direction, 59..61 normal, 62 roughness, 63..65 albedo, 66 constant 1,
-// 67..95 zero.
+// 32 + 8a + 2b is sin(2^b pi x_a) and the next cos(2^b pi x_a). Columns
+// 56..71: the 16 spherical harmonics of the outgoing direction. Then 72..74
+// normal, 75 roughness, 76..78 albedo, 79 constant 1, 80..95 zero.
 __device__ __forceinline__ float2 encode_pair(const float *f, int c, const MlpDev &M)
 {
     if (c < 2 * kGridLevels) return grid_features(M, c >> 1, f[0], f[1], f[2]);
@@ -146,13 +165,12 @@ __device__ __forceinline__ float2 encode_pair(const float *f, int c, const MlpDe
         sincospif(ldexpf(x, band), &s, &co);
         return make_float2(s, co);
     }
+    if (c < 72) return sh_pair(f[3], f[4], f[5], (c - 56) >> 1);
     switch (c) {
-    case 56: return make_float2(f[3], f[4]);
-    case 58: return make_float2(f[5], f[6]);
-    case 60: return make_float2(f[7], f[8]);
-    case 62: return make_float2(f[9], f[10]);
-    case 64: return make_float2(f[11], f[12]);
-    case 66: return make_float2(1.f, 0.f);
+    case 72: return make_float2(f[6], f[7]);
+    case 74: return make_float2(f[8], f[9]);
+    case 76: return make_float2(f[10], f[11]);
+    case 78: return make_float2(f[12], 1.f);
     default: return make_float2(0.f, 0.f);
     }
 }

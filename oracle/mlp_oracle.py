@@ -12,8 +12,9 @@ has no learned component, so this is this project's own oracle):
   cell's eight corners in float32 exactly as the device does it (corner
   order x, y, z bits; every product and sum rounded). Columns 32..55: for
   axis a and band b in 0..3, column 32 + 8a + 2b = sin(2^b pi x_a), the next
-  cos; 56..58 direction, 59..61 normal, 62 roughness, 63..65 albedo, 66
-  constant 1, 67..95 zero.
+  cos; 56..71 the 16 real spherical harmonics of degree < 4 of the outgoing
+  direction; 72..74 normal, 75 roughness, 76..78 albedo, 79 constant 1,
+  80..95 zero.
 * network: 96 -> 64 -> 64 -> 64 -> 64 -> 64 -> 8 (3 used), ReLU after every
   hidden layer, no biases, weights per layer row-major [in][out] in one flat
   vector of 23,040 floats.
@@ -84,6 +85,20 @@ def grid_features(grid, pos):
     return out
 
 
+def sh16(d):
+    """Real spherical harmonics, degree < 4, of unit vectors d (n, 3)."""
+    x, y, z = d[:, 0], d[:, 1], d[:, 2]
+    xx, yy, zz = x * x, y * y, z * z
+    return np.stack([
+        np.full_like(x, 0.28209479177387814), -0.48860251190291987 * y, 0.48860251190291987 * z,
+        -0.48860251190291987 * x, 1.0925484305920792 * x * y, -1.0925484305920792 * y * z,
+        0.94617469575755997 * zz - 0.31539156525251999, -1.0925484305920792 * x * z,
+        0.54627421529603959 * (xx - yy), 0.59004358992664352 * y * (3 * xx - yy),
+        2.8906114426405538 * x * y * z, 0.45704579946446572 * y * (5 * zz - 1),
+        0.3731763325901154 * z * (5 * zz - 3), 0.45704579946446572 * x * (5 * zz - 1),
+        1.4453057213202769 * z * (xx - yy), 0.59004358992664352 * x * (xx - 3 * yy)], 1)
+
+
 def init_grid(seed=0):
     rng = np.random.default_rng(seed + 7)
     return rng.uniform(-1e-4, 1e-4, GRID_PARAMS).astype(np.float32)
@@ -100,11 +115,11 @@ def encode(raw, grid):
             arg = np.pi * r[:, a] * (2.0 ** b)
             x[:, 32 + 8 * a + 2 * b] = np.sin(arg)
             x[:, 32 + 8 * a + 2 * b + 1] = np.cos(arg)
-    x[:, 56:59] = r[:, 3:6]
-    x[:, 59:62] = r[:, 6:9]
-    x[:, 62] = r[:, 9]
-    x[:, 63:66] = r[:, 10:13]
-    x[:, 66] = 1.0
+    x[:, 56:72] = sh16(r[:, 3:6])
+    x[:, 72:75] = r[:, 6:9]
+    x[:, 75] = r[:, 9]
+    x[:, 76:79] = r[:, 10:13]
+    x[:, 79] = 1.0
     return x
 
 
