@@ -609,10 +609,10 @@ static int run_render(ilg_ctx *ctx, std::vector<SceneRec> &recs, uint32_t cap_re
     CK(ctx->hit_tri.reserve(cap)); CK(ctx->hit_t.reserve(cap)); CK(ctx->path_scene.reserve(cap));
     CK(ctx->s_o.reserve((size_t)cap * nl)); CK(ctx->s_d.reserve((size_t)cap * nl)); CK(ctx->s_c.reserve((size_t)cap * nl));
     CK(ctx->s_sid.reserve((size_t)cap * nl));
-    CK(ctx->counts.reserve(8)); CK(ctx->accum.reserve(pixels));
+    CK(ctx->counts.reserve(8)); CK(ctx->accum.reserve((size_t)pixels + 1));
     CK(ctx->scene_table.reserve(recs.size()));
     CK(cudaMemcpyAsync(ctx->scene_table.ptr, recs.data(), recs.size() * sizeof(SceneRec), cudaMemcpyHostToDevice, st));
-    CK(cudaMemsetAsync(ctx->accum.ptr, 0, sizeof(float4) * pixels, st));
+    CK(cudaMemsetAsync(ctx->accum.ptr, 0, sizeof(float4) * ((size_t)pixels + 1), st));
 
     RenderDev R = {};
     R.scenes = ctx->scene_table.ptr; R.n_scenes = (uint32_t)recs.size(); R.depth_max = depth_max;
@@ -624,6 +624,7 @@ static int run_render(ilg_ctx *ctx, std::vector<SceneRec> &recs, uint32_t cap_re
     R.s_o = ctx->s_o.ptr; R.s_d = ctx->s_d.ptr; R.s_c = ctx->s_c.ptr;
     R.sh_count = ctx->counts.ptr + 2; R.sh_capacity = cap * nl;
     R.accum = ctx->accum.ptr; R.err = ctx->derr.ptr;
+    R.discard_pixel = pixels;
     if (aux) {
         CK(ctx->accum_direct.reserve(pixels));
         CK(ctx->accum_albedo.reserve(pixels));

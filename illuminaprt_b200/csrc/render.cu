@@ -298,6 +298,14 @@ __global__ void __launch_bounds__(256) k_shade(RenderDev R, int cur, uint32_t de
         uint32_t px, py;
         path_ident(S, wave_begin + path, pixel, key, px, py);
         pixel += S.pixel_base;
+        // A training path's pixel takes the cache's value at the cache vertex,
+        // as a rendering path's does; what its tail adds from there on (light
+        // samples at that vertex and beyond, escapes after it) only trains the
+        // cache and goes to the discard slot past the last pixel.
+        const uint32_t image_pixel = pixel;
+        if (R.cache_depth && tslot != 0xffffffffu &&
+            (ti >= 0 ? depth >= R.cache_depth : depth > R.cache_depth))
+            pixel = R.discard_pixel;
         float3 beta = make_float3(R.beta[path].x, R.beta[path].y, R.beta[path].z);
         float3 add = make_float3(0.f, 0.f, 0.f);
 
@@ -329,11 +337,15 @@ __global__ void __launch_bounds__(256) k_shade(RenderDev R, int cur, uint32_t de
             // (PathIntegrator.cpp:121); for the GGX conductor, its F0
             if (depth == 0 && R.accum_albedo) add_pixel(R.accum_albedo, pixel, m.kind == 1u ? m.f0 : m.albedo);
 
-            if (depth < S.max_depth && R.cache_depth && tslot == 0xffffffffu && depth == R.cache_depth) {
-                // a rendering path stops here: the cache supplies the radiance leaving this vertex
+            const bool at_cache = depth < S.max_depth && R.cache_depth && depth == R.cache_depth;
+            if (at_cache) {
+                // the cache supplies the radiance leaving this vertex to the pixel
                 query = true;
                 write_features(qf, R, p, wo, W, m);
-                qb = make_float4(beta.x, beta.y, beta.z, __uint_as_float(pixel));
+                qb = make_float4(beta.x, beta.y, beta.z, __uint_as_float(image_pixel));
+            }
+            if (at_cache && tslot == 0xffffffffu) {
+                // a rendering path stops here
             } else if (depth < S.max_depth) {
                 if (tslot != 0xffffffffu && depth >= 1) {
                     // training record of this vertex; its target fills in as the tail is traced

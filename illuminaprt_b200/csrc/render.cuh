@@ -70,7 +70,8 @@ struct RenderDev {
     float4 *s_o, *s_d, *s_c;  // shadow segments and their contribution (w = pixel bits)
     uint32_t *sh_count;
     uint32_t sh_capacity;
-    float4 *accum;         // per pixel rgb sums
+    float4 *accum;         // per pixel rgb sums, plus one discard slot at discard_pixel
+    uint32_t discard_pixel;
     float4 *accum_direct;  // per pixel sums of the first vertex's emission and light samples (or null)
     float4 *accum_albedo;  // per pixel sums of the first hit's albedo (or null)
     uint32_t *err;
