@@ -230,6 +230,22 @@ def bench_path_tracer(dev, local, legs=("box", "field", "mlp", "batch", "cache")
     ms = e0.elapsed_time(e1) / reps
     res["pt_box_256x256x16spp_ms"] = round(ms, 3)
     res["pt_box_msamples_s"] = round(256 * 256 * 16 / (ms / 1e3) / 1e6, 3)
+    # progressive display on the device: accumulate a 1080p frame and tone-map it
+    frame = torch.rand((1080, 1920, 3), device=dev)
+    avg, shown = torch.empty_like(frame), torch.empty_like(frame)
+    sp.accumulate(frame, out=avg)
+    sp.tonemap(avg, "drago", out=shown)
+    sp.sync()
+    e0.record(st)
+    for _ in range(10):
+        sp.accumulate(frame, out=avg)
+        sp.tonemap(avg, "drago", out=shown)
+    e1.record(st)
+    e1.synchronize()
+    pms = e0.elapsed_time(e1) / 10
+    res["post_1080p_accumulate_drago_ms"] = round(pms, 4)
+    # bytes: accumulate reads frame + sum, writes sum + out (48 B/px); Drago reads twice, writes once (36 B/px)
+    res["post_1080p_gbs"] = round(1920 * 1080 * 84 / (pms / 1e3) / 1e9, 1)
     sp.close()
     if "field" in legs:
         bench_field(res, dev, local, e0, e1)

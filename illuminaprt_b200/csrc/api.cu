@@ -846,6 +846,83 @@ int ilg_render_batch(ilg_ctx *runner, const ilg_batch_item *items, uint32_t n, u
 }  // extern "C"
 
 // ---------------------------------------------------------------------------
+// post-processing: progressive accumulation and tone mapping
+// ---------------------------------------------------------------------------
+extern "C" {
+
+int ilg_accumulate_reset(ilg_ctx *ctx)
+{
+    if (!ctx) return ILG_EINVAL;
+    CK(cudaSetDevice(ctx->device));
+    if (ctx->post_pixels) CK(cudaMemsetAsync(ctx->post_acc.ptr, 0, 12ull * ctx->post_pixels, ctx->stream));
+    ctx->post_frames = 0;
+    return ILG_OK;
+}
+
+int ilg_accumulate(ilg_ctx *ctx, const float *frame_rgb, uint32_t n_pixels, float *out_rgb, uint32_t flags)
+{
+    if (!ctx) return ILG_EINVAL;
+    if (!frame_rgb || !out_rgb || n_pixels == 0 || n_pixels > (1u << 28))
+        return fail(ctx, ILG_EINVAL, "ilg_accumulate: bad arguments");
+    if (flags & ~ILG_DEVICE_PTRS) return fail(ctx, ILG_EINVAL, "ilg_accumulate: unknown flags 0x%x", flags);
+    CK(cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    if (n_pixels != ctx->post_pixels) {  // a new image size starts a new accumulation
+        CK(ctx->post_acc.reserve(3ull * n_pixels));
+        CK(cudaMemsetAsync(ctx->post_acc.ptr, 0, 12ull * n_pixels, st));
+        ctx->post_pixels = n_pixels;
+        ctx->post_frames = 0;
+    }
+    ctx->post_frames++;
+    const bool dev = (flags & ILG_DEVICE_PTRS) != 0;
+    const float *in = frame_rgb;
+    float *out = out_rgb;
+    if (!dev) {
+        CK(ctx->post_in.reserve(3ull * n_pixels));
+        CK(ctx->post_out.reserve(3ull * n_pixels));
+        CK(cudaMemcpyAsync(ctx->post_in.ptr, frame_rgb, 12ull * n_pixels, cudaMemcpyHostToDevice, st));
+        in = ctx->post_in.ptr;
+        out = ctx->post_out.ptr;
+    }
+    CK(post_accumulate(in, ctx->post_acc.ptr, out, n_pixels, ctx->post_frames, st));
+    if (!dev) {
+        CK(cudaMemcpyAsync(out_rgb, out, 12ull * n_pixels, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+    }
+    return ILG_OK;
+}
+
+int ilg_tonemap(ilg_ctx *ctx, const float *in_rgb, uint32_t n_pixels, float *out_rgb, uint32_t op, uint32_t flags)
+{
+    if (!ctx) return ILG_EINVAL;
+    if (!in_rgb || !out_rgb || n_pixels == 0 || n_pixels > (1u << 28))
+        return fail(ctx, ILG_EINVAL, "ilg_tonemap: bad arguments");
+    if (op > ILG_TONE_DRAGO) return fail(ctx, ILG_EINVAL, "ilg_tonemap: unknown operator %u", op);
+    if (flags & ~ILG_DEVICE_PTRS) return fail(ctx, ILG_EINVAL, "ilg_tonemap: unknown flags 0x%x", flags);
+    CK(cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    const bool dev = (flags & ILG_DEVICE_PTRS) != 0;
+    const float *in = in_rgb;
+    float *out = out_rgb;
+    if (!dev) {
+        CK(ctx->post_in.reserve(3ull * n_pixels));
+        CK(ctx->post_out.reserve(3ull * n_pixels));
+        CK(cudaMemcpyAsync(ctx->post_in.ptr, in_rgb, 12ull * n_pixels, cudaMemcpyHostToDevice, st));
+        in = ctx->post_in.ptr;
+        out = ctx->post_out.ptr;
+    }
+    CK(ctx->post_scratch.reserve(post_scratch_floats(n_pixels)));
+    CK(post_tonemap(in, out, n_pixels, op, ctx->post_scratch.ptr, st));
+    if (!dev) {
+        CK(cudaMemcpyAsync(out_rgb, out, 12ull * n_pixels, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+    }
+    return ILG_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
 // radiance-cache network
 // ---------------------------------------------------------------------------
 namespace {

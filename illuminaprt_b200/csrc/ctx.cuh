@@ -10,6 +10,7 @@
 #include "trace_api.cuh"
 #include "render.cuh"
 #include "mlp.cuh"
+#include "postproc.cuh"
 
 struct ilg_ctx {
     int device = 0;
@@ -32,6 +33,10 @@ struct ilg_ctx {
     ilg::BuildBuffers bb;
     bool built = false;
     ilg_stats stats = {};
+
+    // progressive accumulation (AccumulationBuffer) and tone-mapping scratch
+    ilg::DevBuf<float> post_acc, post_in, post_out, post_scratch;
+    uint32_t post_pixels = 0, post_frames = 0;
 
     // the watertight test's vertex records (three float4 per triangle record)
     ilg::DevBuf<float4> raw_tris;
@@ -126,6 +131,8 @@ struct ilg_ctx {
         pos.release(); idx.release(); mat.release();
         bb.release_all();
         raw_tris.release(); raw_ready = false;
+        post_acc.release(); post_in.release(); post_out.release(); post_scratch.release();
+        post_pixels = post_frames = 0;
         ro.release(); rd.release(); hprim.release(); ht.release(); hu.release(); hv.release(); hocc.release();
         derr.release(); dstats.release();
         mats.release(); lights.release(); light_first_tri.release(); tri_attr.release(); light_of_prim.release();

@@ -31,7 +31,7 @@ EXPORTED = ["ilg_create", "ilg_destroy", "ilg_last_error", "ilg_set_mesh", "ilg_
             "ilg_mlp_init", "ilg_mlp_get_params", "ilg_mlp_set_params", "ilg_mlp_infer", "ilg_mlp_grads",
             "ilg_mlp_train_step", "ilg_render_batch", "ilg_intersect_excluding", "ilg_occluded_excluding",
             "ilg_camera_frame_of", "ilg_render_region", "ilg_mlp_get_grid", "ilg_mlp_set_grid",
-            "ilg_mlp_get_grid_grads"]
+            "ilg_mlp_get_grid_grads", "ilg_accumulate", "ilg_accumulate_reset", "ilg_tonemap"]
 
 ILG_MLP_RAW = 16
 ILG_MLP_WARP_MMA = 0x10
@@ -133,6 +133,9 @@ def load(build_if_missing: bool = True) -> ctypes.CDLL:
     L.ilg_set_quad_lights.argtypes = [vp, vp, u32]
     L.ilg_render.argtypes = [vp, ctypes.POINTER(ilg_camera), ctypes.POINTER(ilg_render_opts), vp, u32]
     L.ilg_intersect_noalloc.argtypes = [vp, vp, vp, u32, vp, vp, vp, vp]
+    L.ilg_accumulate.argtypes = [vp, vp, u32, vp, u32]
+    L.ilg_accumulate_reset.argtypes = [vp]
+    L.ilg_tonemap.argtypes = [vp, vp, u32, vp, u32, u32]
     L.ilg_camera_frame_of.argtypes = [ctypes.POINTER(ilg_camera), ctypes.POINTER(ilg_camera_frame)]
     L.ilg_render_region.argtypes = [vp, ctypes.POINTER(ilg_camera_frame), ctypes.POINTER(ilg_render_opts),
                                     ctypes.POINTER(ilg_region), vp, vp, vp, u32]
@@ -342,6 +345,33 @@ class GpuSpace:
         img = np.empty((height, width, 3), np.float32)
         self._check(self.L.ilg_render(self.h, ctypes.byref(cam), ctypes.byref(o), img.ctypes.data, 0))
         return img
+
+    # --- post-processing (AccumulationBuffer, tone operators) ---------------
+    TONE = {"global": 0, "auto": 1, "drago": 2}
+
+    def accumulate(self, frame, out=None):
+        """AccumulationBuffer::Apply: running average of the frames given since
+        the last reset (numpy in/out, or CUDA tensors with out given)."""
+        if out is not None:
+            self._check(self.L.ilg_accumulate(self.h, _ptr(frame), frame.numel() // 3, _ptr(out), ILG_DEVICE_PTRS))
+            return out
+        f = np.ascontiguousarray(frame, np.float32)
+        o = np.empty_like(f)
+        self._check(self.L.ilg_accumulate(self.h, f.ctypes.data, f.size // 3, o.ctypes.data, 0))
+        return o
+
+    def accumulate_reset(self):
+        self._check(self.L.ilg_accumulate_reset(self.h))
+
+    def tonemap(self, img, op: str = "global", out=None):
+        if out is not None:
+            self._check(self.L.ilg_tonemap(self.h, _ptr(img), img.numel() // 3, _ptr(out), self.TONE[op],
+                                           ILG_DEVICE_PTRS))
+            return out
+        f = np.ascontiguousarray(img, np.float32)
+        o = np.empty_like(f)
+        self._check(self.L.ilg_tonemap(self.h, f.ctypes.data, f.size // 3, o.ctypes.data, self.TONE[op], 0))
+        return o
 
     # --- radiance-cache network -------------------------------------------
     def mlp_init(self, seed: int = 1, lr: float = 1e-2):

@@ -283,6 +283,27 @@ typedef struct ilg_batch_item {
 int ilg_render_batch(ilg_ctx *runner, const ilg_batch_item *items, uint32_t n, uint32_t paths_per_wave,
                      uint32_t block, uint32_t flags);
 
+/* ------------------------------------------------------------------------
+ * Post-processing on the device, so a progressive renderer copies only the
+ * displayed image back. Images are n_pixels x 3 floats; host pointers unless
+ * ILG_DEVICE_PTRS (then both are device pointers and the call only enqueues).
+ * ---------------------------------------------------------------------- */
+/* AccumulationBuffer::Apply (Core/Postproc/AccumulationBuffer.h:59-87): the
+ * context's running sum gets frame_rgb added (sum = frame + sum) and out_rgb
+ * = sum * (1 / frames so far), bit for bit the reference's arithmetic. A new
+ * image size, or ilg_accumulate_reset (AccumulationBuffer::Reset), starts
+ * over. */
+int ilg_accumulate(ilg_ctx *ctx, const float *frame_rgb, uint32_t n_pixels, float *out_rgb, uint32_t flags);
+int ilg_accumulate_reset(ilg_ctx *ctx);
+
+#define ILG_TONE_GLOBAL 0u /* GlobalTone (Core/Postproc/GlobalTone.h): c / (c + 1) */
+#define ILG_TONE_AUTO 1u   /* AutoTone (AutoTone.h): (c - min) / (max - min), clamped to [0, 1] */
+#define ILG_TONE_DRAGO 2u  /* DragoTone (DragoTone.h): Drago et al. 2003, bias 0.8, scale 0.95 */
+/* Tone mapping of a whole image. GLOBAL and AUTO are bit for bit the
+ * reference's; DRAGO evaluates its logarithms and power in double as the
+ * reference does and agrees to within float rounding. */
+int ilg_tonemap(ilg_ctx *ctx, const float *in_rgb, uint32_t n_pixels, float *out_rgb, uint32_t op, uint32_t flags);
+
 /* Blocks until the context's stream is idle (for ILG_DEVICE_PTRS callers). */
 int ilg_sync(ilg_ctx *ctx);
 

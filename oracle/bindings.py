@@ -172,6 +172,7 @@ class RefLib:
         L.ilref_render_box_aov.argtypes = list(L.ilref_render_box.argtypes) + [_f32p, _f32p]
         L.ilref_render_box_renderer.argtypes = ([c.c_char_p, c.c_char_p] + list(L.ilref_render_box.argtypes[:17])
                                                 + [c.c_float, c.c_int, _f32p, _f32p, _f32p, c.c_char_p, c.c_int])
+        L.ilref_postprocess.argtypes = [c.c_int, _f32p, c.c_int, c.c_int, c.c_int, _f32p]
         L.ilref_compare_spaces.argtypes = [c.c_char_p, c.c_char_p, _f32p, _i32p, c.c_int, c.c_int, _f32p, c.c_int,
                                            _f32p, _f32p, _f32p, _f32p, c.c_long, c.c_void_p, _u8p, _f32p,
                                            c.c_void_p, _u8p, _u8p, _f32p, _u8p, c.c_char_p, c.c_int]
@@ -242,6 +243,19 @@ class RefLib:
         if rc:
             raise RuntimeError(f"ilref_render_box_renderer: {rc}: {err.value.decode(errors='replace')}")
         return tuple(outs)
+
+    def postprocess(self, op: str, frames):
+        """The reference's post-process on float32 images: op 'accumulate'
+        (frames: (F, H, W, 3), returns the F-th accumulated output), 'global',
+        'auto' or 'drago' (frames: (H, W, 3))."""
+        codes = {"accumulate": 0, "global": 1, "auto": 2, "drago": 3}
+        f = np.ascontiguousarray(frames, np.float32)
+        if op != "accumulate":
+            f = f[None]
+        n, h, w = f.shape[0], f.shape[1], f.shape[2]
+        out = np.zeros((h, w, 3), np.float32)
+        self.L.ilref_postprocess(codes[op], f.reshape(-1), n, w, h, out.reshape(-1))
+        return out
 
     def compare_spaces(self, plugin: str, scene: dict, o4, d4, exclude=None, factory: str = "GPU"):
         """BasicSpace vs the plug-in's space on the same primitives, ray by ray

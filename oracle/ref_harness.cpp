@@ -45,6 +45,10 @@
 #include "Sampler/RandomSampler.h"
 #include "Filter/BoxFilter.h"
 #include "System/EngineKernel.h"
+#include "Postproc/AccumulationBuffer.h"
+#include "Postproc/GlobalTone.h"
+#include "Postproc/AutoTone.h"
+#include "Postproc/DragoTone.h"
 #include "System/ArgumentMap.h"
 #include "Device/Device.h"
 #include "Renderer/Renderer.h"
@@ -655,6 +659,43 @@ int ilref_compare_spaces(const char *plugin_path, const char *factory,
 			}
 		}
 	}
+	return 0;
+}
+
+// The reference's post-processes on w x h rgb images (Core/Postproc/*.h).
+// op 0: AccumulationBuffer fed n_frames frames in turn, out = the last
+// Apply's output; op 1 GlobalTone, 2 AutoTone, 3 DragoTone on frames[0].
+int ilref_postprocess(int op, const float *frames, int n_frames, int w, int h, float *out)
+{
+	RadianceBuffer in(w, h), res(w, h), acc(w, h);
+	auto load = [&](const float *img) {
+		for (int y = 0; y < h; y++)
+			for (int x = 0; x < w; x++) {
+				const float *p = img + 3 * ((size_t)y * w + x);
+				RadianceContext *c = in.GetP(x, y);
+				c->Final = Spectrum(p[0], p[1], p[2]);
+				c->Flags = 0;
+			}
+	};
+	if (op == 0) {
+		AccumulationBuffer ab;
+		ab.SetAccumulationBuffer(&acc);
+		ab.Reset();
+		for (int f = 0; f < n_frames; f++) {
+			load(frames + 3 * (size_t)w * h * f);
+			ab.Apply(&in, &res);
+		}
+	} else {
+		load(frames);
+		GlobalTone g;
+		AutoTone a;
+		DragoTone d;
+		IPostProcess *pp = op == 1 ? (IPostProcess *)&g : (op == 2 ? (IPostProcess *)&a : (IPostProcess *)&d);
+		pp->Apply(&in, &res);
+	}
+	for (int y = 0; y < h; y++)
+		for (int x = 0; x < w; x++)
+			for (int k = 0; k < 3; k++) out[3 * ((size_t)y * w + x) + k] = res.GetP(x, y)->Final[k];
 	return 0;
 }
 

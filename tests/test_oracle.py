@@ -112,3 +112,24 @@ def test_watertight_oracle_agrees_with_reference_golden(oracle):
     # t within 1e-5 relative (measured: 4.8e-6 at most on these rays)
     rel = np.abs(wt[same] - rt[same]) / np.abs(rt[same])
     assert np.max(rel) < 1e-5
+
+
+def test_reference_post_processes_restated():
+    # pins the reference's AccumulationBuffer / GlobalTone / AutoTone
+    # arithmetic against a float32 numpy restatement
+    from oracle.bindings import RefLib, ref_available
+    if not ref_available():
+        pytest.skip("reference engine library not built")
+    ref = RefLib()
+    rng = np.random.default_rng(3)
+    fr = (rng.random((4, 9, 11, 3)) * 5).astype(np.float32)
+    acc = np.zeros_like(fr[0])
+    for k in range(4):
+        acc = fr[k] + acc
+        out = acc * np.float32(np.float32(1.0) / np.float32(k + 1))
+    assert np.array_equal(ref.postprocess("accumulate", fr), out)
+    assert np.array_equal(ref.postprocess("global", fr[0]), fr[0] / (fr[0] + np.float32(1)))
+    lo = np.minimum(fr[0].reshape(-1, 3).min(0), np.float32(3.4028235e38))
+    hi = np.maximum(fr[0].reshape(-1, 3).max(0), np.float32(0))
+    want = np.clip((fr[0] - lo) / (hi - lo), 0, 1).astype(np.float32)
+    assert np.array_equal(ref.postprocess("auto", fr[0]), want)
