@@ -647,6 +647,7 @@ static int run_render(ilg_ctx *ctx, std::vector<SceneRec> &recs, uint32_t cap_re
         CK(ctx->qry_feat.reserve((size_t)cap * kMlpRaw));
         CK(ctx->qry_out.reserve((size_t)cap * 3));
         CK(ctx->qry_beta.reserve(cap));
+        CK(ctx->mlp_enc.reserve((size_t)cap * kGridLevels));
         {
             int rc = mlp_reserve_train(ctx, train_batch);
             if (rc) return rc;
@@ -1007,6 +1008,7 @@ int ilg_mlp_infer(ilg_ctx *ctx, const float *raw, uint32_t n, float *out, uint32
     CK(cudaSetDevice(ctx->device));
     cudaStream_t st = ctx->stream;
     const bool warp_mma = (flags & ILG_MLP_WARP_MMA) != 0;
+    if (!warp_mma) CK(ctx->mlp_enc.reserve((size_t)n * kGridLevels));
     auto run = [&](const float *r, float *o) {
         return warp_mma ? mlp_infer_warp(ctx->mlp_view(), r, n, o, st) : mlp_infer(ctx->mlp_view(), r, n, o, st);
     };

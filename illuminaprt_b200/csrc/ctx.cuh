@@ -88,6 +88,7 @@ struct ilg_ctx {
     // radiance-cache network
     ilg::DevBuf<float> mlp_w, mlp_m, mlp_v, mlp_grad, mlp_loss, mlp_raw, mlp_tgt, mlp_out;
     ilg::DevBuf<float> mlp_grid, mlp_grid_grad, mlp_grid_m, mlp_grid_v;
+    ilg::DevBuf<uint32_t> mlp_enc;
     ilg::DevBuf<__nv_bfloat16> mlp_wf, mlp_wb, mlp_wu, mlp_xcm, mlp_hcm, mlp_dzcm;
     bool mlp_ready = false;
     uint32_t mlp_step = 0;
@@ -102,6 +103,8 @@ struct ilg_ctx {
         M.cap = (uint32_t)(mlp_xcm.cap / ilg::kMlpIn);
         M.grid = mlp_grid.ptr; M.grid_grad = mlp_grid_grad.ptr; M.grid_m = mlp_grid_m.ptr; M.grid_v = mlp_grid_v.ptr;
         ilg::grid_resolution(M.grid_res);
+        M.enc = mlp_enc.ptr;
+        M.enc_cap = (uint32_t)(mlp_enc.cap / ilg::kGridLevels);
         return M;
     }
 
@@ -143,7 +146,7 @@ struct ilg_ctx {
         train_slot.release(); rec_of.release(); s_meta.release(); rec_feat.release(); rec_tgt.release();
         qry_feat.release(); qry_out.release(); rec_beta.release(); qry_beta.release();
         mlp_w.release(); mlp_m.release(); mlp_v.release(); mlp_grad.release(); mlp_loss.release();
-        mlp_grid.release(); mlp_grid_grad.release(); mlp_grid_m.release(); mlp_grid_v.release();
+        mlp_grid.release(); mlp_grid_grad.release(); mlp_grid_m.release(); mlp_grid_v.release(); mlp_enc.release();
         mlp_raw.release(); mlp_tgt.release(); mlp_out.release(); mlp_wf.release(); mlp_wb.release(); mlp_wu.release();
         mlp_xcm.release(); mlp_hcm.release(); mlp_dzcm.release();
     }

@@ -82,6 +82,10 @@ struct MlpDev {
     // hash grid: FP32 features [level][entry][feature], their gradient and Adam moments
     float *grid, *grid_grad, *grid_m, *grid_v;
     uint32_t grid_res[kGridLevels];
+    // inference scratch: the grid columns of each query row, one packed BF16
+    // pair per level (enc_cap rows); null = the inference kernel gathers itself
+    uint32_t *enc;
+    uint32_t enc_cap;
 };
 
 // N_l of every level (host).

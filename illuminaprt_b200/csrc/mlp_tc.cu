@@ -120,6 +120,22 @@ __device__ __forceinline__ void put_chunk(unsigned char *a_tile, int r, int c, i
     *reinterpret_cast<uint4 *>(a_tile + (size_t)(r / 8) * kc * 128 + (size_t)c * 128 + (r % 8) * 16) = q;
 }
 
+// The grid columns of every query, one thread per (row, level): the gathers
+// of all levels of all rows in flight at once, at full occupancy, instead of
+// one thread walking its row's sixteen levels in turn inside the tensor-core
+// kernel (whose shared memory allows three CTAs per SM).
+__global__ void __launch_bounds__(256) k_grid_encode(const MlpDev M, const float *__restrict__ raw, uint32_t n,
+                                                     const uint32_t *__restrict__ n_dev)
+{
+    if (n_dev) n = min(n, *n_dev);
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t row = (uint32_t)(i / kGridLevels), l = (uint32_t)(i % kGridLevels);
+    if (row >= n) return;
+    const float *f = raw + (size_t)row * kMlpRaw;
+    const float2 g = grid_features(M, (int)l, f[0], f[1], f[2]);
+    M.enc[i] = pack2(g.x, g.y);
+}
+
 __global__ void __launch_bounds__(kTcRows) k_mlp_infer_tc(const MlpDev M, const float *__restrict__ raw, uint32_t n,
                                                           const uint32_t *__restrict__ n_dev,
                                                           float *__restrict__ out, uint32_t *__restrict__ err)
@@ -169,6 +185,19 @@ __global__ void __launch_bounds__(kTcRows) k_mlp_infer_tc(const MlpDev M, const 
 #pragma unroll
             for (int c = 0; c < kMlpIn / 8; c++) {
                 float v[8];
+                if (M.enc && c < 2 * kGridLevels / 8) {
+                    // grid columns precomputed by k_grid_encode (BF16, exact here)
+                    const uint4 q = row < n ? *reinterpret_cast<const uint4 *>(M.enc + (size_t)row * kGridLevels + 4 * c)
+                                            : make_uint4(0u, 0u, 0u, 0u);
+                    const uint32_t w4[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+                    for (int e = 0; e < 4; e++) {
+                        v[2 * e] = __uint_as_float(w4[e] << 16);
+                        v[2 * e + 1] = __uint_as_float(w4[e] & 0xffff0000u);
+                    }
+                    put_chunk(a_s, tid, c, kMlpIn, v);
+                    continue;
+                }
 #pragma unroll
                 for (int e = 0; e < 8; e += 2) {
                     const float2 p = encode_pair(f, 8 * c + e, M);
@@ -251,7 +280,13 @@ cudaError_t mlp_infer_tc(const MlpDev &M, const float *raw, uint32_t n, float *o
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     const uint32_t tiles = (n + kTcRows - 1) / kTcRows;
     const uint32_t grid = tiles < (uint32_t)sms * 3u ? tiles : (uint32_t)sms * 3u;
-    k_mlp_infer_tc<<<grid, kTcRows, smem, st>>>(M, raw, n, n_dev, out, err);
+    MlpDev Mi = M;
+    if (M.enc && n <= M.enc_cap) {
+        k_grid_encode<<<(unsigned)(((uint64_t)n * kGridLevels + 255) / 256), 256, 0, st>>>(M, raw, n, n_dev);
+    } else {
+        Mi.enc = nullptr;
+    }
+    k_mlp_infer_tc<<<grid, kTcRows, smem, st>>>(Mi, raw, n, n_dev, out, err);
     return cudaGetLastError();
 }
 
