@@ -281,6 +281,17 @@ def bench_cache(res, local):
     sp.close()
 
 
+def pt_bytes_per_sample(counts, samples):
+    """Algorithmic bytes per path sample from a counted render: every
+    closest-hit ray reads its 32-byte ray, the node and triangle records its
+    traversal visits (80 and 48 bytes) and moves ~64 bytes of path state
+    (hit, throughput, next queue entry); every shadow ray reads its 48-byte
+    segment and its records and adds a 16-byte contribution."""
+    cr, cn, ct, sr, sn, st = counts
+    total = cr * (32 + 64) + cn * NODE_BYTES + ct * TRI_BYTES + sr * (48 + 16) + sn * NODE_BYTES + st * TRI_BYTES
+    return total / samples
+
+
 def bench_field(res, dev, local, e0, e1):
     import torch
     from illuminaprt_b200 import scenes
@@ -298,6 +309,14 @@ def bench_field(res, dev, local, e0, e1):
     e1.record(st)
     e1.synchronize()
     ms = e0.elapsed_time(e1)
+    # traversal work of the same frame (a counted render, untimed) -> algorithmic bytes per sample
+    sp.render(field["camera"], W, H, spp, max_depth=12, seed=2, sky=field["sky"], out=out, count=True)
+    sp.sync()
+    bps = pt_bytes_per_sample(sp.render_counts(), W * H * spp)
+    hbm, _ = load_peaks()
+    res["pt_field_alg_bytes_per_sample"] = round(bps, 1)
+    res["pt_field_alg_gbs"] = round(bps * W * H * spp / (ms / 1e3) / 1e9, 1)
+    res["pt_field_roofline_frac"] = round(res["pt_field_alg_gbs"] / hbm, 4)
     res["pt_field_triangles"] = int(field["idx"].shape[0])
     res["pt_field_bvh_build_ms"] = round(sp.stats()["build_ms"], 2)
     res["pt_field_1080p_64spp_ms"] = round(ms, 2)

@@ -577,7 +577,7 @@ static int prepare_scene(ilg_ctx *runner, ilg_ctx *ctx, const ilg_camera_frame &
 // waves of at most `cap_req` paths on the runner's buffers and stream.
 static int run_render(ilg_ctx *ctx, std::vector<SceneRec> &recs, uint32_t cap_req, uint32_t block,
                       uint32_t cache_depth, uint32_t train_every, uint32_t train_steps, uint32_t train_batch,
-                      uint64_t *total_paths_out, bool aux = false)
+                      uint64_t *total_paths_out, bool aux = false, bool count = false)
 {
     cudaStream_t st = ctx->stream;
     uint64_t total = 0, pixels64 = 0;
@@ -625,6 +625,11 @@ static int run_render(ilg_ctx *ctx, std::vector<SceneRec> &recs, uint32_t cap_re
     R.sh_count = ctx->counts.ptr + 2; R.sh_capacity = cap * nl;
     R.accum = ctx->accum.ptr; R.err = ctx->derr.ptr;
     R.discard_pixel = pixels;
+    if (count) {
+        CK(ctx->render_stats.reserve(6));
+        CK(cudaMemsetAsync(ctx->render_stats.ptr, 0, 6 * sizeof(unsigned long long), st));
+        R.stats = ctx->render_stats.ptr;
+    }
     if (aux) {
         CK(ctx->accum_direct.reserve(pixels));
         CK(ctx->accum_albedo.reserve(pixels));
@@ -739,6 +744,7 @@ namespace {
 int render_one(ilg_ctx *ctx, const ilg_camera_frame &frame, const ilg_render_opts *opts, const ilg_region &reg,
                float *final_rgb, float *direct_rgb, float *albedo_rgb, uint32_t flags, bool use_cache)
 {
+    ctx->counted = (flags & ILG_RENDER_COUNT) != 0;
     const uint32_t cache_depth = use_cache ? opts->cache_depth : 0u;
     if (cache_depth) {
         if (!ctx->mlp_ready) return fail(ctx, ILG_ESTATE, "ilg_render: cache_depth set but ilg_mlp_init not called");
@@ -754,7 +760,8 @@ int render_one(ilg_ctx *ctx, const ilg_camera_frame &frame, const ilg_render_opt
     const uint32_t wh = recs[0].wh;
     const bool aux = direct_rgb || albedo_rgb;
     rc = run_render(ctx, recs, opts->paths_per_wave, 128, cache_depth, opts->train_every ? opts->train_every : 16u,
-                    opts->train_steps, opts->train_batch ? opts->train_batch : 16384u, nullptr, aux);
+                    opts->train_steps, opts->train_batch ? opts->train_batch : 16384u, nullptr, aux,
+                    ctx->counted);
     if (rc) return rc;
     const bool dev = (flags & ILG_DEVICE_PTRS) != 0;
     const float4 *sums[3] = {ctx->accum.ptr, ctx->accum_direct.ptr, ctx->accum_albedo.ptr};
@@ -789,11 +796,21 @@ int ilg_render(ilg_ctx *ctx, const ilg_camera *cam, const ilg_render_opts *opts,
 {
     if (!ctx) return ILG_EINVAL;
     if (!cam || !opts || !out_rgb) return fail(ctx, ILG_EINVAL, "ilg_render: null argument");
-    if (flags & ~ILG_DEVICE_PTRS) return fail(ctx, ILG_EINVAL, "ilg_render: unknown flags 0x%x", flags);
+    if (flags & ~(ILG_DEVICE_PTRS | ILG_RENDER_COUNT)) return fail(ctx, ILG_EINVAL, "ilg_render: unknown flags 0x%x", flags);
     ilg_camera_frame frame;
     camera_frame_of(*cam, frame);
     const ilg_region whole = {0u, 0u, opts->width, opts->height};
     return render_one(ctx, frame, opts, whole, out_rgb, nullptr, nullptr, flags, true);
+}
+
+int ilg_render_counts(ilg_ctx *ctx, uint64_t counts[6])
+{
+    if (!ctx || !counts) return ILG_EINVAL;
+    if (!ctx->counted) return fail(ctx, ILG_ESTATE, "ilg_render_counts: the last render was not counted");
+    CK(cudaSetDevice(ctx->device));
+    CK(cudaMemcpyAsync(counts, ctx->render_stats.ptr, 6 * sizeof(uint64_t), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return ILG_OK;
 }
 
 int ilg_render_region(ilg_ctx *ctx, const ilg_camera_frame *frame, const ilg_render_opts *opts,

@@ -74,6 +74,9 @@ struct ilg_ctx {
     uint32_t last_train_records = 0;
     float last_train_loss = 0.f;
     uint32_t last_render_launches = 0;
+    // work counters of the last render made with ILG_RENDER_COUNT
+    ilg::DevBuf<unsigned long long> render_stats;
+    bool counted = false;
     // the last frame's instantiated CUDA graph and the launch configuration it was captured for
     cudaGraphExec_t graph_exec = nullptr;
     std::vector<unsigned char> graph_key;
@@ -133,7 +136,7 @@ struct ilg_ctx {
         drop_graph();
         pos.release(); idx.release(); mat.release();
         bb.release_all();
-        raw_tris.release(); raw_ready = false;
+        raw_tris.release(); raw_ready = false; render_stats.release();
         post_acc.release(); post_in.release(); post_out.release(); post_scratch.release();
         post_pixels = post_frames = 0;
         ro.release(); rd.release(); hprim.release(); ht.release(); hu.release(); hv.release(); hocc.release();

@@ -192,18 +192,42 @@ __device__ __forceinline__ void write_features(float *f, const RenderDev &R, flo
     f[13] = f[14] = f[15] = 0.f;
 }
 
+// Work counters of a counted render: R.stats[k0] += rays, [k0 + 1] += node
+// records read, [k0 + 2] += triangle records tested (one atomic per warp).
+__device__ __forceinline__ void count_work(const RenderDev &R, int k0, bool ray, unsigned long long nn,
+                                           unsigned long long nt)
+{
+    unsigned long long r = ray ? 1ull : 0ull;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        r += __shfl_xor_sync(0xffffffffu, r, o);
+        nn += __shfl_xor_sync(0xffffffffu, nn, o);
+        nt += __shfl_xor_sync(0xffffffffu, nt, o);
+    }
+    if ((threadIdx.x & 31u) == 0u && r) {
+        atomicAdd(R.stats + k0, r);
+        atomicAdd(R.stats + k0 + 1, nn);
+        atomicAdd(R.stats + k0 + 2, nt);
+    }
+}
+
+template <bool kStats>
 __global__ void __launch_bounds__(256) k_extend(RenderDev R, int cur)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= R.count[cur]) return;
-    const float4 o = R.q_o[cur][i], d = R.q_d[cur][i];
-    const SceneRec &S = R.scenes[R.path_scene[R.q_path[cur][i]]];
-    int best;
-    float bt, bu, bv;
+    const bool live = i < R.count[cur];
+    if (!kStats && !live) return;
     unsigned long long nn = 0, nt = 0;
-    trace_one<false, false>(S.nodes, S.tris, S.n_nodes, S.n_tris, o, d, best, bt, bu, bv, R.err, nn, nt);
-    R.hit_tri[i] = best;
-    R.hit_t[i] = bt;
+    if (live) {
+        const float4 o = R.q_o[cur][i], d = R.q_d[cur][i];
+        const SceneRec &S = R.scenes[R.path_scene[R.q_path[cur][i]]];
+        int best;
+        float bt, bu, bv;
+        trace_one<false, kStats>(S.nodes, S.tris, S.n_nodes, S.n_tris, o, d, best, bt, bu, bv, R.err, nn, nt);
+        R.hit_tri[i] = best;
+        R.hit_t[i] = bt;
+    }
+    if (kStats) count_work(R, 0, live, nn, nt);
 }
 
 // GGX conductor (Trowbridge-Reitz D, Smith G1 separable, Schlick F), sampled
@@ -485,17 +509,22 @@ __global__ void k_cache_apply(RenderDev R)
     add_pixel(R.accum, __float_as_uint(b.w), make_float3(b.x * y.x, b.y * y.y, b.z * y.z));
 }
 
+template <bool kStats>
 __global__ void __launch_bounds__(256) k_shadow(RenderDev R)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= *R.sh_count) return;
-    const float4 o = R.s_o[i], d = R.s_d[i];
-    const SceneRec &S = R.scenes[R.s_sid[i]];
-    int best;
-    float bt, bu, bv;
+    const bool live = i < *R.sh_count;
+    if (!kStats && !live) return;
     unsigned long long nn = 0, nt = 0;
-    trace_one<true, false>(S.nodes, S.tris, S.n_nodes, S.n_tris, o, d, best, bt, bu, bv, R.err, nn, nt);
-    if (best == -1) {
+    int best = -2;
+    if (live) {
+        const float4 o = R.s_o[i], d = R.s_d[i];
+        const SceneRec &S = R.scenes[R.s_sid[i]];
+        float bt, bu, bv;
+        trace_one<true, kStats>(S.nodes, S.tris, S.n_nodes, S.n_tris, o, d, best, bt, bu, bv, R.err, nn, nt);
+    }
+    if (kStats) count_work(R, 3, live, nn, nt);
+    if (live && best == -1) {
         const float4 c = R.s_c[i];
         const uint32_t bits = __float_as_uint(c.w);
         add_pixel(R.accum, bits & 0x7fffffffu, make_float3(c.x, c.y, c.z));
@@ -568,7 +597,8 @@ cudaError_t render_wave(const RenderDev &R, uint32_t n_paths, uint64_t wave_begi
     for (uint32_t depth = 0; depth <= R.depth_max; depth++) {
         if ((e = cudaMemsetAsync(R.count + (cur ^ 1), 0, sizeof(uint32_t), st)) != cudaSuccess) return e;
         if ((e = cudaMemsetAsync(R.sh_count, 0, sizeof(uint32_t), st)) != cudaSuccess) return e;
-        k_extend<<<blocks_for(n_paths, T), T, 0, st>>>(R, cur);
+        if (R.stats) k_extend<true><<<blocks_for(n_paths, T), T, 0, st>>>(R, cur);
+        else k_extend<false><<<blocks_for(n_paths, T), T, 0, st>>>(R, cur);
         k_shade<<<blocks_for(n_paths, T), T, 0, st>>>(R, cur, depth, wave_begin);
         n_launch += 2;
         if (R.cache_depth && depth == R.cache_depth && cache) {
@@ -577,7 +607,8 @@ cudaError_t render_wave(const RenderDev &R, uint32_t n_paths, uint64_t wave_begi
             n_launch += 2;
         }
         if (depth < R.depth_max) {
-            k_shadow<<<blocks_for((uint64_t)R.sh_capacity, T), T, 0, st>>>(R);
+            if (R.stats) k_shadow<true><<<blocks_for((uint64_t)R.sh_capacity, T), T, 0, st>>>(R);
+            else k_shadow<false><<<blocks_for((uint64_t)R.sh_capacity, T), T, 0, st>>>(R);
             n_launch++;
         }
         if ((e = cudaGetLastError()) != cudaSuccess) return e;

@@ -75,6 +75,7 @@ struct RenderDev {
     float4 *accum_direct;  // per pixel sums of the first vertex's emission and light samples (or null)
     float4 *accum_albedo;  // per pixel sums of the first hit's albedo (or null)
     uint32_t *err;
+    unsigned long long *stats;  // counted render: [closest rays, nodes, tris, shadow rays, nodes, tris], or null
 
     // radiance cache (cache_depth == 0: plain path tracing, none of this is used)
     uint32_t cache_depth;      // rendering paths stop into the cache at this vertex

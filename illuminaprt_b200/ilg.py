@@ -20,6 +20,7 @@ from . import build as _build
 ILG_OK, ILG_EINVAL, ILG_ENOMEM, ILG_ECUDA, ILG_ETIMEOUT, ILG_EOVERFLOW, ILG_ESTATE = range(7)
 ILG_DEVICE_PTRS = 0x1
 ILG_WATERTIGHT = 0x2
+ILG_RENDER_COUNT = 0x4
 
 STATUS_NAMES = {0: "ILG_OK", 1: "ILG_EINVAL", 2: "ILG_ENOMEM", 3: "ILG_ECUDA", 4: "ILG_ETIMEOUT",
                 5: "ILG_EOVERFLOW", 6: "ILG_ESTATE"}
@@ -31,7 +32,8 @@ EXPORTED = ["ilg_create", "ilg_destroy", "ilg_last_error", "ilg_set_mesh", "ilg_
             "ilg_mlp_init", "ilg_mlp_get_params", "ilg_mlp_set_params", "ilg_mlp_infer", "ilg_mlp_grads",
             "ilg_mlp_train_step", "ilg_render_batch", "ilg_intersect_excluding", "ilg_occluded_excluding",
             "ilg_camera_frame_of", "ilg_render_region", "ilg_mlp_get_grid", "ilg_mlp_set_grid",
-            "ilg_mlp_get_grid_grads", "ilg_accumulate", "ilg_accumulate_reset", "ilg_tonemap"]
+            "ilg_mlp_get_grid_grads", "ilg_accumulate", "ilg_accumulate_reset", "ilg_tonemap",
+            "ilg_render_counts"]
 
 ILG_MLP_RAW = 16
 ILG_MLP_WARP_MMA = 0x10
@@ -133,6 +135,7 @@ def load(build_if_missing: bool = True) -> ctypes.CDLL:
     L.ilg_set_quad_lights.argtypes = [vp, vp, u32]
     L.ilg_render.argtypes = [vp, ctypes.POINTER(ilg_camera), ctypes.POINTER(ilg_render_opts), vp, u32]
     L.ilg_intersect_noalloc.argtypes = [vp, vp, vp, u32, vp, vp, vp, vp]
+    L.ilg_render_counts.argtypes = [vp, vp]
     L.ilg_accumulate.argtypes = [vp, vp, u32, vp, u32]
     L.ilg_accumulate_reset.argtypes = [vp]
     L.ilg_tonemap.argtypes = [vp, vp, u32, vp, u32, u32]
@@ -329,9 +332,16 @@ class GpuSpace:
                                              albedo.ctypes.data if aux else None, 0))
         return final, direct, albedo
 
+    def render_counts(self):
+        """Traversal work of the last render made with count=True:
+        (closest rays, their node reads, their triangle tests, shadow rays, node reads, triangle tests)."""
+        c = np.zeros(6, np.uint64)
+        self._check(self.L.ilg_render_counts(self.h, c.ctypes.data))
+        return tuple(int(x) for x in c)
+
     def render(self, camera: dict, width: int, height: int, spp: int, max_depth: int = 6, epsilon: float = 1e-4,
                seed: int = 1, sky=(0.0, 0.0, 0.0), paths_per_wave: int = 0, out=None, cache_depth: int = 0,
-               train_every: int = 16, train_steps: int = 4, train_batch: int = 16384):
+               train_every: int = 16, train_steps: int = 4, train_batch: int = 16384, count: bool = False):
         """Returns (height, width, 3) float32 (or fills `out`, a CUDA tensor, in place).
         cache_depth > 0 renders with the radiance cache (mlp_init first) and trains it afterwards."""
         cam = self._camera(camera, width, height)
@@ -340,10 +350,12 @@ class GpuSpace:
                             train_steps=train_steps, train_batch=train_batch)
         o.sky[:] = list(sky)
         if out is not None:
-            self._check(self.L.ilg_render(self.h, ctypes.byref(cam), ctypes.byref(o), _ptr(out), ILG_DEVICE_PTRS))
+            self._check(self.L.ilg_render(self.h, ctypes.byref(cam), ctypes.byref(o), _ptr(out),
+                                          ILG_DEVICE_PTRS | (ILG_RENDER_COUNT if count else 0)))
             return out
         img = np.empty((height, width, 3), np.float32)
-        self._check(self.L.ilg_render(self.h, ctypes.byref(cam), ctypes.byref(o), img.ctypes.data, 0))
+        self._check(self.L.ilg_render(self.h, ctypes.byref(cam), ctypes.byref(o), img.ctypes.data,
+                                      ILG_RENDER_COUNT if count else 0))
         return img
 
     # --- post-processing (AccumulationBuffer, tone operators) ---------------

@@ -195,6 +195,13 @@ int ilg_set_quad_lights(ilg_ctx *ctx, const ilg_quad_light *lights, uint32_t n);
 int ilg_render(ilg_ctx *ctx, const ilg_camera *cam, const ilg_render_opts *opts, float *out_rgb,
                uint32_t flags);
 
+/* ilg_render flag: count the traversal work of the render (slower kernels)
+ * for ilg_render_counts: counts = {closest-hit rays, node records they read,
+ * triangle records they tested, shadow rays, node records, triangle records}.
+ * These are the per-sample bytes of the path tracer's memory roofline. */
+#define ILG_RENDER_COUNT 0x4u
+int ilg_render_counts(ilg_ctx *ctx, uint64_t counts[6]);
+
 /* A camera as the reference's ICamera holds it after construction
  * (Core/Camera/Camera.h:23-28: m_centre, m_corner, m_across, m_up): the ray
  * through normalised image point (px, py) is normalize(corner + across * px

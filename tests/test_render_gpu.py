@@ -230,3 +230,23 @@ def test_direct_and_albedo_match_the_reference_aovs(box_space):
     assert e_albedo < 3e-4
     assert np.allclose(direct.mean((0, 1)), ref_direct.mean((0, 1)), rtol=3e-2)
     assert np.allclose(albedo.mean((0, 1)), ref_albedo.mean((0, 1)), rtol=1e-2)
+
+
+def test_counted_render_counts_the_traversal_work(box_space):
+    sp, scene = box_space
+    W = H = 64
+    spp = 4
+    plain = sp.render(scene["camera"], W, H, spp, seed=31)
+    counted = sp.render(scene["camera"], W, H, spp, seed=31, count=True)
+    assert np.allclose(plain, counted, rtol=1e-5, atol=1e-6)  # counting changes no result
+    cr, cn, ct, sr, sn, st = sp.render_counts()
+    samples = W * H * spp
+    # every sample traces its camera ray; the box scene keeps most paths
+    # bouncing, with one light sample per vertex that sees the light
+    assert samples <= cr <= samples * 7
+    assert cn >= cr and ct > 0
+    assert 0 < sr <= cr and sn >= sr
+    from illuminaprt_b200.ilg import IlgError
+    sp.render(scene["camera"], W, H, 1, seed=1)
+    with pytest.raises(IlgError):
+        sp.render_counts()  # the last render was not counted
