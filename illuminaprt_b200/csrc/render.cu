@@ -211,6 +211,20 @@ __device__ __forceinline__ void count_work(const RenderDev &R, int k0, bool ray,
     }
 }
 
+// An unoccluded shadow segment adds its contribution to its pixel (and to
+// Direct when tagged), and credits the training record it belongs to.
+__device__ __forceinline__ void shadow_unoccluded(const RenderDev &R, uint32_t i)
+{
+    const float4 c = R.s_c[i];
+    const uint32_t bits = __float_as_uint(c.w);
+    add_pixel(R.accum, bits & 0x7fffffffu, make_float3(c.x, c.y, c.z));
+    if (bits >> 31) add_pixel(R.accum_direct, bits & 0x7fffffffu, make_float3(c.x, c.y, c.z));
+    if (R.cache_depth) {
+        const uint32_t meta = R.s_meta[i];
+        if (meta != 0xffffffffu) credit(R, meta >> 8, meta & 0xffu, make_float3(c.x, c.y, c.z));
+    }
+}
+
 template <bool kStats>
 __global__ void __launch_bounds__(256) k_extend(RenderDev R, int cur)
 {
@@ -524,16 +538,72 @@ __global__ void __launch_bounds__(256) k_shadow(RenderDev R)
         trace_one<true, kStats>(S.nodes, S.tris, S.n_nodes, S.n_tris, o, d, best, bt, bu, bv, R.err, nn, nt);
     }
     if (kStats) count_work(R, 3, live, nn, nt);
-    if (live && best == -1) {
-        const float4 c = R.s_c[i];
-        const uint32_t bits = __float_as_uint(c.w);
-        add_pixel(R.accum, bits & 0x7fffffffu, make_float3(c.x, c.y, c.z));
-        if (bits >> 31) add_pixel(R.accum_direct, bits & 0x7fffffffu, make_float3(c.x, c.y, c.z));
-        if (R.cache_depth) {
-            const uint32_t meta = R.s_meta[i];
-            if (meta != 0xffffffffu) credit(R, meta >> 8, meta & 0xffu, make_float3(c.x, c.y, c.z));
+    if (live && best == -1) shadow_unoccluded(R, i);
+}
+
+// ---------------------------------------------------------------------------
+// Persistent forms of k_extend and k_shadow: each warp keeps its lanes busy by
+// fetching a new ray from a device counter whenever kRefillLanes lanes are
+// idle (as k_trace_dyn does for batched queries), so the incoherent bounce
+// and shadow rays do not leave lanes waiting on the longest ray of a warp.
+// Rays of one warp may belong to different scenes of a batch; each lane
+// traverses its own scene's tree.
+// ---------------------------------------------------------------------------
+template <bool kAnyHit>
+__device__ __forceinline__ void wave_trace_dyn(const RenderDev &R, uint32_t n, uint32_t *next, int cur)
+{
+    const uint32_t lane = threadIdx.x & 31u;
+    uint2 stack[kMaxStack];
+    RayState r;
+    const Node8 *nodes = nullptr;
+    const Tri *tris = nullptr;
+    uint32_t n_nodes = 0, n_tris = 0;
+    bool active = false, exhausted = false;  // exhausted is warp-uniform
+    uint32_t id = 0;
+    while (true) {
+        const uint32_t idle = __ballot_sync(0xffffffffu, !active);
+        if (!exhausted && (__popc(idle) >= kRefillLanes || idle == 0xffffffffu)) {
+            const uint32_t leader = __ffs(idle) - 1u;
+            uint32_t base = 0;
+            if (lane == leader) base = atomicAdd(next, (uint32_t)__popc(idle));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (base >= n) exhausted = true;
+            if (!active) {
+                const uint32_t k = base + __popc(idle & ((1u << lane) - 1u));
+                if (k < n) {
+                    id = k;
+                    const SceneRec &S = R.scenes[kAnyHit ? R.s_sid[id] : R.path_scene[R.q_path[cur][id]]];
+                    nodes = S.nodes;
+                    tris = S.tris;
+                    n_nodes = S.n_nodes;
+                    n_tris = S.n_tris;
+                    if (kAnyHit) ray_init(r, R.s_o[id], R.s_d[id], n_nodes);
+                    else ray_init(r, R.q_o[cur][id], R.q_d[cur][id], n_nodes);
+                    active = true;
+                }
+            }
+        }
+        if (__ballot_sync(0xffffffffu, active) == 0u) break;
+        if (active && ray_step<kAnyHit>(r, stack, nodes, tris, n_nodes, n_tris, R.err)) {
+            if (kAnyHit) {
+                if (r.best == -1) shadow_unoccluded(R, id);
+            } else {
+                R.hit_tri[id] = r.best;
+                R.hit_t[id] = r.best >= 0 ? r.tcur : __int_as_float(0x7f800000);
+            }
+            active = false;
         }
     }
+}
+
+__global__ void __launch_bounds__(128) k_extend_dyn(RenderDev R, int cur, uint32_t *next)
+{
+    wave_trace_dyn<false>(R, min(R.count[cur], R.capacity), next, cur);
+}
+
+__global__ void __launch_bounds__(128) k_shadow_dyn(RenderDev R, uint32_t *next)
+{
+    wave_trace_dyn<true>(R, min(*R.sh_count, R.sh_capacity), next, 0);
 }
 
 __global__ void k_resolve(const float4 *__restrict__ accum, uint32_t wh, float scale, float *__restrict__ out)
@@ -567,6 +637,21 @@ __global__ void k_light_of_prim(uint32_t *lop, uint32_t n_prims, const uint32_t 
 
 inline uint32_t blocks_for(uint64_t n, uint32_t t) { return (uint32_t)((n + t - 1) / t); }
 
+// Grid of a persistent kernel of 128-thread blocks over at most n items.
+inline uint32_t persistent_blocks(uint64_t n)
+{
+    static int sms = 0;
+    if (!sms) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 148;
+    }
+    const uint32_t b = blocks_for(n, 128);
+    const uint32_t cap = (uint32_t)sms * 16u;
+    return b < 1u ? 1u : (b < cap ? b : cap);
+}
+
 }  // namespace
 
 cudaError_t build_tri_attr(const uint32_t *prim_of, uint32_t n_tris, const uint32_t *mat_ids,
@@ -597,8 +682,14 @@ cudaError_t render_wave(const RenderDev &R, uint32_t n_paths, uint64_t wave_begi
     for (uint32_t depth = 0; depth <= R.depth_max; depth++) {
         if ((e = cudaMemsetAsync(R.count + (cur ^ 1), 0, sizeof(uint32_t), st)) != cudaSuccess) return e;
         if ((e = cudaMemsetAsync(R.sh_count, 0, sizeof(uint32_t), st)) != cudaSuccess) return e;
-        if (R.stats) k_extend<true><<<blocks_for(n_paths, T), T, 0, st>>>(R, cur);
-        else k_extend<false><<<blocks_for(n_paths, T), T, 0, st>>>(R, cur);
+        if (R.stats) {
+            k_extend<true><<<blocks_for(n_paths, T), T, 0, st>>>(R, cur);
+        } else if (!R.persistent) {
+            k_extend<false><<<blocks_for(n_paths, T), T, 0, st>>>(R, cur);
+        } else {
+            if ((e = cudaMemsetAsync(R.count + 6, 0, sizeof(uint32_t), st)) != cudaSuccess) return e;
+            k_extend_dyn<<<persistent_blocks(n_paths), 128, 0, st>>>(R, cur, R.count + 6);
+        }
         k_shade<<<blocks_for(n_paths, T), T, 0, st>>>(R, cur, depth, wave_begin);
         n_launch += 2;
         if (R.cache_depth && depth == R.cache_depth && cache) {
@@ -607,8 +698,14 @@ cudaError_t render_wave(const RenderDev &R, uint32_t n_paths, uint64_t wave_begi
             n_launch += 2;
         }
         if (depth < R.depth_max) {
-            if (R.stats) k_shadow<true><<<blocks_for((uint64_t)R.sh_capacity, T), T, 0, st>>>(R);
-            else k_shadow<false><<<blocks_for((uint64_t)R.sh_capacity, T), T, 0, st>>>(R);
+            if (R.stats) {
+                k_shadow<true><<<blocks_for((uint64_t)R.sh_capacity, T), T, 0, st>>>(R);
+            } else if (!R.persistent) {
+                k_shadow<false><<<blocks_for((uint64_t)R.sh_capacity, T), T, 0, st>>>(R);
+            } else {
+                if ((e = cudaMemsetAsync(R.count + 7, 0, sizeof(uint32_t), st)) != cudaSuccess) return e;
+                k_shadow_dyn<<<persistent_blocks(R.sh_capacity), 128, 0, st>>>(R, R.count + 7);
+            }
             n_launch++;
         }
         if ((e = cudaGetLastError()) != cudaSuccess) return e;

@@ -76,6 +76,9 @@ struct RenderDev {
     float4 *accum_albedo;  // per pixel sums of the first hit's albedo (or null)
     uint32_t *err;
     unsigned long long *stats;  // counted render: [closest rays, nodes, tris, shadow rays, nodes, tris], or null
+    // persistent (dynamic-fetch) extend and shadow kernels; off when every
+    // scene is tiny, where rays are too short for refills to pay
+    uint32_t persistent;
 
     // radiance cache (cache_depth == 0: plain path tracing, none of this is used)
     uint32_t cache_depth;      // rendering paths stop into the cache at this vertex
