@@ -104,10 +104,8 @@ class ClockSampler:
 
 
 def dist_setup():
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    return world, rank, local
+    from illuminaprt_b200 import replicas
+    return replicas.rank_info()
 
 
 def run_reference(args, world, rank):
@@ -137,7 +135,7 @@ def run_reference(args, world, rank):
     tracer(co[:probe // 2], cd[:probe // 2])
     tracer(io[:probe // 2], idr[:probe // 2])
     rate = probe / max(time.perf_counter() - t0, 1e-6)
-    per_step = int(min(co.shape[0], max(8192, rate * 120.0 / max(1, args.steps + args.warmup)))) // 2 * 2
+    per_step = int(min(co.shape[0], max(8192, rate * args.ref_seconds / max(1, args.steps + args.warmup)))) // 2 * 2
     rng = np.random.default_rng(11)
     half = per_step // 2
     for _ in range(args.warmup):
@@ -385,6 +383,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ref-seconds", type=float, default=120.0,
+                    help="reference arm: seconds of CPU work over all steps (sizes each step's sample)")
     ap.add_argument("--no-path-tracer", action="store_true")
     ap.add_argument("--legs", default="box,field,mlp,batch,cache",
                     help="extra measurements after the ray query: box,field,mlp,batch")
@@ -396,13 +396,12 @@ def main():
         return
 
     import torch
-    import torch.distributed as dist
     from illuminaprt_b200 import scenes
     from illuminaprt_b200.ilg import GpuSpace
 
+    from illuminaprt_b200 import replicas
     torch.cuda.set_device(local)
-    if world > 1:
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    replicas.init("nccl")
 
     pos, idx, (co, cd), (io, idr) = scenes.ray_batch_workload()
     n_co, n_in = co.shape[0], io.shape[0]
@@ -434,8 +433,7 @@ def main():
     for _ in range(args.warmup):
         step()
     sp.sync()
-    if world > 1:
-        dist.barrier()
+    replicas.barrier()
     torch.cuda.synchronize()
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * args.steps + 1)]
     with ClockSampler(local) as clk:
@@ -453,13 +451,9 @@ def main():
     clocks = clk.summary()
     t_co = sum(ev[2 * s].elapsed_time(ev[2 * s + 1]) for s in range(args.steps))
     t_in = sum(ev[2 * s + 1].elapsed_time(ev[2 * s + 2]) for s in range(args.steps))
-    total_ms = ev[0].elapsed_time(ev[-1])
-    if world > 1:
-        tt = torch.tensor([total_ms], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        total_ms = float(tt.item())
+    total_ms = replicas.max_over_ranks(ev[0].elapsed_time(ev[-1]), dev)
     rays_per_step = n_co + n_in
-    value = world * rays_per_step * args.steps / (total_ms / 1e3) / 1e6
+    value = replicas.aggregate_rate(rays_per_step * args.steps, world, total_ms / 1e3) / 1e6
 
     # the same incoherent batch with the watertight triangle test (ILG_WATERTIGHT)
     o, d = rays["incoherent"]
@@ -486,20 +480,15 @@ def main():
     for k in ("coherent", "incoherent"):
         sp.intersects_into(*pin[k], *hout[k], device_ptrs=False)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    if world > 1:
-        dist.barrier()
+    replicas.barrier()
     e0.record(stream)
     for _ in range(e2e_steps):
         for k in ("coherent", "incoherent"):
             sp.intersects_into(*pin[k], *hout[k], device_ptrs=False)
     e1.record(stream)
     e1.synchronize()
-    e2e_ms = e0.elapsed_time(e1)
-    if world > 1:
-        tt = torch.tensor([e2e_ms], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_ms = float(tt.item())
-    e2e_value = world * rays_per_step * e2e_steps / (e2e_ms / 1e3) / 1e6
+    e2e_ms = replicas.max_over_ranks(e0.elapsed_time(e1), dev)
+    e2e_value = replicas.aggregate_rate(rays_per_step * e2e_steps, world, e2e_ms / 1e3) / 1e6
     # the e2e hits must equal the device-resident ones
     assert torch.equal(hout["incoherent"][0], out["incoherent"][0].cpu())
     # the copy bound of e2e: the same host->device bytes as one plain pinned copy
@@ -566,9 +555,8 @@ def main():
             line["cpu_baseline"] = cpu_baseline_sample(pos, idx, co, cd, io, idr)
         print(json.dumps(line), flush=True)
     sp.close()
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
+    replicas.barrier()
+    replicas.finish()
 
 
 if __name__ == "__main__":
