@@ -266,6 +266,162 @@ int ilg_build(ilg_ctx *ctx)
     return ILG_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Persistent scenes: the uploaded mesh and the built 8-wide BVH in one file,
+// so a scene is loaded instead of rebuilt. Layout (little-endian): a 64-byte
+// header, then positions (12 B a vertex), indices (12 B a triangle), material
+// ids (4 B a triangle, when present), node records (80 B), triangle records
+// (48 B), record -> input triangle map (4 B), and an FNV-1a 64 checksum of
+// everything after the header.
+// ---------------------------------------------------------------------------
+namespace {
+
+struct SceneFileHeader {
+    char magic[8];  // "ILGBVH8\0"
+    uint32_t version, header_bytes;
+    uint32_t n_verts, n_tris, n_nodes, n_leaf_tris;
+    uint32_t max_depth, has_mat, node_bytes, tri_bytes;
+    uint64_t payload_bytes;
+    uint64_t reserved;
+};
+static_assert(sizeof(SceneFileHeader) == 64, "scene file header is 64 bytes");
+
+constexpr uint32_t kSceneFileVersion = 1;
+
+uint64_t fnv1a(uint64_t h, const void *data, size_t n)
+{
+    const unsigned char *p = static_cast<const unsigned char *>(data);
+    for (size_t i = 0; i < n; i++) {
+        h ^= p[i];
+        h *= 0x100000001B3ull;
+    }
+    return h;
+}
+
+}  // namespace
+
+int ilg_save(ilg_ctx *ctx, const char *path)
+{
+    if (!ctx || !path) return ILG_EINVAL;
+    if (!ctx->built) return fail(ctx, ILG_ESTATE, "ilg_save: scene not built");
+    CK(cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    SceneFileHeader h;
+    memset(&h, 0, sizeof(h));
+    memcpy(h.magic, "ILGBVH8", 8);
+    h.version = kSceneFileVersion;
+    h.header_bytes = sizeof(h);
+    h.n_verts = ctx->n_verts;
+    h.n_tris = ctx->n_tris;
+    h.n_nodes = ctx->stats.n_nodes;
+    h.n_leaf_tris = ctx->stats.n_leaf_tris;
+    h.max_depth = ctx->stats.max_depth;
+    h.has_mat = ctx->has_mat ? 1u : 0u;
+    h.node_bytes = sizeof(Node8);
+    h.tri_bytes = sizeof(Tri);
+    std::vector<float> pos(3ull * h.n_verts);
+    std::vector<uint32_t> idx(3ull * h.n_tris), mat(h.has_mat ? h.n_tris : 0), prim(h.n_leaf_tris);
+    std::vector<Node8> nodes(h.n_nodes);
+    std::vector<Tri> tris(h.n_leaf_tris);
+    CK(cudaMemcpyAsync(pos.data(), ctx->pos.ptr, 12ull * h.n_verts, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(idx.data(), ctx->idx.ptr, 12ull * h.n_tris, cudaMemcpyDeviceToHost, st));
+    if (h.has_mat) CK(cudaMemcpyAsync(mat.data(), ctx->mat.ptr, 4ull * h.n_tris, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(nodes.data(), ctx->bb.nodes, sizeof(Node8) * h.n_nodes, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(tris.data(), ctx->bb.tris, sizeof(Tri) * h.n_leaf_tris, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(prim.data(), ctx->bb.prim_of, 4ull * h.n_leaf_tris, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    const std::pair<const void *, size_t> parts[6] = {
+        {pos.data(), 12ull * h.n_verts}, {idx.data(), 12ull * h.n_tris}, {mat.data(), 4ull * mat.size()},
+        {nodes.data(), sizeof(Node8) * nodes.size()}, {tris.data(), sizeof(Tri) * tris.size()},
+        {prim.data(), 4ull * prim.size()}};
+    uint64_t sum = 0xCBF29CE484222325ull;
+    for (auto &q : parts) {
+        h.payload_bytes += q.second;
+        sum = fnv1a(sum, q.first, q.second);
+    }
+    FILE *f = fopen(path, "wb");
+    if (!f) return fail(ctx, ILG_EINVAL, "ilg_save: cannot open %s for writing", path);
+    bool ok = fwrite(&h, sizeof(h), 1, f) == 1;
+    for (auto &q : parts)
+        if (ok && q.second) ok = fwrite(q.first, 1, q.second, f) == q.second;
+    ok = ok && fwrite(&sum, sizeof(sum), 1, f) == 1;
+    ok = (fclose(f) == 0) && ok;
+    if (!ok) return fail(ctx, ILG_EINVAL, "ilg_save: writing %s failed", path);
+    return ILG_OK;
+}
+
+int ilg_load(ilg_ctx *ctx, const char *path)
+{
+    if (!ctx || !path) return ILG_EINVAL;
+    FILE *f = fopen(path, "rb");
+    if (!f) return fail(ctx, ILG_EINVAL, "ilg_load: cannot open %s", path);
+    SceneFileHeader h;
+    auto bad = [&](const char *why) {
+        fclose(f);
+        return fail(ctx, ILG_EINVAL, "ilg_load: %s: %s", path, why);
+    };
+    if (fread(&h, sizeof(h), 1, f) != 1) return bad("short header");
+    if (memcmp(h.magic, "ILGBVH8", 8) != 0) return bad("not a scene file");
+    if (h.version != kSceneFileVersion || h.header_bytes != sizeof(h)) return bad("unsupported version");
+    if (h.node_bytes != sizeof(Node8) || h.tri_bytes != sizeof(Tri)) return bad("record sizes differ");
+    if (h.n_verts == 0 || h.n_tris == 0 || h.n_tris > (1u << 30) || h.n_leaf_tris != h.n_tris || h.n_nodes == 0 ||
+        h.n_nodes > h.n_tris + 1u || h.has_mat > 1u)
+        return bad("inconsistent counts");
+    const uint64_t expect = 12ull * h.n_verts + 12ull * h.n_tris + (h.has_mat ? 4ull * h.n_tris : 0ull) +
+                            sizeof(Node8) * (uint64_t)h.n_nodes + sizeof(Tri) * (uint64_t)h.n_leaf_tris +
+                            4ull * h.n_leaf_tris;
+    if (h.payload_bytes != expect) return bad("payload size differs from the counts");
+    std::vector<float> pos(3ull * h.n_verts);
+    std::vector<uint32_t> idx(3ull * h.n_tris), mat(h.has_mat ? h.n_tris : 0), prim(h.n_leaf_tris);
+    std::vector<Node8> nodes(h.n_nodes);
+    std::vector<Tri> tris(h.n_leaf_tris);
+    const std::pair<void *, size_t> parts[6] = {
+        {pos.data(), 12ull * h.n_verts}, {idx.data(), 12ull * h.n_tris}, {mat.data(), 4ull * mat.size()},
+        {nodes.data(), sizeof(Node8) * nodes.size()}, {tris.data(), sizeof(Tri) * tris.size()},
+        {prim.data(), 4ull * prim.size()}};
+    uint64_t sum = 0xCBF29CE484222325ull, stored = 0;
+    for (auto &q : parts) {
+        if (q.second && fread(q.first, 1, q.second, f) != q.second) return bad("truncated");
+        sum = fnv1a(sum, q.first, q.second);
+    }
+    if (fread(&stored, sizeof(stored), 1, f) != 1) return bad("truncated checksum");
+    fclose(f);
+    if (stored != sum) return fail(ctx, ILG_EINVAL, "ilg_load: %s: checksum mismatch", path);
+    // record -> triangle map: a permutation of the triangles (the renderer indexes with it)
+    {
+        std::vector<unsigned char> seen(h.n_tris, 0);
+        for (uint32_t p : prim) {
+            if (p >= h.n_tris || seen[p]) return fail(ctx, ILG_EINVAL, "ilg_load: %s: bad triangle map", path);
+            seen[p] = 1;
+        }
+    }
+    int rc = ilg_set_mesh(ctx, pos.data(), h.n_verts, idx.data(), h.n_tris, h.has_mat ? mat.data() : nullptr);
+    if (rc) return rc;
+    CK(cudaSetDevice(ctx->device));
+    cudaStream_t st = ctx->stream;
+    CK(ctx->bb.nodes_b.reserve(h.n_nodes));
+    CK(ctx->bb.tris_b.reserve(h.n_leaf_tris));
+    CK(ctx->bb.prim_of_b.reserve(h.n_leaf_tris));
+    ctx->bb.nodes = ctx->bb.nodes_b.ptr;
+    ctx->bb.tris = ctx->bb.tris_b.ptr;
+    ctx->bb.prim_of = ctx->bb.prim_of_b.ptr;
+    CK(cudaMemcpyAsync(ctx->bb.nodes, nodes.data(), sizeof(Node8) * h.n_nodes, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(ctx->bb.tris, tris.data(), sizeof(Tri) * h.n_leaf_tris, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(ctx->bb.prim_of, prim.data(), 4ull * h.n_leaf_tris, cudaMemcpyHostToDevice, st));
+    CK(cudaStreamSynchronize(st));
+    ctx->stats.n_tris = h.n_tris;
+    ctx->stats.n_nodes = h.n_nodes;
+    ctx->stats.n_leaf_tris = h.n_leaf_tris;
+    ctx->stats.max_depth = h.max_depth;
+    ctx->stats.build_ms = 0.f;
+    ctx->stats.node_bytes = (uint64_t)h.n_nodes * sizeof(Node8);
+    ctx->stats.tri_bytes = (uint64_t)h.n_leaf_tris * sizeof(Tri);
+    ctx->built = true;
+    ctx->attr_dirty = true;
+    ctx->raw_ready = false;
+    return ILG_OK;
+}
+
 int ilg_get_stats(const ilg_ctx *ctx, ilg_stats *out)
 {
     if (!ctx || !out) return ILG_EINVAL;

@@ -33,7 +33,7 @@ EXPORTED = ["ilg_create", "ilg_destroy", "ilg_last_error", "ilg_set_mesh", "ilg_
             "ilg_mlp_train_step", "ilg_render_batch", "ilg_intersect_excluding", "ilg_occluded_excluding",
             "ilg_camera_frame_of", "ilg_render_region", "ilg_mlp_get_grid", "ilg_mlp_set_grid",
             "ilg_mlp_get_grid_grads", "ilg_accumulate", "ilg_accumulate_reset", "ilg_tonemap",
-            "ilg_render_counts"]
+            "ilg_render_counts", "ilg_save", "ilg_load"]
 
 ILG_MLP_RAW = 16
 ILG_MLP_WARP_MMA = 0x10
@@ -136,6 +136,8 @@ def load(build_if_missing: bool = True) -> ctypes.CDLL:
     L.ilg_render.argtypes = [vp, ctypes.POINTER(ilg_camera), ctypes.POINTER(ilg_render_opts), vp, u32]
     L.ilg_intersect_noalloc.argtypes = [vp, vp, vp, u32, vp, vp, vp, vp]
     L.ilg_render_counts.argtypes = [vp, vp]
+    L.ilg_save.argtypes = [vp, ctypes.c_char_p]
+    L.ilg_load.argtypes = [vp, ctypes.c_char_p]
     L.ilg_accumulate.argtypes = [vp, vp, u32, vp, u32]
     L.ilg_accumulate_reset.argtypes = [vp]
     L.ilg_tonemap.argtypes = [vp, vp, u32, vp, u32, u32]
@@ -331,6 +333,14 @@ class GpuSpace:
                                              final.ctypes.data, direct.ctypes.data if aux else None,
                                              albedo.ctypes.data if aux else None, 0))
         return final, direct, albedo
+
+    def save(self, path: str):
+        """Writes the mesh and its built BVH (ilg_save)."""
+        self._check(self.L.ilg_save(self.h, str(path).encode()))
+
+    def load(self, path: str):
+        """Reads a scene written by save: the context is built, no rebuild (ilg_load)."""
+        self._check(self.L.ilg_load(self.h, str(path).encode()))
 
     def render_counts(self):
         """Traversal work of the last render made with count=True:

@@ -80,6 +80,15 @@ int ilg_set_mesh(ilg_ctx *ctx, const float *pos_xyz, uint32_t n_verts,
 int ilg_build(ilg_ctx *ctx);
 int ilg_get_stats(const ilg_ctx *ctx, ilg_stats *out);
 
+/* Persistent scenes (this project's format; the reference's counterpart is
+ * its memory-mapped PersistentMesh, Core/Shape/PersistentMesh.h:22-35): the
+ * uploaded mesh and the built BVH written to / read from one checksummed
+ * file. ilg_load leaves the context as ilg_set_mesh + ilg_build would, with
+ * the same records, without building; malformed or corrupted files are
+ * ILG_EINVAL. */
+int ilg_save(ilg_ctx *ctx, const char *path);
+int ilg_load(ilg_ctx *ctx, const char *path);
+
 /* Closest hit. Rays: ray_o_tmin = N x (ox, oy, oz, tmin), ray_d_tmax =
  * N x (dx, dy, dz, tmax), both float4-aligned. Hits: prim[i] = triangle index
  * (-1 on a miss), t[i] (+inf on a miss), u[i] = beta, v[i] = gamma, in the
