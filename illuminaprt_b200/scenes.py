@@ -263,6 +263,171 @@ def load_box_scene(space, scene=None):
     return scene
 
 
+def _g(x) -> str:
+    """A float32 in the shortest text that reads back to the same value."""
+    return np.format_float_positional(np.float32(x), trim="-")
+
+
+def write_box_script(directory, scene=None, width: int = 64, height: int = 64, spp: int = 16,
+                     space: str = "GPU", renderer: str = "GPU", seed: int = 1, container: str = "BVHMesh") -> str:
+    """Write the box scene as files the reference's own scene loader reads and
+    return the script's path: ``box.obj`` + ``box.mtl`` (every non-light
+    triangle, one MTL material per primitive with Kd = its albedo, a flat
+    per-face normal), and ``box.ilm``, an environment script
+    (Core/Scene/EnvironmentLoader.cpp:150-921 syntax: ``Name = value`` lines
+    and ``Name {`` ... ``}`` blocks) that loads the OBJ as a WavefrontModel
+    into one mesh with a MaterialGroup, adds the light as a Quad shape with a
+    DiffuseArea light and an Emissive primitive, and names the space and
+    renderer factories (``"GPU"`` for the plug-in's, ``"Basic"`` for the
+    reference's), a PathTracing integrator with the scene's depth and
+    epsilon, a Random sampler, a Box filter and a ``Memory`` device of
+    width x height."""
+    import os
+    scene = scene or box_scene()
+    directory = os.path.abspath(str(directory))
+    os.makedirs(directory, exist_ok=True)
+    obj, mtl, ilm = (os.path.join(directory, n) for n in ("box.obj", "box.mtl", "box.ilm"))
+    light = scene["light_prim"]
+    with open(mtl, "w") as f:
+        for p, a in enumerate(scene["albedo"]):
+            if p != light:
+                f.write(f"newmtl prim{p}\nKd {_g(a[0])} {_g(a[1])} {_g(a[2])}\n\n")
+    pos = scene["pos"].reshape(-1, 3, 3).astype(np.float32)
+    with open(obj, "w") as f:
+        f.write("mtllib box.mtl\n")
+        current, nv = None, 0
+        for t, p in enumerate(scene["prim_of_tri"]):
+            if p == light:
+                continue
+            v = pos[t].astype(np.float64)
+            n = np.cross(v[1] - v[0], v[2] - v[0])
+            n /= np.linalg.norm(n)
+            for c in range(3):
+                f.write(f"v {_g(v[c, 0])} {_g(v[c, 1])} {_g(v[c, 2])}\n")
+            f.write(f"vn {_g(n[0])} {_g(n[1])} {_g(n[2])}\n")
+            if p != current:
+                f.write(f"usemtl prim{p}\n")
+                current = p
+            k = nv // 3 + 1  # this triangle's vn
+            f.write(f"f {nv + 1}//{k} {nv + 2}//{k} {nv + 3}//{k}\n")
+            nv += 3
+    q, e, cam = scene["light_quad"], scene["light_emit"], scene["camera"]
+    alb = scene["albedo"][light]
+    vec = lambda v: "{" + ",".join(_g(x) for x in v) + "}"
+    script = f"""# box scene: walls, two boxes and a ceiling quad light
+Shapes {{
+\tShape {{
+\t\tId = box_mesh
+\t\tType = WavefrontModel
+\t\tFilename = {obj}
+\t\tContainer = {container}
+\t\tMaterialGroupId = box_materials
+\t}}
+\tShape {{
+\t\tId = light_quad
+\t\tType = Quad
+\t\tVertices = {{{",".join(vec(v) for v in q)}}}
+\t}}
+}}
+Materials {{
+\tMaterial {{
+\t\tId = light_material
+\t\tType = Matte
+\t\tReflectivity = {vec(alb)}
+\t}}
+}}
+Lights {{
+\tLight {{
+\t\tId = ceiling_light
+\t\tType = DiffuseArea
+\t\tPower = {vec(e)}
+\t\tShape = light_quad
+\t}}
+}}
+Cameras {{
+\tCamera {{
+\t\tId = camera
+\t\tType = Perspective
+\t\tPosition = {vec(cam["eye"])}
+\t\tTarget = {vec(cam["target"])}
+\t\tUp = {vec(cam["up"])}
+\t\tFov = {_g(cam["fov"])}
+\t\tAspect = {_g(cam["aspect"])}
+\t}}
+}}
+Filters {{
+\tFilter {{
+\t\tId = filter
+\t\tType = Box
+\t}}
+}}
+Samplers {{
+\tSampler {{
+\t\tId = sampler
+\t\tType = Random
+\t}}
+}}
+Devices {{
+\tDevice {{
+\t\tId = device
+\t\tType = Memory
+\t\tWidth = {int(width)}
+\t\tHeight = {int(height)}
+\t}}
+}}
+Integrators {{
+\tIntegrator {{
+\t\tId = integrator
+\t\tType = PathTracing
+\t\tRayDepth = {int(scene["max_depth"])}
+\t\tShadowRays = 1
+\t\tEpsilon = {_g(scene["epsilon"])}
+\t}}
+}}
+Renderers {{
+\tRenderer {{
+\t\tId = renderer
+\t\tType = {renderer}
+\t\tSamples = {int(spp)}
+\t\tSeed = {int(seed)}
+\t\tIntegrator = integrator
+\t\tFilter = filter
+\t\tDevice = device
+\t}}
+}}
+Environment {{
+\tRenderer = renderer
+\tScene {{
+\t\tSampler = sampler
+\t\tCamera = camera
+\t\tLights = {{ceiling_light}}
+\t\tSpace {{
+\t\t\tId = space
+\t\t\tType = {space}
+\t\t\tPrimitives {{
+\t\t\t\tPrimitive {{
+\t\t\t\t\tId = box
+\t\t\t\t\tType = Geometry
+\t\t\t\t\tMaterial = box_materials
+\t\t\t\t\tShape = box_mesh
+\t\t\t\t}}
+\t\t\t\tPrimitive {{
+\t\t\t\t\tId = light
+\t\t\t\t\tType = Emissive
+\t\t\t\t\tMaterial = light_material
+\t\t\t\t\tShape = light_quad
+\t\t\t\t\tLight = ceiling_light
+\t\t\t\t}}
+\t\t\t}}
+\t\t}}
+\t}}
+}}
+"""
+    with open(ilm, "w") as f:
+        f.write(script)
+    return ilm
+
+
 # ---------------------------------------------------------------------------
 # Icosphere field (the at-scale path-tracing scene)
 # ---------------------------------------------------------------------------

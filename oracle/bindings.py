@@ -173,6 +173,8 @@ class RefLib:
         L.ilref_render_box_renderer.argtypes = ([c.c_char_p, c.c_char_p] + list(L.ilref_render_box.argtypes[:17])
                                                 + [c.c_float, c.c_int, _f32p, _f32p, _f32p, c.c_char_p, c.c_int])
         L.ilref_postprocess.argtypes = [c.c_int, _f32p, c.c_int, c.c_int, c.c_int, _f32p]
+        L.ilref_render_script.argtypes = [c.c_char_p, c.c_char_p, c.c_int, c.c_int, c.c_int, _f32p, _f32p, _f32p,
+                                          c.c_char_p, c.c_int, c.c_char_p, c.c_int]
         L.ilref_compare_spaces.argtypes = [c.c_char_p, c.c_char_p, _f32p, _i32p, c.c_int, c.c_int, _f32p, c.c_int,
                                            _f32p, _f32p, _f32p, _f32p, c.c_long, c.c_void_p, _u8p, _f32p,
                                            c.c_void_p, _u8p, _u8p, _f32p, _u8p, c.c_char_p, c.c_int]
@@ -243,6 +245,21 @@ class RefLib:
         if rc:
             raise RuntimeError(f"ilref_render_box_renderer: {rc}: {err.value.decode(errors='replace')}")
         return tuple(outs)
+
+    def render_script(self, script: str, width: int, height: int, plugin: str | None = None, tile: int = 0):
+        """A scene script loaded by the reference's Environment::Load and
+        rendered by the renderer it names (see ilref_render_script); with
+        `plugin`, the plug-in's factories are registered first. Returns
+        (final, direct, albedo, info); raises RuntimeError with the loader's
+        or renderer's reason."""
+        outs = [np.zeros((height, width, 3), np.float32) for _ in range(3)]
+        info = ctypes.create_string_buffer(256)
+        err = ctypes.create_string_buffer(1024)
+        rc = self.L.ilref_render_script((plugin or "").encode(), str(script).encode(), width, height, tile,
+                                        *(o.reshape(-1) for o in outs), info, 256, err, 1024)
+        if rc:
+            raise RuntimeError(f"ilref_render_script: {rc}: {err.value.decode(errors='replace')}")
+        return (*outs, info.value.decode())
 
     def postprocess(self, op: str, frames):
         """The reference's post-process on float32 images: op 'accumulate'

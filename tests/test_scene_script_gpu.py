@@ -1,0 +1,72 @@
+"""Scene import onto the device: a scene script loaded by the reference's own
+loader (Environment::Load -> EnvironmentLoader -> WavefrontSceneLoader,
+Core/Scene/*.cpp) with the plug-in's "GPU" space and renderer factories
+registered, so the OBJ mesh (one primitive with a MaterialGroup), the Quad
+light and the camera all arrive through the engine's objects."""
+from __future__ import annotations
+
+import os
+
+import numpy as np
+import pytest
+
+from illuminaprt_b200 import build as pkg_build
+from illuminaprt_b200 import scenes
+from oracle import bindings
+from tests.test_scene_script import GOLDEN, rel_mse
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not (os.path.exists(pkg_build.PLUGIN) and bindings.ref_available()),
+                                 reason="plug-in or reference engine library not built")]
+
+
+def test_script_scene_on_the_gpu_renderer_matches_the_reference_image(tmp_path):
+    script = scenes.write_box_script(tmp_path, width=256, height=256, spp=1024)
+    final, direct, albedo, info = bindings.RefLib().render_script(script, 256, 256, plugin=pkg_build.PLUGIN)
+    assert "space=GpuSpace" in info and "renderer=GpuRenderer" in info, info
+    ref_img = np.load(GOLDEN)["image"]
+    err = rel_mse(final, ref_img)
+    print(f"relMSE(script scene on GpuRenderer 1024 spp, reference 4096 spp) = {err:.2e}")
+    assert np.isfinite(final).all()
+    assert err < 1e-3
+    assert np.allclose(final.mean((0, 1)), ref_img.mean((0, 1)), rtol=1e-2)
+    assert (direct <= final + 1e-4).all() and albedo.mean() > 0.2
+
+
+def test_reference_renderer_over_the_loaded_gpu_space_matches_basic_space(tmp_path):
+    # BasicRenderer + PathIntegrator with the scene's fixed-seed sampler: the
+    # same sample sequence over either space, so paths differ only where a
+    # near tie picks the other of two coincident surfaces
+    w, spp = 32, 2
+    ref = bindings.RefLib()
+    basic = ref.render_script(scenes.write_box_script(tmp_path / "basic", width=w, height=w, spp=spp, space="Basic",
+                                                      renderer="Basic"), w, w)
+    gpu = ref.render_script(scenes.write_box_script(tmp_path / "gpu", width=w, height=w, spp=spp, space="GPU",
+                                                    renderer="Basic"), w, w, plugin=pkg_build.PLUGIN)
+    assert "space=GpuSpace" in gpu[3], gpu[3]
+    same = np.all(basic[0] == gpu[0], axis=2)
+    assert same.mean() >= 0.98, f"{int((~same).sum())} of {same.size} pixels differ"
+
+
+@pytest.mark.parametrize("container", ["KDTreeMesh", "BasicMesh"])
+def test_every_mesh_container_gives_the_same_device_image(tmp_path, container):
+    # GpuSpace flattens any ITriangleMesh in its triangle order, so the device
+    # scene, and with the counter-based samples the image, do not depend on
+    # the container the script chose
+    w, spp = 48, 8
+    ref = bindings.RefLib()
+    a = ref.render_script(scenes.write_box_script(tmp_path / "bvh", width=w, height=w, spp=spp), w, w,
+                          plugin=pkg_build.PLUGIN)
+    b = ref.render_script(scenes.write_box_script(tmp_path / container, width=w, height=w, spp=spp,
+                                                  container=container), w, w, plugin=pkg_build.PLUGIN)
+    for x, y in zip(a[:3], b[:3]):  # float atomics may sum a pixel's samples in another order
+        assert np.allclose(x, y, rtol=1e-5, atol=1e-6)
+
+
+def test_script_scene_regions_tile_the_frame(tmp_path):
+    script = scenes.write_box_script(tmp_path, width=100, height=72, spp=4)
+    ref = bindings.RefLib()
+    whole = ref.render_script(script, 100, 72, plugin=pkg_build.PLUGIN)
+    tiled = ref.render_script(script, 100, 72, plugin=pkg_build.PLUGIN, tile=32)
+    for a, b in zip(whole[:3], tiled[:3]):
+        assert np.allclose(a, b, rtol=1e-5, atol=1e-6)
