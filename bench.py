@@ -277,6 +277,43 @@ def bench_cache(res, local):
         "bias_cached": [round(b, 5) for b in r["bias_cached"]], "seconds": round(r["seconds_cached"], 4),
         "frames_cached": r["frames_cached"], "frames_plain": r["frames_plain"]}
     sp.close()
+    try:
+        res["cache_equal_time"]["cpu_baseline"] = ic_cpu_baseline()
+    except (FileNotFoundError, OSError, RuntimeError) as e:
+        res["cache_equal_time"]["cpu_baseline"] = {"unavailable": str(e)[:200]}
+
+
+def ic_cpu_baseline(width=64, ic_spp=16):
+    """The reference's own caching method as the baseline of the cache leg:
+    its irradiance-cache integrator (Core/Integrator/ICIntegrator.cpp, factory
+    defaults) against its PathIntegrator at equal CPU time, both driven by
+    its BasicRenderer over BasicSpace from a scene script (the box scene at
+    64x64; error against the reference's 4096-spp image of the same scene).
+    The reference renders on one thread."""
+    import tempfile
+
+    from illuminaprt_b200 import scenes
+    from oracle import bindings
+    from tests.test_scene_script import GOLDEN, coarse_expectation, rel_mse
+    ref = bindings.RefLib()
+    expected = coarse_expectation(np.load(GOLDEN)["image"], width)
+    with tempfile.TemporaryDirectory() as tmp:
+        def run(integrator, spp):
+            script = scenes.write_box_script(os.path.join(tmp, f"{integrator}{spp}"), width=width, height=width,
+                                             spp=spp, space="Basic", renderer="Basic", integrator=integrator)
+            t0 = time.perf_counter()
+            img = ref.render_script(script, width, width)[0]
+            return img, time.perf_counter() - t0
+        ic, t_ic = run("IC", ic_spp)
+        _, t_pt4 = run("PathTracing", 4)
+        pt_spp = max(1, int(round(4 * t_ic / t_pt4)))
+        pt, t_pt = run("PathTracing", pt_spp)
+    e_ic, e_pt = rel_mse(ic, expected), rel_mse(pt, expected)
+    bias = (ic.mean((0, 1)) / expected.mean((0, 1)) - 1.0).tolist()
+    return {"kind": "reference", "cores": 1, "gain": round(e_pt / e_ic, 3), "relmse_ic": round(e_ic, 5),
+            "relmse_plain": round(e_pt, 5), "bias_ic": [round(b, 4) for b in bias],
+            "sample": f"box scene {width}x{width}: ICIntegrator {ic_spp} spp in {t_ic:.2f} s vs PathIntegrator "
+                      f"{pt_spp} spp in {t_pt:.2f} s, one thread"}
 
 
 def pt_bytes_per_sample(counts, samples):

@@ -901,10 +901,10 @@ namespace {
 
 // One scene, one region: the body of ilg_render and ilg_render_region.
 int render_one(ilg_ctx *ctx, const ilg_camera_frame &frame, const ilg_render_opts *opts, const ilg_region &reg,
-               float *final_rgb, float *direct_rgb, float *albedo_rgb, uint32_t flags, bool use_cache)
+               float *final_rgb, float *direct_rgb, float *albedo_rgb, uint32_t flags)
 {
     ctx->counted = (flags & ILG_RENDER_COUNT) != 0;
-    const uint32_t cache_depth = use_cache ? opts->cache_depth : 0u;
+    const uint32_t cache_depth = opts->cache_depth;
     if (cache_depth) {
         if (!ctx->mlp_ready) return fail(ctx, ILG_ESTATE, "ilg_render: cache_depth set but ilg_mlp_init not called");
         if (cache_depth >= opts->max_depth)
@@ -959,7 +959,7 @@ int ilg_render(ilg_ctx *ctx, const ilg_camera *cam, const ilg_render_opts *opts,
     ilg_camera_frame frame;
     camera_frame_of(*cam, frame);
     const ilg_region whole = {0u, 0u, opts->width, opts->height};
-    return render_one(ctx, frame, opts, whole, out_rgb, nullptr, nullptr, flags, true);
+    return render_one(ctx, frame, opts, whole, out_rgb, nullptr, nullptr, flags);
 }
 
 int ilg_render_counts(ilg_ctx *ctx, uint64_t counts[6])
@@ -979,7 +979,7 @@ int ilg_render_region(ilg_ctx *ctx, const ilg_camera_frame *frame, const ilg_ren
     if (!ctx) return ILG_EINVAL;
     if (!frame || !opts || !region || !final_rgb) return fail(ctx, ILG_EINVAL, "ilg_render_region: null argument");
     if (flags & ~ILG_DEVICE_PTRS) return fail(ctx, ILG_EINVAL, "ilg_render_region: unknown flags 0x%x", flags);
-    return render_one(ctx, *frame, opts, *region, final_rgb, direct_rgb, albedo_rgb, flags, false);
+    return render_one(ctx, *frame, opts, *region, final_rgb, direct_rgb, albedo_rgb, flags);
 }
 
 int ilg_render_batch(ilg_ctx *runner, const ilg_batch_item *items, uint32_t n, uint32_t paths_per_wave,

@@ -319,11 +319,15 @@ class GpuSpace:
         return f
 
     def render_region(self, frame: ilg_camera_frame, width: int, height: int, spp: int, region, max_depth: int = 6,
-                      epsilon: float = 1e-4, seed: int = 1, sky=(0.0, 0.0, 0.0), aux: bool = True):
+                      epsilon: float = 1e-4, seed: int = 1, sky=(0.0, 0.0, 0.0), aux: bool = True,
+                      cache_depth: int = 0, train_every: int = 16, train_steps: int = 4, train_batch: int = 16384):
         """IRenderer::RenderRegion: region = (x, y, w, h) of the width x height image.
-        Returns (final, direct, albedo), each (h, w, 3) float32 (direct/albedo None without aux)."""
+        Returns (final, direct, albedo), each (h, w, 3) float32 (direct/albedo None without aux).
+        cache_depth > 0 renders with the radiance cache as render() does."""
         x, y, w, h = (int(v) for v in region)
-        o = ilg_render_opts(width=width, height=height, spp=spp, max_depth=max_depth, epsilon=epsilon, seed=seed)
+        o = ilg_render_opts(width=width, height=height, spp=spp, max_depth=max_depth, epsilon=epsilon, seed=seed,
+                            cache_depth=cache_depth, train_every=train_every, train_steps=train_steps,
+                            train_batch=train_batch)
         o.sky[:] = list(sky)
         r = ilg_region(x=x, y=y, width=w, height=h)
         final = np.empty((h, w, 3), np.float32)

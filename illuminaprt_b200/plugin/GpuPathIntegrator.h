@@ -1,0 +1,58 @@
+// GpuPathIntegrator: the reference's PathIntegrator
+// (Core/Integrator/PathIntegrator.h:19-50) with the settings of the device
+// renderer's learned radiance cache attached. It is what a scene script's
+// Integrator { Type = GPU ... } makes (factory "GPU" in the IntegratorManager,
+// registered by the plug-in).
+//
+// Under the reference's own renderers it IS the reference's PathIntegrator:
+// Radiance() is inherited unchanged, so a BasicRenderer over it renders
+// exactly as over Type = PathTracing. Under GpuRenderer its RayDepth and
+// Epsilon drive the device path tracer as a PathIntegrator's do, and with
+// Cache = MLP rendering paths stop into the radiance cache at their
+// CacheDepth-th bounce vertex while one path in 1 / TrainFraction is traced
+// to full depth to train it (TrainSteps Adam steps of TrainBatch records,
+// at LearningRate, after every rendered region). The reference has no such
+// cache; its nearest relative is the irradiance cache of
+// Core/Integrator/ICIntegrator.*.
+#pragma once
+
+#include <cstdint>
+#include <string>
+
+#include "Integrator/PathIntegrator.h"
+
+namespace Illumina {
+namespace PlugIn {
+
+struct RadianceCacheSettings {
+    bool enabled;
+    uint32_t depth;         // bounce vertex where rendering paths stop into the cache (>= 1)
+    uint32_t train_every;   // one training path in this many
+    uint32_t train_steps;   // Adam steps after each rendered region (0 = frozen)
+    uint32_t train_batch;   // records per step
+    float learning_rate;
+    uint32_t seed;          // network initialisation
+
+    RadianceCacheSettings(void)
+        : enabled(false), depth(1), train_every(16), train_steps(4), train_batch(16384), learning_rate(1e-2f),
+          seed(1)
+    {
+    }
+};
+
+class GpuPathIntegrator : public Illumina::Core::PathIntegrator {
+public:
+    GpuPathIntegrator(const std::string &p_strName, int p_nMaxRayDepth, int p_nShadowSampleCount,
+                      float p_fReflectEpsilon, const RadianceCacheSettings &p_cache);
+    GpuPathIntegrator(int p_nMaxRayDepth, int p_nShadowSampleCount, float p_fReflectEpsilon,
+                      const RadianceCacheSettings &p_cache);
+
+    const RadianceCacheSettings &GetCacheSettings(void) const { return m_cache; }
+    std::string ToString(void) const { return "GpuPathIntegrator"; }
+
+private:
+    RadianceCacheSettings m_cache;
+};
+
+}  // namespace PlugIn
+}  // namespace Illumina

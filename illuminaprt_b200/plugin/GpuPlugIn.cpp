@@ -9,11 +9,23 @@
 // GetPlugInSingleton, DisposePlugInSingleton, CreatePlugInInstance,
 // GetPlugInInstance, DisposePlugInInstance, DisposePlugInInstances.
 //
+// Factory "GPU" in its IntegratorManager makes a GpuPathIntegrator, a
+// PathIntegrator that also carries the settings of the device renderer's
+// radiance cache.
+//
 // Factory arguments (ArgumentMap). Space: Id (instance name), Device (CUDA
 // ordinal, default 0). Renderer: Id, Samples (per pixel, default 1, as
 // BasicRendererFactory, Renderer/RendererFactories.h:34-44), Seed (default 1).
+// Integrator: Id, RayDepth (6), ShadowRays (1), Epsilon (1e-4), as the
+// reference's PathIntegratorFactory (Integrator/IntegratorFactories.h:41-58);
+// Cache (None or MLP, default None), CacheDepth (1), TrainFraction (1/16),
+// TrainSteps (4), TrainBatch (16384), LearningRate (0.01), CacheSeed (1).
+// Bad values throw the engine's Exception, as its factories do.
+#include <cmath>
 #include <string>
 
+#include "Exception/Exception.h"
+#include "GpuPathIntegrator.h"
 #include "GpuRenderer.h"
 #include "GpuSpace.h"
 #include "System/ArgumentMap.h"
@@ -57,13 +69,60 @@ public:
     }
 };
 
+class GpuPathIntegratorFactory : public Factory<IIntegrator> {
+public:
+    IIntegrator *CreateInstance(void) { return new GpuPathIntegrator(6, 1, 1e-4f, RadianceCacheSettings()); }
+
+    IIntegrator *CreateInstance(ArgumentMap &p_argumentMap)
+    {
+        int depth = 6, shadow = 1, cache_depth = 1, steps = 4, batch = 16384, seed = 1;
+        float epsilon = 1e-4f, fraction = 1.f / 16.f, lr = 1e-2f;
+        std::string id, cache = "None";
+        p_argumentMap.GetArgument("RayDepth", depth);
+        p_argumentMap.GetArgument("ShadowRays", shadow);
+        p_argumentMap.GetArgument("Epsilon", epsilon);
+        p_argumentMap.GetArgument("Cache", cache);
+        p_argumentMap.GetArgument("CacheDepth", cache_depth);
+        p_argumentMap.GetArgument("TrainFraction", fraction);
+        p_argumentMap.GetArgument("TrainSteps", steps);
+        p_argumentMap.GetArgument("TrainBatch", batch);
+        p_argumentMap.GetArgument("LearningRate", lr);
+        p_argumentMap.GetArgument("CacheSeed", seed);
+
+        RadianceCacheSettings c;
+        if (cache == "MLP")
+            c.enabled = true;
+        else if (cache != "None")
+            throw new Exception("GpuPathIntegratorFactory: Cache must be None or MLP, not '" + cache + "'");
+        if (c.enabled && (cache_depth < 1 || cache_depth >= depth))
+            throw new Exception("GpuPathIntegratorFactory: CacheDepth must be at least 1 and below RayDepth");
+        if (!(fraction > 0.f && fraction <= 1.f))
+            throw new Exception("GpuPathIntegratorFactory: TrainFraction must be in (0, 1]");
+        if (steps < 0 || batch < 1 || !(lr > 0.f))
+            throw new Exception("GpuPathIntegratorFactory: TrainSteps >= 0, TrainBatch >= 1, LearningRate > 0");
+        c.depth = (uint32_t)cache_depth;
+        c.train_every = (uint32_t)std::max(1.f, std::floor(1.f / fraction + 0.5f));
+        c.train_steps = (uint32_t)steps;
+        c.train_batch = (uint32_t)batch;
+        c.learning_rate = lr;
+        c.seed = (uint32_t)seed;
+        if (p_argumentMap.GetArgument("Id", id)) return new GpuPathIntegrator(id, depth, shadow, epsilon, c);
+        return new GpuPathIntegrator(depth, shadow, epsilon, c);
+    }
+};
+
 class GpuPlugIn : public IPlugIn {
 public:
-    GpuPlugIn(void) : m_strName("GPU Space"), m_version(1, 0, 0), m_pFactory(NULL), m_pRendererFactory(NULL) {}
+    GpuPlugIn(void)
+        : m_strName("GPU Space"), m_version(1, 0, 0), m_pFactory(NULL), m_pRendererFactory(NULL),
+          m_pIntegratorFactory(NULL)
+    {
+    }
     ~GpuPlugIn(void)
     {
         delete m_pFactory;
         delete m_pRendererFactory;
+        delete m_pIntegratorFactory;
     }
 
     const std::string &GetName(void) const { return m_strName; }
@@ -73,14 +132,17 @@ public:
     {
         if (!m_pFactory) m_pFactory = new GpuSpaceFactory();
         if (!m_pRendererFactory) m_pRendererFactory = new GpuRendererFactory();
+        if (!m_pIntegratorFactory) m_pIntegratorFactory = new GpuPathIntegratorFactory();
         p_pEngineKernel->GetSpaceManager()->RegisterFactory("GPU", m_pFactory);
         p_pEngineKernel->GetRendererManager()->RegisterFactory("GPU", m_pRendererFactory);
+        p_pEngineKernel->GetIntegratorManager()->RegisterFactory("GPU", m_pIntegratorFactory);
     }
 
     void Unregister(EngineKernel *p_pEngineKernel)
     {
         p_pEngineKernel->GetSpaceManager()->UnregisterFactory("GPU");
         p_pEngineKernel->GetRendererManager()->UnregisterFactory("GPU");
+        p_pEngineKernel->GetIntegratorManager()->UnregisterFactory("GPU");
     }
 
     void Initialise(void) {}
@@ -91,6 +153,7 @@ private:
     Version m_version;
     GpuSpaceFactory *m_pFactory;
     GpuRendererFactory *m_pRendererFactory;
+    GpuPathIntegratorFactory *m_pIntegratorFactory;
 };
 
 }  // namespace PlugIn

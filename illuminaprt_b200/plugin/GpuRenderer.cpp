@@ -10,6 +10,7 @@
 #include "EngineAccess.h"
 #include "Exception/Exception.h"
 #include "Geometry/Intersection.h"
+#include "GpuPathIntegrator.h"
 #include "GpuSpace.h"
 #include "Integrator/PathIntegrator.h"
 #include "Light/DiffuseAreaLight.h"
@@ -48,14 +49,14 @@ GpuRenderer::GpuRenderer(const std::string &p_strName, Scene *p_pScene, IIntegra
                          IDevice *p_pDevice, IFilter *p_pFilter, RadianceBuffer *p_pRadianceBuffer,
                          int p_nSampleCount, uint32_t p_nSeed)
     : BaseRenderer(p_strName, p_pScene, p_pIntegrator, p_pDevice, p_pFilter, p_pRadianceBuffer, p_nSampleCount),
-      m_nSeed(p_nSeed), m_pPreparedScene(NULL), m_nPreparedBuild(0)
+      m_nSeed(p_nSeed), m_pPreparedScene(NULL), m_nPreparedBuild(0), m_pCacheContext(NULL), m_nCacheBuild(0)
 {
 }
 
 GpuRenderer::GpuRenderer(Scene *p_pScene, IIntegrator *p_pIntegrator, IDevice *p_pDevice, IFilter *p_pFilter,
                          RadianceBuffer *p_pRadianceBuffer, int p_nSampleCount, uint32_t p_nSeed)
     : BaseRenderer(p_pScene, p_pIntegrator, p_pDevice, p_pFilter, p_pRadianceBuffer, p_nSampleCount),
-      m_nSeed(p_nSeed), m_pPreparedScene(NULL), m_nPreparedBuild(0)
+      m_nSeed(p_nSeed), m_pPreparedScene(NULL), m_nPreparedBuild(0), m_pCacheContext(NULL), m_nCacheBuild(0)
 {
 }
 
@@ -156,6 +157,21 @@ void GpuRenderer::RenderRegion(RadianceBuffer *p_pRadianceBuffer, int p_nRegionX
     opts.max_depth = (uint32_t)Access::PathTracer::MaxRayDepth(path);
     opts.epsilon = Access::PathTracer::ReflectEpsilon(path);
     opts.seed = m_nSeed;
+    const GpuPathIntegrator *gpu = dynamic_cast<const GpuPathIntegrator *>(path);
+    if (gpu && gpu->GetCacheSettings().enabled) {
+        const RadianceCacheSettings &c = gpu->GetCacheSettings();
+        if (c.depth < 1 || c.depth >= opts.max_depth) Refuse("the radiance cache depth must be in [1, RayDepth)");
+        // a fresh network for every built scene; it then learns across regions and frames
+        if (m_pCacheContext != ctx || m_nCacheBuild != space->GetBuildCount()) {
+            Check(ctx, ilg_mlp_init(ctx, c.seed, c.learning_rate), "ilg_mlp_init");
+            m_pCacheContext = ctx;
+            m_nCacheBuild = space->GetBuildCount();
+        }
+        opts.cache_depth = c.depth;
+        opts.train_every = c.train_every;
+        opts.train_steps = c.train_steps;
+        opts.train_batch = c.train_batch;
+    }
     ilg_region region = {(uint32_t)p_nRegionX, (uint32_t)p_nRegionY, (uint32_t)p_nRegionWidth,
                          (uint32_t)p_nRegionHeight};
     const size_t n = (size_t)p_nRegionWidth * p_nRegionHeight;

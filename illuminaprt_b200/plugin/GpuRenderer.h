@@ -12,7 +12,10 @@
 // Exception, never a CPU fallback):
 //   space       must be a GpuSpace (its device BVH and material slots)
 //   integrator  a PathIntegrator: its RayDepth and Epsilon are used; more
-//               than one shadow ray per light is refused
+//               than one shadow ray per light is refused. A
+//               GpuPathIntegrator with Cache = MLP also turns on the
+//               device's learned radiance cache (a fresh network for each
+//               built scene, trained after every region)
 //   materials   MatteMaterial without a texture (its reflectivity); a
 //               primitive without material renders black
 //   lights      DiffuseAreaLight on a Quad whose EmissivePrimitive is in
@@ -74,6 +77,8 @@ private:
     uint32_t m_nSeed;
     const void *m_pPreparedScene;
     uint64_t m_nPreparedBuild;
+    const ilg_ctx *m_pCacheContext;  // context whose radiance cache this renderer initialised
+    uint64_t m_nCacheBuild;
 };
 
 }  // namespace PlugIn

@@ -269,7 +269,8 @@ def _g(x) -> str:
 
 
 def write_box_script(directory, scene=None, width: int = 64, height: int = 64, spp: int = 16,
-                     space: str = "GPU", renderer: str = "GPU", seed: int = 1, container: str = "BVHMesh") -> str:
+                     space: str = "GPU", renderer: str = "GPU", seed: int = 1, container: str = "BVHMesh",
+                     integrator: str = "PathTracing", integrator_args: dict | None = None) -> str:
     """Write the box scene as files the reference's own scene loader reads and
     return the script's path: ``box.obj`` + ``box.mtl`` (every non-light
     triangle, one MTL material per primitive with Kd = its albedo, a flat
@@ -279,9 +280,10 @@ def write_box_script(directory, scene=None, width: int = 64, height: int = 64, s
     into one mesh with a MaterialGroup, adds the light as a Quad shape with a
     DiffuseArea light and an Emissive primitive, and names the space and
     renderer factories (``"GPU"`` for the plug-in's, ``"Basic"`` for the
-    reference's), a PathTracing integrator with the scene's depth and
-    epsilon, a Random sampler, a Box filter and a ``Memory`` device of
-    width x height."""
+    reference's), an integrator of type `integrator` (``"PathTracing"``, or
+    the plug-in's ``"GPU"``) with the scene's depth and epsilon plus
+    `integrator_args` (e.g. ``{"Cache": "MLP"}``), a Random sampler, a Box
+    filter and a ``Memory`` device of width x height."""
     import os
     scene = scene or box_scene()
     directory = os.path.abspath(str(directory))
@@ -314,6 +316,7 @@ def write_box_script(directory, scene=None, width: int = 64, height: int = 64, s
     q, e, cam = scene["light_quad"], scene["light_emit"], scene["camera"]
     alb = scene["albedo"][light]
     vec = lambda v: "{" + ",".join(_g(x) for x in v) + "}"
+    extra = "".join(f"\t\t{k} = {v}\n" for k, v in (integrator_args or {}).items())
     script = f"""# box scene: walls, two boxes and a ceiling quad light
 Shapes {{
 \tShape {{
@@ -378,11 +381,11 @@ Devices {{
 Integrators {{
 \tIntegrator {{
 \t\tId = integrator
-\t\tType = PathTracing
+\t\tType = {integrator}
 \t\tRayDepth = {int(scene["max_depth"])}
 \t\tShadowRays = 1
 \t\tEpsilon = {_g(scene["epsilon"])}
-\t}}
+{extra}\t}}
 }}
 Renderers {{
 \tRenderer {{

@@ -240,7 +240,10 @@ typedef struct ilg_region {
  * directly and its light samples; Indirect = Final - Direct); albedo_rgb
  * (optional) = RadianceContext::Albedo, the first hit's reflectance. All are
  * per-sample averages. Host pointers unless ILG_DEVICE_PTRS. The radiance
- * cache options of opts are not used here. */
+ * cache options of opts work as in ilg_render: the region's paths query the
+ * cache, its training paths train it after the call (with train_steps 0 a
+ * frozen cache, and regions still tile the image exactly); Direct and Albedo
+ * come from the first vertex, before any cache query. */
 int ilg_render_region(ilg_ctx *ctx, const ilg_camera_frame *frame, const ilg_render_opts *opts,
                       const ilg_region *region, float *final_rgb, float *direct_rgb, float *albedo_rgb,
                       uint32_t flags);

@@ -21,12 +21,15 @@
 // Filter/FilterFactories.h, Sampler/SamplerFactories.h,
 // Material/MaterialFactories.h, Renderer/RendererFactories.h), registered
 // under the names the Sandbox gives them (Utility/Sandbox/Environment.h:
-// 77-189), with two exceptions written here:
+// 77-189), with three exceptions written here:
 //   "PathTracing"  Integrator/IntegratorFactories.h does not compile with a
 //                  current compiler (Integrator/IntegratorHelper.h:285, :444),
 //                  so this file has a factory with the same arguments and
 //                  defaults (RayDepth 6, ShadowRays 1, Epsilon 1e-4) making
 //                  the same PathIntegrator (IntegratorFactories.h:26-69).
+//   "IC"           likewise for the irradiance-cache integrator: the same
+//                  arguments and defaults (IntegratorFactories.h:160-205)
+//                  making the reference's ICIntegrator.
 //   "Memory"       an IDevice that only has a size (Width, Height): the
 //                  reference's devices write image files or displays.
 // A plug-in library, when given, is loaded and registered with the kernel's
@@ -47,6 +50,7 @@
 #include "Device/Device.h"
 #include "Exception/Exception.h"
 #include "Filter/FilterFactories.h"
+#include "Integrator/ICIntegrator.h"
 #include "Integrator/PathIntegrator.h"
 #include "Light/LightFactories.h"
 #include "Material/MaterialFactories.h"
@@ -87,6 +91,32 @@ public:
 		p_argumentMap.GetArgument("Epsilon", epsilon);
 		if (p_argumentMap.GetArgument("Id", id)) return new PathIntegrator(id, depth, shadow, epsilon);
 		return new PathIntegrator(depth, shadow, epsilon);
+	}
+};
+
+class ScriptICIntegratorFactory : public Factory<IIntegrator>
+{
+public:
+	IIntegrator *CreateInstance(void) { throw new Exception("Method not supported!"); }
+
+	IIntegrator *CreateInstance(ArgumentMap &p_argumentMap)
+	{
+		int depth = 6, cache_depth = 16, azimuth = 12, altitude = 4, shadow = 1;
+		float error = 1.f, resolution = 1e-3f, multiplier = 1e+3f, epsilon = 1e-4f;
+		std::string id;
+		p_argumentMap.GetArgument("CacheDepth", cache_depth);
+		p_argumentMap.GetArgument("ErrorThreshold", error);
+		p_argumentMap.GetArgument("AzimuthStrata", azimuth);
+		p_argumentMap.GetArgument("AltitudeStrata", altitude);
+		p_argumentMap.GetArgument("AmbientResolution", resolution);
+		p_argumentMap.GetArgument("AmbientMultiplier", multiplier);
+		p_argumentMap.GetArgument("RayDepth", depth);
+		p_argumentMap.GetArgument("ShadowRays", shadow);
+		p_argumentMap.GetArgument("Epsilon", epsilon);
+		if (p_argumentMap.GetArgument("Id", id))
+			return new ICIntegrator(id, cache_depth, error, resolution, multiplier, azimuth, altitude, depth, shadow,
+			                        epsilon);
+		return new ICIntegrator(cache_depth, error, resolution, multiplier, azimuth, altitude, depth, shadow, epsilon);
 	}
 };
 
@@ -135,6 +165,7 @@ void register_factories(EngineKernel *k)
 	k->GetFilterManager()->RegisterFactory("Box", new BoxFilterFactory());
 	k->GetSpaceManager()->RegisterFactory("Basic", new BasicSpaceFactory());
 	k->GetIntegratorManager()->RegisterFactory("PathTracing", new ScriptPathIntegratorFactory());
+	k->GetIntegratorManager()->RegisterFactory("IC", new ScriptICIntegratorFactory());
 	k->GetRendererManager()->RegisterFactory("Basic", new BasicRendererFactory());
 	k->GetDeviceManager()->RegisterFactory("Memory", new ScriptDeviceFactory());
 	k->GetCameraManager()->RegisterFactory("Perspective", new PerspectiveCameraFactory());

@@ -44,6 +44,34 @@ def test_cache_trains_online(field):
     assert errs[1] < errs[0]
 
 
+def test_cache_in_regions(field):
+    # a frozen cache (train_steps 0): region calls query the same network, so
+    # tiles reproduce the whole image's paths; the whole image as one region
+    # equals ilg_render's cached image; Direct does not depend on the cache
+    sp, s, _ = field
+    sp.mlp_init(seed=3, lr=1e-2)
+    cam = dict(s["camera"], aspect=W / H)
+    frame = sp.camera_frame(cam, W, H)
+    kw = dict(max_depth=12, seed=9, sky=s["sky"])
+    whole = sp.render(cam, W, H, 8, cache_depth=1, train_steps=0, **kw)
+    one, direct, _ = sp.render_region(frame, W, H, 8, (0, 0, W, H), cache_depth=1, train_steps=0, **kw)
+    assert np.allclose(one, whole, rtol=1e-5, atol=1e-6)
+    tiled = np.zeros_like(whole)
+    for y in range(0, H, 40):
+        for x in range(0, W, 64):
+            w, h = min(64, W - x), min(40, H - y)
+            tiled[y:y + h, x:x + w] = sp.render_region(frame, W, H, 8, (x, y, w, h), cache_depth=1, train_steps=0,
+                                                       aux=False, **kw)[0]
+    assert np.allclose(tiled, whole, rtol=1e-5, atol=1e-6)
+    plain, plain_direct, _ = sp.render_region(frame, W, H, 8, (0, 0, W, H), **kw)
+    assert not np.allclose(one, plain, rtol=1e-3, atol=1e-4)  # the cache answered the tails
+    assert np.allclose(direct, plain_direct, rtol=1e-5, atol=1e-6)
+    # training after a region call changes the next call's image
+    sp.render_region(frame, W, H, 1, (0, 0, W, H), cache_depth=1, train_steps=4, aux=False, **kw)
+    after = sp.render_region(frame, W, H, 8, (0, 0, W, H), cache_depth=1, train_steps=0, **kw)[0]
+    assert not np.allclose(after, one, rtol=1e-4, atol=1e-5)
+
+
 def test_equal_time_gain_over_plain_at_scale():
     """The full 64-icosphere field (20,971,530 triangles) at 960 x 540: the
     cached path tracer against plain path tracing at equal wall time."""

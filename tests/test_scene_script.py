@@ -110,3 +110,32 @@ def test_script_naming_the_gpu_space_fails_loudly_without_a_gpu(tmp_path):
     script = scenes.write_box_script(tmp_path, width=16, height=16, spp=1)
     with pytest.raises(RuntimeError, match="GpuRenderer"):
         bindings.RefLib().render_script(script, 16, 16, plugin=pkg_build.PLUGIN)
+
+
+@needs_ref
+@pytest.mark.skipif(not os.path.exists(pkg_build.PLUGIN), reason="plug-in not built")
+def test_gpu_integrator_is_the_reference_path_integrator_under_cpu_renderers(tmp_path):
+    # Integrator { Type = GPU } makes a GpuPathIntegrator; under the
+    # reference's BasicRenderer over BasicSpace it is the reference's
+    # PathIntegrator (same fixed-seed sampler): the same image, bit for bit
+    w, spp = 24, 4
+    ref = bindings.RefLib()
+    a = ref.render_script(scenes.write_box_script(tmp_path / "pt", width=w, height=w, spp=spp, space="Basic",
+                                                  renderer="Basic"), w, w, plugin=pkg_build.PLUGIN)[0]
+    b = ref.render_script(scenes.write_box_script(tmp_path / "gpu", width=w, height=w, spp=spp, space="Basic",
+                                                  renderer="Basic", integrator="GPU",
+                                                  integrator_args={"Cache": "MLP", "TrainFraction": 0.125}),
+                          w, w, plugin=pkg_build.PLUGIN)[0]
+    assert np.array_equal(a, b)
+
+
+@needs_ref
+@pytest.mark.skipif(not os.path.exists(pkg_build.PLUGIN), reason="plug-in not built")
+@pytest.mark.parametrize("args", [{"Cache": "Octree"}, {"Cache": "MLP", "CacheDepth": 6},
+                                  {"TrainFraction": 0}, {"LearningRate": -1}])
+def test_gpu_integrator_factory_refuses_bad_settings(tmp_path, args):
+    # the factory throws; the loader reports it and binds no integrator
+    script = scenes.write_box_script(tmp_path, width=16, height=16, spp=1, space="Basic", renderer="Basic",
+                                     integrator="GPU", integrator_args=args)
+    with pytest.raises(RuntimeError, match="integrator"):
+        bindings.RefLib().render_script(script, 16, 16, plugin=pkg_build.PLUGIN)

@@ -13,7 +13,7 @@ import pytest
 from illuminaprt_b200 import build as pkg_build
 from illuminaprt_b200 import scenes
 from oracle import bindings
-from tests.test_scene_script import GOLDEN, rel_mse
+from tests.test_scene_script import GOLDEN, coarse_expectation, rel_mse
 
 pytestmark = [pytest.mark.gpu,
               pytest.mark.skipif(not (os.path.exists(pkg_build.PLUGIN) and bindings.ref_available()),
@@ -70,3 +70,29 @@ def test_script_scene_regions_tile_the_frame(tmp_path):
     tiled = ref.render_script(script, 100, 72, plugin=pkg_build.PLUGIN, tile=32)
     for a, b in zip(whole[:3], tiled[:3]):
         assert np.allclose(a, b, rtol=1e-5, atol=1e-6)
+
+
+def test_gpu_integrator_with_the_radiance_cache(tmp_path):
+    # Integrator { Type = GPU  Cache = MLP }: the device renderer stops paths
+    # into the learned cache at their first bounce vertex and trains it after
+    # every region; the image stays near the reference's and differs from the
+    # uncached render of the same samples
+    ref = bindings.RefLib()
+    w, spp = 128, 64
+    cached = ref.render_script(scenes.write_box_script(tmp_path / "mlp", width=w, height=w, spp=spp, integrator="GPU",
+                                                       integrator_args={"Cache": "MLP", "CacheDepth": 1,
+                                                                        "TrainSteps": 8}),
+                               w, w, plugin=pkg_build.PLUGIN, tile=32)
+    plain = ref.render_script(scenes.write_box_script(tmp_path / "pt", width=w, height=w, spp=spp, integrator="GPU"),
+                              w, w, plugin=pkg_build.PLUGIN, tile=32)
+    assert "GpuRenderer" in cached[3]
+    assert np.isfinite(cached[0]).all()
+    assert not np.allclose(cached[0], plain[0], rtol=1e-3, atol=1e-4)
+    # Direct and Albedo come from the first vertex, before the cache
+    assert np.allclose(cached[1], plain[1], rtol=1e-5, atol=1e-6)
+    assert np.allclose(cached[2], plain[2], rtol=1e-5, atol=1e-6)
+    expected = coarse_expectation(np.load(GOLDEN)["image"], w)
+    e_cached, e_plain = rel_mse(cached[0], expected), rel_mse(plain[0], expected)
+    print(f"relMSE at {spp} spp: cached {e_cached:.2e}, plain {e_plain:.2e}")
+    assert e_cached < 0.1
+    assert np.allclose(cached[0].mean((0, 1)), expected.mean((0, 1)), rtol=0.15)
