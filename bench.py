@@ -173,9 +173,14 @@ def run_reference(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
-def cpu_baseline_sample(pos, idx, co, cd, io, idr, seconds=10.0):
+def cpu_baseline_sample(pos, idx, co, cd, io, idr, seconds=10.0, gpu_out=None):
     """The reference's CPU path on a bounded random sample (about `seconds` of
-    work on all host cores), for the cpu_baseline key."""
+    work on all host cores), for the cpu_baseline key. With gpu_out (the
+    device results of both ray sets), the sample's reference answers are
+    also compared ray by ray with the device's: hit ids must agree except at
+    near ties (two valid hits of the reference's test less than 1e-5 apart,
+    which the reference decides by visit order), and agreeing hits must agree
+    bit for bit in t, u and v."""
     from oracle import bindings
     nthreads = os.cpu_count() or 1
     try:
@@ -196,12 +201,24 @@ def cpu_baseline_sample(pos, idx, co, cd, io, idr, seconds=10.0):
     pick = rng.choice(co.shape[0], half, replace=False)
     oc, dc, oi, di = co[pick], cd[pick], io[pick], idr[pick]
     t0 = time.perf_counter()
-    tracer(oc, dc)
-    tracer(oi, di)
+    rc = tracer(oc, dc)
+    ri = tracer(oi, di)
     dt = time.perf_counter() - t0
-    return {"value": round(2 * half / dt / 1e6, 4), "unit": UNIT, "cores": nthreads, "kind": kind,
-            "sample": f"{half} random coherent + {half} random incoherent rays of the workload through the {what}, "
-                      f"{dt:.1f} s on {nthreads} threads"}
+    res = {"value": round(2 * half / dt / 1e6, 4), "unit": UNIT, "cores": nthreads, "kind": kind,
+           "sample": f"{half} random coherent + {half} random incoherent rays of the workload through the {what}, "
+                     f"{dt:.1f} s on {nthreads} threads"}
+    if gpu_out is not None:
+        from tests.parity import classify
+        orc = bindings.Oracle()
+        n_same = n_tie = n_bad = 0
+        bits = True
+        for (o4, d4, ref), dev in ((oc, dc, rc), gpu_out["coherent"]), ((oi, di, ri), gpu_out["incoherent"]):
+            got = tuple((x.cpu().numpy() if hasattr(x, "cpu") else np.asarray(x))[pick] for x in dev)
+            same, ties, bad, bits_ok = classify(pos, idx, o4, d4, got, ref, orc)
+            n_same, n_tie, n_bad, bits = n_same + same, n_tie + ties, n_bad + len(bad), bits and bits_ok
+        res["parity"] = {"rays": 2 * half, "same_id": n_same, "near_ties": n_tie, "other_mismatches": n_bad,
+                         "near_tie_rate": round(n_tie / (2 * half), 9), "t_u_v_bit_equal_on_same_id": bits}
+    return res
 
 
 def bench_path_tracer(dev, local, legs=("box", "field", "mlp", "batch", "cache")):
@@ -589,7 +606,7 @@ def main():
             "clocks": clocks,
         }
         if not args.no_cpu_baseline and world == 1:
-            line["cpu_baseline"] = cpu_baseline_sample(pos, idx, co, cd, io, idr)
+            line["cpu_baseline"] = cpu_baseline_sample(pos, idx, co, cd, io, idr, gpu_out=out)
         print(json.dumps(line), flush=True)
     sp.close()
     replicas.barrier()

@@ -139,3 +139,21 @@ def test_gpu_integrator_factory_refuses_bad_settings(tmp_path, args):
                                      integrator="GPU", integrator_args=args)
     with pytest.raises(RuntimeError, match="integrator"):
         bindings.RefLib().render_script(script, 16, 16, plugin=pkg_build.PLUGIN)
+
+
+@needs_ref
+def test_reference_irradiance_cache_baseline(tmp_path):
+    # the reference's own caching method (ICIntegrator, factory defaults), the
+    # baseline the learned cache is compared with: it renders the loaded box
+    # scene, darker than the converged image (its cached indirect light is
+    # biased low here) but close to it
+    w = 32
+    script = scenes.write_box_script(tmp_path, width=w, height=w, spp=4, space="Basic", renderer="Basic",
+                                     integrator="IC")
+    final, direct, albedo, info = bindings.RefLib().render_script(script, w, w)
+    expected = coarse_expectation(np.load(GOLDEN)["image"], w)
+    assert np.isfinite(final).all()
+    ratio = final.mean((0, 1)) / expected.mean((0, 1))
+    print(f"IC / converged mean: {ratio}, relMSE {rel_mse(final, expected):.3f}")
+    assert ((ratio > 0.7) & (ratio < 1.05)).all()
+    assert rel_mse(final, expected) < 0.15
