@@ -76,18 +76,31 @@ __device__ __forceinline__ void ray_init(RayState &r, float4 o, float4 d, uint32
     r.bu = r.bv = 0.f;
 }
 
+// Triangle tests per traversal step in the persistent kernels. A step visits
+// a node group only when no triangles of earlier groups are pending, and
+// tests at most this many of the pending ones, so the lanes of a warp take
+// turns of similar length instead of waiting out the longest leaf (a lane
+// that finishes early takes a new ray). Each ray still visits its nodes and
+// triangles in the same order, so results do not depend on it. Measured on
+// a B200 (1 M-triangle heightfield, 21 M-triangle path-traced field): 2
+// gains 11 % on incoherent rays and on the path tracer and 3 % on camera
+// rays over testing a whole leaf per step; 1 loses 35 %, 3 and 4 gain less.
+// One-ray-per-thread kernels (no refill) test a whole leaf group per step.
+constexpr int kTrisPerStep = 2;
+constexpr int kTrisWholeGroup = 32;
+
 // One traversal step. Returns true when the ray is finished (r.best is the
 // hit record, -1 for a miss, -2 for a reported error).
 // kWT selects the watertight triangle test over `raw` (three float4
 // vertices per triangle record) instead of the reference's Shirley test.
-template <bool kAnyHit, bool kStats = false, bool kSkip = false, bool kWT = false>
+template <bool kAnyHit, bool kStats = false, bool kSkip = false, bool kWT = false, int kTris = kTrisPerStep>
 __device__ __forceinline__ bool ray_step(RayState &r, uint2 *stack, const Node8 *__restrict__ nodes,
                                          const Tri *__restrict__ tris, uint32_t n_nodes_total, uint32_t n_tris_total,
                                          uint32_t *__restrict__ err, unsigned long long *n_nodes = nullptr,
                                          unsigned long long *n_tris = nullptr, Skip skip = Skip{nullptr, 0u, 0u},
                                          const float4 *__restrict__ raw = nullptr)
 {
-    if (r.ng_hits & 0xff000000u) {
+    if (r.tg_hits == 0u && (r.ng_hits & 0xff000000u)) {
         if (r.budget-- == 0u) {
             atomicOr(err, 4u);
             r.best = -2;
@@ -148,7 +161,7 @@ __device__ __forceinline__ bool ray_step(RayState &r, uint2 *stack, const Node8 
         r.tg_base = q1.y;
         r.tg_hits = hits_tri;
     }
-    while (r.tg_hits) {
+    for (int tested = 0; r.tg_hits && tested < kTris; tested++) {
         const uint32_t b = __ffs(r.tg_hits) - 1u;
         r.tg_hits &= r.tg_hits - 1u;
         const uint32_t ti = r.tg_base + b;
@@ -181,7 +194,7 @@ __device__ __forceinline__ bool ray_step(RayState &r, uint2 *stack, const Node8 
             r.whi = window_hi(r.tcur);
         }
     }
-    if (!(r.ng_hits & 0xff000000u)) {
+    if (r.tg_hits == 0u && !(r.ng_hits & 0xff000000u)) {
         if (r.sp == 0) return true;
         const uint2 e = stack[--r.sp];
         r.ng_base = e.x;
@@ -201,8 +214,8 @@ __device__ __forceinline__ void trace_one(const Node8 *__restrict__ nodes, const
     uint2 stack[kMaxStack];
     RayState r;
     ray_init(r, o, d, n_nodes_total);
-    while (!ray_step<kAnyHit, kStats, kSkip>(r, stack, nodes, tris, n_nodes_total, n_tris_total, err, &n_nodes,
-                                             &n_tris, skip)) {
+    while (!ray_step<kAnyHit, kStats, kSkip, false, kTrisWholeGroup>(r, stack, nodes, tris, n_nodes_total,
+                                                                      n_tris_total, err, &n_nodes, &n_tris, skip)) {
     }
     best = r.best;
     bt = r.best >= 0 ? r.tcur : __int_as_float(0x7f800000);
@@ -214,8 +227,9 @@ __device__ __forceinline__ void trace_one(const Node8 *__restrict__ nodes, const
 // Persistent traversal with dynamic ray fetch: each warp keeps its lanes busy
 // by handing a finished lane a new ray from a global counter whenever at least
 // kRefillLanes lanes are idle (Aila & Laine 2009, "Understanding the
-// efficiency of ray traversal on GPUs"). One loop iteration = one node visit
-// and the triangle tests it enables, so lanes stay in step on the same code.
+// efficiency of ray traversal on GPUs"). One loop iteration = one ray_step
+// (a node visit or up to kTrisPerStep triangle tests), so lanes stay in step
+// on the same code.
 // ---------------------------------------------------------------------------
 constexpr uint32_t kRefillLanes = 8;
 
