@@ -25,7 +25,7 @@ def rel_mse(x, gt, eps=1e-2):
 
 def equal_time(space, scene, width, height, gt, frames=64, warmup=8, spp_per_frame=1, cache_depth=1,
                train_every=16, train_steps=4, train_batch=16384, max_depth=12, seed=100, lr=1e-2,
-               ablate_training=False):
+               ablate_training=False, train_tail=0):
     cam = dict(scene["camera"], aspect=width / height)
     sky = scene.get("sky", (0.0, 0.0, 0.0))
     space.mlp_init(seed=seed, lr=lr)
@@ -33,7 +33,7 @@ def equal_time(space, scene, width, height, gt, frames=64, warmup=8, spp_per_fra
     # untimed: first call allocates the wavefront and cache buffers
     space.render(cam, width, height, spp_per_frame, seed=seed + 99991, cache_depth=cache_depth,
                  train_every=train_every, train_steps=0 if ablate_training else train_steps,
-                 train_batch=train_batch, **kw)
+                 train_batch=train_batch, train_tail=train_tail, **kw)
     space.mlp_init(seed=seed, lr=lr)
     acc = np.zeros((height, width, 3))
     n_acc = 0
@@ -41,7 +41,7 @@ def equal_time(space, scene, width, height, gt, frames=64, warmup=8, spp_per_fra
     for f in range(frames):
         img = space.render(cam, width, height, spp_per_frame, seed=seed + f, cache_depth=cache_depth,
                            train_every=train_every, train_steps=0 if ablate_training else train_steps,
-                           train_batch=train_batch, **kw)
+                           train_batch=train_batch, train_tail=train_tail, **kw)
         if f >= warmup:
             acc += img
             n_acc += 1

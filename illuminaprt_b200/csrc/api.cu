@@ -733,7 +733,7 @@ static int prepare_scene(ilg_ctx *runner, ilg_ctx *ctx, const ilg_camera_frame &
 // waves of at most `cap_req` paths on the runner's buffers and stream.
 static int run_render(ilg_ctx *ctx, std::vector<SceneRec> &recs, uint32_t cap_req, uint32_t block,
                       uint32_t cache_depth, uint32_t train_every, uint32_t train_steps, uint32_t train_batch,
-                      uint64_t *total_paths_out, bool aux = false, bool count = false)
+                      uint64_t *total_paths_out, bool aux = false, bool count = false, uint32_t train_tail = 0)
 {
     cudaStream_t st = ctx->stream;
     uint64_t total = 0, pixels64 = 0;
@@ -811,6 +811,7 @@ static int run_render(ilg_ctx *ctx, std::vector<SceneRec> &recs, uint32_t cap_re
         CK(ctx->qry_feat.reserve((size_t)cap * kMlpRaw));
         CK(ctx->qry_out.reserve((size_t)cap * 3));
         CK(ctx->qry_beta.reserve(cap));
+        CK(ctx->qry_meta.reserve(cap));
         CK(ctx->mlp_enc.reserve((size_t)cap * kGridLevels));
         {
             int rc = mlp_reserve_train(ctx, train_batch);
@@ -818,6 +819,8 @@ static int run_render(ilg_ctx *ctx, std::vector<SceneRec> &recs, uint32_t cap_re
         }
         R.cache_depth = cache_depth;
         R.train_every = train_every;
+        R.train_tail = train_tail;
+        R.qry_meta = ctx->qry_meta.ptr;
         R.scene_lo = make_float3(ctx->scene_lo[0], ctx->scene_lo[1], ctx->scene_lo[2]);
         R.scene_inv_ext = make_float3(1.f / std::max(ctx->scene_hi[0] - ctx->scene_lo[0], 1e-20f),
                                       1.f / std::max(ctx->scene_hi[1] - ctx->scene_lo[1], 1e-20f),
@@ -839,6 +842,7 @@ static int run_render(ilg_ctx *ctx, std::vector<SceneRec> &recs, uint32_t cap_re
         CK(cudaMemsetAsync(R.rec_count, 0, sizeof(uint32_t), st));
         mlp = ctx->mlp_view();
     }
+
 
     // The frame (every wave, every bounce) is one CUDA graph. Nothing in it
     // depends on the host between launches (queue counts stay on the device),
@@ -909,6 +913,7 @@ int render_one(ilg_ctx *ctx, const ilg_camera_frame &frame, const ilg_render_opt
         if (!ctx->mlp_ready) return fail(ctx, ILG_ESTATE, "ilg_render: cache_depth set but ilg_mlp_init not called");
         if (cache_depth >= opts->max_depth)
             return fail(ctx, ILG_EINVAL, "ilg_render: cache_depth %u must be below max_depth %u", cache_depth, opts->max_depth);
+        if (opts->train_tail > 64) return fail(ctx, ILG_EINVAL, "ilg_render: train_tail %u above 64", opts->train_tail);
     }
     CK(cudaSetDevice(ctx->device));
     cudaStream_t st = ctx->stream;
@@ -920,7 +925,7 @@ int render_one(ilg_ctx *ctx, const ilg_camera_frame &frame, const ilg_render_opt
     const bool aux = direct_rgb || albedo_rgb;
     rc = run_render(ctx, recs, opts->paths_per_wave, 128, cache_depth, opts->train_every ? opts->train_every : 16u,
                     opts->train_steps, opts->train_batch ? opts->train_batch : 16384u, nullptr, aux,
-                    ctx->counted);
+                    ctx->counted, opts->train_tail);
     if (rc) return rc;
     const bool dev = (flags & ILG_DEVICE_PTRS) != 0;
     const float4 *sums[3] = {ctx->accum.ptr, ctx->accum_direct.ptr, ctx->accum_albedo.ptr};

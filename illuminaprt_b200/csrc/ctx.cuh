@@ -68,7 +68,7 @@ struct ilg_ctx {
     ilg::DevBuf<int> hit_tri;
     ilg::DevBuf<float> hit_t, out_dev;
     // path tracing with the radiance cache
-    ilg::DevBuf<uint32_t> train_slot, rec_of, s_meta;
+    ilg::DevBuf<uint32_t> train_slot, rec_of, s_meta, qry_meta;
     ilg::DevBuf<float> rec_feat, rec_tgt, qry_feat, qry_out;
     ilg::DevBuf<float4> rec_beta, qry_beta;
     uint32_t last_train_records = 0;
@@ -146,7 +146,8 @@ struct ilg_ctx {
         s_d.release(); s_c.release(); accum.release(); accum_direct.release(); accum_albedo.release(); q_p0.release(); q_p1.release(); counts.release();
         hit_tri.release(); hit_t.release(); out_dev.release(); path_scene.release(); s_sid.release();
         scene_table.release();
-        train_slot.release(); rec_of.release(); s_meta.release(); rec_feat.release(); rec_tgt.release();
+        train_slot.release(); rec_of.release(); s_meta.release(); qry_meta.release(); rec_feat.release();
+        rec_tgt.release();
         qry_feat.release(); qry_out.release(); rec_beta.release(); qry_beta.release();
         mlp_w.release(); mlp_m.release(); mlp_v.release(); mlp_grad.release(); mlp_loss.release();
         mlp_grid.release(); mlp_grid_grad.release(); mlp_grid_m.release(); mlp_grid_v.release(); mlp_enc.release();

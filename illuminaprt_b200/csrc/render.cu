@@ -25,6 +25,7 @@
 #include "trace.cuh"
 #include "mlp.cuh"
 
+#include <algorithm>
 #include <cfloat>
 
 namespace ilg {
@@ -323,6 +324,7 @@ __global__ void __launch_bounds__(256) k_shade(RenderDev R, int cur, uint32_t de
     float4 qb = make_float4(0.f, 0.f, 0.f, 0.f);
     float qf[kMlpRaw];
     uint32_t tslot = 0xffffffffu;  // training slot of this path
+    uint32_t qmeta = 0xffffffffu;  // the query's training tail, if it is one
     uint32_t sid = 0;
 
     if (i < R.count[cur]) {
@@ -376,14 +378,25 @@ __global__ void __launch_bounds__(256) k_shade(RenderDev R, int cur, uint32_t de
             if (depth == 0 && R.accum_albedo) add_pixel(R.accum_albedo, pixel, m.kind == 1u ? m.f0 : m.albedo);
 
             const bool at_cache = depth < S.max_depth && R.cache_depth && depth == R.cache_depth;
+            // a training path with a short tail stops into the cache too; the
+            // cache's answer there completes the targets of its records
+            // (self-training), not its pixel
+            const bool at_tail = depth < S.max_depth && R.train_tail && tslot != 0xffffffffu &&
+                                 depth == R.cache_depth + R.train_tail;
             if (at_cache) {
                 // the cache supplies the radiance leaving this vertex to the pixel
                 query = true;
                 write_features(qf, R, p, wo, W, m);
                 qb = make_float4(beta.x, beta.y, beta.z, __uint_as_float(image_pixel));
             }
-            if (at_cache && tslot == 0xffffffffu) {
-                // a rendering path stops here
+            if (at_tail) {
+                query = true;
+                qmeta = (tslot << 8) | depth;
+                write_features(qf, R, p, wo, W, m);
+                qb = make_float4(beta.x, beta.y, beta.z, __uint_as_float(R.discard_pixel));
+            }
+            if ((at_cache && tslot == 0xffffffffu) || at_tail) {
+                // the path stops here
             } else if (depth < S.max_depth) {
                 if (tslot != 0xffffffffu && depth >= 1) {
                     // training record of this vertex; its target fills in as the tail is traced
@@ -505,6 +518,7 @@ __global__ void __launch_bounds__(256) k_shade(RenderDev R, int cur, uint32_t de
 #pragma unroll
                 for (int k = 0; k < kMlpRaw; k++) R.qry_feat[(size_t)q * kMlpRaw + k] = qf[k];
                 R.qry_beta[q] = qb;
+                R.qry_meta[q] = qmeta;
             } else {
                 atomicOr(R.err, 32u);
             }
@@ -512,7 +526,9 @@ __global__ void __launch_bounds__(256) k_shade(RenderDev R, int cur, uint32_t de
     }
 }
 
-// pixel += throughput * max(cache output, 0) for every cache query of the wave
+// pixel += throughput * max(cache output, 0) for every cache query of the
+// wave; a training tail's answer goes to its path's records instead (its
+// pixel is the discard slot)
 __global__ void k_cache_apply(RenderDev R)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -520,7 +536,12 @@ __global__ void k_cache_apply(RenderDev R)
     const float4 b = R.qry_beta[i];
     const float3 y = make_float3(fmaxf(R.qry_out[3 * i], 0.f), fmaxf(R.qry_out[3 * i + 1], 0.f),
                                  fmaxf(R.qry_out[3 * i + 2], 0.f));
-    add_pixel(R.accum, __float_as_uint(b.w), make_float3(b.x * y.x, b.y * y.y, b.z * y.z));
+    const float3 c = make_float3(b.x * y.x, b.y * y.y, b.z * y.z);
+    add_pixel(R.accum, __float_as_uint(b.w), c);
+    if (R.train_tail) {
+        const uint32_t meta = R.qry_meta[i];
+        if (meta != 0xffffffffu) credit(R, meta >> 8, meta & 0xffu, c);
+    }
 }
 
 template <bool kStats>
@@ -679,7 +700,10 @@ cudaError_t render_wave(const RenderDev &R, uint32_t n_paths, uint64_t wave_begi
     k_camera<<<blocks_for(n_paths, 128), 128, 0, st>>>(R, n_paths, wave_begin);  // also sets count[0]
     uint32_t n_launch = 1;
     int cur = 0;
-    for (uint32_t depth = 0; depth <= R.depth_max; depth++) {
+    // with short training tails every path has stopped by the tail vertex
+    const uint32_t tail = R.cache_depth + R.train_tail;
+    const uint32_t last = (R.cache_depth && R.train_tail && cache) ? std::min(R.depth_max, tail) : R.depth_max;
+    for (uint32_t depth = 0; depth <= last; depth++) {
         if ((e = cudaMemsetAsync(R.count + (cur ^ 1), 0, sizeof(uint32_t), st)) != cudaSuccess) return e;
         if ((e = cudaMemsetAsync(R.sh_count, 0, sizeof(uint32_t), st)) != cudaSuccess) return e;
         if (R.stats) {
@@ -692,12 +716,13 @@ cudaError_t render_wave(const RenderDev &R, uint32_t n_paths, uint64_t wave_begi
         }
         k_shade<<<blocks_for(n_paths, T), T, 0, st>>>(R, cur, depth, wave_begin);
         n_launch += 2;
-        if (R.cache_depth && depth == R.cache_depth && cache) {
+        if (R.cache_depth && cache && (depth == R.cache_depth || (R.train_tail && depth == tail))) {
             if ((e = mlp_infer(*cache, R.qry_feat, n_paths, R.qry_out, st, R.qry_count)) != cudaSuccess) return e;
             k_cache_apply<<<blocks_for(n_paths, 128), 128, 0, st>>>(R);
+            if ((e = cudaMemsetAsync(R.qry_count, 0, sizeof(uint32_t), st)) != cudaSuccess) return e;
             n_launch += 2;
         }
-        if (depth < R.depth_max) {
+        if (depth < last) {
             if (R.stats) {
                 k_shadow<true><<<blocks_for((uint64_t)R.sh_capacity, T), T, 0, st>>>(R);
             } else if (!R.persistent) {

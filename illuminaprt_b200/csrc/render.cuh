@@ -83,6 +83,8 @@ struct RenderDev {
     // radiance cache (cache_depth == 0: plain path tracing, none of this is used)
     uint32_t cache_depth;      // rendering paths stop into the cache at this vertex
     uint32_t train_every;      // one path in train_every is a training path
+    uint32_t train_tail;       // training paths stop into the cache at vertex cache_depth + train_tail
+                               // (0: they are traced to the full depth)
     float3 scene_lo, scene_inv_ext;
     uint32_t *train_slot;      // per path of the wave: training slot or ~0
     uint32_t *train_count;     // training slots handed out in this wave
@@ -97,6 +99,7 @@ struct RenderDev {
     float4 *qry_beta;          // throughput (w = pixel bits)
     float *qry_out;            // cap x 3 network outputs
     uint32_t *qry_count;
+    uint32_t *qry_meta;        // per query: (slot << 8 | vertex) of a training path's tail, or ~0
     uint32_t *s_meta;          // per shadow segment: (slot << 8 | vertex) of a training path, or ~0
 };
 

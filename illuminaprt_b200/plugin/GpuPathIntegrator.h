@@ -9,9 +9,11 @@
 // exactly as over Type = PathTracing. Under GpuRenderer its RayDepth and
 // Epsilon drive the device path tracer as a PathIntegrator's do, and with
 // Cache = MLP rendering paths stop into the radiance cache at their
-// CacheDepth-th bounce vertex while one path in 1 / TrainFraction is traced
-// to full depth to train it (TrainSteps Adam steps of TrainBatch records,
-// at LearningRate, after every rendered region). The reference has no such
+// CacheDepth-th bounce vertex while one path in 1 / TrainFraction trains it
+// (TrainSteps Adam steps of TrainBatch records, at LearningRate, after every
+// rendered region); a training path stops into the cache TrainTail vertices
+// later and the cache's answer completes its targets (0: it is traced to
+// RayDepth). The reference has no such
 // cache; its nearest relative is the irradiance cache of
 // Core/Integrator/ICIntegrator.*.
 #pragma once
@@ -30,12 +32,14 @@ struct RadianceCacheSettings {
     uint32_t train_every;   // one training path in this many
     uint32_t train_steps;   // Adam steps after each rendered region (0 = frozen)
     uint32_t train_batch;   // records per step
+    uint32_t train_tail;    // training paths stop into the cache this many vertices after
+                            // the query vertex (self-training); 0 = traced to RayDepth
     float learning_rate;
     uint32_t seed;          // network initialisation
 
     RadianceCacheSettings(void)
-        : enabled(false), depth(1), train_every(16), train_steps(4), train_batch(16384), learning_rate(1e-2f),
-          seed(1)
+        : enabled(false), depth(1), train_every(16), train_steps(4), train_batch(16384), train_tail(2),
+          learning_rate(1e-2f), seed(1)
     {
     }
 };

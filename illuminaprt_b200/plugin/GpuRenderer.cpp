@@ -171,6 +171,7 @@ void GpuRenderer::RenderRegion(RadianceBuffer *p_pRadianceBuffer, int p_nRegionX
         opts.train_every = c.train_every;
         opts.train_steps = c.train_steps;
         opts.train_batch = c.train_batch;
+        opts.train_tail = c.train_tail;
     }
     ilg_region region = {(uint32_t)p_nRegionX, (uint32_t)p_nRegionY, (uint32_t)p_nRegionWidth,
                          (uint32_t)p_nRegionHeight};

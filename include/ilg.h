@@ -189,7 +189,12 @@ typedef struct ilg_render_opts {
     uint32_t train_every;    /* 0 = 16 */
     uint32_t train_steps;    /* Adam steps after the call; 0 = none (the cache stays frozen) */
     uint32_t train_batch;    /* 0 = 16384 */
-    uint32_t reserved[2];
+    /* 0 = training paths are traced to max_depth; k >= 1 = they stop into
+     * the cache at vertex cache_depth + k, and the cache's answer there
+     * completes their targets (self-training; the frame then ends at that
+     * depth) */
+    uint32_t train_tail;
+    uint32_t reserved[1];
 } ilg_render_opts;
 
 /* Materials indexed by the mat_ids given to ilg_set_mesh. */

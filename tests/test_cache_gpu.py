@@ -44,6 +44,30 @@ def test_cache_trains_online(field):
     assert errs[1] < errs[0]
 
 
+def test_self_training_tails(field):
+    # training paths stop into the cache two vertices after the query vertex;
+    # the cache's answer there completes their records' targets. The cache
+    # still learns online, the frame ends at depth 3 (cheaper than tracing
+    # the training paths to depth 12), and a training-free frame is unchanged
+    sp, s, gt = field
+    cam = dict(s["camera"], aspect=W / H)
+    sp.mlp_init(seed=2, lr=1e-2)
+    frozen = lambda f: sp.render(cam, W, H, 64, max_depth=12, seed=77 + f, sky=s["sky"], cache_depth=1,
+                                 train_steps=0, train_tail=2)
+    before = rel_mse(frozen(0), gt)
+    for f in range(40):
+        img = sp.render(cam, W, H, 1, max_depth=12, seed=2000 + f, sky=s["sky"], cache_depth=1, train_tail=2)
+        assert np.isfinite(img).all()
+    after = rel_mse(frozen(1), gt)
+    print(f"self-trained cache, 64-spp relMSE before / after 40 frames: {before:.4f} / {after:.4f}")
+    assert after < before
+    # a frozen cache (no training) renders the same image with or without tails:
+    # tails only change what the training records receive
+    a = sp.render(cam, W, H, 4, max_depth=12, seed=5, sky=s["sky"], cache_depth=1, train_steps=0, train_tail=2)
+    b = sp.render(cam, W, H, 4, max_depth=12, seed=5, sky=s["sky"], cache_depth=1, train_steps=0, train_tail=0)
+    assert np.allclose(a, b, rtol=1e-5, atol=1e-6)
+
+
 def test_cache_in_regions(field):
     # a frozen cache (train_steps 0): region calls query the same network, so
     # tiles reproduce the whole image's paths; the whole image as one region
