@@ -612,9 +612,11 @@ int ilg_set_materials(ilg_ctx *ctx, const ilg_material *mats, uint32_t n)
     if (!mats || n == 0 || n > 0xffffu) return fail(ctx, ILG_EINVAL, "ilg_set_materials: need 1..65535 materials");
     static_assert(sizeof(ilg_material) == sizeof(Mat), "ilg_material layout");
     for (uint32_t i = 0; i < n; i++) {
-        if (mats[i].kind > ILG_MAT_GGX) return fail(ctx, ILG_EINVAL, "ilg_set_materials: material %u has unknown kind %u", i, mats[i].kind);
+        if (mats[i].kind > ILG_MAT_GLASS) return fail(ctx, ILG_EINVAL, "ilg_set_materials: material %u has unknown kind %u", i, mats[i].kind);
         if (mats[i].kind == ILG_MAT_GGX && !(mats[i].alpha > 0.f && mats[i].alpha <= 1.f))
             return fail(ctx, ILG_EINVAL, "ilg_set_materials: material %u needs 0 < alpha <= 1", i);
+        if (mats[i].kind == ILG_MAT_GLASS && !(mats[i].alpha > 0.f && mats[i].alpha < 1e30f))
+            return fail(ctx, ILG_EINVAL, "ilg_set_materials: glass material %u needs eta_i / eta_t > 0 in alpha", i);
     }
     CK(cudaSetDevice(ctx->device));
     CK(ctx->mats.reserve(n));

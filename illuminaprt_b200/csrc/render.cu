@@ -301,11 +301,55 @@ __device__ __forceinline__ float3 ggx_sample_vndf(float3 wo, float a, float u1, 
 
 // BSDF::F for one material in the local frame (Core/Material/BSDF.cpp:214-234:
 // reflection lobes only count when wi.z > 0)
+// BSDF value for a direction pair; the specular materials (mirror, glass)
+// are zero for every pair, as their BxDFs' F is (SpecularReflection::F,
+// SpecularTransmission::F).
 __device__ __forceinline__ float3 bsdf_f(const Mat &m, float3 wo, float3 wi)
 {
     if (m.kind == 1u) return ggx_f(wo, wi, m.f0, m.alpha);
-    if (wi.z > 0.f) return m.albedo * kInvPi;
+    if (m.kind == 0u && wi.z > 0.f) return m.albedo * kInvPi;
     return make_float3(0.f, 0.f, 0.f);
+}
+
+// Specular sampling of the reference's MirrorMaterial and GlassMaterial in
+// the local frame (z = normal). Mirror: SpecularReflection::SampleF
+// (Core/Material/SpecularReflectionBxDF.cpp:26-33): wi = (-wo.x, -wo.y,
+// wo.z), pdf 1, f = reflectivity / |wi.z|. Glass: BSDF::SampleF
+// (Core/Material/BSDF.cpp:141-211) picks one of its two BxDFs with the 1D
+// sample (index (int)(w * 2) % 2: 0 = SpecularTransmission with the
+// transmittance, 1 = SpecularReflection with the reflectivity) and halves
+// the pdf; SpecularTransmission::SampleF
+// (Core/Material/SpecularTransmissionBxDF.cpp:24-58) refracts by the ratio
+// of indices with no Fresnel weight, and total internal reflection gives
+// f = 0 (the path ends). `transmit` tells the caller to offset the next ray
+// origin below the surface (PathIntegrator.cpp:184-187).
+__device__ __forceinline__ void sample_specular(const Mat &m, float3 wo, float w, float3 &wi, float3 &f, float &pdf,
+                                                bool &transmit)
+{
+    transmit = false;
+    const float3 zero = make_float3(0.f, 0.f, 0.f);
+    if (m.kind == 2u || (int)(w * 2.f) % 2 == 1) {
+        wi = make_float3(-wo.x, -wo.y, wo.z);
+        f = m.albedo * (1.f / fabsf(wi.z));
+        pdf = m.kind == 2u ? 1.f : 0.5f;
+        return;
+    }
+    // glass, transmission: m.alpha holds eta_i / eta_t
+    const bool entering = wo.z > 0.f;
+    const float eta = entering ? m.alpha : 1.f / m.alpha;
+    const float sin_i2 = 1.f - wo.z * wo.z;
+    const float sin_t2 = sin_i2 * eta * eta;
+    pdf = 0.5f;
+    if (sin_t2 > 1.f) {
+        wi = zero;
+        f = zero;
+        return;
+    }
+    float cos_t = sqrtf(fmaxf(0.f, 1.f - sin_t2));
+    if (entering) cos_t = -cos_t;
+    wi = make_float3(eta * -wo.x, eta * -wo.y, cos_t);
+    f = m.f0 * (1.f / fabsf(cos_t));
+    transmit = true;
 }
 
 __global__ void __launch_bounds__(256) k_shade(RenderDev R, int cur, uint32_t depth, uint64_t wave_begin)
@@ -346,7 +390,9 @@ __global__ void __launch_bounds__(256) k_shade(RenderDev R, int cur, uint32_t de
         if (R.cache_depth && tslot != 0xffffffffu &&
             (ti >= 0 ? depth >= R.cache_depth : depth > R.cache_depth))
             pixel = R.discard_pixel;
-        float3 beta = make_float3(R.beta[path].x, R.beta[path].y, R.beta[path].z);
+        const float4 beta4 = R.beta[path];
+        float3 beta = make_float3(beta4.x, beta4.y, beta4.z);
+        const bool after_specular = beta4.w != 0.f;  // the previous bounce was a specular one
         float3 add = make_float3(0.f, 0.f, 0.f);
 
         if (ti < 0) {
@@ -369,13 +415,23 @@ __global__ void __launch_bounds__(256) k_shade(RenderDev R, int cur, uint32_t de
             onb_from_w(W, U, V);
             const float3 wo_l = make_float3(dot3(U, wo), dot3(V, wo), dot3(W, wo));
 
-            // emission only at depth 0 (no specular lobes here), one-sided
-            // (DiffuseAreaLight::Radiance, DiffuseAreaLight.cpp:47-50)
-            if (depth == 0 && light_id != 0xffffu && light_id < S.n_lights && dot3(W, wo) > 0.f)
-                add = add + beta * S.lights[light_id].emit;
+            // emission at depth 0 or right after a specular bounce
+            // (PathIntegrator.cpp:126-128), one-sided (DiffuseAreaLight::Radiance,
+            // DiffuseAreaLight.cpp:47-50)
+            if ((depth == 0 || after_specular) && light_id != 0xffffu && light_id < S.n_lights &&
+                dot3(W, wo) > 0.f) {
+                const float3 e = beta * S.lights[light_id].emit;
+                add = add + e;
+                if (tslot != 0xffffffffu && depth >= 2) credit(R, tslot, depth - 1, e);
+            }
             // RadianceContext::Albedo = the first hit's Material::Rho
-            // (PathIntegrator.cpp:121); for the GGX conductor, its F0
-            if (depth == 0 && R.accum_albedo) add_pixel(R.accum_albedo, pixel, m.kind == 1u ? m.f0 : m.albedo);
+            // (PathIntegrator.cpp:121): the reflectance; for the GGX conductor
+            // its F0; for glass the sum over its two BxDFs (BSDF::Rho,
+            // Core/Material/BSDF.cpp:123-139)
+            if (depth == 0 && R.accum_albedo)
+                add_pixel(R.accum_albedo, pixel,
+                          m.kind == 1u ? m.f0 : (m.kind == 3u ? m.albedo + m.f0 : m.albedo));
+            const bool specular = m.kind >= 2u;
 
             const bool at_cache = depth < S.max_depth && R.cache_depth && depth == R.cache_depth;
             // a training path with a short tail stops into the cache too; the
@@ -413,8 +469,9 @@ __global__ void __launch_bounds__(256) k_shade(RenderDev R, int cur, uint32_t de
                     }
                     R.rec_of[tslot * (R.depth_max + 1) + depth] = stored;
                 }
-                // next-event estimation toward every light but the one hit
-                for (uint32_t l = 0; l < S.n_lights && l < kMaxLights; l++) {
+                // next-event estimation toward every light but the one hit (a
+                // specular BSDF's F is zero for every light direction)
+                for (uint32_t l = 0; l < S.n_lights && l < kMaxLights && !specular; l++) {
                     if (l == light_id) continue;
                     const QuadLight &L = S.lights[l];
                     const float u = rnd(key, dim_of(depth, 2 * l)), v = rnd(key, dim_of(depth, 2 * l + 1));
@@ -443,7 +500,10 @@ __global__ void __launch_bounds__(256) k_shade(RenderDev R, int cur, uint32_t de
                 const float u1 = rnd(key, dim_of(depth, 20)), u2 = rnd(key, dim_of(depth, 21));
                 float3 wi_l, f;
                 float pdf;
-                if (m.kind == 1u) {
+                bool transmit = false;
+                if (specular) {
+                    sample_specular(m, wo_l, rnd(key, dim_of(depth, 22)), wi_l, f, pdf, transmit);
+                } else if (m.kind == 1u) {
                     wi_l = ggx_sample_vndf(wo_l, m.alpha, u1, u2);
                     pdf = ggx_pdf(wo_l, wi_l, m.alpha);
                     f = ggx_f(wo_l, wi_l, m.f0, m.alpha);
@@ -467,11 +527,12 @@ __global__ void __launch_bounds__(256) k_shade(RenderDev R, int cur, uint32_t de
                         else beta = beta * (1.f / q);
                     }
                     if (alive) {
-                        const float3 org = p + ng * S.eps;
+                        // a transmitted ray starts below the surface (PathIntegrator.cpp:184-187)
+                        const float3 org = p + ng * (transmit ? -S.eps : S.eps);
                         no = make_float4(org.x, org.y, org.z, S.eps);
                         nd = make_float4(wi.x, wi.y, wi.z, FLT_MAX);
                         cont = true;
-                        R.beta[path] = make_float4(beta.x, beta.y, beta.z, 0.f);
+                        R.beta[path] = make_float4(beta.x, beta.y, beta.z, specular ? 1.f : 0.f);
                     }
                 }
             }

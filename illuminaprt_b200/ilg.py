@@ -43,7 +43,7 @@ ILG_MLP_GRID_PARAMS = 1048576
 # Largest batch ilg_intersect_noalloc accepts (include/ilg.h).
 ILG_NOALLOC_MAX_RAYS = 262144
 
-ILG_MAT_LAMBERT, ILG_MAT_GGX = 0, 1
+ILG_MAT_LAMBERT, ILG_MAT_GGX, ILG_MAT_MIRROR, ILG_MAT_GLASS = 0, 1, 2, 3
 
 
 class IlgError(RuntimeError):
@@ -283,7 +283,9 @@ class GpuSpace:
 
     # --- path tracing: PathIntegrator + RenderRegion over the whole image ----
     def set_materials(self, mats):
-        """mats: sequence of dicts {albedo, kind=0, f0=(0,0,0), alpha=0}."""
+        """mats: sequence of dicts {albedo, kind=0, f0=(0,0,0), alpha=0}; kind 0 Lambertian,
+        1 GGX (f0, alpha), 2 mirror (albedo = reflectivity), 3 glass (albedo = reflectivity,
+        f0 = transmittance, alpha = eta_i / eta_t)."""
         arr = (ilg_material * len(mats))()
         for i, m in enumerate(mats):
             arr[i].albedo[:] = list(m.get("albedo", (0.0, 0.0, 0.0)))

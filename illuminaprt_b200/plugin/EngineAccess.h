@@ -7,7 +7,9 @@
 #include "Camera/Camera.h"
 #include "Integrator/PathIntegrator.h"
 #include "Light/DiffuseAreaLight.h"
+#include "Material/Glass.h"
 #include "Material/Matte.h"
+#include "Material/Mirror.h"
 #include "Shape/Quad.h"
 #include "Shape/Triangle.h"
 
@@ -34,6 +36,50 @@ struct Matte : public Illumina::Core::MatteMaterial {
     static const Illumina::Core::ITexture *Texture(const Illumina::Core::MatteMaterial *p)
     {
         Illumina::Core::ITexture *Illumina::Core::MatteMaterial::*m = &Matte::m_pTexture;
+        return p->*m;
+    }
+};
+
+// MirrorMaterial's reflectivity and texture (Material/Mirror.h).
+struct Mirror : public Illumina::Core::MirrorMaterial {
+    static const Illumina::Core::Spectrum &Reflectivity(const Illumina::Core::MirrorMaterial *p)
+    {
+        Illumina::Core::Spectrum Illumina::Core::MirrorMaterial::*m = &Mirror::m_reflectivity;
+        return p->*m;
+    }
+    static const Illumina::Core::ITexture *Texture(const Illumina::Core::MirrorMaterial *p)
+    {
+        Illumina::Core::ITexture *Illumina::Core::MirrorMaterial::*m = &Mirror::m_pTexture;
+        return p->*m;
+    }
+};
+
+// GlassMaterial's reflectivity, transmittance, indices and texture
+// (Material/Glass.h).
+struct Glass : public Illumina::Core::GlassMaterial {
+    static const Illumina::Core::Spectrum &Reflectivity(const Illumina::Core::GlassMaterial *p)
+    {
+        Illumina::Core::Spectrum Illumina::Core::GlassMaterial::*m = &Glass::m_reflectivity;
+        return p->*m;
+    }
+    static const Illumina::Core::Spectrum &Transmittance(const Illumina::Core::GlassMaterial *p)
+    {
+        Illumina::Core::Spectrum Illumina::Core::GlassMaterial::*m = &Glass::m_transmittance;
+        return p->*m;
+    }
+    static float EtaI(const Illumina::Core::GlassMaterial *p)
+    {
+        float Illumina::Core::GlassMaterial::*m = &Glass::m_fEtaI;
+        return p->*m;
+    }
+    static float EtaT(const Illumina::Core::GlassMaterial *p)
+    {
+        float Illumina::Core::GlassMaterial::*m = &Glass::m_fEtaT;
+        return p->*m;
+    }
+    static const Illumina::Core::ITexture *Texture(const Illumina::Core::GlassMaterial *p)
+    {
+        Illumina::Core::ITexture *Illumina::Core::GlassMaterial::*m = &Glass::m_pTexture;
         return p->*m;
     }
 };

@@ -14,7 +14,9 @@
 #include "GpuSpace.h"
 #include "Integrator/PathIntegrator.h"
 #include "Light/DiffuseAreaLight.h"
+#include "Material/Glass.h"
 #include "Material/Matte.h"
+#include "Material/Mirror.h"
 #include "Scene/EmissivePrimitive.h"
 #include "Scene/Scene.h"
 #include "Shape/Quad.h"
@@ -41,6 +43,13 @@ void Put(float *p_pDst, const Vector3 &p_v)
     p_pDst[0] = p_v.X;
     p_pDst[1] = p_v.Y;
     p_pDst[2] = p_v.Z;
+}
+
+void PutSpectrum(float *p_pDst, const Spectrum &p_s)
+{
+    p_pDst[0] = p_s[0];
+    p_pDst[1] = p_s[1];
+    p_pDst[2] = p_s[2];
 }
 
 }  // namespace
@@ -77,13 +86,25 @@ GpuSpace *GpuRenderer::PrepareScene(void)
         std::memset(&m, 0, sizeof(m));
         m.kind = ILG_MAT_LAMBERT;
         if (slots[k] == NULL) continue;  // no material: black
-        const MatteMaterial *matte = dynamic_cast<const MatteMaterial *>(slots[k]);
-        if (!matte) Refuse("material '" + slots[k]->GetName() + "' is not a MatteMaterial");
-        if (Access::Matte::Texture(matte)) Refuse("textured material '" + slots[k]->GetName() + "'");
-        const Spectrum &r = Access::Matte::Reflectivity(matte);
-        m.albedo[0] = r[0];
-        m.albedo[1] = r[1];
-        m.albedo[2] = r[2];
+        const std::string name = slots[k]->GetName();
+        if (const MatteMaterial *matte = dynamic_cast<const MatteMaterial *>(slots[k])) {
+            if (Access::Matte::Texture(matte)) Refuse("textured material '" + name + "'");
+            PutSpectrum(m.albedo, Access::Matte::Reflectivity(matte));
+        } else if (const MirrorMaterial *mirror = dynamic_cast<const MirrorMaterial *>(slots[k])) {
+            if (Access::Mirror::Texture(mirror)) Refuse("textured material '" + name + "'");
+            m.kind = ILG_MAT_MIRROR;
+            PutSpectrum(m.albedo, Access::Mirror::Reflectivity(mirror));
+        } else if (const GlassMaterial *glass = dynamic_cast<const GlassMaterial *>(slots[k])) {
+            if (Access::Glass::Texture(glass)) Refuse("textured material '" + name + "'");
+            const float ei = Access::Glass::EtaI(glass), et = Access::Glass::EtaT(glass);
+            if (!(ei > 0.f && et > 0.f)) Refuse("glass material '" + name + "' needs positive indices");
+            m.kind = ILG_MAT_GLASS;
+            PutSpectrum(m.albedo, Access::Glass::Reflectivity(glass));
+            PutSpectrum(m.f0, Access::Glass::Transmittance(glass));
+            m.alpha = ei / et;
+        } else {
+            Refuse("material '" + name + "' is not a MatteMaterial, MirrorMaterial or GlassMaterial");
+        }
     }
     Check(ctx, ilg_set_materials(ctx, materials.data(), (uint32_t)materials.size()), "ilg_set_materials");
 

@@ -16,8 +16,9 @@
 //               GpuPathIntegrator with Cache = MLP also turns on the
 //               device's learned radiance cache (a fresh network for each
 //               built scene, trained after every region)
-//   materials   MatteMaterial without a texture (its reflectivity); a
-//               primitive without material renders black
+//   materials   MatteMaterial, MirrorMaterial or GlassMaterial without a
+//               texture (reflectivity; for glass also transmittance and
+//               the two indices); a primitive without material renders black
 //   lights      DiffuseAreaLight on a Quad whose EmissivePrimitive is in
 //               the space
 //   camera      any ICamera: its centre / corner / across / up frame, the

@@ -200,11 +200,16 @@ def _quad_tris(v0, v1, v2, v3):
     return [(v0, v1, v2), (v0, v2, v3)]
 
 
-def box_scene():
+def box_scene(specular: bool = False):
     """Closed box [-1,1]^3 with the front (z = +1) open, walls two triangles
     each (normals inward), left wall red, right green, others grey; two inner
     boxes rotated +-17 deg about y; a 0.5 x 0.4 ceiling quad light with
     radiance (17, 12, 4) facing -y; pinhole camera at z = 3.5, 40 deg.
+
+    With specular=True the short box is a mirror (MirrorMaterial, reflectivity
+    0.9) and the tall one glass (GlassMaterial, reflectivity 0.45,
+    transmittance 0.45, eta 1 / 1.52): "kinds" (0 matte, 2 mirror, 3 glass)
+    and "spec" (per primitive: transmittance rgb, eta_i, eta_t) are added.
 
     Returns a dict with flattened world-space triangles (unshared vertices),
     a per-triangle primitive index, per-primitive albedo, the light quad in
@@ -236,7 +241,7 @@ def box_scene():
             prim_of_tri.append(pi)
     pos = np.asarray(pos, np.float32).reshape(-1, 3)
     n_tris = pos.shape[0] // 3
-    return {
+    out = {
         "pos": pos,
         "idx": np.arange(3 * n_tris, dtype=np.uint32).reshape(-1, 3),
         "prim_of_tri": np.asarray(prim_of_tri, np.uint32),
@@ -248,6 +253,16 @@ def box_scene():
                    "fov": 40.0, "aspect": 1.0},
         "max_depth": 6, "epsilon": 1e-4,
     }
+    if specular:
+        n = len(prims)
+        kinds = np.zeros(n, np.int32)
+        spec = np.zeros((n, 5), np.float32)
+        spec[:, 3], spec[:, 4] = 1.0, 1.52
+        albedo = out["albedo"]
+        kinds[5], albedo[5] = 2, (0.9, 0.9, 0.9)                        # short box: mirror
+        kinds[6], albedo[6], spec[6, :3] = 3, (0.45, 0.45, 0.45), 0.45  # tall box: glass
+        out["kinds"], out["spec"] = kinds, spec
+    return out
 
 
 def load_box_scene(space, scene=None):
@@ -257,7 +272,17 @@ def load_box_scene(space, scene=None):
     scene = scene or box_scene()
     space.initialise(scene["pos"], scene["idx"], scene["prim_of_tri"])
     space.build()
-    space.set_materials([{"albedo": tuple(a)} for a in scene["albedo"]])
+    kinds = scene.get("kinds")
+    spec = scene.get("spec")
+    mats = []
+    for p, a in enumerate(scene["albedo"]):
+        k = 0 if kinds is None else int(kinds[p])
+        m = {"albedo": tuple(a), "kind": k}
+        if k == 3:
+            m["f0"] = tuple(spec[p, :3])
+            m["alpha"] = float(spec[p, 3] / spec[p, 4])
+        mats.append(m)
+    space.set_materials(mats)
     first = int(np.nonzero(scene["prim_of_tri"] == scene["light_prim"])[0][0])
     space.set_quad_lights([{"v": scene["light_quad"], "emit": scene["light_emit"], "first_tri": first}])
     return scene

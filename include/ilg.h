@@ -143,12 +143,15 @@ int ilg_occluded_excluding(ilg_ctx *ctx, const float *ray_o_tmin, const float *r
 
 #define ILG_MAT_LAMBERT 0u /* MatteMaterial: Lambertian BxDF (Core/Material/Matte.h) */
 #define ILG_MAT_GGX 1u     /* GGX conductor (no reference counterpart) */
+#define ILG_MAT_MIRROR 2u  /* MirrorMaterial: SpecularReflection (Core/Material/Mirror.h) */
+#define ILG_MAT_GLASS 3u   /* GlassMaterial: SpecularTransmission + SpecularReflection, picked with
+                            * equal probability, no Fresnel weight (Core/Material/Glass.h) */
 
 typedef struct ilg_material {
-    float albedo[3];  /* Lambertian reflectance */
+    float albedo[3];  /* Lambertian reflectance; mirror and glass: reflectivity */
     uint32_t kind;    /* ILG_MAT_* */
-    float f0[3];      /* GGX: Schlick reflectance at normal incidence */
-    float alpha;      /* GGX: roughness (alpha) */
+    float f0[3];      /* GGX: Schlick reflectance at normal incidence; glass: transmittance */
+    float alpha;      /* GGX: roughness (alpha); glass: eta_i / eta_t (1 / 1.52 by default) */
 } ilg_material;
 
 /* A one-sided area light on a Quad (DiffuseAreaLight over Core/Shape/Quad.cpp).

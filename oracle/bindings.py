@@ -171,7 +171,10 @@ class RefLib:
             c.c_char_p, c.c_int]
         L.ilref_render_box_aov.argtypes = list(L.ilref_render_box.argtypes) + [_f32p, _f32p]
         L.ilref_render_box_renderer.argtypes = ([c.c_char_p, c.c_char_p] + list(L.ilref_render_box.argtypes[:17])
-                                                + [c.c_float, c.c_int, _f32p, _f32p, _f32p, c.c_char_p, c.c_int])
+                                                + [c.c_float, c.c_int, _f32p, _f32p, _f32p, c.c_void_p, c.c_void_p,
+                                                   c.c_char_p, c.c_int])
+        L.ilref_render_box_materials.argtypes = (list(L.ilref_render_box.argtypes[:8]) + [c.c_void_p, c.c_void_p]
+                                                 + list(L.ilref_render_box.argtypes[8:]))
         L.ilref_postprocess.argtypes = [c.c_int, _f32p, c.c_int, c.c_int, c.c_int, _f32p]
         L.ilref_render_script.argtypes = [c.c_char_p, c.c_char_p, c.c_int, c.c_int, c.c_int, _f32p, _f32p, _f32p,
                                           c.c_char_p, c.c_int, c.c_char_p, c.c_int]
@@ -180,11 +183,29 @@ class RefLib:
                                            c.c_void_p, _u8p, _u8p, _f32p, _u8p, c.c_char_p, c.c_int]
         self.L = L
 
+    @staticmethod
+    def _material_args(scene):
+        """(kinds, spec) pointers of a scene with per-primitive material kinds
+        (scenes.box_scene(specular=True)) and the arrays that back them, or
+        (None, None, ())."""
+        if "kinds" not in scene:
+            return None, None, ()
+        kinds = np.ascontiguousarray(scene["kinds"], np.int32)
+        spec = np.ascontiguousarray(scene["spec"], np.float32)
+        return kinds.ctypes.data, spec.ctypes.data, (kinds, spec)
+
     def render_box(self, scene: dict, width: int, height: int, spp: int, seed: int = 1, nthreads=None):
         """The reference's PathIntegrator on the box scene; returns (H, W, 3) float32."""
         f = lambda a: np.ascontiguousarray(a, np.float32)
         cam = scene["camera"]
         out = np.zeros((height, width, 3), np.float32)
+        if "kinds" in scene:
+            kp, sp, keep = self._material_args(scene)
+            self.L.ilref_render_box_materials(*self._scene_args(scene), kp, sp, f(cam["eye"]), f(cam["target"]),
+                                              f(cam["up"]), float(cam["fov"]), float(cam["aspect"]), width, height,
+                                              spp, int(scene["max_depth"]), float(scene["epsilon"]), seed,
+                                              nthreads or os.cpu_count() or 1, out.reshape(-1))
+            return out
         self.L.ilref_render_box(f(scene["pos"]).reshape(-1), np.ascontiguousarray(scene["prim_of_tri"], np.int32),
                                 scene["pos"].shape[0] // 3, scene["albedo"].shape[0], f(scene["albedo"]).reshape(-1),
                                 int(scene["light_prim"]), f(scene["light_quad"]).reshape(-1), f(scene["light_emit"]),
@@ -237,11 +258,12 @@ class RefLib:
         cam = scene["camera"]
         outs = [np.zeros((height, width, 3), np.float32) for _ in range(3)]
         err = ctypes.create_string_buffer(512)
+        kp, sp, keep = self._material_args(scene)
         rc = self.L.ilref_render_box_renderer(plugin.encode(), factory.encode(), *self._scene_args(scene),
                                               f(cam["eye"]), f(cam["target"]), f(cam["up"]), float(cam["fov"]),
                                               float(cam["aspect"]), width, height, spp, int(scene["max_depth"]),
                                               float(scene["epsilon"]), tile, *(o.reshape(-1) for o in outs),
-                                              err, 512)
+                                              kp, sp, err, 512)
         if rc:
             raise RuntimeError(f"ilref_render_box_renderer: {rc}: {err.value.decode(errors='replace')}")
         return tuple(outs)

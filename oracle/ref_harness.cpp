@@ -41,7 +41,9 @@
 #include "Camera/PerspectiveCamera.h"
 #include "Integrator/PathIntegrator.h"
 #include "Light/DiffuseAreaLight.h"
+#include "Material/Glass.h"
 #include "Material/Matte.h"
+#include "Material/Mirror.h"
 #include "Sampler/RandomSampler.h"
 #include "Filter/BoxFilter.h"
 #include "System/EngineKernel.h"
@@ -131,11 +133,24 @@ struct BoxScene
 	ILight *light = nullptr;
 	IShape *quadShape = nullptr;
 
+	// kinds (optional, one per primitive): 0 MatteMaterial(albedo), 2
+	// MirrorMaterial(albedo), 3 GlassMaterial(albedo, transmittance, 1,
+	// eta_i, eta_t) with spec[5 * p ..] = transmittance rgb, eta_i, eta_t.
 	void create(const float *pos, const int32_t *prim_of_tri, int ntris, int nprims, const float *albedo,
-	            int light_prim, const float *quad, const float *emit)
+	            int light_prim, const float *quad, const float *emit, const int32_t *kinds = nullptr,
+	            const float *spec = nullptr)
 	{
 		for (int p = 0; p < nprims; p++) {
-			IMaterial *m = new MatteMaterial(Spectrum(albedo[3 * p], albedo[3 * p + 1], albedo[3 * p + 2]));
+			const Spectrum a(albedo[3 * p], albedo[3 * p + 1], albedo[3 * p + 2]);
+			const int kind = kinds ? kinds[p] : 0;
+			IMaterial *m;
+			if (kind == 2)
+				m = new MirrorMaterial(a);
+			else if (kind == 3)
+				m = new GlassMaterial(a, Spectrum(spec[5 * p], spec[5 * p + 1], spec[5 * p + 2]), 1.f, spec[5 * p + 3],
+				                      spec[5 * p + 4]);
+			else
+				m = new MatteMaterial(a);
 			mats.push_back(m);
 			if (p == light_prim) {
 				Quad *qs = new Quad(Vector3(quad[0], quad[1], quad[2]), Vector3(quad[3], quad[4], quad[5]),
@@ -473,6 +488,24 @@ int ilref_render_box(const float *pos, const int32_t *prim_of_tri, int ntris, in
 	return 0;
 }
 
+// ilref_render_box with a material kind per primitive (BoxScene::create):
+// mirrors and glass next to the matte walls.
+int ilref_render_box_materials(const float *pos, const int32_t *prim_of_tri, int ntris, int nprims,
+                               const float *albedo, int light_prim, const float *quad, const float *emit,
+                               const int32_t *kinds, const float *spec,
+                               const float *eye, const float *target, const float *up, float fov, float aspect,
+                               int width, int height, int spp, int max_depth, float eps, uint32_t seed,
+                               int nthreads, float *out)
+{
+	BoxScene scene;
+	scene.create(pos, prim_of_tri, ntris, nprims, albedo, light_prim, quad, emit, kinds, spec);
+	BasicSpace space;
+	scene.fill(space);
+	render_over(space, scene.light, eye, target, up, fov, aspect, width, height, spp, max_depth, eps, seed,
+	            nthreads, out);
+	return 0;
+}
+
 // ilref_render_box plus the RadianceContext's Direct and Albedo per pixel,
 // averaged over the samples as BaseRenderer::RenderRegion averages them
 // (Core/Renderer/BaseRenderer.cpp:95-130).
@@ -503,7 +536,8 @@ int ilref_render_box_renderer(const char *plugin_path, const char *factory,
                               const float *albedo, int light_prim, const float *quad, const float *emit,
                               const float *eye, const float *target, const float *up, float fov, float aspect,
                               int width, int height, int spp, int max_depth, float eps, int tile,
-                              float *out, float *out_direct, float *out_albedo, char *err, int err_len)
+                              float *out, float *out_direct, float *out_albedo, const int32_t *kinds,
+                              const float *spec, char *err, int err_len)
 {
 	PluginSpace ps;
 	int rc = ps.open(plugin_path, factory, err, err_len);
@@ -514,7 +548,7 @@ int ilref_render_box_renderer(const char *plugin_path, const char *factory,
 		return -3;
 	}
 	BoxScene boxes;
-	boxes.create(pos, prim_of_tri, ntris, nprims, albedo, light_prim, quad, emit);
+	boxes.create(pos, prim_of_tri, ntris, nprims, albedo, light_prim, quad, emit, kinds, spec);
 	boxes.fill(*ps.space);
 	if (!ps.space->Initialise() || !ps.space->Build()) {
 		ps.report_build_failure(err, err_len);

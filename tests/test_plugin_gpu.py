@@ -118,3 +118,21 @@ def test_gpu_renderer_regions_tile_the_frame():
     tiled = ref.render_box_renderer(pkg_build.PLUGIN, scene, 100, 72, 4, tile=32)
     for a, b in zip(whole, tiled):  # same paths; float atomics may sum them in another order
         assert np.allclose(a, b, rtol=1e-5, atol=1e-6)
+
+
+def test_gpu_renderer_renders_mirror_and_glass_like_the_reference():
+    # MirrorMaterial and GlassMaterial reach the device through the engine's
+    # objects: GpuRenderer reads their reflectivity, transmittance and indices
+    p4096 = os.path.join(os.path.dirname(__file__), "golden", "box_specular_128_4096spp_seed1.npz")
+    if not os.path.exists(p4096):
+        pytest.skip("no reference image")
+    ref_img = np.load(p4096)["image"]
+    floor = _rel_mse(np.load(p4096.replace("4096spp_seed1", "1024spp_seed2"))["image"], ref_img)
+    scene = scenes.box_scene(specular=True)
+    final, direct, albedo = bindings.RefLib().render_box_renderer(pkg_build.PLUGIN, scene, 128, 128, 8192)
+    err = _rel_mse(final, ref_img)
+    print(f"relMSE(GpuRenderer 8192 spp, reference 4096 spp) = {err:.2e}; reference floor {floor:.2e}")
+    assert np.isfinite(final).all()
+    # independent noise alone gives (1/8192 + 1/4096) / (1/1024 + 1/4096) = 0.3 of the floor
+    assert err < 0.5 * floor
+    assert np.allclose(final.mean((0, 1)), ref_img.mean((0, 1)), rtol=1e-2)

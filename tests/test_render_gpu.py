@@ -45,6 +45,38 @@ def test_box_4096spp_matches_reference(box_space):
     assert np.allclose(img.mean((0, 1)), ref.mean((0, 1)), rtol=5e-3)
 
 
+def specular_golden(spp, seed):
+    p = os.path.join(GOLDEN_DIR, f"box_specular_128_{spp}spp_seed{seed}.npz")
+    if not os.path.exists(p):
+        pytest.skip(f"no {spp}-spp reference image of the specular box")
+    return np.load(p)["image"]
+
+
+def test_mirror_and_glass_match_reference():
+    # the reference's MirrorMaterial and GlassMaterial (equal-probability
+    # reflection / transmission, no Fresnel weight) on the box's two inner
+    # boxes, emission seen after specular bounces, transmitted rays offset
+    # below the surface: the device image against the reference's 4096-spp
+    # render, judged against the noise between two reference renders
+    from illuminaprt_b200.ilg import GpuSpace
+    sp = GpuSpace()
+    scene = scenes.load_box_scene(sp, scenes.box_scene(specular=True))
+    ref, ref2 = specular_golden(4096, 1), specular_golden(1024, 2)
+    floor = rel_mse(ref2, ref)
+    img = sp.render(scene["camera"], 128, 128, 16384, max_depth=6, epsilon=1e-4, seed=777)
+    err = rel_mse(img, ref)
+    print(f"relMSE(GPU 16384 spp, reference 4096 spp) = {err:.3e}; reference 1024 vs 4096 spp: {floor:.3e}")
+    assert np.isfinite(img).all()
+    # independent noise alone gives (1/16384 + 1/4096) / (1/1024 + 1/4096) = 0.25 of the floor
+    assert err < 0.4 * floor
+    assert np.allclose(img.mean((0, 1)), ref.mean((0, 1)), rtol=1e-2)
+    # the specular boxes matter: the matte-only scene renders differently there
+    plain = scenes.load_box_scene(sp, scenes.box_scene())
+    other = sp.render(plain["camera"], 128, 128, 256, max_depth=6, epsilon=1e-4, seed=777)
+    assert rel_mse(other, ref) > 10 * max(err, 1e-4)
+    sp.close()
+
+
 def test_box_error_falls_with_samples(box_space):
     sp, scene = box_space
     ref = golden(4096)
