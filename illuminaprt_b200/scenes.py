@@ -265,6 +265,23 @@ def box_scene(specular: bool = False):
     return out
 
 
+def box_materials(scene):
+    """One material dict per primitive of a box scene (GpuSpace.set_materials
+    form): matte by default; with the scene's "kinds", mirror (reflectivity =
+    albedo) and glass (transmittance and eta_i / eta_t from "spec")."""
+    kinds = scene.get("kinds")
+    spec = scene.get("spec")
+    mats = []
+    for p, a in enumerate(scene["albedo"]):
+        k = 0 if kinds is None else int(kinds[p])
+        m = {"albedo": tuple(float(x) for x in a), "kind": k}
+        if k == 3:
+            m["f0"] = tuple(float(x) for x in spec[p, :3])
+            m["alpha"] = float(spec[p, 3] / spec[p, 4])
+        mats.append(m)
+    return mats
+
+
 def load_box_scene(space, scene=None):
     """Upload the box scene to a GpuSpace: mesh with per-triangle material
     ids (one material per primitive, as MatteMaterial per primitive), the
@@ -272,17 +289,7 @@ def load_box_scene(space, scene=None):
     scene = scene or box_scene()
     space.initialise(scene["pos"], scene["idx"], scene["prim_of_tri"])
     space.build()
-    kinds = scene.get("kinds")
-    spec = scene.get("spec")
-    mats = []
-    for p, a in enumerate(scene["albedo"]):
-        k = 0 if kinds is None else int(kinds[p])
-        m = {"albedo": tuple(a), "kind": k}
-        if k == 3:
-            m["f0"] = tuple(spec[p, :3])
-            m["alpha"] = float(spec[p, 3] / spec[p, 4])
-        mats.append(m)
-    space.set_materials(mats)
+    space.set_materials(box_materials(scene))
     first = int(np.nonzero(scene["prim_of_tri"] == scene["light_prim"])[0][0])
     space.set_quad_lights([{"v": scene["light_quad"], "emit": scene["light_emit"], "first_tri": first}])
     return scene

@@ -145,8 +145,38 @@ typedef struct {
 static f3 bsdf_f(const orc_material *m, f3 wo, f3 wi)
 {
     if (m->kind == 1u) return ggx_f(wo, wi, ld(m->f0), m->alpha);
-    if (wi.z > 0.f) return mul(ld(m->albedo), 0.318309886183790671538f);
-    return mk(0, 0, 0);
+    if (m->kind == 0u && wi.z > 0.f) return mul(ld(m->albedo), 0.318309886183790671538f);
+    return mk(0, 0, 0);  /* mirror, glass: SpecularReflection / SpecularTransmission::F are 0 */
+}
+
+/* Mirror (kind 2): SpecularReflectionBxDF.cpp:26-33. Glass (kind 3): BSDF::SampleF
+ * (BSDF.cpp:141-211) picks SpecularTransmission ((int)(w * 2) % 2 == 0, with the
+ * transmittance in f0) or SpecularReflection (the reflectivity in albedo) and
+ * halves the pdf; SpecularTransmissionBxDF.cpp:24-58 refracts by the index
+ * ratio (alpha = eta_i / eta_t) with no Fresnel weight; total internal
+ * reflection gives f = 0. Returns 1 when the sampled ray is transmitted. */
+static int sample_specular(const orc_material *m, f3 wo, float w, f3 *wi, f3 *f, float *pdf)
+{
+    if (m->kind == 2u || (int)(w * 2.f) % 2 == 1) {
+        *wi = mk(-wo.x, -wo.y, wo.z);
+        *f = mul(ld(m->albedo), 1.f / fabsf(wi->z));
+        *pdf = m->kind == 2u ? 1.f : 0.5f;
+        return 0;
+    }
+    const int entering = wo.z > 0.f;
+    const float eta = entering ? m->alpha : 1.f / m->alpha;
+    const float sin_t2 = (1.f - wo.z * wo.z) * eta * eta;
+    *pdf = 0.5f;
+    if (sin_t2 > 1.f) {
+        *wi = mk(0, 0, 0);
+        *f = mk(0, 0, 0);
+        return 0;
+    }
+    float cos_t = sqrtf(fmaxf(0.f, 1.f - sin_t2));
+    if (entering) cos_t = -cos_t;
+    *wi = mk(eta * -wo.x, eta * -wo.y, cos_t);
+    *f = mul(ld(m->f0), 1.f / fabsf(cos_t));
+    return 1;
 }
 
 static int light_of(const pt_ctx *c, int32_t tri)
@@ -167,6 +197,7 @@ static f3 radiance(pt_ctx *c, uint32_t pixel, uint64_t sample)
     f3 o = c->centre, d = nrm(sub(target, c->centre));
     float tmin = 0.f;
     f3 beta = mk(1, 1, 1), L = mk(0, 0, 0);
+    int after_specular = 0;
     for (uint32_t depth = 0; depth <= c->max_depth; depth++) {
         float t;
         float oo[3] = {o.x, o.y, o.z}, dd[3] = {d.x, d.y, d.z};
@@ -187,8 +218,11 @@ static f3 radiance(pt_ctx *c, uint32_t pixel, uint64_t sample)
         onb(W, &U, &V);
         f3 wo_l = mk(dot(U, wo), dot(V, wo), dot(W, wo));
         int lid = light_of(c, tri);
-        if (depth == 0 && lid >= 0 && dot(W, wo) > 0.f) L = add(L, mulv(beta, ld(c->lights[lid].emit)));
-        for (uint32_t l = 0; l < c->nlights; l++) {
+        /* emission at depth 0 or after a specular bounce (PathIntegrator.cpp:126-128) */
+        if ((depth == 0 || after_specular) && lid >= 0 && dot(W, wo) > 0.f)
+            L = add(L, mulv(beta, ld(c->lights[lid].emit)));
+        const int specular = m->kind >= 2u;
+        for (uint32_t l = 0; l < c->nlights && !specular; l++) {
             if ((int)l == lid) continue;
             const orc_quad_light *ql = &c->lights[l];
             float u = rnd(key, dim_of(depth, 2 * l)), v = rnd(key, dim_of(depth, 2 * l + 1));
@@ -211,7 +245,10 @@ static f3 radiance(pt_ctx *c, uint32_t pixel, uint64_t sample)
         float u1 = rnd(key, dim_of(depth, 20)), u2 = rnd(key, dim_of(depth, 21));
         f3 wi_l, f;
         float pdf;
-        if (m->kind == 1u) {
+        int transmit = 0;
+        if (specular) {
+            transmit = sample_specular(m, wo_l, rnd(key, dim_of(depth, 22)), &wi_l, &f, &pdf);
+        } else if (m->kind == 1u) {
             wi_l = ggx_sample(wo_l, m->alpha, u1, u2);
             pdf = ggx_pdf(wo_l, wi_l, m->alpha);
             f = ggx_f(wo_l, wi_l, ld(m->f0), m->alpha);
@@ -230,9 +267,11 @@ static f3 radiance(pt_ctx *c, uint32_t pixel, uint64_t sample)
             if (rnd(key, dim_of(depth, 23)) > q) break;
             beta = mul(beta, 1.f / q);
         }
-        o = add(p, mul(ng, c->eps));
+        /* a transmitted ray starts below the surface (PathIntegrator.cpp:184-187) */
+        o = add(p, mul(ng, transmit ? -c->eps : c->eps));
         d = wi;
         tmin = c->eps;
+        after_specular = specular;
     }
     return L;
 }

@@ -81,6 +81,25 @@ def test_path_tracer_port_matches_reference_image(oracle):
     assert np.allclose(img.mean((0, 1)), ref.mean((0, 1)), rtol=1e-2)
 
 
+def test_path_tracer_port_matches_reference_specular_image(oracle):
+    """The C restatement with the reference's MirrorMaterial and GlassMaterial
+    against the reference's own 4096-spp render of the specular box
+    (tests/golden/make_box_golden.py 4096 1 1 128)."""
+    from illuminaprt_b200.scenes import box_materials, box_scene
+    golden = os.path.join(os.path.dirname(__file__), "golden", "box_specular_128_{}spp_seed{}.npz")
+    ref = np.load(golden.format(4096, 1))["image"].astype(np.float64)
+    floor = np.mean((np.load(golden.format(1024, 2))["image"] - ref) ** 2 / (ref ** 2 + 1e-2))
+    s = box_scene(specular=True)
+    first = int(np.nonzero(s["prim_of_tri"] == s["light_prim"])[0][0])
+    img = oracle.render(s["pos"], s["idx"], s["prim_of_tri"], box_materials(s),
+                        [{"v": s["light_quad"], "emit": s["light_emit"], "first_tri": first}], s["camera"],
+                        128, 128, 256, seed=3)
+    rel = np.mean((img - ref) ** 2 / (ref ** 2 + 1e-2))
+    # independent noise alone: (1/256 + 1/4096) / (1/1024 + 1/4096) = 3.4 floors
+    assert rel < 5.0 * floor, (rel, floor)
+    assert np.allclose(img.mean((0, 1)), ref.mean((0, 1)), rtol=1e-2)
+
+
 def test_watertight_oracle_closes_edge_cracks(oracle):
     # the watertight restatement (Woop, Benthin and Wald 2013) never lets a
     # ray through a shared edge; the reference's test does, on a few percent

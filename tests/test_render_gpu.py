@@ -137,6 +137,26 @@ def test_gpu_follows_the_cpu_port_path_for_path(box_space, oracle):
     assert close > 0.97
 
 
+def test_specular_box_gpu_follows_the_cpu_port_path_for_path(oracle):
+    """Mirror and glass with the same counter-based random numbers on both
+    sides: the device's specular sampling, its emission after specular
+    bounces and its transmitted-ray offsets are the C restatement's."""
+    from illuminaprt_b200.ilg import GpuSpace
+    sp = GpuSpace()
+    s = scenes.load_box_scene(sp, scenes.box_scene(specular=True))
+    first = int(np.nonzero(s["prim_of_tri"] == s["light_prim"])[0][0])
+    cpu = oracle.render(s["pos"], s["idx"], s["prim_of_tri"], scenes.box_materials(s),
+                        [{"v": s["light_quad"], "emit": s["light_emit"], "first_tri": first}], s["camera"],
+                        96, 96, 16, seed=23)
+    gpu = sp.render(s["camera"], 96, 96, 16, seed=23)
+    err = rel_mse(gpu, cpu)
+    close = np.mean(np.abs(gpu - cpu) <= 1e-3 * (np.abs(cpu) + 1e-3))
+    print(f"specular box, GPU vs CPU port, same paths: relMSE {err:.3e}, {100 * close:.2f}% of pixels within 0.1%")
+    assert err < 2e-4
+    assert close > 0.95
+    sp.close()
+
+
 @pytest.fixture(scope="module")
 def field_space():
     from illuminaprt_b200.ilg import GpuSpace
