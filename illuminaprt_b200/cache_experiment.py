@@ -25,40 +25,73 @@ def rel_mse(x, gt, eps=1e-2):
 
 def equal_time(space, scene, width, height, gt, frames=64, warmup=8, spp_per_frame=1, cache_depth=1,
                train_every=16, train_steps=4, train_batch=16384, max_depth=12, seed=100, lr=1e-2,
-               ablate_training=False, train_tail=0):
+               ablate_training=False, train_tail=0, device_accumulate=False):
+    """device_accumulate: frames are rendered into a device tensor and summed
+    on the device (as a progressive renderer's accumulation buffer would be),
+    with a synchronisation after every frame in both runs; otherwise each
+    frame comes back to the host and is summed there."""
     cam = dict(scene["camera"], aspect=width / height)
     sky = scene.get("sky", (0.0, 0.0, 0.0))
-    space.mlp_init(seed=seed, lr=lr)
     kw = dict(max_depth=max_depth, sky=sky)
-    # untimed: first call allocates the wavefront and cache buffers
-    space.render(cam, width, height, spp_per_frame, seed=seed + 99991, cache_depth=cache_depth,
-                 train_every=train_every, train_steps=0 if ablate_training else train_steps,
-                 train_batch=train_batch, train_tail=train_tail, **kw)
+    out = acc_dev = None
+    if device_accumulate:
+        import torch
+        out = torch.empty((height, width, 3), dtype=torch.float32, device=f"cuda:{space.device}")
+        acc_dev = torch.zeros((height, width, 3), dtype=torch.float64, device=out.device)
+
+    def frame(**args):
+        """One frame, summed into the accumulator when `keep`."""
+        keep = args.pop("keep")
+        if device_accumulate:
+            space.render(cam, width, height, spp_per_frame, out=out, **args, **kw)
+            if keep:
+                acc_dev.add_(out)
+            space.sync()
+            return None
+        img = space.render(cam, width, height, spp_per_frame, **args, **kw)
+        return img if keep else None
+
+    def reset():
+        if device_accumulate:
+            acc_dev.zero_()
+        return np.zeros((height, width, 3))
+
+    def result(acc, n):
+        total = acc_dev.cpu().numpy() if device_accumulate else acc
+        return total / max(1, n)
+
+    cache_kw = dict(cache_depth=cache_depth, train_every=train_every,
+                    train_steps=0 if ablate_training else train_steps, train_batch=train_batch,
+                    train_tail=train_tail)
     space.mlp_init(seed=seed, lr=lr)
-    acc = np.zeros((height, width, 3))
+    # untimed: first call allocates the wavefront and cache buffers
+    frame(seed=seed + 99991, keep=False, **cache_kw)
+    space.mlp_init(seed=seed, lr=lr)
+    acc = reset()
     n_acc = 0
     t0 = time.perf_counter()
     for f in range(frames):
-        img = space.render(cam, width, height, spp_per_frame, seed=seed + f, cache_depth=cache_depth,
-                           train_every=train_every, train_steps=0 if ablate_training else train_steps,
-                           train_batch=train_batch, train_tail=train_tail, **kw)
+        img = frame(seed=seed + f, keep=f >= warmup, **cache_kw)
         if f >= warmup:
-            acc += img
+            if img is not None:
+                acc += img
             n_acc += 1
     t_cache = time.perf_counter() - t0
-    cached = acc / max(1, n_acc)
+    cached = result(acc, n_acc)
     # plain path tracing for the same wall time
-    space.render(cam, width, height, spp_per_frame, seed=seed + 77777, **kw)
-    acc = np.zeros((height, width, 3))
+    frame(seed=seed + 77777, keep=False)
+    acc = reset()
     n_plain = 0
     t0 = time.perf_counter()
     while True:
-        acc += space.render(cam, width, height, spp_per_frame, seed=seed + 500000 + n_plain, **kw)
+        img = frame(seed=seed + 500000 + n_plain, keep=True)
+        if img is not None:
+            acc += img
         n_plain += 1
         if time.perf_counter() - t0 >= t_cache:
             break
     t_plain = time.perf_counter() - t0
-    plain = acc / n_plain
+    plain = result(acc, n_plain)
     e_plain, e_cache = rel_mse(plain, gt), rel_mse(cached, gt)
     return {
         "relmse_plain": e_plain,

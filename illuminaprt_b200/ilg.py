@@ -189,6 +189,7 @@ class GpuSpace:
         rc = self.L.ilg_create(ctypes.byref(self.h), ctypes.byref(opts))
         if rc != ILG_OK:
             raise IlgError(rc, f"ilg_create(device={device}) failed")
+        self.device = device
         self.n_tris = 0
 
     def _check(self, rc: int):

@@ -149,11 +149,18 @@ def test_specular_box_gpu_follows_the_cpu_port_path_for_path(oracle):
                         [{"v": s["light_quad"], "emit": s["light_emit"], "first_tri": first}], s["camera"],
                         96, 96, 16, seed=23)
     gpu = sp.render(s["camera"], 96, 96, 16, seed=23)
-    err = rel_mse(gpu, cpu)
-    close = np.mean(np.abs(gpu - cpu) <= 1e-3 * (np.abs(cpu) + 1e-3))
-    print(f"specular box, GPU vs CPU port, same paths: relMSE {err:.3e}, {100 * close:.2f}% of pixels within 0.1%")
-    assert err < 2e-4
-    assert close > 0.95
+    per_pixel = np.mean((gpu.astype(np.float64) - cpu) ** 2 / (cpu.astype(np.float64) ** 2 + 1e-2), axis=2)
+    close = np.mean(np.all(np.abs(gpu - cpu) <= 1e-3 * (np.abs(cpu) + 1e-3), axis=2))
+    # where float rounding flips one decision of a path (a refraction, a
+    # glass lobe, a grazing hit) the two paths part and the pixel differs
+    # outright; glass without a Fresnel weight carries up to twice its
+    # throughput per interaction, so such pixels can be fireflies. The rest
+    # must agree: the error over all but the worst 1 % of pixels
+    trimmed = float(np.mean(np.sort(per_pixel.ravel())[: int(0.99 * per_pixel.size)]))
+    print(f"specular box, GPU vs CPU port, same paths: {100 * close:.2f}% of pixels within 0.1%, "
+          f"relMSE without the worst 1 %: {trimmed:.3e}")
+    assert close > 0.99
+    assert trimmed < 2e-5
     sp.close()
 
 
