@@ -315,23 +315,53 @@ def write_box_script(directory, scene=None, width: int = 64, height: int = 64, s
     reference's), an integrator of type `integrator` (``"PathTracing"``, or
     the plug-in's ``"GPU"``) with the scene's depth and epsilon plus
     `integrator_args` (e.g. ``{"Cache": "MLP"}``), a Random sampler, a Box
-    filter and a ``Memory`` device of width x height."""
+    filter and a ``Memory`` device of width x height.
+
+    For a scene with material kinds (box_scene(specular=True)) a mirror
+    primitive's MTL material gets ``illum 5`` and Ks = its reflectivity (the
+    loader's Mirror, WavefrontSceneLoader.cpp:212-232), and a glass primitive
+    goes to ``glass.obj``, its own Geometry primitive with a Glass material
+    declared in the script (Reflectivity = {reflectivity, transmittance},
+    Absorption, Eta = {eta_i, eta_t}; MaterialFactories.h:105-135): the MTL
+    route has no indices for glass."""
     import os
     scene = scene or box_scene()
     directory = os.path.abspath(str(directory))
     os.makedirs(directory, exist_ok=True)
     obj, mtl, ilm = (os.path.join(directory, n) for n in ("box.obj", "box.mtl", "box.ilm"))
     light = scene["light_prim"]
+    kinds = scene.get("kinds")
+    kind_of = (lambda p: 0) if kinds is None else (lambda p: int(kinds[p]))
+    glass = [p for p in range(len(scene["albedo"])) if kind_of(p) == 3]
     with open(mtl, "w") as f:
         for p, a in enumerate(scene["albedo"]):
-            if p != light:
-                f.write(f"newmtl prim{p}\nKd {_g(a[0])} {_g(a[1])} {_g(a[2])}\n\n")
+            if p == light or p in glass:
+                continue
+            f.write(f"newmtl prim{p}\nKd {_g(a[0])} {_g(a[1])} {_g(a[2])}\n")
+            if kind_of(p) == 2:
+                f.write(f"Ks {_g(a[0])} {_g(a[1])} {_g(a[2])}\nillum 5\n")
+            f.write("\n")
     pos = scene["pos"].reshape(-1, 3, 3).astype(np.float32)
+    if glass:
+        with open(os.path.join(directory, "glass.obj"), "w") as f:
+            nv = 0
+            for t, p in enumerate(scene["prim_of_tri"]):
+                if p not in glass:
+                    continue
+                v = pos[t].astype(np.float64)
+                n = np.cross(v[1] - v[0], v[2] - v[0])
+                n /= np.linalg.norm(n)
+                for c in range(3):
+                    f.write(f"v {_g(v[c, 0])} {_g(v[c, 1])} {_g(v[c, 2])}\n")
+                f.write(f"vn {_g(n[0])} {_g(n[1])} {_g(n[2])}\n")
+                k = nv // 3 + 1
+                f.write(f"f {nv + 1}//{k} {nv + 2}//{k} {nv + 3}//{k}\n")
+                nv += 3
     with open(obj, "w") as f:
         f.write("mtllib box.mtl\n")
         current, nv = None, 0
         for t, p in enumerate(scene["prim_of_tri"]):
-            if p == light:
+            if p == light or p in glass:
                 continue
             v = pos[t].astype(np.float64)
             n = np.cross(v[1] - v[0], v[2] - v[0])
@@ -349,6 +379,18 @@ def write_box_script(directory, scene=None, width: int = 64, height: int = 64, s
     alb = scene["albedo"][light]
     vec = lambda v: "{" + ",".join(_g(x) for x in v) + "}"
     extra = "".join(f"\t\t{k} = {v}\n" for k, v in (integrator_args or {}).items())
+    glass_shape = glass_material = glass_prim = ""
+    if glass:
+        g = glass[0]
+        r, t, eta = scene["albedo"][g], scene["spec"][g, :3], scene["spec"][g, 3:5]
+        gobj = os.path.join(directory, "glass.obj")
+        glass_shape = (f"\tShape {{\n\t\tId = glass_mesh\n\t\tType = WavefrontModel\n\t\tFilename = {gobj}\n"
+                       f"\t\tContainer = {container}\n\t}}\n")
+        glass_material = (f"\tMaterial {{\n\t\tId = glass_material\n\t\tType = Glass\n"
+                          f"\t\tReflectivity = {{{vec(r)},{vec(t)}}}\n\t\tAbsorption = 1\n"
+                          f"\t\tEta = {vec(eta)}\n\t}}\n")
+        glass_prim = ("\t\t\t\tPrimitive {\n\t\t\t\t\tId = glass\n\t\t\t\t\tType = Geometry\n"
+                      "\t\t\t\t\tMaterial = glass_material\n\t\t\t\t\tShape = glass_mesh\n\t\t\t\t}\n")
     script = f"""# box scene: walls, two boxes and a ceiling quad light
 Shapes {{
 \tShape {{
@@ -363,14 +405,14 @@ Shapes {{
 \t\tType = Quad
 \t\tVertices = {{{",".join(vec(v) for v in q)}}}
 \t}}
-}}
+{glass_shape}}}
 Materials {{
 \tMaterial {{
 \t\tId = light_material
 \t\tType = Matte
 \t\tReflectivity = {vec(alb)}
 \t}}
-}}
+{glass_material}}}
 Lights {{
 \tLight {{
 \t\tId = ceiling_light
@@ -453,7 +495,7 @@ Environment {{
 \t\t\t\t\tShape = light_quad
 \t\t\t\t\tLight = ceiling_light
 \t\t\t\t}}
-\t\t\t}}
+{glass_prim}\t\t\t}}
 \t\t}}
 \t}}
 }}

@@ -176,6 +176,8 @@ void register_factories(EngineKernel *k)
 	k->GetShapeManager()->RegisterFactory("Quad", new QuadMeshShapeFactory());
 	k->GetShapeManager()->RegisterFactory("Triangle", new TriangleShapeFactory());
 	k->GetMaterialManager()->RegisterFactory("Matte", new MatteMaterialFactory());
+	k->GetMaterialManager()->RegisterFactory("Mirror", new MirrorMaterialFactory());
+	k->GetMaterialManager()->RegisterFactory("Glass", new GlassMaterialFactory());
 	k->GetMaterialManager()->RegisterFactory("Group", new MaterialGroupFactory());
 }
 

@@ -13,7 +13,7 @@ import pytest
 from illuminaprt_b200 import build as pkg_build
 from illuminaprt_b200 import scenes
 from oracle import bindings
-from tests.test_scene_script import GOLDEN, coarse_expectation, rel_mse
+from tests.test_scene_script import GOLDEN, SPECULAR, coarse_expectation, rel_mse
 
 pytestmark = [pytest.mark.gpu,
               pytest.mark.skipif(not (os.path.exists(pkg_build.PLUGIN) and bindings.ref_available()),
@@ -96,3 +96,20 @@ def test_gpu_integrator_with_the_radiance_cache(tmp_path):
     print(f"relMSE at {spp} spp: cached {e_cached:.2e}, plain {e_plain:.2e}")
     assert e_cached < 0.1
     assert np.allclose(cached[0].mean((0, 1)), expected.mean((0, 1)), rtol=0.15)
+
+
+def test_specular_script_scene_on_the_gpu_renderer(tmp_path):
+    # the script's mirror (MTL illum 5) and glass (script Glass material)
+    # reach the device through GpuSpace / GpuRenderer
+    ref = np.load(SPECULAR.format(4096, 1))["image"]
+    floor = rel_mse(np.load(SPECULAR.format(1024, 2))["image"], ref)
+    script = scenes.write_box_script(tmp_path, scene=scenes.box_scene(specular=True), width=128, height=128,
+                                     spp=8192)
+    final, direct, albedo, info = bindings.RefLib().render_script(script, 128, 128, plugin=pkg_build.PLUGIN)
+    assert "space=GpuSpace" in info and "primitives=3" in info, info
+    err = rel_mse(final, ref)
+    print(f"relMSE(specular script on GpuRenderer 8192 spp, reference 4096 spp) = {err:.2e}; floor {floor:.2e}")
+    assert np.isfinite(final).all()
+    # independent noise alone gives (1/8192 + 1/4096) / (1/1024 + 1/4096) = 0.3 of the floor
+    assert err < 0.5 * floor
+    assert np.allclose(final.mean((0, 1)), ref.mean((0, 1)), rtol=1e-2)
