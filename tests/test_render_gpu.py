@@ -11,7 +11,7 @@ from illuminaprt_b200 import scenes
 pytestmark = pytest.mark.gpu
 
 GOLDEN_DIR = os.path.join(os.path.dirname(__file__), "golden")
-REL_MSE_TOL = 1e-3  # north-star parity bar for the converged image
+REL_MSE_TOL = 1e-3  # parity bar for the converged image (relMSE against the reference)
 
 
 def rel_mse(x, ref, eps=1e-2):
