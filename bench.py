@@ -281,9 +281,10 @@ def bench_cache(res, local):
     tracing on the 20,971,530-triangle icosphere field at 480x270 (reduced
     from 1080p so the ground truth fits the bench's time: 4096 spp instead of
     16384), 64 frames of 1 spp, cache at the first bounce vertex, 8 Adam
-    steps of 32768 records per frame, training paths stopping into the cache
-    one vertex later (self-training); the same with training paths traced to
-    full depth is reported beside it. Frames accumulate on the device, as a
+    steps of 32768 records per frame run twice over the frame's records,
+    training paths stopping into the cache one vertex later (self-training);
+    one pass, a two-vertex tail and training paths traced to full depth are
+    reported beside it. Frames accumulate on the device, as a
     progressive renderer's accumulation buffer does, in both runs."""
     from illuminaprt_b200 import scenes
     from illuminaprt_b200.cache_experiment import equal_time
@@ -294,14 +295,16 @@ def bench_cache(res, local):
     scenes.load_sphere_field(sp, field)
     gt = sp.render(dict(field["camera"], aspect=w / h), w, h, 4096, max_depth=12, seed=424242, sky=field["sky"])
     kw = dict(frames=64, warmup=8, cache_depth=1, train_steps=8, train_batch=32768, device_accumulate=True)
-    r = equal_time(sp, field, w, h, gt, train_tail=1, **kw)
-    tail2 = equal_time(sp, field, w, h, gt, train_tail=2, **kw)
+    r = equal_time(sp, field, w, h, gt, train_tail=1, train_epochs=2, **kw)
+    one_pass = equal_time(sp, field, w, h, gt, train_tail=1, **kw)
+    tail2 = equal_time(sp, field, w, h, gt, train_tail=2, train_epochs=2, **kw)
     full = equal_time(sp, field, w, h, gt, **kw)
     res["cache_equal_time"] = {
         "scene": "icosphere field 480x270, ground truth 4096 spp", "relmse_plain": round(r["relmse_plain"], 6),
         "relmse_cached": round(r["relmse_cached"], 6), "gain": round(r["gain"], 3),
         "bias_cached": [round(b, 5) for b in r["bias_cached"]], "seconds": round(r["seconds_cached"], 4),
         "frames_cached": r["frames_cached"], "frames_plain": r["frames_plain"], "train_tail": 1,
+        "train_epochs": 2, "gain_one_pass": round(one_pass["gain"], 3),
         "gain_train_tail_2": round(tail2["gain"], 3), "gain_full_depth_training": round(full["gain"], 3),
         "accumulation": "device"}
     sp.close()

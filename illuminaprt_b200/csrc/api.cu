@@ -735,7 +735,8 @@ static int prepare_scene(ilg_ctx *runner, ilg_ctx *ctx, const ilg_camera_frame &
 // waves of at most `cap_req` paths on the runner's buffers and stream.
 static int run_render(ilg_ctx *ctx, std::vector<SceneRec> &recs, uint32_t cap_req, uint32_t block,
                       uint32_t cache_depth, uint32_t train_every, uint32_t train_steps, uint32_t train_batch,
-                      uint64_t *total_paths_out, bool aux = false, bool count = false, uint32_t train_tail = 0)
+                      uint64_t *total_paths_out, bool aux = false, bool count = false, uint32_t train_tail = 0,
+                      uint32_t train_epochs = 1)
 {
     cudaStream_t st = ctx->stream;
     uint64_t total = 0, pixels64 = 0;
@@ -888,6 +889,7 @@ static int run_render(ilg_ctx *ctx, std::vector<SceneRec> &recs, uint32_t cap_re
         CK(cudaStreamSynchronize(st));
         n_rec = std::min(n_rec, R.rec_cap);
         ctx->last_train_records = n_rec;
+        for (uint32_t ep = 0; ep < train_epochs; ep++)
         for (uint32_t s = 0; s < train_steps && (uint64_t)s * train_batch < n_rec; s++) {
             const uint32_t nb = std::min(train_batch, n_rec - s * train_batch);
             CK(mlp_grads(mlp, R.rec_feat + (size_t)s * train_batch * kMlpRaw, R.rec_tgt + (size_t)s * train_batch * 3,
@@ -916,6 +918,8 @@ int render_one(ilg_ctx *ctx, const ilg_camera_frame &frame, const ilg_render_opt
         if (cache_depth >= opts->max_depth)
             return fail(ctx, ILG_EINVAL, "ilg_render: cache_depth %u must be below max_depth %u", cache_depth, opts->max_depth);
         if (opts->train_tail > 64) return fail(ctx, ILG_EINVAL, "ilg_render: train_tail %u above 64", opts->train_tail);
+        if (opts->train_epochs > 64)
+            return fail(ctx, ILG_EINVAL, "ilg_render: train_epochs %u above 64", opts->train_epochs);
     }
     CK(cudaSetDevice(ctx->device));
     cudaStream_t st = ctx->stream;
@@ -927,7 +931,7 @@ int render_one(ilg_ctx *ctx, const ilg_camera_frame &frame, const ilg_render_opt
     const bool aux = direct_rgb || albedo_rgb;
     rc = run_render(ctx, recs, opts->paths_per_wave, 128, cache_depth, opts->train_every ? opts->train_every : 16u,
                     opts->train_steps, opts->train_batch ? opts->train_batch : 16384u, nullptr, aux,
-                    ctx->counted, opts->train_tail);
+                    ctx->counted, opts->train_tail, opts->train_epochs ? opts->train_epochs : 1u);
     if (rc) return rc;
     const bool dev = (flags & ILG_DEVICE_PTRS) != 0;
     const float4 *sums[3] = {ctx->accum.ptr, ctx->accum_direct.ptr, ctx->accum_albedo.ptr};

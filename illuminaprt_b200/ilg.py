@@ -95,7 +95,7 @@ class ilg_render_opts(ctypes.Structure):
                 ("max_depth", ctypes.c_uint32), ("epsilon", ctypes.c_float), ("seed", ctypes.c_uint32),
                 ("paths_per_wave", ctypes.c_uint32), ("sky", ctypes.c_float * 3), ("cache_depth", ctypes.c_uint32),
                 ("train_every", ctypes.c_uint32), ("train_steps", ctypes.c_uint32), ("train_batch", ctypes.c_uint32),
-                ("train_tail", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 1)]
+                ("train_tail", ctypes.c_uint32), ("train_epochs", ctypes.c_uint32)]
 
 
 ilg_batch_item._fields_ = [("scene", ctypes.c_void_p), ("camera", ilg_camera), ("width", ctypes.c_uint32),
@@ -324,14 +324,14 @@ class GpuSpace:
     def render_region(self, frame: ilg_camera_frame, width: int, height: int, spp: int, region, max_depth: int = 6,
                       epsilon: float = 1e-4, seed: int = 1, sky=(0.0, 0.0, 0.0), aux: bool = True,
                       cache_depth: int = 0, train_every: int = 16, train_steps: int = 4, train_batch: int = 16384,
-                      train_tail: int = 0):
+                      train_tail: int = 0, train_epochs: int = 1):
         """IRenderer::RenderRegion: region = (x, y, w, h) of the width x height image.
         Returns (final, direct, albedo), each (h, w, 3) float32 (direct/albedo None without aux).
         cache_depth > 0 renders with the radiance cache as render() does."""
         x, y, w, h = (int(v) for v in region)
         o = ilg_render_opts(width=width, height=height, spp=spp, max_depth=max_depth, epsilon=epsilon, seed=seed,
                             cache_depth=cache_depth, train_every=train_every, train_steps=train_steps,
-                            train_batch=train_batch, train_tail=train_tail)
+                            train_batch=train_batch, train_tail=train_tail, train_epochs=train_epochs)
         o.sky[:] = list(sky)
         r = ilg_region(x=x, y=y, width=w, height=h)
         final = np.empty((h, w, 3), np.float32)
@@ -360,13 +360,14 @@ class GpuSpace:
     def render(self, camera: dict, width: int, height: int, spp: int, max_depth: int = 6, epsilon: float = 1e-4,
                seed: int = 1, sky=(0.0, 0.0, 0.0), paths_per_wave: int = 0, out=None, cache_depth: int = 0,
                train_every: int = 16, train_steps: int = 4, train_batch: int = 16384, count: bool = False,
-               train_tail: int = 0):
+               train_tail: int = 0, train_epochs: int = 1):
         """Returns (height, width, 3) float32 (or fills `out`, a CUDA tensor, in place).
         cache_depth > 0 renders with the radiance cache (mlp_init first) and trains it afterwards."""
         cam = self._camera(camera, width, height)
         o = ilg_render_opts(width=width, height=height, spp=spp, max_depth=max_depth, epsilon=epsilon, seed=seed,
                             paths_per_wave=paths_per_wave, cache_depth=cache_depth, train_every=train_every,
-                            train_steps=train_steps, train_batch=train_batch, train_tail=train_tail)
+                            train_steps=train_steps, train_batch=train_batch, train_tail=train_tail,
+                            train_epochs=train_epochs)
         o.sky[:] = list(sky)
         if out is not None:
             self._check(self.L.ilg_render(self.h, ctypes.byref(cam), ctypes.byref(o), _ptr(out),

@@ -34,12 +34,13 @@ struct RadianceCacheSettings {
     uint32_t train_batch;   // records per step
     uint32_t train_tail;    // training paths stop into the cache this many vertices after
                             // the query vertex (self-training); 0 = traced to RayDepth
+    uint32_t train_epochs;  // passes over each region's training records
     float learning_rate;
     uint32_t seed;          // network initialisation
 
     RadianceCacheSettings(void)
         : enabled(false), depth(1), train_every(16), train_steps(4), train_batch(16384), train_tail(2),
-          learning_rate(1e-2f), seed(1)
+          train_epochs(2), learning_rate(1e-2f), seed(1)
     {
     }
 };

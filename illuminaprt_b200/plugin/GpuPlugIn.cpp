@@ -19,8 +19,8 @@
 // Integrator: Id, RayDepth (6), ShadowRays (1), Epsilon (1e-4), as the
 // reference's PathIntegratorFactory (Integrator/IntegratorFactories.h:41-58);
 // Cache (None or MLP, default None), CacheDepth (1), TrainFraction (1/16),
-// TrainSteps (4), TrainBatch (16384), TrainTail (2), LearningRate (0.01),
-// CacheSeed (1).
+// TrainSteps (4), TrainBatch (16384), TrainTail (2), TrainEpochs (2),
+// LearningRate (0.01), CacheSeed (1).
 // Bad values throw the engine's Exception, as its factories do.
 #include <cmath>
 #include <string>
@@ -76,7 +76,7 @@ public:
 
     IIntegrator *CreateInstance(ArgumentMap &p_argumentMap)
     {
-        int depth = 6, shadow = 1, cache_depth = 1, steps = 4, batch = 16384, tail = 2, seed = 1;
+        int depth = 6, shadow = 1, cache_depth = 1, steps = 4, batch = 16384, tail = 2, epochs = 2, seed = 1;
         float epsilon = 1e-4f, fraction = 1.f / 16.f, lr = 1e-2f;
         std::string id, cache = "None";
         p_argumentMap.GetArgument("RayDepth", depth);
@@ -88,6 +88,7 @@ public:
         p_argumentMap.GetArgument("TrainSteps", steps);
         p_argumentMap.GetArgument("TrainBatch", batch);
         p_argumentMap.GetArgument("TrainTail", tail);
+        p_argumentMap.GetArgument("TrainEpochs", epochs);
         p_argumentMap.GetArgument("LearningRate", lr);
         p_argumentMap.GetArgument("CacheSeed", seed);
 
@@ -100,14 +101,16 @@ public:
             throw new Exception("GpuPathIntegratorFactory: CacheDepth must be at least 1 and below RayDepth");
         if (!(fraction > 0.f && fraction <= 1.f))
             throw new Exception("GpuPathIntegratorFactory: TrainFraction must be in (0, 1]");
-        if (steps < 0 || batch < 1 || !(lr > 0.f) || tail < 0 || tail > 64)
+        if (steps < 0 || batch < 1 || !(lr > 0.f) || tail < 0 || tail > 64 || epochs < 1 || epochs > 64)
             throw new Exception(
-                "GpuPathIntegratorFactory: TrainSteps >= 0, TrainBatch >= 1, TrainTail 0..64, LearningRate > 0");
+                "GpuPathIntegratorFactory: TrainSteps >= 0, TrainBatch >= 1, TrainTail 0..64, TrainEpochs 1..64, "
+                "LearningRate > 0");
         c.depth = (uint32_t)cache_depth;
         c.train_every = (uint32_t)std::max(1.f, std::floor(1.f / fraction + 0.5f));
         c.train_steps = (uint32_t)steps;
         c.train_batch = (uint32_t)batch;
         c.train_tail = (uint32_t)tail;
+        c.train_epochs = (uint32_t)epochs;
         c.learning_rate = lr;
         c.seed = (uint32_t)seed;
         if (p_argumentMap.GetArgument("Id", id)) return new GpuPathIntegrator(id, depth, shadow, epsilon, c);

@@ -193,6 +193,7 @@ void GpuRenderer::RenderRegion(RadianceBuffer *p_pRadianceBuffer, int p_nRegionX
         opts.train_steps = c.train_steps;
         opts.train_batch = c.train_batch;
         opts.train_tail = c.train_tail;
+        opts.train_epochs = c.train_epochs;
     }
     ilg_region region = {(uint32_t)p_nRegionX, (uint32_t)p_nRegionY, (uint32_t)p_nRegionWidth,
                          (uint32_t)p_nRegionHeight};

@@ -197,7 +197,9 @@ typedef struct ilg_render_opts {
      * completes their targets (self-training; the frame then ends at that
      * depth) */
     uint32_t train_tail;
-    uint32_t reserved[1];
+    /* passes over the call's training records (0 = 1): each pass runs the
+     * same train_steps Adam steps on the same records again */
+    uint32_t train_epochs;
 } ilg_render_opts;
 
 /* Materials indexed by the mat_ids given to ilg_set_mesh. */
