@@ -132,7 +132,8 @@ def test_gpu_integrator_is_the_reference_path_integrator_under_cpu_renderers(tmp
 @needs_ref
 @pytest.mark.skipif(not os.path.exists(pkg_build.PLUGIN), reason="plug-in not built")
 @pytest.mark.parametrize("args", [{"Cache": "Octree"}, {"Cache": "MLP", "CacheDepth": 6},
-                                  {"TrainFraction": 0}, {"LearningRate": -1}, {"TrainTail": -1}])
+                                  {"TrainFraction": 0}, {"LearningRate": -1}, {"TrainTail": -1},
+                                  {"TrainEpochs": 0}])
 def test_gpu_integrator_factory_refuses_bad_settings(tmp_path, args):
     # the factory throws; the loader reports it and binds no integrator
     script = scenes.write_box_script(tmp_path, width=16, height=16, spp=1, space="Basic", renderer="Basic",
