@@ -41,3 +41,18 @@ def test_create_without_gpu_fails_loudly():
     from illuminaprt_b200.ilg import GpuSpace, IlgError
     with pytest.raises(IlgError):
         GpuSpace()
+
+
+def test_binding_constants_match_the_header():
+    # every #define of the C ABI that the Python binding also names has the
+    # same value there (flags, material kinds, sizes)
+    from illuminaprt_b200 import ilg
+    text = open(os.path.join(ROOT, "include", "ilg.h")).read()
+    defines = {m.group(1): int(m.group(2), 0) for m in re.finditer(r"#define (ILG_\w+) (0x[0-9a-fA-F]+|\d+)u", text)}
+    shared = [k for k in defines if hasattr(ilg, k)]
+    assert {"ILG_MAT_MIRROR", "ILG_MAT_GLASS", "ILG_DEVICE_PTRS", "ILG_WATERTIGHT"} <= set(shared), shared
+    for k in shared:
+        assert getattr(ilg, k) == defines[k], k
+    # the option structs have the header's layout size
+    assert ctypes.sizeof(ilg.ilg_render_opts) == 4 * (7 + 3 + 6)
+    assert ctypes.sizeof(ilg.ilg_material) == 32
