@@ -308,6 +308,21 @@ def bench_cache(res, local):
         "gain_train_tail_2": round(tail2["gain"], 3), "gain_full_depth_training": round(full["gain"], 3),
         "accumulation": "device"}
     sp.close()
+    # the same comparison at 1920x1080 (4 Adam steps of 16384 records, two passes)
+    w, h = 1920, 1080
+    field = scenes.sphere_field(8, 7, seed=3, width=w, height=h)
+    sp = GpuSpace(device=local)
+    scenes.load_sphere_field(sp, field)
+    gt = sp.render(dict(field["camera"], aspect=w / h), w, h, 4096, max_depth=12, seed=424242, sky=field["sky"])
+    r = equal_time(sp, field, w, h, gt, frames=64, warmup=8, cache_depth=1, train_steps=4, train_batch=16384,
+                   train_tail=1, train_epochs=2, device_accumulate=True)
+    res["cache_equal_time_1080p"] = {
+        "scene": "icosphere field 1920x1080, ground truth 4096 spp", "relmse_plain": round(r["relmse_plain"], 6),
+        "relmse_cached": round(r["relmse_cached"], 6), "gain": round(r["gain"], 3),
+        "bias_cached": [round(b, 5) for b in r["bias_cached"]], "seconds": round(r["seconds_cached"], 4),
+        "frames_cached": r["frames_cached"], "frames_plain": r["frames_plain"], "train_tail": 1, "train_epochs": 2,
+        "accumulation": "device"}
+    sp.close()
     try:
         res["cache_equal_time"]["cpu_baseline"] = ic_cpu_baseline()
     except (FileNotFoundError, OSError, RuntimeError) as e:
