@@ -284,7 +284,8 @@ def bench_cache(res, local):
     steps of 32768 records per frame run twice over the frame's records,
     training paths stopping into the cache one vertex later (self-training);
     one pass, a two-vertex tail and training paths traced to full depth are
-    reported beside it. Frames accumulate on the device, as a
+    reported beside it, and the non-learned hash-grid cache in the network's
+    place (ILG_RENDER_HASH_CACHE). Frames accumulate on the device, as a
     progressive renderer's accumulation buffer does, in both runs."""
     from illuminaprt_b200 import scenes
     from illuminaprt_b200.cache_experiment import equal_time
@@ -299,6 +300,7 @@ def bench_cache(res, local):
     one_pass = equal_time(sp, field, w, h, gt, train_tail=1, **kw)
     tail2 = equal_time(sp, field, w, h, gt, train_tail=2, train_epochs=2, **kw)
     full = equal_time(sp, field, w, h, gt, **kw)
+    hashed = equal_time(sp, field, w, h, gt, train_tail=1, hash_cache=True, **kw)
     res["cache_equal_time"] = {
         "scene": "icosphere field 480x270, ground truth 4096 spp", "relmse_plain": round(r["relmse_plain"], 6),
         "relmse_cached": round(r["relmse_cached"], 6), "gain": round(r["gain"], 3),
@@ -306,6 +308,7 @@ def bench_cache(res, local):
         "frames_cached": r["frames_cached"], "frames_plain": r["frames_plain"], "train_tail": 1,
         "train_epochs": 2, "gain_one_pass": round(one_pass["gain"], 3),
         "gain_train_tail_2": round(tail2["gain"], 3), "gain_full_depth_training": round(full["gain"], 3),
+        "gain_hash_grid_cache": round(hashed["gain"], 3), "bias_hash_grid_cache": [round(b, 5) for b in hashed["bias_cached"]],
         "accumulation": "device"}
     sp.close()
     # the same comparison at 1920x1080 (4 Adam steps of 16384 records, two passes)

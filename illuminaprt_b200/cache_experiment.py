@@ -25,7 +25,7 @@ def rel_mse(x, gt, eps=1e-2):
 
 def equal_time(space, scene, width, height, gt, frames=64, warmup=8, spp_per_frame=1, cache_depth=1,
                train_every=16, train_steps=4, train_batch=16384, max_depth=12, seed=100, lr=1e-2,
-               ablate_training=False, train_tail=0, device_accumulate=False, train_epochs=1):
+               ablate_training=False, train_tail=0, device_accumulate=False, train_epochs=1, hash_cache=False):
     """device_accumulate: frames are rendered into a device tensor and summed
     on the device (as a progressive renderer's accumulation buffer would be),
     with a synchronisation after every frame in both runs; otherwise each
@@ -62,11 +62,12 @@ def equal_time(space, scene, width, height, gt, frames=64, warmup=8, spp_per_fra
 
     cache_kw = dict(cache_depth=cache_depth, train_every=train_every,
                     train_steps=0 if ablate_training else train_steps, train_batch=train_batch,
-                    train_tail=train_tail, train_epochs=train_epochs)
-    space.mlp_init(seed=seed, lr=lr)
+                    train_tail=train_tail, train_epochs=train_epochs, hash_cache=hash_cache)
+    reset_cache = space.hash_cache_reset if hash_cache else (lambda: space.mlp_init(seed=seed, lr=lr))
+    reset_cache()
     # untimed: first call allocates the wavefront and cache buffers
     frame(seed=seed + 99991, keep=False, **cache_kw)
-    space.mlp_init(seed=seed, lr=lr)
+    reset_cache()
     acc = reset()
     n_acc = 0
     t0 = time.perf_counter()

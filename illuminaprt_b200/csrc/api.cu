@@ -736,7 +736,7 @@ static int prepare_scene(ilg_ctx *runner, ilg_ctx *ctx, const ilg_camera_frame &
 static int run_render(ilg_ctx *ctx, std::vector<SceneRec> &recs, uint32_t cap_req, uint32_t block,
                       uint32_t cache_depth, uint32_t train_every, uint32_t train_steps, uint32_t train_batch,
                       uint64_t *total_paths_out, bool aux = false, bool count = false, uint32_t train_tail = 0,
-                      uint32_t train_epochs = 1)
+                      uint32_t train_epochs = 1, bool hash_cache = false)
 {
     cudaStream_t st = ctx->stream;
     uint64_t total = 0, pixels64 = 0;
@@ -816,7 +816,7 @@ static int run_render(ilg_ctx *ctx, std::vector<SceneRec> &recs, uint32_t cap_re
         CK(ctx->qry_beta.reserve(cap));
         CK(ctx->qry_meta.reserve(cap));
         CK(ctx->mlp_enc.reserve((size_t)cap * kGridLevels));
-        {
+        if (!hash_cache) {
             int rc = mlp_reserve_train(ctx, train_batch);
             if (rc) return rc;
         }
@@ -824,6 +824,11 @@ static int run_render(ilg_ctx *ctx, std::vector<SceneRec> &recs, uint32_t cap_re
         R.train_every = train_every;
         R.train_tail = train_tail;
         R.qry_meta = ctx->qry_meta.ptr;
+        if (hash_cache) {
+            if (!ctx->hc_keys.ptr) return fail(ctx, ILG_ESTATE, "render: hash cache not reset (ilg_hash_cache_reset)");
+            R.hc_keys = ctx->hc_keys.ptr;
+            R.hc_vals = ctx->hc_vals.ptr;
+        }
         R.scene_lo = make_float3(ctx->scene_lo[0], ctx->scene_lo[1], ctx->scene_lo[2]);
         R.scene_inv_ext = make_float3(1.f / std::max(ctx->scene_hi[0] - ctx->scene_lo[0], 1e-20f),
                                       1.f / std::max(ctx->scene_hi[1] - ctx->scene_lo[1], 1e-20f),
@@ -889,6 +894,11 @@ static int run_render(ilg_ctx *ctx, std::vector<SceneRec> &recs, uint32_t cap_re
         CK(cudaStreamSynchronize(st));
         n_rec = std::min(n_rec, R.rec_cap);
         ctx->last_train_records = n_rec;
+        if (hash_cache) {
+            CK(hash_cache_update(R, n_rec, st));
+            launches += 1;
+            train_epochs = 0;
+        }
         for (uint32_t ep = 0; ep < train_epochs; ep++)
         for (uint32_t s = 0; s < train_steps && (uint64_t)s * train_batch < n_rec; s++) {
             const uint32_t nb = std::min(train_batch, n_rec - s * train_batch);
@@ -912,9 +922,14 @@ int render_one(ilg_ctx *ctx, const ilg_camera_frame &frame, const ilg_render_opt
                float *final_rgb, float *direct_rgb, float *albedo_rgb, uint32_t flags)
 {
     ctx->counted = (flags & ILG_RENDER_COUNT) != 0;
+    const bool hash_cache = (flags & ILG_RENDER_HASH_CACHE) != 0;
     const uint32_t cache_depth = opts->cache_depth;
+    if (hash_cache && !cache_depth) return fail(ctx, ILG_EINVAL, "ilg_render: ILG_RENDER_HASH_CACHE needs cache_depth");
     if (cache_depth) {
-        if (!ctx->mlp_ready) return fail(ctx, ILG_ESTATE, "ilg_render: cache_depth set but ilg_mlp_init not called");
+        if (!hash_cache && !ctx->mlp_ready)
+            return fail(ctx, ILG_ESTATE, "ilg_render: cache_depth set but ilg_mlp_init not called");
+        if (hash_cache && !ctx->hc_keys.ptr)
+            return fail(ctx, ILG_ESTATE, "ilg_render: ILG_RENDER_HASH_CACHE but ilg_hash_cache_reset not called");
         if (cache_depth >= opts->max_depth)
             return fail(ctx, ILG_EINVAL, "ilg_render: cache_depth %u must be below max_depth %u", cache_depth, opts->max_depth);
         if (opts->train_tail > 64) return fail(ctx, ILG_EINVAL, "ilg_render: train_tail %u above 64", opts->train_tail);
@@ -931,7 +946,7 @@ int render_one(ilg_ctx *ctx, const ilg_camera_frame &frame, const ilg_render_opt
     const bool aux = direct_rgb || albedo_rgb;
     rc = run_render(ctx, recs, opts->paths_per_wave, 128, cache_depth, opts->train_every ? opts->train_every : 16u,
                     opts->train_steps, opts->train_batch ? opts->train_batch : 16384u, nullptr, aux,
-                    ctx->counted, opts->train_tail, opts->train_epochs ? opts->train_epochs : 1u);
+                    ctx->counted, opts->train_tail, opts->train_epochs ? opts->train_epochs : 1u, hash_cache);
     if (rc) return rc;
     const bool dev = (flags & ILG_DEVICE_PTRS) != 0;
     const float4 *sums[3] = {ctx->accum.ptr, ctx->accum_direct.ptr, ctx->accum_albedo.ptr};
@@ -966,7 +981,8 @@ int ilg_render(ilg_ctx *ctx, const ilg_camera *cam, const ilg_render_opts *opts,
 {
     if (!ctx) return ILG_EINVAL;
     if (!cam || !opts || !out_rgb) return fail(ctx, ILG_EINVAL, "ilg_render: null argument");
-    if (flags & ~(ILG_DEVICE_PTRS | ILG_RENDER_COUNT)) return fail(ctx, ILG_EINVAL, "ilg_render: unknown flags 0x%x", flags);
+    if (flags & ~(ILG_DEVICE_PTRS | ILG_RENDER_COUNT | ILG_RENDER_HASH_CACHE))
+        return fail(ctx, ILG_EINVAL, "ilg_render: unknown flags 0x%x", flags);
     ilg_camera_frame frame;
     camera_frame_of(*cam, frame);
     const ilg_region whole = {0u, 0u, opts->width, opts->height};
@@ -989,8 +1005,21 @@ int ilg_render_region(ilg_ctx *ctx, const ilg_camera_frame *frame, const ilg_ren
 {
     if (!ctx) return ILG_EINVAL;
     if (!frame || !opts || !region || !final_rgb) return fail(ctx, ILG_EINVAL, "ilg_render_region: null argument");
-    if (flags & ~ILG_DEVICE_PTRS) return fail(ctx, ILG_EINVAL, "ilg_render_region: unknown flags 0x%x", flags);
+    if (flags & ~(ILG_DEVICE_PTRS | ILG_RENDER_HASH_CACHE))
+        return fail(ctx, ILG_EINVAL, "ilg_render_region: unknown flags 0x%x", flags);
     return render_one(ctx, *frame, opts, *region, final_rgb, direct_rgb, albedo_rgb, flags);
+}
+
+int ilg_hash_cache_reset(ilg_ctx *ctx)
+{
+    if (!ctx) return ILG_EINVAL;
+    CK(cudaSetDevice(ctx->device));
+    CK(ctx->hc_keys.reserve(kHashCacheCells));
+    CK(ctx->hc_vals.reserve(kHashCacheCells));
+    CK(cudaMemsetAsync(ctx->hc_keys.ptr, 0, sizeof(unsigned long long) * kHashCacheCells, ctx->stream));
+    CK(cudaMemsetAsync(ctx->hc_vals.ptr, 0, sizeof(float4) * kHashCacheCells, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return ILG_OK;
 }
 
 int ilg_render_batch(ilg_ctx *runner, const ilg_batch_item *items, uint32_t n, uint32_t paths_per_wave,

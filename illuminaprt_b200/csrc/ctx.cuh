@@ -69,6 +69,9 @@ struct ilg_ctx {
     ilg::DevBuf<float> hit_t, out_dev;
     // path tracing with the radiance cache
     ilg::DevBuf<uint32_t> train_slot, rec_of, s_meta, qry_meta;
+    // hash-grid radiance cache (ILG_RENDER_HASH_CACHE)
+    ilg::DevBuf<unsigned long long> hc_keys;
+    ilg::DevBuf<float4> hc_vals;
     ilg::DevBuf<float> rec_feat, rec_tgt, qry_feat, qry_out;
     ilg::DevBuf<float4> rec_beta, qry_beta;
     uint32_t last_train_records = 0;
@@ -147,6 +150,7 @@ struct ilg_ctx {
         hit_tri.release(); hit_t.release(); out_dev.release(); path_scene.release(); s_sid.release();
         scene_table.release();
         train_slot.release(); rec_of.release(); s_meta.release(); qry_meta.release(); rec_feat.release();
+        hc_keys.release(); hc_vals.release();
         rec_tgt.release();
         qry_feat.release(); qry_out.release(); rec_beta.release(); qry_beta.release();
         mlp_w.release(); mlp_m.release(); mlp_v.release(); mlp_grad.release(); mlp_loss.release();

@@ -745,6 +745,86 @@ cudaError_t build_tri_attr(const uint32_t *prim_of, uint32_t n_tris, const uint3
     return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// Hash-grid radiance cache: a non-learned stand-in for the network, the
+// baseline the learned cache is measured against. A cell is a voxel of the
+// scene's bounding box (256 per axis) crossed with the normal's dominant
+// axis and sign (6) and the octant of the outgoing direction (8); it holds
+// the running mean of the training records that fell in it. Lookup is
+// open addressing over kHashCacheCells cells, 8 probes; a query that finds
+// no filled cell answers 0.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned long long hc_key(const float *f)
+{
+    const uint32_t x = (uint32_t)fminf(fmaxf(f[0] * 256.f, 0.f), 255.f);
+    const uint32_t y = (uint32_t)fminf(fmaxf(f[1] * 256.f, 0.f), 255.f);
+    const uint32_t z = (uint32_t)fminf(fmaxf(f[2] * 256.f, 0.f), 255.f);
+    const float ax = fabsf(f[6]), ay = fabsf(f[7]), az = fabsf(f[8]);
+    const uint32_t axis = ax >= ay && ax >= az ? 0u : (ay >= az ? 1u : 2u);
+    const uint32_t nsign = (axis == 0u ? f[6] : axis == 1u ? f[7] : f[8]) < 0.f ? 1u : 0u;
+    const uint32_t oct = (f[3] < 0.f ? 1u : 0u) | (f[4] < 0.f ? 2u : 0u) | (f[5] < 0.f ? 4u : 0u);
+    return (unsigned long long)x | ((unsigned long long)y << 8) | ((unsigned long long)z << 16) |
+           ((unsigned long long)(axis * 2u + nsign) << 24) | ((unsigned long long)oct << 27);
+}
+
+__device__ __forceinline__ uint32_t hc_slot(unsigned long long key, uint32_t mask)
+{
+    unsigned long long h = key * 0x9E3779B97F4A7C15ull;
+    h ^= h >> 29;
+    return (uint32_t)h & mask;
+}
+
+__global__ void k_hc_update(RenderDev R, uint32_t n)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float *f = R.rec_feat + (size_t)i * kMlpRaw;
+    const unsigned long long key = hc_key(f) + 1ull;
+    const uint32_t mask = kHashCacheCells - 1u;
+    uint32_t s = hc_slot(key, mask);
+    for (int probe = 0; probe < 8; probe++, s = (s + 1u) & mask) {
+        const unsigned long long prev = atomicCAS(R.hc_keys + s, 0ull, key);
+        if (prev == 0ull || prev == key) {
+            float *v = reinterpret_cast<float *>(R.hc_vals + s);
+            atomicAdd(v, fmaxf(R.rec_tgt[3 * i], 0.f));
+            atomicAdd(v + 1, fmaxf(R.rec_tgt[3 * i + 1], 0.f));
+            atomicAdd(v + 2, fmaxf(R.rec_tgt[3 * i + 2], 0.f));
+            atomicAdd(v + 3, 1.f);
+            return;
+        }
+    }
+}
+
+__global__ void k_hc_query(RenderDev R, uint32_t cap)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= *R.qry_count || i >= cap) return;
+    const float *f = R.qry_feat + (size_t)i * kMlpRaw;
+    const unsigned long long key = hc_key(f) + 1ull;
+    const uint32_t mask = kHashCacheCells - 1u;
+    uint32_t s = hc_slot(key, mask);
+    float3 y = make_float3(0.f, 0.f, 0.f);
+    for (int probe = 0; probe < 8; probe++, s = (s + 1u) & mask) {
+        const unsigned long long k = R.hc_keys[s];
+        if (k == 0ull) break;
+        if (k == key) {
+            const float4 v = R.hc_vals[s];
+            if (v.w > 0.f) y = make_float3(v.x / v.w, v.y / v.w, v.z / v.w);
+            break;
+        }
+    }
+    R.qry_out[3 * i] = y.x;
+    R.qry_out[3 * i + 1] = y.y;
+    R.qry_out[3 * i + 2] = y.z;
+}
+
+cudaError_t hash_cache_update(const RenderDev &R, uint32_t n_rec, cudaStream_t st)
+{
+    if (n_rec == 0) return cudaSuccess;
+    k_hc_update<<<blocks_for(n_rec, 256), 256, 0, st>>>(R, n_rec);
+    return cudaGetLastError();
+}
+
 cudaError_t render_wave(const RenderDev &R, uint32_t n_paths, uint64_t wave_begin, cudaStream_t st,
                         uint32_t *launches, const MlpDev *cache, uint32_t block)
 {
@@ -778,7 +858,10 @@ cudaError_t render_wave(const RenderDev &R, uint32_t n_paths, uint64_t wave_begi
         k_shade<<<blocks_for(n_paths, T), T, 0, st>>>(R, cur, depth, wave_begin);
         n_launch += 2;
         if (R.cache_depth && cache && (depth == R.cache_depth || (R.train_tail && depth == tail))) {
-            if ((e = mlp_infer(*cache, R.qry_feat, n_paths, R.qry_out, st, R.qry_count)) != cudaSuccess) return e;
+            if (R.hc_keys)
+                k_hc_query<<<blocks_for(n_paths, 256), 256, 0, st>>>(R, R.capacity);
+            else if ((e = mlp_infer(*cache, R.qry_feat, n_paths, R.qry_out, st, R.qry_count)) != cudaSuccess)
+                return e;
             k_cache_apply<<<blocks_for(n_paths, 128), 128, 0, st>>>(R);
             if ((e = cudaMemsetAsync(R.qry_count, 0, sizeof(uint32_t), st)) != cudaSuccess) return e;
             n_launch += 2;

@@ -100,6 +100,9 @@ struct RenderDev {
     float *qry_out;            // cap x 3 network outputs
     uint32_t *qry_count;
     uint32_t *qry_meta;        // per query: (slot << 8 | vertex) of a training path's tail, or ~0
+    // hash-grid radiance cache (the non-learned baseline; null: the network answers queries)
+    unsigned long long *hc_keys;  // hc_mask + 1 cells: key + 1, 0 = empty
+    float4 *hc_vals;              // per cell: radiance sum (xyz) and sample count (w)
     uint32_t *s_meta;          // per shadow segment: (slot << 8 | vertex) of a training path, or ~0
 };
 
@@ -111,5 +114,10 @@ struct MlpDev;
 cudaError_t render_wave(const RenderDev &R, uint32_t n_paths, uint64_t wave_begin, cudaStream_t st,
                         uint32_t *launches, const MlpDev *cache, uint32_t block = 128);
 cudaError_t render_resolve(const float4 *accum, uint32_t wh, float scale, float *out, cudaStream_t st);
+
+// Hash-grid radiance cache: the n_rec training records of a call (raw
+// features + targets) are added to their cells.
+constexpr uint32_t kHashCacheCells = 1u << 22;
+cudaError_t hash_cache_update(const RenderDev &R, uint32_t n_rec, cudaStream_t st);
 
 }  // namespace ilg

@@ -21,6 +21,7 @@ ILG_OK, ILG_EINVAL, ILG_ENOMEM, ILG_ECUDA, ILG_ETIMEOUT, ILG_EOVERFLOW, ILG_ESTA
 ILG_DEVICE_PTRS = 0x1
 ILG_WATERTIGHT = 0x2
 ILG_RENDER_COUNT = 0x4
+ILG_RENDER_HASH_CACHE = 0x8
 
 STATUS_NAMES = {0: "ILG_OK", 1: "ILG_EINVAL", 2: "ILG_ENOMEM", 3: "ILG_ECUDA", 4: "ILG_ETIMEOUT",
                 5: "ILG_EOVERFLOW", 6: "ILG_ESTATE"}
@@ -33,7 +34,7 @@ EXPORTED = ["ilg_create", "ilg_destroy", "ilg_last_error", "ilg_set_mesh", "ilg_
             "ilg_mlp_train_step", "ilg_render_batch", "ilg_intersect_excluding", "ilg_occluded_excluding",
             "ilg_camera_frame_of", "ilg_render_region", "ilg_mlp_get_grid", "ilg_mlp_set_grid",
             "ilg_mlp_get_grid_grads", "ilg_accumulate", "ilg_accumulate_reset", "ilg_tonemap",
-            "ilg_render_counts", "ilg_save", "ilg_load"]
+            "ilg_render_counts", "ilg_save", "ilg_load", "ilg_hash_cache_reset"]
 
 ILG_MLP_RAW = 16
 ILG_MLP_WARP_MMA = 0x10
@@ -136,6 +137,7 @@ def load(build_if_missing: bool = True) -> ctypes.CDLL:
     L.ilg_render.argtypes = [vp, ctypes.POINTER(ilg_camera), ctypes.POINTER(ilg_render_opts), vp, u32]
     L.ilg_intersect_noalloc.argtypes = [vp, vp, vp, u32, vp, vp, vp, vp]
     L.ilg_render_counts.argtypes = [vp, vp]
+    L.ilg_hash_cache_reset.argtypes = [vp]
     L.ilg_save.argtypes = [vp, ctypes.c_char_p]
     L.ilg_load.argtypes = [vp, ctypes.c_char_p]
     L.ilg_accumulate.argtypes = [vp, vp, u32, vp, u32]
@@ -360,23 +362,29 @@ class GpuSpace:
     def render(self, camera: dict, width: int, height: int, spp: int, max_depth: int = 6, epsilon: float = 1e-4,
                seed: int = 1, sky=(0.0, 0.0, 0.0), paths_per_wave: int = 0, out=None, cache_depth: int = 0,
                train_every: int = 16, train_steps: int = 4, train_batch: int = 16384, count: bool = False,
-               train_tail: int = 0, train_epochs: int = 1):
+               train_tail: int = 0, train_epochs: int = 1, hash_cache: bool = False):
         """Returns (height, width, 3) float32 (or fills `out`, a CUDA tensor, in place).
-        cache_depth > 0 renders with the radiance cache (mlp_init first) and trains it afterwards."""
+        cache_depth > 0 renders with the radiance cache (mlp_init first) and trains it afterwards;
+        with hash_cache the non-learned hash-grid cache stands in for the network
+        (hash_cache_reset first)."""
         cam = self._camera(camera, width, height)
         o = ilg_render_opts(width=width, height=height, spp=spp, max_depth=max_depth, epsilon=epsilon, seed=seed,
                             paths_per_wave=paths_per_wave, cache_depth=cache_depth, train_every=train_every,
                             train_steps=train_steps, train_batch=train_batch, train_tail=train_tail,
                             train_epochs=train_epochs)
         o.sky[:] = list(sky)
+        flags = (ILG_RENDER_COUNT if count else 0) | (ILG_RENDER_HASH_CACHE if hash_cache else 0)
         if out is not None:
             self._check(self.L.ilg_render(self.h, ctypes.byref(cam), ctypes.byref(o), _ptr(out),
-                                          ILG_DEVICE_PTRS | (ILG_RENDER_COUNT if count else 0)))
+                                          ILG_DEVICE_PTRS | flags))
             return out
         img = np.empty((height, width, 3), np.float32)
-        self._check(self.L.ilg_render(self.h, ctypes.byref(cam), ctypes.byref(o), img.ctypes.data,
-                                      ILG_RENDER_COUNT if count else 0))
+        self._check(self.L.ilg_render(self.h, ctypes.byref(cam), ctypes.byref(o), img.ctypes.data, flags))
         return img
+
+    def hash_cache_reset(self):
+        """Empties the hash-grid radiance cache (allocated on first use)."""
+        self._check(self.L.ilg_hash_cache_reset(self.h))
 
     # --- post-processing (AccumulationBuffer, tone operators) ---------------
     TONE = {"global": 0, "auto": 1, "drago": 2}

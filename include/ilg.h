@@ -221,6 +221,19 @@ int ilg_render(ilg_ctx *ctx, const ilg_camera *cam, const ilg_render_opts *opts,
 #define ILG_RENDER_COUNT 0x4u
 int ilg_render_counts(ilg_ctx *ctx, uint64_t counts[6]);
 
+/* ilg_render / ilg_render_region flag: with cache_depth set, a hash-grid
+ * radiance cache answers the cache queries instead of the network: a cell
+ * per voxel of the scene's box (256 per axis) x normal direction (6) x
+ * octant of the outgoing direction (8) holds the running mean of the
+ * training records that fell in it (4 M cells, 80 MB, open addressing); a
+ * query that finds no filled cell answers 0. It is the non-learned baseline
+ * the network is measured against (the reference's own cache, the
+ * irradiance cache of Core/Integrator/ICIntegrator.*, inserts its records
+ * one query at a time). train_steps / train_batch / train_epochs do not
+ * apply; call ilg_hash_cache_reset first. */
+#define ILG_RENDER_HASH_CACHE 0x8u
+int ilg_hash_cache_reset(ilg_ctx *ctx);
+
 /* A camera as the reference's ICamera holds it after construction
  * (Core/Camera/Camera.h:23-28: m_centre, m_corner, m_across, m_up): the ray
  * through normalised image point (px, py) is normalize(corner + across * px

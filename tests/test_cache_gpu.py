@@ -68,6 +68,28 @@ def test_self_training_tails(field):
     assert np.allclose(a, b, rtol=1e-5, atol=1e-6)
 
 
+def test_hash_grid_cache_baseline(field):
+    # the non-learned baseline: an empty hash-grid cache answers 0 (the image
+    # lacks everything past the cache vertex); filled by the training paths
+    # of 40 frames it approaches the truth, and it needs no network
+    from illuminaprt_b200.ilg import IlgError
+    sp, s, gt = field
+    cam = dict(s["camera"], aspect=W / H)
+    kw = dict(max_depth=12, sky=s["sky"], cache_depth=1, hash_cache=True)
+    sp.hash_cache_reset()
+    empty = sp.render(cam, W, H, 64, seed=7, **kw)
+    for f in range(40):
+        img = sp.render(cam, W, H, 1, seed=3000 + f, train_tail=2, **kw)
+        assert np.isfinite(img).all()
+    filled = sp.render(cam, W, H, 64, seed=8, **kw)
+    e0, e1 = rel_mse(empty, gt), rel_mse(filled, gt)
+    print(f"hash-grid cache, 64-spp relMSE empty / after 40 frames: {e0:.4f} / {e1:.4f}")
+    assert e1 < 0.5 * e0
+    assert np.allclose(filled.mean((0, 1)), gt.mean((0, 1)), rtol=0.1)
+    with pytest.raises(IlgError):
+        sp.render(cam, W, H, 1, seed=1, max_depth=12, sky=s["sky"], hash_cache=True)  # needs cache_depth
+
+
 def test_cache_in_regions(field):
     # a frozen cache (train_steps 0): region calls query the same network, so
     # tiles reproduce the whole image's paths; the whole image as one region
