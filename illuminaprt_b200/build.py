@@ -55,7 +55,9 @@ def build(force: bool = False, verbose: bool = False, ptxas_v: bool = False) -> 
 
 PLUGIN_DIR = os.path.join(PKG, "plugin")
 PLUGIN = os.path.join(PLUGIN_DIR, "libilg_gpuspace.so")
-REF_CORE = os.environ.get("ILLUMINA_CORE", "/root/reference/Core")
+# the engine's Core tree: $ILLUMINA_CORE, else a checkout named "reference"
+# beside this repository
+REF_CORE = os.environ.get("ILLUMINA_CORE", os.path.join(os.path.dirname(ROOT), "reference", "Core"))
 
 
 def build_plugin() -> str | None:

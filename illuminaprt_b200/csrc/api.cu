@@ -161,6 +161,12 @@ int ilg_create(ilg_ctx **out, const ilg_opts *opts)
     }
     cudaMemsetAsync(ctx->derr.ptr, 0, 4 * sizeof(uint32_t), ctx->stream);
     cudaStreamSynchronize(ctx->stream);
+    // the allocation-free query's fixed array becomes resident here, not at
+    // its first call; a failure only disables that entry point
+    if (noalloc_prepare(&ctx->noalloc_scratch) != cudaSuccess) {
+        ctx->noalloc_scratch = nullptr;
+        cudaGetLastError();
+    }
     *out = ctx;
     return ILG_OK;
 }
@@ -230,6 +236,7 @@ int ilg_set_mesh(ilg_ctx *ctx, const float *pos_xyz, uint32_t n_verts, const uin
     CK(cudaStreamSynchronize(ctx->stream));
     ctx->n_verts = n_verts;
     ctx->n_tris = n_tris;
+    ctx->mesh_gen++;
     ctx->has_mat = mat_ids != nullptr;
     ctx->max_abs = maxabs;
     ctx->built = false;
@@ -626,40 +633,96 @@ int ilg_set_materials(ilg_ctx *ctx, const ilg_material *mats, uint32_t n)
     return ILG_OK;
 }
 
+int ilg_set_lights(ilg_ctx *ctx, const ilg_light *lights, uint32_t n)
+{
+    if (!ctx) return ILG_EINVAL;
+    if (n > kMaxLights) return fail(ctx, ILG_EINVAL, "ilg_set_lights: at most %u lights", kMaxLights);
+    if (n && !lights) return fail(ctx, ILG_EINVAL, "ilg_set_lights: null lights");
+    Light hl[kMaxLights];
+    uint2 range[kMaxLights];
+    float inf = 0.f;
+    bool uses_mesh = false;
+    CK(cudaSetDevice(ctx->device));
+    for (uint32_t i = 0; i < n; i++) {
+        const ilg_light &L = lights[i];
+        Light &d = hl[i];
+        memset(&d, 0, sizeof(d));
+        d.kind = L.kind;
+        d.emit = make_float3(L.emit[0], L.emit[1], L.emit[2]);
+        if (!(std::isfinite(L.emit[0]) && std::isfinite(L.emit[1]) && std::isfinite(L.emit[2])))
+            return fail(ctx, ILG_EINVAL, "ilg_set_lights: light %u has a non-finite radiance", i);
+        range[i] = make_uint2(0u, 0u);
+        if (L.kind == ILG_LIGHT_QUAD) {
+            if (ctx->n_tris && (uint64_t)L.first_tri + 2 > ctx->n_tris)
+                return fail(ctx, ILG_EINVAL, "ilg_set_lights: light %u triangles out of range", i);
+            V3 p0 = v3(L.v[0]), p1 = v3(L.v[1]), p2 = v3(L.v[2]), p3 = v3(L.v[3]);
+            V3 n0 = cross(p2 - p0, p1 - p0);   // triangle (v1, v3, v2)
+            V3 n1 = cross(p3 - p0, p2 - p0);   // triangle (v1, v4, v3)
+            float area = 0.5f * std::sqrt(dot(n0, n0)) + 0.5f * std::sqrt(dot(n1, n1));
+            if (!(area > 0.f)) return fail(ctx, ILG_EINVAL, "ilg_set_lights: light %u has zero area", i);
+            d.p[0] = f3(p0); d.p[1] = f3(p1); d.p[2] = f3(p2); d.p[3] = f3(p3);
+            d.n = f3(normalize(n0));
+            d.area = area;
+            d.first_tri = L.first_tri;
+            d.tri_count = 2;
+            range[i] = make_uint2(L.first_tri, 2u);
+        } else if (L.kind == ILG_LIGHT_MESH) {
+            if (!ctx->n_tris || L.tri_count == 0 || (uint64_t)L.first_tri + L.tri_count > ctx->n_tris)
+                return fail(ctx, ILG_EINVAL, "ilg_set_lights: mesh light %u triangles out of range", i);
+            // ITriangleMesh::ComputeArea (Core/Shape/TriangleMesh.cpp:163-168): the
+            // triangles' areas summed in order in float
+            ilg::DevBuf<float> areas;
+            CK(areas.reserve(L.tri_count));
+            CK(triangle_areas(ctx->pos.ptr, ctx->idx.ptr, L.first_tri, L.tri_count, areas.ptr, ctx->stream));
+            std::vector<float> ha(L.tri_count);
+            CK(cudaMemcpyAsync(ha.data(), areas.ptr, 4ull * L.tri_count, cudaMemcpyDeviceToHost, ctx->stream));
+            CK(cudaStreamSynchronize(ctx->stream));
+            areas.release();
+            float area = 0.f;
+            for (float a : ha) area += a;
+            if (!(area > 0.f)) return fail(ctx, ILG_EINVAL, "ilg_set_lights: mesh light %u has zero area", i);
+            d.area = area;
+            d.first_tri = L.first_tri;
+            d.tri_count = L.tri_count;
+            range[i] = make_uint2(L.first_tri, L.tri_count);
+            uses_mesh = true;
+        } else if (L.kind == ILG_LIGHT_INFINITE) {
+            inf += 1.f;
+        } else {
+            return fail(ctx, ILG_EINVAL, "ilg_set_lights: light %u has unknown kind %u", i, L.kind);
+        }
+    }
+    CK(ctx->lights.reserve(kMaxLights));
+    CK(ctx->light_range.reserve(kMaxLights));
+    if (n) {
+        CK(cudaMemcpyAsync(ctx->lights.ptr, hl, n * sizeof(Light), cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaMemcpyAsync(ctx->light_range.ptr, range, n * sizeof(uint2), cudaMemcpyHostToDevice, ctx->stream));
+    }
+    CK(cudaStreamSynchronize(ctx->stream));
+    ctx->n_lights = n;
+    memcpy(ctx->light_range_host, range, n * sizeof(uint2));
+    ctx->inf_escape = inf;
+    ctx->lights_use_mesh = uses_mesh;
+    ctx->lights_mesh_gen = ctx->mesh_gen;
+    ctx->attr_dirty = true;
+    return ILG_OK;
+}
+
 int ilg_set_quad_lights(ilg_ctx *ctx, const ilg_quad_light *lights, uint32_t n)
 {
     if (!ctx) return ILG_EINVAL;
     if (n > kMaxLights) return fail(ctx, ILG_EINVAL, "ilg_set_quad_lights: at most %u lights", kMaxLights);
     if (n && !lights) return fail(ctx, ILG_EINVAL, "ilg_set_quad_lights: null lights");
-    QuadLight hl[kMaxLights];
-    uint32_t first[kMaxLights];
+    ilg_light all[kMaxLights];
     for (uint32_t i = 0; i < n; i++) {
-        const ilg_quad_light &L = lights[i];
-        if (ctx->n_tris && (uint64_t)L.first_tri + 1 >= ctx->n_tris)
-            return fail(ctx, ILG_EINVAL, "ilg_set_quad_lights: light %u triangles out of range", i);
-        V3 p0 = v3(L.v[0]), p1 = v3(L.v[1]), p2 = v3(L.v[2]), p3 = v3(L.v[3]);
-        V3 n0 = cross(p2 - p0, p1 - p0);   // triangle (v1, v3, v2)
-        V3 n1 = cross(p3 - p0, p2 - p0);   // triangle (v1, v4, v3)
-        float area = 0.5f * std::sqrt(dot(n0, n0)) + 0.5f * std::sqrt(dot(n1, n1));
-        if (!(area > 0.f)) return fail(ctx, ILG_EINVAL, "ilg_set_quad_lights: light %u has zero area", i);
-        hl[i].p[0] = f3(p0); hl[i].p[1] = f3(p1); hl[i].p[2] = f3(p2); hl[i].p[3] = f3(p3);
-        hl[i].emit = make_float3(L.emit[0], L.emit[1], L.emit[2]);
-        hl[i].n = f3(normalize(n0));
-        hl[i].area = area;
-        first[i] = L.first_tri;
+        memset(&all[i], 0, sizeof(ilg_light));
+        all[i].kind = ILG_LIGHT_QUAD;
+        memcpy(all[i].emit, lights[i].emit, sizeof(all[i].emit));
+        memcpy(all[i].v, lights[i].v, sizeof(all[i].v));
+        all[i].first_tri = lights[i].first_tri;
+        all[i].tri_count = 2;
     }
-    CK(cudaSetDevice(ctx->device));
-    CK(ctx->lights.reserve(kMaxLights));
-    CK(ctx->light_first_tri.reserve(kMaxLights));
-    if (n) {
-        CK(cudaMemcpyAsync(ctx->lights.ptr, hl, n * sizeof(QuadLight), cudaMemcpyHostToDevice, ctx->stream));
-        CK(cudaMemcpyAsync(ctx->light_first_tri.ptr, first, n * sizeof(uint32_t), cudaMemcpyHostToDevice, ctx->stream));
-    }
-    CK(cudaStreamSynchronize(ctx->stream));
-    ctx->n_lights = n;
-    memcpy(ctx->light_first_host, first, n * sizeof(uint32_t));
-    ctx->attr_dirty = true;
-    return ILG_OK;
+    return ilg_set_lights(ctx, n ? all : nullptr, n);
 }
 
 // The camera frame PerspectiveCamera(eye, normalize(target - eye), up,
@@ -706,13 +769,15 @@ static int prepare_scene(ilg_ctx *runner, ilg_ctx *ctx, const ilg_camera_frame &
         return fail(runner, ILG_EINVAL, "ilg_render: region %u,%u %ux%u outside the %ux%u image", rx, ry, rw, rh, W, H);
     if (max_depth == 0 || max_depth > 64) return fail(runner, ILG_EINVAL, "ilg_render: max_depth must be 1..64");
     for (uint32_t l = 0; l < ctx->n_lights; l++)
-        if ((uint64_t)ctx->light_first_host[l] + 1 >= ctx->n_tris)
+        if ((uint64_t)ctx->light_range_host[l].x + ctx->light_range_host[l].y > ctx->n_tris)
             return fail(runner, ILG_EINVAL, "ilg_render: light %u triangles out of range of the mesh", l);
+    if (ctx->lights_use_mesh && ctx->lights_mesh_gen != ctx->mesh_gen)
+        return fail(runner, ILG_ESTATE, "ilg_render: mesh lights were set for an earlier mesh (call ilg_set_lights again)");
     const uint32_t n = ctx->n_tris;
     if (ctx->attr_dirty) {
         CK2(runner, ctx->tri_attr.reserve(n));
         CK2(runner, ctx->light_of_prim.reserve(n));
-        CK2(runner, build_tri_attr(ctx->bb.prim_of, n, ctx->mat.ptr, ctx->light_first_tri.ptr, ctx->n_lights,
+        CK2(runner, build_tri_attr(ctx->bb.prim_of, n, ctx->mat.ptr, ctx->light_range.ptr, ctx->n_lights,
                                    ctx->light_of_prim.ptr, ctx->tri_attr.ptr, st));
         ctx->attr_dirty = false;
     }
@@ -721,6 +786,8 @@ static int prepare_scene(ilg_ctx *runner, ilg_ctx *ctx, const ilg_camera_frame &
     S.tri_attr = ctx->tri_attr.ptr; S.mats = ctx->mats.ptr; S.n_mats = ctx->n_mats;
     S.lights = ctx->lights.ptr; S.n_lights = ctx->n_lights;
     S.sky = make_float3(sky[0], sky[1], sky[2]);
+    S.inf_escape = ctx->inf_escape;
+    S.pos = ctx->pos.ptr; S.idx = ctx->idx.ptr;
     S.centre = make_float3(cam.centre[0], cam.centre[1], cam.centre[2]);
     S.corner = make_float3(cam.corner[0], cam.corner[1], cam.corner[2]);
     S.across = make_float3(cam.across[0], cam.across[1], cam.across[2]);
@@ -768,7 +835,7 @@ static int run_render(ilg_ctx *ctx, std::vector<SceneRec> &recs, uint32_t cap_re
     CK(ctx->hit_tri.reserve(cap)); CK(ctx->hit_t.reserve(cap)); CK(ctx->path_scene.reserve(cap));
     CK(ctx->s_o.reserve((size_t)cap * nl)); CK(ctx->s_d.reserve((size_t)cap * nl)); CK(ctx->s_c.reserve((size_t)cap * nl));
     CK(ctx->s_sid.reserve((size_t)cap * nl));
-    CK(ctx->counts.reserve(8)); CK(ctx->accum.reserve((size_t)pixels + 1));
+    CK(ctx->counts.reserve(9)); CK(ctx->accum.reserve((size_t)pixels + 1));
     CK(ctx->scene_table.reserve(recs.size()));
     CK(cudaMemcpyAsync(ctx->scene_table.ptr, recs.data(), recs.size() * sizeof(SceneRec), cudaMemcpyHostToDevice, st));
     CK(cudaMemsetAsync(ctx->accum.ptr, 0, sizeof(float4) * ((size_t)pixels + 1), st));
@@ -828,6 +895,7 @@ static int run_render(ilg_ctx *ctx, std::vector<SceneRec> &recs, uint32_t cap_re
             if (!ctx->hc_keys.ptr) return fail(ctx, ILG_ESTATE, "render: hash cache not reset (ilg_hash_cache_reset)");
             R.hc_keys = ctx->hc_keys.ptr;
             R.hc_vals = ctx->hc_vals.ptr;
+            R.hc_dropped = ctx->counts.ptr + 8;
         }
         R.scene_lo = make_float3(ctx->scene_lo[0], ctx->scene_lo[1], ctx->scene_lo[2]);
         R.scene_inv_ext = make_float3(1.f / std::max(ctx->scene_hi[0] - ctx->scene_lo[0], 1e-20f),
@@ -894,7 +962,9 @@ static int run_render(ilg_ctx *ctx, std::vector<SceneRec> &recs, uint32_t cap_re
         CK(cudaStreamSynchronize(st));
         n_rec = std::min(n_rec, R.rec_cap);
         ctx->last_train_records = n_rec;
+        ctx->last_hash_update = hash_cache;
         if (hash_cache) {
+            CK(cudaMemsetAsync(R.hc_dropped, 0, sizeof(uint32_t), st));
             CK(hash_cache_update(R, n_rec, st));
             launches += 1;
             train_epochs = 0;
@@ -919,7 +989,8 @@ namespace {
 
 // One scene, one region: the body of ilg_render and ilg_render_region.
 int render_one(ilg_ctx *ctx, const ilg_camera_frame &frame, const ilg_render_opts *opts, const ilg_region &reg,
-               float *final_rgb, float *direct_rgb, float *albedo_rgb, uint32_t flags)
+               float *final_rgb, float *direct_rgb, float *albedo_rgb, uint32_t flags,
+               const float4 *ray_o = nullptr, const float4 *ray_d = nullptr)
 {
     ctx->counted = (flags & ILG_RENDER_COUNT) != 0;
     const bool hash_cache = (flags & ILG_RENDER_HASH_CACHE) != 0;
@@ -942,6 +1013,8 @@ int render_one(ilg_ctx *ctx, const ilg_camera_frame &frame, const ilg_render_opt
     int rc = prepare_scene(ctx, ctx, frame, opts->width, opts->height, reg.x, reg.y, reg.width, reg.height,
                            opts->spp, opts->max_depth, opts->epsilon, opts->seed, opts->sky, st, recs[0]);
     if (rc) return rc;
+    recs[0].ray_o = ray_o;
+    recs[0].ray_d = ray_d;
     const uint32_t wh = recs[0].wh;
     const bool aux = direct_rgb || albedo_rgb;
     rc = run_render(ctx, recs, opts->paths_per_wave, 128, cache_depth, opts->train_every ? opts->train_every : 16u,
@@ -1010,6 +1083,50 @@ int ilg_render_region(ilg_ctx *ctx, const ilg_camera_frame *frame, const ilg_ren
     return render_one(ctx, *frame, opts, *region, final_rgb, direct_rgb, albedo_rgb, flags);
 }
 
+int ilg_radiance(ilg_ctx *ctx, const float *ray_o_tmin, const float *ray_d_tmax, uint32_t n,
+                 const ilg_render_opts *opts, float *final_rgb, float *direct_rgb, float *albedo_rgb, uint32_t flags)
+{
+    if (!ctx) return ILG_EINVAL;
+    if (!ray_o_tmin || !ray_d_tmax || !opts || !final_rgb) return fail(ctx, ILG_EINVAL, "ilg_radiance: null argument");
+    if (flags & ~(ILG_DEVICE_PTRS | ILG_RENDER_HASH_CACHE))
+        return fail(ctx, ILG_EINVAL, "ilg_radiance: unknown flags 0x%x", flags);
+    if (n == 0) return ILG_OK;
+    if (n > (1u << 26)) return fail(ctx, ILG_EINVAL, "ilg_radiance: %u rays exceed 2^26", n);
+    const bool dev = (flags & ILG_DEVICE_PTRS) != 0;
+    if (((uintptr_t)ray_o_tmin | (uintptr_t)ray_d_tmax) & 15u)
+        return fail(ctx, ILG_EINVAL, "ilg_radiance: ray arrays must be 16-byte aligned");
+    CK(cudaSetDevice(ctx->device));
+    const float4 *ro = (const float4 *)ray_o_tmin, *rd = (const float4 *)ray_d_tmax;
+    if (!dev) {
+        CK(ctx->ro.reserve(n));
+        CK(ctx->rd.reserve(n));
+        CK(cudaMemcpyAsync(ctx->ro.ptr, ray_o_tmin, 16ull * n, cudaMemcpyHostToDevice, ctx->stream));
+        CK(cudaMemcpyAsync(ctx->rd.ptr, ray_d_tmax, 16ull * n, cudaMemcpyHostToDevice, ctx->stream));
+        ro = ctx->ro.ptr;
+        rd = ctx->rd.ptr;
+    }
+    ilg_render_opts o = *opts;
+    o.width = n;
+    o.height = 1;
+    ilg_camera_frame frame;
+    memset(&frame, 0, sizeof(frame));
+    const ilg_region whole = {0u, 0u, n, 1u};
+    return render_one(ctx, frame, &o, whole, final_rgb, direct_rgb, albedo_rgb, flags, ro, rd);
+}
+
+int ilg_last_train_stats(ilg_ctx *ctx, uint32_t *records, uint32_t *dropped)
+{
+    if (!ctx || !records || !dropped) return ILG_EINVAL;
+    *records = ctx->last_train_records;
+    *dropped = 0;
+    if (ctx->last_hash_update && ctx->counts.ptr) {
+        CK(cudaSetDevice(ctx->device));
+        CK(cudaMemcpyAsync(dropped, ctx->counts.ptr + 8, sizeof(uint32_t), cudaMemcpyDeviceToHost, ctx->stream));
+        CK(cudaStreamSynchronize(ctx->stream));
+    }
+    return ILG_OK;
+}
+
 int ilg_hash_cache_reset(ilg_ctx *ctx)
 {
     if (!ctx) return ILG_EINVAL;
@@ -1027,7 +1144,8 @@ int ilg_render_batch(ilg_ctx *runner, const ilg_batch_item *items, uint32_t n, u
 {
     if (!runner) return ILG_EINVAL;
     if (!items || n == 0 || n > 4096) return fail(runner, ILG_EINVAL, "ilg_render_batch: need 1..4096 items");
-    if (flags & ~ILG_DEVICE_PTRS) return fail(runner, ILG_EINVAL, "ilg_render_batch: unknown flags 0x%x", flags);
+    if (flags & ~(ILG_DEVICE_PTRS | ILG_RENDER_COUNT))
+        return fail(runner, ILG_EINVAL, "ilg_render_batch: unknown flags 0x%x", flags);
     if (block != 0 && block != 64 && block != 128 && block != 256)
         return fail(runner, ILG_EINVAL, "ilg_render_batch: block must be 64, 128 or 256");
     CK2(runner, cudaSetDevice(runner->device));
@@ -1042,7 +1160,9 @@ int ilg_render_batch(ilg_ctx *runner, const ilg_batch_item *items, uint32_t n, u
                                it.max_depth, it.epsilon, it.seed, it.sky, st, recs[i]);
         if (rc) return rc;
     }
-    int rc = run_render(runner, recs, paths_per_wave, block ? block : 128, 0, 16, 0, 16384, nullptr);
+    runner->counted = (flags & ILG_RENDER_COUNT) != 0;
+    int rc = run_render(runner, recs, paths_per_wave, block ? block : 128, 0, 16, 0, 16384, nullptr, false,
+                        runner->counted);
     if (rc) return rc;
     uint32_t max_wh = 0;
     for (auto &S : recs) max_wh = std::max(max_wh, S.wh);
@@ -1160,9 +1280,19 @@ extern "C" {
 
 int ilg_mlp_init(ilg_ctx *ctx, uint32_t seed, float learning_rate)
 {
+    return ilg_mlp_init_encoding(ctx, seed, learning_rate, ILG_MLP_ENC_HASHGRID);
+}
+
+int ilg_mlp_init_encoding(ilg_ctx *ctx, uint32_t seed, float learning_rate, uint32_t encoding)
+{
     if (!ctx) return ILG_EINVAL;
     if (!(learning_rate > 0.f)) return fail(ctx, ILG_EINVAL, "ilg_mlp_init: learning rate must be > 0");
+    if (encoding != ILG_MLP_ENC_HASHGRID && encoding != ILG_MLP_ENC_FREQ12)
+        return fail(ctx, ILG_EINVAL, "ilg_mlp_init: unknown encoding %u", encoding);
+    static_assert(ILG_MLP_ENC_HASHGRID == kEncHashGrid && ILG_MLP_ENC_FREQ12 == kEncFreq12, "encoding ids");
     CK(cudaSetDevice(ctx->device));
+    ctx->mlp_encoding = encoding;
+    ctx->drop_graph();
     CK(ctx->mlp_w.reserve(kMlpParams)); CK(ctx->mlp_m.reserve(kMlpParams)); CK(ctx->mlp_v.reserve(kMlpParams));
     CK(ctx->mlp_grad.reserve(kMlpParams)); CK(ctx->mlp_loss.reserve(1));
     CK(ctx->mlp_wf.reserve(kFwdElems)); CK(ctx->mlp_wb.reserve(kBwdElems)); CK(ctx->mlp_wu.reserve(kUmmaElems));

@@ -12,6 +12,12 @@
 #include "mlp.cuh"
 #include "postproc.cuh"
 
+namespace ilg {
+// noalloc.cu: the device address of the allocation-free query's fixed array
+// on the current device, with the traversal kernel it launches loaded.
+cudaError_t noalloc_prepare(void **out);
+}  // namespace ilg
+
 struct ilg_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -20,6 +26,9 @@ struct ilg_ctx {
     cudaStream_t side[2] = {nullptr, nullptr};
     cudaEvent_t side_ev[3] = {nullptr, nullptr, nullptr};
     char err[512] = {0};
+    // device address of the fixed array ilg_intersect_noalloc stages through
+    // (looked up by ilg_create; null if that failed)
+    void *noalloc_scratch = nullptr;
 
     // mesh as uploaded
     ilg::DevBuf<float> pos;
@@ -55,10 +64,14 @@ struct ilg_ctx {
     // path tracing: scene attributes
     ilg::DevBuf<ilg::Mat> mats;
     uint32_t n_mats = 0;
-    ilg::DevBuf<ilg::QuadLight> lights;
-    ilg::DevBuf<uint32_t> light_first_tri;
+    ilg::DevBuf<ilg::Light> lights;
+    ilg::DevBuf<uint2> light_range;  // per light: (first triangle, triangle count)
     uint32_t n_lights = 0;
-    uint32_t light_first_host[ilg::kMaxLights] = {};
+    uint2 light_range_host[ilg::kMaxLights] = {};
+    float inf_escape = 0.f;          // number of infinite lights
+    bool lights_use_mesh = false;    // some light samples the uploaded mesh's triangles
+    uint32_t mesh_gen = 0;           // bumped by every ilg_set_mesh / ilg_load
+    uint32_t lights_mesh_gen = 0;    // mesh_gen the mesh lights' areas were computed for
     ilg::DevBuf<uint32_t> tri_attr, light_of_prim;
     bool attr_dirty = true;
     // path tracing: wavefront buffers
@@ -75,6 +88,7 @@ struct ilg_ctx {
     ilg::DevBuf<float> rec_feat, rec_tgt, qry_feat, qry_out;
     ilg::DevBuf<float4> rec_beta, qry_beta;
     uint32_t last_train_records = 0;
+    bool last_hash_update = false;  // the last cached render updated the hash-grid cache
     float last_train_loss = 0.f;
     uint32_t last_render_launches = 0;
     // work counters of the last render made with ILG_RENDER_COUNT
@@ -97,6 +111,7 @@ struct ilg_ctx {
     ilg::DevBuf<uint32_t> mlp_enc;
     ilg::DevBuf<__nv_bfloat16> mlp_wf, mlp_wb, mlp_wu, mlp_xcm, mlp_hcm, mlp_dzcm;
     bool mlp_ready = false;
+    uint32_t mlp_encoding = 0;  // ILG_MLP_ENC_*
     uint32_t mlp_step = 0;
     float mlp_lr = 1e-2f;
 
@@ -109,8 +124,10 @@ struct ilg_ctx {
         M.cap = (uint32_t)(mlp_xcm.cap / ilg::kMlpIn);
         M.grid = mlp_grid.ptr; M.grid_grad = mlp_grid_grad.ptr; M.grid_m = mlp_grid_m.ptr; M.grid_v = mlp_grid_v.ptr;
         ilg::grid_resolution(M.grid_res);
-        M.enc = mlp_enc.ptr;
-        M.enc_cap = (uint32_t)(mlp_enc.cap / ilg::kGridLevels);
+        M.encoding = mlp_encoding;
+        // the frequency-only encoding has no grid columns to precompute
+        M.enc = mlp_encoding == ilg::kEncHashGrid ? mlp_enc.ptr : nullptr;
+        M.enc_cap = M.enc ? (uint32_t)(mlp_enc.cap / ilg::kGridLevels) : 0u;
         return M;
     }
 
@@ -122,12 +139,13 @@ struct ilg_ctx {
     int check_device_error()
     {
         uint32_t h = 0;
-        if (cudaMemcpy(&h, derr.ptr, sizeof(h), cudaMemcpyDeviceToHost) != cudaSuccess) {
+        if (cudaMemcpyAsync(&h, derr.ptr, sizeof(h), cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
+            cudaStreamSynchronize(stream) != cudaSuccess) {
             snprintf(err, sizeof(err), "reading the device error word failed");
             return ILG_ECUDA;
         }
         if (h) {
-            cudaMemset(derr.ptr, 0, sizeof(uint32_t));
+            cudaMemsetAsync(derr.ptr, 0, sizeof(uint32_t), stream);
             snprintf(err, sizeof(err), "device reported error flags 0x%x (bit0: traversal stack bound, bit1: node/triangle index out of range, bit2: node visit budget)", h);
             return ILG_EOVERFLOW;
         }
@@ -144,7 +162,7 @@ struct ilg_ctx {
         post_pixels = post_frames = 0;
         ro.release(); rd.release(); hprim.release(); ht.release(); hu.release(); hv.release(); hocc.release();
         derr.release(); dstats.release();
-        mats.release(); lights.release(); light_first_tri.release(); tri_attr.release(); light_of_prim.release();
+        mats.release(); lights.release(); light_range.release(); tri_attr.release(); light_of_prim.release();
         q_o0.release(); q_d0.release(); q_o1.release(); q_d1.release(); beta.release(); s_o.release();
         s_d.release(); s_c.release(); accum.release(); accum_direct.release(); accum_albedo.release(); q_p0.release(); q_p1.release(); counts.release();
         hit_tri.release(); hit_t.release(); out_dev.release(); path_scene.release(); s_sid.release();

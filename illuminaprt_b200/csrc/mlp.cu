@@ -17,6 +17,7 @@
 //                    hash-grid corners of every level (FP32 atomics)
 // followed by k_mlp_adam (FP32 master weights, refreshes the BF16 copies)
 // and k_grid_adam (the grid features).
+#include "devinfo.cuh"
 #include "mlp.cuh"
 
 #include <cmath>
@@ -480,17 +481,7 @@ inline uint32_t grid_for(uint32_t n_rows, int sms)
     return blocks < 1 ? 1 : (blocks > cap ? cap : blocks);
 }
 
-int num_sms()
-{
-    static int sms = 0;
-    if (!sms) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (sms <= 0) sms = 148;
-    }
-    return sms;
-}
+int num_sms() { return current_sm_count(); }
 
 }  // namespace
 
@@ -527,12 +518,8 @@ cudaError_t mlp_infer_warp(const MlpDev &M, const float *raw, uint32_t n, float 
 {
     if (n == 0) return cudaSuccess;
     const size_t smem = kFwdElems * sizeof(__nv_bfloat16);
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_mlp_fwd<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        cudaFuncSetAttribute(k_mlp_fwd<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        attr = true;
-    }
+    cudaError_t e = ensure_dynamic_smem((const void *)k_mlp_fwd<false>, (int)smem);
+    if (e != cudaSuccess) return e;
     k_mlp_fwd<false><<<grid_for(n, num_sms()), 128, smem, st>>>(M, raw, n, out, n_dev);
     return cudaGetLastError();
 }
@@ -546,20 +533,16 @@ cudaError_t mlp_grads(const MlpDev &M, const float *raw, const float *target, ui
     // write exact zeros for them, but clear once so stale rows never leak
     if ((e = cudaMemsetAsync(M.grad, 0, kMlpParams * sizeof(float), st)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(M.loss, 0, sizeof(float), st)) != cudaSuccess) return e;
-    if ((e = cudaMemsetAsync(M.grid_grad, 0, kGridParams * sizeof(float), st)) != cudaSuccess) return e;
+    const bool has_grid = M.encoding == kEncHashGrid;
+    if (has_grid && (e = cudaMemsetAsync(M.grid_grad, 0, kGridParams * sizeof(float), st)) != cudaSuccess) return e;
     const size_t smem_f = kFwdElems * sizeof(__nv_bfloat16);
     const size_t smem_b = (kFwdElems + kBwdElems) * sizeof(__nv_bfloat16);
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_mlp_fwd<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_f);
-        cudaFuncSetAttribute(k_mlp_fwd<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_f);
-        cudaFuncSetAttribute(k_mlp_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_b);
-        attr = true;
-    }
+    if ((e = ensure_dynamic_smem((const void *)k_mlp_fwd<true>, (int)smem_f)) != cudaSuccess) return e;
+    if ((e = ensure_dynamic_smem((const void *)k_mlp_bwd, (int)smem_b)) != cudaSuccess) return e;
     const uint32_t grid = grid_for(n, num_sms());
     k_mlp_fwd<true><<<grid, 128, smem_f, st>>>(M, raw, n, nullptr, nullptr);
     k_mlp_bwd<<<grid, 128, smem_b, st>>>(M, raw, target, n);
-    k_grid_bwd<<<(n + kGridBwdThreads - 1) / kGridBwdThreads, kGridBwdThreads, 0, st>>>(M, raw, n);
+    if (has_grid) k_grid_bwd<<<(n + kGridBwdThreads - 1) / kGridBwdThreads, kGridBwdThreads, 0, st>>>(M, raw, n);
     const uint32_t chunks = (n_pad + kDwChunk - 1) / kDwChunk;
     for (int l = 0; l < kMlpLayers; l++) {
         const __nv_bfloat16 *A = l == 0 ? M.xcm : M.hcm + (size_t)(l - 1) * kMlpHid * M.cap;
@@ -578,7 +561,7 @@ cudaError_t mlp_adam(const MlpDev &M, uint32_t step, float lr, cudaStream_t st)
 {
     const float bc1 = 1.f - powf(0.9f, (float)step), bc2 = 1.f - powf(0.99f, (float)step);
     k_mlp_adam<<<(kMlpParams + 255) / 256, 256, 0, st>>>(M, lr, bc1, bc2);
-    k_grid_adam<<<(kGridParams + 255) / 256, 256, 0, st>>>(M, lr, bc1, bc2);
+    if (M.encoding == kEncHashGrid) k_grid_adam<<<(kGridParams + 255) / 256, 256, 0, st>>>(M, lr, bc1, bc2);
     return cudaGetLastError();
 }
 

@@ -20,6 +20,11 @@ constexpr int kMlpHid = 64;
 constexpr int kMlpOutP = 8;    // output columns computed (3 used)
 constexpr int kMlpLayers = 6;
 constexpr int kMlpBands = 4;       // frequency bands of position next to the grid
+constexpr int kMlpBandsFreq = 12;  // frequency bands of position in the frequency-only encoding
+
+// Input encodings (MlpDev::encoding)
+constexpr uint32_t kEncHashGrid = 0;  // hash grid + 4 bands + spherical harmonics (below)
+constexpr uint32_t kEncFreq12 = 1;    // 12 sine/cosine bands of position + raw direction, normal, roughness, albedo
 
 // Hash grid: kGridLevels levels of kGridFeat trainable features, each level a
 // table of kGridSize entries. Level l has resolution N_l = floor(16 *
@@ -86,6 +91,7 @@ struct MlpDev {
     // pair per level (enc_cap rows); null = the inference kernel gathers itself
     uint32_t *enc;
     uint32_t enc_cap;
+    uint32_t encoding;        // kEncHashGrid or kEncFreq12 (no grid: enc null, grid untouched)
 };
 
 // N_l of every level (host).
@@ -159,8 +165,32 @@ __device__ __forceinline__ float2 sh_pair(float x, float y, float z, int k)
 // 32 + 8a + 2b is sin(2^b pi x_a) and the next cos(2^b pi x_a). Columns
 // 56..71: the 16 spherical harmonics of the outgoing direction. Then 72..74
 // normal, 75 roughness, 76..78 albedo, 79 constant 1, 80..95 zero.
+// The frequency-only encoding (kEncFreq12): for axis a and band b < 12,
+// column 24a + 2b is sin(2^b pi x_a) and the next cos(2^b pi x_a); then
+// 72..74 outgoing direction, 75..77 normal, 78 roughness, 79..81 albedo,
+// 82 constant 1, 83..95 zero.
+__device__ __forceinline__ float2 encode_pair_freq(const float *f, int c)
+{
+    if (c < 6 * kMlpBandsFreq) {
+        const int axis = c / (2 * kMlpBandsFreq), band = (c % (2 * kMlpBandsFreq)) >> 1;
+        float s, co;
+        sincospif(ldexpf(f[axis], band), &s, &co);
+        return make_float2(s, co);
+    }
+    switch (c) {
+    case 72: return make_float2(f[3], f[4]);
+    case 74: return make_float2(f[5], f[6]);
+    case 76: return make_float2(f[7], f[8]);
+    case 78: return make_float2(f[9], f[10]);
+    case 80: return make_float2(f[11], f[12]);
+    case 82: return make_float2(1.f, 0.f);
+    default: return make_float2(0.f, 0.f);
+    }
+}
+
 __device__ __forceinline__ float2 encode_pair(const float *f, int c, const MlpDev &M)
 {
+    if (M.encoding == kEncFreq12) return encode_pair_freq(f, c);
     if (c < 2 * kGridLevels) return grid_features(M, c >> 1, f[0], f[1], f[2]);
     if (c < 56) {
         const int k = c - 32, axis = k >> 3, band = (k & 7) >> 1;

@@ -1,23 +1,28 @@
 // Radiance-cache inference on the 5th-generation tensor cores.
 //
-// One CTA of 128 threads owns 128 query rows at a time (one row per thread,
-// which is the TMEM lane the row's accumulator lives in). All six layers run
-// without leaving the CTA:
-//   * the weights (all layers, 46 KiB of BF16) sit in shared memory as W^T in
-//     the UMMA K-major no-swizzle layout: 8-row x 16-byte core matrices, the
-//     two K halves of one instruction 128 bytes apart (LBO), consecutive
-//     8-row groups K/8 x 128 bytes apart (SBO);
+// A CTA runs kTcGroups independent pipelines of 128 threads. Each group owns
+// one 128-row tile of queries at a time (one row per thread, which is the
+// TMEM lane the row's accumulator lives in) and takes it through all six
+// layers without leaving the CTA:
+//   * the weights (all layers, 46 KiB of BF16) sit in shared memory once per
+//     CTA, as W^T in the UMMA K-major no-swizzle layout: 8-row x 16-byte core
+//     matrices, the two K halves of one instruction 128 bytes apart (LBO),
+//     consecutive 8-row groups K/8 x 128 bytes apart (SBO);
 //   * each thread writes its row's activations (the encoded input, then each
-//     hidden layer after ReLU and rounding to BF16) into a shared-memory A
-//     tile in the same layout;
-//   * one elected thread issues the layer's K/16 tcgen05.mma instructions
-//     (M = 128, N = 64 or 16, K = 16, BF16 x BF16 -> FP32 in TMEM) and
-//     commits them to an mbarrier;
-//   * every thread waits on the mbarrier (bounded), reads its row back from
-//     TMEM with tcgen05.ld, applies ReLU and writes the next A tile.
-// The TMEM accumulator (64 columns) is allocated once per CTA and freed on
-// exit; every wait has an iteration limit that raises an error bit instead of
-// hanging.
+//     hidden layer after ReLU and rounding to BF16) into its group's
+//     shared-memory A tile in the same layout;
+//   * one elected thread per group issues the layer's K/16 tcgen05.mma
+//     instructions (M = 128, N = 64 or 16, K = 16, BF16 x BF16 -> FP32 into
+//     the group's 64 TMEM columns) and commits them to the group's mbarrier;
+//   * the group's threads wait on it (bounded), read their rows back from
+//     TMEM with tcgen05.ld, apply ReLU and write the next A tile.
+// The groups synchronise on their own named barriers, so while one group
+// drains its accumulator and writes activations, the tensor core runs the
+// other groups' layers: kTcGroups tiles are in flight per SM (the A tiles
+// share one copy of the weights, so shared memory holds six). TMEM is
+// allocated once per CTA and freed on exit; every wait has an iteration
+// limit that raises an error bit instead of hanging.
+#include "devinfo.cuh"
 #include "mlp.cuh"
 
 namespace ilg {
@@ -25,7 +30,12 @@ namespace ilg {
 namespace {
 
 constexpr int kTcRows = 128;
-constexpr uint32_t kTmemCols = 64;
+constexpr int kTcGroups = 6;         // tile pipelines per CTA
+constexpr uint32_t kTmemCols = 512;  // power of two >= 64 per group
+constexpr size_t kWBytes = ((kUmmaElems * 2 + 1023) / 1024) * 1024;
+constexpr size_t kATileBytes = (size_t)kTcRows * kMlpIn * 2;
+static_assert(64 * kTcGroups <= (int)kTmemCols, "TMEM columns for every group");
+static_assert(kWBytes + kTcGroups * kATileBytes <= 227 * 1024, "shared memory per CTA");
 constexpr uint32_t kWaitLimit = 1u << 22;  // try_wait calls before giving up (seconds at most)
 constexpr uint32_t kErrWait = 64u;
 
@@ -106,6 +116,29 @@ __device__ __forceinline__ void fence_before_sync() { asm volatile("tcgen05.fenc
 __device__ __forceinline__ void fence_after_sync() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
+// Barrier of one group's 128 threads (named barrier 1 + group).
+__device__ __forceinline__ void group_sync(int id)
+{
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "r"(kTcRows) : "memory");
+}
+
+// Barrier of one group's threads that also ANDs a predicate over them.
+__device__ __forceinline__ bool group_and(int id, bool v)
+{
+    uint32_t r;
+    asm volatile(
+        "{\n\t"
+        ".reg .pred p, q;\n\t"
+        "setp.ne.u32 p, %1, 0;\n\t"
+        "bar.red.and.pred q, %2, %3, p;\n\t"
+        "selp.u32 %0, 1, 0, q;\n\t"
+        "}\n"
+        : "=r"(r)
+        : "r"((uint32_t)v), "r"(id), "r"(kTcRows)
+        : "memory");
+    return r != 0;
+}
+
 __device__ __forceinline__ uint32_t pack2(float a, float b)
 {
     __nv_bfloat162 v = __floats2bfloat162_rn(a, b);
@@ -136,23 +169,25 @@ __global__ void __launch_bounds__(256) k_grid_encode(const MlpDev M, const float
     M.enc[i] = pack2(g.x, g.y);
 }
 
-__global__ void __launch_bounds__(kTcRows) k_mlp_infer_tc(const MlpDev M, const float *__restrict__ raw, uint32_t n,
-                                                          const uint32_t *__restrict__ n_dev,
-                                                          float *__restrict__ out, uint32_t *__restrict__ err)
+__global__ void __launch_bounds__(kTcRows * kTcGroups, 1)
+    k_mlp_infer_tc(const MlpDev M, const float *__restrict__ raw, uint32_t n, const uint32_t *__restrict__ n_dev,
+                   float *__restrict__ out, uint32_t *__restrict__ err)
 {
     extern __shared__ __align__(1024) unsigned char smem[];
-    unsigned char *w_s = smem;                                         // kUmmaElems bf16
-    unsigned char *a_s = smem + ((kUmmaElems * 2 + 1023) / 1024) * 1024;  // 128 x 96 bf16
-    __shared__ __align__(8) uint64_t bar;
+    unsigned char *w_s = smem;  // kUmmaElems bf16
+    __shared__ __align__(8) uint64_t bar[kTcGroups];
     __shared__ uint32_t tmem_base_s;
 
     if (n_dev) n = min(n, *n_dev);
     const int tid = threadIdx.x, warp = tid >> 5;
+    const int grp = tid / kTcRows, lt = tid % kTcRows;
+    const int bar_id = 1 + grp;
+    unsigned char *a_s = smem + kWBytes + (size_t)grp * kATileBytes;  // this group's 128 x 96 bf16 tile
     // weights -> shared memory (16-byte vectors)
     {
         const uint4 *src = reinterpret_cast<const uint4 *>(M.wu);
         uint4 *dst = reinterpret_cast<uint4 *>(w_s);
-        for (int i = tid; i < kUmmaElems / 8; i += kTcRows) dst[i] = src[i];
+        for (int i = tid; i < kUmmaElems / 8; i += blockDim.x) dst[i] = src[i];
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_s)),
@@ -160,23 +195,25 @@ __global__ void __launch_bounds__(kTcRows) k_mlp_infer_tc(const MlpDev M, const 
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
-    if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bar)) : "memory");
+    if (tid < kTcGroups) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&bar[tid])) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     fence_async_smem();
     fence_before_sync();
     __syncthreads();
     fence_after_sync();
-    const uint32_t tmem = tmem_base_s;
-    const uint32_t bar_a = smem_u32(&bar);
+    // this group's 64 accumulator columns; this warp's 32 TMEM lanes
+    const uint32_t tmem = tmem_base_s + (uint32_t)(64 * grp);
+    const uint32_t taddr = tmem + ((uint32_t)((warp & 3) * 32) << 16);
+    const uint32_t bar_a = smem_u32(&bar[grp]);
     const uint32_t w_a = smem_u32(w_s), a_a = smem_u32(a_s);
     uint32_t phase = 0;
     bool ok = true;
 
     const uint32_t n_tiles = (n + kTcRows - 1) / kTcRows;
-    for (uint32_t tile = blockIdx.x; tile < n_tiles && ok; tile += gridDim.x) {
-        const uint32_t row = tile * kTcRows + tid;
+    for (uint32_t tile = blockIdx.x * kTcGroups + grp; tile < n_tiles && ok; tile += gridDim.x * kTcGroups) {
+        const uint32_t row = tile * kTcRows + lt;
         // encoded input row -> A tile (K = 96)
         {
             float f[kMlpRaw];
@@ -195,7 +232,7 @@ __global__ void __launch_bounds__(kTcRows) k_mlp_infer_tc(const MlpDev M, const 
                         v[2 * e] = __uint_as_float(w4[e] << 16);
                         v[2 * e + 1] = __uint_as_float(w4[e] & 0xffff0000u);
                     }
-                    put_chunk(a_s, tid, c, kMlpIn, v);
+                    put_chunk(a_s, lt, c, kMlpIn, v);
                     continue;
                 }
 #pragma unroll
@@ -204,7 +241,7 @@ __global__ void __launch_bounds__(kTcRows) k_mlp_infer_tc(const MlpDev M, const 
                     v[e] = row < n ? p.x : 0.f;
                     v[e + 1] = row < n ? p.y : 0.f;
                 }
-                put_chunk(a_s, tid, c, kMlpIn, v);
+                put_chunk(a_s, lt, c, kMlpIn, v);
             }
         }
 #pragma unroll 1
@@ -212,9 +249,9 @@ __global__ void __launch_bounds__(kTcRows) k_mlp_infer_tc(const MlpDev M, const 
             const int K = mlp_in(l), N = umma_n(l);
             fence_async_smem();
             fence_before_sync();
-            __syncthreads();
+            group_sync(bar_id);
             fence_after_sync();
-            if (tid == 0) {
+            if (lt == 0) {
                 const uint32_t idesc = umma_idesc(kTcRows, N);
                 for (int s = 0; s < K / 16; s++) {
                     // K step s covers core-matrix chunks 2s, 2s+1
@@ -226,11 +263,10 @@ __global__ void __launch_bounds__(kTcRows) k_mlp_infer_tc(const MlpDev M, const 
             }
             const bool waited = mbar_wait(bar_a, phase);
             if (!waited) atomicOr(err, kErrWait);
-            ok = __syncthreads_and(waited) != 0;  // every thread leaves together
+            ok = group_and(bar_id, waited);  // the group's threads leave together
             if (!ok) break;
             phase ^= 1u;
             fence_after_sync();
-            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16);
             if (l < kMlpLayers - 1) {
 #pragma unroll
                 for (int q = 0; q < 4; q++) {
@@ -239,8 +275,8 @@ __global__ void __launch_bounds__(kTcRows) k_mlp_infer_tc(const MlpDev M, const 
                     tmem_wait_ld();
 #pragma unroll
                     for (int e = 0; e < 16; e++) v[e] = fmaxf(v[e], 0.f);
-                    put_chunk(a_s, tid, 2 * q, kMlpHid, v);
-                    put_chunk(a_s, tid, 2 * q + 1, kMlpHid, v + 8);
+                    put_chunk(a_s, lt, 2 * q, kMlpHid, v);
+                    put_chunk(a_s, lt, 2 * q + 1, kMlpHid, v + 8);
                 }
             } else {
                 float v[16];
@@ -258,7 +294,8 @@ __global__ void __launch_bounds__(kTcRows) k_mlp_infer_tc(const MlpDev M, const 
     __syncthreads();
     fence_after_sync();
     if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base_s), "r"(kTmemCols)
+                     : "memory");
 }
 
 }  // namespace
@@ -267,26 +304,20 @@ cudaError_t mlp_infer_tc(const MlpDev &M, const float *raw, uint32_t n, float *o
                          const uint32_t *n_dev, uint32_t *err)
 {
     if (n == 0) return cudaSuccess;
-    const size_t smem = ((kUmmaElems * 2 + 1023) / 1024) * 1024 + (size_t)kTcRows * kMlpIn * 2;
-    static bool attr = false;
-    if (!attr) {
-        cudaError_t e =
-            cudaFuncSetAttribute(k_mlp_infer_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
-    int dev = 0, sms = 148;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const size_t smem = kWBytes + kTcGroups * kATileBytes;
+    cudaError_t e = ensure_dynamic_smem((const void *)k_mlp_infer_tc, (int)smem);
+    if (e != cudaSuccess) return e;
+    const int sms = current_sm_count();
     const uint32_t tiles = (n + kTcRows - 1) / kTcRows;
-    const uint32_t grid = tiles < (uint32_t)sms * 3u ? tiles : (uint32_t)sms * 3u;
+    const uint32_t ctas = (tiles + kTcGroups - 1) / kTcGroups;
+    const uint32_t grid = ctas < (uint32_t)sms ? ctas : (uint32_t)sms;  // one CTA per SM (shared memory)
     MlpDev Mi = M;
     if (M.enc && n <= M.enc_cap) {
         k_grid_encode<<<(unsigned)(((uint64_t)n * kGridLevels + 255) / 256), 256, 0, st>>>(M, raw, n, n_dev);
     } else {
         Mi.enc = nullptr;
     }
-    k_mlp_infer_tc<<<grid, kTcRows, smem, st>>>(Mi, raw, n, n_dev, out, err);
+    k_mlp_infer_tc<<<grid, kTcRows * kTcGroups, smem, st>>>(Mi, raw, n, n_dev, out, err);
     return cudaGetLastError();
 }
 

@@ -8,26 +8,27 @@
 // host process whose device memory is owned by another allocator (a caching
 // pool that would fail or stall a cudaMalloc issued behind its back). For
 // them this entry point stages through one file-scope device array of fixed
-// size instead, so the call performs copies and one kernel launch and nothing
-// else.
+// size instead, so the call performs copies, two small memsets and one kernel
+// launch and nothing else.
 //
 // Limits and sharing:
 //   * at most ILG_NOALLOC_MAX_RAYS rays per call; larger batches are rejected
 //     with ILG_EINVAL before any device work;
 //   * the array exists once per GPU that loads this library and stays
-//     resident until the process exits (12 MiB);
+//     resident until the process exits (12 MiB + 256 bytes);
+//   * ilg_create loads the array's module on its device and looks up the
+//     array's device address there (cudaGetSymbolAddress), so the array
+//     becomes resident when the first context on a device is created, and a
+//     query never triggers that load itself;
 //   * every call on a device uses the same array and leaves the previous
-//     call's rays and hits in it; each call writes every element it later
-//     reads, so nothing has to be cleared;
+//     call's rays and hits in it. The ray counter of the persistent kernel
+//     and the call's error word (also in the array) are cleared on the
+//     stream before the launch; everything else a call reads it has written
+//     itself first;
 //   * calls whose device work overlaps (two contexts on one device used from
 //     two threads, or calls on different streams) race on the array: the
-//     caller must serialise them;
-//   * the first call on a device looks the array's device address up with
-//     cudaGetSymbolAddress (once per device, with that device current); make
-//     that first call before any stream capture.
+//     caller must serialise them.
 #include "ilg.h"
-
-#include <mutex>
 
 #include "ctx.cuh"
 #include "trace_api.cuh"
@@ -35,38 +36,34 @@
 namespace {
 
 constexpr uint32_t kMaxRays = ILG_NOALLOC_MAX_RAYS;
-// rays (o4, d4) then hits (prim, t, u, v): 32 + 16 bytes per ray
-constexpr size_t kScratchBytes = (size_t)kMaxRays * 48;
+// rays (o4, d4) then hits (prim, t, u, v): 32 + 16 bytes per ray; then one
+// 256-byte block: word 0 = the persistent kernel's ray counter, word 1 = this
+// call's device error flags
+constexpr size_t kRayBytes = (size_t)kMaxRays * 48;
+constexpr size_t kScratchBytes = kRayBytes + 256;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_lock;
-void *g_scratch_addr[kMaxDevices] = {};
+}  // namespace
 
-// Device address of this device's copy of g_noalloc_scratch (the host-side
-// name is only a stand-in and must never be handed to a kernel).
-int scratch_for(int device, void **out, char *err, size_t err_len)
+namespace ilg {
+
+// Called by ilg_create with `device` current: the device address of this
+// device's copy of g_noalloc_scratch (the host-side name is only a stand-in
+// and must never be handed to a kernel), and the traversal kernel's code
+// loaded, so that a query loads nothing.
+cudaError_t noalloc_prepare(void **out)
 {
-    if (device < 0 || device >= kMaxDevices) {
-        snprintf(err, err_len, "ilg_intersect_noalloc: device %d out of range", device);
-        return ILG_EINVAL;
-    }
-    std::lock_guard<std::mutex> g(g_lock);
-    if (!g_scratch_addr[device]) {
-        void *p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-        if (e != cudaSuccess || !p) {
-            snprintf(err, err_len, "ilg_intersect_noalloc: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
-            return ILG_ECUDA;
-        }
-        g_scratch_addr[device] = p;
-    }
-    *out = g_scratch_addr[device];
-    return ILG_OK;
+    *out = nullptr;
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return e;
+    if ((e = preload_closest_dyn()) != cudaSuccess) return e;
+    *out = p;
+    return cudaSuccess;
 }
 
-}  // namespace
+}  // namespace ilg
 
 #define NA_CK(call)                                                                                \
     do {                                                                                           \
@@ -96,25 +93,39 @@ extern "C" int ilg_intersect_noalloc(ilg_ctx *ctx, const float *ray_o_tmin, cons
         snprintf(ctx->err, sizeof(ctx->err), "ilg_intersect_noalloc: null array");
         return ILG_EINVAL;
     }
+    if (!ctx->noalloc_scratch) {
+        snprintf(ctx->err, sizeof(ctx->err),
+                 "ilg_intersect_noalloc: the fixed device array is unavailable (its lookup in ilg_create failed)");
+        return ILG_ECUDA;
+    }
     NA_CK(cudaSetDevice(ctx->device));
-    void *base = nullptr;
-    int rc = scratch_for(ctx->device, &base, ctx->err, sizeof(ctx->err));
-    if (rc != ILG_OK) return rc;
-    unsigned char *b = (unsigned char *)base;
+    unsigned char *b = (unsigned char *)ctx->noalloc_scratch;
     float4 *ro = (float4 *)b;
     float4 *rd = (float4 *)(b + (size_t)kMaxRays * 16);
     int32_t *hprim = (int32_t *)(b + (size_t)kMaxRays * 32);
     float *ht = (float *)(b + (size_t)kMaxRays * 36);
     float *hu = (float *)(b + (size_t)kMaxRays * 40);
     float *hv = (float *)(b + (size_t)kMaxRays * 44);
+    uint32_t *next = (uint32_t *)(b + kRayBytes);
+    uint32_t *derr = next + 1;
     cudaStream_t st = ctx->stream;
+    uint32_t flags = 0;
+    NA_CK(cudaMemsetAsync(derr, 0, sizeof(uint32_t), st));
     NA_CK(cudaMemcpyAsync(ro, ray_o_tmin, 16ull * n, cudaMemcpyHostToDevice, st));
     NA_CK(cudaMemcpyAsync(rd, ray_d_tmax, 16ull * n, cudaMemcpyHostToDevice, st));
-    NA_CK(ilg::launch_closest(ctx->view(), ro, rd, n, hprim, ht, hu, hv, ctx->derr.ptr, nullptr, st));
+    NA_CK(ilg::launch_closest_dyn(ctx->view(), ro, rd, n, hprim, ht, hu, hv, next, derr, st));
     NA_CK(cudaMemcpyAsync(prim, hprim, 4ull * n, cudaMemcpyDeviceToHost, st));
     NA_CK(cudaMemcpyAsync(t, ht, 4ull * n, cudaMemcpyDeviceToHost, st));
     NA_CK(cudaMemcpyAsync(u, hu, 4ull * n, cudaMemcpyDeviceToHost, st));
     NA_CK(cudaMemcpyAsync(v, hv, 4ull * n, cudaMemcpyDeviceToHost, st));
+    NA_CK(cudaMemcpyAsync(&flags, derr, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
     NA_CK(cudaStreamSynchronize(st));
-    return ctx->check_device_error();
+    if (flags) {
+        snprintf(ctx->err, sizeof(ctx->err),
+                 "ilg_intersect_noalloc: device reported error flags 0x%x (bit0: traversal stack bound, bit1: "
+                 "node/triangle index out of range, bit2: node visit budget)",
+                 flags);
+        return ILG_EOVERFLOW;
+    }
+    return ILG_OK;
 }

@@ -24,6 +24,7 @@
 #include "render.cuh"
 #include "trace.cuh"
 #include "mlp.cuh"
+#include "devinfo.cuh"
 
 #include <algorithm>
 #include <cfloat>
@@ -142,13 +143,20 @@ __global__ void k_camera(RenderDev R, uint32_t n_paths, uint64_t wave_begin)
     uint32_t pixel, x, y;
     uint64_t key;
     path_ident(S, g, pixel, key, x, y);
-    // BoxFilter shifts the [0,1) sample by -0.5 (Core/Filter/BoxFilter.cpp:20-28)
-    const float xi1 = rnd(key, kDimCam) - 0.5f, xi2 = rnd(key, kDimCam + 1) - 0.5f;
-    const float fx = x * S.rcp_w + xi1 * S.rcp_w, fy = y * S.rcp_h + xi2 * S.rcp_h;
-    const float3 target = S.corner + S.across * fx + S.up * fy;
-    const float3 d = normalize3(target - S.centre);
-    R.q_o[0][p] = make_float4(S.centre.x, S.centre.y, S.centre.z, 0.f);
-    R.q_d[0][p] = make_float4(d.x, d.y, d.z, FLT_MAX);
+    if (S.ray_o) {
+        // a path from the caller's ray (IIntegrator::Radiance(..., ray, ...),
+        // whose first intersection uses the ray's own [Min, Max])
+        R.q_o[0][p] = S.ray_o[pixel];
+        R.q_d[0][p] = S.ray_d[pixel];
+    } else {
+        // BoxFilter shifts the [0,1) sample by -0.5 (Core/Filter/BoxFilter.cpp:20-28)
+        const float xi1 = rnd(key, kDimCam) - 0.5f, xi2 = rnd(key, kDimCam + 1) - 0.5f;
+        const float fx = x * S.rcp_w + xi1 * S.rcp_w, fy = y * S.rcp_h + xi2 * S.rcp_h;
+        const float3 target = S.corner + S.across * fx + S.up * fy;
+        const float3 d = normalize3(target - S.centre);
+        R.q_o[0][p] = make_float4(S.centre.x, S.centre.y, S.centre.z, 0.f);
+        R.q_d[0][p] = make_float4(d.x, d.y, d.z, FLT_MAX);
+    }
     R.q_path[0][p] = p;
     R.path_scene[p] = sid;
     R.beta[p] = make_float4(1.f, 1.f, 1.f, 0.f);
@@ -398,6 +406,9 @@ __global__ void __launch_bounds__(256) k_shade(RenderDev R, int cur, uint32_t de
         if (ti < 0) {
             // escape: constant environment (zero for the reference's area-light scenes)
             add = beta * S.sky;
+            // the reference's infinite lights, seen by a camera ray or after a
+            // specular bounce (PathIntegrator.cpp:84-92 and :194-198)
+            if ((depth == 0 || after_specular) && S.inf_escape > 0.f) add = add + beta * S.inf_escape;
             if (tslot != 0xffffffffu && depth >= 2 && !is_black(add)) credit(R, tslot, depth - 1, add);
         } else if (depth <= S.max_depth) {
             const uint32_t attr = S.tri_attr[ti];
@@ -473,16 +484,57 @@ __global__ void __launch_bounds__(256) k_shade(RenderDev R, int cur, uint32_t de
                 // specular BSDF's F is zero for every light direction)
                 for (uint32_t l = 0; l < S.n_lights && l < kMaxLights && !specular; l++) {
                     if (l == light_id) continue;
-                    const QuadLight &L = S.lights[l];
+                    const Light &L = S.lights[l];
                     const float u = rnd(key, dim_of(depth, 2 * l)), v = rnd(key, dim_of(depth, 2 * l + 1));
-                    // Quad::SamplePoint (Core/Shape/Quad.cpp:144-153): a bilinear
-                    // patch over the reference's tessellation vertices
-                    const float3 P = L.p[0] + (L.p[2] - L.p[0]) * u + (L.p[3] - L.p[2]) * v +
-                                     (L.p[0] - L.p[2] + L.p[1] - L.p[3]) * (u * v);
+                    if (L.kind == kLightInfinite) {
+                        // InfiniteAreaLight::SampleRadiance (InfiniteAreaLight.cpp:73-83):
+                        // a direction in the cone cos(theta) >= 1e-4 about the shading
+                        // normal (Montecarlo::UniformSampleCone, Montecarlo.h:74-80), the
+                        // light's intensity with no division by the pdf, a shadow ray
+                        // over [1e-4, FLT_MAX] from the point itself
+                        const float ct = (1.f - u) + u * 1e-4f;
+                        const float st = sqrtf(1.f - ct * ct);
+                        float sp, cp;
+                        sincosf(kTwoPi * v, &sp, &cp);
+                        const float3 wi = U * (cp * st) + V * (sp * st) + W * ct;
+                        const float3 wi_l = make_float3(dot3(U, wi), dot3(V, wi), dot3(W, wi));
+                        const float3 c = beta * L.emit * fmaxf(0.f, dot3(wi, W)) * bsdf_f(m, wo_l, wi_l);
+                        if (is_black(c)) continue;
+                        so[n_sh] = make_float4(p.x, p.y, p.z, 1e-4f);
+                        sd[n_sh] = make_float4(wi.x, wi.y, wi.z, FLT_MAX);
+                        sc[n_sh] = c;
+                        n_sh++;
+                        continue;
+                    }
+                    float3 P, nl;
+                    if (L.kind == kLightMesh) {
+                        // ITriangleMesh::SamplePoint (Core/Shape/TriangleMesh.cpp:142-161):
+                        // a triangle picked uniformly by index (not by area), a uniform
+                        // point on it (IndexedTriangle::SamplePoint, Montecarlo.h:59-64),
+                        // its normal (p3 - p1) x (p2 - p1) turned to face the shaded
+                        // point; the pdf is 1 / the mesh's whole area (DiffuseAreaLight.cpp:36-40)
+                        const uint32_t k = min((uint32_t)((float)L.tri_count * rnd(key, dim_of(depth, 24 + l))),
+                                               L.tri_count - 1u);
+                        const uint32_t *tv = S.idx + 3ull * (L.first_tri + k);
+                        const float *a = S.pos + 3ull * tv[0], *b = S.pos + 3ull * tv[1], *cc = S.pos + 3ull * tv[2];
+                        const float3 p1 = make_float3(a[0], a[1], a[2]), p2 = make_float3(b[0], b[1], b[2]),
+                                     p3 = make_float3(cc[0], cc[1], cc[2]);
+                        const float su = sqrtf(u);
+                        const float b1 = 1.f - su, b2 = v * su;
+                        P = p1 * b1 + p2 * b2 + p3 * (1.f - b1 - b2);
+                        nl = normalize3(cross3(p3 - p1, p2 - p1));
+                        if (dot3(P - p, nl) > 0.f) nl = nl * -1.f;
+                    } else {
+                        // Quad::SamplePoint (Core/Shape/Quad.cpp:144-153): a bilinear
+                        // patch over the reference's tessellation vertices
+                        P = L.p[0] + (L.p[2] - L.p[0]) * u + (L.p[3] - L.p[2]) * v +
+                            (L.p[0] - L.p[2] + L.p[1] - L.p[3]) * (u * v);
+                        nl = L.n;
+                    }
                     float3 win = p - P;
                     const float dist2 = dot3(win, win);
                     win = normalize3(win);
-                    const float cl = fmaxf(0.f, dot3(win, L.n));
+                    const float cl = fmaxf(0.f, dot3(win, nl));
                     const float3 Ls = L.emit * (cl * L.area / dist2);
                     if (is_black(Ls)) continue;
                     const float3 wi = win * -1.f;
@@ -707,14 +759,27 @@ __global__ void k_tri_attr(const uint32_t *__restrict__ prim_of, uint32_t n, con
     attr[i] = (mat_ids ? (mat_ids[p] & 0xffffu) : 0u) | (light_of_prim[p] << 16);
 }
 
-__global__ void k_light_of_prim(uint32_t *lop, uint32_t n_prims, const uint32_t *first_tri, uint32_t n_lights)
+__global__ void k_light_of_prim(uint32_t *lop, uint32_t n_prims, const uint2 *range, uint32_t n_lights)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n_prims) return;
     uint32_t id = 0xffffu;
     for (uint32_t l = 0; l < n_lights; l++)
-        if (i == first_tri[l] || i == first_tri[l] + 1u) id = l;
+        if (i - range[l].x < range[l].y) id = l;
     lop[i] = id;
+}
+
+__global__ void k_tri_area(const float *__restrict__ pos, const uint32_t *__restrict__ idx, uint32_t first,
+                           uint32_t count, float *__restrict__ area)
+{
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= count) return;
+    const uint32_t *tv = idx + 3ull * (first + k);
+    const float *a = pos + 3ull * tv[0], *b = pos + 3ull * tv[1], *c = pos + 3ull * tv[2];
+    const float3 e1 = make_float3(b[0] - a[0], b[1] - a[1], b[2] - a[2]);
+    const float3 e2 = make_float3(c[0] - a[0], c[1] - a[1], c[2] - a[2]);
+    const float3 n = cross3(e1, e2);
+    area[k] = sqrtf(dot3(n, n)) * 0.5f;
 }
 
 inline uint32_t blocks_for(uint64_t n, uint32_t t) { return (uint32_t)((n + t - 1) / t); }
@@ -722,13 +787,7 @@ inline uint32_t blocks_for(uint64_t n, uint32_t t) { return (uint32_t)((n + t - 
 // Grid of a persistent kernel of 128-thread blocks over at most n items.
 inline uint32_t persistent_blocks(uint64_t n)
 {
-    static int sms = 0;
-    if (!sms) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (sms <= 0) sms = 148;
-    }
+    const int sms = current_sm_count();
     const uint32_t b = blocks_for(n, 128);
     const uint32_t cap = (uint32_t)sms * 16u;
     return b < 1u ? 1u : (b < cap ? b : cap);
@@ -736,11 +795,19 @@ inline uint32_t persistent_blocks(uint64_t n)
 
 }  // namespace
 
+cudaError_t triangle_areas(const float *pos, const uint32_t *idx, uint32_t first, uint32_t count, float *area,
+                           cudaStream_t st)
+{
+    if (count == 0) return cudaSuccess;
+    k_tri_area<<<blocks_for(count, 256), 256, 0, st>>>(pos, idx, first, count, area);
+    return cudaGetLastError();
+}
+
 cudaError_t build_tri_attr(const uint32_t *prim_of, uint32_t n_tris, const uint32_t *mat_ids,
-                           const uint32_t *light_first_tri, uint32_t n_lights, uint32_t *light_of_prim,
+                           const uint2 *light_range, uint32_t n_lights, uint32_t *light_of_prim,
                            uint32_t *attr, cudaStream_t st)
 {
-    k_light_of_prim<<<blocks_for(n_tris, 256), 256, 0, st>>>(light_of_prim, n_tris, light_first_tri, n_lights);
+    k_light_of_prim<<<blocks_for(n_tris, 256), 256, 0, st>>>(light_of_prim, n_tris, light_range, n_lights);
     k_tri_attr<<<blocks_for(n_tris, 256), 256, 0, st>>>(prim_of, n_tris, mat_ids, light_of_prim, attr);
     return cudaGetLastError();
 }
@@ -793,6 +860,8 @@ __global__ void k_hc_update(RenderDev R, uint32_t n)
             return;
         }
     }
+    // all 8 probed cells hold other keys: the record is dropped (and counted)
+    atomicAdd(R.hc_dropped, 1u);
 }
 
 __global__ void k_hc_query(RenderDev R, uint32_t cap)

@@ -18,11 +18,16 @@ struct Mat {  // mirrors ilg_material (32 bytes)
 };
 static_assert(sizeof(Mat) == 32, "material record is 32 bytes");
 
-struct QuadLight {
-    float3 p[4];   // the reference's Quad vertices v1..v4
-    float3 emit;
-    float3 n;      // unit normal (v3 - v1) x (v2 - v1), as Quad::SamplePoint returns it, normalised
-    float area;    // area of the two tessellation triangles
+// Light kinds (ilg_light::kind)
+constexpr uint32_t kLightQuad = 0, kLightMesh = 1, kLightInfinite = 2;
+
+struct Light {
+    float3 p[4];   // quad: the reference's Quad vertices v1..v4
+    float3 emit;   // quad, mesh: emitted radiance; infinite: intensity (scales its light samples only)
+    float3 n;      // quad: unit normal (v3 - v1) x (v2 - v1), as Quad::SamplePoint returns it, normalised
+    float area;    // quad: area of the two tessellation triangles; mesh: summed area of its triangles
+    uint32_t kind;
+    uint32_t first_tri, tri_count;  // quad, mesh: its triangles in the uploaded mesh
 };
 
 // One scene of a (batched) render: its BVH, shading data, camera and where
@@ -34,9 +39,19 @@ struct SceneRec {
     const uint32_t *tri_attr;  // per triangle record: material (low 16) | light (high 16, 0xffff none)
     const Mat *mats;
     uint32_t n_mats;
-    const QuadLight *lights;
+    const Light *lights;
     uint32_t n_lights;
     float3 sky;
+    // what an escaping path sees of the scene's infinite lights at depth 0 or
+    // after a specular bounce: 1 per light (InfiniteAreaLight::Radiance
+    // ignores its intensity, Core/Light/InfiniteAreaLight.cpp:39-56)
+    float inf_escape;
+    // the uploaded mesh (mesh lights sample points on its triangles)
+    const float *pos;
+    const uint32_t *idx;
+    // rays given by the caller (ilg_radiance): pixel i of the region starts
+    // its paths with ray i instead of a camera ray; null for camera paths
+    const float4 *ray_o, *ray_d;
     // camera (PerspectiveCamera after SetFieldOfView)
     float3 centre, corner, across, up;
     uint32_t width, height;  // the whole image (the camera's normalisation)
@@ -103,12 +118,18 @@ struct RenderDev {
     // hash-grid radiance cache (the non-learned baseline; null: the network answers queries)
     unsigned long long *hc_keys;  // hc_mask + 1 cells: key + 1, 0 = empty
     float4 *hc_vals;              // per cell: radiance sum (xyz) and sample count (w)
+    uint32_t *hc_dropped;         // records of the call that found no free cell in their probe window
     uint32_t *s_meta;          // per shadow segment: (slot << 8 | vertex) of a training path, or ~0
 };
 
+// light_range: per light (first triangle, triangle count) in the uploaded mesh
 cudaError_t build_tri_attr(const uint32_t *prim_of, uint32_t n_tris, const uint32_t *mat_ids,
-                           const uint32_t *light_first_tri, uint32_t n_lights, uint32_t *light_of_prim,
+                           const uint2 *light_range, uint32_t n_lights, uint32_t *light_of_prim,
                            uint32_t *attr, cudaStream_t st);
+// area[k] = area of uploaded triangle first + k (0.5 |(v1 - v0) x (v2 - v0)|,
+// IndexedTriangle::GetArea, Core/Shape/IndexedTriangle.cpp:386-393)
+cudaError_t triangle_areas(const float *pos, const uint32_t *idx, uint32_t first, uint32_t count, float *area,
+                           cudaStream_t st);
 struct MlpDev;
 // One wave: global paths [wave_begin, wave_begin + n_paths).
 cudaError_t render_wave(const RenderDev &R, uint32_t n_paths, uint64_t wave_begin, cudaStream_t st,

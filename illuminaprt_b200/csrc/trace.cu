@@ -1,6 +1,7 @@
 // Batched closest-hit / any-hit kernels over the 8-wide BVH.
 #include "trace.cuh"
 #include "trace_api.cuh"
+#include "devinfo.cuh"
 
 #include <algorithm>
 
@@ -105,19 +106,15 @@ __global__ void __launch_bounds__(128) k_trace_dyn(const Node8 *__restrict__ nod
     }
 }
 
-int sm_count()
-{
-    static int sms = 0;
-    if (!sms) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (sms <= 0) sms = 148;
-    }
-    return sms;
-}
+int sm_count() { return current_sm_count(); }
 
 }  // namespace
+
+cudaError_t preload_closest_dyn()
+{
+    cudaFuncAttributes a;
+    return cudaFuncGetAttributes(&a, (const void *)k_trace_dyn<false>);
+}
 
 cudaError_t launch_closest_dyn(const SceneView &s, const float4 *ro, const float4 *rd, uint32_t n, int32_t *prim,
                                float *t, float *u, float *v, uint32_t *next, uint32_t *err, cudaStream_t st)

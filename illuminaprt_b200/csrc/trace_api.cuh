@@ -37,6 +37,10 @@ cudaError_t launch_any_wt(const SceneView &s, const float4 *raw, const float4 *r
 cudaError_t build_raw_tris(const uint32_t *prim_of, const uint32_t *idx, const float *pos, uint32_t n, float4 *raw,
                            cudaStream_t st);
 
+// Loads the code of the closest-hit persistent kernel on the current device
+// (kernels load lazily on first launch otherwise, which may allocate).
+cudaError_t preload_closest_dyn();
+
 // Persistent variants with dynamic ray fetch; `next` is a device counter word.
 cudaError_t launch_closest_dyn(const SceneView &s, const float4 *ro, const float4 *rd, uint32_t n, int32_t *prim,
                                float *t, float *u, float *v, uint32_t *next, uint32_t *err, cudaStream_t st);

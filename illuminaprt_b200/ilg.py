@@ -34,7 +34,7 @@ EXPORTED = ["ilg_create", "ilg_destroy", "ilg_last_error", "ilg_set_mesh", "ilg_
             "ilg_mlp_train_step", "ilg_render_batch", "ilg_intersect_excluding", "ilg_occluded_excluding",
             "ilg_camera_frame_of", "ilg_render_region", "ilg_mlp_get_grid", "ilg_mlp_set_grid",
             "ilg_mlp_get_grid_grads", "ilg_accumulate", "ilg_accumulate_reset", "ilg_tonemap",
-            "ilg_render_counts", "ilg_save", "ilg_load", "ilg_hash_cache_reset"]
+            "ilg_render_counts", "ilg_save", "ilg_load", "ilg_hash_cache_reset", "ilg_last_train_stats", "ilg_probe_read_gbs", "ilg_set_lights", "ilg_radiance", "ilg_mlp_init_encoding"]
 
 ILG_MLP_RAW = 16
 ILG_MLP_WARP_MMA = 0x10
@@ -70,6 +70,14 @@ class ilg_material(ctypes.Structure):
 
 class ilg_quad_light(ctypes.Structure):
     _fields_ = [("v", (ctypes.c_float * 3) * 4), ("emit", ctypes.c_float * 3), ("first_tri", ctypes.c_uint32)]
+
+
+ILG_LIGHT_QUAD, ILG_LIGHT_MESH, ILG_LIGHT_INFINITE = 0, 1, 2
+
+
+class ilg_light(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_uint32), ("emit", ctypes.c_float * 3), ("v", (ctypes.c_float * 3) * 4),
+                ("first_tri", ctypes.c_uint32), ("tri_count", ctypes.c_uint32)]
 
 
 class ilg_camera(ctypes.Structure):
@@ -134,10 +142,14 @@ def load(build_if_missing: bool = True) -> ctypes.CDLL:
     L.ilg_occluded.argtypes = [vp, vp, vp, u32, vp, u32]
     L.ilg_set_materials.argtypes = [vp, vp, u32]
     L.ilg_set_quad_lights.argtypes = [vp, vp, u32]
+    L.ilg_set_lights.argtypes = [vp, vp, u32]
+    L.ilg_radiance.argtypes = [vp, vp, vp, u32, ctypes.POINTER(ilg_render_opts), vp, vp, vp, u32]
     L.ilg_render.argtypes = [vp, ctypes.POINTER(ilg_camera), ctypes.POINTER(ilg_render_opts), vp, u32]
     L.ilg_intersect_noalloc.argtypes = [vp, vp, vp, u32, vp, vp, vp, vp]
     L.ilg_render_counts.argtypes = [vp, vp]
     L.ilg_hash_cache_reset.argtypes = [vp]
+    L.ilg_last_train_stats.argtypes = [vp, vp, vp]
+    L.ilg_probe_read_gbs.argtypes = [vp, ctypes.c_uint64, u32, vp]
     L.ilg_save.argtypes = [vp, ctypes.c_char_p]
     L.ilg_load.argtypes = [vp, ctypes.c_char_p]
     L.ilg_accumulate.argtypes = [vp, vp, u32, vp, u32]
@@ -150,6 +162,7 @@ def load(build_if_missing: bool = True) -> ctypes.CDLL:
     L.ilg_occluded_excluding.argtypes = [vp, vp, vp, u32, u32, u32, vp, u32]
     L.ilg_intersect_noalloc.restype = i32
     L.ilg_mlp_init.argtypes = [vp, u32, ctypes.c_float]
+    L.ilg_mlp_init_encoding.argtypes = [vp, u32, ctypes.c_float, u32]
     L.ilg_mlp_get_params.argtypes = [vp, vp]
     L.ilg_mlp_set_params.argtypes = [vp, vp]
     L.ilg_mlp_get_grid.argtypes = [vp, vp]
@@ -307,6 +320,22 @@ class GpuSpace:
             arr[i].first_tri = int(l["first_tri"])
         self._check(self.L.ilg_set_quad_lights(self.h, ctypes.addressof(arr), len(lights)))
 
+    def set_lights(self, lights):
+        """lights: sequence of dicts with "kind" ("quad", "mesh" or "infinite")
+        and "emit"; quads add "v" (4x3, reference Quad order) and "first_tri",
+        meshes "first_tri" and "tri_count"."""
+        kinds = {"quad": ILG_LIGHT_QUAD, "mesh": ILG_LIGHT_MESH, "infinite": ILG_LIGHT_INFINITE}
+        arr = (ilg_light * max(1, len(lights)))()
+        for i, l in enumerate(lights):
+            arr[i].kind = kinds[l["kind"]]
+            arr[i].emit[:] = [float(x) for x in l["emit"]]
+            if "v" in l:
+                for k in range(4):
+                    arr[i].v[k][:] = [float(x) for x in l["v"][k]]
+            arr[i].first_tri = int(l.get("first_tri", 0))
+            arr[i].tri_count = int(l.get("tri_count", 2 if l["kind"] == "quad" else 0))
+        self._check(self.L.ilg_set_lights(self.h, ctypes.addressof(arr), len(lights)))
+
     @staticmethod
     def _camera(camera: dict, width: int, height: int) -> ilg_camera:
         cam = ilg_camera()
@@ -382,9 +411,37 @@ class GpuSpace:
         self._check(self.L.ilg_render(self.h, ctypes.byref(cam), ctypes.byref(o), img.ctypes.data, flags))
         return img
 
+    def radiance(self, o4, d4, spp: int = 1, max_depth: int = 6, epsilon: float = 1e-4, seed: int = 1,
+                 sky=(0.0, 0.0, 0.0), aux: bool = False):
+        """IIntegrator::Radiance over the rays (float32 (n, 4) origin/Min and
+        direction/Max): per ray the average of spp device paths started with
+        it; returns final (n, 3), or (final, direct, albedo) with aux."""
+        o4 = np.ascontiguousarray(o4, np.float32)
+        d4 = np.ascontiguousarray(d4, np.float32)
+        n = o4.shape[0]
+        o = ilg_render_opts(width=n, height=1, spp=spp, max_depth=max_depth, epsilon=epsilon, seed=seed)
+        o.sky[:] = list(sky)
+        outs = [np.empty((n, 3), np.float32) for _ in range(3 if aux else 1)]
+        ptrs = [x.ctypes.data for x in outs] + [None] * (3 - len(outs))
+        self._check(self.L.ilg_radiance(self.h, o4.ctypes.data, d4.ctypes.data, n, ctypes.byref(o), *ptrs, 0))
+        return tuple(outs) if aux else outs[0]
+
     def hash_cache_reset(self):
         """Empties the hash-grid radiance cache (allocated on first use)."""
         self._check(self.L.ilg_hash_cache_reset(self.h))
+
+    def probe_read_gbs(self, nbytes: int, reps: int = 64) -> float:
+        """Streaming read bandwidth (GB/s) over a device buffer of nbytes."""
+        g = ctypes.c_float(0.0)
+        self._check(self.L.ilg_probe_read_gbs(self.h, int(nbytes), int(reps), ctypes.byref(g)))
+        return float(g.value)
+
+    def last_train_stats(self):
+        """(training records of the last cached render, of those dropped by
+        the hash-grid cache for want of a free cell)."""
+        rec, drop = ctypes.c_uint32(0), ctypes.c_uint32(0)
+        self._check(self.L.ilg_last_train_stats(self.h, ctypes.byref(rec), ctypes.byref(drop)))
+        return int(rec.value), int(drop.value)
 
     # --- post-processing (AccumulationBuffer, tone operators) ---------------
     TONE = {"global": 0, "auto": 1, "drago": 2}
@@ -414,8 +471,13 @@ class GpuSpace:
         return o
 
     # --- radiance-cache network -------------------------------------------
-    def mlp_init(self, seed: int = 1, lr: float = 1e-2):
-        self._check(self.L.ilg_mlp_init(self.h, seed, lr))
+    MLP_ENCODINGS = {"hashgrid": 0, "freq12": 1}
+
+    def mlp_init(self, seed: int = 1, lr: float = 1e-2, encoding: str = "hashgrid"):
+        """A fresh cache network; encoding "hashgrid" (hash grid + bands +
+        spherical harmonics) or "freq12" (12 frequency bands of position and
+        the raw direction, normal, roughness and albedo)."""
+        self._check(self.L.ilg_mlp_init_encoding(self.h, seed, lr, self.MLP_ENCODINGS[encoding]))
 
     def mlp_params(self) -> np.ndarray:
         p = np.empty(ILG_MLP_PARAMS, np.float32)
@@ -468,7 +530,8 @@ class GpuSpace:
                                               ctypes.byref(loss), 0))
         return loss.value
 
-    def render_batch(self, items, paths_per_wave: int = 0, block: int = 0, device_ptrs: bool = False):
+    def render_batch(self, items, paths_per_wave: int = 0, block: int = 0, device_ptrs: bool = False,
+                     count: bool = False):
         """items: list of dicts {space: GpuSpace, camera, width, height, spp, max_depth=6, epsilon=1e-4,
         seed=1, sky=(0,0,0), out=None}. Renders all in one wavefront on this context; returns the images
         (numpy arrays, or the given CUDA tensors when device_ptrs)."""
@@ -495,8 +558,9 @@ class GpuSpace:
                 out = np.empty((it["height"], it["width"], 3), np.float32)
                 a.out_rgb = out.ctypes.data
             outs.append(out)
+        flags = (ILG_DEVICE_PTRS if device_ptrs else 0) | (ILG_RENDER_COUNT if count else 0)
         self._check(self.L.ilg_render_batch(self.h, ctypes.addressof(arr), len(items), paths_per_wave, block,
-                                            ILG_DEVICE_PTRS if device_ptrs else 0))
+                                            flags))
         return outs
 
     def sync(self):

@@ -1,12 +1,20 @@
 // GpuPathIntegrator: the reference's PathIntegrator
-// (Core/Integrator/PathIntegrator.h:19-50) with the settings of the device
-// renderer's learned radiance cache attached. It is what a scene script's
-// Integrator { Type = GPU ... } makes (factory "GPU" in the IntegratorManager,
-// registered by the plug-in).
+// (Core/Integrator/PathIntegrator.h:19-50) whose bounce loop runs on the
+// device, with the settings of the device renderer's learned radiance cache
+// attached. It is what a scene script's Integrator { Type = GPU ... } makes
+// (factory "GPU" in the IntegratorManager, registered by the plug-in).
 //
-// Under the reference's own renderers it IS the reference's PathIntegrator:
-// Radiance() is inherited unchanged, so a BasicRenderer over it renders
-// exactly as over Type = PathTracing. Under GpuRenderer its RayDepth and
+// Under the reference's own renderers (BasicRenderer and the others, which
+// call Radiance once per pixel sample) both Radiance overloads run the path
+// on the device: the first intersection is found by the scene (so
+// p_intersection and the RadianceContext's spatial fields are filled as
+// PathIntegrator::Radiance fills them), and the path itself, started with the
+// same ray, is one ilg_radiance call (Direct, Indirect and Albedo come back).
+// There is no CPU path: the scene's space must be a GpuSpace, the
+// materials and lights ones the device renders (DeviceScene.h), one shadow
+// ray per light, and Cache = MLP is refused there (the cache trains on
+// whole regions; use GpuRenderer). Calls are serialised on one device
+// context. Under GpuRenderer its RayDepth and
 // Epsilon drive the device path tracer as a PathIntegrator's do, and with
 // Cache = MLP rendering paths stop into the radiance cache at their
 // CacheDepth-th bounce vertex while one path in 1 / TrainFraction trains it
@@ -19,6 +27,7 @@
 #pragma once
 
 #include <cstdint>
+#include <mutex>
 #include <string>
 
 #include "Integrator/PathIntegrator.h"
@@ -55,8 +64,28 @@ public:
     const RadianceCacheSettings &GetCacheSettings(void) const { return m_cache; }
     std::string ToString(void) const { return "GpuPathIntegrator"; }
 
+    // IIntegrator::Radiance on the device (see above).
+    Illumina::Core::Spectrum Radiance(Illumina::Core::IntegratorContext *p_pContext,
+                                      Illumina::Core::Scene *p_pScene, const Illumina::Core::Ray &p_ray,
+                                      Illumina::Core::Intersection &p_intersection,
+                                      Illumina::Core::RadianceContext *p_pRadianceContext = NULL);
+    Illumina::Core::Spectrum Radiance(Illumina::Core::IntegratorContext *p_pContext,
+                                      Illumina::Core::Scene *p_pScene, Illumina::Core::Intersection &p_intersection,
+                                      Illumina::Core::RadianceContext *p_pRadianceContext = NULL);
+
+    // Paths started so far; the next call's sample sequence starts after them.
+    uint64_t GetPathCount(void) const { return m_nPaths; }
+
 private:
+    // The path of p_ray (its first hit p_intersection, found by the scene)
+    // traced on the device.
+    Illumina::Core::Spectrum DeviceRadiance(Illumina::Core::Scene *p_pScene, const Illumina::Core::Ray &p_ray,
+                                            Illumina::Core::Intersection &p_intersection,
+                                            Illumina::Core::RadianceContext *p_pRadianceContext);
+
     RadianceCacheSettings m_cache;
+    std::mutex m_mutex;
+    uint64_t m_nPaths;
 };
 
 }  // namespace PlugIn

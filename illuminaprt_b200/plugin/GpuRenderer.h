@@ -19,8 +19,9 @@
 //   materials   MatteMaterial, MirrorMaterial or GlassMaterial without a
 //               texture (reflectivity; for glass also transmittance and
 //               the two indices); a primitive without material renders black
-//   lights      DiffuseAreaLight on a Quad whose EmissivePrimitive is in
-//               the space
+//   lights      DiffuseAreaLight on a Quad or on a triangle mesh whose
+//               EmissivePrimitive is in the space, and InfiniteAreaLight
+//               without a texture (PrepareDeviceScene, DeviceScene.h)
 //   camera      any ICamera: its centre / corner / across / up frame, the
 //               same numbers its GetRay uses
 //   device      GetWidth() / GetHeight() give the image size, as in
@@ -71,13 +72,7 @@ public:
     std::string ToString(void) const { return "GpuRenderer"; }
 
 private:
-    // Uploads materials and lights of m_pScene to the space's context when
-    // the space was rebuilt or the scene changed.
-    GpuSpace *PrepareScene(void);
-
     uint32_t m_nSeed;
-    const void *m_pPreparedScene;
-    uint64_t m_nPreparedBuild;
     const ilg_ctx *m_pCacheContext;  // context whose radiance cache this renderer initialised
     uint64_t m_nCacheBuild;
 };

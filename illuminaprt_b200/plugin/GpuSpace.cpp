@@ -38,13 +38,13 @@ inline Vector3 EdgeCross(const Vector3 &a, const Vector3 &b)
 
 GpuSpace::GpuSpace(const std::string &p_strName, int p_nDevice)
     : ISpace(p_strName), m_nDevice(p_nDevice), m_pContext(NULL), m_bBuilt(false), m_nBuildCount(0),
-      m_pOrigin4(NULL), m_pDirection4(NULL)
+      m_pPreparedScene(NULL), m_nPreparedBuild(0), m_pOrigin4(NULL), m_pDirection4(NULL)
 {
 }
 
 GpuSpace::GpuSpace(void)
-    : ISpace(), m_nDevice(0), m_pContext(NULL), m_bBuilt(false), m_nBuildCount(0), m_pOrigin4(NULL),
-      m_pDirection4(NULL)
+    : ISpace(), m_nDevice(0), m_pContext(NULL), m_bBuilt(false), m_nBuildCount(0), m_pPreparedScene(NULL),
+      m_nPreparedBuild(0), m_pOrigin4(NULL), m_pDirection4(NULL)
 {
 }
 

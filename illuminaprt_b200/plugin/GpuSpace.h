@@ -89,6 +89,18 @@ public:
                           uint32_t &p_nCount) const;
     uint64_t GetBuildCount(void) const { return m_nBuildCount; }
     const std::string &GetLastError(void) const { return m_strLastError; }
+
+    // Whether the device's materials and lights were last uploaded for this
+    // scene and this build (PrepareDeviceScene, DeviceScene.h).
+    bool IsPreparedFor(const void *p_pScene) const
+    {
+        return m_pPreparedScene == p_pScene && m_nPreparedBuild == m_nBuildCount;
+    }
+    void SetPreparedFor(const void *p_pScene)
+    {
+        m_pPreparedScene = p_pScene;
+        m_nPreparedBuild = m_nBuildCount;
+    }
     std::string ToString(void) const { return "GpuSpace"; }
 
 private:
@@ -122,6 +134,8 @@ private:
     std::vector<PrimitiveRange> m_ranges;
     std::vector<Illumina::Core::IMaterial *> m_materials;
     uint64_t m_nBuildCount;
+    const void *m_pPreparedScene;
+    uint64_t m_nPreparedBuild;
     std::string m_strLastError;
 
     // staging for the device calls (guarded by m_mutex)

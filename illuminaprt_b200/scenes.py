@@ -200,7 +200,25 @@ def _quad_tris(v0, v1, v2, v3):
     return [(v0, v1, v2), (v0, v2, v3)]
 
 
-def box_scene(specular: bool = False):
+def _fan_light_tris(yl: float):
+    """A flat 6-triangle fan under the ceiling, emitting downward (every
+    triangle's (v1 - v0) x (v2 - v0) points to -y), with triangles of unequal
+    area, so the reference's index-uniform choice of a triangle to sample
+    (ITriangleMesh::SamplePoint) is not the area-uniform one."""
+    c = np.array((0.02, yl, -0.01))
+    ang = np.radians([0.0, 50.0, 110.0, 170.0, 235.0, 300.0])
+    rad = [0.28, 0.22, 0.30, 0.20, 0.26, 0.24]
+    pts = [c + np.array((r * np.cos(a), 0.0, r * np.sin(a))) for r, a in zip(rad, ang)]
+    tris = []
+    for k in range(6):
+        a, b = pts[k], pts[(k + 1) % 6]
+        if np.cross(a - c, b - c)[1] > 0:
+            a, b = b, a
+        tris.append((c, a, b))
+    return tris
+
+
+def box_scene(specular: bool = False, light: str = "quad", infinite=None, fov: float = 40.0):
     """Closed box [-1,1]^3 with the front (z = +1) open, walls two triangles
     each (normals inward), left wall red, right green, others grey; two inner
     boxes rotated +-17 deg about y; a 0.5 x 0.4 ceiling quad light with
@@ -210,6 +228,13 @@ def box_scene(specular: bool = False):
     0.9) and the tall one glass (GlassMaterial, reflectivity 0.45,
     transmittance 0.45, eta 1 / 1.52): "kinds" (0 matte, 2 mirror, 3 glass)
     and "spec" (per primitive: transmittance rgb, eta_i, eta_t) are added.
+
+    With light="mesh" the ceiling light is a 6-triangle mesh of unequal
+    triangles (a DiffuseAreaLight on a triangle mesh, "light_kind" 1) with the
+    same radiance; with infinite = (r, g, b) an InfiniteAreaLight of that
+    intensity (no texture) joins the lights ("inf"). fov: the camera's field
+    of view (at 60 deg the border pixels see past the box, where an infinite
+    light is seen directly).
 
     Returns a dict with flattened world-space triangles (unshared vertices),
     a per-triangle primitive index, per-primitive albedo, the light quad in
@@ -232,7 +257,11 @@ def box_scene(specular: bool = False):
     # and (v1, v4, v3) (Core/Shape/Quad.cpp), normal (v3-v1) x (v2-v1) = -y
     yl = 0.999
     q = np.array([(-0.25, yl, -0.2), (-0.25, yl, 0.2), (0.25, yl, 0.2), (0.25, yl, -0.2)], np.float64)
-    light_tris = [(q[0], q[2], q[1]), (q[0], q[3], q[2])]
+    # the mesh light hangs 0.2 below the ceiling: the reference samples mesh
+    # lights from both sides (the normal turned toward the shaded point), so
+    # ceiling points right above a light flush with it would see it at ~0
+    # distance (fireflies); at 0.2 the ceiling gets a smooth glow instead
+    light_tris = [(q[0], q[2], q[1]), (q[0], q[3], q[2])] if light == "quad" else _fan_light_tris(0.8)
     prims.append((light_tris, GREY))
     pos, prim_of_tri = [], []
     for pi, (tris, _) in enumerate(prims):
@@ -250,9 +279,12 @@ def box_scene(specular: bool = False):
         "light_quad": q.astype(np.float32),
         "light_emit": np.array([17.0, 12.0, 4.0], np.float32),
         "camera": {"eye": (0.0, 0.0, 3.5), "target": (0.0, 0.0, 0.0), "up": (0.0, 1.0, 0.0),
-                   "fov": 40.0, "aspect": 1.0},
+                   "fov": float(fov), "aspect": 1.0},
         "max_depth": 6, "epsilon": 1e-4,
+        "light_kind": 0 if light == "quad" else 1,
     }
+    if infinite is not None:
+        out["inf"] = np.asarray(infinite, np.float32)
     if specular:
         n = len(prims)
         kinds = np.zeros(n, np.int32)
@@ -290,9 +322,22 @@ def load_box_scene(space, scene=None):
     space.initialise(scene["pos"], scene["idx"], scene["prim_of_tri"])
     space.build()
     space.set_materials(box_materials(scene))
-    first = int(np.nonzero(scene["prim_of_tri"] == scene["light_prim"])[0][0])
-    space.set_quad_lights([{"v": scene["light_quad"], "emit": scene["light_emit"], "first_tri": first}])
+    space.set_lights(box_lights(scene))
     return scene
+
+
+def box_lights(scene):
+    """The box scene's lights (GpuSpace.set_lights form), in the order of the
+    reference scene's LightList: the area light, then the infinite light."""
+    sel = np.nonzero(scene["prim_of_tri"] == scene["light_prim"])[0]
+    first = int(sel[0])
+    if scene.get("light_kind", 0) == 1:
+        lights = [{"kind": "mesh", "emit": scene["light_emit"], "first_tri": first, "tri_count": int(sel.size)}]
+    else:
+        lights = [{"kind": "quad", "v": scene["light_quad"], "emit": scene["light_emit"], "first_tri": first}]
+    if "inf" in scene:
+        lights.append({"kind": "infinite", "emit": scene["inf"]})
+    return lights
 
 
 def _g(x) -> str:

@@ -111,9 +111,12 @@ int ilg_intersect_counted(ilg_ctx *ctx, const float *ray_o_tmin, const float *ra
  * one fixed device array per GPU (12 MiB, resident until exit) instead of the
  * context's growable buffers. At most ILG_NOALLOC_MAX_RAYS rays per call
  * (more is ILG_EINVAL). All calls on a device share that array, so calls whose
- * device work overlaps race; serialise them. The first call on each device
- * looks the array up (cudaGetSymbolAddress); make it before any stream
- * capture. Results equal ilg_intersect's. */
+ * device work overlaps race; serialise them. The array becomes resident, and
+ * its device address is looked up (cudaGetSymbolAddress), when a context is
+ * created on the device (ilg_create), so a call itself only copies, clears
+ * two words of the array and launches one kernel. The status covers this call
+ * only: its device error flags are kept in the array, not in the context.
+ * Results equal ilg_intersect's. */
 #define ILG_NOALLOC_MAX_RAYS 262144u
 int ilg_intersect_noalloc(ilg_ctx *ctx, const float *ray_o_tmin, const float *ray_d_tmax, uint32_t n,
                           int32_t *prim, float *t, float *u, float *v);
@@ -165,6 +168,37 @@ typedef struct ilg_quad_light {
     uint32_t first_tri;
 } ilg_quad_light;
 
+/* Lights of every kind the device path tracer samples (ilg_set_lights):
+ *   ILG_LIGHT_QUAD      DiffuseAreaLight on a Quad, as ilg_quad_light
+ *                       (Core/Light/DiffuseAreaLight.cpp, Core/Shape/Quad.cpp)
+ *   ILG_LIGHT_MESH      DiffuseAreaLight on a triangle mesh whose triangles
+ *                       are [first_tri, first_tri + tri_count) of the mesh
+ *                       given to ilg_set_mesh: one-sided emission seen by the
+ *                       path, light samples as the reference takes them
+ *                       (ITriangleMesh::SamplePoint, TriangleMesh.cpp:142-161:
+ *                       a triangle uniform by index, a uniform point on it,
+ *                       its normal turned toward the shaded point, pdf 1 / the
+ *                       mesh's area)
+ *   ILG_LIGHT_INFINITE  InfiniteAreaLight without a texture, with the
+ *                       reference's semantics (InfiniteAreaLight.cpp:39-90):
+ *                       a camera ray that escapes, or a path escaping right
+ *                       after a specular bounce, sees radiance 1 whatever the
+ *                       intensity; its light samples take a direction in the
+ *                       cone cos(theta) >= 1e-4 about the normal and add
+ *                       intensity * cos * BSDF, not divided by their pdf.
+ * Set the lights after the mesh: a mesh light's area is computed from the
+ * mesh uploaded at the time. */
+#define ILG_LIGHT_QUAD 0u
+#define ILG_LIGHT_MESH 1u
+#define ILG_LIGHT_INFINITE 2u
+typedef struct ilg_light {
+    uint32_t kind;       /* ILG_LIGHT_* */
+    float emit[3];       /* quad, mesh: emitted radiance; infinite: intensity */
+    float v[4][3];       /* quad: its vertices, as ilg_quad_light::v */
+    uint32_t first_tri;  /* quad, mesh: first of its triangles in the mesh */
+    uint32_t tri_count;  /* mesh: its number of triangles (quad: 2; infinite: unused) */
+} ilg_light;
+
 /* Pinhole camera as the reference's camera factory builds it
  * (Core/Camera/CameraFactories.h:40-80): frame from (target - eye, up),
  * image plane at distance 1, SetFieldOfView(fov_deg, aspect). */
@@ -205,6 +239,9 @@ typedef struct ilg_render_opts {
 /* Materials indexed by the mat_ids given to ilg_set_mesh. */
 int ilg_set_materials(ilg_ctx *ctx, const ilg_material *mats, uint32_t n);
 int ilg_set_quad_lights(ilg_ctx *ctx, const ilg_quad_light *lights, uint32_t n);
+/* At most 8 lights of any kinds (replaces the lights set before); the
+ * scene's LightList (Core/Scene/Scene.h) in the order the reference samples it. */
+int ilg_set_lights(ilg_ctx *ctx, const ilg_light *lights, uint32_t n);
 
 /* Renders width x height pixels at spp samples each into out_rgb
  * (height x width x 3 floats, row y = image-plane 'up' coordinate y, as the
@@ -233,6 +270,14 @@ int ilg_render_counts(ilg_ctx *ctx, uint64_t counts[6]);
  * apply; call ilg_hash_cache_reset first. */
 #define ILG_RENDER_HASH_CACHE 0x8u
 int ilg_hash_cache_reset(ilg_ctx *ctx);
+
+/* Training records of the last cached render (ILG_RENDER_* with
+ * cache_depth): *records = records its training paths produced; *dropped =
+ * those the hash-grid cache could not store because all 8 cells of their
+ * probe window held other keys (0 unless the render used
+ * ILG_RENDER_HASH_CACHE). Synchronises the context's stream. This project's
+ * own statistics; no counterpart in the reference. */
+int ilg_last_train_stats(ilg_ctx *ctx, uint32_t *records, uint32_t *dropped);
 
 /* A camera as the reference's ICamera holds it after construction
  * (Core/Camera/Camera.h:23-28: m_centre, m_corner, m_across, m_up): the ray
@@ -271,6 +316,22 @@ int ilg_render_region(ilg_ctx *ctx, const ilg_camera_frame *frame, const ilg_ren
                       const ilg_region *region, float *final_rgb, float *direct_rgb, float *albedo_rgb,
                       uint32_t flags);
 
+/* IIntegrator::Radiance(context, scene, ray, intersection, radiance_context)
+ * of the reference's PathIntegrator (Core/Integrator/Integrator.h:53-54,
+ * PathIntegrator.cpp:44-367), batched over n caller-given rays: ray i
+ * (float4 (o, Min) and (d, Max), 16-byte aligned; its first intersection
+ * uses its own [Min, Max]) starts opts->spp paths through the device bounce
+ * loop, and final_rgb / direct_rgb / albedo_rgb (n x 3 each; the last two
+ * optional) receive their averages of Direct + Indirect, Direct and Albedo,
+ * as the reference's RadianceContext holds them. opts->width and
+ * opts->height are ignored; max_depth, epsilon, seed, sky and the cache
+ * options mean what they mean for ilg_render. Host pointers unless
+ * ILG_DEVICE_PTRS (then the ray and output arrays are device pointers and
+ * the call only enqueues). */
+int ilg_radiance(ilg_ctx *ctx, const float *ray_o_tmin, const float *ray_d_tmax, uint32_t n,
+                 const ilg_render_opts *opts, float *final_rgb, float *direct_rgb, float *albedo_rgb,
+                 uint32_t flags);
+
 /* ------------------------------------------------------------------------
  * Radiance-cache network (no counterpart in the reference, whose closest
  * analogue is the irradiance cache of Core/Integrator/ICIntegrator.*): a
@@ -288,6 +349,14 @@ int ilg_render_region(ilg_ctx *ctx, const ilg_camera_frame *frame, const ilg_ren
 #define ILG_MLP_GRID_PARAMS 1048576u /* FP32 grid features [level][entry][feature] */
 
 int ilg_mlp_init(ilg_ctx *ctx, uint32_t seed, float learning_rate);
+/* ilg_mlp_init with a choice of input encoding: ILG_MLP_ENC_HASHGRID (the
+ * encoding above, ilg_mlp_init's) or ILG_MLP_ENC_FREQ12: 12 sine/cosine
+ * frequency bands per position axis (sin and cos of 2^b pi x, b < 12) next
+ * to the raw outgoing direction, normal, roughness and albedo and a
+ * constant 1 (84 of the 96 input columns; no grid is read or trained). */
+#define ILG_MLP_ENC_HASHGRID 0u
+#define ILG_MLP_ENC_FREQ12 1u
+int ilg_mlp_init_encoding(ilg_ctx *ctx, uint32_t seed, float learning_rate, uint32_t encoding);
 int ilg_mlp_get_params(ilg_ctx *ctx, float *params /* ILG_MLP_PARAMS */);
 int ilg_mlp_set_params(ilg_ctx *ctx, const float *params);
 int ilg_mlp_get_grid(ilg_ctx *ctx, float *grid /* ILG_MLP_GRID_PARAMS */);
@@ -311,7 +380,9 @@ int ilg_mlp_train_step(ilg_ctx *ctx, const float *raw, const float *target, uint
  * path lengths share the queues. The runner context supplies the wavefront
  * buffers and the stream; all contexts must be on its device.
  * paths_per_wave: 0 = automatic; block: threads per block of the extend,
- * shade and shadow kernels (64, 128 or 256; 0 = 128). */
+ * shade and shadow kernels (64, 128 or 256; 0 = 128). flags: ILG_DEVICE_PTRS,
+ * ILG_RENDER_COUNT (the batch's traversal work for ilg_render_counts on the
+ * runner). */
 typedef struct ilg_batch_item {
     ilg_ctx *scene;
     ilg_camera camera;
@@ -345,6 +416,14 @@ int ilg_accumulate_reset(ilg_ctx *ctx);
  * reference's; DRAGO evaluates its logarithms and power in double as the
  * reference does and agrees to within float rounding. */
 int ilg_tonemap(ilg_ctx *ctx, const float *in_rgb, uint32_t n_pixels, float *out_rgb, uint32_t op, uint32_t flags);
+
+/* Device probe (this project's measurement tool; no counterpart in the
+ * reference): *gbs = bytes read per second by a streaming read kernel that
+ * passes `reps` times over a device buffer of `bytes` bytes (1 MiB .. 8 GiB),
+ * with L2-only loads. A buffer below the device's L2 size gives the L2 read
+ * bandwidth, the roofline denominator of traversal over scenes that fit in
+ * L2. Allocates and frees its buffer; synchronous. */
+int ilg_probe_read_gbs(ilg_ctx *ctx, uint64_t bytes, uint32_t reps, float *gbs);
 
 /* Blocks until the context's stream is idle (for ILG_DEVICE_PTRS callers). */
 int ilg_sync(ilg_ctx *ctx);

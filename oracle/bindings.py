@@ -16,7 +16,10 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libilref.so")
-REF_TREE = "/root/reference/Core"
+# the reference's Core tree: $ILLUMINA_CORE, else a checkout named "reference"
+# beside this repository
+REF_TREE = os.environ.get("ILLUMINA_CORE",
+                          os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference", "Core"))
 
 _f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
 _u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
@@ -175,6 +178,13 @@ class RefLib:
                                                    c.c_char_p, c.c_int])
         L.ilref_render_box_materials.argtypes = (list(L.ilref_render_box.argtypes[:8]) + [c.c_void_p, c.c_void_p]
                                                  + list(L.ilref_render_box.argtypes[8:]))
+        L.ilref_render_box_lights.argtypes = (list(L.ilref_render_box.argtypes[:8]) + [c.c_void_p, c.c_void_p, c.c_int,
+                                                                                      c.c_void_p]
+                                              + list(L.ilref_render_box.argtypes[8:]) + [_f32p, _f32p])
+        L.ilref_render_box_engine.argtypes = ([c.c_char_p] * 5 + list(L.ilref_render_box.argtypes[:8])
+                                              + [c.c_void_p, c.c_void_p, c.c_int, c.c_void_p]
+                                              + list(L.ilref_render_box.argtypes[8:17])
+                                              + [c.c_float, c.c_int, _f32p, _f32p, _f32p, c.c_char_p, c.c_int])
         L.ilref_postprocess.argtypes = [c.c_int, _f32p, c.c_int, c.c_int, c.c_int, _f32p]
         L.ilref_render_script.argtypes = [c.c_char_p, c.c_char_p, c.c_int, c.c_int, c.c_int, _f32p, _f32p, _f32p,
                                           c.c_char_p, c.c_int, c.c_char_p, c.c_int]
@@ -237,6 +247,55 @@ class RefLib:
         if rc:
             raise RuntimeError(f"ilref_render_box_plugin: {rc}: {err.value.decode(errors='replace')}")
         return out
+
+    @staticmethod
+    def _light_args(scene):
+        """(light_kind, inf pointer, backing arrays) of a box scene's lights."""
+        inf = scene.get("inf")
+        if inf is None:
+            return int(scene.get("light_kind", 0)), None, ()
+        inf = np.ascontiguousarray(inf, np.float32)
+        return int(scene.get("light_kind", 0)), inf.ctypes.data, (inf,)
+
+    def render_box_lights(self, scene: dict, width: int, height: int, spp: int, seed: int = 1, nthreads=None):
+        """The reference's PathIntegrator on a box scene with any of its light
+        choices (mesh light, infinite light) and materials: (final, direct, albedo)."""
+        f = lambda a: np.ascontiguousarray(a, np.float32)
+        cam = scene["camera"]
+        outs = [np.zeros((height, width, 3), np.float32) for _ in range(3)]
+        kp, sp, keep = self._material_args(scene)
+        kind, ip, keep2 = self._light_args(scene)
+        self.L.ilref_render_box_lights(*self._scene_args(scene), kp, sp, kind, ip, f(cam["eye"]), f(cam["target"]),
+                                       f(cam["up"]), float(cam["fov"]), float(cam["aspect"]), width, height, spp,
+                                       int(scene["max_depth"]), float(scene["epsilon"]), seed,
+                                       nthreads or os.cpu_count() or 1, *(o.reshape(-1) for o in outs))
+        return tuple(outs)
+
+    def render_box_engine(self, plugin: str, scene: dict, width: int, height: int, spp: int, tile: int = 0,
+                          space: str = "GPU", renderer: str = "GPU", integrator: str = "",
+                          integrator_args: dict | None = None):
+        """The box scene driven by the engine's objects over the plug-in's
+        space, with the renderer made by factory `renderer` ("" = the
+        reference's BasicRenderer) and the integrator made by factory
+        `integrator` ("" = the reference's PathIntegrator) with
+        `integrator_args`. Returns (final, direct, albedo) from the
+        RadianceBuffer; raises RuntimeError with the engine's message."""
+        f = lambda a: np.ascontiguousarray(a, np.float32)
+        cam = scene["camera"]
+        outs = [np.zeros((height, width, 3), np.float32) for _ in range(3)]
+        err = ctypes.create_string_buffer(1024)
+        kp, sp, keep = self._material_args(scene)
+        kind, ip, keep2 = self._light_args(scene)
+        extra = ";".join(f"{k}={v}" for k, v in (integrator_args or {}).items())
+        rc = self.L.ilref_render_box_engine(plugin.encode(), space.encode(), renderer.encode(), integrator.encode(),
+                                            extra.encode(), *self._scene_args(scene), kp, sp, kind, ip,
+                                            f(cam["eye"]), f(cam["target"]), f(cam["up"]), float(cam["fov"]),
+                                            float(cam["aspect"]), width, height, spp, int(scene["max_depth"]),
+                                            float(scene["epsilon"]), tile, *(o.reshape(-1) for o in outs), err,
+                                            1024)
+        if rc:
+            raise RuntimeError(f"ilref_render_box_engine: {rc}: {err.value.decode(errors='replace')}")
+        return tuple(outs)
 
     def render_box_aov(self, scene: dict, width: int, height: int, spp: int, seed: int = 1, nthreads=None):
         """render_box plus the RadianceContext Direct and Albedo: (final, direct, albedo)."""

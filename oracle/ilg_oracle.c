@@ -201,6 +201,43 @@ static int cmp_key(const void *a, const void *b)
     return ia < ib ? -1 : (ia > ib);
 }
 
+/* Total order of the median split: centroid on the axis, then index. */
+static int key_less(const float *cent, int axis, uint32_t a, uint32_t b)
+{
+    float ca = cent[3 * a + axis], cb = cent[3 * b + axis];
+    return ca < cb || (ca == cb && a < b);
+}
+
+/* Rearranges v[0..n) so that v[k] is the element a full sort by key_less
+ * would put there, with every element before it smaller and every one after
+ * it larger (quickselect, median-of-three pivots). The two sides hold the
+ * same sets as after a full sort, which is all the split uses. */
+static void select_kth(uint32_t *v, uint32_t n, uint32_t k, const float *cent, int axis)
+{
+    uint32_t lo = 0, hi = n - 1;
+    while (hi > lo) {
+        uint32_t mid = lo + (hi - lo) / 2;
+        if (key_less(cent, axis, v[mid], v[lo])) { uint32_t t = v[mid]; v[mid] = v[lo]; v[lo] = t; }
+        if (key_less(cent, axis, v[hi], v[lo])) { uint32_t t = v[hi]; v[hi] = v[lo]; v[lo] = t; }
+        if (key_less(cent, axis, v[hi], v[mid])) { uint32_t t = v[hi]; v[hi] = v[mid]; v[mid] = t; }
+        uint32_t pivot = v[mid];
+        uint32_t i = lo, j = hi;
+        while (i <= j) {
+            while (key_less(cent, axis, v[i], pivot)) i++;
+            while (key_less(cent, axis, pivot, v[j])) j--;
+            if (i <= j) {
+                uint32_t t = v[i]; v[i] = v[j]; v[j] = t;
+                i++;
+                if (j == 0) break;
+                j--;
+            }
+        }
+        if (k <= j) hi = j;
+        else if (k >= i) lo = i;
+        else return;
+    }
+}
+
 /* Build with explicit sibling slots: children of node k live at (left, left+1). */
 static void build_iter(obvh *b, build_ctx *c)
 {
@@ -229,10 +266,15 @@ static void build_iter(obvh *b, build_ctx *c)
         }
         int axis = 0;
         for (int k = 1; k < 3; k++) if (chi[k] - clo[k] > chi[axis] - clo[axis]) axis = k;
+        uint32_t half = it.count / 2;
+        /* the median split of a full sort by (centroid on the axis, index);
+         * a child that becomes a leaf keeps the sorted order, as the leaf's
+         * triangle order decides which of two equal hits is tested first */
+        select_kth(b->order + it.first, it.count, half, c->cent, axis);
         cmp_axis = axis;
         cmp_cent = c->cent;
-        qsort(b->order + it.first, it.count, sizeof(uint32_t), cmp_key);
-        uint32_t half = it.count / 2;
+        if (half <= 4) qsort(b->order + it.first, half, sizeof(uint32_t), cmp_key);
+        if (it.count - half <= 4) qsort(b->order + it.first + half, it.count - half, sizeof(uint32_t), cmp_key);
         int32_t l = b->nnodes;
         b->nnodes += 2;
         nd->left = l; nd->first = 0; nd->count = 0;

@@ -15,6 +15,10 @@ has no learned component, so this is this project's own oracle):
   cos; 56..71 the 16 real spherical harmonics of degree < 4 of the outgoing
   direction; 72..74 normal, 75 roughness, 76..78 albedo, 79 constant 1,
   80..95 zero.
+* encoding "freq12" (the frequency-only one): for axis a and band b < 12,
+  column 24a + 2b = sin(2^b pi x_a), the next cos; 72..74 outgoing
+  direction, 75..77 normal, 78 roughness, 79..81 albedo, 82 constant 1,
+  83..95 zero; no grid.
 * network: 96 -> 64 -> 64 -> 64 -> 64 -> 64 -> 8 (3 used), ReLU after every
   hidden layer, no biases, weights per layer row-major [in][out] in one flat
   vector of 23,040 floats.
@@ -104,7 +108,22 @@ def init_grid(seed=0):
     return rng.uniform(-1e-4, 1e-4, GRID_PARAMS).astype(np.float32)
 
 
-def encode(raw, grid):
+def encode_freq12(raw):
+    r = np.asarray(raw, np.float32).astype(np.float64)
+    x = np.zeros((r.shape[0], IN))
+    for a in range(3):
+        for b in range(12):
+            arg = np.pi * r[:, a] * (2.0 ** b)
+            x[:, 24 * a + 2 * b] = np.sin(arg)
+            x[:, 24 * a + 2 * b + 1] = np.cos(arg)
+    x[:, 72:82] = r[:, 3:13]
+    x[:, 82] = 1.0
+    return x
+
+
+def encode(raw, grid, encoding="hashgrid"):
+    if encoding == "freq12":
+        return encode_freq12(raw)
     raw = np.asarray(raw, np.float32)
     n = raw.shape[0]
     x = np.zeros((n, IN))
@@ -128,10 +147,10 @@ def unflatten(params):
     return [p[OFFS[l]:OFFS[l + 1]].reshape(DIMS[l]) for l in range(LAYERS)]
 
 
-def forward(params, raw, grid, bf=True):
+def forward(params, raw, grid, bf=True, encoding="hashgrid"):
     r = bf16 if bf else (lambda v: v)
     W = [r(w) for w in unflatten(params)]
-    h = r(encode(raw, grid))
+    h = r(encode(raw, grid, encoding))
     acts = [h]
     for l in range(LAYERS - 1):
         h = r(np.maximum(h @ W[l], 0.0))
@@ -140,10 +159,10 @@ def forward(params, raw, grid, bf=True):
     return y[:, :3], acts, W
 
 
-def loss_and_grads(params, raw, target, grid, bf=True):
-    """(loss, weight gradient, grid gradient)."""
+def loss_and_grads(params, raw, target, grid, bf=True, encoding="hashgrid"):
+    """(loss, weight gradient, grid gradient; zero without a grid)."""
     r = bf16 if bf else (lambda v: v)
-    y, acts, W = forward(params, raw, grid, bf)
+    y, acts, W = forward(params, raw, grid, bf, encoding)
     t = np.asarray(target, np.float64)
     n = y.shape[0]
     den = y * y + 0.01
@@ -160,8 +179,10 @@ def loss_and_grads(params, raw, target, grid, bf=True):
     g = np.concatenate([gl.reshape(-1) for gl in grads])
     g[OFFS[5]:].reshape(HID, OUTP)[:, 3:] = 0.0
     # through the encoding: dX of the grid columns, scattered to the corners
-    dx = dz @ W[0].T
     gg = np.zeros((GRID_LEVELS, GRID_SIZE, GRID_FEAT))
+    if encoding != "hashgrid":
+        return loss, g, gg.reshape(-1)
+    dx = dz @ W[0].T
     pos = np.asarray(raw, np.float32)[:, 0:3]
     for l in range(GRID_LEVELS):
         idx, w = grid_corners(pos, l)

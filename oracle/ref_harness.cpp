@@ -41,6 +41,8 @@
 #include "Camera/PerspectiveCamera.h"
 #include "Integrator/PathIntegrator.h"
 #include "Light/DiffuseAreaLight.h"
+#include "Light/InfiniteAreaLight.h"
+#include "Renderer/BasicRenderer.h"
 #include "Material/Glass.h"
 #include "Material/Matte.h"
 #include "Material/Mirror.h"
@@ -131,15 +133,30 @@ struct BoxScene
 	std::vector<IPrimitive *> prims;
 	std::vector<IMaterial *> mats;
 	ILight *light = nullptr;
+	ILight *infinite = nullptr;
 	IShape *quadShape = nullptr;
+
+	// The scene's LightList: the area light, then the infinite light.
+	std::vector<ILight *> lights() const
+	{
+		std::vector<ILight *> l;
+		if (light) l.push_back(light);
+		if (infinite) l.push_back(infinite);
+		return l;
+	}
 
 	// kinds (optional, one per primitive): 0 MatteMaterial(albedo), 2
 	// MirrorMaterial(albedo), 3 GlassMaterial(albedo, transmittance, 1,
 	// eta_i, eta_t) with spec[5 * p ..] = transmittance rgb, eta_i, eta_t.
+	// light_kind 0: primitive light_prim is the Quad(quad) light; 1: it is
+	// the BVHMesh of its own triangles, emitting as a DiffuseAreaLight on
+	// that mesh; -1: no area light. inf (optional): an InfiniteAreaLight
+	// of that intensity, without a texture, joins the lights.
 	void create(const float *pos, const int32_t *prim_of_tri, int ntris, int nprims, const float *albedo,
 	            int light_prim, const float *quad, const float *emit, const int32_t *kinds = nullptr,
-	            const float *spec = nullptr)
+	            const float *spec = nullptr, int light_kind = 0, const float *inf = nullptr)
 	{
+		if (inf) infinite = new InfiniteAreaLight(Spectrum(inf[0], inf[1], inf[2]));
 		for (int p = 0; p < nprims; p++) {
 			const Spectrum a(albedo[3 * p], albedo[3 * p + 1], albedo[3 * p + 2]);
 			const int kind = kinds ? kinds[p] : 0;
@@ -152,7 +169,7 @@ struct BoxScene
 			else
 				m = new MatteMaterial(a);
 			mats.push_back(m);
-			if (p == light_prim) {
+			if (p == light_prim && light_kind == 0) {
 				Quad *qs = new Quad(Vector3(quad[0], quad[1], quad[2]), Vector3(quad[3], quad[4], quad[5]),
 				                    Vector3(quad[6], quad[7], quad[8]), Vector3(quad[9], quad[10], quad[11]));
 				qs->ComputeBoundingVolume();
@@ -186,6 +203,16 @@ struct BoxScene
 			mesh->ComputeBoundingVolume();
 			mesh->Compile();
 			meshes.push_back(mesh);
+			if (p == light_prim && light_kind == 1) {
+				EmissivePrimitive *ep = new EmissivePrimitive();
+				ep->SetShape(mesh);
+				ep->SetMaterial(m);
+				DiffuseAreaLight *dl = new DiffuseAreaLight(nullptr, mesh, Spectrum(emit[0], emit[1], emit[2]));
+				ep->SetLight(dl);
+				light = dl;
+				prims.push_back(ep);
+				continue;
+			}
 			GeometricPrimitive *gp = new GeometricPrimitive();
 			gp->SetShape(mesh);
 			gp->SetMaterial(m);
@@ -206,14 +233,15 @@ struct BoxScene
 		for (auto *m : meshes) delete m;
 		for (auto *m : mats) delete m;
 		delete light;
+		delete infinite;
 		delete quadShape;
 	}
 };
 
 // Reference renderer loop over any space (see ilref_render_box).
-void render_over(ISpace &space, ILight *light, const float *eye, const float *target, const float *up, float fov,
-                 float aspect, int width, int height, int spp, int max_depth, float eps, uint32_t seed,
-                 int nthreads, float *out, float *out_direct = nullptr, float *out_albedo = nullptr)
+void render_over(ISpace &space, const std::vector<ILight *> &lights, const float *eye, const float *target,
+                 const float *up, float fov, float aspect, int width, int height, int spp, int max_depth, float eps,
+                 uint32_t seed, int nthreads, float *out, float *out_direct = nullptr, float *out_albedo = nullptr)
 {
 	PerspectiveCamera camera(Vector3(eye[0], eye[1], eye[2]),
 	                         Vector3::Normalize(Vector3(target[0], target[1], target[2]) - Vector3(eye[0], eye[1], eye[2])),
@@ -229,7 +257,7 @@ void render_over(ISpace &space, ILight *light, const float *eye, const float *ta
 	auto worker = [&]() {
 		RandomSampler sampler;
 		Scene scene(&space, &camera, &sampler);
-		if (light) scene.LightList.PushBack(light);
+		for (ILight *l : lights) scene.LightList.PushBack(l);
 		PathIntegrator integrator(max_depth, 1, eps);
 		integrator.Initialise(&scene, &camera);
 		BoxFilter filter;
@@ -483,7 +511,7 @@ int ilref_render_box(const float *pos, const int32_t *prim_of_tri, int ntris, in
 	scene.create(pos, prim_of_tri, ntris, nprims, albedo, light_prim, quad, emit);
 	BasicSpace space;
 	scene.fill(space);
-	render_over(space, scene.light, eye, target, up, fov, aspect, width, height, spp, max_depth, eps, seed,
+	render_over(space, scene.lights(), eye, target, up, fov, aspect, width, height, spp, max_depth, eps, seed,
 	            nthreads, out);
 	return 0;
 }
@@ -501,7 +529,7 @@ int ilref_render_box_materials(const float *pos, const int32_t *prim_of_tri, int
 	scene.create(pos, prim_of_tri, ntris, nprims, albedo, light_prim, quad, emit, kinds, spec);
 	BasicSpace space;
 	scene.fill(space);
-	render_over(space, scene.light, eye, target, up, fov, aspect, width, height, spp, max_depth, eps, seed,
+	render_over(space, scene.lights(), eye, target, up, fov, aspect, width, height, spp, max_depth, eps, seed,
 	            nthreads, out);
 	return 0;
 }
@@ -519,36 +547,53 @@ int ilref_render_box_aov(const float *pos, const int32_t *prim_of_tri, int ntris
 	scene.create(pos, prim_of_tri, ntris, nprims, albedo, light_prim, quad, emit);
 	BasicSpace space;
 	scene.fill(space);
-	render_over(space, scene.light, eye, target, up, fov, aspect, width, height, spp, max_depth, eps, seed,
+	render_over(space, scene.lights(), eye, target, up, fov, aspect, width, height, spp, max_depth, eps, seed,
 	            nthreads, out, out_direct, out_albedo);
 	return 0;
 }
 
-// The box scene through a plug-in's renderer and space (both made by the
-// factories registered under `factory`): the engine's own objects (Scene,
-// PerspectiveCamera, PathIntegrator(max_depth, 1, eps), BoxFilter,
-// RadianceBuffer) wired to the renderer as the Sandbox wires a BasicRenderer,
-// and rendered with IRenderer::Render(buffer) (tile <= 0) or with
-// RenderRegion(buffer, x, y, w, h, x, y) over tile x tile regions. Outputs
-// the buffer's Final, Direct and Albedo (height x width x 3 each).
-int ilref_render_box_renderer(const char *plugin_path, const char *factory,
-                              const float *pos, const int32_t *prim_of_tri, int ntris, int nprims,
-                              const float *albedo, int light_prim, const float *quad, const float *emit,
-                              const float *eye, const float *target, const float *up, float fov, float aspect,
-                              int width, int height, int spp, int max_depth, float eps, int tile,
-                              float *out, float *out_direct, float *out_albedo, const int32_t *kinds,
-                              const float *spec, char *err, int err_len)
+// The box scene rendered by the engine's own objects (Scene,
+// PerspectiveCamera, BoxFilter, RadianceBuffer) over a plug-in's space (made
+// by the factory `space_factory`), wired to a renderer as the Sandbox wires
+// one: the renderer made by `renderer_factory` (or the reference's
+// BasicRenderer when it is empty) and the integrator made by
+// `integrator_factory` with the arguments RayDepth = max_depth, ShadowRays =
+// 1, Epsilon = eps plus `integrator_args` ("Key=Value;..."; or the
+// reference's PathIntegrator(max_depth, 1, eps) when the factory name is
+// empty). Rendered with IRenderer::Render(buffer) (tile <= 0) or with
+// RenderRegion(buffer, x, y, w, h, x, y) over tile x tile regions. Outputs the
+// buffer's Final, Direct and Albedo (height x width x 3 each). light_kind and
+// inf choose the lights as BoxScene::create does.
+int ilref_render_box_engine(const char *plugin_path, const char *space_factory, const char *renderer_factory,
+                            const char *integrator_factory, const char *integrator_args,
+                            const float *pos, const int32_t *prim_of_tri, int ntris, int nprims,
+                            const float *albedo, int light_prim, const float *quad, const float *emit,
+                            const int32_t *kinds, const float *spec, int light_kind, const float *inf,
+                            const float *eye, const float *target, const float *up, float fov, float aspect,
+                            int width, int height, int spp, int max_depth, float eps, int tile,
+                            float *out, float *out_direct, float *out_albedo, char *err, int err_len)
 {
 	PluginSpace ps;
-	int rc = ps.open(plugin_path, factory, err, err_len);
+	int rc = ps.open(plugin_path, space_factory, err, err_len);
 	if (rc) return rc;
-	Factory<IRenderer> *rf = ps.kernel->GetRendererManager()->RequestFactory(factory);
-	if (!rf) {
-		report(err, err_len, std::string("no renderer factory named ") + factory);
-		return -3;
+	Factory<IRenderer> *rf = nullptr;
+	if (renderer_factory && *renderer_factory) {
+		rf = ps.kernel->GetRendererManager()->RequestFactory(renderer_factory);
+		if (!rf) {
+			report(err, err_len, std::string("no renderer factory named ") + renderer_factory);
+			return -3;
+		}
+	}
+	Factory<IIntegrator> *inf_factory = nullptr;
+	if (integrator_factory && *integrator_factory) {
+		inf_factory = ps.kernel->GetIntegratorManager()->RequestFactory(integrator_factory);
+		if (!inf_factory) {
+			report(err, err_len, std::string("no integrator factory named ") + integrator_factory);
+			return -3;
+		}
 	}
 	BoxScene boxes;
-	boxes.create(pos, prim_of_tri, ntris, nprims, albedo, light_prim, quad, emit, kinds, spec);
+	boxes.create(pos, prim_of_tri, ntris, nprims, albedo, light_prim, quad, emit, kinds, spec, light_kind, inf);
 	boxes.fill(*ps.space);
 	if (!ps.space->Initialise() || !ps.space->Build()) {
 		ps.report_build_failure(err, err_len);
@@ -560,22 +605,48 @@ int ilref_render_box_renderer(const char *plugin_path, const char *factory,
 	camera.SetFieldOfView(fov, aspect);
 	RandomSampler sampler;
 	Scene scene(ps.space, &camera, &sampler);
-	if (boxes.light) scene.LightList.PushBack(boxes.light);
-	PathIntegrator integrator(max_depth, 1, eps);
-	integrator.Initialise(&scene, &camera);
+	for (ILight *l : boxes.lights()) scene.LightList.PushBack(l);
 	BoxFilter filter;
 	MemoryDevice device(width, height);
 	RadianceBuffer buffer(width, height);
 	IRenderer *renderer = nullptr;
+	IIntegrator *integrator = nullptr;
 	try {
-		std::map<std::string, std::string> args;
-		args["Samples"] = std::to_string(spp);
-		ArgumentMap am(args);
-		renderer = rf->CreateInstance(am);
-		renderer->SetScene(&scene);
-		renderer->SetIntegrator(&integrator);
-		renderer->SetDevice(&device);
-		renderer->SetFilter(&filter);
+		if (inf_factory) {
+			std::map<std::string, std::string> args;
+			args["RayDepth"] = std::to_string(max_depth);
+			args["ShadowRays"] = "1";
+			char e[32];
+			snprintf(e, sizeof(e), "%.9g", eps);
+			args["Epsilon"] = e;
+			std::string extra = integrator_args ? integrator_args : "";
+			size_t at = 0;
+			while (at < extra.size()) {
+				size_t semi = extra.find(';', at);
+				if (semi == std::string::npos) semi = extra.size();
+				const std::string kv = extra.substr(at, semi - at);
+				const size_t eq = kv.find('=');
+				if (eq != std::string::npos) args[kv.substr(0, eq)] = kv.substr(eq + 1);
+				at = semi + 1;
+			}
+			ArgumentMap am(args);
+			integrator = inf_factory->CreateInstance(am);
+		} else {
+			integrator = new PathIntegrator(max_depth, 1, eps);
+		}
+		integrator->Initialise(&scene, &camera);
+		if (rf) {
+			std::map<std::string, std::string> args;
+			args["Samples"] = std::to_string(spp);
+			ArgumentMap am(args);
+			renderer = rf->CreateInstance(am);
+			renderer->SetScene(&scene);
+			renderer->SetIntegrator(integrator);
+			renderer->SetDevice(&device);
+			renderer->SetFilter(&filter);
+		} else {
+			renderer = new BasicRenderer(&scene, integrator, &device, &filter, &buffer, spp);
+		}
 		// (IRenderer::SetRadianceBuffer is declared but never defined in the
 		// engine, so the buffer goes to the calls that take one)
 		renderer->Initialise();
@@ -590,6 +661,12 @@ int ilref_render_box_renderer(const char *plugin_path, const char *factory,
 	} catch (const Exception &e) {
 		report(err, err_len, e.GetMessage());
 		delete renderer;
+		delete integrator;
+		return -5;
+	} catch (const Exception *e) {
+		report(err, err_len, e->GetMessage());
+		delete renderer;
+		delete integrator;
 		return -5;
 	}
 	for (int y = 0; y < height; y++)
@@ -603,6 +680,42 @@ int ilref_render_box_renderer(const char *plugin_path, const char *factory,
 			}
 		}
 	delete renderer;
+	delete integrator;
+	return 0;
+}
+
+// ilref_render_box_engine with the plug-in's renderer (factory `factory`), its
+// space (the same factory name) and the reference's PathIntegrator.
+int ilref_render_box_renderer(const char *plugin_path, const char *factory,
+                              const float *pos, const int32_t *prim_of_tri, int ntris, int nprims,
+                              const float *albedo, int light_prim, const float *quad, const float *emit,
+                              const float *eye, const float *target, const float *up, float fov, float aspect,
+                              int width, int height, int spp, int max_depth, float eps, int tile,
+                              float *out, float *out_direct, float *out_albedo, const int32_t *kinds,
+                              const float *spec, char *err, int err_len)
+{
+	return ilref_render_box_engine(plugin_path, factory, factory, "", "", pos, prim_of_tri, ntris, nprims, albedo,
+	                               light_prim, quad, emit, kinds, spec, 0, nullptr, eye, target, up, fov, aspect,
+	                               width, height, spp, max_depth, eps, tile, out, out_direct, out_albedo, err,
+	                               err_len);
+}
+
+// The box scene through the reference's PathIntegrator (render_over) with a
+// choice of lights (BoxScene::create: light_kind, inf) and materials, plus
+// the RadianceContext's Direct and Albedo (either may be null).
+int ilref_render_box_lights(const float *pos, const int32_t *prim_of_tri, int ntris, int nprims,
+                            const float *albedo, int light_prim, const float *quad, const float *emit,
+                            const int32_t *kinds, const float *spec, int light_kind, const float *inf,
+                            const float *eye, const float *target, const float *up, float fov, float aspect,
+                            int width, int height, int spp, int max_depth, float eps, uint32_t seed,
+                            int nthreads, float *out, float *out_direct, float *out_albedo)
+{
+	BoxScene scene;
+	scene.create(pos, prim_of_tri, ntris, nprims, albedo, light_prim, quad, emit, kinds, spec, light_kind, inf);
+	BasicSpace space;
+	scene.fill(space);
+	render_over(space, scene.lights(), eye, target, up, fov, aspect, width, height, spp, max_depth, eps, seed,
+	            nthreads, out, out_direct, out_albedo);
 	return 0;
 }
 
@@ -630,7 +743,7 @@ int ilref_render_box_plugin(const char *plugin_path, const char *factory,
 		ps.report_build_failure(err, err_len);
 		return -4;
 	}
-	render_over(*ps.space, scene.light, eye, target, up, fov, aspect, width, height, spp, max_depth, eps, seed,
+	render_over(*ps.space, scene.lights(), eye, target, up, fov, aspect, width, height, spp, max_depth, eps, seed,
 	            nthreads, out);
 	return 0;
 }

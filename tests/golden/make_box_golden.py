@@ -2,13 +2,20 @@
 its sources into oracle/_ref/libilref.so) and store the image as the
 path-tracing parity fixture.
 
-    python tests/golden/make_box_golden.py [spp] [seed] [specular] [size]
+    python tests/golden/make_box_golden.py [spp] [seed] [variant] [size]
 
 Default: 256 x 256 at 4096 samples per pixel, seed 1 (about 7 minutes on 8
 cores). The GPU path tracer's converged image must match it within
-relMSE 1e-3 (tests/test_render_gpu.py). With `specular` = 1 the scene's
-short box is a mirror and its tall box glass (scenes.box_scene(True)); the
-fixture is named box_specular_<size>_<spp>spp_seed<seed>.npz.
+relMSE 1e-3 (tests/test_render_gpu.py). Variants (scenes.box_scene):
+  0 / plain   the box scene: box_<size>_<spp>spp_seed<seed>.npz
+  1 / specular  short box a mirror, tall box glass: box_specular_...
+  meshlight   the ceiling light a 6-triangle mesh of unequal triangles
+              (DiffuseAreaLight on a triangle mesh): box_meshlight_...
+  infinite    the specular box plus an InfiniteAreaLight of intensity
+              (0.5, 0.6, 0.8), camera at 60 deg so border pixels see past
+              the box: box_infinite_...
+The mesh-light and infinite-light fixtures also hold the RadianceContext's
+Direct ("direct").
 """
 from __future__ import annotations
 
@@ -25,19 +32,33 @@ from illuminaprt_b200.scenes import box_scene  # noqa: E402
 from oracle.bindings import RefLib, build  # noqa: E402
 
 
+VARIANTS = {
+    "plain": ("box", lambda: box_scene()),
+    "specular": ("box_specular", lambda: box_scene(True)),
+    "meshlight": ("box_meshlight", lambda: box_scene(light="mesh")),
+    "infinite": ("box_infinite", lambda: box_scene(True, infinite=(0.5, 0.6, 0.8), fov=60.0)),
+}
+
+
 def main():
     spp = int(sys.argv[1]) if len(sys.argv) > 1 else 4096
     seed = int(sys.argv[2]) if len(sys.argv) > 2 else 1
-    specular = len(sys.argv) > 3 and sys.argv[3] == "1"
+    variant = sys.argv[3] if len(sys.argv) > 3 else "plain"
+    variant = {"0": "plain", "1": "specular"}.get(variant, variant)
     size = int(sys.argv[4]) if len(sys.argv) > 4 else 256
     build(ref=True)
-    scene = box_scene(specular)
+    prefix, make = VARIANTS[variant]
+    scene = make()
     t0 = time.time()
-    img = RefLib().render_box(scene, size, size, spp, seed)
+    extra = {}
+    if variant in ("plain", "specular"):
+        img = RefLib().render_box(scene, size, size, spp, seed)
+    else:
+        img, direct, _ = RefLib().render_box_lights(scene, size, size, spp, seed)
+        extra["direct"] = direct
     dt = time.time() - t0
-    name = f"box_specular_{size}" if specular else f"box_{size}"
-    path = os.path.join(HERE, f"{name}_{spp}spp_seed{seed}.npz")
-    np.savez_compressed(path, image=img, spp=spp, seed=seed, seconds=dt, threads=os.cpu_count())
+    path = os.path.join(HERE, f"{prefix}_{size}_{spp}spp_seed{seed}.npz")
+    np.savez_compressed(path, image=img, spp=spp, seed=seed, seconds=dt, threads=os.cpu_count(), **extra)
     print(path, f"{dt:.1f} s", img.mean(axis=(0, 1)))
 
 

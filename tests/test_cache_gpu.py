@@ -78,9 +78,14 @@ def test_hash_grid_cache_baseline(field):
     kw = dict(max_depth=12, sky=s["sky"], cache_depth=1, hash_cache=True)
     sp.hash_cache_reset()
     empty = sp.render(cam, W, H, 64, seed=7, **kw)
+    dropped = records = 0
     for f in range(40):
         img = sp.render(cam, W, H, 1, seed=3000 + f, train_tail=2, **kw)
         assert np.isfinite(img).all()
+        r, d = sp.last_train_stats()
+        records, dropped = records + r, dropped + d
+    # every record found a cell: none was lost to a full probe window
+    assert records > 0 and dropped <= records // 10000
     filled = sp.render(cam, W, H, 64, seed=8, **kw)
     e0, e1 = rel_mse(empty, gt), rel_mse(filled, gt)
     print(f"hash-grid cache, 64-spp relMSE empty / after 40 frames: {e0:.4f} / {e1:.4f}")

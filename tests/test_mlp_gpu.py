@@ -101,3 +101,31 @@ def test_tcgen05_inference_matches_warp_mma(net, n):
     print(f"n={n}: tcgen05 vs mma.sync {d_warp:.2e}, vs oracle {d_ref:.2e}")
     assert d_warp < 1e-2 and d_ref < 1e-2
     assert np.mean(np.abs(y_tc - y_warp)) / (np.mean(np.abs(y_warp)) + 1e-9) < 2e-3
+
+
+@pytest.mark.parametrize("n", [16, 5000])
+def test_frequency_encoding_matches_oracle(n):
+    """The frequency-only encoding (12 bands of position + raw direction,
+    normal, roughness, albedo): forward and gradients against the oracle."""
+    from illuminaprt_b200.ilg import GpuSpace
+    sp = GpuSpace()
+    sp.mlp_init(seed=5, lr=1e-2, encoding="freq12")
+    raw, tgt = mo.random_batch(n, seed=n + 1)
+    for _ in range(2):  # move the weights away from their initial values
+        sp.mlp_train_step(raw, tgt)
+    p = sp.mlp_params()
+    y_ref, _, _ = mo.forward(p, raw, None, bf=True, encoding="freq12")
+    y = sp.mlp_infer(raw)
+    y_warp = sp.mlp_infer(raw, warp_mma=True)
+    scale = np.abs(y_ref).max()
+    assert np.abs(y - y_ref).max() / scale < 1e-2 and np.abs(y_warp - y_ref).max() / scale < 1e-2
+    loss_g, g_gpu = sp.mlp_grads(raw, tgt)
+    loss_r, g_ref, gg_ref = mo.loss_and_grads(p, raw, tgt, None, bf=True, encoding="freq12")
+    _, g_exact, _ = mo.loss_and_grads(p, raw, tgt, None, bf=False, encoding="freq12")
+    rel = np.linalg.norm(g_gpu - g_ref) / np.linalg.norm(g_ref)
+    cos_exact = g_gpu @ g_exact / (np.linalg.norm(g_gpu) * np.linalg.norm(g_exact))
+    print(f"freq12 n={n}: loss {loss_g:.6f} / {loss_r:.6f}; grad rel err {rel:.2e}; cosine vs exact {cos_exact:.5f}")
+    assert abs(loss_g - loss_r) <= 1e-3 * abs(loss_r) + 1e-6
+    assert rel < 3e-2 and cos_exact > 0.995
+    assert not gg_ref.any()
+    sp.close()

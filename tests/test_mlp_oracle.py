@@ -88,3 +88,31 @@ def test_grid_indexing():
     # a constant grid encodes to that constant everywhere
     g = np.full(mo.GRID_PARAMS, 0.25, np.float32)
     assert np.allclose(mo.grid_features(g, pos), 0.25, atol=1e-6)
+
+
+def test_frequency_encoding_backward_matches_autograd():
+    import torch
+    raw, tgt = mo.random_batch(48, seed=8)
+    x = mo.encode(raw, None, "freq12")
+    # columns as documented: band 11 of axis 2, then the raw features and the constant
+    assert np.allclose(x[:, 24 * 2 + 22], np.sin(np.pi * raw[:, 2].astype(np.float64) * 2048))
+    assert np.array_equal(x[:, 72:82], raw[:, 3:13].astype(np.float64)) and (x[:, 82] == 1).all()
+    assert not x[:, 83:].any()
+    p = mo.init_params(seed=2).astype(np.float64)
+    loss, g, gg = mo.loss_and_grads(p, raw, tgt, None, bf=False, encoding="freq12")
+    pt = torch.tensor(p, dtype=torch.float64, requires_grad=True)
+    h = torch.tensor(x, dtype=torch.float64)
+    for l in range(mo.LAYERS):
+        w = pt[mo.OFFS[l]:mo.OFFS[l + 1]].reshape(mo.DIMS[l])
+        h = h @ w
+        if l < mo.LAYERS - 1:
+            h = torch.relu(h)
+    y = h[:, :3]
+    t = torch.tensor(tgt, dtype=torch.float64)
+    lt = ((y - t) ** 2 / (y.detach() ** 2 + 0.01)).mean()
+    lt.backward()
+    gref = pt.grad.numpy().copy()
+    gref[mo.OFFS[5]:].reshape(mo.HID, mo.OUTP)[:, 3:] = 0.0
+    assert abs(loss - lt.item()) < 1e-12
+    assert np.allclose(g, gref, rtol=1e-9, atol=1e-12)
+    assert not gg.any()

@@ -136,3 +136,56 @@ def test_gpu_renderer_renders_mirror_and_glass_like_the_reference():
     # independent noise alone gives (1/8192 + 1/4096) / (1/1024 + 1/4096) = 0.3 of the floor
     assert err < 0.5 * floor
     assert np.allclose(final.mean((0, 1)), ref_img.mean((0, 1)), rtol=1e-2)
+
+
+@pytest.mark.parametrize("prefix,kw", [("box_meshlight", dict(light="mesh")),
+                                       ("box_infinite", dict(specular=True, infinite=(0.5, 0.6, 0.8), fov=60.0))])
+def test_gpu_renderer_renders_mesh_and_infinite_lights_like_the_reference(prefix, kw):
+    # a DiffuseAreaLight on a triangle mesh and an InfiniteAreaLight reach the
+    # device through the engine's LightList (PrepareDeviceScene)
+    p4096 = os.path.join(os.path.dirname(__file__), "golden", f"{prefix}_128_4096spp_seed1.npz")
+    if not os.path.exists(p4096):
+        pytest.skip("no reference image")
+    ref_img = np.load(p4096)["image"]
+    floor = _rel_mse(np.load(p4096.replace("4096spp_seed1", "1024spp_seed2"))["image"], ref_img)
+    scene = scenes.box_scene(**kw)
+    final, direct, albedo = bindings.RefLib().render_box_engine(pkg_build.PLUGIN, scene, 128, 128, 8192)
+    err = _rel_mse(final, ref_img)
+    print(f"{prefix}: relMSE(GpuRenderer 8192 spp, reference 4096 spp) = {err:.2e}; reference floor {floor:.2e}")
+    assert np.isfinite(final).all()
+    assert err < 0.5 * floor
+    assert np.allclose(final.mean((0, 1)), ref_img.mean((0, 1)), rtol=1e-2)
+
+
+@pytest.mark.parametrize("kw", [dict(), dict(light="mesh"), dict(specular=True, infinite=(0.5, 0.6, 0.8), fov=60.0)],
+                         ids=["quad", "meshlight", "infinite"])
+def test_reference_renderer_over_the_device_integrator(kw):
+    # the reference's BasicRenderer calling GpuPathIntegrator::Radiance once
+    # per pixel sample: every path runs on the device (ilg_radiance), none on
+    # the CPU. Its image against the reference's own PathIntegrator at 4096
+    # spp: no further from it than a 64-spp reference render is
+    scene = scenes.box_scene(**kw)
+    w = h = 32
+    ref = bindings.RefLib()
+    truth = ref.render_box_lights(scene, w, h, 4096, seed=1)[0]
+    noisy = ref.render_box_lights(scene, w, h, 64, seed=2)[0]
+    floor = _rel_mse(noisy, truth)
+    final, direct, albedo = ref.render_box_engine(pkg_build.PLUGIN, scene, w, h, 64, renderer="", integrator="GPU")
+    err = _rel_mse(final, truth)
+    print(f"{kw}: relMSE(BasicRenderer + device Radiance 64 spp, reference 4096 spp) = {err:.2e}; "
+          f"reference 64 spp: {floor:.2e}")
+    assert np.isfinite(final).all()
+    assert err < 1.5 * floor
+    assert np.allclose(final.mean((0, 1)), truth.mean((0, 1)), rtol=3e-2)
+    # Direct is part of Final, and the first hit's albedo is filled
+    assert (direct <= final + 1e-4).all() and albedo.mean() > 0.1
+
+
+def test_device_integrator_refuses_what_it_cannot_run():
+    # no CPU fallback: the learned cache under a per-sample renderer is
+    # refused with the reason (it would never train there)
+    scene = scenes.box_scene()
+    ref = bindings.RefLib()
+    with pytest.raises(RuntimeError, match="Cache = MLP"):
+        ref.render_box_engine(pkg_build.PLUGIN, scene, 8, 8, 1, renderer="", integrator="GPU",
+                              integrator_args={"Cache": "MLP"})

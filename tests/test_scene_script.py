@@ -114,19 +114,17 @@ def test_script_naming_the_gpu_space_fails_loudly_without_a_gpu(tmp_path):
 
 @needs_ref
 @pytest.mark.skipif(not os.path.exists(pkg_build.PLUGIN), reason="plug-in not built")
-def test_gpu_integrator_is_the_reference_path_integrator_under_cpu_renderers(tmp_path):
-    # Integrator { Type = GPU } makes a GpuPathIntegrator; under the
-    # reference's BasicRenderer over BasicSpace it is the reference's
-    # PathIntegrator (same fixed-seed sampler): the same image, bit for bit
-    w, spp = 24, 4
-    ref = bindings.RefLib()
-    a = ref.render_script(scenes.write_box_script(tmp_path / "pt", width=w, height=w, spp=spp, space="Basic",
-                                                  renderer="Basic"), w, w, plugin=pkg_build.PLUGIN)[0]
-    b = ref.render_script(scenes.write_box_script(tmp_path / "gpu", width=w, height=w, spp=spp, space="Basic",
-                                                  renderer="Basic", integrator="GPU",
-                                                  integrator_args={"Cache": "MLP", "TrainFraction": 0.125}),
-                          w, w, plugin=pkg_build.PLUGIN)[0]
-    assert np.array_equal(a, b)
+@pytest.mark.parametrize("args,reason", [({}, "not a GpuSpace"), ({"Cache": "MLP"}, "Cache = MLP")])
+def test_gpu_integrator_has_no_cpu_path(tmp_path, args, reason):
+    # Integrator { Type = GPU } makes a GpuPathIntegrator, whose Radiance runs
+    # on the device: under the reference's BasicRenderer over its BasicSpace
+    # there is no device scene, and the learned cache cannot train one sample
+    # at a time, so both are refused with the reason (no device call is
+    # made, so this runs without a GPU)
+    script = scenes.write_box_script(tmp_path, width=8, height=8, spp=1, space="Basic", renderer="Basic",
+                                     integrator="GPU", integrator_args=args)
+    with pytest.raises(RuntimeError, match=reason):
+        bindings.RefLib().render_script(script, 8, 8, plugin=pkg_build.PLUGIN)
 
 
 @needs_ref

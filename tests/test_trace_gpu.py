@@ -73,7 +73,10 @@ def test_full_size_heightfield_sample(oracle):
     ref = oracle.bvh(pos, idx).intersect(o4, d4)
     n_same, ties, bad, bits_ok = classify(pos, idx, o4, d4, got, ref, oracle)
     assert bad == [] and bits_ok
-    assert ties / len(o4) < 1e-3
+    # near ties (two valid hits < 1e-5 apart, decided by visit order) came to
+    # 1.5e-5 of the full 8,388,608-ray workload against the reference's BVH;
+    # the reference's own KD-tree and BVH disagree at 1.3e-5
+    assert ties / len(o4) < 5e-5
     # size-independent property on the whole incoherent set: a ray that hits
     # reports a t inside its window and barycentrics inside the triangle
     p, t, u, v = sp.intersects(io, idr)

@@ -59,6 +59,30 @@ def test_noalloc_matches_intersect_on_two_calls_in_a_row():
     sp.close()
 
 
+def test_noalloc_allocates_no_device_memory():
+    """The property the entry point exists for: once a context exists, a call
+    leaves the device's free memory unchanged (ilg_create made the fixed array
+    resident and loaded the traversal kernel). Checked on a fresh context
+    before any ilg_intersect call, which would grow the context's staging."""
+    import torch
+    from illuminaprt_b200.ilg import GpuSpace, ILG_OK
+    pos, idx = scenes.heightfield(128, 64, 0.2, 9)
+    sp = GpuSpace()
+    sp.initialise(pos, idx)
+    sp.build()
+    io, idr = scenes.incoherent_rays(pos, idx, 1 << 16, 3)
+    rc, first = _noalloc(sp, io[:1000], idr[:1000])
+    assert rc == ILG_OK, sp.L.ilg_last_error(sp.h)
+    torch.cuda.synchronize()
+    free_before = torch.cuda.mem_get_info(0)[0]
+    rc, second = _noalloc(sp, io, idr)
+    assert rc == ILG_OK, sp.L.ilg_last_error(sp.h)
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info(0)[0] == free_before
+    assert _same(second, sp.intersects(io, idr))
+    sp.close()
+
+
 def test_noalloc_rejects_batches_over_the_limit():
     from illuminaprt_b200.ilg import GpuSpace, ILG_EINVAL, ILG_NOALLOC_MAX_RAYS
     pos, idx = scenes.heightfield(16, 8, 0.2, 5)
