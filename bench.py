@@ -489,18 +489,26 @@ def bench_batch(res, local):
         batch.append({"space": sp_i, "camera": s["camera"], "width": s["width"], "height": s["height"],
                       "spp": s["spp"], "max_depth": s["max_depth"], "seed": 7 + i, "sky": s["sky"]})
     runner = GpuSpace(device=local)
-    choice, _ = tune_batch(runner, batch, waves=(1 << 21, 1 << 22, 1 << 23), blocks=(128, 256))
+    choice, sweep = tune_batch(runner, batch, waves=(1 << 21, 1 << 22, 1 << 23), blocks=(128, 256))
+    kw = {k: choice[k] for k in ("paths_per_wave", "block", "one_launch")}
+    runner.render_batch(batch, **kw)  # this setting's graph
     t0 = time.perf_counter()
-    runner.render_batch(batch, paths_per_wave=choice["paths_per_wave"], block=choice["block"])
+    runner.render_batch(batch, **kw)
     dt = time.perf_counter() - t0
+    best_wave = min((r for r in sweep if not r["one_launch"]), key=lambda r: r["seconds"])
+    one = [r for r in sweep if r["one_launch"]]
+    res["pt_batch32_schedules_msamples_s"] = {
+        "wavefront_best": round(sum(b["width"] * b["height"] * b["spp"] for b in batch) / best_wave["seconds"] / 1e6, 3),
+        "one_launch": round(sum(b["width"] * b["height"] * b["spp"] for b in batch) / one[0]["seconds"] / 1e6, 3)
+        if one else None}
     samples = sum(b["width"] * b["height"] * b["spp"] for b in batch)
     res["pt_batch32_triangles"] = int(sum(s["idx"].shape[0] for s in items))
     res["pt_batch32_samples"] = int(samples)
     res["pt_batch32_ms"] = round(dt * 1e3, 2)
     res["pt_batch32_msamples_s"] = round(samples / dt / 1e6, 3)
-    res["pt_batch32_autotuned"] = {"paths_per_wave": choice["paths_per_wave"], "block": choice["block"]}
+    res["pt_batch32_autotuned"] = kw
     # traversal work of the same batch (a counted render, untimed) -> algorithmic bytes per sample
-    runner.render_batch(batch, paths_per_wave=choice["paths_per_wave"], block=choice["block"], count=True)
+    runner.render_batch(batch, paths_per_wave=choice["paths_per_wave"] or (1 << 22), block=choice["block"], count=True)
     bps = pt_bytes_per_sample(runner.render_counts(), samples)
     hbm, _ = load_peaks()
     gbs = bps * samples / dt / 1e9

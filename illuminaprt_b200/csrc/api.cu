@@ -803,8 +803,11 @@ static int prepare_scene(ilg_ctx *runner, ilg_ctx *ctx, const ilg_camera_frame &
 static int run_render(ilg_ctx *ctx, std::vector<SceneRec> &recs, uint32_t cap_req, uint32_t block,
                       uint32_t cache_depth, uint32_t train_every, uint32_t train_steps, uint32_t train_batch,
                       uint64_t *total_paths_out, bool aux = false, bool count = false, uint32_t train_tail = 0,
-                      uint32_t train_epochs = 1, bool hash_cache = false)
+                      uint32_t train_epochs = 1, bool hash_cache = false, bool one_launch = false)
 {
+    if (one_launch && (cache_depth || aux || count))
+        return fail(ctx, ILG_EINVAL,
+                    "render: ILG_RENDER_PERSISTENT renders plain images only (no cache, Direct / Albedo or counts)");
     cudaStream_t st = ctx->stream;
     uint64_t total = 0, pixels64 = 0;
     uint32_t pixels = 0, depth_max = 0, nl = 1;
@@ -927,18 +930,23 @@ static int run_render(ilg_ctx *ctx, std::vector<SceneRec> &recs, uint32_t cap_re
     uint32_t launches = 0;
     unsigned char key[sizeof(RenderDev) + sizeof(MlpDev) + 4 * sizeof(uint64_t)];
     {
-        const uint64_t extra[4] = {cap, total, block, cache_depth};
+        const uint64_t extra[4] = {cap, total, block, cache_depth | (one_launch ? 0x100000000ull : 0ull)};
         memcpy(key, &R, sizeof(RenderDev));
         memcpy(key + sizeof(RenderDev), &mlp, sizeof(MlpDev));
         memcpy(key + sizeof(RenderDev) + sizeof(MlpDev), extra, sizeof(extra));
     }
     if (!ctx->graph_exec || ctx->graph_key.size() != sizeof(key) || memcmp(ctx->graph_key.data(), key, sizeof(key))) {
         ctx->drop_graph();
+        if (one_launch) CK(ctx->persist_next.reserve(1));
         CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
         cudaError_t ce = cudaSuccess;
-        for (uint64_t g0 = 0; g0 < total && ce == cudaSuccess; g0 += cap) {
-            const uint32_t k = (uint32_t)std::min<uint64_t>(cap, total - g0);
-            ce = render_wave(R, k, g0, st, &launches, cache_depth ? &mlp : nullptr, block);
+        if (one_launch) {
+            ce = render_persistent(R, total, ctx->persist_next.ptr, &launches, st);
+        } else {
+            for (uint64_t g0 = 0; g0 < total && ce == cudaSuccess; g0 += cap) {
+                const uint32_t k = (uint32_t)std::min<uint64_t>(cap, total - g0);
+                ce = render_wave(R, k, g0, st, &launches, cache_depth ? &mlp : nullptr, block);
+            }
         }
         cudaGraph_t graph = nullptr;
         const cudaError_t ee = cudaStreamEndCapture(st, &graph);
@@ -1019,7 +1027,8 @@ int render_one(ilg_ctx *ctx, const ilg_camera_frame &frame, const ilg_render_opt
     const bool aux = direct_rgb || albedo_rgb;
     rc = run_render(ctx, recs, opts->paths_per_wave, 128, cache_depth, opts->train_every ? opts->train_every : 16u,
                     opts->train_steps, opts->train_batch ? opts->train_batch : 16384u, nullptr, aux,
-                    ctx->counted, opts->train_tail, opts->train_epochs ? opts->train_epochs : 1u, hash_cache);
+                    ctx->counted, opts->train_tail, opts->train_epochs ? opts->train_epochs : 1u, hash_cache,
+                    (flags & ILG_RENDER_PERSISTENT) != 0);
     if (rc) return rc;
     const bool dev = (flags & ILG_DEVICE_PTRS) != 0;
     const float4 *sums[3] = {ctx->accum.ptr, ctx->accum_direct.ptr, ctx->accum_albedo.ptr};
@@ -1054,7 +1063,7 @@ int ilg_render(ilg_ctx *ctx, const ilg_camera *cam, const ilg_render_opts *opts,
 {
     if (!ctx) return ILG_EINVAL;
     if (!cam || !opts || !out_rgb) return fail(ctx, ILG_EINVAL, "ilg_render: null argument");
-    if (flags & ~(ILG_DEVICE_PTRS | ILG_RENDER_COUNT | ILG_RENDER_HASH_CACHE))
+    if (flags & ~(ILG_DEVICE_PTRS | ILG_RENDER_COUNT | ILG_RENDER_HASH_CACHE | ILG_RENDER_PERSISTENT))
         return fail(ctx, ILG_EINVAL, "ilg_render: unknown flags 0x%x", flags);
     ilg_camera_frame frame;
     camera_frame_of(*cam, frame);
@@ -1144,7 +1153,7 @@ int ilg_render_batch(ilg_ctx *runner, const ilg_batch_item *items, uint32_t n, u
 {
     if (!runner) return ILG_EINVAL;
     if (!items || n == 0 || n > 4096) return fail(runner, ILG_EINVAL, "ilg_render_batch: need 1..4096 items");
-    if (flags & ~(ILG_DEVICE_PTRS | ILG_RENDER_COUNT))
+    if (flags & ~(ILG_DEVICE_PTRS | ILG_RENDER_COUNT | ILG_RENDER_PERSISTENT))
         return fail(runner, ILG_EINVAL, "ilg_render_batch: unknown flags 0x%x", flags);
     if (block != 0 && block != 64 && block != 128 && block != 256)
         return fail(runner, ILG_EINVAL, "ilg_render_batch: block must be 64, 128 or 256");
@@ -1162,7 +1171,7 @@ int ilg_render_batch(ilg_ctx *runner, const ilg_batch_item *items, uint32_t n, u
     }
     runner->counted = (flags & ILG_RENDER_COUNT) != 0;
     int rc = run_render(runner, recs, paths_per_wave, block ? block : 128, 0, 16, 0, 16384, nullptr, false,
-                        runner->counted);
+                        runner->counted, 0, 1, false, (flags & ILG_RENDER_PERSISTENT) != 0);
     if (rc) return rc;
     uint32_t max_wh = 0;
     for (auto &S : recs) max_wh = std::max(max_wh, S.wh);

@@ -93,6 +93,8 @@ struct ilg_ctx {
     uint32_t last_render_launches = 0;
     // work counters of the last render made with ILG_RENDER_COUNT
     ilg::DevBuf<unsigned long long> render_stats;
+    // path counter of the one-launch renderer (ILG_RENDER_PERSISTENT)
+    ilg::DevBuf<unsigned long long> persist_next;
     bool counted = false;
     // the last frame's instantiated CUDA graph and the launch configuration it was captured for
     cudaGraphExec_t graph_exec = nullptr;
@@ -157,7 +159,7 @@ struct ilg_ctx {
         drop_graph();
         pos.release(); idx.release(); mat.release();
         bb.release_all();
-        raw_tris.release(); raw_ready = false; render_stats.release();
+        raw_tris.release(); raw_ready = false; render_stats.release(); persist_next.release();
         post_acc.release(); post_in.release(); post_out.release(); post_scratch.release();
         post_pixels = post_frames = 0;
         ro.release(); rd.release(); hprim.release(); ht.release(); hu.release(); hv.release(); hocc.release();

@@ -360,6 +360,122 @@ __device__ __forceinline__ void sample_specular(const Mat &m, float3 wo, float w
     transmit = true;
 }
 
+// One light sample of next-event estimation at a shading point
+// (IIntegrator::EstimateDirectLighting, Core/Integrator/Integrator.cpp:114-139,
+// with the light's SampleRadiance): light l's shadow segment and the
+// contribution it adds when unoccluded; false when the sample adds nothing.
+// The shading frame is (U, V, W) with W the shading normal; wo_l is the
+// outgoing direction in it.
+__device__ __forceinline__ bool light_sample(const SceneRec &S, uint32_t l, uint64_t key, uint32_t depth, float3 p,
+                                             float3 U, float3 V, float3 W, float3 wo_l, const Mat &m, float3 beta,
+                                             float4 &so, float4 &sd, float3 &c)
+{
+    const Light &L = S.lights[l];
+    const float u = rnd(key, dim_of(depth, 2 * l)), v = rnd(key, dim_of(depth, 2 * l + 1));
+    if (L.kind == kLightInfinite) {
+        // InfiniteAreaLight::SampleRadiance (InfiniteAreaLight.cpp:73-83):
+        // a direction in the cone cos(theta) >= 1e-4 about the shading
+        // normal (Montecarlo::UniformSampleCone, Montecarlo.h:74-80), the
+        // light's intensity with no division by the pdf, a shadow ray
+        // over [1e-4, FLT_MAX] from the point itself
+        const float ct = (1.f - u) + u * 1e-4f;
+        const float st = sqrtf(1.f - ct * ct);
+        float sp, cp;
+        sincosf(kTwoPi * v, &sp, &cp);
+        const float3 wi = U * (cp * st) + V * (sp * st) + W * ct;
+        const float3 wi_l = make_float3(dot3(U, wi), dot3(V, wi), dot3(W, wi));
+        c = beta * L.emit * fmaxf(0.f, dot3(wi, W)) * bsdf_f(m, wo_l, wi_l);
+        if (is_black(c)) return false;
+        so = make_float4(p.x, p.y, p.z, 1e-4f);
+        sd = make_float4(wi.x, wi.y, wi.z, FLT_MAX);
+        return true;
+    }
+    float3 P, nl;
+    if (L.kind == kLightMesh) {
+        // ITriangleMesh::SamplePoint (Core/Shape/TriangleMesh.cpp:142-161):
+        // a triangle picked uniformly by index (not by area), a uniform
+        // point on it (IndexedTriangle::SamplePoint, Montecarlo.h:59-64),
+        // its normal (p3 - p1) x (p2 - p1) turned to face the shaded
+        // point; the pdf is 1 / the mesh's whole area (DiffuseAreaLight.cpp:36-40)
+        const uint32_t k = min((uint32_t)((float)L.tri_count * rnd(key, dim_of(depth, 24 + l))),
+                               L.tri_count - 1u);
+        const uint32_t *tv = S.idx + 3ull * (L.first_tri + k);
+        const float *a = S.pos + 3ull * tv[0], *b = S.pos + 3ull * tv[1], *cc = S.pos + 3ull * tv[2];
+        const float3 p1 = make_float3(a[0], a[1], a[2]), p2 = make_float3(b[0], b[1], b[2]),
+                     p3 = make_float3(cc[0], cc[1], cc[2]);
+        const float su = sqrtf(u);
+        const float b1 = 1.f - su, b2 = v * su;
+        P = p1 * b1 + p2 * b2 + p3 * (1.f - b1 - b2);
+        nl = normalize3(cross3(p3 - p1, p2 - p1));
+        if (dot3(P - p, nl) > 0.f) nl = nl * -1.f;
+    } else {
+        // Quad::SamplePoint (Core/Shape/Quad.cpp:144-153): a bilinear
+        // patch over the reference's tessellation vertices
+        P = L.p[0] + (L.p[2] - L.p[0]) * u + (L.p[3] - L.p[2]) * v +
+            (L.p[0] - L.p[2] + L.p[1] - L.p[3]) * (u * v);
+        nl = L.n;
+    }
+    float3 win = p - P;
+    const float dist2 = dot3(win, win);
+    win = normalize3(win);
+    const float cl = fmaxf(0.f, dot3(win, nl));
+    const float3 Ls = L.emit * (cl * L.area / dist2);
+    if (is_black(Ls)) return false;
+    const float3 wi = win * -1.f;
+    const float3 wi_l = make_float3(dot3(U, wi), dot3(V, wi), dot3(W, wi));
+    c = beta * Ls * (fmaxf(0.f, dot3(wi, W))) * bsdf_f(m, wo_l, wi_l);
+    if (is_black(c)) return false;
+    const float3 seg = P - p;
+    so = make_float4(p.x, p.y, p.z, S.eps);
+    sd = make_float4(seg.x, seg.y, seg.z, 1.f - S.eps);
+    return true;
+}
+
+// The path's next ray (PathIntegrator.cpp:141-187): a BSDF sample
+// (BSDF::SampleF, Core/Material/BSDF.cpp:141-211), the throughput update,
+// Russian roulette after depth 3 and the spawn offset along the geometric
+// normal (below the surface for a transmitted ray). False when the path
+// ends here; beta is updated when it continues.
+__device__ __forceinline__ bool continue_path(const SceneRec &S, uint64_t key, uint32_t depth, const Mat &m,
+                                              bool specular, float3 p, float3 ng, float3 U, float3 V, float3 W,
+                                              float3 wo_l, float3 &beta, float4 &no, float4 &nd)
+{
+    const float u1 = rnd(key, dim_of(depth, 20)), u2 = rnd(key, dim_of(depth, 21));
+    float3 wi_l, f;
+    float pdf;
+    bool transmit = false;
+    if (specular) {
+        sample_specular(m, wo_l, rnd(key, dim_of(depth, 22)), wi_l, f, pdf, transmit);
+    } else if (m.kind == 1u) {
+        wi_l = ggx_sample_vndf(wo_l, m.alpha, u1, u2);
+        pdf = ggx_pdf(wo_l, wi_l, m.alpha);
+        f = ggx_f(wo_l, wi_l, m.f0, m.alpha);
+    } else {
+        // Lambertian::SampleF (Core/Material/LambertianBxDF.cpp:27-37)
+        const float r = sqrtf(u1);
+        float s, c;
+        sincosf(kTwoPi * u2, &s, &c);
+        wi_l = make_float3(r * c, r * s, sqrtf(1.f - u1));
+        if (wo_l.z < 0.f) wi_l.z = -wi_l.z;
+        pdf = fabsf(wi_l.z) * kInvPi;
+        f = bsdf_f(m, wo_l, wi_l);
+    }
+    if (is_black(f) || !(pdf > 0.f)) return false;
+    const float3 wi = U * wi_l.x + V * wi_l.y + W * wi_l.z;
+    float3 b = beta * f * (fabsf(dot3(wi, W)) / pdf);
+    if (depth > 3) {
+        const float q = fminf(0.5f, 0.212671f * b.x + 0.715160f * b.y + 0.072169f * b.z);
+        if (rnd(key, dim_of(depth, 23)) > q) return false;
+        b = b * (1.f / q);
+    }
+    beta = b;
+    // a transmitted ray starts below the surface (PathIntegrator.cpp:184-187)
+    const float3 org = p + ng * (transmit ? -S.eps : S.eps);
+    no = make_float4(org.x, org.y, org.z, S.eps);
+    nd = make_float4(wi.x, wi.y, wi.z, FLT_MAX);
+    return true;
+}
+
 __global__ void __launch_bounds__(256) k_shade(RenderDev R, int cur, uint32_t depth, uint64_t wave_begin)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -484,108 +600,12 @@ __global__ void __launch_bounds__(256) k_shade(RenderDev R, int cur, uint32_t de
                 // specular BSDF's F is zero for every light direction)
                 for (uint32_t l = 0; l < S.n_lights && l < kMaxLights && !specular; l++) {
                     if (l == light_id) continue;
-                    const Light &L = S.lights[l];
-                    const float u = rnd(key, dim_of(depth, 2 * l)), v = rnd(key, dim_of(depth, 2 * l + 1));
-                    if (L.kind == kLightInfinite) {
-                        // InfiniteAreaLight::SampleRadiance (InfiniteAreaLight.cpp:73-83):
-                        // a direction in the cone cos(theta) >= 1e-4 about the shading
-                        // normal (Montecarlo::UniformSampleCone, Montecarlo.h:74-80), the
-                        // light's intensity with no division by the pdf, a shadow ray
-                        // over [1e-4, FLT_MAX] from the point itself
-                        const float ct = (1.f - u) + u * 1e-4f;
-                        const float st = sqrtf(1.f - ct * ct);
-                        float sp, cp;
-                        sincosf(kTwoPi * v, &sp, &cp);
-                        const float3 wi = U * (cp * st) + V * (sp * st) + W * ct;
-                        const float3 wi_l = make_float3(dot3(U, wi), dot3(V, wi), dot3(W, wi));
-                        const float3 c = beta * L.emit * fmaxf(0.f, dot3(wi, W)) * bsdf_f(m, wo_l, wi_l);
-                        if (is_black(c)) continue;
-                        so[n_sh] = make_float4(p.x, p.y, p.z, 1e-4f);
-                        sd[n_sh] = make_float4(wi.x, wi.y, wi.z, FLT_MAX);
-                        sc[n_sh] = c;
-                        n_sh++;
-                        continue;
-                    }
-                    float3 P, nl;
-                    if (L.kind == kLightMesh) {
-                        // ITriangleMesh::SamplePoint (Core/Shape/TriangleMesh.cpp:142-161):
-                        // a triangle picked uniformly by index (not by area), a uniform
-                        // point on it (IndexedTriangle::SamplePoint, Montecarlo.h:59-64),
-                        // its normal (p3 - p1) x (p2 - p1) turned to face the shaded
-                        // point; the pdf is 1 / the mesh's whole area (DiffuseAreaLight.cpp:36-40)
-                        const uint32_t k = min((uint32_t)((float)L.tri_count * rnd(key, dim_of(depth, 24 + l))),
-                                               L.tri_count - 1u);
-                        const uint32_t *tv = S.idx + 3ull * (L.first_tri + k);
-                        const float *a = S.pos + 3ull * tv[0], *b = S.pos + 3ull * tv[1], *cc = S.pos + 3ull * tv[2];
-                        const float3 p1 = make_float3(a[0], a[1], a[2]), p2 = make_float3(b[0], b[1], b[2]),
-                                     p3 = make_float3(cc[0], cc[1], cc[2]);
-                        const float su = sqrtf(u);
-                        const float b1 = 1.f - su, b2 = v * su;
-                        P = p1 * b1 + p2 * b2 + p3 * (1.f - b1 - b2);
-                        nl = normalize3(cross3(p3 - p1, p2 - p1));
-                        if (dot3(P - p, nl) > 0.f) nl = nl * -1.f;
-                    } else {
-                        // Quad::SamplePoint (Core/Shape/Quad.cpp:144-153): a bilinear
-                        // patch over the reference's tessellation vertices
-                        P = L.p[0] + (L.p[2] - L.p[0]) * u + (L.p[3] - L.p[2]) * v +
-                            (L.p[0] - L.p[2] + L.p[1] - L.p[3]) * (u * v);
-                        nl = L.n;
-                    }
-                    float3 win = p - P;
-                    const float dist2 = dot3(win, win);
-                    win = normalize3(win);
-                    const float cl = fmaxf(0.f, dot3(win, nl));
-                    const float3 Ls = L.emit * (cl * L.area / dist2);
-                    if (is_black(Ls)) continue;
-                    const float3 wi = win * -1.f;
-                    const float3 wi_l = make_float3(dot3(U, wi), dot3(V, wi), dot3(W, wi));
-                    const float3 c = beta * Ls * (fmaxf(0.f, dot3(wi, W))) * bsdf_f(m, wo_l, wi_l);
-                    if (is_black(c)) continue;
-                    const float3 seg = P - p;
-                    so[n_sh] = make_float4(p.x, p.y, p.z, S.eps);
-                    sd[n_sh] = make_float4(seg.x, seg.y, seg.z, 1.f - S.eps);
-                    sc[n_sh] = c;
-                    n_sh++;
+                    if (light_sample(S, l, key, depth, p, U, V, W, wo_l, m, beta, so[n_sh], sd[n_sh], sc[n_sh])) n_sh++;
                 }
 
-                // sample the BSDF (BSDF::SampleF, Core/Material/BSDF.cpp:141-211)
-                const float u1 = rnd(key, dim_of(depth, 20)), u2 = rnd(key, dim_of(depth, 21));
-                float3 wi_l, f;
-                float pdf;
-                bool transmit = false;
-                if (specular) {
-                    sample_specular(m, wo_l, rnd(key, dim_of(depth, 22)), wi_l, f, pdf, transmit);
-                } else if (m.kind == 1u) {
-                    wi_l = ggx_sample_vndf(wo_l, m.alpha, u1, u2);
-                    pdf = ggx_pdf(wo_l, wi_l, m.alpha);
-                    f = ggx_f(wo_l, wi_l, m.f0, m.alpha);
-                } else {
-                    // Lambertian::SampleF (Core/Material/LambertianBxDF.cpp:27-37)
-                    const float r = sqrtf(u1);
-                    float s, c;
-                    sincosf(kTwoPi * u2, &s, &c);
-                    wi_l = make_float3(r * c, r * s, sqrtf(1.f - u1));
-                    if (wo_l.z < 0.f) wi_l.z = -wi_l.z;
-                    pdf = fabsf(wi_l.z) * kInvPi;
-                    f = bsdf_f(m, wo_l, wi_l);
-                }
-                if (!is_black(f) && pdf > 0.f) {
-                    const float3 wi = U * wi_l.x + V * wi_l.y + W * wi_l.z;
-                    beta = beta * f * (fabsf(dot3(wi, W)) / pdf);
-                    bool alive = true;
-                    if (depth > 3) {
-                        const float q = fminf(0.5f, 0.212671f * beta.x + 0.715160f * beta.y + 0.072169f * beta.z);
-                        if (rnd(key, dim_of(depth, 23)) > q) alive = false;
-                        else beta = beta * (1.f / q);
-                    }
-                    if (alive) {
-                        // a transmitted ray starts below the surface (PathIntegrator.cpp:184-187)
-                        const float3 org = p + ng * (transmit ? -S.eps : S.eps);
-                        no = make_float4(org.x, org.y, org.z, S.eps);
-                        nd = make_float4(wi.x, wi.y, wi.z, FLT_MAX);
-                        cont = true;
-                        R.beta[path] = make_float4(beta.x, beta.y, beta.z, specular ? 1.f : 0.f);
-                    }
+                if (continue_path(S, key, depth, m, specular, p, ng, U, V, W, wo_l, beta, no, nd)) {
+                    cont = true;
+                    R.beta[path] = make_float4(beta.x, beta.y, beta.z, specular ? 1.f : 0.f);
                 }
             }
         }
@@ -738,6 +758,197 @@ __global__ void __launch_bounds__(128) k_extend_dyn(RenderDev R, int cur, uint32
 __global__ void __launch_bounds__(128) k_shadow_dyn(RenderDev R, uint32_t *next)
 {
     wave_trace_dyn<true>(R, min(*R.sh_count, R.sh_capacity), next, 0);
+}
+
+// ---------------------------------------------------------------------------
+// The whole render as one persistent launch: each lane carries one path from
+// its camera ray through every bounce (closest hit, shading, one shadow ray
+// per light, the next ray) and takes a new path from a device counter when
+// its path ends; a warp refills once kRefillLanes of its lanes are idle. The
+// paths of every scene of a batch, of any length, flow through the same
+// kernel with no host round trip and no queue in memory. Closest-hit and
+// shadow rays share one traversal loop (ray_step<kMixed>), so lanes tracing
+// either kind stay on the same code; shading runs in the lane whose ray just
+// finished. The sample sequence, the shading code (light_sample,
+// continue_path) and the traversal are the wavefront's, so every path is the
+// wavefront path of the same index and the images agree up to the order of
+// the float additions into each pixel. Plain renders only: no radiance
+// cache, no Direct / Albedo outputs, no work counters.
+// ---------------------------------------------------------------------------
+struct PathLane {
+    uint32_t sid, pixel, depth;
+    uint64_t key;
+    float3 beta;           // throughput at the current vertex
+    bool after_specular;   // the previous bounce was specular
+    // the vertex being lit: light samples still to trace, then the next ray
+    float3 p, W, wo_l, nee_beta, next_beta;
+    uint32_t mat_id, light_id, next_light;
+    bool specular, cont;
+    float4 no, nd;         // the next ray (when cont)
+    float3 c;              // contribution of the shadow ray in flight
+};
+
+__device__ __forceinline__ void start_path(const RenderDev &R, uint64_t g, PathLane &P, RayState &r)
+{
+    const uint32_t sid = scene_of(R, g);
+    const SceneRec &S = R.scenes[sid];
+    uint32_t pixel, x, y;
+    uint64_t key;
+    path_ident(S, g, pixel, key, x, y);
+    float4 o, d;
+    if (S.ray_o) {
+        o = S.ray_o[pixel];
+        d = S.ray_d[pixel];
+    } else {
+        const float xi1 = rnd(key, kDimCam) - 0.5f, xi2 = rnd(key, kDimCam + 1) - 0.5f;
+        const float fx = x * S.rcp_w + xi1 * S.rcp_w, fy = y * S.rcp_h + xi2 * S.rcp_h;
+        const float3 target = S.corner + S.across * fx + S.up * fy;
+        const float3 dd = normalize3(target - S.centre);
+        o = make_float4(S.centre.x, S.centre.y, S.centre.z, 0.f);
+        d = make_float4(dd.x, dd.y, dd.z, FLT_MAX);
+    }
+    P.sid = sid;
+    P.pixel = pixel + S.pixel_base;
+    P.depth = 0;
+    P.key = key;
+    P.beta = make_float3(1.f, 1.f, 1.f);
+    P.after_specular = false;
+    ray_init(r, o, d, S.n_nodes);
+    r.any = false;
+}
+
+// The next light sample of the vertex with a contribution, as a shadow ray
+// in r; false when none is left.
+__device__ __forceinline__ bool next_light_sample(const RenderDev &R, PathLane &P, RayState &r)
+{
+    const SceneRec &S = R.scenes[P.sid];
+    if (P.specular) return false;
+    float3 U, V;
+    onb_from_w(P.W, U, V);
+    const Mat m = S.mats[P.mat_id < S.n_mats ? P.mat_id : 0];
+    for (uint32_t l = P.next_light; l < S.n_lights && l < kMaxLights; l++) {
+        if (l == P.light_id) continue;
+        float4 so, sd;
+        if (light_sample(S, l, P.key, P.depth, P.p, U, V, P.W, P.wo_l, m, P.nee_beta, so, sd, P.c)) {
+            P.next_light = l + 1;
+            ray_init(r, so, sd, S.n_nodes);
+            r.any = true;
+            return true;
+        }
+    }
+    return false;
+}
+
+// After the vertex's light samples: the next ray, or the end of the path.
+__device__ __forceinline__ bool next_bounce(const RenderDev &R, PathLane &P, RayState &r)
+{
+    if (!P.cont) return false;
+    P.beta = P.next_beta;
+    P.after_specular = P.specular;
+    P.depth++;
+    ray_init(r, P.no, P.nd, R.scenes[P.sid].n_nodes);
+    r.any = false;
+    return true;
+}
+
+// The closest hit of the path's ray is in r: what the vertex adds, and its
+// light samples and next ray (k_shade's rules). Returns whether the lane has
+// a ray to trace.
+__device__ __forceinline__ bool shade_vertex(const RenderDev &R, PathLane &P, RayState &r, float4 o, float4 d)
+{
+    const SceneRec &S = R.scenes[P.sid];
+    const int ti = r.best;
+    const uint32_t depth = P.depth;
+    float3 add = make_float3(0.f, 0.f, 0.f);
+    if (ti < 0) {
+        if (ti == -1) {
+            add = P.beta * S.sky;
+            if ((depth == 0 || P.after_specular) && S.inf_escape > 0.f) add = add + P.beta * S.inf_escape;
+            if (!is_black(add)) add_pixel(R.accum, P.pixel, add);
+        }
+        return false;
+    }
+    if (depth > S.max_depth) return false;
+    const uint32_t attr = S.tri_attr[ti];
+    const uint32_t mat_id = attr & 0xffffu, light_id = attr >> 16;
+    const Mat m = S.mats[mat_id < S.n_mats ? mat_id : 0];
+    const Tri tr = S.tris[ti];
+    const float3 ng = normalize3(make_float3(tr.a.w, tr.b.w, tr.c.w));
+    const float t = r.tcur;
+    const float3 p = make_float3(o.x + t * d.x, o.y + t * d.y, o.z + t * d.z);
+    const float3 wo = normalize3(make_float3(d.x, d.y, d.z)) * -1.f;
+    const float3 W = ng;
+    float3 U, V;
+    onb_from_w(W, U, V);
+    const float3 wo_l = make_float3(dot3(U, wo), dot3(V, wo), dot3(W, wo));
+    if ((depth == 0 || P.after_specular) && light_id != 0xffffu && light_id < S.n_lights && dot3(W, wo) > 0.f)
+        add = add + P.beta * S.lights[light_id].emit;
+    if (!is_black(add)) add_pixel(R.accum, P.pixel, add);
+    if (depth >= S.max_depth) return false;
+    P.specular = m.kind >= 2u;
+    P.p = p;
+    P.W = W;
+    P.wo_l = wo_l;
+    P.mat_id = mat_id;
+    P.light_id = light_id;
+    P.next_light = 0;
+    P.nee_beta = P.beta;
+    P.next_beta = P.beta;
+    P.cont = continue_path(S, P.key, depth, m, P.specular, p, ng, U, V, W, wo_l, P.next_beta, P.no, P.nd);
+    if (next_light_sample(R, P, r)) return true;
+    return next_bounce(R, P, r);
+}
+
+__global__ void __launch_bounds__(128) k_render_persistent(RenderDev R, uint64_t total, unsigned long long *next)
+{
+    const uint32_t lane = threadIdx.x & 31u;
+    uint2 stack[kMaxStack];
+    RayState r;
+    PathLane P;
+    float4 ro = make_float4(0.f, 0.f, 0.f, 0.f), rd = ro;  // the closest-hit ray in flight (for shading)
+    bool active = false, exhausted = false;  // exhausted is warp-uniform
+    const Node8 *nodes = nullptr;
+    const Tri *tris = nullptr;
+    uint32_t n_nodes = 0, n_tris = 0;
+    while (true) {
+        const uint32_t idle = __ballot_sync(0xffffffffu, !active);
+        if (!exhausted && (__popc(idle) >= kRefillLanes || idle == 0xffffffffu)) {
+            const uint32_t leader = __ffs(idle) - 1u;
+            unsigned long long base = 0;
+            if (lane == leader) base = atomicAdd(next, (unsigned long long)__popc(idle));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (base >= total) exhausted = true;
+            if (!active) {
+                const uint64_t k = base + __popc(idle & ((1u << lane) - 1u));
+                if (k < total) {
+                    start_path(R, k, P, r);
+                    const SceneRec &S = R.scenes[P.sid];
+                    nodes = S.nodes;
+                    tris = S.tris;
+                    n_nodes = S.n_nodes;
+                    n_tris = S.n_tris;
+                    ro = make_float4(r.ox, r.oy, r.oz, r.tmin);
+                    rd = make_float4(r.dx, r.dy, r.dz, r.tcur);
+                    active = true;
+                }
+            }
+        }
+        if (__ballot_sync(0xffffffffu, active) == 0u) break;
+        if (active && ray_step<false, false, false, false, kTrisPerStep, true>(r, stack, nodes, tris, n_nodes, n_tris,
+                                                                               R.err)) {
+            if (r.any) {
+                // a shadow ray: its light sample counts when nothing is in the way
+                if (r.best == -1) add_pixel(R.accum, P.pixel, P.c);
+                active = next_light_sample(R, P, r) || next_bounce(R, P, r);
+            } else {
+                active = shade_vertex(R, P, r, ro, rd);
+            }
+            if (active && !r.any) {
+                ro = make_float4(r.ox, r.oy, r.oz, r.tmin);
+                rd = make_float4(r.dx, r.dy, r.dz, r.tcur);
+            }
+        }
+    }
 }
 
 __global__ void k_resolve(const float4 *__restrict__ accum, uint32_t wh, float scale, float *__restrict__ out)
@@ -951,6 +1162,22 @@ cudaError_t render_wave(const RenderDev &R, uint32_t n_paths, uint64_t wave_begi
     }
     if (launches) *launches += n_launch;
     return cudaSuccess;
+}
+
+cudaError_t render_persistent(const RenderDev &R, uint64_t total, unsigned long long *next, uint32_t *launches,
+                              cudaStream_t st)
+{
+    cudaError_t e = cudaMemsetAsync(next, 0, sizeof(unsigned long long), st);
+    if (e != cudaSuccess) return e;
+    int per_sm = 0;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_render_persistent, 128, 0)) != cudaSuccess)
+        return e;
+    const uint64_t want = (total + 127) / 128;
+    const uint64_t cap = (uint64_t)current_sm_count() * (uint64_t)(per_sm > 0 ? per_sm : 1);
+    const uint32_t blocks = (uint32_t)(want < cap ? (want > 0 ? want : 1) : cap);
+    k_render_persistent<<<blocks, 128, 0, st>>>(R, total, next);
+    if (launches) *launches += 1;
+    return cudaGetLastError();
 }
 
 cudaError_t render_resolve(const float4 *accum, uint32_t wh, float scale, float *out, cudaStream_t st)

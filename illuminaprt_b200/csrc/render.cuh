@@ -135,6 +135,10 @@ struct MlpDev;
 cudaError_t render_wave(const RenderDev &R, uint32_t n_paths, uint64_t wave_begin, cudaStream_t st,
                         uint32_t *launches, const MlpDev *cache, uint32_t block = 128);
 cudaError_t render_resolve(const float4 *accum, uint32_t wh, float scale, float *out, cudaStream_t st);
+// Every path of the render ([0, total)) in one persistent launch
+// (k_render_persistent); `next` is a device counter. Plain renders only.
+cudaError_t render_persistent(const RenderDev &R, uint64_t total, unsigned long long *next, uint32_t *launches,
+                              cudaStream_t st);
 
 // Hash-grid radiance cache: the n_rec training records of a call (raw
 // features + targets) are added to their cells.

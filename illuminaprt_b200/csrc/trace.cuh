@@ -50,6 +50,7 @@ struct RayState {
     int best;
     float bu, bv;
     Shear sh;  // watertight test only
+    bool any;  // kMixed traversals: this ray is an any-hit (shadow) ray
 };
 
 template <bool kWT = false>
@@ -93,7 +94,9 @@ constexpr int kTrisWholeGroup = 32;
 // hit record, -1 for a miss, -2 for a reported error).
 // kWT selects the watertight triangle test over `raw` (three float4
 // vertices per triangle record) instead of the reference's Shirley test.
-template <bool kAnyHit, bool kStats = false, bool kSkip = false, bool kWT = false, int kTris = kTrisPerStep>
+// kMixed: closest- and any-hit rays share one instance (r.any chooses per ray).
+template <bool kAnyHit, bool kStats = false, bool kSkip = false, bool kWT = false, int kTris = kTrisPerStep,
+          bool kMixed = false>
 __device__ __forceinline__ bool ray_step(RayState &r, uint2 *stack, const Node8 *__restrict__ nodes,
                                          const Tri *__restrict__ tris, uint32_t n_nodes_total, uint32_t n_tris_total,
                                          uint32_t *__restrict__ err, unsigned long long *n_nodes = nullptr,
@@ -187,7 +190,7 @@ __device__ __forceinline__ bool ray_step(RayState &r, uint2 *stack, const Node8 
         }
         if (hit) {
             r.best = (int)ti;
-            if (kAnyHit) return true;
+            if (kAnyHit || (kMixed && r.any)) return true;
             r.bu = bh;
             r.bv = gh;
             r.tcur = th;

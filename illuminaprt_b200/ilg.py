@@ -22,6 +22,7 @@ ILG_DEVICE_PTRS = 0x1
 ILG_WATERTIGHT = 0x2
 ILG_RENDER_COUNT = 0x4
 ILG_RENDER_HASH_CACHE = 0x8
+ILG_RENDER_PERSISTENT = 0x20
 
 STATUS_NAMES = {0: "ILG_OK", 1: "ILG_EINVAL", 2: "ILG_ENOMEM", 3: "ILG_ECUDA", 4: "ILG_ETIMEOUT",
                 5: "ILG_EOVERFLOW", 6: "ILG_ESTATE"}
@@ -391,8 +392,9 @@ class GpuSpace:
     def render(self, camera: dict, width: int, height: int, spp: int, max_depth: int = 6, epsilon: float = 1e-4,
                seed: int = 1, sky=(0.0, 0.0, 0.0), paths_per_wave: int = 0, out=None, cache_depth: int = 0,
                train_every: int = 16, train_steps: int = 4, train_batch: int = 16384, count: bool = False,
-               train_tail: int = 0, train_epochs: int = 1, hash_cache: bool = False):
+               train_tail: int = 0, train_epochs: int = 1, hash_cache: bool = False, one_launch: bool = False):
         """Returns (height, width, 3) float32 (or fills `out`, a CUDA tensor, in place).
+        one_launch renders with the persistent one-launch kernel (ILG_RENDER_PERSISTENT).
         cache_depth > 0 renders with the radiance cache (mlp_init first) and trains it afterwards;
         with hash_cache the non-learned hash-grid cache stands in for the network
         (hash_cache_reset first)."""
@@ -402,7 +404,8 @@ class GpuSpace:
                             train_steps=train_steps, train_batch=train_batch, train_tail=train_tail,
                             train_epochs=train_epochs)
         o.sky[:] = list(sky)
-        flags = (ILG_RENDER_COUNT if count else 0) | (ILG_RENDER_HASH_CACHE if hash_cache else 0)
+        flags = ((ILG_RENDER_COUNT if count else 0) | (ILG_RENDER_HASH_CACHE if hash_cache else 0)
+                 | (ILG_RENDER_PERSISTENT if one_launch else 0))
         if out is not None:
             self._check(self.L.ilg_render(self.h, ctypes.byref(cam), ctypes.byref(o), _ptr(out),
                                           ILG_DEVICE_PTRS | flags))
@@ -531,7 +534,7 @@ class GpuSpace:
         return loss.value
 
     def render_batch(self, items, paths_per_wave: int = 0, block: int = 0, device_ptrs: bool = False,
-                     count: bool = False):
+                     count: bool = False, one_launch: bool = False):
         """items: list of dicts {space: GpuSpace, camera, width, height, spp, max_depth=6, epsilon=1e-4,
         seed=1, sky=(0,0,0), out=None}. Renders all in one wavefront on this context; returns the images
         (numpy arrays, or the given CUDA tensors when device_ptrs)."""
@@ -558,7 +561,8 @@ class GpuSpace:
                 out = np.empty((it["height"], it["width"], 3), np.float32)
                 a.out_rgb = out.ctypes.data
             outs.append(out)
-        flags = (ILG_DEVICE_PTRS if device_ptrs else 0) | (ILG_RENDER_COUNT if count else 0)
+        flags = ((ILG_DEVICE_PTRS if device_ptrs else 0) | (ILG_RENDER_COUNT if count else 0)
+                 | (ILG_RENDER_PERSISTENT if one_launch else 0))
         self._check(self.L.ilg_render_batch(self.h, ctypes.addressof(arr), len(items), paths_per_wave, block,
                                             flags))
         return outs

@@ -256,6 +256,15 @@ int ilg_render(ilg_ctx *ctx, const ilg_camera *cam, const ilg_render_opts *opts,
  * triangle records they tested, shadow rays, node records, triangle records}.
  * These are the per-sample bytes of the path tracer's memory roofline. */
 #define ILG_RENDER_COUNT 0x4u
+/* ilg_render / ilg_render_batch flag: the whole render as one persistent
+ * kernel launch instead of the wavefront's launches per bounce. Each GPU
+ * thread carries one path through all its bounces (closest hit, shading, a
+ * shadow ray per light, the next ray) and takes a new path, of any scene of
+ * a batch, when its path ends. Same paths as the wavefront (same sample
+ * sequence and arithmetic): the images agree up to float summation order.
+ * Plain renders only (no cache options, ILG_RENDER_COUNT, or Direct /
+ * Albedo outputs). */
+#define ILG_RENDER_PERSISTENT 0x20u
 int ilg_render_counts(ilg_ctx *ctx, uint64_t counts[6]);
 
 /* ilg_render / ilg_render_region flag: with cache_depth set, a hash-grid
