@@ -467,6 +467,26 @@ def bench_mlp(res, dev, local, e0, e1):
             tag = key if enc == "hashgrid" else f"{key}_{enc}"
             res[f"mlp_infer_{tag}_mqueries_s"] = round(nq / (ms / 1e3) / 1e6, 1)
             res[f"mlp_infer_{tag}_tflops"] = round(nq * 45440 / (ms / 1e3) / 1e12, 2)
+    # training step (forward, loss, backward, weight gradients) on 16384
+    # rows: 3 x 45,440 FLOP per row
+    nt = 16384
+    tq = torch.rand((nt, 16), device=dev)
+    tt = torch.rand((nt, 3), device=dev)
+    g = torch.empty(23040, device=dev)
+    loss = torch.empty(1, device=dev)
+    for enc in ("hashgrid", "freq12"):
+        sp.mlp_init(seed=1, encoding=enc)
+        for flag, key in ((0, "tcgen05"), (0x10, "mma_sync")):
+            sp.L.ilg_mlp_grads(sp.h, tq.data_ptr(), tt.data_ptr(), nt, g.data_ptr(), loss.data_ptr(), 0x1 | flag)
+            sp.sync()
+            e0.record(st)
+            for _ in range(10):
+                sp.L.ilg_mlp_grads(sp.h, tq.data_ptr(), tt.data_ptr(), nt, g.data_ptr(), loss.data_ptr(), 0x1 | flag)
+            e1.record(st)
+            e1.synchronize()
+            ms = e0.elapsed_time(e1) / 10
+            res[f"mlp_train_{key}_{enc}_16384_rows_us"] = round(ms * 1e3, 1)
+            res[f"mlp_train_{key}_{enc}_tflops"] = round(nt * 3 * 45440 / (ms / 1e3) / 1e12, 2)
     if peak:
         t = res["mlp_infer_tcgen05_freq12_tflops"]
         res["mlp_infer_roofline"] = {"bound": "tensor", "achieved": t, "peak": peak, "unit": "TFLOP/s",
@@ -657,7 +677,7 @@ def main():
     # library's own streaming read probe (an L2-resident buffer read 64 times)
     l2_size = torch.cuda.get_device_properties(local).L2_cache_size
     scene_bytes = stats["node_bytes"] + stats["tri_bytes"]
-    l2_probe = {f"{mb}MB": round(sp.probe_read_gbs(mb << 20, 64), 1) for mb in (16, 32, 48)}
+    l2_probe = {f"{mb}MB": round(sp.probe_read_gbs(mb << 20, 64), 1) for mb in (32, 64, 96)}
     l2_gbs = max(l2_probe.values())
     hbm_read_gbs = round(sp.probe_read_gbs(2 << 30, 4), 1)
 
@@ -705,7 +725,7 @@ def main():
                          "traffic": traffic,
                          "kernel": "k_trace_dyn<closest> (incoherent launch)",
                          "peak_source": (f"measured L2 read bandwidth (ilg_probe_read_gbs, L2-only loads, best of "
-                                         f"16/32/48 MB buffers, this run): scene {scene_bytes / 1e6:.1f} MB <= L2 "
+                                         f"32/64/96 MB buffers, this run): scene {scene_bytes / 1e6:.1f} MB <= L2 "
                                          f"{l2_size / 1e6:.1f} MB" if scene_bytes <= l2_size else
                                          f"{peak_kind} hbm_gbs (scene exceeds L2)"),
                          "l2_probe_gbs": l2_probe, "hbm_read_probe_gbs": hbm_read_gbs,

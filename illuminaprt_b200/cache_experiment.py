@@ -211,5 +211,7 @@ ARMS = {
     "spec_freq12_full_depth_cache_depth_1": dict(encoding="freq12", cache_depth=1, train_tail=0),
     "spec_freq12_full_depth_cache_depth_2": dict(encoding="freq12", cache_depth=2, train_tail=0),
     "hashgrid_self_training": dict(encoding="hashgrid", cache_depth=1, train_tail=1, train_epochs=2),
+    "hashgrid_self_training_8_steps": dict(encoding="hashgrid", cache_depth=1, train_tail=1, train_epochs=2,
+                                           train_steps=8),
     "hash_grid_cache": dict(hash_cache=True, cache_depth=1, train_tail=1),
 }

@@ -1305,6 +1305,7 @@ int ilg_mlp_init_encoding(ilg_ctx *ctx, uint32_t seed, float learning_rate, uint
     CK(ctx->mlp_w.reserve(kMlpParams)); CK(ctx->mlp_m.reserve(kMlpParams)); CK(ctx->mlp_v.reserve(kMlpParams));
     CK(ctx->mlp_grad.reserve(kMlpParams)); CK(ctx->mlp_loss.reserve(1));
     CK(ctx->mlp_wf.reserve(kFwdElems)); CK(ctx->mlp_wb.reserve(kBwdElems)); CK(ctx->mlp_wu.reserve(kUmmaElems));
+    CK(ctx->mlp_wv.reserve(kUmmaBwdElems));
     CK(ctx->mlp_grid.reserve(kGridParams)); CK(ctx->mlp_grid_grad.reserve(kGridParams));
     CK(ctx->mlp_grid_m.reserve(kGridParams)); CK(ctx->mlp_grid_v.reserve(kGridParams));
     CK(mlp_init(ctx->mlp_view(), seed, ctx->stream));
@@ -1360,6 +1361,8 @@ int ilg_mlp_infer(ilg_ctx *ctx, const float *raw, uint32_t n, float *out, uint32
     if (n == 0) return ILG_OK;
     if (!raw || !out) return fail(ctx, ILG_EINVAL, "ilg_mlp_infer: null array");
     if (flags & ~(ILG_DEVICE_PTRS | ILG_MLP_WARP_MMA)) return fail(ctx, ILG_EINVAL, "ilg_mlp_infer: unknown flags");
+    if ((flags & ILG_DEVICE_PTRS) && ((uintptr_t)raw & 15u))
+        return fail(ctx, ILG_EINVAL, "ilg_mlp_infer: device query rows must start 16-byte aligned");
     CK(cudaSetDevice(ctx->device));
     cudaStream_t st = ctx->stream;
     const bool warp_mma = (flags & ILG_MLP_WARP_MMA) != 0;
@@ -1398,10 +1401,12 @@ static int mlp_grads_common(ilg_ctx *ctx, const float *raw, const float *target,
         draw = ctx->mlp_raw.ptr;
         dtgt = ctx->mlp_tgt.ptr;
     }
-    CK(mlp_grads(ctx->mlp_view(), draw, dtgt, n, st));
+    if ((flags & ILG_DEVICE_PTRS) && ((uintptr_t)draw & 15u) && !(flags & ILG_MLP_WARP_MMA))
+        return fail(ctx, ILG_EINVAL, "device training rows must start 16-byte aligned");
+    CK(mlp_grads(ctx->mlp_view(), draw, dtgt, n, st, (flags & ILG_MLP_WARP_MMA) != 0));
     if (loss) {
-        CK(cudaMemcpyAsync(loss, ctx->mlp_loss.ptr, sizeof(float), cudaMemcpyDeviceToHost, st));
-        CK(cudaStreamSynchronize(st));
+        CK(cudaMemcpyAsync(loss, ctx->mlp_loss.ptr, sizeof(float), cudaMemcpyDefault, st));
+        if (!(flags & ILG_DEVICE_PTRS)) CK(cudaStreamSynchronize(st));
     }
     return ILG_OK;
 }
@@ -1413,8 +1418,9 @@ int ilg_mlp_grads(ilg_ctx *ctx, const float *raw, const float *target, uint32_t 
     if (!grad) return fail(ctx, ILG_EINVAL, "ilg_mlp_grads: null grad");
     int rc = mlp_grads_common(ctx, raw, target, n, flags, loss);
     if (rc) return rc;
-    CK(cudaMemcpyAsync(grad, ctx->mlp_grad.ptr, sizeof(float) * kMlpParams, cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
+    // (cudaMemcpyDefault: grad is a device pointer with ILG_DEVICE_PTRS)
+    CK(cudaMemcpyAsync(grad, ctx->mlp_grad.ptr, sizeof(float) * kMlpParams, cudaMemcpyDefault, ctx->stream));
+    if (!(flags & ILG_DEVICE_PTRS)) CK(cudaStreamSynchronize(ctx->stream));
     return ILG_OK;
 }
 

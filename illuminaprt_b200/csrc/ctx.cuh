@@ -111,7 +111,7 @@ struct ilg_ctx {
     ilg::DevBuf<float> mlp_w, mlp_m, mlp_v, mlp_grad, mlp_loss, mlp_raw, mlp_tgt, mlp_out;
     ilg::DevBuf<float> mlp_grid, mlp_grid_grad, mlp_grid_m, mlp_grid_v;
     ilg::DevBuf<uint32_t> mlp_enc;
-    ilg::DevBuf<__nv_bfloat16> mlp_wf, mlp_wb, mlp_wu, mlp_xcm, mlp_hcm, mlp_dzcm;
+    ilg::DevBuf<__nv_bfloat16> mlp_wf, mlp_wb, mlp_wu, mlp_wv, mlp_xcm, mlp_hcm, mlp_dzcm;
     bool mlp_ready = false;
     uint32_t mlp_encoding = 0;  // ILG_MLP_ENC_*
     uint32_t mlp_step = 0;
@@ -122,7 +122,7 @@ struct ilg_ctx {
         ilg::MlpDev M;
         memset(&M, 0, sizeof(M));  // zero padding: the struct's bytes key the cached render graph
         M.w = mlp_w.ptr; M.m = mlp_m.ptr; M.v = mlp_v.ptr; M.grad = mlp_grad.ptr; M.loss = mlp_loss.ptr;
-        M.wf = mlp_wf.ptr; M.wb = mlp_wb.ptr; M.wu = mlp_wu.ptr; M.err = derr.ptr; M.xcm = mlp_xcm.ptr; M.hcm = mlp_hcm.ptr; M.dzcm = mlp_dzcm.ptr;
+        M.wf = mlp_wf.ptr; M.wb = mlp_wb.ptr; M.wu = mlp_wu.ptr; M.wv = mlp_wv.ptr; M.err = derr.ptr; M.xcm = mlp_xcm.ptr; M.hcm = mlp_hcm.ptr; M.dzcm = mlp_dzcm.ptr;
         M.cap = (uint32_t)(mlp_xcm.cap / ilg::kMlpIn);
         M.grid = mlp_grid.ptr; M.grid_grad = mlp_grid_grad.ptr; M.grid_m = mlp_grid_m.ptr; M.grid_v = mlp_grid_v.ptr;
         ilg::grid_resolution(M.grid_res);
@@ -175,7 +175,7 @@ struct ilg_ctx {
         qry_feat.release(); qry_out.release(); rec_beta.release(); qry_beta.release();
         mlp_w.release(); mlp_m.release(); mlp_v.release(); mlp_grad.release(); mlp_loss.release();
         mlp_grid.release(); mlp_grid_grad.release(); mlp_grid_m.release(); mlp_grid_v.release(); mlp_enc.release();
-        mlp_raw.release(); mlp_tgt.release(); mlp_out.release(); mlp_wf.release(); mlp_wb.release(); mlp_wu.release();
+        mlp_raw.release(); mlp_tgt.release(); mlp_out.release(); mlp_wf.release(); mlp_wb.release(); mlp_wu.release(); mlp_wv.release();
         mlp_xcm.release(); mlp_hcm.release(); mlp_dzcm.release();
     }
 };

@@ -356,6 +356,11 @@ __device__ __forceinline__ void write_copies(const MlpDev &M, int i, float w)
         const int kc = mlp_in(l) / 8;
         M.wu[umma_off(l) + (o / 8) * kc * 64 + (in / 8) * 64 + (o % 8) * 8 + (in % 8)] = b;
     }
+    if (M.wv && l >= 1) {
+        // element (n = in, k = o) of the backward copy
+        const int kc = umma_bk(l) / 8;
+        M.wv[umma_boff(l) + (in / 8) * kc * 64 + (o / 8) * 64 + (in % 8) * 8 + (o % 8)] = b;
+    }
 }
 
 __device__ __forceinline__ float hash_uniform(uint32_t seed, uint32_t i)
@@ -497,6 +502,7 @@ cudaError_t mlp_init(const MlpDev &M, uint32_t seed, cudaStream_t st)
     if ((e = cudaMemsetAsync(M.wf, 0, kFwdElems * sizeof(__nv_bfloat16), st)) != cudaSuccess) return e;
     if ((e = cudaMemsetAsync(M.wb, 0, kBwdElems * sizeof(__nv_bfloat16), st)) != cudaSuccess) return e;
     if (M.wu && (e = cudaMemsetAsync(M.wu, 0, kUmmaElems * sizeof(__nv_bfloat16), st)) != cudaSuccess) return e;
+    if (M.wv && (e = cudaMemsetAsync(M.wv, 0, kUmmaBwdElems * sizeof(__nv_bfloat16), st)) != cudaSuccess) return e;
     k_mlp_init<<<(kMlpParams + 255) / 256, 256, 0, st>>>(M, seed);
     return cudaGetLastError();
 }
@@ -524,11 +530,23 @@ cudaError_t mlp_infer_warp(const MlpDev &M, const float *raw, uint32_t n, float 
     return cudaGetLastError();
 }
 
-cudaError_t mlp_grads(const MlpDev &M, const float *raw, const float *target, uint32_t n, cudaStream_t st)
+cudaError_t mlp_grads(const MlpDev &M, const float *raw, const float *target, uint32_t n, cudaStream_t st,
+                      bool warp_mma)
 {
     if (n == 0 || n > M.cap) return cudaErrorInvalidValue;
     cudaError_t e;
     const uint32_t n_pad = (n + 15) / 16 * 16;
+    if (!warp_mma && M.wv) {
+        if ((e = cudaMemsetAsync(M.grad, 0, kMlpParams * sizeof(float), st)) != cudaSuccess) return e;
+        if ((e = cudaMemsetAsync(M.loss, 0, sizeof(float), st)) != cudaSuccess) return e;
+        const bool has_grid = M.encoding == kEncHashGrid;
+        if (has_grid && (e = cudaMemsetAsync(M.grid_grad, 0, kGridParams * sizeof(float), st)) != cudaSuccess)
+            return e;
+        if ((e = mlp_train_tc(M, raw, target, n, st)) != cudaSuccess) return e;
+        if (has_grid) k_grid_bwd<<<(n + kGridBwdThreads - 1) / kGridBwdThreads, kGridBwdThreads, 0, st>>>(M, raw, n);
+        if ((e = mlp_dw_tc(M, n_pad, st)) != cudaSuccess) return e;
+        return cudaGetLastError();
+    }
     // rows n..n_pad of the column-major scratch must be zero; the kernels
     // write exact zeros for them, but clear once so stale rows never leak
     if ((e = cudaMemsetAsync(M.grad, 0, kMlpParams * sizeof(float), st)) != cudaSuccess) return e;

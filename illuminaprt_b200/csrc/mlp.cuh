@@ -69,6 +69,14 @@ __host__ __device__ constexpr int umma_off(int l)
     return l == 0 ? 0 : umma_off(l - 1) + umma_n(l - 1) * mlp_in(l - 1);
 }
 constexpr int kUmmaElems = umma_off(kMlpLayers);
+// tensor-core backward copy (layers 1..5): W_l as N = in x K = out, K-major
+// core matrices, for dH_{l-1} = dZ_l W_l^T; the output layer's K padded to 16
+__host__ __device__ constexpr int umma_bk(int l) { return l == kMlpLayers - 1 ? 16 : mlp_out(l); }
+__host__ __device__ constexpr int umma_boff(int l)
+{
+    return l <= 1 ? 0 : umma_boff(l - 1) + mlp_in(l - 1) * umma_bk(l - 1);
+}
+constexpr int kUmmaBwdElems = umma_boff(kMlpLayers);
 
 struct MlpDev {
     float *w;                 // FP32 master weights (kMlpParams)
@@ -77,6 +85,7 @@ struct MlpDev {
     __nv_bfloat16 *wf;        // forward copy (kFwdElems)
     __nv_bfloat16 *wb;        // backward copy (kBwdElems)
     __nv_bfloat16 *wu;        // tensor-core copy (kUmmaElems)
+    __nv_bfloat16 *wv;        // tensor-core backward copy (kUmmaBwdElems)
     float *loss;              // [1] loss sum of the last step
     // training scratch, column-major [feature][row_padded]
     __nv_bfloat16 *xcm;       // kMlpIn x cap
@@ -165,16 +174,33 @@ __device__ __forceinline__ float2 sh_pair(float x, float y, float z, int k)
 // 32 + 8a + 2b is sin(2^b pi x_a) and the next cos(2^b pi x_a). Columns
 // 56..71: the 16 spherical harmonics of the outgoing direction. Then 72..74
 // normal, 75 roughness, 76..78 albedo, 79 constant 1, 80..95 zero.
+// sin and cos of 2^b pi x for the frequency-only encoding: bands 0, 4 and 8
+// from sincospif, the three bands after each of them by the double-angle
+// identities sin 2a = 2 sin a cos a, cos 2a = (cos a - sin a)(cos a + sin a),
+// every product and sum rounded separately (a quarter of the sincospif
+// calls; three doublings at most keep the error within a few ulp).
+__device__ __forceinline__ void freq_double(float &s, float &c)
+{
+    const float s2 = __fmul_rn(__fmul_rn(2.f, s), c);
+    c = __fmul_rn(__fsub_rn(c, s), __fadd_rn(c, s));
+    s = s2;
+}
+__device__ __forceinline__ void freq_band(float x, int b, float &s, float &c)
+{
+    sincospif(ldexpf(x, b & ~3), &s, &c);
+    for (int k = 0; k < (b & 3); k++) freq_double(s, c);
+}
+
 // The frequency-only encoding (kEncFreq12): for axis a and band b < 12,
-// column 24a + 2b is sin(2^b pi x_a) and the next cos(2^b pi x_a); then
-// 72..74 outgoing direction, 75..77 normal, 78 roughness, 79..81 albedo,
-// 82 constant 1, 83..95 zero.
+// column 24a + 2b is sin(2^b pi x_a) and the next cos(2^b pi x_a) (by
+// freq_band); then 72..74 outgoing direction, 75..77 normal, 78 roughness,
+// 79..81 albedo, 82 constant 1, 83..95 zero.
 __device__ __forceinline__ float2 encode_pair_freq(const float *f, int c)
 {
     if (c < 6 * kMlpBandsFreq) {
         const int axis = c / (2 * kMlpBandsFreq), band = (c % (2 * kMlpBandsFreq)) >> 1;
         float s, co;
-        sincospif(ldexpf(f[axis], band), &s, &co);
+        freq_band(f[axis], band, s, co);
         return make_float2(s, co);
     }
     switch (c) {
@@ -224,7 +250,15 @@ cudaError_t mlp_infer_warp(const MlpDev &M, const float *raw, uint32_t n, float 
 // TMEM); err gets bit 64 set if a bounded wait ran out.
 cudaError_t mlp_infer_tc(const MlpDev &M, const float *raw, uint32_t n, float *out, cudaStream_t st,
                          const uint32_t *n_dev, uint32_t *err);
-cudaError_t mlp_grads(const MlpDev &M, const float *raw, const float *target, uint32_t n, cudaStream_t st);
+// warp_mma: the warp-level mma.sync kernels; otherwise the tcgen05 ones
+// (mlp_train_tc.cu).
+cudaError_t mlp_grads(const MlpDev &M, const float *raw, const float *target, uint32_t n, cudaStream_t st,
+                      bool warp_mma = false);
+// Forward with activations kept, loss and backward (tcgen05): X, H_0..H_4 and
+// dZ_0..dZ_5 into M.xcm / hcm / dzcm, the loss into M.loss.
+cudaError_t mlp_train_tc(const MlpDev &M, const float *raw, const float *target, uint32_t n, cudaStream_t st);
+// dW_l += H_{l-1}^T dZ_l for every layer from the column-major activations (tcgen05).
+cudaError_t mlp_dw_tc(const MlpDev &M, uint32_t n_pad, cudaStream_t st);
 cudaError_t mlp_adam(const MlpDev &M, uint32_t step, float lr, cudaStream_t st);
 
 }  // namespace ilg

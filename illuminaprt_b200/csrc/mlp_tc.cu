@@ -24,10 +24,13 @@
 // limit that raises an error bit instead of hanging.
 #include "devinfo.cuh"
 #include "mlp.cuh"
+#include "umma.cuh"
 
 namespace ilg {
 
 namespace {
+
+using namespace umma;
 
 constexpr int kTcRows = 128;
 constexpr int kTcGroups = 6;         // tile pipelines per CTA
@@ -36,85 +39,6 @@ constexpr size_t kWBytes = ((kUmmaElems * 2 + 1023) / 1024) * 1024;
 constexpr size_t kATileBytes = (size_t)kTcRows * kMlpIn * 2;
 static_assert(64 * kTcGroups <= (int)kTmemCols, "TMEM columns for every group");
 static_assert(kWBytes + kTcGroups * kATileBytes <= 227 * 1024, "shared memory per CTA");
-constexpr uint32_t kWaitLimit = 1u << 22;  // try_wait calls before giving up (seconds at most)
-constexpr uint32_t kErrWait = 64u;
-
-__device__ __forceinline__ uint32_t smem_u32(const void *p)
-{
-    return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-// UMMA shared-memory matrix descriptor, K-major, no swizzle.
-__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo_bytes, uint32_t sbo_bytes)
-{
-    uint64_t d = 0;
-    d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
-    d |= (uint64_t)((lbo_bytes >> 4) & 0x3FFFu) << 16;
-    d |= (uint64_t)((sbo_bytes >> 4) & 0x3FFFu) << 32;
-    d |= (uint64_t)1 << 46;  // descriptor version for sm_100
-    // base offset 0, legacy LBO mode, layout type 0 = no swizzle
-    return d;
-}
-
-// Instruction descriptor: D = F32, A = B = BF16, both K-major, M x N.
-__host__ __device__ constexpr uint32_t umma_idesc(int m, int n)
-{
-    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
-}
-
-__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc,
-                                         uint32_t accumulate)
-{
-    asm volatile(
-        "{\n\t"
-        ".reg .pred p;\n\t"
-        "setp.ne.b32 p, %4, 0;\n\t"
-        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t"
-        "}\n"
-        :
-        : "r"(tmem_d), "l"(da), "l"(db), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
-}
-
-__device__ __forceinline__ void mma_commit(uint32_t bar)
-{
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
-                 : "memory");
-}
-
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
-{
-    for (uint32_t it = 0; it < kWaitLimit; it++) {
-        uint32_t done;
-        asm volatile(
-            "{\n\t"
-            ".reg .pred p;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-            "selp.u32 %0, 1, 0, p;\n\t"
-            "}\n"
-            : "=r"(done)
-            : "r"(bar), "r"(parity)
-            : "memory");
-        if (done) return true;
-    }
-    return false;
-}
-
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16])
-{
-    uint32_t r[16];
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];\n"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-        : "r"(taddr));
-#pragma unroll
-    for (int i = 0; i < 16; i++) v[i] = __uint_as_float(r[i]);
-}
-
-__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
-__device__ __forceinline__ void fence_before_sync() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void fence_after_sync() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
 // Barrier of one group's 128 threads (named barrier 1 + group).
 __device__ __forceinline__ void group_sync(int id)
@@ -137,20 +61,6 @@ __device__ __forceinline__ bool group_and(int id, bool v)
         : "r"((uint32_t)v), "r"(id), "r"(kTcRows)
         : "memory");
     return r != 0;
-}
-
-__device__ __forceinline__ uint32_t pack2(float a, float b)
-{
-    __nv_bfloat162 v = __floats2bfloat162_rn(a, b);
-    return *reinterpret_cast<uint32_t *>(&v);
-}
-
-// 8 consecutive K values (one 16-byte core-matrix row) of row r at K chunk c
-__device__ __forceinline__ void put_chunk(unsigned char *a_tile, int r, int c, int k_total, const float *v)
-{
-    const int kc = k_total / 8;
-    uint4 q = make_uint4(pack2(v[0], v[1]), pack2(v[2], v[3]), pack2(v[4], v[5]), pack2(v[6], v[7]));
-    *reinterpret_cast<uint4 *>(a_tile + (size_t)(r / 8) * kc * 128 + (size_t)c * 128 + (r % 8) * 16) = q;
 }
 
 // The grid columns of every query, one thread per (row, level): the gathers
@@ -212,13 +122,58 @@ __global__ void __launch_bounds__(kTcRows * kTcGroups, 1)
     bool ok = true;
 
     const uint32_t n_tiles = (n + kTcRows - 1) / kTcRows;
+    // the row's 16 raw features as four 16-byte loads, issued one tile ahead
+    float4 fv[4];
+    auto load_row = [&](uint32_t tile) {
+        const uint32_t row = tile * kTcRows + lt;
+        const float4 *src = reinterpret_cast<const float4 *>(raw + (size_t)row * kMlpRaw);
+#pragma unroll
+        for (int k = 0; k < 4; k++) fv[k] = (tile < n_tiles && row < n) ? src[k] : make_float4(0.f, 0.f, 0.f, 0.f);
+    };
+    load_row(blockIdx.x * kTcGroups + grp);
     for (uint32_t tile = blockIdx.x * kTcGroups + grp; tile < n_tiles && ok; tile += gridDim.x * kTcGroups) {
         const uint32_t row = tile * kTcRows + lt;
         // encoded input row -> A tile (K = 96)
         {
             float f[kMlpRaw];
 #pragma unroll
-            for (int k = 0; k < kMlpRaw; k++) f[k] = row < n ? raw[(size_t)row * kMlpRaw + k] : 0.f;
+            for (int k = 0; k < 4; k++) {
+                f[4 * k] = fv[k].x;
+                f[4 * k + 1] = fv[k].y;
+                f[4 * k + 2] = fv[k].z;
+                f[4 * k + 3] = fv[k].w;
+            }
+            load_row(tile + gridDim.x * kTcGroups);
+            if (M.encoding == kEncFreq12) {
+                // per axis: the anchors of bands 0, 4, 8 and three doublings
+                // each (the values freq_band gives), one chunk per anchor
+#pragma unroll
+                for (int a = 0; a < 3; a++) {
+#pragma unroll
+                    for (int j = 0; j < 3; j++) {
+                        float v[8], sn, cs;
+                        sincospif(ldexpf(f[a], 4 * j), &sn, &cs);
+#pragma unroll
+                        for (int k = 0; k < 4; k++) {
+                            if (k) freq_double(sn, cs);
+                            v[2 * k] = row < n ? sn : 0.f;
+                            v[2 * k + 1] = row < n ? cs : 0.f;
+                        }
+                        put_chunk(a_s, lt, 3 * a + j, kMlpIn, v);
+                    }
+                }
+#pragma unroll
+                for (int c = 9; c < kMlpIn / 8; c++) {
+                    float v[8];
+#pragma unroll
+                    for (int e = 0; e < 8; e += 2) {
+                        const float2 p = encode_pair_freq(f, 8 * c + e);
+                        v[e] = row < n ? p.x : 0.f;
+                        v[e + 1] = row < n ? p.y : 0.f;
+                    }
+                    put_chunk(a_s, lt, c, kMlpIn, v);
+                }
+            } else
 #pragma unroll
             for (int c = 0; c < kMlpIn / 8; c++) {
                 float v[8];
@@ -304,6 +259,7 @@ cudaError_t mlp_infer_tc(const MlpDev &M, const float *raw, uint32_t n, float *o
                          const uint32_t *n_dev, uint32_t *err)
 {
     if (n == 0) return cudaSuccess;
+    if ((uintptr_t)raw & 15u) return cudaErrorMisalignedAddress;  // rows are read as 16-byte vectors
     const size_t smem = kWBytes + kTcGroups * kATileBytes;
     cudaError_t e = ensure_dynamic_smem((const void *)k_mlp_infer_tc, (int)smem);
     if (e != cudaSuccess) return e;

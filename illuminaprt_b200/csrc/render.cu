@@ -907,9 +907,18 @@ __global__ void __launch_bounds__(128) k_render_persistent(RenderDev R, uint64_t
     PathLane P;
     float4 ro = make_float4(0.f, 0.f, 0.f, 0.f), rd = ro;  // the closest-hit ray in flight (for shading)
     bool active = false, exhausted = false;  // exhausted is warp-uniform
+    // 0: tracing; 1: closest hit found, waiting to shade; 2: shadow ray done, waiting to be counted
+    uint32_t state = 0;
     const Node8 *nodes = nullptr;
     const Tri *tris = nullptr;
     uint32_t n_nodes = 0, n_tris = 0;
+    auto bind_scene = [&]() {
+        const SceneRec &S = R.scenes[P.sid];
+        nodes = S.nodes;
+        tris = S.tris;
+        n_nodes = S.n_nodes;
+        n_tris = S.n_tris;
+    };
     while (true) {
         const uint32_t idle = __ballot_sync(0xffffffffu, !active);
         if (!exhausted && (__popc(idle) >= kRefillLanes || idle == 0xffffffffu)) {
@@ -922,30 +931,42 @@ __global__ void __launch_bounds__(128) k_render_persistent(RenderDev R, uint64_t
                 const uint64_t k = base + __popc(idle & ((1u << lane) - 1u));
                 if (k < total) {
                     start_path(R, k, P, r);
-                    const SceneRec &S = R.scenes[P.sid];
-                    nodes = S.nodes;
-                    tris = S.tris;
-                    n_nodes = S.n_nodes;
-                    n_tris = S.n_tris;
+                    bind_scene();
                     ro = make_float4(r.ox, r.oy, r.oz, r.tmin);
                     rd = make_float4(r.dx, r.dy, r.dz, r.tcur);
                     active = true;
+                    state = 0;
                 }
             }
         }
-        if (__ballot_sync(0xffffffffu, active) == 0u) break;
-        if (active && ray_step<false, false, false, false, kTrisPerStep, true>(r, stack, nodes, tris, n_nodes, n_tris,
-                                                                               R.err)) {
-            if (r.any) {
+        const uint32_t live = __ballot_sync(0xffffffffu, active);
+        if (live == 0u) break;
+        if (active && state == 0 &&
+            ray_step<false, false, false, false, kTrisPerStep, true>(r, stack, nodes, tris, n_nodes, n_tris, R.err))
+            state = r.any ? 2u : 1u;
+        // Shading and shadow results run for the waiting lanes together, once
+        // half of the warp's paths wait or none is tracing, so that this code
+        // runs with most lanes converged instead of one lane at a time.
+        const uint32_t waiting = __ballot_sync(0xffffffffu, active && state != 0u);
+        const uint32_t tracing = live & ~waiting;
+        if (waiting && (2u * __popc(waiting) >= __popc(live) || tracing == 0u)) {
+            if (active && state == 2u) {
                 // a shadow ray: its light sample counts when nothing is in the way
                 if (r.best == -1) add_pixel(R.accum, P.pixel, P.c);
                 active = next_light_sample(R, P, r) || next_bounce(R, P, r);
-            } else {
-                active = shade_vertex(R, P, r, ro, rd);
+                state = 0;
+                if (active && !r.any) {
+                    ro = make_float4(r.ox, r.oy, r.oz, r.tmin);
+                    rd = make_float4(r.dx, r.dy, r.dz, r.tcur);
+                }
             }
-            if (active && !r.any) {
-                ro = make_float4(r.ox, r.oy, r.oz, r.tmin);
-                rd = make_float4(r.dx, r.dy, r.dz, r.tcur);
+            if (active && state == 1u) {
+                active = shade_vertex(R, P, r, ro, rd);
+                state = 0;
+                if (active && !r.any) {
+                    ro = make_float4(r.ox, r.oy, r.oz, r.tmin);
+                    rd = make_float4(r.dx, r.dy, r.dz, r.tcur);
+                }
             }
         }
     }

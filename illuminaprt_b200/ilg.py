@@ -516,13 +516,15 @@ class GpuSpace:
                                          ILG_MLP_WARP_MMA if warp_mma else 0))
         return out
 
-    def mlp_grads(self, raw, target):
+    def mlp_grads(self, raw, target, warp_mma: bool = False):
+        """(loss, gradient) of the batch; on the tcgen05 kernels, or with
+        warp_mma on the warp-level mma.sync ones."""
         raw = np.ascontiguousarray(raw, np.float32).reshape(-1, ILG_MLP_RAW)
         target = np.ascontiguousarray(target, np.float32).reshape(-1, 3)
         g = np.empty(ILG_MLP_PARAMS, np.float32)
         loss = ctypes.c_float()
         self._check(self.L.ilg_mlp_grads(self.h, raw.ctypes.data, target.ctypes.data, raw.shape[0], g.ctypes.data,
-                                         ctypes.byref(loss), 0))
+                                         ctypes.byref(loss), ILG_MLP_WARP_MMA if warp_mma else 0))
         return loss.value, g
 
     def mlp_train_step(self, raw, target) -> float:

@@ -2,6 +2,7 @@
 #include "GpuRenderer.h"
 
 #include <cstring>
+#include <memory>
 #include <sstream>
 #include <vector>
 
@@ -116,17 +117,28 @@ void GpuRenderer::RenderRegion(RadianceBuffer *p_pRadianceBuffer, int p_nRegionX
           "ilg_render_region");
 
     const float rcpWidth = 1.f / opts.width, rcpHeight = 1.f / opts.height;
+    // the view ray of every pixel (its corner sample, as RenderRegion's last
+    // GetRay would make it) and its first hit, in one batched device query:
+    // the spatial fields PathIntegrator::Radiance sets from that hit
+    // (RadianceContext::SetSpatialContext, Core/Geometry/Intersection.h:92-103)
+    std::vector<Ray> rays(n);
+    std::vector<Intersection> hits(n);
+    std::unique_ptr<bool[]> hit(new bool[n]);
+    for (int j = 0; j < p_nRegionHeight; j++)
+        for (int i = 0; i < p_nRegionWidth; i++)
+            m_pScene->GetCamera()->GetRay((p_nRegionX + i) * rcpWidth, (p_nRegionY + j) * rcpHeight, 0.f, 0.f,
+                                          rays[(size_t)j * p_nRegionWidth + i]);
+    space->IntersectsBatch(rays.data(), n, hits.data(), hit.get());
     for (int j = 0; j < p_nRegionHeight; j++) {
         for (int i = 0; i < p_nRegionWidth; i++) {
-            const size_t k = 3 * ((size_t)j * p_nRegionWidth + i);
+            const size_t p = (size_t)j * p_nRegionWidth + i, k = 3 * p;
             RadianceContext *rc = p_pRadianceBuffer->GetP(p_nBufferX + i, p_nBufferY + j);
             rc->Final = Spectrum(final_rgb[k], final_rgb[k + 1], final_rgb[k + 2]);
             rc->Direct = Spectrum(direct_rgb[k], direct_rgb[k + 1], direct_rgb[k + 2]);
             rc->Indirect = rc->Final - rc->Direct;
             rc->Albedo = Spectrum(albedo_rgb[k], albedo_rgb[k + 1], albedo_rgb[k + 2]);
-            // the ray through the pixel's corner sample, as RenderRegion's last GetRay would
-            m_pScene->GetCamera()->GetRay((p_nRegionX + i) * rcpWidth, (p_nRegionY + j) * rcpHeight, 0.f, 0.f,
-                                          rc->ViewRay);
+            rc->ViewRay = rays[p];
+            if (hit[p]) rc->SetSpatialContext(&hits[p]);
             rc->Flags |= RadianceContext::DF_Computed;
         }
     }

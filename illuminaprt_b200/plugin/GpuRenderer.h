@@ -6,7 +6,9 @@
 // under the reference's own driver loops: Render(), RenderRegion(...) and
 // Commit() keep their meaning, and the RadianceBuffer receives Final,
 // Direct, Indirect (= Final - Direct) and Albedo per pixel with
-// DF_Computed set, each averaged over the renderer's samples per pixel.
+// DF_Computed set, each averaged over the renderer's samples per pixel, and
+// the view ray through the pixel's corner with its first hit's Position,
+// Normal and Distance (one batched device query per region).
 //
 // What it takes from the engine's objects, and what it refuses (with an
 // Exception, never a CPU fallback):

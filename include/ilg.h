@@ -372,12 +372,16 @@ int ilg_mlp_get_grid(ilg_ctx *ctx, float *grid /* ILG_MLP_GRID_PARAMS */);
 int ilg_mlp_set_grid(ilg_ctx *ctx, const float *grid);
 /* The grid part of the gradient the last ilg_mlp_grads computed. */
 int ilg_mlp_get_grid_grads(ilg_ctx *ctx, float *grad /* ILG_MLP_GRID_PARAMS */);
-/* out: n x 3 radiance. Host pointers unless ILG_DEVICE_PTRS. Runs on the
+/* out: n x 3 radiance. Host pointers unless ILG_DEVICE_PTRS (device query
+ * rows must start 16-byte aligned). Runs on the
  * tcgen05 tensor cores (accumulators in TMEM); ILG_MLP_WARP_MMA selects the
  * warp-level mma.sync kernel that training's forward pass uses instead. */
 #define ILG_MLP_WARP_MMA 0x10u
 int ilg_mlp_infer(ilg_ctx *ctx, const float *raw, uint32_t n, float *out, uint32_t flags);
-/* Gradient of the mean relative L2 loss over the batch (no update). */
+/* Gradient of the mean relative L2 loss over the batch (no update). Runs on
+ * the tcgen05 tensor cores (forward, loss and backward in one kernel, the
+ * weight gradients in another, accumulators in TMEM; device rows 16-byte
+ * aligned); with ILG_MLP_WARP_MMA on the warp-level mma.sync kernels. */
 int ilg_mlp_grads(ilg_ctx *ctx, const float *raw, const float *target, uint32_t n, float *grad /* ILG_MLP_PARAMS */,
                   float *loss, uint32_t flags);
 /* One Adam step on the batch; *loss (optional) receives the loss before the step. */

@@ -16,7 +16,11 @@ has no learned component, so this is this project's own oracle):
   direction; 72..74 normal, 75 roughness, 76..78 albedo, 79 constant 1,
   80..95 zero.
 * encoding "freq12" (the frequency-only one): for axis a and band b < 12,
-  column 24a + 2b = sin(2^b pi x_a), the next cos; 72..74 outgoing
+  column 24a + 2b = sin(2^b pi x_a), the next cos, with bands 0, 4, 8 from
+  the sine and cosine (float64, rounded to float32) and the three bands
+  after each by float32 double-angle steps (sin 2a = (2 sin a) cos a,
+  cos 2a = (cos a - sin a)(cos a + sin a)), as the device computes them;
+  72..74 outgoing
   direction, 75..77 normal, 78 roughness, 79..81 albedo, 82 constant 1,
   83..95 zero; no grid.
 * network: 96 -> 64 -> 64 -> 64 -> 64 -> 64 -> 8 (3 used), ReLU after every
@@ -111,11 +115,17 @@ def init_grid(seed=0):
 def encode_freq12(raw):
     r = np.asarray(raw, np.float32).astype(np.float64)
     x = np.zeros((r.shape[0], IN))
+    two = np.float32(2)
     for a in range(3):
-        for b in range(12):
-            arg = np.pi * r[:, a] * (2.0 ** b)
-            x[:, 24 * a + 2 * b] = np.sin(arg)
-            x[:, 24 * a + 2 * b + 1] = np.cos(arg)
+        for j in range(3):
+            arg = np.pi * r[:, a] * (2.0 ** (4 * j))
+            s, c = np.sin(arg).astype(np.float32), np.cos(arg).astype(np.float32)
+            for k in range(4):
+                if k:
+                    s, c = (two * s) * c, (c - s) * (c + s)
+                b = 4 * j + k
+                x[:, 24 * a + 2 * b] = s
+                x[:, 24 * a + 2 * b + 1] = c
     x[:, 72:82] = r[:, 3:13]
     x[:, 82] = 1.0
     return x

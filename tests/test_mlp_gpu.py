@@ -129,3 +129,28 @@ def test_frequency_encoding_matches_oracle(n):
     assert rel < 3e-2 and cos_exact > 0.995
     assert not gg_ref.any()
     sp.close()
+
+
+@pytest.mark.parametrize("encoding", ["hashgrid", "freq12"])
+def test_tcgen05_training_matches_warp_mma_training(encoding):
+    """Training's forward, loss, backward and weight gradients on tcgen05
+    (the default) against the warp-level mma.sync kernels on the same batch:
+    the same BF16 rounding points, FP32 accumulation in another order."""
+    from illuminaprt_b200.ilg import GpuSpace
+    sp = GpuSpace()
+    sp.mlp_init(seed=13, lr=1e-2, encoding=encoding)
+    if encoding == "hashgrid":
+        sp.mlp_set_grid(GRID)
+    raw, tgt = mo.random_batch(3000, seed=21)  # 23.4 tiles of 128 rows: ragged last tile
+    for _ in range(2):
+        sp.mlp_train_step(raw, tgt)
+    l_tc, g_tc = sp.mlp_grads(raw, tgt)
+    l_mma, g_mma = sp.mlp_grads(raw, tgt, warp_mma=True)
+    rel = np.linalg.norm(g_tc - g_mma) / np.linalg.norm(g_mma)
+    print(f"{encoding}: loss tcgen05 {l_tc:.6f} mma.sync {l_mma:.6f}; grad rel diff {rel:.2e}")
+    assert abs(l_tc - l_mma) <= 1e-3 * abs(l_mma) + 1e-7
+    assert rel < 1e-2
+    for l in range(mo.LAYERS):
+        a, b = g_tc[mo.OFFS[l]:mo.OFFS[l + 1]], g_mma[mo.OFFS[l]:mo.OFFS[l + 1]]
+        assert np.linalg.norm(a - b) <= 2e-2 * np.linalg.norm(b) + 1e-9, l
+    sp.close()
