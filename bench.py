@@ -658,6 +658,24 @@ def main():
     e2e_value = replicas.aggregate_rate(rays_per_step * e2e_steps, world, e2e_ms / 1e3) / 1e6
     # the e2e hits must equal the device-resident ones
     assert torch.equal(hout["incoherent"][0], out["incoherent"][0].cpu())
+    # the same from pageable host memory (plain CPU tensors, as a host
+    # application's own arrays are): the library stages them through its two
+    # page-locked slots
+    page = {k: (v[0].clone(), v[1].clone()) for k, v in pin.items()}
+    hpage = {k: tuple(torch.empty_like(x, pin_memory=False) for x in v) for k, v in hout.items()}
+    for k in ("coherent", "incoherent"):
+        sp.intersects_into(*page[k], *hpage[k], device_ptrs=False)
+    replicas.barrier()
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        for k in ("coherent", "incoherent"):
+            sp.intersects_into(*page[k], *hpage[k], device_ptrs=False)
+    e1.record(stream)
+    e1.synchronize()
+    e2e_page_ms = replicas.max_over_ranks(e0.elapsed_time(e1), dev)
+    e2e_page_value = replicas.aggregate_rate(rays_per_step * e2e_steps, world, e2e_page_ms / 1e3) / 1e6
+    assert torch.equal(hpage["incoherent"][0], out["incoherent"][0].cpu())
+    del page, hpage
     # the copy bound of e2e: the same host->device bytes as one plain pinned copy
     h2d_src = torch.cat([pin["coherent"][0], pin["coherent"][1], pin["incoherent"][0],
                          pin["incoherent"][1]]).pin_memory()
@@ -716,6 +734,7 @@ def main():
                     "d2h_bytes_per_step": rays_per_step * HIT_OUT,
                     "pinned_h2d_gbs": round(h2d_gbs, 2),
                     "copy_bound_mrays_s": round(h2d_gbs * 1e3 / RAY_IN, 3),
+                    "e2e_pageable_mrays_s": round(e2e_page_value, 3),
                     "pipeline": "host-buffer calls run in chunks over three streams: upload, traversal and "
                                 "download of neighbouring chunks overlap"},
             "gpu_launches": 2 * args.steps,

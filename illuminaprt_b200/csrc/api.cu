@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <cstring>
 #include <new>
+#include <thread>
 #include <vector>
 
 #include "build.cuh"
@@ -61,6 +62,129 @@ int ensure_raw_tris(ilg_ctx *ctx)
     return ILG_OK;
 }
 
+// Whether p is host memory the device cannot reach directly (not
+// page-locked): copies from it go through a staging buffer.
+bool pageable(const void *p)
+{
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return true;
+    }
+    return a.type == cudaMemoryTypeUnregistered;
+}
+
+// memcpy split over up to 8 host threads (pageable <-> page-locked copies of
+// tens of MB run at a few GB/s on one core)
+void host_copy(void *dst, const void *src, size_t bytes)
+{
+    const size_t kMinPiece = 4u << 20;
+    unsigned th = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+    th = (unsigned)std::min<size_t>(th, (bytes + kMinPiece - 1) / kMinPiece);
+    if (th <= 1) {
+        memcpy(dst, src, bytes);
+        return;
+    }
+    const size_t piece = (bytes + th - 1) / th;
+    std::vector<std::thread> pool;
+    for (unsigned k = 1; k < th; k++) {
+        const size_t off = k * piece;
+        if (off >= bytes) break;
+        pool.emplace_back([=] { memcpy((char *)dst + off, (const char *)src + off, std::min(piece, bytes - off)); });
+    }
+    memcpy(dst, src, std::min(piece, bytes));
+    for (auto &t : pool) t.join();
+}
+
+// Closest hit (occ == nullptr) or any hit of rays in pageable host memory:
+// chunks of rays go through two page-locked slots owned by the context, so
+// the host copies of one chunk (rays in, hits out) overlap the device's work
+// on the other.
+int query_host_pageable(ilg_ctx *ctx, const float *o4, const float *d4, uint32_t n, int32_t *prim, float *t,
+                        float *u, float *v, uint8_t *occ, bool wt)
+{
+    const bool any = occ != nullptr;
+    constexpr uint32_t kChunk = 1u << 19;
+    const size_t in_bytes = 32ull * kChunk, out_bytes = (any ? 1ull : 16ull) * kChunk;
+    const size_t slot_bytes = in_bytes + 16ull * kChunk;
+    if (!ctx->pin_buf) {
+        CK(cudaHostAlloc(&ctx->pin_buf, 2 * slot_bytes, cudaHostAllocDefault));
+        for (int k = 0; k < 2; k++) CK(cudaEventCreateWithFlags(&ctx->pin_ev[k], cudaEventDisableTiming));
+    }
+    (void)out_bytes;
+    const uint32_t m = std::min(n, kChunk);
+    CK(ctx->ro.reserve(m));
+    CK(ctx->rd.reserve(m));
+    if (any) {
+        CK(ctx->hocc.reserve(2ull * m));
+    } else {
+        CK(ctx->hprim.reserve(2ull * m));
+        CK(ctx->ht.reserve(2ull * m));
+        CK(ctx->hu.reserve(2ull * m));
+        CK(ctx->hv.reserve(2ull * m));
+    }
+    const SceneView sv = ctx->view();
+    cudaStream_t st = ctx->stream;
+    uint32_t *next = ctx->derr.ptr + 1;
+    const uint32_t chunks = (n + kChunk - 1) / kChunk;
+    // the results of chunk c, from its slot to the caller's arrays
+    auto copy_out = [&](uint32_t c) -> int {
+        const int s = c & 1;
+        const uint32_t off = c * kChunk, len = std::min(kChunk, n - off);
+        unsigned char *slot = (unsigned char *)ctx->pin_buf + s * slot_bytes + in_bytes;
+        CK(cudaEventSynchronize(ctx->pin_ev[s]));
+        if (any) {
+            host_copy(occ + off, slot, len);
+        } else {
+            host_copy(prim + off, slot, 4ull * len);
+            host_copy(t + off, slot + 4ull * kChunk, 4ull * len);
+            host_copy(u + off, slot + 8ull * kChunk, 4ull * len);
+            host_copy(v + off, slot + 12ull * kChunk, 4ull * len);
+        }
+        return ILG_OK;
+    };
+    for (uint32_t c = 0; c < chunks; c++) {
+        const int s = c & 1;
+        if (c >= 2) {
+            int rc = copy_out(c - 2);
+            if (rc) return rc;
+        }
+        const uint32_t off = c * kChunk, len = std::min(kChunk, n - off);
+        unsigned char *slot = (unsigned char *)ctx->pin_buf + s * slot_bytes;
+        host_copy(slot, o4 + 4ull * off, 16ull * len);
+        host_copy(slot + 16ull * kChunk, d4 + 4ull * off, 16ull * len);
+        // device buffers: rays shared (the previous chunk's kernel is ordered before
+        // this copy on the stream), hits per slot (read back by the slot's copy)
+        float4 *dro = ctx->ro.ptr, *drd = ctx->rd.ptr;
+        CK(cudaMemcpyAsync(dro, slot, 16ull * len, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(drd, slot + 16ull * kChunk, 16ull * len, cudaMemcpyHostToDevice, st));
+        unsigned char *out = slot + in_bytes;
+        if (any) {
+            uint8_t *docc = ctx->hocc.ptr + (size_t)s * m;
+            if (wt) CK(launch_any_wt(sv, ctx->raw_tris.ptr, dro, drd, len, docc, next, ctx->derr.ptr, st));
+            else CK(launch_any_dyn(sv, dro, drd, len, docc, next, ctx->derr.ptr, st));
+            CK(cudaMemcpyAsync(out, docc, len, cudaMemcpyDeviceToHost, st));
+        } else {
+            int32_t *dp = ctx->hprim.ptr + (size_t)s * m;
+            float *dt = ctx->ht.ptr + (size_t)s * m, *du = ctx->hu.ptr + (size_t)s * m, *dv = ctx->hv.ptr + (size_t)s * m;
+            if (wt)
+                CK(launch_closest_wt(sv, ctx->raw_tris.ptr, dro, drd, len, dp, dt, du, dv, next, ctx->derr.ptr, st));
+            else
+                CK(launch_closest_dyn(sv, dro, drd, len, dp, dt, du, dv, next, ctx->derr.ptr, st));
+            CK(cudaMemcpyAsync(out, dp, 4ull * len, cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(out + 4ull * kChunk, dt, 4ull * len, cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(out + 8ull * kChunk, du, 4ull * len, cudaMemcpyDeviceToHost, st));
+            CK(cudaMemcpyAsync(out + 12ull * kChunk, dv, 4ull * len, cudaMemcpyDeviceToHost, st));
+        }
+        CK(cudaEventRecord(ctx->pin_ev[s], st));
+    }
+    for (uint32_t c = chunks >= 2 ? chunks - 2 : 0; c < chunks; c++) {
+        int rc = copy_out(c);
+        if (rc) return rc;
+    }
+    return ctx->check_device_error();
+}
+
 // Closest hit (occ == nullptr) or any hit of rays in host memory. Large
 // batches go in chunks round-robin over three streams, so the upload of one
 // chunk, the traversal of the previous one and the download of the one
@@ -70,6 +194,9 @@ int query_host(ilg_ctx *ctx, const float *o4, const float *d4, uint32_t n, int32
                float *v, uint8_t *occ, bool wt)
 {
     const bool any = occ != nullptr;
+    if (n >= (1u << 16) && (pageable(o4) || pageable(d4) || (any ? pageable(occ) : pageable(prim) || pageable(t) ||
+                                                                   pageable(u) || pageable(v))))
+        return query_host_pageable(ctx, o4, d4, n, prim, t, u, v, occ, wt);
     CK(ctx->ro.reserve(n));
     CK(ctx->rd.reserve(n));
     if (any) {
@@ -183,6 +310,9 @@ int ilg_destroy(ilg_ctx *ctx)
     cudaEventDestroy(ctx->ev1);
     for (auto e : ctx->side_ev)
         if (e) cudaEventDestroy(e);
+    for (auto e : ctx->pin_ev)
+        if (e) cudaEventDestroy(e);
+    if (ctx->pin_buf) cudaFreeHost(ctx->pin_buf);
     for (auto s : ctx->side)
         if (s) cudaStreamDestroy(s);
     cudaStreamDestroy(ctx->stream);

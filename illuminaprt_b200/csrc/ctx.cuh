@@ -53,6 +53,9 @@ struct ilg_ctx {
 
     // staging for host-pointer queries
     ilg::DevBuf<float4> ro, rd;
+    // two page-locked slots for queries from pageable host memory (made on first use)
+    void *pin_buf = nullptr;
+    cudaEvent_t pin_ev[2] = {nullptr, nullptr};
     ilg::DevBuf<int32_t> hprim;
     ilg::DevBuf<float> ht, hu, hv;
     ilg::DevBuf<uint8_t> hocc;

@@ -215,3 +215,28 @@ def test_watertight_mode_closes_the_reference_edge_cracks(oracle):
     assert np.array_equal(ref_mode < 0, brute < 0)  # the reference test's cracks, reproduced
     assert (ref_mode < 0).sum() > 100
     assert (wt_mode < 0).sum() == 0
+
+
+def test_pageable_host_buffers_give_the_pinned_results():
+    """Host rays and hits in pageable memory (plain numpy) go through the
+    context's two page-locked slots in chunks of 524,288 rays; the answers
+    must equal those from page-locked buffers, for both queries and both
+    triangle tests, on a ragged three-chunk batch."""
+    import torch
+    from illuminaprt_b200.ilg import GpuSpace
+    pos, idx = scenes.heightfield(256, 128, 0.2, 4)
+    sp = GpuSpace()
+    sp.initialise(pos, idx)
+    sp.build()
+    o4, d4 = scenes.incoherent_rays(pos, idx, 1_300_001, 6)
+    po, pd = torch.from_numpy(o4).pin_memory(), torch.from_numpy(d4).pin_memory()
+    n = o4.shape[0]
+    for wt in (False, True):
+        pinned = (torch.empty(n, dtype=torch.int32).pin_memory(), *(torch.empty(n).pin_memory() for _ in range(3)))
+        sp.intersects_into(po, pd, *pinned, device_ptrs=False, watertight=wt)
+        got = sp.intersects(o4, d4, watertight=wt)
+        for a, b in zip(got, pinned):
+            assert np.array_equal(np.asarray(a).view(np.uint32), b.numpy().view(np.uint32))
+        occ = sp.occluded(o4, d4, watertight=wt)
+        assert np.array_equal(occ.astype(bool), pinned[0].numpy() >= 0)
+    sp.close()
