@@ -63,7 +63,12 @@ class Oracle:
                                  ctypes.c_uint32, ctypes.c_void_p, ctypes.c_uint32, _f32p, ctypes.c_uint32,
                                  ctypes.c_uint32, ctypes.c_uint32, ctypes.c_uint32, ctypes.c_float, ctypes.c_uint32,
                                  _f32p, ctypes.c_int, _f32p]
+        L.orc_last_render_seconds.restype = ctypes.c_double
         self.L = L
+
+    def last_render_seconds(self) -> float:
+        """Wall seconds of the last render's paths, its tree build excluded."""
+        return float(self.L.orc_last_render_seconds())
 
     def render(self, pos, idx, mat_ids, mats, lights, camera, width, height, spp, max_depth=6, epsilon=1e-4,
                seed=1, sky=(0.0, 0.0, 0.0), nthreads=None):

@@ -21,12 +21,14 @@
  * sky are this project's own (the reference has neither) and are restated
  * here from the same formulas as the device code.
  *
- * Only tests/ may call it. */
+ * Test infrastructure: only tests/ and bench.py's CPU-baseline legs call it. */
+#define _POSIX_C_SOURCE 199309L /* clock_gettime under -std=c11 */
 #include "ilg_oracle.h"
 
 #include <float.h>
 #include <math.h>
 #include <pthread.h>
+#include <time.h>
 #include <stdlib.h>
 #include <string.h>
 
@@ -296,6 +298,17 @@ static void *pt_worker(void *arg)
     return NULL;
 }
 
+/* Wall seconds of the last orc_render's paths (its tree build excluded). */
+static double g_render_seconds;
+double orc_last_render_seconds(void) { return g_render_seconds; }
+
+static double now_seconds(void)
+{
+    struct timespec ts;
+    clock_gettime(CLOCK_MONOTONIC, &ts);
+    return (double)ts.tv_sec + 1e-9 * (double)ts.tv_nsec;
+}
+
 int orc_render(const float *pos, uint32_t nverts, const uint32_t *idx, uint32_t ntris, const uint32_t *mat_ids,
                const orc_material *mats, uint32_t nmats, const orc_quad_light *lights, uint32_t nlights,
                const float cam[11], uint32_t W, uint32_t H, uint32_t spp, uint32_t max_depth, float eps,
@@ -338,8 +351,10 @@ int orc_render(const float *pos, uint32_t nverts, const uint32_t *idx, uint32_t 
     if (nthreads < 1) nthreads = 1;
     if (nthreads > 256) nthreads = 256;
     pthread_t th[256];
+    const double t0 = now_seconds();
     for (int i = 0; i < nthreads; i++) pthread_create(&th[i], NULL, pt_worker, &c);
     for (int i = 0; i < nthreads; i++) pthread_join(th[i], NULL);
+    g_render_seconds = now_seconds() - t0;
     pthread_mutex_destroy(&c.lock);
     orc_bvh_destroy(c.bvh);
     return 0;
