@@ -74,12 +74,12 @@ bool pageable(const void *p)
     return a.type == cudaMemoryTypeUnregistered;
 }
 
-// memcpy split over up to 8 host threads (pageable <-> page-locked copies of
-// tens of MB run at a few GB/s on one core)
+// memcpy split over up to 16 host threads, 1 MB a thread at least
+// (pageable <-> page-locked copies run at about 10 GB/s on one core)
 void host_copy(void *dst, const void *src, size_t bytes)
 {
-    const size_t kMinPiece = 4u << 20;
-    unsigned th = std::max(1u, std::min(8u, std::thread::hardware_concurrency()));
+    const size_t kMinPiece = 1u << 20;
+    unsigned th = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
     th = (unsigned)std::min<size_t>(th, (bytes + kMinPiece - 1) / kMinPiece);
     if (th <= 1) {
         memcpy(dst, src, bytes);

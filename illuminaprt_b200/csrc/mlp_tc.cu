@@ -223,15 +223,19 @@ __global__ void __launch_bounds__(kTcRows * kTcGroups, 1)
             phase ^= 1u;
             fence_after_sync();
             if (l < kMlpLayers - 1) {
+                // 64 columns in four 16-column loads; ReLU and the BF16
+                // rounding in one cvt per pair
 #pragma unroll
-                for (int q = 0; q < 4; q++) {
-                    float v[16];
-                    tmem_ld16(taddr + q * 16, v);
+                for (int h = 0; h < 4; h++) {
+                    uint32_t r[16];
+                    tmem_ld16(taddr + h * 16, r);
                     tmem_wait_ld();
 #pragma unroll
-                    for (int e = 0; e < 16; e++) v[e] = fmaxf(v[e], 0.f);
-                    put_chunk(a_s, lt, 2 * q, kMlpHid, v);
-                    put_chunk(a_s, lt, 2 * q + 1, kMlpHid, v + 8);
+                    for (int c = 0; c < 2; c++)
+                        put_chunk_bits(a_s, lt, 2 * h + c, kMlpHid,
+                                       make_uint4(pack2_relu(r[8 * c], r[8 * c + 1]), pack2_relu(r[8 * c + 2], r[8 * c + 3]),
+                                                  pack2_relu(r[8 * c + 4], r[8 * c + 5]),
+                                                  pack2_relu(r[8 * c + 6], r[8 * c + 7])));
                 }
             } else {
                 float v[16];

@@ -69,13 +69,16 @@ __global__ void __launch_bounds__(128) k_trace_dyn(const Node8 *__restrict__ nod
                                                    uint32_t *__restrict__ err, const float4 *__restrict__ raw = nullptr)
 {
     const uint32_t lane = threadIdx.x & 31u;
-    uint2 stack[kMaxStack];
+    static_assert(kStackColumns == 128, "k_trace_dyn runs 128 threads a block");
+    __shared__ uint2 sstack[kShortStack * kStackColumns];
+    uint2 lstack[kMaxStack - kShortStack];
+    const SplitStack stack{sstack + threadIdx.x, lstack};
     RayState r;
     bool active = false, exhausted = false;  // exhausted is warp-uniform
     uint32_t id = 0;
     while (true) {
         const uint32_t idle = __ballot_sync(0xffffffffu, !active);
-        if (!exhausted && (__popc(idle) >= kRefillLanes || idle == 0xffffffffu)) {
+        if (!exhausted && (__popc(idle) >= kRefillLanesQuery || idle == 0xffffffffu)) {
             const uint32_t leader = __ffs(idle) - 1u;
             uint32_t base = 0;
             if (lane == leader) base = atomicAdd(next, (uint32_t)__popc(idle));
@@ -91,7 +94,7 @@ __global__ void __launch_bounds__(128) k_trace_dyn(const Node8 *__restrict__ nod
             }
         }
         if (__ballot_sync(0xffffffffu, active) == 0u) break;
-        if (active && ray_step<kAnyHit, false, false, kWT>(r, stack, nodes, tris, n_nodes_total, n_tris_total, err,
+        if (active && ray_step<kAnyHit, false, false, kWT, kTrisPerStep, false, SplitStack>(r, stack, nodes, tris, n_nodes_total, n_tris_total, err,
                                                             nullptr, nullptr, Skip{nullptr, 0u, 0u}, raw)) {
             if (kAnyHit) {
                 occ[id] = r.best >= 0 ? 1 : 0;

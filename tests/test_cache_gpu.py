@@ -123,21 +123,6 @@ def test_cache_in_regions(field):
     assert not np.allclose(after, one, rtol=1e-4, atol=1e-5)
 
 
-def test_equal_time_gain_over_plain_at_scale():
-    """The full 64-icosphere field (20,971,530 triangles) at 960 x 540: the
-    cached path tracer against plain path tracing at equal wall time."""
-    from illuminaprt_b200.ilg import GpuSpace
-    w, h = 960, 540
-    s = scenes.sphere_field(8, 7, seed=3, width=w, height=h)
-    sp = GpuSpace()
-    scenes.load_sphere_field(sp, s)
-    gt = sp.render(dict(s["camera"], aspect=w / h), w, h, 4096, max_depth=12, seed=424242, sky=s["sky"])
-    r = equal_time(sp, s, w, h, gt, frames=64, warmup=8, cache_depth=1, train_steps=8, train_batch=32768)
-    print({k: v for k, v in r.items() if not k.endswith("image")})
-    assert r["relmse_cached"] < r["relmse_plain"]
-    assert max(abs(b) for b in r["bias_cached"]) < 0.02
-
-
 def test_training_is_what_helps(field):
     """Ablation: the same cached renderer with a network that never trains."""
     sp, s, gt = field
@@ -145,3 +130,26 @@ def test_training_is_what_helps(field):
     frozen = equal_time(sp, s, W, H, gt, frames=48, warmup=16, cache_depth=1, ablate_training=True)
     print(f"relMSE trained {trained['relmse_cached']:.5f} vs untrained {frozen['relmse_cached']:.5f}")
     assert trained["relmse_cached"] < frozen["relmse_cached"] / 2
+
+
+def test_gain_at_equal_time_under_the_fair_protocol():
+    """The full 64-icosphere field (20,971,530 triangles) at 960 x 540 and a
+    0.25 s budget: plain path tracing renders its budget in calls that fill a
+    wave (no per-frame synchronisation), and the self-training hash-grid
+    cache must still beat it by a set factor, against a 4096-spp ground
+    truth. (On cheap scenes, where plain path tracing converges within the
+    budget, the cache's approximation error floor makes it lose; that is the
+    expected crossover, not a failure.)"""
+    from illuminaprt_b200.ilg import GpuSpace
+    from illuminaprt_b200.cache_experiment import ARMS, gain_versus_budget
+    w, h = 960, 540
+    s = scenes.sphere_field(8, 7, seed=3, width=w, height=h)
+    sp = GpuSpace()
+    scenes.load_sphere_field(sp, s)
+    gt = sp.render(dict(s["camera"], aspect=w / h), w, h, 4096, max_depth=12, seed=424242, sky=s["sky"])
+    arms = {k: ARMS[k] for k in ("hashgrid_self_training", "spec_freq12_full_depth_cache_depth_1")}
+    r = gain_versus_budget(sp, s, w, h, gt, budgets=(0.25,), arms=arms)
+    print(r)
+    best = r["arms"]["hashgrid_self_training"][0]
+    assert best["gain"] >= 2.5  # 3.6x measured on a B200
+    assert max(abs(b) for b in best["bias"]) < 0.02
