@@ -325,6 +325,65 @@ def bench_cache(res, local, budgets=(0.5, 2.0)):
         r["cpu_baseline"] = ic_cpu_baseline()
     except (FileNotFoundError, OSError, RuntimeError) as e:
         r["cpu_baseline"] = {"unavailable": str(e)[:200]}
+    res["cache_matte_field"] = cache_matte_field(local)
+
+
+def cache_matte_field(local, gpu_size=(960, 540), cpu_size=(240, 135), gpu_budgets=(0.25, 1.0), ic_spp=4):
+    """The reference's irradiance cache and this project's learned caches on
+    one scene the reference can render (scenes.matte_field: the icosphere
+    field with every sphere Lambertian, 81,924 triangles, one quad light).
+    On the device: plain path tracing against the hash-grid network with
+    self-training tails and against the hash-grid cache, at equal wall time
+    (gpu_budgets, 960x540, 16384-spp ground truth of this renderer). On the
+    host (one thread: the reference's ICIntegrator shares one octree of
+    records and is not thread-safe): the reference's ICIntegrator (factory
+    defaults, ic_spp samples per pixel) against its PathIntegrator at equal
+    CPU time (time of the integrators' Initialise to Commit, scene loading
+    excluded), both through its BasicRenderer from a scene script, relMSE
+    against this renderer's 16384-spp image at the same size."""
+    import tempfile
+
+    from illuminaprt_b200 import scenes
+    from illuminaprt_b200.cache_experiment import ARMS, gain_versus_budget, rel_mse
+    from illuminaprt_b200.ilg import GpuSpace
+    gw, gh = gpu_size
+    sc = scenes.matte_field(width=gw, height=gh)
+    sp = GpuSpace(device=local)
+    scenes.load_box_scene(sp, sc)
+    cam = dict(sc["camera"], aspect=gw / gh)
+    gt = sp.render(cam, gw, gh, 16384, max_depth=12, seed=424242)
+    arms = {k: ARMS[k] for k in ("hashgrid_self_training", "hash_grid_cache")}
+    out = {"scene": f"matte icosphere field ({sc['prim_of_tri'].size} triangles, one quad light)",
+           "device": gain_versus_budget(sp, sc, gw, gh, gt, budgets=gpu_budgets, arms=arms)}
+    out["device"]["size"] = f"{gw}x{gh}"
+    cw, ch = cpu_size
+    gt_small = sp.render(dict(sc["camera"], aspect=cw / ch), cw, ch, 16384, max_depth=12, seed=424243)
+    sp.close()
+    try:
+        from oracle import bindings
+        ref = bindings.RefLib()
+        with tempfile.TemporaryDirectory() as tmp:
+            def run(integrator, spp):
+                script = scenes.write_box_script(os.path.join(tmp, f"{integrator}{spp}"), scene=sc, width=cw,
+                                                 height=ch, spp=spp, space="Basic", renderer="Basic",
+                                                 integrator=integrator)
+                img, _, _, info = ref.render_script(script, cw, ch)
+                return img, float(info.rsplit("render_s=", 1)[1])
+            ic, t_ic = run("IC", ic_spp)
+            _, t_pt1 = run("PathTracing", 1)
+            pt_spp = max(1, int(round(t_ic / t_pt1)))
+            pt, t_pt = run("PathTracing", pt_spp)
+        e_ic, e_pt = rel_mse(ic, gt_small), rel_mse(pt, gt_small)
+        out["reference_ic"] = {
+            "kind": "reference", "cores": 1, "size": f"{cw}x{ch}", "gain": round(e_pt / e_ic, 3),
+            "relmse_ic": round(e_ic, 5), "relmse_plain": round(e_pt, 5),
+            "bias_ic": [round(b, 4) for b in (ic.mean((0, 1)) / gt_small.mean((0, 1)) - 1.0).tolist()],
+            "bias_plain": [round(b, 4) for b in (pt.mean((0, 1)) / gt_small.mean((0, 1)) - 1.0).tolist()],
+            "sample": f"ICIntegrator {ic_spp} spp in {t_ic:.2f} s vs PathIntegrator {pt_spp} spp in {t_pt:.2f} s, "
+                      f"one thread, {cw}x{ch}"}
+    except (FileNotFoundError, OSError, RuntimeError, ValueError, IndexError) as e:
+        out["reference_ic"] = {"unavailable": str(e)[:200]}
+    return out
 
 
 def ic_cpu_baseline(width=64, ic_spp=16):

@@ -642,6 +642,43 @@ def sphere_field(n_side: int = 8, subdiv: int = 7, seed: int = 3, width: int = 1
     }
 
 
+def matte_field(n_side: int = 8, subdiv: int = 3, seed: int = 3, width: int = 480, height: int = 270):
+    """The icosphere field in the box-scene form (write_box_script,
+    load_box_scene), with what the reference's own integrators can render:
+    every sphere Lambertian (a conductor of sphere_field gets its F0 as
+    albedo), the 100 x 100 ground (albedo 0.5), and one 4 x 4 quad light at
+    height 6 over the field's centre with radiance 20 (the power of
+    sphere_field's four 2 x 2 lights at their mean radiance); no sky. The
+    camera looks down on the field so that every camera ray hits the ground
+    (the reference's ICIntegrator answers a camera ray that escapes with a
+    fixed colour, ICIntegrator.cpp:432). The scene on which the reference's
+    irradiance cache and this project's learned cache are compared."""
+    f = sphere_field(n_side, subdiv, seed, width, height)
+    n_geo = f["idx"].shape[0] - 8  # the spheres and the ground (the four lights' triangles dropped)
+    tris = f["pos"][f["idx"][:n_geo].astype(np.int64)]  # (n_geo, 3, 3)
+    prim_of_tri = f["mat_ids"][:n_geo].astype(np.uint32)
+    albedo = [m["albedo"] if m["kind"] == 0 else m["f0"] for m in f["materials"]]
+    y, h = 6.0, 2.0
+    q = np.array([(-h, y, -h), (-h, y, h), (h, y, h), (h, y, -h)], np.float32)
+    light_tris = np.array([(q[0], q[2], q[1]), (q[0], q[3], q[2])], np.float32)  # normal -y
+    light_prim = len(albedo)
+    albedo.append((0.0, 0.0, 0.0))
+    pos = np.concatenate([tris, light_tris]).reshape(-1, 3).astype(np.float32)
+    n_tris = pos.shape[0] // 3
+    return {
+        "pos": pos,
+        "idx": np.arange(3 * n_tris, dtype=np.uint32).reshape(-1, 3),
+        "prim_of_tri": np.concatenate([prim_of_tri, np.full(2, light_prim, np.uint32)]),
+        "albedo": np.asarray(albedo, np.float32),
+        "light_prim": light_prim,
+        "light_quad": q,
+        "light_emit": np.array([20.0, 20.0, 20.0], np.float32),
+        "camera": {"eye": (0.0, 4.5, 8.0), "target": (0.0, 0.0, 0.0), "up": (0.0, 1.0, 0.0), "fov": 40.0,
+                   "aspect": width / height},
+        "max_depth": 12, "epsilon": 1e-4, "light_kind": 0,
+    }
+
+
 def load_sphere_field(space, scene):
     space.initialise(scene["pos"], scene["idx"], scene["mat_ids"])
     space.build()

@@ -36,6 +36,7 @@
 // PlugInManager (its "GPU" space and renderer factories).
 //
 // Only tests/ load the library this file builds.
+#include <chrono>
 #include <cstdint>
 #include <cstring>
 #include <fstream>
@@ -217,7 +218,8 @@ extern "C" {
 // the script's device) with Render (tile <= 0) or RenderRegion over tile x
 // tile regions, then Commit. Outputs Final, Direct and Albedo (height x width
 // x 3 each) and, in info, "space=<name> renderer=<name> primitives=<n>
-// lights=<n>". Returns 0, or a negative code with the reason in err: -1
+// lights=<n> render_s=<seconds from the integrator's Initialise to Commit>".
+// Returns 0, or a negative code with the reason in err: -1
 // script or a file it names missing, -2 plug-in load, -3 load or parse
 // exception, -4 the script left no renderer, scene, camera, integrator or
 // device, -5 device size differs, -6 render exception.
@@ -298,6 +300,7 @@ int ilref_render_script(const char *plugin_path, const char *script, int width, 
 
 	RadianceBuffer buffer(width, height);
 	int rc = 0;
+	const auto t0 = std::chrono::steady_clock::now();
 	try {
 		renderer->GetIntegrator()->Initialise(scene, scene->GetCamera());
 		renderer->Initialise();
@@ -317,6 +320,12 @@ int ilref_render_script(const char *plugin_path, const char *script, int width, 
 		rc = -6;
 	}
 	if (rc == 0) {
+		const double render_s = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+		if (info && info_len > 0) {
+			std::ostringstream s;
+			s << info << " render_s=" << render_s;
+			report(info, info_len, s.str());
+		}
 		for (int y = 0; y < height; y++)
 			for (int x = 0; x < width; x++) {
 				const RadianceContext *c = buffer.GetP(x, y);
