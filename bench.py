@@ -597,8 +597,67 @@ def bench_batch(res, local):
     return res
 
 
+PROFILE_CASES = ("trace_heightfield", "mlp_infer_freq12", "mlp_infer_hashgrid", "mlp_train_hashgrid",
+                 "mlp_train_freq12", "field_frame", "field_frame_one_launch")
+
+
+def profile_case(name):
+    """Small fixed workloads for kernel profiles (one process, cuda:0):
+    trace_heightfield: two coherent then two incoherent closest-hit launches
+    on the 1 M-triangle heightfield; mlp_infer_*: three inference launches
+    of 2,097,152 random queries; mlp_train_*: three training steps of
+    16,384 random rows; field_frame(_one_launch): two 960x540 1-spp frames
+    of the 20,971,530-triangle icosphere field (wavefront, or the one-launch
+    renderer)."""
+    import torch
+    from illuminaprt_b200 import scenes
+    from illuminaprt_b200.ilg import GpuSpace
+    sp = GpuSpace(device=0)
+    if name == "trace_heightfield":
+        pos, idx, rays_c, rays_i = scenes.ray_batch_workload()
+        sp.initialise(pos, idx)
+        sp.build()
+        for o, d in (rays_c, rays_i):
+            O, D = torch.from_numpy(o).cuda(), torch.from_numpy(d).cuda()
+            out = (torch.empty(O.shape[0], dtype=torch.int32, device="cuda"),
+                   *(torch.empty(O.shape[0], device="cuda") for _ in range(3)))
+            for _ in range(2):
+                sp.intersects_into(O, D, *out, device_ptrs=True)
+            sp.sync()
+    elif name.startswith("mlp_infer_"):
+        nq = 1 << 21
+        q = torch.rand((nq, 16), device="cuda:0")
+        y = torch.empty((nq, 3), device="cuda:0")
+        sp.mlp_init(seed=1, encoding=name[len("mlp_infer_"):])
+        for _ in range(3):
+            sp._check(sp.L.ilg_mlp_infer(sp.h, q.data_ptr(), nq, y.data_ptr(), 0x1))
+        sp.sync()
+    elif name.startswith("mlp_train_"):
+        n = 16384
+        q = torch.rand((n, 16), device="cuda:0")
+        t = torch.rand((n, 3), device="cuda:0")
+        g = torch.empty(23040, device="cuda:0")
+        loss = torch.empty(1, device="cuda:0")
+        sp.mlp_init(seed=1, encoding=name[len("mlp_train_"):])
+        for _ in range(3):
+            sp._check(sp.L.ilg_mlp_grads(sp.h, q.data_ptr(), t.data_ptr(), n, g.data_ptr(), loss.data_ptr(), 0x1))
+        sp.sync()
+    elif name.startswith("field_frame"):
+        f = scenes.sphere_field(8, 7, seed=3)
+        scenes.load_sphere_field(sp, f)
+        cam = dict(f["camera"], aspect=960 / 540)
+        for k in range(2):
+            sp.render(cam, 960, 540, 1, max_depth=12, seed=1 + k, sky=f["sky"],
+                      one_launch=name.endswith("one_launch"))
+        sp.sync()
+    sp.close()
+    print(f"{name}: ok", flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
+    ap.add_argument("--case", choices=PROFILE_CASES,
+                    help="run one small profiling workload on cuda:0 and exit (no JSON line)")
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
@@ -612,6 +671,9 @@ def main():
     ap.add_argument("--legs", default="box,field,mlp,batch,cache",
                     help="extra measurements after the ray query: box,field,mlp,batch")
     args = ap.parse_args()
+    if args.case:
+        profile_case(args.case)
+        return
     world, rank, local = dist_setup()
 
     if args.impl == "reference":
