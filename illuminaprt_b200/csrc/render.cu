@@ -854,10 +854,10 @@ __device__ __forceinline__ bool next_bounce(const RenderDev &R, PathLane &P, Ray
     return true;
 }
 
-// The closest hit of the path's ray is in r: what the vertex adds, and its
-// light samples and next ray (k_shade's rules). Returns whether the lane has
-// a ray to trace.
-__device__ __forceinline__ bool shade_vertex(const RenderDev &R, PathLane &P, RayState &r, float4 o, float4 d)
+// The closest hit of the path's ray is in r: what the vertex adds, and the
+// vertex's state for its light samples and next ray (k_shade's rules).
+// Returns whether the path goes on from this vertex.
+__device__ __forceinline__ bool shade_vertex(const RenderDev &R, PathLane &P, const RayState &r, float4 o, float4 d)
 {
     const SceneRec &S = R.scenes[P.sid];
     const int ti = r.best;
@@ -898,8 +898,7 @@ __device__ __forceinline__ bool shade_vertex(const RenderDev &R, PathLane &P, Ra
     P.nee_beta = P.beta;
     P.next_beta = P.beta;
     P.cont = continue_path(S, P.key, depth, m, P.specular, p, ng, U, V, W, wo_l, P.next_beta, P.no, P.nd);
-    if (next_light_sample(R, P, r)) return true;
-    return next_bounce(R, P, r);
+    return true;
 }
 
 constexpr int kPersistThreads = 128;
@@ -962,18 +961,14 @@ __global__ void __launch_bounds__(kPersistThreads) k_render_persistent(RenderDev
         const uint32_t waiting = __ballot_sync(0xffffffffu, active && state != 0u);
         const uint32_t tracing = live & ~waiting;
         if (waiting && (2u * __popc(waiting) >= __popc(live) || tracing == 0u)) {
-            if (active && state == 2u) {
-                // a shadow ray: its light sample counts when nothing is in the way
-                if (r.best == -1) add_pixel(R.accum, P.pixel, P.c);
+            // a shadow ray's light sample counts when nothing is in the way;
+            // a closest hit is shaded; then either lane takes the vertex's
+            // next light sample or its next ray (one copy of that code, so
+            // the kernel stays small enough for the instruction cache)
+            if (active && state == 2u && r.best == -1) add_pixel(R.accum, P.pixel, P.c);
+            if (active && state == 1u) active = shade_vertex(R, P, r, ro, rd);
+            if (active && state != 0u) {
                 active = next_light_sample(R, P, r) || next_bounce(R, P, r);
-                state = 0;
-                if (active && !r.any) {
-                    ro = make_float4(r.ox, r.oy, r.oz, r.tmin);
-                    rd = make_float4(r.dx, r.dy, r.dz, r.tcur);
-                }
-            }
-            if (active && state == 1u) {
-                active = shade_vertex(R, P, r, ro, rd);
                 state = 0;
                 if (active && !r.any) {
                     ro = make_float4(r.ox, r.oy, r.oz, r.tmin);
