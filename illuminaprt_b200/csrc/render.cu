@@ -767,12 +767,12 @@ __global__ void __launch_bounds__(kStackColumns) k_shadow_dyn(RenderDev R, uint3
 // The whole render as one persistent launch: each lane carries one path from
 // its camera ray through every bounce (closest hit, shading, one shadow ray
 // per light, the next ray) and takes a new path from a device counter when
-// its path ends; a warp refills once kRefillLanes of its lanes are idle. The
-// paths of every scene of a batch, of any length, flow through the same
-// kernel with no host round trip and no queue in memory. Closest-hit and
-// shadow rays share one traversal loop (ray_step<kMixed>), so lanes tracing
-// either kind stay on the same code; shading runs in the lane whose ray just
-// finished. The sample sequence, the shading code (light_sample,
+// its path ends; a warp refills once kRefillLanesPersistent of its lanes are
+// idle. The paths of every scene of a batch, of any length, flow through the
+// same kernel with no host round trip and no queue in memory. Closest-hit
+// and shadow rays share one traversal loop (ray_step<kMixed>), so lanes
+// tracing either kind stay on the same code; lanes whose ray finished wait
+// and shade together. The sample sequence, the shading code (light_sample,
 // continue_path) and the traversal are the wavefront's, so every path is the
 // wavefront path of the same index and the images agree up to the order of
 // the float additions into each pixel. Plain renders only: no radiance
@@ -902,6 +902,10 @@ __device__ __forceinline__ bool shade_vertex(const RenderDev &R, PathLane &P, co
 }
 
 constexpr int kPersistThreads = 128;
+// A warp of the one-launch renderer takes new paths once 16 of its lanes are
+// idle (a path start costs a camera ray and a scene lookup; 8 measured 2 %
+// slower on the 32-scene batch, 4 5 % slower).
+constexpr uint32_t kRefillLanesPersistent = 16;
 
 __global__ void __launch_bounds__(kPersistThreads) k_render_persistent(RenderDev R, uint64_t total, unsigned long long *next)
 {
@@ -932,7 +936,7 @@ __global__ void __launch_bounds__(kPersistThreads) k_render_persistent(RenderDev
     };
     while (true) {
         const uint32_t idle = __ballot_sync(0xffffffffu, !active);
-        if (!exhausted && (__popc(idle) >= kRefillLanes || idle == 0xffffffffu)) {
+        if (!exhausted && (__popc(idle) >= kRefillLanesPersistent || idle == 0xffffffffu)) {
             const uint32_t leader = __ffs(idle) - 1u;
             unsigned long long base = 0;
             if (lane == leader) base = atomicAdd(next, (unsigned long long)__popc(idle));
@@ -956,11 +960,14 @@ __global__ void __launch_bounds__(kPersistThreads) k_render_persistent(RenderDev
             ray_step<false, false, false, false, kTrisPerStep, true>(r, stack, nodes, tris, n_nodes, n_tris, R.err))
             state = r.any ? 2u : 1u;
         // Shading and shadow results run for the waiting lanes together, once
-        // half of the warp's paths wait or none is tracing, so that this code
-        // runs with most lanes converged instead of one lane at a time.
+        // three quarters of the warp's paths wait or none is tracing, so that
+        // this code runs with most lanes converged instead of one lane at a
+        // time (measured on a B200: half the warp 215, three quarters 233,
+        // seven eighths 243, all 239 Msamples/s on the 32-scene batch; on the
+        // field 175 / 184 / 179 / 152).
         const uint32_t waiting = __ballot_sync(0xffffffffu, active && state != 0u);
         const uint32_t tracing = live & ~waiting;
-        if (waiting && (2u * __popc(waiting) >= __popc(live) || tracing == 0u)) {
+        if (waiting && (4u * __popc(waiting) >= 3u * __popc(live) || tracing == 0u)) {
             // a shadow ray's light sample counts when nothing is in the way;
             // a closest hit is shaded; then either lane takes the vertex's
             // next light sample or its next ray (one copy of that code, so
