@@ -598,7 +598,7 @@ def bench_batch(res, local):
 
 
 PROFILE_CASES = ("trace_heightfield", "mlp_infer_freq12", "mlp_infer_hashgrid", "mlp_train_hashgrid",
-                 "mlp_train_freq12", "field_frame", "field_frame_one_launch")
+                 "mlp_train_freq12", "field_frame", "field_frame_one_launch", "cache_frames_1080p")
 
 
 def profile_case(name):
@@ -608,7 +608,10 @@ def profile_case(name):
     of 2,097,152 random queries; mlp_train_*: three training steps of
     16,384 random rows; field_frame(_one_launch): two 960x540 1-spp frames
     of the 20,971,530-triangle icosphere field (wavefront, or the one-launch
-    renderer)."""
+    renderer); cache_frames_1080p: eight 1920x1080 1-spp frames of that
+    field with the radiance cache (hash-grid network, cache at the first
+    bounce, 1-vertex self-training tails, two passes of 4 Adam steps of 16,384
+    records: the equal-time comparison's best arm), then eight plain ones."""
     import torch
     from illuminaprt_b200 import scenes
     from illuminaprt_b200.ilg import GpuSpace
@@ -641,6 +644,17 @@ def profile_case(name):
         sp.mlp_init(seed=1, encoding=name[len("mlp_train_"):])
         for _ in range(3):
             sp._check(sp.L.ilg_mlp_grads(sp.h, q.data_ptr(), t.data_ptr(), n, g.data_ptr(), loss.data_ptr(), 0x1))
+        sp.sync()
+    elif name == "cache_frames_1080p":
+        f = scenes.sphere_field(8, 7, seed=3)
+        scenes.load_sphere_field(sp, f)
+        cam = dict(f["camera"], aspect=1920 / 1080)
+        sp.mlp_init(seed=1, lr=1e-2)
+        for k in range(8):
+            sp.render(cam, 1920, 1080, 1, max_depth=12, seed=k, sky=f["sky"], cache_depth=1, train_steps=4,
+                      train_batch=16384, train_tail=1, train_epochs=2)
+        for k in range(8):
+            sp.render(cam, 1920, 1080, 1, max_depth=12, seed=k, sky=f["sky"])
         sp.sync()
     elif name.startswith("field_frame"):
         f = scenes.sphere_field(8, 7, seed=3)

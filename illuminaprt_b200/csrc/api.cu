@@ -90,7 +90,12 @@ void host_copy(void *dst, const void *src, size_t bytes)
     for (unsigned k = 1; k < th; k++) {
         const size_t off = k * piece;
         if (off >= bytes) break;
-        pool.emplace_back([=] { memcpy((char *)dst + off, (const char *)src + off, std::min(piece, bytes - off)); });
+        auto copy = [=] { memcpy((char *)dst + off, (const char *)src + off, std::min(piece, bytes - off)); };
+        try {
+            pool.emplace_back(copy);
+        } catch (...) {  // no thread to be had: this piece on the calling thread
+            copy();
+        }
     }
     memcpy(dst, src, std::min(piece, bytes));
     for (auto &t : pool) t.join();
@@ -100,8 +105,8 @@ void host_copy(void *dst, const void *src, size_t bytes)
 // chunks of rays go through two page-locked slots owned by the context, so
 // the host copies of one chunk (rays in, hits out) overlap the device's work
 // on the other.
-int query_host_pageable(ilg_ctx *ctx, const float *o4, const float *d4, uint32_t n, int32_t *prim, float *t,
-                        float *u, float *v, uint8_t *occ, bool wt)
+int query_host_pageable_run(ilg_ctx *ctx, const float *o4, const float *d4, uint32_t n, int32_t *prim, float *t,
+                            float *u, float *v, uint8_t *occ, bool wt)
 {
     const bool any = occ != nullptr;
     constexpr uint32_t kChunk = 1u << 19;
@@ -183,6 +188,16 @@ int query_host_pageable(ilg_ctx *ctx, const float *o4, const float *d4, uint32_t
         if (rc) return rc;
     }
     return ctx->check_device_error();
+}
+
+int query_host_pageable(ilg_ctx *ctx, const float *o4, const float *d4, uint32_t n, int32_t *prim, float *t,
+                        float *u, float *v, uint8_t *occ, bool wt)
+{
+    const int rc = query_host_pageable_run(ctx, o4, d4, n, prim, t, u, v, occ, wt);
+    // after a failure, copies of this call may still be in flight into the
+    // page-locked slots that the next call fills from the host
+    if (rc != ILG_OK) cudaStreamSynchronize(ctx->stream);
+    return rc;
 }
 
 // Closest hit (occ == nullptr) or any hit of rays in host memory. Large

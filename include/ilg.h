@@ -28,6 +28,13 @@
 
 #include <stdint.h>
 
+/* Only the ilg_* entry points are exported from libilg.so. */
+#if defined(__GNUC__)
+#define ILG_API __attribute__((visibility("default")))
+#else
+#define ILG_API
+#endif
+
 #ifdef __cplusplus
 extern "C" {
 #endif
@@ -69,16 +76,16 @@ typedef struct ilg_stats {
     uint64_t tri_bytes;     /* bytes of triangle records */
 } ilg_stats;
 
-int ilg_create(ilg_ctx **out, const ilg_opts *opts);
-int ilg_destroy(ilg_ctx *ctx);
-const char *ilg_last_error(const ilg_ctx *ctx);
+ILG_API int ilg_create(ilg_ctx **out, const ilg_opts *opts);
+ILG_API int ilg_destroy(ilg_ctx *ctx);
+ILG_API const char *ilg_last_error(const ilg_ctx *ctx);
 
 /* Positions are n_verts x 3 floats (world space), indices n_tris x 3.
  * mat_ids (optional, n_tris) tags each triangle with a material slot. */
-int ilg_set_mesh(ilg_ctx *ctx, const float *pos_xyz, uint32_t n_verts,
+ILG_API int ilg_set_mesh(ilg_ctx *ctx, const float *pos_xyz, uint32_t n_verts,
                  const uint32_t *idx, uint32_t n_tris, const uint32_t *mat_ids);
-int ilg_build(ilg_ctx *ctx);
-int ilg_get_stats(const ilg_ctx *ctx, ilg_stats *out);
+ILG_API int ilg_build(ilg_ctx *ctx);
+ILG_API int ilg_get_stats(const ilg_ctx *ctx, ilg_stats *out);
 
 /* Persistent scenes (this project's format; the reference's counterpart is
  * its memory-mapped PersistentMesh, Core/Shape/PersistentMesh.h:22-35): the
@@ -86,14 +93,14 @@ int ilg_get_stats(const ilg_ctx *ctx, ilg_stats *out);
  * file. ilg_load leaves the context as ilg_set_mesh + ilg_build would, with
  * the same records, without building; malformed or corrupted files are
  * ILG_EINVAL. */
-int ilg_save(ilg_ctx *ctx, const char *path);
-int ilg_load(ilg_ctx *ctx, const char *path);
+ILG_API int ilg_save(ilg_ctx *ctx, const char *path);
+ILG_API int ilg_load(ilg_ctx *ctx, const char *path);
 
 /* Closest hit. Rays: ray_o_tmin = N x (ox, oy, oz, tmin), ray_d_tmax =
  * N x (dx, dy, dz, tmax), both float4-aligned. Hits: prim[i] = triangle index
  * (-1 on a miss), t[i] (+inf on a miss), u[i] = beta, v[i] = gamma, in the
  * reference's Shirley arithmetic and rejection window. */
-int ilg_intersect(ilg_ctx *ctx, const float *ray_o_tmin, const float *ray_d_tmax, uint32_t n,
+ILG_API int ilg_intersect(ilg_ctx *ctx, const float *ray_o_tmin, const float *ray_d_tmax, uint32_t n,
                   int32_t *prim, float *t, float *u, float *v, uint32_t flags);
 
 /* ilg_intersect plus work counters: counts[0] = node records read,
@@ -101,7 +108,7 @@ int ilg_intersect(ilg_ctx *ctx, const float *ray_o_tmin, const float *ray_d_tmax
  * work behind the reference's tree statistics, TreeMeshStatistics,
  * Core/Shape/TreeMesh.cpp:11-29). Synchronous; used to state algorithmic
  * bytes per ray. */
-int ilg_intersect_counted(ilg_ctx *ctx, const float *ray_o_tmin, const float *ray_d_tmax, uint32_t n,
+ILG_API int ilg_intersect_counted(ilg_ctx *ctx, const float *ray_o_tmin, const float *ray_d_tmax, uint32_t n,
                           int32_t *prim, float *t, float *u, float *v, uint64_t counts[2], uint32_t flags);
 
 /* Closest hit from host buffers that allocates no device memory. This entry
@@ -118,11 +125,11 @@ int ilg_intersect_counted(ilg_ctx *ctx, const float *ray_o_tmin, const float *ra
  * only: its device error flags are kept in the array, not in the context.
  * Results equal ilg_intersect's. */
 #define ILG_NOALLOC_MAX_RAYS 262144u
-int ilg_intersect_noalloc(ilg_ctx *ctx, const float *ray_o_tmin, const float *ray_d_tmax, uint32_t n,
+ILG_API int ilg_intersect_noalloc(ilg_ctx *ctx, const float *ray_o_tmin, const float *ray_d_tmax, uint32_t n,
                           int32_t *prim, float *t, float *u, float *v);
 
 /* Any hit: occ[i] = 1 when some triangle is hit inside the ray's window. */
-int ilg_occluded(ilg_ctx *ctx, const float *ray_o_tmin, const float *ray_d_tmax, uint32_t n,
+ILG_API int ilg_occluded(ilg_ctx *ctx, const float *ray_o_tmin, const float *ray_d_tmax, uint32_t n,
                  uint8_t *occ, uint32_t flags);
 
 /* Closest hit / any hit that ignore the input triangles [skip_first,
@@ -132,10 +139,10 @@ int ilg_occluded(ilg_ctx *ctx, const float *ray_o_tmin, const float *ray_d_tmax,
  * BasicSpace.cpp:75-91,104-115), once a primitive's triangles occupy one
  * contiguous range of the mesh given to ilg_set_mesh. Same arguments and
  * results as ilg_intersect / ilg_occluded otherwise. */
-int ilg_intersect_excluding(ilg_ctx *ctx, const float *ray_o_tmin, const float *ray_d_tmax, uint32_t n,
+ILG_API int ilg_intersect_excluding(ilg_ctx *ctx, const float *ray_o_tmin, const float *ray_d_tmax, uint32_t n,
                             uint32_t skip_first, uint32_t skip_count, int32_t *prim, float *t, float *u,
                             float *v, uint32_t flags);
-int ilg_occluded_excluding(ilg_ctx *ctx, const float *ray_o_tmin, const float *ray_d_tmax, uint32_t n,
+ILG_API int ilg_occluded_excluding(ilg_ctx *ctx, const float *ray_o_tmin, const float *ray_d_tmax, uint32_t n,
                            uint32_t skip_first, uint32_t skip_count, uint8_t *occ, uint32_t flags);
 
 /* ------------------------------------------------------------------------
@@ -237,18 +244,18 @@ typedef struct ilg_render_opts {
 } ilg_render_opts;
 
 /* Materials indexed by the mat_ids given to ilg_set_mesh. */
-int ilg_set_materials(ilg_ctx *ctx, const ilg_material *mats, uint32_t n);
-int ilg_set_quad_lights(ilg_ctx *ctx, const ilg_quad_light *lights, uint32_t n);
+ILG_API int ilg_set_materials(ilg_ctx *ctx, const ilg_material *mats, uint32_t n);
+ILG_API int ilg_set_quad_lights(ilg_ctx *ctx, const ilg_quad_light *lights, uint32_t n);
 /* At most 8 lights of any kinds (replaces the lights set before); the
  * scene's LightList (Core/Scene/Scene.h) in the order the reference samples it. */
-int ilg_set_lights(ilg_ctx *ctx, const ilg_light *lights, uint32_t n);
+ILG_API int ilg_set_lights(ilg_ctx *ctx, const ilg_light *lights, uint32_t n);
 
 /* Renders width x height pixels at spp samples each into out_rgb
  * (height x width x 3 floats, row y = image-plane 'up' coordinate y, as the
  * reference's RenderRegion indexes its buffer). Host pointer unless
  * ILG_DEVICE_PTRS. Needs ilg_build, ilg_set_mesh with mat_ids, and
  * ilg_set_materials. */
-int ilg_render(ilg_ctx *ctx, const ilg_camera *cam, const ilg_render_opts *opts, float *out_rgb,
+ILG_API int ilg_render(ilg_ctx *ctx, const ilg_camera *cam, const ilg_render_opts *opts, float *out_rgb,
                uint32_t flags);
 
 /* ilg_render flag: count the traversal work of the render (slower kernels)
@@ -265,7 +272,7 @@ int ilg_render(ilg_ctx *ctx, const ilg_camera *cam, const ilg_render_opts *opts,
  * Plain renders only (no cache options, ILG_RENDER_COUNT, or Direct /
  * Albedo outputs). */
 #define ILG_RENDER_PERSISTENT 0x20u
-int ilg_render_counts(ilg_ctx *ctx, uint64_t counts[6]);
+ILG_API int ilg_render_counts(ilg_ctx *ctx, uint64_t counts[6]);
 
 /* ilg_render / ilg_render_region flag: with cache_depth set, a hash-grid
  * radiance cache answers the cache queries instead of the network: a cell
@@ -278,7 +285,7 @@ int ilg_render_counts(ilg_ctx *ctx, uint64_t counts[6]);
  * one query at a time). train_steps / train_batch / train_epochs do not
  * apply; call ilg_hash_cache_reset first. */
 #define ILG_RENDER_HASH_CACHE 0x8u
-int ilg_hash_cache_reset(ilg_ctx *ctx);
+ILG_API int ilg_hash_cache_reset(ilg_ctx *ctx);
 
 /* Training records of the last cached render (ILG_RENDER_* with
  * cache_depth): *records = records its training paths produced; *dropped =
@@ -286,7 +293,7 @@ int ilg_hash_cache_reset(ilg_ctx *ctx);
  * probe window held other keys (0 unless the render used
  * ILG_RENDER_HASH_CACHE). Synchronises the context's stream. This project's
  * own statistics; no counterpart in the reference. */
-int ilg_last_train_stats(ilg_ctx *ctx, uint32_t *records, uint32_t *dropped);
+ILG_API int ilg_last_train_stats(ilg_ctx *ctx, uint32_t *records, uint32_t *dropped);
 
 /* A camera as the reference's ICamera holds it after construction
  * (Core/Camera/Camera.h:23-28: m_centre, m_corner, m_across, m_up): the ray
@@ -301,7 +308,7 @@ typedef struct ilg_camera_frame {
 
 /* The frame PerspectiveCamera(eye, normalize(target - eye), up, -1, 1, -1, 1, 1)
  * + SetFieldOfView(fov_deg, aspect) builds (Core/Camera/Camera.cpp:30-44). */
-int ilg_camera_frame_of(const ilg_camera *cam, ilg_camera_frame *out);
+ILG_API int ilg_camera_frame_of(const ilg_camera *cam, ilg_camera_frame *out);
 
 /* Pixels [x, x + width) x [y, y + height) of the opts->width x opts->height image. */
 typedef struct ilg_region {
@@ -321,7 +328,7 @@ typedef struct ilg_region {
  * cache, its training paths train it after the call (with train_steps 0 a
  * frozen cache, and regions still tile the image exactly); Direct and Albedo
  * come from the first vertex, before any cache query. */
-int ilg_render_region(ilg_ctx *ctx, const ilg_camera_frame *frame, const ilg_render_opts *opts,
+ILG_API int ilg_render_region(ilg_ctx *ctx, const ilg_camera_frame *frame, const ilg_render_opts *opts,
                       const ilg_region *region, float *final_rgb, float *direct_rgb, float *albedo_rgb,
                       uint32_t flags);
 
@@ -337,7 +344,7 @@ int ilg_render_region(ilg_ctx *ctx, const ilg_camera_frame *frame, const ilg_ren
  * options mean what they mean for ilg_render. Host pointers unless
  * ILG_DEVICE_PTRS (then the ray and output arrays are device pointers and
  * the call only enqueues). */
-int ilg_radiance(ilg_ctx *ctx, const float *ray_o_tmin, const float *ray_d_tmax, uint32_t n,
+ILG_API int ilg_radiance(ilg_ctx *ctx, const float *ray_o_tmin, const float *ray_d_tmax, uint32_t n,
                  const ilg_render_opts *opts, float *final_rgb, float *direct_rgb, float *albedo_rgb,
                  uint32_t flags);
 
@@ -357,7 +364,7 @@ int ilg_radiance(ilg_ctx *ctx, const float *ray_o_tmin, const float *ray_d_tmax,
 #define ILG_MLP_PARAMS 23040u /* FP32 weights, per layer row-major [in][out] */
 #define ILG_MLP_GRID_PARAMS 1048576u /* FP32 grid features [level][entry][feature] */
 
-int ilg_mlp_init(ilg_ctx *ctx, uint32_t seed, float learning_rate);
+ILG_API int ilg_mlp_init(ilg_ctx *ctx, uint32_t seed, float learning_rate);
 /* ilg_mlp_init with a choice of input encoding: ILG_MLP_ENC_HASHGRID (the
  * encoding above, ilg_mlp_init's) or ILG_MLP_ENC_FREQ12: 12 sine/cosine
  * frequency bands per position axis (sin and cos of 2^b pi x, b < 12) next
@@ -365,27 +372,27 @@ int ilg_mlp_init(ilg_ctx *ctx, uint32_t seed, float learning_rate);
  * constant 1 (84 of the 96 input columns; no grid is read or trained). */
 #define ILG_MLP_ENC_HASHGRID 0u
 #define ILG_MLP_ENC_FREQ12 1u
-int ilg_mlp_init_encoding(ilg_ctx *ctx, uint32_t seed, float learning_rate, uint32_t encoding);
-int ilg_mlp_get_params(ilg_ctx *ctx, float *params /* ILG_MLP_PARAMS */);
-int ilg_mlp_set_params(ilg_ctx *ctx, const float *params);
-int ilg_mlp_get_grid(ilg_ctx *ctx, float *grid /* ILG_MLP_GRID_PARAMS */);
-int ilg_mlp_set_grid(ilg_ctx *ctx, const float *grid);
+ILG_API int ilg_mlp_init_encoding(ilg_ctx *ctx, uint32_t seed, float learning_rate, uint32_t encoding);
+ILG_API int ilg_mlp_get_params(ilg_ctx *ctx, float *params /* ILG_MLP_PARAMS */);
+ILG_API int ilg_mlp_set_params(ilg_ctx *ctx, const float *params);
+ILG_API int ilg_mlp_get_grid(ilg_ctx *ctx, float *grid /* ILG_MLP_GRID_PARAMS */);
+ILG_API int ilg_mlp_set_grid(ilg_ctx *ctx, const float *grid);
 /* The grid part of the gradient the last ilg_mlp_grads computed. */
-int ilg_mlp_get_grid_grads(ilg_ctx *ctx, float *grad /* ILG_MLP_GRID_PARAMS */);
+ILG_API int ilg_mlp_get_grid_grads(ilg_ctx *ctx, float *grad /* ILG_MLP_GRID_PARAMS */);
 /* out: n x 3 radiance. Host pointers unless ILG_DEVICE_PTRS (device query
  * rows must start 16-byte aligned). Runs on the
  * tcgen05 tensor cores (accumulators in TMEM); ILG_MLP_WARP_MMA selects the
  * warp-level mma.sync kernel that training's forward pass uses instead. */
 #define ILG_MLP_WARP_MMA 0x10u
-int ilg_mlp_infer(ilg_ctx *ctx, const float *raw, uint32_t n, float *out, uint32_t flags);
+ILG_API int ilg_mlp_infer(ilg_ctx *ctx, const float *raw, uint32_t n, float *out, uint32_t flags);
 /* Gradient of the mean relative L2 loss over the batch (no update). Runs on
  * the tcgen05 tensor cores (forward, loss and backward in one kernel, the
  * weight gradients in another, accumulators in TMEM; device rows 16-byte
  * aligned); with ILG_MLP_WARP_MMA on the warp-level mma.sync kernels. */
-int ilg_mlp_grads(ilg_ctx *ctx, const float *raw, const float *target, uint32_t n, float *grad /* ILG_MLP_PARAMS */,
+ILG_API int ilg_mlp_grads(ilg_ctx *ctx, const float *raw, const float *target, uint32_t n, float *grad /* ILG_MLP_PARAMS */,
                   float *loss, uint32_t flags);
 /* One Adam step on the batch; *loss (optional) receives the loss before the step. */
-int ilg_mlp_train_step(ilg_ctx *ctx, const float *raw, const float *target, uint32_t n, float *loss, uint32_t flags);
+ILG_API int ilg_mlp_train_step(ilg_ctx *ctx, const float *raw, const float *target, uint32_t n, float *loss, uint32_t flags);
 
 /* Many independent scenes rendered together: one wavefront over the paths of
  * every item (a scene context with its built mesh, materials and lights, a
@@ -406,7 +413,7 @@ typedef struct ilg_batch_item {
     float *out_rgb; /* height x width x 3 */
 } ilg_batch_item;
 
-int ilg_render_batch(ilg_ctx *runner, const ilg_batch_item *items, uint32_t n, uint32_t paths_per_wave,
+ILG_API int ilg_render_batch(ilg_ctx *runner, const ilg_batch_item *items, uint32_t n, uint32_t paths_per_wave,
                      uint32_t block, uint32_t flags);
 
 /* ------------------------------------------------------------------------
@@ -419,8 +426,8 @@ int ilg_render_batch(ilg_ctx *runner, const ilg_batch_item *items, uint32_t n, u
  * = sum * (1 / frames so far), bit for bit the reference's arithmetic. A new
  * image size, or ilg_accumulate_reset (AccumulationBuffer::Reset), starts
  * over. */
-int ilg_accumulate(ilg_ctx *ctx, const float *frame_rgb, uint32_t n_pixels, float *out_rgb, uint32_t flags);
-int ilg_accumulate_reset(ilg_ctx *ctx);
+ILG_API int ilg_accumulate(ilg_ctx *ctx, const float *frame_rgb, uint32_t n_pixels, float *out_rgb, uint32_t flags);
+ILG_API int ilg_accumulate_reset(ilg_ctx *ctx);
 
 #define ILG_TONE_GLOBAL 0u /* GlobalTone (Core/Postproc/GlobalTone.h): c / (c + 1) */
 #define ILG_TONE_AUTO 1u   /* AutoTone (AutoTone.h): (c - min) / (max - min), clamped to [0, 1] */
@@ -428,7 +435,7 @@ int ilg_accumulate_reset(ilg_ctx *ctx);
 /* Tone mapping of a whole image. GLOBAL and AUTO are bit for bit the
  * reference's; DRAGO evaluates its logarithms and power in double as the
  * reference does and agrees to within float rounding. */
-int ilg_tonemap(ilg_ctx *ctx, const float *in_rgb, uint32_t n_pixels, float *out_rgb, uint32_t op, uint32_t flags);
+ILG_API int ilg_tonemap(ilg_ctx *ctx, const float *in_rgb, uint32_t n_pixels, float *out_rgb, uint32_t op, uint32_t flags);
 
 /* Device probe (this project's measurement tool; no counterpart in the
  * reference): *gbs = bytes read per second by a streaming read kernel that
@@ -436,14 +443,14 @@ int ilg_tonemap(ilg_ctx *ctx, const float *in_rgb, uint32_t n_pixels, float *out
  * with L2-only loads. A buffer below the device's L2 size gives the L2 read
  * bandwidth, the roofline denominator of traversal over scenes that fit in
  * L2. Allocates and frees its buffer; synchronous. */
-int ilg_probe_read_gbs(ilg_ctx *ctx, uint64_t bytes, uint32_t reps, float *gbs);
+ILG_API int ilg_probe_read_gbs(ilg_ctx *ctx, uint64_t bytes, uint32_t reps, float *gbs);
 
 /* Blocks until the context's stream is idle (for ILG_DEVICE_PTRS callers). */
-int ilg_sync(ilg_ctx *ctx);
+ILG_API int ilg_sync(ilg_ctx *ctx);
 
 /* The context's CUDA stream (a cudaStream_t), for callers that time or order
  * their own work against it. */
-void *ilg_stream(ilg_ctx *ctx);
+ILG_API void *ilg_stream(ilg_ctx *ctx);
 
 #ifdef __cplusplus
 }

@@ -13,7 +13,7 @@ def declared_symbols():
     for h in os.listdir(os.path.join(ROOT, "include")):
         if h.endswith(".h"):
             src = open(os.path.join(ROOT, "include", h)).read()
-            names |= set(re.findall(r"^\s*(?:const\s+)?(?:int|void|const char|char)\s*\*?\s*(ilg_\w+)\s*\(", src, re.M))
+            names |= set(re.findall(r"^\s*(?:ILG_API\s+)?(?:const\s+)?(?:int|void|const char|char)\s*\*?\s*(ilg_\w+)\s*\(", src, re.M))
     return sorted(names)
 
 
@@ -28,6 +28,19 @@ def test_library_exports_every_declared_symbol():
     lib = ctypes.CDLL(build.build())
     missing = [s for s in declared_symbols() if not hasattr(lib, s)]
     assert missing == []
+
+
+def test_library_exports_only_the_entry_points():
+    import shutil
+    import subprocess
+    from illuminaprt_b200 import build
+    if shutil.which("nm") is None:
+        pytest.skip("no nm")
+    out = subprocess.run(["nm", "-D", "--defined-only", build.build()], capture_output=True, text=True,
+                         check=True).stdout
+    code = [ln.split()[-1] for ln in out.splitlines() if len(ln.split()) == 3 and ln.split()[1] == "T"]
+    assert code and all(name.startswith("ilg_") for name in code), [n for n in code if not n.startswith("ilg_")][:5]
+    assert sorted(code) == sorted(declared_symbols())
 
 
 def test_binding_lists_every_symbol():
