@@ -808,19 +808,37 @@ def main():
     e2e_page_value = replicas.aggregate_rate(rays_per_step * e2e_steps, world, e2e_page_ms / 1e3) / 1e6
     assert torch.equal(hpage["incoherent"][0], out["incoherent"][0].cpu())
     del page, hpage
-    # the copy bound of e2e: the same host->device bytes as one plain pinned copy
+    # the copy bound of e2e: a step's host->device bytes (rays) and
+    # device->host bytes (hits) as plain pinned copies, each alone and both at
+    # once on two streams (the link is full duplex; e2e overlaps the two)
     h2d_src = torch.cat([pin["coherent"][0], pin["coherent"][1], pin["incoherent"][0],
                          pin["incoherent"][1]]).pin_memory()
     h2d_dst = torch.empty_like(h2d_src, device=dev)
-    h2d_dst.copy_(h2d_src, non_blocking=True)
-    c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    c0.record()
-    for _ in range(3):
-        h2d_dst.copy_(h2d_src, non_blocking=True)
-    c1.record()
-    c1.synchronize()
-    h2d_gbs = 3 * h2d_src.numel() * h2d_src.element_size() / (c0.elapsed_time(c1) / 1e3) / 1e9
-    del h2d_src, h2d_dst
+    d2h_src = torch.empty(rays_per_step * HIT_OUT // 4, dtype=torch.float32, device=dev)
+    d2h_dst = torch.empty(d2h_src.shape, dtype=torch.float32, pin_memory=True)
+    up, down = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
+
+    def copies(h2d=True, d2h=True, reps=3):
+        ev = []
+        torch.cuda.synchronize(dev)
+        for st_, on, (dst, src) in ((up, h2d, (h2d_dst, h2d_src)), (down, d2h, (d2h_dst, d2h_src))):
+            if not on:
+                continue
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(st_):
+                dst.copy_(src, non_blocking=True)  # untimed first copy
+                a.record(st_)
+                for _ in range(reps):
+                    dst.copy_(src, non_blocking=True)
+                b.record(st_)
+            ev.append((a, b))
+        torch.cuda.synchronize(dev)
+        return max(a.elapsed_time(b) for a, b in ev) / reps  # ms per step's bytes
+
+    h2d_ms, d2h_ms, duplex_ms = copies(d2h=False), copies(h2d=False), copies()
+    h2d_gbs = h2d_src.numel() * h2d_src.element_size() / (h2d_ms / 1e3) / 1e9
+    d2h_gbs = d2h_src.numel() * d2h_src.element_size() / (d2h_ms / 1e3) / 1e9
+    del h2d_src, h2d_dst, d2h_src, d2h_dst
 
     # the memory level that holds the traversal's working set: L2 when the
     # scene's node and triangle records fit in it, measured here by the
@@ -865,7 +883,9 @@ def main():
             "e2e": {"value": round(e2e_value, 3), "unit": UNIT, "h2d_bytes_per_step": rays_per_step * RAY_IN,
                     "d2h_bytes_per_step": rays_per_step * HIT_OUT,
                     "pinned_h2d_gbs": round(h2d_gbs, 2),
-                    "copy_bound_mrays_s": round(h2d_gbs * 1e3 / RAY_IN, 3),
+                    "pinned_d2h_gbs": round(d2h_gbs, 2),
+                    "copy_bound_mrays_s": round(rays_per_step / (duplex_ms / 1e3) / 1e6, 3),
+                    "copy_bound": "a step's ray bytes up and hit bytes down as two plain pinned copies at once",
                     "e2e_pageable_mrays_s": round(e2e_page_value, 3),
                     "pipeline": "host-buffer calls run in chunks over three streams: upload, traversal and "
                                 "download of neighbouring chunks overlap"},

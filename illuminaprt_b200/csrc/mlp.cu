@@ -422,47 +422,52 @@ __global__ void k_grid_init(MlpDev M, uint32_t seed)
 // Gradient of the loss with respect to the grid features: per row, dX of the
 // 32 grid columns = dZ0 W0^T (W0 as the forward used it, in BF16), then
 // scattered to the eight corners of every level with the trilinear weights.
-constexpr int kGridBwdThreads = 128;
+constexpr int kGridBwdThreads = 256;
 
+// One thread per (row, level), as k_grid_encode: the sixteen levels of a row
+// run in parallel (a batch of 16,384 rows is 262,144 threads, where one
+// thread per row left the SMs a few warps each). The row's dZ0 loads are
+// shared by the 16 lanes of a half-warp (one address per load); W0's rows are
+// padded to 65 floats so that the 16 levels of a half-warp read 16 banks.
 __global__ void __launch_bounds__(kGridBwdThreads) k_grid_bwd(MlpDev M, const float *__restrict__ raw, uint32_t n)
 {
-    __shared__ float w0[2 * kGridLevels][kMlpHid];
+    __shared__ float w0[2 * kGridLevels][kMlpHid + 1];
     for (int i = threadIdx.x; i < 2 * kGridLevels * kMlpHid; i += blockDim.x)
         w0[i / kMlpHid][i % kMlpHid] = __bfloat162float(__float2bfloat16_rn(M.w[mlp_off(0) + i]));
     __syncthreads();
-    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t r = (uint32_t)(i / kGridLevels), l = (uint32_t)(i % kGridLevels);
     if (r >= n) return;
-    float dz[kMlpHid];
-#pragma unroll
-    for (int j = 0; j < kMlpHid; j++) dz[j] = __bfloat162float(M.dzcm[(size_t)j * M.cap + r]);
-    const float x = raw[(size_t)r * kMlpRaw], y = raw[(size_t)r * kMlpRaw + 1], z = raw[(size_t)r * kMlpRaw + 2];
-    float2 *gg = reinterpret_cast<float2 *>(M.grid_grad);
-#pragma unroll 1
-    for (int l = 0; l < kGridLevels; l++) {
-        float d0 = 0.f, d1 = 0.f;
-#pragma unroll
-        for (int j = 0; j < kMlpHid; j++) {
-            d0 = fmaf(dz[j], w0[2 * l][j], d0);
-            d1 = fmaf(dz[j], w0[2 * l + 1][j], d1);
-        }
-        if (d0 == 0.f && d1 == 0.f) continue;
-        const uint32_t res = M.grid_res[l];
-        uint32_t ix, iy, iz;
-        float fx, fy, fz;
-        grid_cell(x, res, ix, fx);
-        grid_cell(y, res, iy, fy);
-        grid_cell(z, res, iz, fz);
-#pragma unroll
-        for (int c = 0; c < 8; c++) {
-            const float wx = (c & 1) ? fx : __fsub_rn(1.f, fx);
-            const float wy = (c & 2) ? fy : __fsub_rn(1.f, fy);
-            const float wz = (c & 4) ? fz : __fsub_rn(1.f, fz);
-            const float w = __fmul_rn(__fmul_rn(wx, wy), wz);
-            float2 *e = gg + (size_t)l * kGridSize + grid_index(res, ix + (c & 1), iy + ((c >> 1) & 1), iz + (c >> 2));
-            atomicAdd(&e->x, w * d0);
-            atomicAdd(&e->y, w * d1);
-        }
+    float d0 = 0.f, d1 = 0.f;
+#pragma unroll 16
+    for (int j = 0; j < kMlpHid; j++) {
+        const float dz = __bfloat162float(M.dzcm[(size_t)j * M.cap + r]);
+        d0 = fmaf(dz, w0[2 * l][j], d0);
+        d1 = fmaf(dz, w0[2 * l + 1][j], d1);
     }
+    if (d0 == 0.f && d1 == 0.f) return;
+    const float x = raw[(size_t)r * kMlpRaw], y = raw[(size_t)r * kMlpRaw + 1], z = raw[(size_t)r * kMlpRaw + 2];
+    const uint32_t res = M.grid_res[l];
+    uint32_t ix, iy, iz;
+    float fx, fy, fz;
+    grid_cell(x, res, ix, fx);
+    grid_cell(y, res, iy, fy);
+    grid_cell(z, res, iz, fz);
+    float2 *gg = reinterpret_cast<float2 *>(M.grid_grad) + (size_t)l * kGridSize;
+#pragma unroll
+    for (int c = 0; c < 8; c++) {
+        const float wx = (c & 1) ? fx : __fsub_rn(1.f, fx);
+        const float wy = (c & 2) ? fy : __fsub_rn(1.f, fy);
+        const float wz = (c & 4) ? fz : __fsub_rn(1.f, fz);
+        const float w = __fmul_rn(__fmul_rn(wx, wy), wz);
+        // both features of the corner in one vector atomic (sm_90 and later)
+        atomicAdd(gg + grid_index(res, ix + (c & 1), iy + ((c >> 1) & 1), iz + (c >> 2)), make_float2(w * d0, w * d1));
+    }
+}
+
+inline unsigned grid_bwd_blocks(uint32_t n)
+{
+    return (unsigned)(((uint64_t)n * kGridLevels + kGridBwdThreads - 1) / kGridBwdThreads);
 }
 
 __global__ void k_grid_adam(MlpDev M, float lr, float bc1, float bc2)
@@ -543,7 +548,8 @@ cudaError_t mlp_grads(const MlpDev &M, const float *raw, const float *target, ui
         if (has_grid && (e = cudaMemsetAsync(M.grid_grad, 0, kGridParams * sizeof(float), st)) != cudaSuccess)
             return e;
         if ((e = mlp_train_tc(M, raw, target, n, st)) != cudaSuccess) return e;
-        if (has_grid) k_grid_bwd<<<(n + kGridBwdThreads - 1) / kGridBwdThreads, kGridBwdThreads, 0, st>>>(M, raw, n);
+        if (has_grid)
+            k_grid_bwd<<<grid_bwd_blocks(n), kGridBwdThreads, 0, st>>>(M, raw, n);
         if ((e = mlp_dw_tc(M, n_pad, st)) != cudaSuccess) return e;
         return cudaGetLastError();
     }
@@ -560,7 +566,7 @@ cudaError_t mlp_grads(const MlpDev &M, const float *raw, const float *target, ui
     const uint32_t grid = grid_for(n, num_sms());
     k_mlp_fwd<true><<<grid, 128, smem_f, st>>>(M, raw, n, nullptr, nullptr);
     k_mlp_bwd<<<grid, 128, smem_b, st>>>(M, raw, target, n);
-    if (has_grid) k_grid_bwd<<<(n + kGridBwdThreads - 1) / kGridBwdThreads, kGridBwdThreads, 0, st>>>(M, raw, n);
+    if (has_grid) k_grid_bwd<<<grid_bwd_blocks(n), kGridBwdThreads, 0, st>>>(M, raw, n);
     const uint32_t chunks = (n_pad + kDwChunk - 1) / kDwChunk;
     for (int l = 0; l < kMlpLayers; l++) {
         const __nv_bfloat16 *A = l == 0 ? M.xcm : M.hcm + (size_t)(l - 1) * kMlpHid * M.cap;
