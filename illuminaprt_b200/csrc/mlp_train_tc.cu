@@ -16,7 +16,7 @@
 // weight gradients.
 //
 // k_mlp_dw_tc: dW_l = H_{l-1}^T dZ_l for every layer l, split over the
-// batch: a CTA owns 1024 rows of one layer and accumulates, 64 rows at a
+// batch: a CTA owns 512 rows of one layer and accumulates, 64 rows at a
 // time, M = 128 features (the layer's 96 or 64, the rest zero) x N = 64 (16
 // for the output layer) in TMEM, both operands loaded from the column-major
 // activations, which are K-major for this product; the partial sums are
@@ -249,7 +249,9 @@ __global__ void __launch_bounds__(kTrRows, 1) k_mlp_train_tc(const MlpDev M, con
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTrTmemCols) : "memory");
 }
 
-constexpr uint32_t kDwTcRowsPerCta = 1024;  // the batch rows (K) one CTA sums over
+// the batch rows (K) one CTA sums; measured on a B200 (16,384-row step):
+// 1024 rows 12 % slower, 256 rows 2 % slower
+constexpr uint32_t kDwTcRowsPerCta = 512;
 constexpr int kDwTcK = 64;                  // rows per MMA group
 
 __global__ void __launch_bounds__(128) k_mlp_dw_tc(const MlpDev M, uint32_t n_pad)
