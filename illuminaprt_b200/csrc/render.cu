@@ -753,6 +753,66 @@ __device__ __forceinline__ void wave_trace_dyn(const RenderDev &R, uint32_t n, u
     }
 }
 
+// The shadow rays of depth d and the extension rays of depth d + 1 in one
+// persistent launch: both come from k_shade at depth d and neither reads
+// what the other writes (shadow rays add to the pixel sums and training
+// targets, extension rays write hit records), so one traversal loop
+// (ray_step<kMixed>) takes the extension rays first, then the shadow rays:
+// twice the rays in flight and one launch tail instead of two. `cur` is the
+// queue the extension rays are in.
+__global__ void __launch_bounds__(kStackColumns) k_trace_mixed(RenderDev R, int cur, uint32_t *next)
+{
+    const uint32_t lane = threadIdx.x & 31u;
+    __shared__ uint2 sstack[kShortStack * kStackColumns];  // launched with kStackColumns threads a block
+    uint2 lstack[kMaxStack - kShortStack];
+    const SplitStack stack{sstack + threadIdx.x, lstack};
+    const uint32_t n_ext = min(R.count[cur], R.capacity), n_sh = min(*R.sh_count, R.sh_capacity);
+    const uint32_t n = n_ext + n_sh;
+    RayState r;
+    const Node8 *nodes = nullptr;
+    const Tri *tris = nullptr;
+    uint32_t n_nodes = 0, n_tris = 0;
+    bool active = false, exhausted = false;  // exhausted is warp-uniform
+    uint32_t id = 0;
+    while (true) {
+        const uint32_t idle = __ballot_sync(0xffffffffu, !active);
+        if (!exhausted && (__popc(idle) >= kRefillLanes || idle == 0xffffffffu)) {
+            const uint32_t leader = __ffs(idle) - 1u;
+            uint32_t base = 0;
+            if (lane == leader) base = atomicAdd(next, (uint32_t)__popc(idle));
+            base = __shfl_sync(0xffffffffu, base, leader);
+            if (base >= n) exhausted = true;
+            if (!active) {
+                const uint32_t k = base + __popc(idle & ((1u << lane) - 1u));
+                if (k < n) {
+                    const bool shadow = k >= n_ext;
+                    id = shadow ? k - n_ext : k;
+                    const SceneRec &S = R.scenes[shadow ? R.s_sid[id] : R.path_scene[R.q_path[cur][id]]];
+                    nodes = S.nodes;
+                    tris = S.tris;
+                    n_nodes = S.n_nodes;
+                    n_tris = S.n_tris;
+                    if (shadow) ray_init(r, R.s_o[id], R.s_d[id], n_nodes);
+                    else ray_init(r, R.q_o[cur][id], R.q_d[cur][id], n_nodes);
+                    r.any = shadow;
+                    active = true;
+                }
+            }
+        }
+        if (__ballot_sync(0xffffffffu, active) == 0u) break;
+        if (active && ray_step<false, false, false, false, kTrisPerStep, true, SplitStack>(r, stack, nodes, tris,
+                                                                                             n_nodes, n_tris, R.err)) {
+            if (r.any) {
+                if (r.best == -1) shadow_unoccluded(R, id);
+            } else {
+                R.hit_tri[id] = r.best;
+                R.hit_t[id] = r.best >= 0 ? r.tcur : __int_as_float(0x7f800000);
+            }
+            active = false;
+        }
+    }
+}
+
 __global__ void __launch_bounds__(kStackColumns) k_extend_dyn(RenderDev R, int cur, uint32_t *next)
 {
     wave_trace_dyn<false>(R, min(R.count[cur], R.capacity), next, cur);
@@ -1159,19 +1219,27 @@ cudaError_t render_wave(const RenderDev &R, uint32_t n_paths, uint64_t wave_begi
     // with short training tails every path has stopped by the tail vertex
     const uint32_t tail = R.cache_depth + R.train_tail;
     const uint32_t last = (R.cache_depth && R.train_tail && cache) ? std::min(R.depth_max, tail) : R.depth_max;
+    // persistent traversal: the shadow rays of depth d and the extension rays
+    // of depth d + 1 go in one launch (k_trace_mixed)
+    const bool merge = R.persistent && !R.stats;
+    bool traced = false;  // this depth's extension rays were traced with the previous depth's shadow rays
     for (uint32_t depth = 0; depth <= last; depth++) {
-        if ((e = cudaMemsetAsync(R.count + (cur ^ 1), 0, sizeof(uint32_t), st)) != cudaSuccess) return e;
-        if ((e = cudaMemsetAsync(R.sh_count, 0, sizeof(uint32_t), st)) != cudaSuccess) return e;
-        if (R.stats) {
-            k_extend<true><<<blocks_for(n_paths, T), T, 0, st>>>(R, cur);
-        } else if (!R.persistent) {
-            k_extend<false><<<blocks_for(n_paths, T), T, 0, st>>>(R, cur);
-        } else {
-            if ((e = cudaMemsetAsync(R.count + 6, 0, sizeof(uint32_t), st)) != cudaSuccess) return e;
-            k_extend_dyn<<<persistent_blocks(n_paths), kStackColumns, 0, st>>>(R, cur, R.count + 6);
+        if (!traced) {
+            if ((e = cudaMemsetAsync(R.count + (cur ^ 1), 0, sizeof(uint32_t), st)) != cudaSuccess) return e;
+            if ((e = cudaMemsetAsync(R.sh_count, 0, sizeof(uint32_t), st)) != cudaSuccess) return e;
+            if (R.stats) {
+                k_extend<true><<<blocks_for(n_paths, T), T, 0, st>>>(R, cur);
+            } else if (!R.persistent) {
+                k_extend<false><<<blocks_for(n_paths, T), T, 0, st>>>(R, cur);
+            } else {
+                if ((e = cudaMemsetAsync(R.count + 6, 0, sizeof(uint32_t), st)) != cudaSuccess) return e;
+                k_extend_dyn<<<persistent_blocks(n_paths), kStackColumns, 0, st>>>(R, cur, R.count + 6);
+            }
+            n_launch++;
         }
+        traced = false;
         k_shade<<<blocks_for(n_paths, T), T, 0, st>>>(R, cur, depth, wave_begin);
-        n_launch += 2;
+        n_launch++;
         if (R.cache_depth && cache && (depth == R.cache_depth || (R.train_tail && depth == tail))) {
             if (R.hc_keys)
                 k_hc_query<<<blocks_for(n_paths, 256), 256, 0, st>>>(R, R.capacity);
@@ -1181,7 +1249,16 @@ cudaError_t render_wave(const RenderDev &R, uint32_t n_paths, uint64_t wave_begi
             if ((e = cudaMemsetAsync(R.qry_count, 0, sizeof(uint32_t), st)) != cudaSuccess) return e;
             n_launch += 2;
         }
-        if (depth < last) {
+        if (depth < last && merge) {
+            if ((e = cudaMemsetAsync(R.count + 6, 0, sizeof(uint32_t), st)) != cudaSuccess) return e;
+            k_trace_mixed<<<persistent_blocks((uint64_t)n_paths + R.sh_capacity), kStackColumns, 0, st>>>(
+                R, cur ^ 1, R.count + 6);
+            // the queues the next k_shade appends to, now that they are consumed
+            if ((e = cudaMemsetAsync(R.count + cur, 0, sizeof(uint32_t), st)) != cudaSuccess) return e;
+            if ((e = cudaMemsetAsync(R.sh_count, 0, sizeof(uint32_t), st)) != cudaSuccess) return e;
+            n_launch++;
+            traced = true;
+        } else if (depth < last) {
             if (R.stats) {
                 k_shadow<true><<<blocks_for((uint64_t)R.sh_capacity, T), T, 0, st>>>(R);
             } else if (!R.persistent) {
