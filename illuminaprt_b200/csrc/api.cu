@@ -222,8 +222,14 @@ int query_host(ilg_ctx *ctx, const float *o4, const float *d4, uint32_t n, int32
         CK(ctx->hu.reserve(n));
         CK(ctx->hv.reserve(n));
     }
-    const uint32_t kMinChunk = 1u << 18, kMaxChunks = 8u;
-    const uint32_t chunks = n >= 2u * kMinChunk ? std::min<uint32_t>(kMaxChunks, n / kMinChunk) : 1u;
+    // up to 8 chunks of >= 256 K rays, more for large batches so that no chunk
+    // exceeds about 512 K rays (measured on a B200: 8.4 M rays in one call ran
+    // 3 % slower in 8 chunks than as two calls of 4.2 M in 8 chunks each)
+    const uint32_t kMinChunk = 1u << 18, kTargetChunk = 1u << 19, kMaxChunks = 64u;
+    const uint32_t chunks =
+        n >= 2u * kMinChunk ? std::min<uint32_t>(kMaxChunks, std::max<uint32_t>(std::min<uint32_t>(8u, n / kMinChunk),
+                                                                                n / kTargetChunk))
+                            : 1u;
     const uint32_t chunk = ((n + chunks - 1) / chunks + 127u) & ~127u;
     cudaStream_t ss[3] = {ctx->stream, ctx->stream, ctx->stream};
     if (chunks > 1) {
