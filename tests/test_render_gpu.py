@@ -432,3 +432,20 @@ def test_counted_render_counts_the_traversal_work(box_space):
     sp.render(scene["camera"], W, H, 1, seed=1)
     with pytest.raises(IlgError):
         sp.render_counts()  # the last render was not counted
+
+
+def test_merged_traversal_renders_the_separate_launches_paths():
+    # a scene of >= 4096 triangles renders with the persistent traversal, the
+    # shadow rays of depth d and the extension rays of depth d + 1 in one
+    # launch (k_trace_mixed); a counted render traces the same paths with one
+    # launch per ray kind (k_extend / k_shadow), so the images agree up to the
+    # order of the float additions into each pixel
+    from illuminaprt_b200.ilg import GpuSpace
+    s = scenes.sphere_field(4, 3, seed=5, width=96, height=54)
+    sp = GpuSpace()
+    scenes.load_sphere_field(sp, s)
+    cam = dict(s["camera"], aspect=96 / 54)
+    merged = sp.render(cam, 96, 54, 16, max_depth=8, seed=12, sky=s["sky"])
+    separate = sp.render(cam, 96, 54, 16, max_depth=8, seed=12, sky=s["sky"], count=True)
+    assert np.isfinite(merged).all() and merged.mean() > 0
+    assert np.allclose(merged, separate, rtol=1e-4, atol=1e-5)
