@@ -57,7 +57,7 @@ def test_mirror_and_glass_match_reference():
     # reflection / transmission, no Fresnel weight) on the box's two inner
     # boxes, emission seen after specular bounces, transmitted rays offset
     # below the surface: the device image against the reference's 4096-spp
-    # render, judged against the noise between two reference renders
+    # render, compared with the noise between two reference renders
     from illuminaprt_b200.ilg import GpuSpace
     sp = GpuSpace()
     scene = scenes.load_box_scene(sp, scenes.box_scene(specular=True))
@@ -101,7 +101,7 @@ def test_mesh_and_infinite_lights_match_reference(prefix):
     # escaping camera rays and after specular bounces, light samples of
     # intensity * cos * BSDF not divided by their pdf) next to a quad light
     # in the specular box: device images and Direct against the reference's
-    # 4096-spp renders, judged against the noise between two reference renders
+    # 4096-spp renders, compared with the noise between two reference renders
     from illuminaprt_b200.ilg import GpuSpace
     sp = GpuSpace()
     scene = scenes.load_box_scene(sp, scenes.box_scene(**LIGHT_VARIANTS[prefix]))
