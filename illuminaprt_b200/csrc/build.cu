@@ -9,6 +9,8 @@
 //   4. k_karras       binary radix tree over the sorted codes (Karras 2012),
 //                     duplicate codes split by index
 //   5. k_refit        bottom-up AABBs, one atomic arrival counter per node
+//   5b. k_treelet     bottom-up treelet restructuring for least SAH cost
+//                     (Karras & Aila 2013); subtree triangle counts
 //   6. k_collapse     level by level: each work item turns one binary node
 //                     into one 8-wide node (greedy: open the widest child
 //                     with more than 3 triangles until 8 slots are used),
@@ -195,6 +197,168 @@ __global__ void k_refit(int n, const uint32_t *__restrict__ sorted_tri, const fl
     }
 }
 
+// ------------------------------------------------------------- step 5b ----
+// Treelet restructuring (Karras & Aila 2013, "Fast parallel construction of
+// high-quality bounding volume hierarchies"): a second bottom-up pass over
+// the binary tree. At each internal node p, once both of its subtrees are
+// final, the treelet of p (p and the internal nodes below it found by
+// repeatedly opening the treelet leaf of largest surface area, until
+// kTreeletLeaves leaves) is rebuilt with the topology of least SAH cost over
+// those leaves, found by dynamic programming over the leaves' subsets. The
+// treelet keeps its node indices and its root's box; only the topology
+// below the root changes. The pass also leaves every internal node's
+// triangle count in cnt (the collapse reads it).
+// SAH cost model: internal node kSahCi x its area, triangle kSahCt x its area.
+constexpr int kTreeletLeaves = 7;
+constexpr float kSahCi = 1.2f, kSahCt = 1.0f;
+
+__device__ __forceinline__ void handle_box(int c, const uint32_t *sorted_tri, const float4 *tlo, const float4 *thi,
+                                           const float4 *nlo, const float4 *nhi, float3 &lo, float3 &hi)
+{
+    float4 a, b;
+    if (c >= 0) { a = __ldcg(&nlo[c]); b = __ldcg(&nhi[c]); }
+    else { const uint32_t t = sorted_tri[~c]; a = tlo[t]; b = thi[t]; }
+    lo = make_float3(a.x, a.y, a.z);
+    hi = make_float3(b.x, b.y, b.z);
+}
+
+__global__ void __launch_bounds__(128) k_treelet(int n, const uint32_t *__restrict__ sorted_tri,
+                                                 const float4 *__restrict__ tlo, const float4 *__restrict__ thi,
+                                                 int2 *child, int *parent_int, int *parent_leaf,
+                                                 uint32_t *__restrict__ arrivals, float4 *nlo, float4 *nhi, int *cnt,
+                                                 float *cost, int restructure)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int p = parent_leaf[i];
+    for (int guard = 0; p >= 0 && p < n - 1 && guard < n; guard++) {
+        __threadfence();
+        if (atomicAdd(&arrivals[p], 1u) == 0) return;
+        __threadfence();
+        // both subtrees of p are final: its count and cost
+        const int2 c = __ldcg(&child[p]);
+        float3 plo, phi;
+        handle_box(p, sorted_tri, tlo, thi, nlo, nhi, plo, phi);
+        auto sub_cost = [&](int h) {
+            if (h >= 0) return __ldcg(&cost[h]);
+            float3 lo, hi;
+            handle_box(h, sorted_tri, tlo, thi, nlo, nhi, lo, hi);
+            return kSahCt * area(lo, hi);
+        };
+        auto sub_cnt = [&](int h) { return h >= 0 ? __ldcg(&cnt[h]) : 1; };
+        const int cp = sub_cnt(c.x) + sub_cnt(c.y);
+        const float costp = kSahCi * area(plo, phi) + sub_cost(c.x) + sub_cost(c.y);
+        __stcg(&cnt[p], cp);
+        __stcg(&cost[p], costp);
+        if (restructure && cp >= kTreeletLeaves) {
+            // form the treelet: open the internal leaf of largest area
+            int tl[kTreeletLeaves], tin[kTreeletLeaves - 1];
+            int n_l = 2, n_in = 1;
+            tl[0] = c.x;
+            tl[1] = c.y;
+            tin[0] = p;
+            float cur = kSahCi * area(plo, phi);  // the treelet's present cost: its internal areas + leaf costs
+            while (n_l < kTreeletLeaves) {
+                int best = -1;
+                float best_a = -1.f;
+                for (int k = 0; k < n_l; k++) {
+                    if (tl[k] < 0) continue;
+                    float3 lo, hi;
+                    handle_box(tl[k], sorted_tri, tlo, thi, nlo, nhi, lo, hi);
+                    const float a = area(lo, hi);
+                    if (a > best_a) { best_a = a; best = k; }
+                }
+                if (best < 0) break;
+                const int2 cc = __ldcg(&child[tl[best]]);
+                tin[n_in++] = tl[best];
+                cur += kSahCi * best_a;
+                tl[best] = cc.x;
+                tl[n_l++] = cc.y;
+            }
+            if (n_l == kTreeletLeaves) {
+                float3 llo[kTreeletLeaves], lhi[kTreeletLeaves];
+                float lc[kTreeletLeaves];
+                int ln[kTreeletLeaves];
+                for (int k = 0; k < kTreeletLeaves; k++) {
+                    handle_box(tl[k], sorted_tri, tlo, thi, nlo, nhi, llo[k], lhi[k]);
+                    lc[k] = sub_cost(tl[k]);
+                    ln[k] = sub_cnt(tl[k]);
+                    cur += lc[k];
+                }
+                // least cost of every subset of the leaves, and its best split
+                constexpr int kSubsets = 1 << kTreeletLeaves;
+                float copt[kSubsets];
+                uint8_t split[kSubsets];
+                for (int S = 1; S < kSubsets; S++) {
+                    if ((S & (S - 1)) == 0) {
+                        copt[S] = lc[__ffs(S) - 1];
+                        split[S] = 0;
+                        continue;
+                    }
+                    float3 lo = make_float3(FLT_MAX, FLT_MAX, FLT_MAX), hi = make_float3(-FLT_MAX, -FLT_MAX, -FLT_MAX);
+                    for (int k = 0; k < kTreeletLeaves; k++) {
+                        if (!(S & (1 << k))) continue;
+                        lo = make_float3(fminf(lo.x, llo[k].x), fminf(lo.y, llo[k].y), fminf(lo.z, llo[k].z));
+                        hi = make_float3(fmaxf(hi.x, lhi[k].x), fmaxf(hi.y, lhi[k].y), fmaxf(hi.z, lhi[k].z));
+                    }
+                    // splits P | S ^ P with P holding S's lowest leaf (each split once)
+                    const int low = S & -S;
+                    float best = FLT_MAX;
+                    int bp = low;
+                    for (int P = (S - 1) & S; P > 0; P = (P - 1) & S) {
+                        if (!(P & low)) continue;
+                        const float cc = copt[P] + copt[S ^ P];
+                        if (cc < best) { best = cc; bp = P; }
+                    }
+                    copt[S] = kSahCi * area(lo, hi) + best;
+                    split[S] = (uint8_t)bp;
+                }
+                if (copt[kSubsets - 1] < cur * 0.9999f) {
+                    // rebuild below p with the treelet's own internal nodes
+                    int st_s[kTreeletLeaves], st_node[kTreeletLeaves];
+                    int sp = 0, pool = 1;
+                    st_s[sp] = kSubsets - 1;
+                    st_node[sp++] = p;
+                    for (int it = 0; it < kTreeletLeaves && sp > 0; it++) {
+                        const int S = st_s[--sp], node = st_node[sp];
+                        const int parts[2] = {split[S], S ^ split[S]};
+                        int h[2];
+                        for (int q = 0; q < 2; q++) {
+                            const int P = parts[q];
+                            if ((P & (P - 1)) == 0) {
+                                h[q] = tl[__ffs(P) - 1];
+                            } else {
+                                h[q] = tin[pool++];
+                                st_s[sp] = P;
+                                st_node[sp++] = h[q];
+                            }
+                            if (h[q] >= 0) __stcg(&parent_int[h[q]], node);
+                            else __stcg(&parent_leaf[~h[q]], node);
+                        }
+                        __stcg(&child[node], make_int2(h[0], h[1]));
+                        if (node != p) {
+                            float3 lo = make_float3(FLT_MAX, FLT_MAX, FLT_MAX),
+                                   hi = make_float3(-FLT_MAX, -FLT_MAX, -FLT_MAX);
+                            int cn = 0;
+                            for (int k = 0; k < kTreeletLeaves; k++) {
+                                if (!(S & (1 << k))) continue;
+                                lo = make_float3(fminf(lo.x, llo[k].x), fminf(lo.y, llo[k].y), fminf(lo.z, llo[k].z));
+                                hi = make_float3(fmaxf(hi.x, lhi[k].x), fmaxf(hi.y, lhi[k].y), fmaxf(hi.z, lhi[k].z));
+                                cn += ln[k];
+                            }
+                            __stcg(&nlo[node], make_float4(lo.x, lo.y, lo.z, 0.f));
+                            __stcg(&nhi[node], make_float4(hi.x, hi.y, hi.z, 0.f));
+                            __stcg(&cnt[node], cn);
+                        }
+                        __stcg(&cost[node], copt[S]);
+                    }
+                }
+            }
+        }
+        p = __ldcg(&parent_int[p]);
+    }
+}
+
 // ---------------------------------------------------------------- step 6 ----
 struct Work {
     int bin;       // binary node: >= 0 internal, < 0 leaf ~sorted_pos (only for n == 1)
@@ -213,9 +377,26 @@ __device__ __forceinline__ void child_box(int c, const uint32_t *sorted_tri, con
     hi = make_float3(b.x, b.y, b.z);
 }
 
-__device__ __forceinline__ int2 child_range(int c, const int2 *range)
+// triangles below handle c (an internal node's count from k_treelet)
+__device__ __forceinline__ int child_count(int c, const int *cnt) { return c >= 0 ? cnt[c] : 1; }
+
+// The sorted positions of the triangles below handle c, which holds at most
+// kLeafMax of them, left to right. Returns how many.
+__device__ __forceinline__ int leaf_tris(int c, const int2 *child, int (&out)[kLeafMax])
 {
-    return c >= 0 ? range[c] : make_int2(~c, ~c);
+    int st[2 * kLeafMax], sp = 0, m = 0;
+    st[sp++] = c;
+    for (int it = 0; it < 4 * kLeafMax && sp > 0; it++) {
+        const int x = st[--sp];
+        if (x < 0) {
+            if (m < kLeafMax) out[m++] = ~x;
+        } else if (sp + 2 <= 2 * kLeafMax) {
+            const int2 cc = child[x];
+            st[sp++] = cc.y;
+            st[sp++] = cc.x;
+        }
+    }
+    return m;
 }
 
 // Quantisation step for one axis: the smallest power of two 2^e with
@@ -235,7 +416,7 @@ __device__ __forceinline__ float exp2i(int e) { return ldexpf(1.0f, e); }
 
 __global__ void k_collapse(const Work *__restrict__ in, const uint32_t *__restrict__ in_count, Work *__restrict__ out,
                            uint32_t *__restrict__ out_count, uint32_t out_cap, const int2 *__restrict__ child,
-                           const int2 *__restrict__ range, const float4 *__restrict__ nlo,
+                           const int *__restrict__ cnt, const float4 *__restrict__ nlo,
                            const float4 *__restrict__ nhi, const uint32_t *__restrict__ sorted_tri,
                            const float4 *__restrict__ tlo, const float4 *__restrict__ thi,
                            const float *__restrict__ pos, const uint32_t *__restrict__ idx, Node8 *__restrict__ nodes,
@@ -259,8 +440,7 @@ __global__ void k_collapse(const Work *__restrict__ in, const uint32_t *__restri
             float best_a = -1.f;
             for (int k = 0; k < m; k++) {
                 if (ch[k] < 0) continue;
-                int2 r = range[ch[k]];
-                if (r.y - r.x + 1 <= kLeafMax) continue;
+                if (cnt[ch[k]] <= kLeafMax) continue;
                 float3 lo, hi;
                 child_box(ch[k], sorted_tri, tlo, thi, nlo, nhi, lo, hi);
                 float a = area(lo, hi);
@@ -283,10 +463,9 @@ __global__ void k_collapse(const Work *__restrict__ in, const uint32_t *__restri
         child_box(ch[k], sorted_tri, tlo, thi, nlo, nhi, clo[k], chi[k]);
         plo = make_float3(fminf(plo.x, clo[k].x), fminf(plo.y, clo[k].y), fminf(plo.z, clo[k].z));
         phi = make_float3(fmaxf(phi.x, chi[k].x), fmaxf(phi.y, chi[k].y), fmaxf(phi.z, chi[k].z));
-        int2 r = child_range(ch[k], range);
-        int cnt = r.y - r.x + 1;
-        if (ch[k] >= 0 && cnt > kLeafMax) n_int++;
-        else n_leaf_tris += cnt;
+        const int nk = child_count(ch[k], cnt);
+        if (ch[k] >= 0 && nk > kLeafMax) n_int++;
+        else n_leaf_tris += nk;
     }
 
     // slot assignment: slot s is the corner with bit k set = positive along axis k
@@ -340,10 +519,8 @@ __global__ void k_collapse(const Work *__restrict__ in, const uint32_t *__restri
 
     // internal children in slot order -> contiguous child nodes
     uint32_t imask = 0;
-    for (int k = 0; k < m; k++) {
-        int2 r = child_range(ch[k], range);
-        if (ch[k] >= 0 && r.y - r.x + 1 > kLeafMax) imask |= 1u << slot_of[k];
-    }
+    for (int k = 0; k < m; k++)
+        if (ch[k] >= 0 && child_count(ch[k], cnt) > kLeafMax) imask |= 1u << slot_of[k];
     int tri_off = 0;
     for (int s = 0; s < 8; s++) {
         int k = -1;
@@ -362,8 +539,6 @@ __global__ void k_collapse(const Work *__restrict__ in, const uint32_t *__restri
         qhx[s] = (uint8_t)fmin(fmax(hx, 0.0), 255.0);
         qhy[s] = (uint8_t)fmin(fmax(hy, 0.0), 255.0);
         qhz[s] = (uint8_t)fmin(fmax(hz, 0.0), 255.0);
-        int2 r = child_range(ch[k], range);
-        int cnt = r.y - r.x + 1;
         if (imask & (1u << s)) {
             meta[s] = (uint8_t)kMetaInternal;
             uint32_t ci = child_base + __popc(imask & ((1u << s) - 1u));
@@ -371,9 +546,11 @@ __global__ void k_collapse(const Work *__restrict__ in, const uint32_t *__restri
             if (slot >= out_cap) { atomicOr(err, 8u); continue; }
             out[slot] = Work{ch[k], ci};
         } else {
-            meta[s] = (uint8_t)((cnt << 5) | tri_off);
-            for (int q = 0; q < cnt; q++) {
-                uint32_t t = sorted_tri[r.x + q];
+            int pos_of[kLeafMax];
+            const int nt = leaf_tris(ch[k], child, pos_of);
+            meta[s] = (uint8_t)((nt << 5) | tri_off);
+            for (int q = 0; q < nt; q++) {
+                uint32_t t = sorted_tri[pos_of[q]];
                 uint32_t a = idx[3 * t], b = idx[3 * t + 1], c = idx[3 * t + 2];
                 float v0x = pos[3 * a], v0y = pos[3 * a + 1], v0z = pos[3 * a + 2];
                 float e1x = __fsub_rn(pos[3 * b], v0x), e1y = __fsub_rn(pos[3 * b + 1], v0y),
@@ -390,7 +567,7 @@ __global__ void k_collapse(const Work *__restrict__ in, const uint32_t *__restri
                 tris[tri_base + tri_off + q] = tr;
                 prim_of[tri_base + tri_off + q] = t;
             }
-            tri_off += cnt;
+            tri_off += nt;
         }
     }
 
@@ -460,6 +637,11 @@ int bvh_build(BuildBuffers &B, const float *d_pos, uint32_t n_verts, const uint3
         k_refit<<<div_up(n, T), T, 0, st>>>((int)n, B.vals_alt, B.tlo, B.thi, B.child, B.parent_int, B.parent_leaf,
                                              B.arrivals, B.nlo, B.nhi);
         ILG_CK(cudaGetLastError());
+        ILG_CK(cudaMemsetAsync(B.arrivals, 0, sizeof(uint32_t) * (n - 1), st));
+        k_treelet<<<div_up(n, 128), 128, 0, st>>>((int)n, B.vals_alt, B.tlo, B.thi, B.child, B.parent_int,
+                                                  B.parent_leaf, B.arrivals, B.nlo, B.nhi, B.cnt, B.cost,
+                                                  res.treelets ? 1 : 0);
+        ILG_CK(cudaGetLastError());
     }
     ILG_CK(cudaMemsetAsync(B.counters, 0, 4 * sizeof(uint32_t), st));
     // counters: [0] node_count, [1] tri_count, [2] queue A count, [3] queue B count
@@ -473,7 +655,7 @@ int bvh_build(BuildBuffers &B, const float *d_pos, uint32_t n_verts, const uint3
     uint32_t depth = 0;
     while (host_in > 0) {
         ILG_CK(cudaMemsetAsync(cout, 0, sizeof(uint32_t), st));
-        k_collapse<<<div_up(host_in, 64), 64, 0, st>>>(qin, cin, qout, cout, queue_cap, B.child, B.range, B.nlo,
+        k_collapse<<<div_up(host_in, 64), 64, 0, st>>>(qin, cin, qout, cout, queue_cap, B.child, B.cnt, B.nlo,
                                                         B.nhi, B.vals_alt, B.tlo, B.thi, d_pos, d_idx, B.nodes,
                                                         B.counters + 0, node_cap, B.tris, B.prim_of, B.counters + 1,
                                                         tri_cap, min_step, B.err);
