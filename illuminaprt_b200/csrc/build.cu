@@ -210,7 +210,10 @@ __global__ void k_refit(int n, const uint32_t *__restrict__ sorted_tri, const fl
 // triangle count in cnt (the collapse reads it).
 // SAH cost model: internal node kSahCi x its area, triangle kSahCt x its area.
 constexpr int kTreeletLeaves = 7;
-constexpr int kTreeletPasses = 2;  // measured on a B200: 1 pass 6686 / 2250 Mrays/s (coherent / incoherent), 2 passes 6928 / 2319, 3 passes 6988 / 2331
+// passes of the restructuring; measured on a B200 (1 M-triangle heightfield,
+// coherent / incoherent Mrays/s): none 5835 / 2043, 1 pass 6686 / 2250,
+// 2 passes 6928 / 2319, 3 passes 6988 / 2331
+constexpr int kTreeletPasses = 2;
 constexpr float kSahCi = 1.2f, kSahCt = 1.0f;
 
 __device__ __forceinline__ void handle_box(int c, const uint32_t *sorted_tri, const float4 *tlo, const float4 *thi,
