@@ -226,140 +226,218 @@ __device__ __forceinline__ void handle_box(int c, const uint32_t *sorted_tri, co
     hi = make_float3(b.x, b.y, b.z);
 }
 
-__global__ void __launch_bounds__(128) k_treelet(int n, const uint32_t *__restrict__ sorted_tri,
-                                                 const float4 *__restrict__ tlo, const float4 *__restrict__ thi,
-                                                 int2 *child, int *parent_int, int *parent_leaf,
-                                                 uint32_t *__restrict__ arrivals, float4 *nlo, float4 *nhi, int *cnt,
-                                                 float *cost, int restructure)
+// The 127 non-empty subsets of the 7 treelet leaves ordered by size (7 of
+// size 1, 21 of size 2, 35, 35, 21, 7, 1), and where each size starts.
+struct SubsetTable {
+    uint8_t s[127];
+    uint8_t start[8];
+};
+__constant__ SubsetTable c_subsets;
+
+SubsetTable make_subset_table()
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    int p = parent_leaf[i];
-    for (int guard = 0; p >= 0 && p < n - 1 && guard < n; guard++) {
-        __threadfence();
-        if (atomicAdd(&arrivals[p], 1u) == 0) return;
-        __threadfence();
-        // both subtrees of p are final: its count and cost
-        const int2 c = __ldcg(&child[p]);
-        float3 plo, phi;
-        handle_box(p, sorted_tri, tlo, thi, nlo, nhi, plo, phi);
-        auto sub_cost = [&](int h) {
-            if (h >= 0) return __ldcg(&cost[h]);
+    SubsetTable t{};
+    int k = 0;
+    for (int size = 1; size <= kTreeletLeaves; size++) {
+        t.start[size - 1] = (uint8_t)k;
+        for (int S = 1; S < (1 << kTreeletLeaves); S++)
+            if (__builtin_popcount(S) == size) t.s[k++] = (uint8_t)S;
+    }
+    t.start[kTreeletLeaves] = (uint8_t)k;
+    return t;
+}
+
+constexpr int kTreeletThreads = 128;
+constexpr int kTreeletWarps = kTreeletThreads / 32;
+
+// One warp rebuilds the treelet of root p: every lane forms the same treelet
+// (the reads are the same), the lanes fill the subsets of one size per round
+// (each its own subsets' splits, against the smaller subsets of the rounds
+// before), then lane 0 writes the new topology below p if it is cheaper.
+// p's count and cost are final. All 32 lanes call this together.
+__device__ void treelet_warp(int p, float costp, const uint32_t *sorted_tri, const float4 *tlo, const float4 *thi,
+                             int2 *child, int *parent_int, int *parent_leaf, float4 *nlo, float4 *nhi, int *cnt,
+                             float *cost, float *s_copt, uint8_t *s_split, float *s_box)
+{
+    const int lane = threadIdx.x & 31;
+    __syncwarp();
+    __threadfence();  // the subtree below p is final: written before its nodes' arrivals
+    auto sub_cost = [&](int h) {
+        if (h >= 0) return __ldcg(&cost[h]);
+        float3 lo, hi;
+        handle_box(h, sorted_tri, tlo, thi, nlo, nhi, lo, hi);
+        return kSahCt * area(lo, hi);
+    };
+    int tl[kTreeletLeaves], tin[kTreeletLeaves - 1];
+    const int2 c = __ldcg(&child[p]);
+    float3 plo, phi;
+    handle_box(p, sorted_tri, tlo, thi, nlo, nhi, plo, phi);
+    int n_l = 2, n_in = 1;
+    tl[0] = c.x;
+    tl[1] = c.y;
+    tin[0] = p;
+    float cur = kSahCi * area(plo, phi);
+    while (n_l < kTreeletLeaves) {
+        int best = -1;
+        float best_a = -1.f;
+        for (int k = 0; k < n_l; k++) {
+            if (tl[k] < 0) continue;
             float3 lo, hi;
-            handle_box(h, sorted_tri, tlo, thi, nlo, nhi, lo, hi);
-            return kSahCt * area(lo, hi);
-        };
-        auto sub_cnt = [&](int h) { return h >= 0 ? __ldcg(&cnt[h]) : 1; };
-        const int cp = sub_cnt(c.x) + sub_cnt(c.y);
-        const float costp = kSahCi * area(plo, phi) + sub_cost(c.x) + sub_cost(c.y);
-        __stcg(&cnt[p], cp);
-        __stcg(&cost[p], costp);
-        if (restructure && cp >= kTreeletLeaves) {
-            // form the treelet: open the internal leaf of largest area
-            int tl[kTreeletLeaves], tin[kTreeletLeaves - 1];
-            int n_l = 2, n_in = 1;
-            tl[0] = c.x;
-            tl[1] = c.y;
-            tin[0] = p;
-            float cur = kSahCi * area(plo, phi);  // the treelet's present cost: its internal areas + leaf costs
-            while (n_l < kTreeletLeaves) {
-                int best = -1;
-                float best_a = -1.f;
-                for (int k = 0; k < n_l; k++) {
-                    if (tl[k] < 0) continue;
-                    float3 lo, hi;
-                    handle_box(tl[k], sorted_tri, tlo, thi, nlo, nhi, lo, hi);
-                    const float a = area(lo, hi);
-                    if (a > best_a) { best_a = a; best = k; }
-                }
-                if (best < 0) break;
-                const int2 cc = __ldcg(&child[tl[best]]);
-                tin[n_in++] = tl[best];
-                cur += kSahCi * best_a;
-                tl[best] = cc.x;
-                tl[n_l++] = cc.y;
+            handle_box(tl[k], sorted_tri, tlo, thi, nlo, nhi, lo, hi);
+            const float a = area(lo, hi);
+            if (a > best_a) { best_a = a; best = k; }
+        }
+        if (best < 0) break;
+        const int2 cc = __ldcg(&child[tl[best]]);
+        tin[n_in++] = tl[best];
+        cur += kSahCi * best_a;
+        tl[best] = cc.x;
+        tl[n_l++] = cc.y;
+    }
+    if (n_l < kTreeletLeaves) return;  // (not reached: p has >= 7 triangles)
+    // leaf boxes and costs, one lane each
+    if (lane < kTreeletLeaves) {
+        float3 lo, hi;
+        handle_box(tl[lane], sorted_tri, tlo, thi, nlo, nhi, lo, hi);
+        float *bx = s_box + 6 * lane;
+        bx[0] = lo.x; bx[1] = lo.y; bx[2] = lo.z; bx[3] = hi.x; bx[4] = hi.y; bx[5] = hi.z;
+        s_copt[1 << lane] = sub_cost(tl[lane]);
+    }
+    __syncwarp();
+    for (int k = 0; k < kTreeletLeaves; k++) cur += s_copt[1 << k];
+    for (int size = 2; size <= kTreeletLeaves; size++) {
+        for (int j = c_subsets.start[size - 1] + lane; j < c_subsets.start[size]; j += 32) {
+            const int S = c_subsets.s[j];
+            float3 lo = make_float3(FLT_MAX, FLT_MAX, FLT_MAX), hi = make_float3(-FLT_MAX, -FLT_MAX, -FLT_MAX);
+            for (int k = 0; k < kTreeletLeaves; k++) {
+                if (!(S & (1 << k))) continue;
+                const float *bx = s_box + 6 * k;
+                lo = make_float3(fminf(lo.x, bx[0]), fminf(lo.y, bx[1]), fminf(lo.z, bx[2]));
+                hi = make_float3(fmaxf(hi.x, bx[3]), fmaxf(hi.y, bx[4]), fmaxf(hi.z, bx[5]));
             }
-            if (n_l == kTreeletLeaves) {
-                float3 llo[kTreeletLeaves], lhi[kTreeletLeaves];
-                float lc[kTreeletLeaves];
-                int ln[kTreeletLeaves];
+            // splits P | S ^ P with P holding S's lowest leaf (each split once)
+            const int low = S & -S;
+            float best = FLT_MAX;
+            int bp = low;
+            for (int P = (S - 1) & S; P > 0; P = (P - 1) & S) {
+                if (!(P & low)) continue;
+                const float cc = s_copt[P] + s_copt[S ^ P];
+                if (cc < best) { best = cc; bp = P; }
+            }
+            s_copt[S] = kSahCi * area(lo, hi) + best;
+            s_split[S] = (uint8_t)bp;
+        }
+        __syncwarp();
+    }
+    constexpr int kAll = (1 << kTreeletLeaves) - 1;
+    if (lane == 0 && s_copt[kAll] < cur * 0.9999f) {
+        // rebuild below p with the treelet's own internal nodes
+        int st_s[kTreeletLeaves], st_node[kTreeletLeaves];
+        int sp = 0, pool = 1;
+        st_s[sp] = kAll;
+        st_node[sp++] = p;
+        for (int it = 0; it < kTreeletLeaves && sp > 0; it++) {
+            const int S = st_s[--sp], node = st_node[sp];
+            const int parts[2] = {s_split[S], S ^ s_split[S]};
+            int h[2];
+            for (int q = 0; q < 2; q++) {
+                const int P = parts[q];
+                if ((P & (P - 1)) == 0) {
+                    h[q] = tl[__ffs(P) - 1];
+                } else {
+                    h[q] = tin[pool++];
+                    st_s[sp] = P;
+                    st_node[sp++] = h[q];
+                }
+                if (h[q] >= 0) __stcg(&parent_int[h[q]], node);
+                else __stcg(&parent_leaf[~h[q]], node);
+            }
+            __stcg(&child[node], make_int2(h[0], h[1]));
+            if (node != p) {
+                float3 lo = make_float3(FLT_MAX, FLT_MAX, FLT_MAX), hi = make_float3(-FLT_MAX, -FLT_MAX, -FLT_MAX);
+                int cn = 0;
                 for (int k = 0; k < kTreeletLeaves; k++) {
-                    handle_box(tl[k], sorted_tri, tlo, thi, nlo, nhi, llo[k], lhi[k]);
-                    lc[k] = sub_cost(tl[k]);
-                    ln[k] = sub_cnt(tl[k]);
-                    cur += lc[k];
+                    if (!(S & (1 << k))) continue;
+                    const float *bx = s_box + 6 * k;
+                    lo = make_float3(fminf(lo.x, bx[0]), fminf(lo.y, bx[1]), fminf(lo.z, bx[2]));
+                    hi = make_float3(fmaxf(hi.x, bx[3]), fmaxf(hi.y, bx[4]), fmaxf(hi.z, bx[5]));
+                    cn += tl[k] >= 0 ? __ldcg(&cnt[tl[k]]) : 1;
                 }
-                // least cost of every subset of the leaves, and its best split
-                constexpr int kSubsets = 1 << kTreeletLeaves;
-                float copt[kSubsets];
-                uint8_t split[kSubsets];
-                for (int S = 1; S < kSubsets; S++) {
-                    if ((S & (S - 1)) == 0) {
-                        copt[S] = lc[__ffs(S) - 1];
-                        split[S] = 0;
-                        continue;
-                    }
-                    float3 lo = make_float3(FLT_MAX, FLT_MAX, FLT_MAX), hi = make_float3(-FLT_MAX, -FLT_MAX, -FLT_MAX);
-                    for (int k = 0; k < kTreeletLeaves; k++) {
-                        if (!(S & (1 << k))) continue;
-                        lo = make_float3(fminf(lo.x, llo[k].x), fminf(lo.y, llo[k].y), fminf(lo.z, llo[k].z));
-                        hi = make_float3(fmaxf(hi.x, lhi[k].x), fmaxf(hi.y, lhi[k].y), fmaxf(hi.z, lhi[k].z));
-                    }
-                    // splits P | S ^ P with P holding S's lowest leaf (each split once)
-                    const int low = S & -S;
-                    float best = FLT_MAX;
-                    int bp = low;
-                    for (int P = (S - 1) & S; P > 0; P = (P - 1) & S) {
-                        if (!(P & low)) continue;
-                        const float cc = copt[P] + copt[S ^ P];
-                        if (cc < best) { best = cc; bp = P; }
-                    }
-                    copt[S] = kSahCi * area(lo, hi) + best;
-                    split[S] = (uint8_t)bp;
-                }
-                if (copt[kSubsets - 1] < cur * 0.9999f) {
-                    // rebuild below p with the treelet's own internal nodes
-                    int st_s[kTreeletLeaves], st_node[kTreeletLeaves];
-                    int sp = 0, pool = 1;
-                    st_s[sp] = kSubsets - 1;
-                    st_node[sp++] = p;
-                    for (int it = 0; it < kTreeletLeaves && sp > 0; it++) {
-                        const int S = st_s[--sp], node = st_node[sp];
-                        const int parts[2] = {split[S], S ^ split[S]};
-                        int h[2];
-                        for (int q = 0; q < 2; q++) {
-                            const int P = parts[q];
-                            if ((P & (P - 1)) == 0) {
-                                h[q] = tl[__ffs(P) - 1];
-                            } else {
-                                h[q] = tin[pool++];
-                                st_s[sp] = P;
-                                st_node[sp++] = h[q];
-                            }
-                            if (h[q] >= 0) __stcg(&parent_int[h[q]], node);
-                            else __stcg(&parent_leaf[~h[q]], node);
-                        }
-                        __stcg(&child[node], make_int2(h[0], h[1]));
-                        if (node != p) {
-                            float3 lo = make_float3(FLT_MAX, FLT_MAX, FLT_MAX),
-                                   hi = make_float3(-FLT_MAX, -FLT_MAX, -FLT_MAX);
-                            int cn = 0;
-                            for (int k = 0; k < kTreeletLeaves; k++) {
-                                if (!(S & (1 << k))) continue;
-                                lo = make_float3(fminf(lo.x, llo[k].x), fminf(lo.y, llo[k].y), fminf(lo.z, llo[k].z));
-                                hi = make_float3(fmaxf(hi.x, lhi[k].x), fmaxf(hi.y, lhi[k].y), fmaxf(hi.z, lhi[k].z));
-                                cn += ln[k];
-                            }
-                            __stcg(&nlo[node], make_float4(lo.x, lo.y, lo.z, 0.f));
-                            __stcg(&nhi[node], make_float4(hi.x, hi.y, hi.z, 0.f));
-                            __stcg(&cnt[node], cn);
-                        }
-                        __stcg(&cost[node], copt[S]);
+                __stcg(&nlo[node], make_float4(lo.x, lo.y, lo.z, 0.f));
+                __stcg(&nhi[node], make_float4(hi.x, hi.y, hi.z, 0.f));
+                __stcg(&cnt[node], cn);
+            }
+            __stcg(&cost[node], s_copt[S]);
+        }
+    }
+    (void)costp;
+    __syncwarp();
+}
+
+// The bottom-up pass: every lane walks up from its leaf; a lane whose node
+// has both subtrees final (second arrival) sets the node's count and cost,
+// and the warp then rebuilds, one after another, the treelets of the nodes
+// its lanes hold that have >= kTreeletLeaves triangles. Lanes stay in the
+// loop until the whole warp is done (the treelet work uses all 32).
+__global__ void __launch_bounds__(kTreeletThreads) k_treelet(int n, const uint32_t *__restrict__ sorted_tri,
+                                                             const float4 *__restrict__ tlo,
+                                                             const float4 *__restrict__ thi, int2 *child,
+                                                             int *parent_int, int *parent_leaf,
+                                                             uint32_t *__restrict__ arrivals, float4 *nlo,
+                                                             float4 *nhi, int *cnt, float *cost, int restructure)
+{
+    __shared__ float s_copt[kTreeletWarps][1 << kTreeletLeaves];
+    __shared__ uint8_t s_split[kTreeletWarps][1 << kTreeletLeaves];
+    __shared__ float s_box[kTreeletWarps][6 * kTreeletLeaves];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int w = threadIdx.x >> 5;
+    int p = i < n ? parent_leaf[i] : -1;
+    bool alive = i < n;
+    for (int guard = 0; guard <= n; guard++) {
+        bool ready = false;
+        float costp = 0.f;
+        if (alive && (p < 0 || p >= n - 1)) alive = false;
+        if (alive) {
+            __threadfence();
+            if (atomicAdd(&arrivals[p], 1u) == 0) {
+                alive = false;
+            } else {
+                __threadfence();
+                ready = true;
+                const int2 c = __ldcg(&child[p]);
+                float3 plo, phi;
+                handle_box(p, sorted_tri, tlo, thi, nlo, nhi, plo, phi);
+                int cp = 0;
+                float cc = kSahCi * area(plo, phi);
+                for (int q = 0; q < 2; q++) {
+                    const int h = q ? c.y : c.x;
+                    if (h >= 0) {
+                        cp += __ldcg(&cnt[h]);
+                        cc += __ldcg(&cost[h]);
+                    } else {
+                        float3 lo, hi;
+                        handle_box(h, sorted_tri, tlo, thi, nlo, nhi, lo, hi);
+                        cp += 1;
+                        cc += kSahCt * area(lo, hi);
                     }
                 }
+                __stcg(&cnt[p], cp);
+                __stcg(&cost[p], cc);
+                costp = cc;
+                ready = restructure && cp >= kTreeletLeaves;
             }
         }
-        p = __ldcg(&parent_int[p]);
+        unsigned todo = __ballot_sync(0xffffffffu, ready);
+        while (todo) {
+            const int leader = __ffs(todo) - 1;
+            todo &= todo - 1;
+            const int q = __shfl_sync(0xffffffffu, p, leader);
+            const float qc = __shfl_sync(0xffffffffu, costp, leader);
+            treelet_warp(q, qc, sorted_tri, tlo, thi, child, parent_int, parent_leaf, nlo, nhi, cnt, cost, s_copt[w],
+                         s_split[w], s_box[w]);
+        }
+        if (alive) p = __ldcg(&parent_int[p]);
+        if (!__any_sync(0xffffffffu, alive)) break;
     }
 }
 
@@ -641,9 +719,13 @@ int bvh_build(BuildBuffers &B, const float *d_pos, uint32_t n_verts, const uint3
         k_refit<<<div_up(n, T), T, 0, st>>>((int)n, B.vals_alt, B.tlo, B.thi, B.child, B.parent_int, B.parent_leaf,
                                              B.arrivals, B.nlo, B.nhi);
         ILG_CK(cudaGetLastError());
+        if (res.treelets) {
+            static const SubsetTable table = make_subset_table();
+            ILG_CK(cudaMemcpyToSymbolAsync(c_subsets, &table, sizeof(table), 0, cudaMemcpyHostToDevice, st));
+        }
         for (int pass = 0; pass < (res.treelets ? kTreeletPasses : 1); pass++) {
             ILG_CK(cudaMemsetAsync(B.arrivals, 0, sizeof(uint32_t) * (n - 1), st));
-            k_treelet<<<div_up(n, 128), 128, 0, st>>>((int)n, B.vals_alt, B.tlo, B.thi, B.child, B.parent_int,
+            k_treelet<<<div_up(n, kTreeletThreads), kTreeletThreads, 0, st>>>((int)n, B.vals_alt, B.tlo, B.thi, B.child, B.parent_int,
                                                       B.parent_leaf, B.arrivals, B.nlo, B.nhi, B.cnt, B.cost,
                                                       res.treelets ? 1 : 0);
             ILG_CK(cudaGetLastError());
