@@ -39,7 +39,11 @@ struct __align__(16) Tri {
 static_assert(sizeof(Tri) == 48, "triangle record must be 48 bytes");
 
 constexpr int kMaxStack = 64;      // traversal stack entries (node groups)
-constexpr int kLeafMax = 3;        // triangles per leaf child
+// triangles per leaf child; measured on a B200 with the treelet-restructured
+// tree (1 M-triangle heightfield, coherent / incoherent Mrays/s; 21 M-triangle
+// field, 960x540x16 ms): 1: 6790 / 2254, 25.6; 2: 7100 / 2357, 26.0;
+// 3: 6920 / 2316, 26.7
+constexpr int kLeafMax = 2;
 constexpr uint32_t kMetaInternal = 0x80u;
 
 // Lower bound of the reference's triangle window, `t < 1e-5` evaluated in
