@@ -11,9 +11,11 @@
 //   5. k_refit        bottom-up AABBs, one atomic arrival counter per node
 //   5b. k_treelet     bottom-up treelet restructuring for least SAH cost
 //                     (Karras & Aila 2013); subtree triangle counts
+//   5c. k_collapse_cost  bottom-up SAH costs of the binary subtrees as 1..8
+//                     roots of an 8-wide node (Ylitie et al. 2017)
 //   6. k_collapse     level by level: each work item turns one binary node
-//                     into one 8-wide node (greedy: open the widest child
-//                     with more than 3 triangles until 8 slots are used),
+//                     into one 8-wide node (its children: the roots the
+//                     step 5c costs chose; a root is a leaf or a node),
 //                     orders the slots by octant, quantises the child boxes
 //                     to 8 bits against the node origin, and writes the
 //                     triangle records of its leaf children.
@@ -441,6 +443,98 @@ __global__ void __launch_bounds__(kTreeletThreads) k_treelet(int n, const uint32
     }
 }
 
+// ------------------------------------------------------------- step 5c ----
+// Which binary nodes become 8-wide nodes, and which leaves, for least SAH
+// cost (the dynamic program of Ylitie, Karras & Laine 2017, "Efficient
+// incoherent ray traversal on GPUs through compressed wide BVHs", without its
+// leaf reordering): bottom-up, for each binary node n and i = 1..8, the least
+// cost of the subtree of n as at most i roots under an 8-wide parent. One
+// root is n itself, as a leaf (<= kLeafMax triangles: its area x kColTri x
+// its triangles) or as an 8-wide node (its area x kColNode + the least cost
+// of its subtree below as at most 8 roots); more roots split the subtree
+// between n's two children. Decisions per node (dpd, 16 bytes): [0] n as one
+// root is a leaf (1) or an 8-wide node (0); [j - 1], j = 2..8: the left
+// child's share of a j-root split; [8 + i - 1]: the roots (1 = n itself, or
+// the split j) that give the least cost with at most i roots.
+constexpr float kColNode = 1.0f, kColTri = 0.3f;
+
+__device__ __forceinline__ void root_costs(int h, const uint32_t *sorted_tri, const float4 *tlo, const float4 *thi,
+                                           const float *dpc, float (&c)[8])
+{
+    if (h < 0) {
+        const uint32_t t = sorted_tri[~h];
+        const float4 lo = tlo[t], hi = thi[t];
+        const float a = kColTri * area(make_float3(lo.x, lo.y, lo.z), make_float3(hi.x, hi.y, hi.z));
+#pragma unroll
+        for (int i = 0; i < 8; i++) c[i] = a;
+    } else {
+        const float4 *src = reinterpret_cast<const float4 *>(dpc + 8 * (size_t)h);
+        const float4 x = __ldcg(src), y = __ldcg(src + 1);
+        c[0] = x.x; c[1] = x.y; c[2] = x.z; c[3] = x.w; c[4] = y.x; c[5] = y.y; c[6] = y.z; c[7] = y.w;
+    }
+}
+
+__global__ void __launch_bounds__(128) k_collapse_cost(int n, const uint32_t *__restrict__ sorted_tri,
+                                                       const float4 *__restrict__ tlo, const float4 *__restrict__ thi,
+                                                       const int2 *__restrict__ child, const int *__restrict__ parent_int,
+                                                       const int *__restrict__ parent_leaf,
+                                                       uint32_t *__restrict__ arrivals, const float4 *__restrict__ nlo,
+                                                       const float4 *__restrict__ nhi, const int *__restrict__ cnt,
+                                                       float *dpc, uint8_t *__restrict__ dpd)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int p = parent_leaf[i];
+    for (int guard = 0; p >= 0 && p < n - 1 && guard < n; guard++) {
+        __threadfence();
+        if (atomicAdd(&arrivals[p], 1u) == 0) return;
+        __threadfence();
+        const int2 c = child[p];
+        float ca[8], cb[8];
+        root_costs(c.x, sorted_tri, tlo, thi, dpc, ca);
+        root_costs(c.y, sorted_tri, tlo, thi, dpc, cb);
+        uint8_t dec[16];
+        float split[8];  // [j - 1]: least cost of j roots split between the children
+#pragma unroll
+        for (int j = 2; j <= 8; j++) {
+            float best = FLT_MAX;
+            int bk = 1;
+#pragma unroll
+            for (int k = 1; k < j; k++) {
+                const float v = ca[k - 1] + cb[j - k - 1];
+                if (v < best) { best = v; bk = k; }
+            }
+            split[j - 1] = best;
+            dec[j - 1] = (uint8_t)bk;
+        }
+        const float4 lo = nlo[p], hi = nhi[p];
+        const float a = area(make_float3(lo.x, lo.y, lo.z), make_float3(hi.x, hi.y, hi.z));
+        const int np = cnt[p];
+        const float as_leaf = np <= kLeafMax ? kColTri * a * (float)np : FLT_MAX;
+        const float as_node = kColNode * a + split[7];
+        float cost[8];
+        cost[0] = fminf(as_leaf, as_node);
+        dec[0] = as_leaf <= as_node ? 1u : 0u;
+        dec[8] = 1;
+#pragma unroll
+        for (int k = 2; k <= 8; k++) {
+            cost[k - 1] = cost[k - 2];
+            dec[8 + k - 1] = dec[8 + k - 2];
+            if (split[k - 1] < cost[k - 1]) {
+                cost[k - 1] = split[k - 1];
+                dec[8 + k - 1] = (uint8_t)k;
+            }
+        }
+        float4 *dst = reinterpret_cast<float4 *>(dpc + 8 * (size_t)p);
+        __stcg(dst, make_float4(cost[0], cost[1], cost[2], cost[3]));
+        __stcg(dst + 1, make_float4(cost[4], cost[5], cost[6], cost[7]));
+        uint4 d;
+        memcpy(&d, dec, 16);
+        *reinterpret_cast<uint4 *>(dpd + 16 * (size_t)p) = d;
+        p = parent_int[p];
+    }
+}
+
 // ---------------------------------------------------------------- step 6 ----
 struct Work {
     int bin;       // binary node: >= 0 internal, < 0 leaf ~sorted_pos (only for n == 1)
@@ -461,6 +555,9 @@ __device__ __forceinline__ void child_box(int c, const uint32_t *sorted_tri, con
 
 // triangles below handle c (an internal node's count from k_treelet)
 __device__ __forceinline__ int child_count(int c, const int *cnt) { return c >= 0 ? cnt[c] : 1; }
+
+// whether root handle c becomes an 8-wide node (else a leaf child)
+__device__ __forceinline__ bool is_node_root(int c, const uint8_t *dpd) { return c >= 0 && dpd[16 * (size_t)c] == 0; }
 
 // The sorted positions of the triangles below handle c, which holds at most
 // kLeafMax of them, left to right. Returns how many.
@@ -498,7 +595,7 @@ __device__ __forceinline__ float exp2i(int e) { return ldexpf(1.0f, e); }
 
 __global__ void k_collapse(const Work *__restrict__ in, const uint32_t *__restrict__ in_count, Work *__restrict__ out,
                            uint32_t *__restrict__ out_count, uint32_t out_cap, const int2 *__restrict__ child,
-                           const int *__restrict__ cnt, const float4 *__restrict__ nlo,
+                           const int *__restrict__ cnt, const uint8_t *__restrict__ dpd, const float4 *__restrict__ nlo,
                            const float4 *__restrict__ nhi, const uint32_t *__restrict__ sorted_tri,
                            const float4 *__restrict__ tlo, const float4 *__restrict__ thi,
                            const float *__restrict__ pos, const uint32_t *__restrict__ idx, Node8 *__restrict__ nodes,
@@ -513,26 +610,31 @@ __global__ void k_collapse(const Work *__restrict__ in, const uint32_t *__restri
     int ch[8];
     int m = 0;
     if (job.bin >= 0) {
-        int2 c = child[job.bin];
-        ch[m++] = c.x;
-        ch[m++] = c.y;
-        // open the widest child that must stay internal until 8 slots are used
-        while (m < 8) {
-            int best = -1;
-            float best_a = -1.f;
-            for (int k = 0; k < m; k++) {
-                if (ch[k] < 0) continue;
-                if (cnt[ch[k]] <= kLeafMax) continue;
-                float3 lo, hi;
-                child_box(ch[k], sorted_tri, tlo, thi, nlo, nhi, lo, hi);
-                float a = area(lo, hi);
-                if (a > best_a) { best_a = a; best = k; }
+        // the roots the collapse costs chose for this node's subtree below
+        // it: its children's split of 8 roots, each side followed down to the
+        // handles that stand as one root
+        const int2 c = child[job.bin];
+        const int k8 = dpd[16 * (size_t)job.bin + 7];
+        int st_h[16], st_i[16], sp = 0;
+        st_h[sp] = c.y;
+        st_i[sp++] = 8 - k8;
+        st_h[sp] = c.x;
+        st_i[sp++] = k8;
+        for (int it = 0; it < 32 && sp > 0 && m < 8; it++) {
+            const int h = st_h[--sp], r = st_i[sp];
+            const int j = h >= 0 ? dpd[16 * (size_t)h + 8 + r - 1] : 1;
+            if (j <= 1 || sp + 2 > 16) {
+                ch[m++] = h;
+                continue;
             }
-            if (best < 0) break;
-            int2 c2 = child[ch[best]];
-            ch[best] = c2.x;
-            ch[m++] = c2.y;
+            const int k = dpd[16 * (size_t)h + j - 1];
+            const int2 cc = child[h];
+            st_h[sp] = cc.y;
+            st_i[sp++] = j - k;
+            st_h[sp] = cc.x;
+            st_i[sp++] = k;
         }
+        if (sp > 0) { atomicOr(err, 16u); return; }
     } else {
         ch[m++] = job.bin;  // single-triangle scene
     }
@@ -545,9 +647,8 @@ __global__ void k_collapse(const Work *__restrict__ in, const uint32_t *__restri
         child_box(ch[k], sorted_tri, tlo, thi, nlo, nhi, clo[k], chi[k]);
         plo = make_float3(fminf(plo.x, clo[k].x), fminf(plo.y, clo[k].y), fminf(plo.z, clo[k].z));
         phi = make_float3(fmaxf(phi.x, chi[k].x), fmaxf(phi.y, chi[k].y), fmaxf(phi.z, chi[k].z));
-        const int nk = child_count(ch[k], cnt);
-        if (ch[k] >= 0 && nk > kLeafMax) n_int++;
-        else n_leaf_tris += nk;
+        if (is_node_root(ch[k], dpd)) n_int++;
+        else n_leaf_tris += child_count(ch[k], cnt);
     }
 
     // slot assignment: slot s is the corner with bit k set = positive along axis k
@@ -602,7 +703,7 @@ __global__ void k_collapse(const Work *__restrict__ in, const uint32_t *__restri
     // internal children in slot order -> contiguous child nodes
     uint32_t imask = 0;
     for (int k = 0; k < m; k++)
-        if (ch[k] >= 0 && child_count(ch[k], cnt) > kLeafMax) imask |= 1u << slot_of[k];
+        if (is_node_root(ch[k], dpd)) imask |= 1u << slot_of[k];
     int tri_off = 0;
     for (int s = 0; s < 8; s++) {
         int k = -1;
@@ -730,6 +831,10 @@ int bvh_build(BuildBuffers &B, const float *d_pos, uint32_t n_verts, const uint3
                                                       res.treelets ? 1 : 0);
             ILG_CK(cudaGetLastError());
         }
+        ILG_CK(cudaMemsetAsync(B.arrivals, 0, sizeof(uint32_t) * (n - 1), st));
+        k_collapse_cost<<<div_up(n, 128), 128, 0, st>>>((int)n, B.vals_alt, B.tlo, B.thi, B.child, B.parent_int,
+                                                        B.parent_leaf, B.arrivals, B.nlo, B.nhi, B.cnt, B.dpc, B.dpd);
+        ILG_CK(cudaGetLastError());
     }
     ILG_CK(cudaMemsetAsync(B.counters, 0, 4 * sizeof(uint32_t), st));
     // counters: [0] node_count, [1] tri_count, [2] queue A count, [3] queue B count
@@ -743,7 +848,7 @@ int bvh_build(BuildBuffers &B, const float *d_pos, uint32_t n_verts, const uint3
     uint32_t depth = 0;
     while (host_in > 0) {
         ILG_CK(cudaMemsetAsync(cout, 0, sizeof(uint32_t), st));
-        k_collapse<<<div_up(host_in, 64), 64, 0, st>>>(qin, cin, qout, cout, queue_cap, B.child, B.cnt, B.nlo,
+        k_collapse<<<div_up(host_in, 64), 64, 0, st>>>(qin, cin, qout, cout, queue_cap, B.child, B.cnt, B.dpd, B.nlo,
                                                         B.nhi, B.vals_alt, B.tlo, B.thi, d_pos, d_idx, B.nodes,
                                                         B.counters + 0, node_cap, B.tris, B.prim_of, B.counters + 1,
                                                         tri_cap, min_step, B.err);

@@ -39,7 +39,8 @@ struct BuildBuffers {
     DevBuf<uint32_t> keys_b, keys_alt_b, vals_b, vals_alt_b, arrivals_b, cb_b, counters_b, err_b;
     DevBuf<int2> child_b, range_b;
     DevBuf<int> parent_int_b, parent_leaf_b, cnt_b;
-    DevBuf<float> cost_b;
+    DevBuf<float> cost_b, dpc_b;
+    DevBuf<uint8_t> dpd_b;
     DevBuf<unsigned char> sort_tmp_b;
     DevBuf<uint64_t> qa_b, qb_b;  // work items, 8 bytes each
     // outputs (the built scene)
@@ -51,7 +52,8 @@ struct BuildBuffers {
     uint32_t *keys, *keys_alt, *vals, *vals_alt, *arrivals, *cbounds, *counters, *err;
     int2 *child, *range;
     int *parent_int, *parent_leaf, *cnt;
-    float *cost;
+    float *cost, *dpc;  // dpc: 8 collapse costs a binary node
+    uint8_t *dpd;       // 16 collapse decisions a binary node
     void *sort_tmp;
     void *qa_raw, *qb_raw;  // two 8-byte work-item queues
     Node8 *nodes;
@@ -66,7 +68,7 @@ struct BuildBuffers {
         ILG_R(keys_b, n) ILG_R(keys_alt_b, n) ILG_R(vals_b, n) ILG_R(vals_alt_b, n) ILG_R(arrivals_b, n)
         ILG_R(cb_b, 8) ILG_R(counters_b, 8) ILG_R(err_b, 1)
         ILG_R(child_b, n) ILG_R(range_b, n) ILG_R(parent_int_b, n) ILG_R(parent_leaf_b, n) ILG_R(cnt_b, n)
-        ILG_R(cost_b, n)
+        ILG_R(cost_b, n) ILG_R(dpc_b, 8 * n) ILG_R(dpd_b, 16 * n)
         ILG_R(sort_tmp_b, sort_bytes) ILG_R(qa_b, queue_cap) ILG_R(qb_b, queue_cap)
         ILG_R(nodes_b, node_cap) ILG_R(tris_b, n) ILG_R(prim_of_b, n)
 #undef ILG_R
@@ -74,7 +76,7 @@ struct BuildBuffers {
         keys = keys_b.ptr; keys_alt = keys_alt_b.ptr; vals = vals_b.ptr; vals_alt = vals_alt_b.ptr;
         arrivals = arrivals_b.ptr; cbounds = cb_b.ptr; counters = counters_b.ptr; err = err_b.ptr;
         child = child_b.ptr; range = range_b.ptr; parent_int = parent_int_b.ptr; parent_leaf = parent_leaf_b.ptr;
-        cnt = cnt_b.ptr; cost = cost_b.ptr;
+        cnt = cnt_b.ptr; cost = cost_b.ptr; dpc = dpc_b.ptr; dpd = dpd_b.ptr;
         sort_tmp = sort_tmp_b.ptr; qa_raw = qa_b.ptr; qb_raw = qb_b.ptr;
         nodes = nodes_b.ptr; tris = tris_b.ptr; prim_of = prim_of_b.ptr;
         return cudaSuccess;
@@ -86,7 +88,7 @@ struct BuildBuffers {
         tlo_b.release(); thi_b.release(); nlo_b.release(); nhi_b.release();
         keys_b.release(); keys_alt_b.release(); vals_b.release(); vals_alt_b.release(); arrivals_b.release();
         child_b.release(); range_b.release(); parent_int_b.release(); parent_leaf_b.release();
-        cnt_b.release(); cost_b.release();
+        cnt_b.release(); cost_b.release(); dpc_b.release(); dpd_b.release();
         sort_tmp_b.release(); qa_b.release(); qb_b.release();
     }
 
