@@ -301,6 +301,7 @@ int ilg_create(ilg_ctx **out, const ilg_opts *opts)
     ilg_ctx *ctx = new (std::nothrow) ilg_ctx();
     if (!ctx) return ILG_ENOMEM;
     ctx->device = dev;
+    ctx->build_flags = opts ? opts->build_flags : 0u;
     if (cudaSetDevice(dev) != cudaSuccess || cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreate(&ctx->ev0) != cudaSuccess || cudaEventCreate(&ctx->ev1) != cudaSuccess ||
         ctx->derr.reserve(4) != cudaSuccess || ctx->dstats.reserve(2) != cudaSuccess) {
@@ -402,6 +403,7 @@ int ilg_build(ilg_ctx *ctx)
     CK(cudaSetDevice(ctx->device));
     BuildResult res;
     res.min_step = std::max(ctx->max_abs * 0x1p-19f, 1e-30f);
+    res.treelets = !(ctx->build_flags & ILG_BUILD_FAST);
     CK(cudaEventRecord(ctx->ev0, ctx->stream));
     int rc = bvh_build(ctx->bb, ctx->pos.ptr, ctx->n_verts, ctx->idx.ptr, ctx->n_tris, ctx->stream, res, ctx->err,
                        sizeof(ctx->err));

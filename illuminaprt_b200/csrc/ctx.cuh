@@ -20,6 +20,7 @@ cudaError_t noalloc_prepare(void **out);
 
 struct ilg_ctx {
     int device = 0;
+    uint32_t build_flags = 0;  // ILG_BUILD_*
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     // two more streams for chunked host-buffer queries (made on first use)

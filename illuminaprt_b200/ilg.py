@@ -55,7 +55,10 @@ class IlgError(RuntimeError):
 
 
 class ilg_opts(ctypes.Structure):
-    _fields_ = [("device", ctypes.c_int32), ("reserved", ctypes.c_uint32 * 7)]
+    _fields_ = [("device", ctypes.c_int32), ("build_flags", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 6)]
+
+
+ILG_BUILD_FAST = 0x1
 
 
 class ilg_stats(ctypes.Structure):
@@ -198,10 +201,11 @@ def _ptr(a) -> int:
 class GpuSpace:
     """A triangle scene on one GPU with batched closest-hit / any-hit queries."""
 
-    def __init__(self, device: int = 0):
+    def __init__(self, device: int = 0, fast_build: bool = False):
+        """fast_build: ILG_BUILD_FAST (the Morton tree without treelet restructuring)."""
         self.L = load()
         self.h = ctypes.c_void_p()
-        opts = ilg_opts(device=device)
+        opts = ilg_opts(device=device, build_flags=ILG_BUILD_FAST if fast_build else 0)
         rc = self.L.ilg_create(ctypes.byref(self.h), ctypes.byref(opts))
         if rc != ILG_OK:
             raise IlgError(rc, f"ilg_create(device={device}) failed")

@@ -240,3 +240,25 @@ def test_pageable_host_buffers_give_the_pinned_results():
         occ = sp.occluded(o4, d4, watertight=wt)
         assert np.array_equal(occ.astype(bool), pinned[0].numpy() >= 0)
     sp.close()
+
+
+def test_fast_build_answers_the_same_queries_with_more_work(oracle):
+    # ILG_BUILD_FAST keeps the Morton tree (no treelet restructuring): the same
+    # hits up to near ties, and more node and triangle visits a ray than the
+    # default SAH-restructured tree
+    import torch
+    from illuminaprt_b200.ilg import GpuSpace
+    pos, idx = scenes.heightfield(256, 128, 0.2, 7)
+    io, idr = scenes.incoherent_rays(pos, idx, 65536, 9)
+    spaces = {}
+    for fast in (False, True):
+        sp = GpuSpace(fast_build=fast)
+        sp.initialise(pos, idx)
+        sp.build()
+        spaces[fast] = sp
+    best, fast = spaces[False].intersects(io, idr), spaces[True].intersects(io, idr)
+    n_same, ties, bad, bits_ok = classify(pos, idx, io, idr, best, fast, oracle)
+    assert bad == [] and bits_ok and ties <= len(io) // 10000 + 2
+    O, D = torch.from_numpy(io).cuda(), torch.from_numpy(idr).cuda()
+    work = {k: sum(sp.traversal_counts(O, D)) for k, sp in spaces.items()}
+    assert work[False] < 0.95 * work[True], work
