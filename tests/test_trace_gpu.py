@@ -262,3 +262,63 @@ def test_fast_build_answers_the_same_queries_with_more_work(oracle):
     O, D = torch.from_numpy(io).cuda(), torch.from_numpy(idr).cuda()
     work = {k: sum(sp.traversal_counts(O, D)) for k, sp in spaces.items()}
     assert work[False] < 0.95 * work[True], work
+
+
+def test_ray_interval_edges_match_oracle(oracle):
+    # the ray's [Min, Max] interval: Max before the first hit, Min before it,
+    # Min past Max. The reference's triangle test ignores Min (it rejects
+    # t < 1e-5 instead, IndexedTriangle.cpp:115); only its trees' box tests
+    # use Min, so a hit before Min is reported or not as the tree's boxes
+    # decide. Rays whose Min lies past their first hit are therefore checked
+    # apart: whatever the device reports must be a genuine hit of the
+    # reference's test, and a ray the device misses must have its first hit
+    # before Min.
+    pos, idx = scenes.heightfield(64, 32, 0.2, 5)
+    co, cd = scenes.pinhole_rays(64, 64, (0.5, -0.6, 0.8), (0.5, 0.5, 0.0), (0, 0, 1), 60.0)
+    n = co.shape[0]
+    rng = np.random.default_rng(3)
+    o4, d4 = co.copy(), cd.copy()
+    full = space_for(pos, idx).intersects(co, cd)
+    t_hit = np.where(full[0] >= 0, full[1], 2.0).astype(np.float32)
+    kind = rng.integers(0, 4, n)
+    o4[kind == 0, 3] = 0.5 * t_hit[kind == 0]          # Min before the hit
+    o4[kind == 1, 3] = 1.5 * t_hit[kind == 1]          # Min past the hit
+    d4[kind == 2, 3] = 0.5 * t_hit[kind == 2]          # Max before the hit
+    o4[kind == 3, 3] = 1.0
+    d4[kind == 3, 3] = 0.5                              # Min > Max
+    got = space_for(pos, idx).intersects(o4, d4)
+    ref = oracle.intersect_brute(pos, idx, o4, d4)
+    keep = kind != 1
+    sub = lambda r: tuple(x[keep] for x in r)
+    n_same, ties, bad, bits_ok = classify(pos, idx, o4[keep], d4[keep], sub(got), sub(ref), oracle)
+    assert bad == [] and bits_ok
+    assert (got[0][kind == 2] == -1).all()
+    for i in np.nonzero(kind == 1)[0]:
+        if got[0][i] >= 0:
+            acc, t, _, _ = oracle.shirley(pos, idx.reshape(-1), got[0][i], o4[i], d4[i], d4[i, 3])
+            assert acc and np.float32(t).view(np.uint32) == got[1][i].view(np.uint32)
+        else:
+            assert full[0][i] == -1 or full[1][i] < o4[i, 3]
+
+
+def test_large_host_batch_in_many_chunks():
+    # a host-buffer call of 5,000,003 rays runs in 9 chunks of about 512 K
+    # over three streams, the last one short; its hits equal the
+    # device-pointer call's
+    import torch
+    from illuminaprt_b200.ilg import GpuSpace
+    pos, idx = scenes.heightfield(256, 128, 0.2, 2)
+    io, idr = scenes.incoherent_rays(pos, idx, 5_000_003, 4)
+    sp = GpuSpace()
+    sp.initialise(pos, idx)
+    sp.build()
+    n = io.shape[0]
+    host = (torch.empty(n, dtype=torch.int32).pin_memory(), *(torch.empty(n).pin_memory() for _ in range(3)))
+    sp.intersects_into(torch.from_numpy(io).pin_memory(), torch.from_numpy(idr).pin_memory(), *host,
+                       device_ptrs=False)
+    O, D = torch.from_numpy(io).cuda(), torch.from_numpy(idr).cuda()
+    dev = (torch.empty(n, dtype=torch.int32, device="cuda"), *(torch.empty(n, device="cuda") for _ in range(3)))
+    sp.intersects_into(O, D, *dev, device_ptrs=True)
+    sp.sync()
+    for a, b in zip(host, dev):
+        assert torch.equal(a, b.cpu())
