@@ -906,8 +906,10 @@ def main():
                     "d2h_bytes_per_step": rays_per_step * HIT_OUT,
                     "pinned_h2d_gbs": round(h2d_gbs, 2),
                     "pinned_d2h_gbs": round(d2h_gbs, 2),
-                    "copy_bound_mrays_s": round(rays_per_step / (duplex_ms / 1e3) / 1e6, 3),
-                    "copy_bound": "a step's ray bytes up and hit bytes down as two plain pinned copies at once",
+                    "copy_bound_mrays_s": round(rays_per_step / (max(h2d_ms, d2h_ms) / 1e3) / 1e6, 3),
+                    "copy_bound": "a step's ray bytes up and hit bytes down as plain pinned copies, each alone, "
+                                  "overlapped perfectly: the slower direction's time",
+                    "duplex_copies_mrays_s": round(rays_per_step / (duplex_ms / 1e3) / 1e6, 3),
                     "e2e_pageable_mrays_s": round(e2e_page_value, 3),
                     "pipeline": "host-buffer calls run in chunks over three streams: upload, traversal and "
                                 "download of neighbouring chunks overlap"},
