@@ -870,7 +870,10 @@ def main():
     l2_gbs = max(l2_probe.values())
     hbm_read_gbs = round(sp.probe_read_gbs(2 << 30, 4), 1)
 
-    pt = {} if args.no_path_tracer else bench_path_tracer(
+    # the path-tracing, network, batch and cache legs describe one GPU: a
+    # multi-GPU run measures the ray query alone (its metric), so that it
+    # holds the GPUs for the timed work only
+    pt = {} if args.no_path_tracer or world > 1 else bench_path_tracer(
         dev, local, tuple(args.legs.split(",")), tuple(float(b) for b in args.cache_budgets.split(",")))
     hbm, peak_kind = load_peaks()
     # algorithmic bytes of one incoherent launch (the dominant kernel): rays in,
