@@ -483,10 +483,6 @@ __global__ void __launch_bounds__(256) k_shade(RenderDev R, int cur, uint32_t de
     bool cont = false;
     float4 no = make_float4(0.f, 0.f, 0.f, 0.f), nd = no;
     uint32_t path = 0;
-    // shadow segments of this vertex (at most kMaxLights)
-    float4 so[kMaxLights], sd[kMaxLights];
-    float3 sc[kMaxLights];
-    uint32_t n_sh = 0;
     uint32_t pixel = 0;
     bool query = false;           // rendering path stopping into the cache here
     float4 qb = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -597,10 +593,28 @@ __global__ void __launch_bounds__(256) k_shade(RenderDev R, int cur, uint32_t de
                     R.rec_of[tslot * (R.depth_max + 1) + depth] = stored;
                 }
                 // next-event estimation toward every light but the one hit (a
-                // specular BSDF's F is zero for every light direction)
+                // specular BSDF's F is zero for every light direction); each
+                // sample goes to the shadow queue as it is made
                 for (uint32_t l = 0; l < S.n_lights && l < kMaxLights && !specular; l++) {
                     if (l == light_id) continue;
-                    if (light_sample(S, l, key, depth, p, U, V, W, wo_l, m, beta, so[n_sh], sd[n_sh], sc[n_sh])) n_sh++;
+                    float4 so, sd;
+                    float3 sc;
+                    const bool ok = light_sample(S, l, key, depth, p, U, V, W, wo_l, m, beta, so, sd, sc);
+                    const uint32_t s = push_slot(ok, R.sh_count);
+                    if (ok) {
+                        if (s < R.sh_capacity) {
+                            R.s_o[s] = so;
+                            R.s_d[s] = sd;
+                            // bit 31 marks a light sample of the first vertex (Direct)
+                            const uint32_t tag = (depth == 0 && R.accum_direct) ? 0x80000000u : 0u;
+                            R.s_c[s] = make_float4(sc.x, sc.y, sc.z, __uint_as_float(pixel | tag));
+                            R.s_sid[s] = sid;
+                            if (R.cache_depth)
+                                R.s_meta[s] = tslot == 0xffffffffu ? 0xffffffffu : ((tslot << 8) | depth);
+                        } else {
+                            atomicOr(R.err, 16u);
+                        }
+                    }
                 }
 
                 if (continue_path(S, key, depth, m, specular, p, ng, U, V, W, wo_l, beta, no, nd)) {
@@ -625,24 +639,6 @@ __global__ void __launch_bounds__(256) k_shade(RenderDev R, int cur, uint32_t de
         } else {
             atomicOr(R.err, 8u);
         }
-    }
-    for (uint32_t k = 0; k < kMaxLights; k++) {
-        const bool want = k < n_sh;
-        const uint32_t s = push_slot(want, R.sh_count);
-        if (want) {
-            if (s < R.sh_capacity) {
-                R.s_o[s] = so[k];
-                R.s_d[s] = sd[k];
-                // bit 31 marks a light sample of the first vertex (Direct)
-                const uint32_t tag = (depth == 0 && R.accum_direct) ? 0x80000000u : 0u;
-                R.s_c[s] = make_float4(sc[k].x, sc[k].y, sc[k].z, __uint_as_float(pixel | tag));
-                R.s_sid[s] = sid;
-                if (R.cache_depth) R.s_meta[s] = tslot == 0xffffffffu ? 0xffffffffu : ((tslot << 8) | depth);
-            } else {
-                atomicOr(R.err, 16u);
-            }
-        }
-        if (!__any_sync(__activemask(), k + 1 < n_sh)) break;
     }
     if (R.cache_depth) {
         const uint32_t q = push_slot(query, R.qry_count);
