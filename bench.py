@@ -814,7 +814,7 @@ def main():
     # the e2e hits must equal the device-resident ones
     assert torch.equal(hout_all[0], all_out[0].cpu())
     # the same from pageable host memory (plain CPU tensors, as a host
-    # application's own arrays are): the library stages them through its two
+    # application's own arrays are): the library stages them through its three
     # page-locked slots
     page = (pin_all[0].clone(), pin_all[1].clone())
     hpage = tuple(torch.empty_like(x, pin_memory=False) for x in hout_all)

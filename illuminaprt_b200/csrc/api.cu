@@ -13,6 +13,7 @@
 #include "build.cuh"
 #include "trace_api.cuh"
 #include "ctx.cuh"
+#include "hostpool.h"
 #include "render.cuh"
 
 using namespace ilg;
@@ -74,93 +75,99 @@ bool pageable(const void *p)
     return a.type == cudaMemoryTypeUnregistered;
 }
 
-// memcpy split over up to 16 host threads, 1 MB a thread at least
-// (pageable <-> page-locked copies run at about 10 GB/s on one core)
-void host_copy(void *dst, const void *src, size_t bytes)
+// host copies of pageable queries: up to 16 parts (the calling thread and
+// the context's pool), 1 MB a part at least
+constexpr unsigned kCopyParts = 16u;
+
+void pool_copy_ctx(ilg_ctx *ctx, const CopySeg *seg, int nseg)
 {
-    const size_t kMinPiece = 1u << 20;
-    unsigned th = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
-    th = (unsigned)std::min<size_t>(th, (bytes + kMinPiece - 1) / kMinPiece);
-    if (th <= 1) {
-        memcpy(dst, src, bytes);
-        return;
+    if (!ctx->host_pool) ctx->host_pool = new (std::nothrow) HostPool();
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    if (ctx->host_pool) {
+        pool_copy(*ctx->host_pool, seg, nseg, std::min(kCopyParts, hw));
+    } else {
+        for (int i = 0; i < nseg; i++) memcpy(seg[i].dst, seg[i].src, seg[i].bytes);
     }
-    const size_t piece = (bytes + th - 1) / th;
-    std::vector<std::thread> pool;
-    for (unsigned k = 1; k < th; k++) {
-        const size_t off = k * piece;
-        if (off >= bytes) break;
-        auto copy = [=] { memcpy((char *)dst + off, (const char *)src + off, std::min(piece, bytes - off)); };
-        try {
-            pool.emplace_back(copy);
-        } catch (...) {  // no thread to be had: this piece on the calling thread
-            copy();
-        }
-    }
-    memcpy(dst, src, std::min(piece, bytes));
-    for (auto &t : pool) t.join();
 }
 
 // Closest hit (occ == nullptr) or any hit of rays in pageable host memory:
-// chunks of rays go through two page-locked slots owned by the context, so
-// the host copies of one chunk (rays in, hits out) overlap the device's work
-// on the other.
+// chunks of rays go through three page-locked slots owned by the context,
+// each with its own stream and device buffers. For chunk c the host waits
+// for the slot's previous chunk (c - 3), then copies that chunk's hits out
+// and chunk c's rays in as one job over the host threads, and queues chunk
+// c's upload, traversal and download on the slot's stream; the device works
+// on the other slots' chunks meanwhile.
+constexpr uint32_t kPinSlots = 3u;
+
 int query_host_pageable_run(ilg_ctx *ctx, const float *o4, const float *d4, uint32_t n, int32_t *prim, float *t,
                             float *u, float *v, uint8_t *occ, bool wt)
 {
     const bool any = occ != nullptr;
     constexpr uint32_t kChunk = 1u << 19;
-    const size_t in_bytes = 32ull * kChunk, out_bytes = (any ? 1ull : 16ull) * kChunk;
+    const size_t in_bytes = 32ull * kChunk;
     const size_t slot_bytes = in_bytes + 16ull * kChunk;
     if (!ctx->pin_buf) {
-        CK(cudaHostAlloc(&ctx->pin_buf, 2 * slot_bytes, cudaHostAllocDefault));
-        for (int k = 0; k < 2; k++) CK(cudaEventCreateWithFlags(&ctx->pin_ev[k], cudaEventDisableTiming));
+        CK(cudaHostAlloc(&ctx->pin_buf, kPinSlots * slot_bytes, cudaHostAllocDefault));
+        for (uint32_t k = 0; k < kPinSlots; k++) CK(cudaEventCreateWithFlags(&ctx->pin_ev[k], cudaEventDisableTiming));
     }
-    (void)out_bytes;
     const uint32_t m = std::min(n, kChunk);
-    CK(ctx->ro.reserve(m));
-    CK(ctx->rd.reserve(m));
+    CK(ctx->ro.reserve(kPinSlots * (size_t)m));
+    CK(ctx->rd.reserve(kPinSlots * (size_t)m));
     if (any) {
-        CK(ctx->hocc.reserve(2ull * m));
+        CK(ctx->hocc.reserve(kPinSlots * (size_t)m));
     } else {
-        CK(ctx->hprim.reserve(2ull * m));
-        CK(ctx->ht.reserve(2ull * m));
-        CK(ctx->hu.reserve(2ull * m));
-        CK(ctx->hv.reserve(2ull * m));
+        CK(ctx->hprim.reserve(kPinSlots * (size_t)m));
+        CK(ctx->ht.reserve(kPinSlots * (size_t)m));
+        CK(ctx->hu.reserve(kPinSlots * (size_t)m));
+        CK(ctx->hv.reserve(kPinSlots * (size_t)m));
     }
     const SceneView sv = ctx->view();
-    cudaStream_t st = ctx->stream;
-    uint32_t *next = ctx->derr.ptr + 1;
     const uint32_t chunks = (n + kChunk - 1) / kChunk;
-    // the results of chunk c, from its slot to the caller's arrays
-    auto copy_out = [&](uint32_t c) -> int {
-        const int s = c & 1;
-        const uint32_t off = c * kChunk, len = std::min(kChunk, n - off);
-        unsigned char *slot = (unsigned char *)ctx->pin_buf + s * slot_bytes + in_bytes;
-        CK(cudaEventSynchronize(ctx->pin_ev[s]));
-        if (any) {
-            host_copy(occ + off, slot, len);
-        } else {
-            host_copy(prim + off, slot, 4ull * len);
-            host_copy(t + off, slot + 4ull * kChunk, 4ull * len);
-            host_copy(u + off, slot + 8ull * kChunk, 4ull * len);
-            host_copy(v + off, slot + 12ull * kChunk, 4ull * len);
+    cudaStream_t ss[kPinSlots] = {ctx->stream, ctx->stream, ctx->stream};
+    if (chunks > 1) {
+        for (int k = 0; k < 2; k++)
+            if (!ctx->side[k]) CK(cudaStreamCreateWithFlags(&ctx->side[k], cudaStreamNonBlocking));
+        if (!ctx->side_ev[2]) CK(cudaEventCreateWithFlags(&ctx->side_ev[2], cudaEventDisableTiming));
+        // the side streams start after everything already queued on the main one
+        CK(cudaEventRecord(ctx->side_ev[2], ctx->stream));
+        for (int k = 0; k < 2; k++) {
+            CK(cudaStreamWaitEvent(ctx->side[k], ctx->side_ev[2], 0));
+            ss[1 + k] = ctx->side[k];
         }
-        return ILG_OK;
+    }
+    auto slot_of = [&](uint32_t c) { return (unsigned char *)ctx->pin_buf + (c % kPinSlots) * slot_bytes; };
+    // the copies from chunk c's slot to the caller's hit arrays
+    auto out_segs = [&](uint32_t c, CopySeg *seg) -> int {
+        const uint32_t off = c * kChunk, len = std::min(kChunk, n - off);
+        const unsigned char *out = slot_of(c) + in_bytes;
+        if (any) {
+            seg[0] = {occ + off, out, len};
+            return 1;
+        }
+        seg[0] = {prim + off, out, 4ull * len};
+        seg[1] = {t + off, out + 4ull * kChunk, 4ull * len};
+        seg[2] = {u + off, out + 8ull * kChunk, 4ull * len};
+        seg[3] = {v + off, out + 12ull * kChunk, 4ull * len};
+        return 4;
     };
     for (uint32_t c = 0; c < chunks; c++) {
-        const int s = c & 1;
-        if (c >= 2) {
-            int rc = copy_out(c - 2);
-            if (rc) return rc;
-        }
+        const uint32_t s = c % kPinSlots;
+        cudaStream_t st = ss[s];
         const uint32_t off = c * kChunk, len = std::min(kChunk, n - off);
-        unsigned char *slot = (unsigned char *)ctx->pin_buf + s * slot_bytes;
-        host_copy(slot, o4 + 4ull * off, 16ull * len);
-        host_copy(slot + 16ull * kChunk, d4 + 4ull * off, 16ull * len);
-        // device buffers: rays shared (the previous chunk's kernel is ordered before
-        // this copy on the stream), hits per slot (read back by the slot's copy)
-        float4 *dro = ctx->ro.ptr, *drd = ctx->rd.ptr;
+        unsigned char *slot = slot_of(c);
+        CopySeg seg[6];
+        int nseg = 0;
+        if (c >= kPinSlots) {
+            // the slot's previous chunk has left the device (its download was
+            // the last of its work on this stream)
+            CK(cudaEventSynchronize(ctx->pin_ev[s]));
+            nseg = out_segs(c - kPinSlots, seg);
+        }
+        seg[nseg++] = {slot, o4 + 4ull * off, 16ull * len};
+        seg[nseg++] = {slot + 16ull * kChunk, d4 + 4ull * off, 16ull * len};
+        pool_copy_ctx(ctx, seg, nseg);
+        float4 *dro = ctx->ro.ptr + (size_t)s * m, *drd = ctx->rd.ptr + (size_t)s * m;
+        uint32_t *next = ctx->derr.ptr + 1 + s;  // ray counter of this stream's persistent kernels
         CK(cudaMemcpyAsync(dro, slot, 16ull * len, cudaMemcpyHostToDevice, st));
         CK(cudaMemcpyAsync(drd, slot + 16ull * kChunk, 16ull * len, cudaMemcpyHostToDevice, st));
         unsigned char *out = slot + in_bytes;
@@ -183,9 +190,12 @@ int query_host_pageable_run(ilg_ctx *ctx, const float *o4, const float *d4, uint
         }
         CK(cudaEventRecord(ctx->pin_ev[s], st));
     }
-    for (uint32_t c = chunks >= 2 ? chunks - 2 : 0; c < chunks; c++) {
-        int rc = copy_out(c);
-        if (rc) return rc;
+    // the last chunks' hits, in order
+    for (uint32_t c = chunks > kPinSlots ? chunks - kPinSlots : 0; c < chunks; c++) {
+        CK(cudaEventSynchronize(ctx->pin_ev[c % kPinSlots]));
+        CopySeg seg[4];
+        const int nseg = out_segs(c, seg);
+        pool_copy_ctx(ctx, seg, nseg);
     }
     return ctx->check_device_error();
 }
@@ -196,7 +206,11 @@ int query_host_pageable(ilg_ctx *ctx, const float *o4, const float *d4, uint32_t
     const int rc = query_host_pageable_run(ctx, o4, d4, n, prim, t, u, v, occ, wt);
     // after a failure, copies of this call may still be in flight into the
     // page-locked slots that the next call fills from the host
-    if (rc != ILG_OK) cudaStreamSynchronize(ctx->stream);
+    if (rc != ILG_OK) {
+        cudaStreamSynchronize(ctx->stream);
+        for (auto sd : ctx->side)
+            if (sd) cudaStreamSynchronize(sd);
+    }
     return rc;
 }
 
@@ -335,6 +349,7 @@ int ilg_destroy(ilg_ctx *ctx)
     for (auto e : ctx->pin_ev)
         if (e) cudaEventDestroy(e);
     if (ctx->pin_buf) cudaFreeHost(ctx->pin_buf);
+    delete ctx->host_pool;
     for (auto s : ctx->side)
         if (s) cudaStreamDestroy(s);
     cudaStreamDestroy(ctx->stream);

@@ -13,6 +13,7 @@
 #include "postproc.cuh"
 
 namespace ilg {
+class HostPool;  // hostpool.h
 // noalloc.cu: the device address of the allocation-free query's fixed array
 // on the current device, with the traversal kernel it launches loaded.
 cudaError_t noalloc_prepare(void **out);
@@ -54,9 +55,11 @@ struct ilg_ctx {
 
     // staging for host-pointer queries
     ilg::DevBuf<float4> ro, rd;
-    // two page-locked slots for queries from pageable host memory (made on first use)
+    // three page-locked slots for queries from pageable host memory, and the
+    // host threads that copy through them (made on first use)
     void *pin_buf = nullptr;
-    cudaEvent_t pin_ev[2] = {nullptr, nullptr};
+    cudaEvent_t pin_ev[3] = {nullptr, nullptr, nullptr};
+    ilg::HostPool *host_pool = nullptr;
     ilg::DevBuf<int32_t> hprim;
     ilg::DevBuf<float> ht, hu, hv;
     ilg::DevBuf<uint8_t> hocc;

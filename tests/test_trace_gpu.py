@@ -219,16 +219,16 @@ def test_watertight_mode_closes_the_reference_edge_cracks(oracle):
 
 def test_pageable_host_buffers_give_the_pinned_results():
     """Host rays and hits in pageable memory (plain numpy) go through the
-    context's two page-locked slots in chunks of 524,288 rays; the answers
+    context's three page-locked slots in chunks of 524,288 rays; the answers
     must equal those from page-locked buffers, for both queries and both
-    triangle tests, on a ragged three-chunk batch."""
+    triangle tests, on a ragged six-chunk batch (every slot used twice)."""
     import torch
     from illuminaprt_b200.ilg import GpuSpace
     pos, idx = scenes.heightfield(256, 128, 0.2, 4)
     sp = GpuSpace()
     sp.initialise(pos, idx)
     sp.build()
-    o4, d4 = scenes.incoherent_rays(pos, idx, 1_300_001, 6)
+    o4, d4 = scenes.incoherent_rays(pos, idx, 2_700_001, 6)
     po, pd = torch.from_numpy(o4).pin_memory(), torch.from_numpy(d4).pin_memory()
     n = o4.shape[0]
     for wt in (False, True):
