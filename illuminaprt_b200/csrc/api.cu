@@ -110,7 +110,11 @@ int query_host_pageable_run(ilg_ctx *ctx, const float *o4, const float *d4, uint
         CK(cudaHostAlloc(&ctx->pin_buf, kPinSlots * slot_bytes, cudaHostAllocDefault));
         for (uint32_t k = 0; k < kPinSlots; k++) CK(cudaEventCreateWithFlags(&ctx->pin_ev[k], cudaEventDisableTiming));
     }
-    const uint32_t m = std::min(n, kChunk);
+    // chunks of 512 K rays (the slots' size), or of an eighth of the batch,
+    // 256 K rays at least, when that is smaller: short batches then still
+    // run in enough chunks to overlap host copies and device work
+    const uint32_t chunk = std::min<uint32_t>(kChunk, std::max<uint32_t>(1u << 18, ((n + 7u) / 8u + 127u) & ~127u));
+    const uint32_t m = std::min(n, chunk);
     CK(ctx->ro.reserve(kPinSlots * (size_t)m));
     CK(ctx->rd.reserve(kPinSlots * (size_t)m));
     if (any) {
@@ -122,7 +126,7 @@ int query_host_pageable_run(ilg_ctx *ctx, const float *o4, const float *d4, uint
         CK(ctx->hv.reserve(kPinSlots * (size_t)m));
     }
     const SceneView sv = ctx->view();
-    const uint32_t chunks = (n + kChunk - 1) / kChunk;
+    const uint32_t chunks = (n + chunk - 1) / chunk;
     cudaStream_t ss[kPinSlots] = {ctx->stream, ctx->stream, ctx->stream};
     if (chunks > 1) {
         for (int k = 0; k < 2; k++)
@@ -138,7 +142,7 @@ int query_host_pageable_run(ilg_ctx *ctx, const float *o4, const float *d4, uint
     auto slot_of = [&](uint32_t c) { return (unsigned char *)ctx->pin_buf + (c % kPinSlots) * slot_bytes; };
     // the copies from chunk c's slot to the caller's hit arrays
     auto out_segs = [&](uint32_t c, CopySeg *seg) -> int {
-        const uint32_t off = c * kChunk, len = std::min(kChunk, n - off);
+        const uint32_t off = c * chunk, len = std::min(chunk, n - off);
         const unsigned char *out = slot_of(c) + in_bytes;
         if (any) {
             seg[0] = {occ + off, out, len};
@@ -153,7 +157,7 @@ int query_host_pageable_run(ilg_ctx *ctx, const float *o4, const float *d4, uint
     for (uint32_t c = 0; c < chunks; c++) {
         const uint32_t s = c % kPinSlots;
         cudaStream_t st = ss[s];
-        const uint32_t off = c * kChunk, len = std::min(kChunk, n - off);
+        const uint32_t off = c * chunk, len = std::min(chunk, n - off);
         unsigned char *slot = slot_of(c);
         CopySeg seg[6];
         int nseg = 0;

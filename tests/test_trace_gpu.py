@@ -219,9 +219,10 @@ def test_watertight_mode_closes_the_reference_edge_cracks(oracle):
 
 def test_pageable_host_buffers_give_the_pinned_results():
     """Host rays and hits in pageable memory (plain numpy) go through the
-    context's three page-locked slots in chunks of 524,288 rays; the answers
-    must equal those from page-locked buffers, for both queries and both
-    triangle tests, on a ragged six-chunk batch (every slot used twice)."""
+    context's three page-locked slots in chunks (here eight of 337,536 rays);
+    the answers must equal those from page-locked buffers, for both queries
+    and both triangle tests, on a ragged batch that uses every slot more
+    than once."""
     import torch
     from illuminaprt_b200.ilg import GpuSpace
     pos, idx = scenes.heightfield(256, 128, 0.2, 4)
