@@ -106,14 +106,13 @@ int query_host_pageable_run(ilg_ctx *ctx, const float *o4, const float *d4, uint
     constexpr uint32_t kChunk = 1u << 19;
     const size_t in_bytes = 32ull * kChunk;
     const size_t slot_bytes = in_bytes + 16ull * kChunk;
-    if (!ctx->pin_buf) {
-        CK(cudaHostAlloc(&ctx->pin_buf, kPinSlots * slot_bytes, cudaHostAllocDefault));
-        for (uint32_t k = 0; k < kPinSlots; k++) CK(cudaEventCreateWithFlags(&ctx->pin_ev[k], cudaEventDisableTiming));
-    }
+    if (!ctx->pin_buf) CK(cudaHostAlloc(&ctx->pin_buf, kPinSlots * slot_bytes, cudaHostAllocDefault));
+    for (uint32_t k = 0; k < kPinSlots; k++)
+        if (!ctx->pin_ev[k]) CK(cudaEventCreateWithFlags(&ctx->pin_ev[k], cudaEventDisableTiming));
     // chunks of 512 K rays (the slots' size), or of an eighth of the batch,
     // 256 K rays at least, when that is smaller: short batches then still
     // run in enough chunks to overlap host copies and device work
-    const uint32_t chunk = std::min<uint32_t>(kChunk, std::max<uint32_t>(1u << 18, ((n + 7u) / 8u + 127u) & ~127u));
+    const uint32_t chunk = (uint32_t)std::min<uint64_t>(kChunk, std::max<uint64_t>(1u << 18, ((n + 7ull) / 8u + 127u) & ~127ull));
     const uint32_t m = std::min(n, chunk);
     CK(ctx->ro.reserve(kPinSlots * (size_t)m));
     CK(ctx->rd.reserve(kPinSlots * (size_t)m));
@@ -126,7 +125,7 @@ int query_host_pageable_run(ilg_ctx *ctx, const float *o4, const float *d4, uint
         CK(ctx->hv.reserve(kPinSlots * (size_t)m));
     }
     const SceneView sv = ctx->view();
-    const uint32_t chunks = (n + chunk - 1) / chunk;
+    const uint32_t chunks = (uint32_t)((n + (uint64_t)chunk - 1) / chunk);
     cudaStream_t ss[kPinSlots] = {ctx->stream, ctx->stream, ctx->stream};
     if (chunks > 1) {
         for (int k = 0; k < 2; k++)
