@@ -69,3 +69,34 @@ def test_binding_constants_match_the_header():
     # the option structs have the header's layout size
     assert ctypes.sizeof(ilg.ilg_render_opts) == 4 * (7 + 3 + 6)
     assert ctypes.sizeof(ilg.ilg_material) == 32
+
+
+def test_plain_c_client_builds_and_links(tmp_path):
+    # the header is plain C99 (what a cgo, JNI or C host includes) and a C
+    # program links against the library; without a GPU, ilg_create fails
+    # with ILG_ECUDA and leaves the handle null
+    import shutil
+    import subprocess
+    from illuminaprt_b200 import build
+    if shutil.which("gcc") is None:
+        pytest.skip("no gcc")
+    lib = build.build()
+    src = tmp_path / "client.c"
+    src.write_text(
+        '#include "ilg.h"\n#include <stdio.h>\n'
+        "int main(void) {\n"
+        "    ilg_ctx *ctx = 0;\n    ilg_opts o = {0};\n"
+        "    int rc = ilg_create(&ctx, &o);\n"
+        '    printf("create %d %d %s\\n", rc, ctx != 0, ilg_last_error(ctx));\n'
+        "    if (rc == ILG_OK) ilg_destroy(ctx);\n    return 0;\n}\n")
+    exe = tmp_path / "client"
+    libdir = os.path.dirname(lib)
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Wextra", "-Werror", "-pedantic", "-I",
+                    os.path.join(ROOT, "include"), str(src), "-L", libdir, "-l:" + os.path.basename(lib),
+                    "-Wl,-rpath," + libdir, "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120, check=True).stdout.split()
+    assert out[0] == "create"
+    if not cuda_available():
+        assert out[1] == "3" and out[2] == "0"  # ILG_ECUDA, no handle
+    else:
+        assert out[1] == "0" and out[2] == "1"
